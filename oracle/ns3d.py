@@ -1,0 +1,855 @@
+"""CPU oracle for the 3D staggered-grid Navier-Stokes step -- TEST INFRASTRUCTURE ONLY.
+
+This module is the checker, never the product: only ``tests/``, ``__graft_entry__.smoke()``
+and the ``cpu_baseline`` / ``--impl reference`` legs of ``bench.py`` may import it.  The
+CUDA path in ``aerolume_b200`` never calls into it.
+
+It restates, in numpy, the reference's plain-torch 3D step with the placed physics that
+the sm_100a kernels implement (Aerolume ``src/aerolume/solvers/ns3d``):
+
+* ``step3d_phys``        core.py:765-883   SSP-RK3 with a projection after every stage
+* ``pad3``/ghost rules   core.py:147-272   two ghost layers, rules composed axis by axis
+* ``advection3``         core.py:331-390   upwind3 / central conservative advection
+* ``sgs_divergence3d``   core.py:400-524   Smagorinsky / WALE / Vreman eddy viscosity
+* ``penalise3d``         core.py:615-634   implicit Brinkman penalisation on the window
+* ``force_coefficients`` core.py:653-678
+* ``PoissonSolver3D``    poisson.py:74-157 exact solve in the per-axis eigenbases
+* ``ThermalOps``         physics.py:494-790 heat equation, buoyancy, heat rates
+* ``Physics3D.dt_rule``  physics.py:1230-1262
+* smoke                  dye.py:232-312    MUSCL / van Leer advection, solids, nozzles
+
+Parity is pinned: ``tests/test_oracle_golden.py`` checks this module against golden
+vectors that ``tests/golden/make_golden.py`` produced by running the reference itself
+(float64 to 1e-12, float32 to round-off).
+
+Inputs are duck-typed objects with the reference's attribute names (see
+``aerolume_b200.ns3d`` for the concrete containers); arrays are numpy, C order
+``(nz, ny, nx)`` with the staggered shapes of core.py:11-14.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+SSP_RK3 = ((0.0, 1.0), (0.75, 0.25), (1.0 / 3.0, 2.0 / 3.0))     # ns2d/core.py:47
+FORCE_WEIGHTS = (1.0 / 6.0, 2.0 / 3.0, 1.0)                       # ns2d/core.py:49
+VISCOUS_DT = 1.0 / 6.0                                            # ns3d/core.py:51
+THETA_COURANT_MAX = 0.5                                           # ns3d/physics.py:82
+DYE_FLOOR = 1e-8                                                  # ns3d/dye.py:63
+_SQRT_EPS = 1e-30                                                 # ns3d/core.py:54
+
+
+def lerp(start, end, weight):
+    """torch.lerp's two-branch formula (the reference's RK stage blend, core.py:823)."""
+    T = start.dtype.type
+    if weight < 0.5:
+        return start + T(weight) * (end - start)
+    return end - (end - start) * T(1.0 - weight)
+
+
+def _narrow(x, dim, start, length):
+    sl = [slice(None)] * x.ndim
+    sl[dim] = slice(start, start + length)
+    return x[tuple(sl)]
+
+
+# ---------------------------------------------------------------------------
+# ghost cells (core.py:223-278)
+# ---------------------------------------------------------------------------
+
+def _ghost_slabs(x, dim, lo, hi):
+    """The two ghost layers below and above ``x`` along ``dim`` (core.py:223-246)."""
+    n = x.shape[dim]
+
+    def make(rule, side):
+        kind, val = rule
+        low = side == "lo"
+        if kind == "edge":
+            return _narrow(x, dim, 0 if low else n - 1, 1)
+        if kind in ("even", "odd", "affine"):
+            m = np.flip(_narrow(x, dim, 0 if low else n - 2, 2), dim)
+            if kind == "even":
+                return m
+            if kind == "odd":
+                return -m
+            return x.dtype.type(2.0 * val) - m
+        if kind == "face_odd":
+            return -np.flip(_narrow(x, dim, 1 if low else n - 3, 2), dim)
+        if kind == "periodic_cell":
+            return _narrow(x, dim, n - 2 if low else 0, 2)
+        if kind == "periodic_face":
+            return _narrow(x, dim, n - 3 if low else 1, 2)
+        raise ValueError(kind)
+
+    return make(lo, "lo"), make(hi, "hi")
+
+
+def pad3(x, rules):
+    """``x`` with two ghost layers per side, x first, then y, then z (core.py:249-272)."""
+    nz, ny, nx = x.shape
+    out = np.empty((nz + 4, ny + 4, nx + 4), dtype=x.dtype)
+    rx, ry, rz = rules
+    lo, hi = _ghost_slabs(x, 2, *rx)
+    out[2:-2, 2:-2, 2:-2] = x
+    out[2:-2, 2:-2, 0:2] = lo
+    out[2:-2, 2:-2, nx + 2:] = hi
+    mid = out[2:-2]
+    lo, hi = _ghost_slabs(mid[:, 2:-2], 1, *ry)
+    out[2:-2, 0:2] = lo
+    out[2:-2, ny + 2:] = hi
+    lo, hi = _ghost_slabs(out[2:-2], 0, *rz)
+    out[0:2] = lo
+    out[nz + 2:] = hi
+    return out
+
+
+def pad_velocity(u, v, w, ops):
+    g = ops.ghost
+    return pad3(u, g["u"]), pad3(v, g["v"]), pad3(w, g["w"])
+
+
+def inlet_outlet(u, ops):
+    """Inlet profile and outlet mass balance (core.py:281-297)."""
+    u = u.copy()
+    if ops.closed:
+        u[..., 0] = 0.0
+        u[..., -1] = 0.0
+        return u
+    T = u.dtype.type
+    corr = (ops.u_inlet.sum(dtype=u.dtype) - u[..., -1].sum(dtype=u.dtype)) * T(1.0 / (ops.nz * ops.ny))
+    u[..., -1] = u[..., -1] + corr
+    u[..., 0] = ops.u_inlet
+    return u
+
+
+def sync_periodic(u, v, w, ops):
+    """Duplicate faces of periodic axes (core.py:300-309)."""
+    px, py, pz = ops.periodic_axes
+    if px:
+        u = u.copy()
+        u[..., -1] = u[..., 0]
+    if py:
+        v = v.copy()
+        v[:, -1] = v[:, 0]
+    if pz:
+        w = w.copy()
+        w[-1] = w[0]
+    return u, v, w
+
+
+def apply_boundary_values(u, v, w, ops):
+    """All Dirichlet values (core.py:312-324)."""
+    px, py, pz = ops.periodic_axes
+    if not px:
+        u = inlet_outlet(u, ops)
+    if not py:
+        v = v.copy()
+        v[:, 0] = 0.0
+        v[:, -1] = 0.0
+    if not pz:
+        w = w.copy()
+        w[0] = 0.0
+        w[-1] = 0.0
+    return sync_periodic(u, v, w, ops)
+
+
+# ---------------------------------------------------------------------------
+# right-hand side (core.py:331-570)
+# ---------------------------------------------------------------------------
+
+def face_flux(vsum, a, b, c, d, upwind):
+    """Scaled upwind3 / central flux through the b|c face (core.py:331-345)."""
+    T = b.dtype.type
+    s = b + c
+    vsum = s if vsum is None else vsum
+    if not upwind:
+        return vsum * s
+    cen = s + T(-1.0 / 7.0) * (a + d)
+    dis = (b - c) + T(-1.0 / 3.0) * (a - d)
+    return vsum * cen + T(3.0 / 7.0) * np.abs(vsum) * dis
+
+
+def advection_scale(ops):
+    return (7.0 / 24.0 if ops.advection == "upwind3" else 0.25) / ops.h        # core.py:348-350
+
+
+def advection3(U, V, W, ops):
+    """-div(u u) at the u-, v- and w-faces (core.py:353-390)."""
+    nz, ny, nx = ops.nz, ops.ny, ops.nx
+    up = ops.advection == "upwind3"
+    k = U.dtype.type(advection_scale(ops))
+    m = slice(2, -2)
+    fx = face_flux(None, U[m, m, 0:nx + 2], U[m, m, 1:nx + 3], U[m, m, 2:nx + 4], U[m, m, 3:nx + 5], up)
+    au = fx[..., :-1] - fx[..., 1:]
+    vs = V[m, 2:ny + 3, 1:nx + 2] + V[m, 2:ny + 3, 2:nx + 3]
+    g = face_flux(vs, U[m, 0:ny + 1, m], U[m, 1:ny + 2, m], U[m, 2:ny + 3, m], U[m, 3:ny + 4, m], up)
+    au = au + (g[:, :-1] - g[:, 1:])
+    ws = W[2:nz + 3, m, 1:nx + 2] + W[2:nz + 3, m, 2:nx + 3]
+    g = face_flux(ws, U[0:nz + 1, m, m], U[1:nz + 2, m, m], U[2:nz + 3, m, m], U[3:nz + 4, m, m], up)
+    au = (au + (g[:-1] - g[1:])) * k
+    us = U[m, 1:ny + 2, m] + U[m, 2:ny + 3, m]
+    g = face_flux(us, V[m, m, 0:nx + 1], V[m, m, 1:nx + 2], V[m, m, 2:nx + 3], V[m, m, 3:nx + 4], up)
+    av = g[..., :-1] - g[..., 1:]
+    g = face_flux(None, V[m, 0:ny + 2, m], V[m, 1:ny + 3, m], V[m, 2:ny + 4, m], V[m, 3:ny + 5, m], up)
+    av = av + (g[:, :-1] - g[:, 1:])
+    ws = W[2:nz + 3, 1:ny + 2, m] + W[2:nz + 3, 2:ny + 3, m]
+    g = face_flux(ws, V[0:nz + 1, m, m], V[1:nz + 2, m, m], V[2:nz + 3, m, m], V[3:nz + 4, m, m], up)
+    av = (av + (g[:-1] - g[1:])) * k
+    us = U[1:nz + 2, m, m] + U[2:nz + 3, m, m]
+    g = face_flux(us, W[m, m, 0:nx + 1], W[m, m, 1:nx + 2], W[m, m, 2:nx + 3], W[m, m, 3:nx + 4], up)
+    aw = g[..., :-1] - g[..., 1:]
+    vs = V[1:nz + 2, m, m] + V[2:nz + 3, m, m]
+    g = face_flux(vs, W[m, 0:ny + 1, m], W[m, 1:ny + 2, m], W[m, 2:ny + 3, m], W[m, 3:ny + 4, m], up)
+    aw = aw + (g[:, :-1] - g[:, 1:])
+    g = face_flux(None, W[0:nz + 2, m, m], W[1:nz + 3, m, m], W[2:nz + 4, m, m], W[3:nz + 5, m, m], up)
+    aw = (aw + (g[:-1] - g[1:])) * k
+    return au, av, aw
+
+
+def laplacian_padded(P):
+    """h^2 times the 7-point Laplacian on the interior (core.py:393-397)."""
+    m = slice(2, -2)
+    ring = (P[m, m, 3:-1] + P[m, m, 1:-3]) + (P[m, 3:-1, m] + P[m, 1:-3, m]) + (P[3:-1, m, m] + P[1:-3, m, m])
+    return ring - P.dtype.type(6.0) * P[m, m, m]
+
+
+def velocity_gradient(U, V, W, h):
+    """Gradient tensor at centres -1..n and edge shears (core.py:400-434)."""
+    nz, ny, nx = U.shape[0] - 4, U.shape[1] - 4, U.shape[2] - 5
+    inv = U.dtype.type(1.0 / h)
+    q = U.dtype.type(0.25)
+    g11 = (U[1:nz + 3, 1:ny + 3, 2:nx + 4] - U[1:nz + 3, 1:ny + 3, 1:nx + 3]) * inv
+    g22 = (V[1:nz + 3, 2:ny + 4, 1:nx + 3] - V[1:nz + 3, 1:ny + 3, 1:nx + 3]) * inv
+    g33 = (W[2:nz + 4, 1:ny + 3, 1:nx + 3] - W[1:nz + 3, 1:ny + 3, 1:nx + 3]) * inv
+    dudy = (U[1:nz + 3, 1:ny + 4, 1:nx + 4] - U[1:nz + 3, 0:ny + 3, 1:nx + 4]) * inv
+    dvdx = (V[1:nz + 3, 1:ny + 4, 1:nx + 4] - V[1:nz + 3, 1:ny + 4, 0:nx + 3]) * inv
+    dudz = (U[1:nz + 4, 1:ny + 3, 1:nx + 4] - U[0:nz + 3, 1:ny + 3, 1:nx + 4]) * inv
+    dwdx = (W[1:nz + 4, 1:ny + 3, 1:nx + 4] - W[1:nz + 4, 1:ny + 3, 0:nx + 3]) * inv
+    dvdz = (V[1:nz + 4, 1:ny + 4, 1:nx + 3] - V[0:nz + 3, 1:ny + 4, 1:nx + 3]) * inv
+    dwdy = (W[1:nz + 4, 1:ny + 4, 1:nx + 3] - W[1:nz + 4, 0:ny + 3, 1:nx + 3]) * inv
+
+    def a_xy(t):
+        return (t[:, :-1, :-1] + t[:, 1:, :-1] + t[:, :-1, 1:] + t[:, 1:, 1:]) * q
+
+    def a_xz(t):
+        return (t[:-1, :, :-1] + t[1:, :, :-1] + t[:-1, :, 1:] + t[1:, :, 1:]) * q
+
+    def a_yz(t):
+        return (t[:-1, :-1] + t[1:, :-1] + t[:-1, 1:] + t[1:, 1:]) * q
+
+    g = ((g11, a_xy(dudy), a_xz(dudz)),
+         (a_xy(dvdx), g22, a_yz(dvdz)),
+         (a_xz(dwdx), a_yz(dwdy), g33))
+    return {"g": g, "sxy": dudy + dvdx, "sxz": dudz + dwdx, "syz": dvdz + dwdy}
+
+
+def traceless(g):
+    """g33 := -(g11 + g22) (core.py:437-445)."""
+    return (g[0], g[1], (g[2][0], g[2][1], -(g[0][0] + g[1][1])))
+
+
+def eddy_viscosity3d(g, ops):
+    """Smagorinsky / WALE / Vreman eddy viscosity (core.py:448-482)."""
+    T = g[0][0].dtype.type
+    delta2 = ops.h * ops.h
+    c = ops.les_c
+    s = [[T(0.5) * (g[i][j] + g[j][i]) for j in range(3)] for i in range(3)]
+    ss = 0
+    for i in range(3):
+        for j in range(3):
+            ss = ss + s[i][j] * s[i][j]
+    if ops.turbulence == "smagorinsky":
+        return T(c * c * delta2) * np.sqrt(T(2.0) * ss + T(_SQRT_EPS))
+    if ops.turbulence == "wale":
+        g2 = [[sum(g[i][k] * g[k][j] for k in range(3)) for j in range(3)] for i in range(3)]
+        tr3 = (g2[0][0] + g2[1][1] + g2[2][2]) * T(1.0 / 3.0)
+        sd = T(0.0)
+        for i in range(3):
+            for j in range(3):
+                sdij = T(0.5) * (g2[i][j] + g2[j][i])
+                if i == j:
+                    sdij = sdij - tr3
+                sd = sd + sdij * sdij
+        sdp = np.maximum(sd, T(0.0))
+        num = sdp ** T(1.5)
+        den = np.maximum(ss, T(0.0)) ** T(2.5) + sdp ** T(1.25) + T(1e-30)
+        return T(c * c * delta2) * num / den
+    if ops.turbulence == "vreman":
+        b = [[sum(g[i][m] * g[j][m] for m in range(3)) for j in range(3)] for i in range(3)]
+        bb = np.maximum(b[0][0] * b[1][1] - b[0][1] * b[0][1] + b[0][0] * b[2][2] - b[0][2] * b[0][2]
+                        + b[1][1] * b[2][2] - b[1][2] * b[1][2], T(0.0))
+        aa = 0
+        for i in range(3):
+            for j in range(3):
+                aa = aa + g[i][j] * g[i][j]
+        return T(c * delta2) * np.sqrt(bb / (aa + T(1e-30)) + T(_SQRT_EPS))
+    raise ValueError(ops.turbulence)
+
+
+def sgs_divergence3d(U, V, W, geom, ops):
+    """div(2 nu_t S) on the faces, nu_t (with ghost ring) and its max (core.py:485-524)."""
+    nz, ny, nx = ops.nz, ops.ny, ops.nx
+    T = U.dtype.type
+    inv = T(1.0 / ops.h)
+    gr = velocity_gradient(U, V, W, ops.h)
+    g = gr["g"]
+    nut = eddy_viscosity3d(traceless(g), ops)
+    if not geom.empty:
+        k0, k1, j0, j1, i0, i1 = geom.window
+        nut = nut.copy()
+        nut[k0 + 1:k1 + 1, j0 + 1:j1 + 1, i0 + 1:i1 + 1] *= (T(1.0) - geom.chi_c)
+    i = slice(1, -1)
+    q = T(0.25)
+    n_xy = nut[i]
+    n_xy = (n_xy[:, :-1, :-1] + n_xy[:, 1:, :-1] + n_xy[:, :-1, 1:] + n_xy[:, 1:, 1:]) * q
+    n_xz = nut[:, i]
+    n_xz = (n_xz[:-1, :, :-1] + n_xz[1:, :, :-1] + n_xz[:-1, :, 1:] + n_xz[1:, :, 1:]) * q
+    n_yz = nut[:, :, i]
+    n_yz = (n_yz[:-1, :-1] + n_yz[1:, :-1] + n_yz[:-1, 1:] + n_yz[1:, 1:]) * q
+    t12 = n_xy * gr["sxy"][1:nz + 1, 1:ny + 2, 1:nx + 2]
+    t13 = n_xz * gr["sxz"][1:nz + 2, 1:ny + 1, 1:nx + 2]
+    t23 = n_yz * gr["syz"][1:nz + 2, 1:ny + 2, 1:nx + 1]
+    two = T(2.0)
+    t11 = two * nut[i, i] * g[0][0][i, i]
+    t22 = two * nut[i, :, i] * g[1][1][i, :, i]
+    t33 = two * nut[:, i, i] * g[2][2][:, i, i]
+    fu = (t11[..., 1:] - t11[..., :-1] + t12[:, 1:] - t12[:, :-1] + t13[1:] - t13[:-1]) * inv
+    fv = (t12[..., 1:] - t12[..., :-1] + t22[:, 1:] - t22[:, :-1] + t23[1:] - t23[:-1]) * inv
+    fw = (t13[..., 1:] - t13[..., :-1] + t23[:, 1:] - t23[:, :-1] + t33[1:] - t33[:-1]) * inv
+    return fu, fv, fw, nut, nut.max()
+
+
+def boundary_tendencies(u, lu, lv, lw, ops):
+    """Inlet 0, convective outlet, walls 0 (core.py:527-543)."""
+    px, py, pz = ops.periodic_axes
+    T = u.dtype.type
+    lu, lv, lw = lu.copy(), lv.copy(), lw.copy()
+    if not px:
+        out = (u[..., -2] - u[..., -1]) * T(1.0 / ops.h)
+        if ops.closed:
+            out = np.zeros_like(out)
+        lu[..., 0] = 0.0
+        lu[..., -1] = out
+    if not py:
+        lv[:, 0] = 0.0
+        lv[:, -1] = 0.0
+    if not pz:
+        lw[0] = 0.0
+        lw[-1] = 0.0
+    return lu, lv, lw
+
+
+def momentum_rhs3d(u, v, w, geom, ops):
+    """Explicit tendencies, nu_t field and max (core.py:546-570)."""
+    T = u.dtype.type
+    U, V, W = pad_velocity(u, v, w, ops)
+    au, av, aw = advection3(U, V, W, ops)
+    nu_h2 = T(T(ops.nu_value) * T(1.0 / ops.h ** 2))
+    lu = au + nu_h2 * laplacian_padded(U)
+    lv = av + nu_h2 * laplacian_padded(V)
+    lw = aw + nu_h2 * laplacian_padded(W)
+    nut = nut_max = None
+    if ops.turbulence != "none":
+        fu, fv, fw, nut, nut_max = sgs_divergence3d(U, V, W, geom, ops)
+        lu, lv, lw = lu + fu, lv + fv, lw + fw
+    lu, lv, lw = boundary_tendencies(u, lu, lv, lw, ops)
+    return lu, lv, lw, nut, nut_max
+
+
+# ---------------------------------------------------------------------------
+# projection (core.py:577-612; poisson.py:74-157)
+# ---------------------------------------------------------------------------
+
+def divergence3d(u, v, w, h):
+    return ((u[..., 1:] - u[..., :-1]) + (v[:, 1:] - v[:, :-1]) + (w[1:] - w[:-1])) * u.dtype.type(1.0 / h)
+
+
+def neumann_basis(n):
+    """Orthonormal DCT-II matrix and eigenvalues for h = 1 (poisson.py:74-81)."""
+    k = np.arange(n, dtype=np.float64)[:, None]
+    j = np.arange(n, dtype=np.float64)[None, :]
+    q = np.cos(math.pi * k * (j + 0.5) / n) * math.sqrt(2.0 / n)
+    q[0] *= math.sqrt(0.5)
+    lam = 2.0 * np.cos(math.pi * np.arange(n, dtype=np.float64) / n) - 2.0
+    return q, lam
+
+
+def periodic_basis(n):
+    """Orthonormal discrete Hartley matrix and periodic eigenvalues (poisson.py:84-90)."""
+    k = np.arange(n, dtype=np.float64)
+    ang = 2.0 * math.pi * k[:, None] * k[None, :] / n
+    q = (np.cos(ang) + np.sin(ang)) / math.sqrt(n)
+    lam = 2.0 * np.cos(2.0 * math.pi * k / n) - 2.0
+    return q, lam
+
+
+class PoissonSolver3D:
+    """Exact ``L psi = f`` with zero mean (poisson.py:93-157)."""
+
+    def __init__(self, nx, ny, nz, h, periodic, dtype):
+        self.shape = (nz, ny, nx)
+        mats, lams = [], []
+        for n, per in zip((nx, ny, nz), periodic):
+            q, lam = periodic_basis(n) if per else neumann_basis(n)
+            mats.append(q.astype(dtype))
+            lams.append(lam / (h * h))
+        self.qx, self.qy, self.qz = mats
+        lx, ly, lz = lams
+        lam = lz[:, None, None] + ly[None, :, None] + lx[None, None, :]
+        inv = np.where(lam != 0, 1.0 / np.where(lam != 0, lam, 1.0), 0.0)
+        inv[0, 0, 0] = 0.0
+        self.inv_lam = inv.astype(dtype)
+
+    def solve(self, f):
+        nz, ny, nx = f.shape
+        a = (f.reshape(-1, nx) @ self.qx.T).reshape(nz, ny, nx)
+        a = np.matmul(self.qy, a)
+        a = (self.qz @ a.reshape(nz, -1)).reshape(nz, ny, nx)
+        a = a * self.inv_lam
+        a = (self.qz.T @ a.reshape(nz, -1)).reshape(nz, ny, nx)
+        a = np.matmul(self.qy.T, a)
+        return (a.reshape(-1, nx) @ self.qx).reshape(nz, ny, nx)
+
+    def laplacian(self, psi, h, periodic):
+        """The discrete operator itself (poisson.py:160-173)."""
+        pe = psi
+        for dim, per in zip((2, 1, 0), periodic):
+            n = pe.shape[dim]
+            if per:
+                lo, hi = _narrow(pe, dim, n - 1, 1), _narrow(pe, dim, 0, 1)
+            else:
+                lo, hi = _narrow(pe, dim, 0, 1), _narrow(pe, dim, n - 1, 1)
+            pe = np.concatenate([lo, pe, hi], axis=dim)
+        c = pe[1:-1, 1:-1, 1:-1]
+        ring = (pe[1:-1, 1:-1, 2:] + pe[1:-1, 1:-1, :-2] + pe[1:-1, 2:, 1:-1] + pe[1:-1, :-2, 1:-1]
+                + pe[2:, 1:-1, 1:-1] + pe[:-2, 1:-1, 1:-1])
+        return (ring - 6.0 * c) / (h * h)
+
+
+def pressure_gradient(psi, ops):
+    """grad psi on every face, zero on non-periodic boundary faces (core.py:582-601)."""
+    T = psi.dtype.type
+    inv = T(1.0 / ops.h)
+    px, py, pz = ops.periodic_axes
+    nz, ny, nx = psi.shape
+    if px:
+        gx = (psi - np.roll(psi, 1, axis=2)) * inv
+        gx = np.concatenate([gx, gx[..., :1]], axis=2)
+    else:
+        gx = np.zeros((nz, ny, nx + 1), psi.dtype)
+        gx[..., 1:-1] = (psi[..., 1:] - psi[..., :-1]) * inv
+    if py:
+        gy = (psi - np.roll(psi, 1, axis=1)) * inv
+        gy = np.concatenate([gy, gy[:, :1]], axis=1)
+    else:
+        gy = np.zeros((nz, ny + 1, nx), psi.dtype)
+        gy[:, 1:-1] = (psi[:, 1:] - psi[:, :-1]) * inv
+    if pz:
+        gz = (psi - np.roll(psi, 1, axis=0)) * inv
+        gz = np.concatenate([gz, gz[:1]], axis=0)
+    else:
+        gz = np.zeros((nz + 1, ny, nx), psi.dtype)
+        gz[1:-1] = (psi[1:] - psi[:-1]) * inv
+    return gx, gy, gz
+
+
+def project3d(u, v, w, ops, poisson):
+    psi = poisson.solve(divergence3d(u, v, w, ops.h))
+    gx, gy, gz = pressure_gradient(psi, ops)
+    return u - gx, v - gy, w - gz, psi
+
+
+# ---------------------------------------------------------------------------
+# penalisation, dt, forces (core.py:615-678)
+# ---------------------------------------------------------------------------
+
+def penalise3d(u, v, w, geom, ops, bdt):
+    """Implicit Brinkman on the window; returns fields and increments (core.py:615-634)."""
+    T = u.dtype.type
+    k0, k1, j0, j1, i0, i1 = geom.window
+    k = T(bdt / T(ops.eta))
+    u, v, w = u.copy(), v.copy(), w.copy()
+    uw = u[k0:k1, j0:j1, i0:i1 + 1]
+    vw = v[k0:k1, j0:j1 + 1, i0:i1]
+    ww = w[k0:k1 + 1, j0:j1, i0:i1]
+    un = (uw + k * geom.a_u) / (T(1.0) + k * geom.chi_u)
+    vn = (vw + k * geom.a_v) / (T(1.0) + k * geom.chi_v)
+    wn = (ww + k * geom.a_w) / (T(1.0) + k * geom.chi_w)
+    du, dv, dw = un - uw, vn - vw, wn - ww
+    u[k0:k1, j0:j1, i0:i1 + 1] = un
+    v[k0:k1, j0:j1 + 1, i0:i1] = vn
+    w[k0:k1 + 1, j0:j1, i0:i1] = wn
+    return u, v, w, du, dv, dw
+
+
+def speed_sum(u, v, w):
+    return max(float(np.abs(u).max()) + float(np.abs(v).max()) + float(np.abs(w).max()), 1e-6)
+
+
+def cfl_dt3d(u, v, w, ops, nut_max=None):
+    """CFL and viscous limit (core.py:637-646)."""
+    T = u.dtype.type
+    umax = np.maximum(np.abs(u).max() + np.abs(v).max() + np.abs(w).max(), T(1e-6))
+    dt = T(ops.cfl * ops.h) / umax
+    nu = T(ops.nu_value) if nut_max is None else T(ops.nu_value) + nut_max
+    return np.minimum(dt, T(VISCOUS_DT * ops.h * ops.h) / nu), umax
+
+
+def force_coefficients(acc, geom, ops, dt):
+    """[CD, CS, CL, C_roll, Cm, Cn] per body (core.py:653-678); sums in float64."""
+    acc_u, acc_v, acc_w = (a.astype(np.float64) for a in acc)
+    scale = -(ops.h ** 3) / float(dt)
+    ru = np.einsum("bkzyx,zyx->bk", geom.k_u.astype(np.float64), acc_u) * scale
+    rv = np.einsum("bkzyx,zyx->bk", geom.k_v.astype(np.float64), acc_v) * scale
+    rw = np.einsum("bkzyx,zyx->bk", geom.k_w.astype(np.float64), acc_w) * scale
+    fx, fy, fz = ru[:, 0], rv[:, 0], rw[:, 0]
+    mx, my, mz = rv[:, 1] + rw[:, 1], ru[:, 1] + rw[:, 2], ru[:, 2] + rv[:, 2]
+    if ops.symmetry:
+        dy = ops.moment_ref[1] - ops.y0
+        fx, fz, my = 2.0 * fx, 2.0 * fz, 2.0 * my
+        fy = np.zeros_like(fy)
+        mx = -dy * fz
+        mz = dy * fx
+    q_a = 0.5 * ops.ref_area
+    return np.stack([fx / q_a, fy / q_a, fz / q_a, mx / (q_a * ops.span_ref), my / (q_a * ops.length_ref),
+                     mz / (q_a * ops.span_ref)], axis=1)
+
+
+# ---------------------------------------------------------------------------
+# heat equation (physics.py:494-790)
+# ---------------------------------------------------------------------------
+
+def _theta_ghosts(th, c, dim, side):
+    """Ghost layers of one domain side (physics.py:589-607)."""
+    n = c.shape[dim]
+    lo = side % 2 == 0
+    kind = th.side_kinds[side]
+    T = c.dtype.type
+    if kind == "periodic":
+        return _narrow(c, dim, n - 2, 2) if lo else _narrow(c, dim, 0, 2)
+    if kind == "outflow":
+        e = _narrow(c, dim, 0 if lo else n - 1, 1)
+        return np.concatenate([e, e], axis=dim)
+    mirror = np.flip(_narrow(c, dim, 0, 2), dim) if lo else np.flip(_narrow(c, dim, n - 2, 2), dim)
+    if kind == "adiabatic":
+        return mirror
+    val = T(th.side_vals[side])
+    if kind == "inflow":
+        return np.zeros_like(mirror) + val
+    if kind == "temperature":
+        return T(2.0) * val - mirror
+    wts = np.array([3.0, 1.0] if lo else [1.0, 3.0]) * th.h
+    shape = [1, 1, 1]
+    shape[dim] = 2
+    return mirror + val * wts.astype(c.dtype).reshape(shape)          # heat flux (physics.py:541-548)
+
+
+def theta_pad(th, c):
+    """Two ghost layers on the six faces (physics.py:609-621)."""
+    nz, ny, nx = c.shape
+    P = np.zeros((nz + 4, ny + 4, nx + 4), dtype=c.dtype)
+    m = slice(2, -2)
+    P[m, m, m] = c
+    P[m, m, 0:2] = _theta_ghosts(th, c, 2, 0)
+    P[m, m, nx + 2:] = _theta_ghosts(th, c, 2, 1)
+    P[m, 0:2, m] = _theta_ghosts(th, c, 1, 2)
+    P[m, ny + 2:, m] = _theta_ghosts(th, c, 1, 3)
+    P[0:2, m, m] = _theta_ghosts(th, c, 0, 4)
+    P[nz + 2:, m, m] = _theta_ghosts(th, c, 0, 5)
+    return P
+
+
+def _van_leer(p, q):
+    """dye.py:266-270."""
+    T = p.dtype.type
+    pq = p * q
+    pos = pq > 0
+    return np.where(pos, T(2.0) * pq / np.where(pos, p + q, T(1.0)), T(0.0))
+
+
+def muscl_flux(a, b, c, d, vel):
+    """Upwind MUSCL / van Leer face flux (dye.py:273-277)."""
+    T = b.dtype.type
+    up = b + T(0.5) * _van_leer(b - a, c - b)
+    dn = c - T(0.5) * _van_leer(c - b, d - c)
+    return vel * np.where(vel > 0, up, dn)
+
+
+def face_kappa(th, nut, ops, dtype):
+    """kappa / h on the faces, with nu_t / Pr_t when LES is on (physics.py:624-645)."""
+    T = dtype.type
+    kh = T(th.kappa / ops.h)
+    if nut is None:
+        return kh, kh, kh
+    c = T(0.5 / (th.prt * ops.h))
+    m = slice(1, -1)
+    kx = kh + c * (nut[m, m, :-1] + nut[m, m, 1:])
+    ky = kh + c * (nut[m, :-1, m] + nut[m, 1:, m])
+    kz = kh + c * (nut[:-1, m, m] + nut[1:, m, m])
+    px, py, pz = ops.periodic_axes
+    if not px:
+        kx[..., 0] = kh
+        kx[..., -1] = kh
+    if not py:
+        ky[:, 0] = kh
+        ky[:, -1] = kh
+    if not pz:
+        kz[0] = kh
+        kz[-1] = kh
+    return kx, ky, kz
+
+
+def _face_slices(win, g):
+    k0, k1, j0, j1, i0, i1 = win
+    return (slice(k0, k1 + (1 if g == "w" else 0)), slice(j0, j1 + (1 if g == "v" else 0)),
+            slice(i0, i1 + (1 if g == "u" else 0)))
+
+
+def theta_fluxes(th, c, u, v, w, ops, nut):
+    """Advective minus diffusive theta fluxes on every face (physics.py:647-676)."""
+    nz, ny, nx = c.shape
+    P = theta_pad(th, c)
+    m = slice(2, -2)
+    kx, ky, kz = face_kappa(th, nut, ops, c.dtype)
+    sx = (P[m, m, 0:nx + 1], P[m, m, 1:nx + 2], P[m, m, 2:nx + 3], P[m, m, 3:nx + 4])
+    sy = (P[m, 0:ny + 1, m], P[m, 1:ny + 2, m], P[m, 2:ny + 3, m], P[m, 3:ny + 4, m])
+    sz = (P[0:nz + 1, m, m], P[1:nz + 2, m, m], P[2:nz + 3, m, m], P[3:nz + 4, m, m])
+    out = []
+    for st, vel, kf in ((sx, u, kx), (sy, v, ky), (sz, w, kz)):
+        out.append(muscl_flux(*st, vel) - kf * (st[2] - st[1]))
+    g = th.geom
+    if g.adia is not None:
+        k0, k1, j0, j1, i0, i1 = g.window
+        K, J, I = slice(k0 + 2, k1 + 2), slice(j0 + 2, j1 + 2), slice(i0 + 2, i1 + 2)
+        cu, cv, cw = g.adia
+        dx = P[K, J, i0 + 2:i1 + 3] - P[K, J, i0 + 1:i1 + 2]
+        dy = P[K, j0 + 2:j1 + 3, I] - P[K, j0 + 1:j1 + 2, I]
+        dz = P[k0 + 2:k1 + 3, J, I] - P[k0 + 1:k1 + 2, J, I]
+        for f, kf, d, chi, gg in ((out[0], kx, dx, cu, "u"), (out[1], ky, dy, cv, "v"), (out[2], kz, dz, cw, "w")):
+            sl = _face_slices(g.window, gg)
+            kw = kf if np.ndim(kf) == 0 else kf[sl]
+            f[sl] += kw * chi * d
+    return out
+
+
+def theta_stage(th, c_prev, c0, up, vp, wp, a, bdt, wgt, ops, nut, heat_acc):
+    """One RK stage of theta with the body penalisation (physics.py:678-708)."""
+    T = c_prev.dtype.type
+    fx, fy, fz = theta_fluxes(th, c_prev, up, vp, wp, ops, nut)
+    D = ((fx[..., 1:] - fx[..., :-1]) + (fy[:, 1:] - fy[:, :-1]) + (fz[1:] - fz[:-1])) * T(1.0 / ops.h)
+    base = c_prev if a == 0.0 else lerp(c_prev, c0, a)
+    ch = base - bdt * D
+    bk = T(bdt * T(th.kappa))
+    g = th.geom
+    if g.skin is not None:
+        ch[_face_slices(g.window, "c")] += bk * g.skin
+    if g.chi_t is not None:
+        sl = _face_slices(g.window, "c")
+        win = ch[sl]
+        k = T(bdt / T(th.eta))
+        new = (win + k * g.a_t) / (T(1.0) + k * g.chi_t)
+        inc = (new - win) * T(wgt)
+        ch[sl] = new
+        contrib = np.einsum("bzyx,zyx->b", g.w_t.astype(np.float64), inc.astype(np.float64))
+        for n, b in enumerate(g.t_index):
+            heat_acc[b] += contrib[n]
+    return ch
+
+
+def add_buoyancy(th, wh, theta, bdt, wgt, geom, ops):
+    """Buoyancy after the penalisation and the solids' share (physics.py:744-790)."""
+    T = wh.dtype.type
+    if th.ri == 0.0 or theta is None:
+        return wh, None
+    wh = wh.copy()
+    tf = T(0.5) * (theta[1:] + theta[:-1])
+    wh[1:-1] = wh[1:-1] + tf * T(bdt * T(th.ri))
+    if ops.periodic_axes[2]:
+        edge = (theta[:1] + theta[-1:]) * T(0.5 * th.ri) * bdt
+        wh[:1] = wh[:1] + edge
+        wh[-1:] = wh[-1:] + edge
+    if geom.empty:
+        return wh, None
+    k0, k1, j0, j1, i0, i1 = geom.window
+    lo, hi = max(k0 - 1, 0), min(k1, ops.nz - 1)
+    tc = theta[lo:hi + 1, j0:j1, i0:i1]
+    pz = ops.periodic_axes[2]
+    if k0 == 0:
+        tc = np.concatenate([theta[-1:, j0:j1, i0:i1] if pz else tc[:1], tc], axis=0)
+    if k1 == ops.nz:
+        tc = np.concatenate([tc, theta[:1, j0:j1, i0:i1] if pz else tc[-1:]], axis=0)
+    tw = T(0.5) * (tc[1:] + tc[:-1])
+    vol = th.geom.vol_w if th.geom.vol_w is not None else geom.chi_w
+    share = (tw * vol) * T(bdt * T(th.ri * wgt))
+    return wh, share
+
+
+def thermal_dt_limit(th, nut_max, ops, umax):
+    """Combined advection-diffusion bound (physics.py:723-742)."""
+    T = umax.dtype.type
+    kap = T(th.kappa) if nut_max is None else T(th.kappa) + nut_max / T(th.prt)
+    diff_rate = kap / T(VISCOUS_DT * ops.h * ops.h)
+    return T(1.0) / (umax * T(1.0 / (THETA_COURANT_MAX * ops.h)) + diff_rate)
+
+
+def dt_rule(u0, v0, w0, ops, nut_max, th, theta):
+    """Physics3D.dt_rule without fans, ports or PID (physics.py:1230-1262)."""
+    T = u0.dtype.type
+    dt, umax = cfl_dt3d(u0, v0, w0, ops, nut_max)
+    if th is not None:
+        dt = np.minimum(dt, thermal_dt_limit(th, nut_max, ops, umax))
+        if th.ri != 0.0 and theta is not None:
+            acc = np.maximum(T(abs(th.ri)) * np.abs(theta).max(), T(1e-12))
+            dt = np.minimum(dt, T(ops.cfl) * np.sqrt(T(ops.h) / acc))
+        if getattr(th, "heat_max", None) is not None:
+            s_max = max(T(th.heat_max), T(1e-12))
+            dt = np.minimum(dt, T(1.0) / s_max)
+            if th.ri != 0.0:
+                dt = np.minimum(dt, (T(6.0 * ops.cfl * ops.h) / (T(abs(th.ri)) * s_max)) ** T(1.0 / 3.0))
+    return T(dt)
+
+
+# ---------------------------------------------------------------------------
+# the step (core.py:765-883)
+# ---------------------------------------------------------------------------
+
+class StepResult:
+    """What one step returns: new u, v, w, p, t, dt, per-body coefficients (nb, 6),
+    theta (or None), heat rates (nb) (or None), and the per-stage traces."""
+
+    def __init__(self, **kw):
+        self.__dict__.update(kw)
+
+
+def step3d_phys(u0, v0, w0, t, geom, ops, poisson, *, th=None, theta=None, dt=None, trace=False):
+    """One SSP-RK3 step (core.py:765-883, fixed physics: thermal, buoyancy; no fans/ports/paint)."""
+    T = u0.dtype.type
+    up, vp, wp = u0, v0, w0
+    acc = None
+    psi_w = None
+    thermal = th is not None and theta is not None
+    t0 = tp = theta
+    heat_acc = np.zeros(geom.nbody if not geom.empty else max(geom.nbody, 0), dtype=np.float64)
+    stages = []
+    nut_stage1 = None
+    for s, ((a, b), wgt) in enumerate(zip(SSP_RK3, FORCE_WEIGHTS)):
+        lu, lv, lw, nut, nut_max = momentum_rhs3d(up, vp, wp, geom, ops)
+        if s == 0:
+            nut_stage1 = nut
+            if dt is None:
+                if ops.dt_fixed is not None:
+                    dt = T(ops.dt_fixed)
+                elif thermal or th is not None:
+                    dt = dt_rule(u0, v0, w0, ops, nut_max, th, t0)
+                else:
+                    dt = cfl_dt3d(u0, v0, w0, ops, nut_max)[0]
+            dt = T(dt)
+        bdt = T(dt * T(b))
+        if a == 0.0:
+            uh, vh, wh = up + lu * bdt, vp + lv * bdt, wp + lw * bdt
+        else:
+            uh = lerp(up, u0, a) + lu * bdt
+            vh = lerp(vp, v0, a) + lv * bdt
+            wh = lerp(wp, w0, a) + lw * bdt
+        if not ops.periodic_axes[0]:
+            uh = inlet_outlet(uh, ops)
+        if not geom.empty:
+            uh, vh, wh, du, dv, dw = penalise3d(uh, vh, wh, geom, ops, bdt)
+            wg = T(wgt)
+            acc = [du * wg, dv * wg, dw * wg] if acc is None else [acc[0] + du * wg, acc[1] + dv * wg,
+                                                                    acc[2] + dw * wg]
+            if any(ops.periodic_axes):
+                uh, vh, wh = sync_periodic(uh, vh, wh, ops)
+        if thermal and th.ri != 0.0:
+            wh, share = add_buoyancy(th, wh, tp, bdt, wgt, geom, ops)
+            if share is not None:
+                acc[2] = acc[2] + share
+        if thermal:
+            tp_new = theta_stage(th, tp, t0, up, vp, wp, a, bdt, wgt, ops,
+                                 nut if ops.turbulence != "none" else None, heat_acc)
+        div = divergence3d(uh, vh, wh, ops.h)
+        psi = poisson.solve(div)
+        gx, gy, gz = pressure_gradient(psi, ops)
+        if trace:
+            stages.append({"lu": lu, "lv": lv, "lw": lw, "uh": uh, "vh": vh, "wh": wh, "div": div, "psi": psi})
+        up, vp, wp = uh - gx, vh - gy, wh - gz
+        if thermal:
+            tp = tp_new
+        psi_w = psi * T(wgt) if psi_w is None else psi_w + T(wgt) * psi
+    p = psi_w * T(T(1.0) / dt)
+    if geom.empty:
+        coeffs = np.zeros((geom.nbody, 6))
+    else:
+        coeffs = force_coefficients(acc, geom, ops, dt)
+    heat_rate = None
+    if thermal:
+        scale = (2.0 if ops.symmetry else 1.0) * ops.h ** 3 * th.pe
+        heat_rate = heat_acc * (scale / float(dt))
+        if getattr(th.geom, "flux_rate", None) is not None:
+            heat_rate = heat_rate + np.asarray(th.geom.flux_rate, np.float64) * (2.0 if ops.symmetry else 1.0)
+    return StepResult(u=up, v=vp, w=wp, p=p, t=T(t + dt), dt=dt, coeffs=coeffs, theta=tp if thermal else None,
+                      heat_rate=heat_rate, stages=stages, nut_stage1=nut_stage1)
+
+
+# ---------------------------------------------------------------------------
+# smoke (dye.py:232-312)
+# ---------------------------------------------------------------------------
+
+def pad_dye(c, ops):
+    """dye.py:232-263 (edges and corners left at zero: never read)."""
+    nz, ny, nx = c.shape
+    P = np.zeros((nz + 4, ny + 4, nx + 4), dtype=c.dtype)
+    P[2:-2, 2:-2, 2:-2] = c
+    px, py, pz = ops.periodic_axes
+    m = slice(2, -2)
+    if px:
+        P[m, m, 0:2] = c[..., nx - 2:]
+        P[m, m, nx + 2:] = c[..., :2]
+    else:
+        P[m, m, 0:2] = 0.0
+        P[m, m, nx + 2:] = c[..., nx - 1:]
+    if py:
+        P[m, 0:2, m] = c[:, ny - 2:]
+        P[m, ny + 2:, m] = c[:, :2]
+    else:
+        P[m, 0:2, m] = np.flip(c[:, :2], 1)
+        P[m, ny + 2:, m] = np.flip(c[:, ny - 2:], 1)
+    if pz:
+        P[0:2, m, m] = c[nz - 2:]
+        P[nz + 2:, m, m] = c[:2]
+    else:
+        P[0:2, m, m] = np.flip(c[:2], 0)
+        P[nz + 2:, m, m] = np.flip(c[nz - 2:], 0)
+    return P
+
+
+def advect_dye3d(c, u, v, w, dt, ops):
+    """Forward Euler MUSCL step, clipped and floored (dye.py:280-298)."""
+    T = c.dtype.type
+    nz, ny, nx = c.shape
+    P = pad_dye(c, ops)
+    m = slice(2, -2)
+    fx = muscl_flux(P[m, m, 0:nx + 1], P[m, m, 1:nx + 2], P[m, m, 2:nx + 3], P[m, m, 3:nx + 4], u)
+    fy = muscl_flux(P[m, 0:ny + 1, m], P[m, 1:ny + 2, m], P[m, 2:ny + 3, m], P[m, 3:ny + 4, m], v)
+    fz = muscl_flux(P[0:nz + 1, m, m], P[1:nz + 2, m, m], P[2:nz + 3, m, m], P[3:nz + 4, m, m], w)
+    k = T(dt * T(1.0 / ops.h))
+    r = c - k * ((fx[..., 1:] - fx[..., :-1]) + (fy[:, 1:] - fy[:, :-1]) + (fz[1:] - fz[:-1]))
+    r = np.minimum(r, T(1.0))
+    return np.where(r < T(DYE_FLOOR), T(0.0), r)
+
+
+def apply_solids_and_sources(c, t, geom, src):
+    """Solid cells cleared, nozzles relaxed to 1 (dye.py:301-312)."""
+    T = c.dtype.type
+    c = c.copy()
+    if geom is not None and not geom.empty:
+        k0, k1, j0, j1, i0, i1 = geom.window
+        win = c[k0:k1, j0:j1, i0:i1]
+        win[geom.chi_c > 0.5] = 0.0
+    if src is not None and not src.empty:
+        k0, k1, j0, j1, i0, i1 = src.window
+        win = c[k0:k1, j0:j1, i0:i1]
+        on = T(1.0) if float(np.remainder(T(t), T(src.pulse[1]))) < float(T(src.pulse[0])) else T(0.0)
+        win += src.weight * on * (T(1.0) - win)
+    return c

@@ -1,0 +1,47 @@
+"""Load the committed golden fixtures into the package's containers (test helper)."""
+from __future__ import annotations
+
+import json
+from pathlib import Path
+
+import numpy as np
+
+from aerolume_b200.ns3d.types import DyeSources, Geometry3D, Ops3D, ThermalGeometry, ThermalOps
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+CASES_3D = sorted(p.stem[len("ns3d_"):] for p in GOLDEN.glob("ns3d_*.npz"))
+
+
+def load_case(name):
+    z = np.load(GOLDEN / f"ns3d_{name}.npz")
+    meta = json.loads(str(z["meta"]))
+    arr = {k: z[k] for k in z.files if k != "meta"}
+    dt = np.float64 if meta["dtype"] == "float64" else np.float32
+    ghost = {k: tuple(tuple((r[0], float(r[1])) for r in ax) for ax in v) for k, v in meta["ghost"].items()}
+    ops = Ops3D(nx=meta["nx"], ny=meta["ny"], nz=meta["nz"], h=meta["h"], x0=meta["x0"], y0=meta["y0"],
+                z0=meta["z0"], periodic_axes=tuple(meta["periodic_axes"]), closed=meta["closed"],
+                symmetry=meta["symmetry"], advection=meta["advection"], turbulence=meta["turbulence"],
+                les_c=meta["les_c"], nu_value=meta["nu_value"], eta=meta["eta"], cfl=meta["cfl"],
+                dt_fixed=meta["dt_fixed"], ghost=ghost, u_inlet=arr["u_inlet"].astype(dt),
+                ref_area=meta["ref_area"], length_ref=meta["length_ref"], span_ref=meta["span_ref"],
+                moment_ref=tuple(meta["moment_ref"]), dtype=meta["dtype"])
+    win = tuple(meta["window"])
+    geom = Geometry3D(win, nbody=meta["nbody"])
+    if not geom.empty:
+        for n in ("chi_u", "chi_v", "chi_w", "chi_c", "a_u", "a_v", "a_w", "k_u", "k_v", "k_w"):
+            setattr(geom, n, arr[n].astype(dt))
+    th = None
+    if "thermal" in meta:
+        t = meta["thermal"]
+        adia = tuple(arr["th_adia_" + c].astype(dt) for c in "uvw") if "th_adia_u" in arr else None
+        tg = ThermalGeometry(win, nbody=meta["nbody"], chi_t=arr.get("th_chi_t"), a_t=arr.get("th_a_t"),
+                             w_t=arr.get("th_w_t"), t_index=list(t["t_index"]), adia=adia,
+                             vol_w=arr.get("th_vol_w"), skin=arr.get("th_skin"),
+                             flux_rate=np.asarray(t["flux_rate"], np.float64))
+        th = ThermalOps(kappa=t["kappa"], pe=t["pe"], ri=t["ri"], prt=t["prt"], eta=t["eta"],
+                        side_kinds=tuple(t["side_kinds"]), side_vals=tuple(t["side_vals"]), geom=tg,
+                        h=meta["h"], symmetry=meta["symmetry"], heat_max=t["heat_max"])
+    src = None
+    if "dye" in meta:
+        src = DyeSources(tuple(meta["dye"]["window"]), arr["dye_weight"].astype(dt), tuple(meta["dye"]["pulse"]))
+    return meta, ops, geom, th, src, arr
