@@ -1,0 +1,115 @@
+"""ctypes binding of ``libaero_b200.so`` (declarations in ``include/aero_b200.h``).
+
+The library is built in-tree (``python -m aerolume_b200.build``).  There is no fallback:
+:func:`lib` raises ``RuntimeError`` when the library is missing or cannot be loaded, and
+every call that returns a negative status raises ``RuntimeError`` with the library's
+message (``aero_last_error``).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libaero_b200.so"
+ABI_VERSION = 1
+MAX_BODIES = 8
+TRACE_EVENTS = 19
+
+F32, F64 = 0, 1
+ADV = {"upwind3": 0, "central": 1}
+LES = {"none": 0, "laminar": 0, "smagorinsky": 1, "wale": 2, "vreman": 3}
+GHOST = {"edge": 0, "even": 1, "odd": 2, "affine": 3, "face_odd": 4, "periodic_cell": 5, "periodic_face": 6}
+THETA_SIDE = {"periodic": 0, "outflow": 1, "adiabatic": 2, "inflow": 3, "temperature": 4, "heat_flux": 5}
+
+# every symbol include/aero_b200.h declares
+EXPORTS = ("aero_abi_version", "aero_last_error", "aero_ns3d_plan_create", "aero_ns3d_plan_destroy",
+           "aero_ns3d_workspace_bytes", "aero_ns3d_workspace_init", "aero_ns3d_step", "aero_ns3d_step_traced",
+           "aero_ns3d_smoke",
+           "aero_ns3d_poisson_solve",
+           "aero_ns3d_project", "aero_ns3d_read_status")
+
+
+class Ns3dConfig(C.Structure):
+    _fields_ = [
+        ("abi_version", C.c_int32), ("dtype", C.c_int32),
+        ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+        ("h", C.c_double),
+        ("periodic", C.c_int32 * 3), ("closed", C.c_int32), ("symmetry", C.c_int32),
+        ("advection", C.c_int32), ("les", C.c_int32), ("les_c", C.c_double),
+        ("nu", C.c_double), ("eta", C.c_double), ("cfl", C.c_double),
+        ("has_dt_fixed", C.c_int32), ("dt_fixed", C.c_double),
+        ("ghost_kind", ((C.c_int32 * 2) * 3) * 3), ("ghost_val", ((C.c_double * 2) * 3) * 3),
+        ("ref_area", C.c_double), ("length_ref", C.c_double), ("span_ref", C.c_double),
+        ("moment_ref", C.c_double * 3), ("y0", C.c_double),
+        ("window", C.c_int32 * 6), ("nbody", C.c_int32),
+        ("thermal", C.c_int32), ("kappa", C.c_double), ("pe", C.c_double), ("ri", C.c_double),
+        ("prt", C.c_double), ("eta_t", C.c_double),
+        ("side_kind", C.c_int32 * 6), ("side_val", C.c_double * 6),
+        ("has_heat_max", C.c_int32), ("heat_max", C.c_double),
+        ("n_tbody", C.c_int32), ("t_index", C.c_int32 * MAX_BODIES),
+        ("has_adia", C.c_int32), ("has_skin", C.c_int32),
+        ("flux_rate", C.c_double * MAX_BODIES),
+        ("smoke", C.c_int32), ("dye_window", C.c_int32 * 6),
+        ("pulse_on", C.c_double), ("pulse_period", C.c_double),
+    ]
+
+
+class Ns3dGeom(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in (
+        "chi_u", "chi_v", "chi_w", "chi_c", "a_u", "a_v", "a_w", "k_u", "k_v", "k_w",
+        "chi_t", "a_t", "w_t", "adia_u", "adia_v", "adia_w", "vol_w", "skin", "dye_weight", "u_inlet")]
+
+
+class Ns3dFields(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in (
+        "u0", "v0", "w0", "theta0", "dye0", "t0",
+        "u", "v", "w", "p", "theta", "dye", "t", "dt", "coeffs", "heat_rate")]
+
+
+_LIB = None
+
+
+def lib() -> C.CDLL:
+    """The loaded library (raises RuntimeError when it is missing: no fallback)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not LIB_PATH.exists():
+        raise RuntimeError(f"{LIB_PATH.name} is not built; run `python -m aerolume_b200.build` "
+                           "(the B200 step has no CPU fallback)")
+    try:
+        L = C.CDLL(str(LIB_PATH))
+    except OSError as exc:
+        raise RuntimeError(f"cannot load {LIB_PATH}: {exc}") from exc
+    L.aero_abi_version.restype = C.c_int
+    L.aero_last_error.restype = C.c_char_p
+    L.aero_ns3d_plan_create.argtypes = [C.POINTER(Ns3dConfig), C.POINTER(C.c_void_p)]
+    L.aero_ns3d_plan_destroy.argtypes = [C.c_void_p]
+    L.aero_ns3d_plan_destroy.restype = None
+    L.aero_ns3d_workspace_bytes.argtypes = [C.c_void_p]
+    L.aero_ns3d_workspace_bytes.restype = C.c_size_t
+    L.aero_ns3d_workspace_init.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    L.aero_ns3d_step.argtypes = [C.c_void_p, C.POINTER(Ns3dFields), C.POINTER(Ns3dGeom), C.c_void_p, C.c_void_p,
+                                 C.c_void_p]
+    L.aero_ns3d_step_traced.argtypes = [C.c_void_p, C.POINTER(Ns3dFields), C.POINTER(Ns3dGeom), C.c_void_p,
+                                        C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p), C.c_int32]
+    L.aero_ns3d_smoke.argtypes = [C.c_void_p, C.POINTER(Ns3dFields), C.POINTER(Ns3dGeom), C.c_void_p]
+    L.aero_ns3d_poisson_solve.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.aero_ns3d_project.argtypes = [C.c_void_p] + [C.c_void_p] * 6
+    L.aero_ns3d_read_status.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_int32), C.c_void_p]
+    for name in ("aero_ns3d_plan_create", "aero_ns3d_workspace_init", "aero_ns3d_step", "aero_ns3d_step_traced",
+                 "aero_ns3d_smoke",
+                 "aero_ns3d_poisson_solve",
+                 "aero_ns3d_project", "aero_ns3d_read_status"):
+        getattr(L, name).restype = C.c_int
+    if L.aero_abi_version() != ABI_VERSION:
+        raise RuntimeError(f"{LIB_PATH.name} has ABI {L.aero_abi_version()}, expected {ABI_VERSION}; rebuild it")
+    _LIB = L
+    return L
+
+
+def check(rc: int, what: str) -> None:
+    if rc != 0:
+        msg = lib().aero_last_error().decode(errors="replace")
+        kind = {-1: "invalid argument", -2: "unsupported", -3: "CUDA error"}.get(rc, f"error {rc}")
+        raise RuntimeError(f"{what}: {kind}: {msg}")

@@ -1,0 +1,659 @@
+// C ABI of libaero_b200.so: plans, workspace layout and the launch sequence of a step.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "ns3d.cuh"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string &msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define CUDA_TRY(expr)                                                                              \
+  do {                                                                                              \
+    cudaError_t e__ = (expr);                                                                       \
+    if (e__ != cudaSuccess) return fail(AERO_ECUDA, std::string(#expr) + ": " + cudaGetErrorString(e__)); \
+  } while (0)
+
+constexpr size_t ALIGN = 256;
+size_t align_up(size_t x) { return (x + ALIGN - 1) & ~(ALIGN - 1); }
+
+// radix sequence (4s, then 2, then 3s) for n = 2^a 3^b, else empty
+int factor(int n, int *fac) {
+  int k = 0;
+  while (n % 4 == 0) { fac[k++] = 4; n /= 4; }
+  while (n % 2 == 0) { fac[k++] = 2; n /= 2; }
+  while (n % 3 == 0) { fac[k++] = 3; n /= 3; }
+  return n == 1 ? k : -1;
+}
+
+struct AxisInfo {
+  int n, kind, method, nfac, L;
+  int fac[16];
+  size_t off_tw, off_post, off_cs, off_lam, off_dense;
+};
+
+}  // namespace
+
+struct AeroNs3dPlan {
+  AeroNs3dConfig cfg;
+  size_t esz;                     // bytes per element
+  size_t nu, nv, nw, nc;          // element counts of u, v, w and cell arrays
+  size_t off_uh, off_vh, off_wh, off_up, off_vp, off_wp, off_tha, off_thb, off_pa;
+  size_t off_small, off_scalars, off_status, off_partials, total;
+  AxisInfo ax[3];
+  int zc, nblocks, nq;
+};
+
+namespace {
+
+template <typename T>
+aero::AxisTables<T> axis_tables(const AeroNs3dPlan *p, int a, unsigned char *ws) {
+  const AxisInfo &x = p->ax[a];
+  aero::AxisTables<T> A{};
+  A.n = x.n;
+  A.method = x.method;
+  A.kind = x.kind;
+  A.nfac = x.nfac;
+  for (int i = 0; i < x.nfac; ++i) A.fac[i] = x.fac[i];
+  A.tw = reinterpret_cast<const T *>(ws + x.off_tw);
+  A.post = reinterpret_cast<const T *>(ws + x.off_post);
+  A.cs = reinterpret_cast<const T *>(ws + x.off_cs);
+  A.lam = reinterpret_cast<const double *>(ws + x.off_lam);
+  A.dense = x.method == 1 ? reinterpret_cast<const T *>(ws + x.off_dense) : nullptr;
+  A.s0 = T(std::sqrt(1.0 / x.n));
+  A.s1 = T(std::sqrt(2.0 / x.n));
+  A.rsqrt_n = T(1.0 / std::sqrt((double)x.n));
+  return A;
+}
+
+// psi = L^{-1} f through five passes: x, y forward; z forward-solve-inverse; y, x inverse.
+// Every pass owns whole lines per block, so after the first pass the solve runs in place.
+template <typename T>
+int poisson_passes(const AeroNs3dPlan *p, const T *f, T *psi, unsigned char *ws, cudaStream_t s) {
+  const AeroNs3dConfig &c = p->cfg;
+  aero::TransformParams<T> P{};
+  P.nx = c.nx;
+  P.ny = c.ny;
+  P.nz = c.nz;
+  P.lam_x = reinterpret_cast<const double *>(ws + p->ax[0].off_lam);
+  P.lam_y = reinterpret_cast<const double *>(ws + p->ax[1].off_lam);
+  const int axes[5] = {0, 1, 2, 1, 0}, modes[5] = {0, 0, 2, 1, 1};
+  for (int q = 0; q < 5; ++q) {
+    P.axis = axes[q];
+    P.mode = modes[q];
+    P.in = q == 0 ? f : psi;
+    P.out = psi;
+    P.L = p->ax[axes[q]].L;
+    P.A = axis_tables<T>(p, axes[q], ws);
+    CUDA_TRY(aero::launch_transform<T>(P, s));
+  }
+  return AERO_OK;
+}
+
+template <typename T>
+aero::CompRules<T> comp_rules(const AeroNs3dConfig &c, int comp) {
+  aero::CompRules<T> r{};
+  r.n0 = c.nx + (comp == 0);
+  r.n1 = c.ny + (comp == 1);
+  r.n2 = c.nz + (comp == 2);
+  for (int a = 0; a < 3; ++a)
+    for (int s = 0; s < 2; ++s) {
+      r.kind[a][s] = c.ghost_kind[comp][a][s];
+      r.val[a][s] = T(c.ghost_val[comp][a][s]);
+    }
+  return r;
+}
+
+// sum of a[r * stride + off] over rows, in a fixed order, into out (double)
+template <typename T>
+__global__ void plane_sum_kernel(const T *a0, size_t stride0, size_t off0, double *out0, const T *a1, size_t stride1,
+                                 size_t off1, double *out1, int rows) {
+  __shared__ double red[2][32];
+  double s0 = 0.0, s1 = 0.0;
+  for (int r = threadIdx.x; r < rows; r += blockDim.x) {
+    if (a0) s0 += (double)a0[(size_t)r * stride0 + off0];
+    if (a1) s1 += (double)a1[(size_t)r * stride1 + off1];
+  }
+  s0 = aero::warp_sum(s0);
+  s1 = aero::warp_sum(s1);
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = s0;
+    red[1][threadIdx.x >> 5] = s1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double x = 0.0, y = 0.0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) {
+      x += red[0][q];
+      y += red[1][q];
+    }
+    if (a0) *out0 = x;
+    if (a1) *out1 = y;
+  }
+}
+
+template <typename T>
+int smoke_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom *g, const T *dt, const T *t_new,
+               cudaStream_t s) {
+  const AeroNs3dConfig &c = p->cfg;
+  const bool has_win = !(c.window[1] <= c.window[0] || c.window[3] <= c.window[2] || c.window[5] <= c.window[4]) &&
+                       c.nbody > 0;
+  aero::SmokeParams<T> M{};
+  M.nx = c.nx;
+  M.ny = c.ny;
+  M.nz = c.nz;
+  M.px = c.periodic[0];
+  M.py = c.periodic[1];
+  M.pz = c.periodic[2];
+  M.inv_h = T(1.0 / c.h);
+  M.c0 = static_cast<const T *>(f->dye0);
+  M.u = static_cast<const T *>(f->u);
+  M.v = static_cast<const T *>(f->v);
+  M.w = static_cast<const T *>(f->w);
+  M.dt = dt;
+  M.t0 = static_cast<const T *>(f->t0);
+  M.t_new = t_new;
+  M.c = static_cast<T *>(f->dye);
+  M.chi_c = has_win ? static_cast<const T *>(g->chi_c) : nullptr;
+  for (int q = 0; q < 6; ++q) {
+    M.win[q] = has_win ? c.window[q] : 0;
+    M.dwin[q] = c.dye_window[q];
+  }
+  const bool dye_src = !(c.dye_window[1] <= c.dye_window[0] || c.dye_window[3] <= c.dye_window[2] ||
+                         c.dye_window[5] <= c.dye_window[4]);
+  M.weight = dye_src ? static_cast<const T *>(g->dye_weight) : nullptr;
+  M.pulse_on = c.pulse_on;
+  M.pulse_period = c.pulse_period;
+  CUDA_TRY(aero::launch_smoke<T>(M, s));
+  return AERO_OK;
+}
+
+template <typename T>
+int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom *g, const void *dt_in,
+              unsigned char *ws, cudaStream_t s, void *const *events = nullptr, int nevents = 0) {
+  auto mark = [&](int i) -> cudaError_t {
+    if (!events || i >= nevents || !events[i]) return cudaSuccess;
+    return cudaEventRecordWithFlags(static_cast<cudaEvent_t>(events[i]), s, cudaEventRecordExternal);
+  };
+  const AeroNs3dConfig &c = p->cfg;
+  const int nx = c.nx, ny = c.ny, nz = c.nz;
+  T *uh = reinterpret_cast<T *>(ws + p->off_uh), *vh = reinterpret_cast<T *>(ws + p->off_vh),
+    *wh = reinterpret_cast<T *>(ws + p->off_wh);
+  T *upb = reinterpret_cast<T *>(ws + p->off_up), *vpb = reinterpret_cast<T *>(ws + p->off_vp),
+    *wpb = reinterpret_cast<T *>(ws + p->off_wp);
+  T *tha = reinterpret_cast<T *>(ws + p->off_tha), *thb = reinterpret_cast<T *>(ws + p->off_thb);
+  T *pa = reinterpret_cast<T *>(ws + p->off_pa);
+  T *small = reinterpret_cast<T *>(ws + p->off_small);  // [0] dt, [1] outlet corr
+  double *sc = reinterpret_cast<double *>(ws + p->off_scalars);
+  int *status = reinterpret_cast<int *>(ws + p->off_status);
+  double *partials = reinterpret_cast<double *>(ws + p->off_partials);
+  unsigned long long *bits = reinterpret_cast<unsigned long long *>(sc);
+
+  const T *u0 = static_cast<const T *>(f->u0), *v0 = static_cast<const T *>(f->v0),
+          *w0 = static_cast<const T *>(f->w0);
+  const bool thermal = c.thermal != 0;
+  const bool les = c.les != AERO_LES_NONE;
+  const bool has_win = !(c.window[1] <= c.window[0] || c.window[3] <= c.window[2] || c.window[5] <= c.window[4]) &&
+                       c.nbody > 0;
+  const bool tunnel = !c.periodic[0] && !c.closed;
+  const T *th0 = thermal ? static_cast<const T *>(f->theta0) : nullptr;
+
+  CUDA_TRY(mark(0));
+  CUDA_TRY(cudaMemsetAsync(sc, 0, sizeof(double) * aero::SC_COUNT, s));
+  CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(int), s));
+
+  // ---- time step
+  const bool need_max = dt_in == nullptr && !c.has_dt_fixed;
+  if (need_max) {
+    CUDA_TRY(aero::launch_absmax<T>(u0, p->nu, bits + aero::SC_MAXU, s));
+    CUDA_TRY(aero::launch_absmax<T>(v0, p->nv, bits + aero::SC_MAXV, s));
+    CUDA_TRY(aero::launch_absmax<T>(w0, p->nw, bits + aero::SC_MAXW, s));
+    if (thermal) CUDA_TRY(aero::launch_absmax<T>(th0, p->nc, bits + aero::SC_MAXT, s));
+  }
+
+  aero::StageParams<T> S{};
+  S.nx = nx;
+  S.ny = ny;
+  S.nz = nz;
+  S.zc = p->zc;
+  S.h = T(c.h);
+  S.inv_h = T(1.0 / c.h);
+  S.ru = comp_rules<T>(c, 0);
+  S.rv = comp_rules<T>(c, 1);
+  S.rw = comp_rules<T>(c, 2);
+  S.px = c.periodic[0];
+  S.py = c.periodic[1];
+  S.pz = c.periodic[2];
+  S.closed = c.closed;
+  S.upwind = c.advection == AERO_ADV_UPWIND3;
+  S.les = c.les;
+  S.kadv = T((c.advection == AERO_ADV_UPWIND3 ? 7.0 / 24.0 : 0.25) / c.h);
+  S.nu_h2 = T(T(c.nu) * T(1.0 / (c.h * c.h)));
+  S.les_cd2 = T(c.les == AERO_LES_VREMAN ? c.les_c * c.h * c.h : c.les_c * c.les_c * c.h * c.h);
+  S.dt = small;
+  S.u0 = u0;
+  S.v0 = v0;
+  S.w0 = w0;
+  S.uh = uh;
+  S.vh = vh;
+  S.wh = wh;
+  S.u_inlet = static_cast<const T *>(g->u_inlet);
+  S.outlet_corr = small + 1;
+  S.has_win = has_win;
+  for (int q = 0; q < 6; ++q) S.win[q] = has_win ? c.window[q] : 0;
+  S.wnx = c.window[5] - c.window[4];
+  S.wny = c.window[3] - c.window[2];
+  S.nbody = has_win ? c.nbody : 0;
+  S.nq = p->nq;
+  S.eta = T(c.eta);
+  S.chi_u = static_cast<const T *>(g->chi_u);
+  S.chi_v = static_cast<const T *>(g->chi_v);
+  S.chi_w = static_cast<const T *>(g->chi_w);
+  S.chi_c = static_cast<const T *>(g->chi_c);
+  S.a_u = static_cast<const T *>(g->a_u);
+  S.a_v = static_cast<const T *>(g->a_v);
+  S.a_w = static_cast<const T *>(g->a_w);
+  S.k_u = static_cast<const T *>(g->k_u);
+  S.k_v = static_cast<const T *>(g->k_v);
+  S.k_w = static_cast<const T *>(g->k_w);
+  S.thermal = thermal;
+  if (thermal) {
+    S.has_adia = c.has_adia;
+    S.n_tbody = has_win ? c.n_tbody : 0;
+    for (int q = 0; q < 6; ++q) {
+      S.sides.kind[q] = c.side_kind[q];
+      S.sides.val[q] = c.side_val[q];
+    }
+    S.kh = T(c.kappa / c.h);
+    S.kprt = T(0.5 / (c.prt * c.h));
+    S.kappa = T(c.kappa);
+    S.ri = T(c.ri);
+    S.eta_t = T(c.eta_t);
+    S.th0 = th0;
+    S.chi_t = static_cast<const T *>(g->chi_t);
+    S.a_t = static_cast<const T *>(g->a_t);
+    S.w_t = static_cast<const T *>(g->w_t);
+    S.adia_u = static_cast<const T *>(g->adia_u);
+    S.adia_v = static_cast<const T *>(g->adia_v);
+    S.adia_w = static_cast<const T *>(g->adia_w);
+    S.vol_w = static_cast<const T *>(g->vol_w);
+    S.skin = static_cast<const T *>(g->skin);
+    if (!has_win) {
+      S.chi_t = S.a_t = S.w_t = S.adia_u = S.adia_v = S.adia_w = S.vol_w = S.skin = nullptr;
+      S.has_adia = 0;
+    }
+  }
+
+  if (need_max && les) {
+    aero::StageParams<T> N = S;
+    N.mode = aero::MODE_NUT_ONLY;
+    N.up = u0;
+    N.vp = v0;
+    N.wp = w0;
+    N.thermal = 0;
+    N.nut_max = bits + aero::SC_NUTMAX;
+    CUDA_TRY(aero::launch_stage<T>(N, s));
+  }
+
+  aero::DtParams D{};
+  D.scalars = sc;
+  D.dt_in = dt_in;
+  D.dt_out = small;
+  D.status = status;
+  D.has_dt_fixed = c.has_dt_fixed;
+  D.dt_fixed = c.dt_fixed;
+  D.les = les;
+  D.thermal = thermal;
+  D.has_heat_max = c.has_heat_max;
+  D.cfl = c.cfl;
+  D.h = c.h;
+  D.nu = c.nu;
+  D.viscous_dt = 1.0 / 6.0;
+  D.kappa = c.kappa;
+  D.prt = c.prt;
+  D.ri = c.ri;
+  D.heat_max = c.heat_max;
+  CUDA_TRY(aero::launch_dt<T>(D, s));
+
+  const int rows = nz * ny;
+  if (tunnel) {
+    plane_sum_kernel<T><<<1, 1024, 0, s>>>(u0, nx + 1, nx, sc + aero::SC_SUM_U0, S.u_inlet, 1, 0,
+                                          sc + aero::SC_SUM_INLET, rows);
+    CUDA_TRY(cudaGetLastError());
+  }
+
+  CUDA_TRY(mark(1));
+  static const double RK[3][3] = {{0.0, 1.0, 1.0 / 6.0}, {0.75, 0.25, 2.0 / 3.0}, {1.0 / 3.0, 2.0 / 3.0, 1.0}};
+  T *p_out = static_cast<T *>(f->p);
+  for (int st = 0; st < 3; ++st) {
+    const T *up = st == 0 ? u0 : upb, *vp = st == 0 ? v0 : vpb, *wp = st == 0 ? w0 : wpb;
+    if (tunnel) {
+      double *sums = sc + aero::SC_SUMS + 3 * st;
+      plane_sum_kernel<T><<<1, 1024, 0, s>>>(up, nx + 1, nx, sums, up, nx + 1, nx - 1, sums + 1, rows);
+      CUDA_TRY(cudaGetLastError());
+      CUDA_TRY(aero::launch_outlet_corr<T>(sums, sc + aero::SC_SUM_U0, sc + aero::SC_SUM_INLET, small, RK[st][0],
+                                           RK[st][1], 1.0 / c.h, 1.0 / rows, small + 1, s));
+    }
+    CUDA_TRY(mark(2 + 5 * st));
+    aero::StageParams<T> P = S;
+    P.mode = aero::MODE_STAGE;
+    P.a = T(RK[st][0]);
+    P.bdt_scale = T(RK[st][1]);
+    P.wgt = T(RK[st][2]);
+    P.up = up;
+    P.vp = vp;
+    P.wp = wp;
+    P.partials = has_win ? partials + (size_t)st * p->nblocks * p->nq : nullptr;
+    P.nut_max = nullptr;
+    if (thermal) {
+      P.thp = st == 0 ? th0 : (st == 1 ? tha : thb);
+      P.thh = st == 0 ? tha : (st == 1 ? thb : static_cast<T *>(f->theta));
+    }
+    CUDA_TRY(aero::launch_stage<T>(P, s));
+    CUDA_TRY(mark(3 + 5 * st));
+    CUDA_TRY(aero::launch_divergence<T>(uh, vh, wh, nx, ny, nz, c.periodic[0], c.periodic[1], c.periodic[2],
+                                        T(1.0 / c.h), pa, s));
+    CUDA_TRY(mark(4 + 5 * st));
+    const int rc = poisson_passes<T>(p, pa, pa, ws, s);
+    if (rc) return rc;
+    CUDA_TRY(aero::launch_psi_accumulate<T>(pa, p_out, p->nc, T(RK[st][2]), st == 0, s));
+    CUDA_TRY(mark(5 + 5 * st));
+    aero::CorrectParams<T> C{};
+    C.nx = nx;
+    C.ny = ny;
+    C.nz = nz;
+    C.px = c.periodic[0];
+    C.py = c.periodic[1];
+    C.pz = c.periodic[2];
+    C.inv_h = T(1.0 / c.h);
+    C.uh = uh;
+    C.vh = vh;
+    C.wh = wh;
+    C.psi = pa;
+    C.u = st == 2 ? static_cast<T *>(f->u) : upb;
+    C.v = st == 2 ? static_cast<T *>(f->v) : vpb;
+    C.w = st == 2 ? static_cast<T *>(f->w) : wpb;
+    CUDA_TRY(aero::launch_correct<T>(C, s));
+    CUDA_TRY(mark(6 + 5 * st));
+  }
+
+  const T *t0 = static_cast<const T *>(f->t0);
+  if (c.smoke) {
+    const int rc = smoke_impl<T>(p, f, g, small, nullptr, s);
+    if (rc) return rc;
+  }
+  CUDA_TRY(mark(17));
+
+  aero::FinalizeParams<T> F{};
+  F.ncell = p->nc;
+  F.nbody = has_win ? c.nbody : 0;
+  F.nq = p->nq;
+  F.nblocks = p->nblocks;
+  F.n_tbody = thermal && has_win ? c.n_tbody : 0;
+  F.symmetry = c.symmetry;
+  F.partials = partials;
+  F.h = c.h;
+  F.pe = c.pe;
+  F.y0 = c.y0;
+  F.moment_ref_y = c.moment_ref[1];
+  F.ref_area = c.ref_area;
+  F.span_ref = c.span_ref;
+  F.length_ref = c.length_ref;
+  for (int q = 0; q < AERO_MAX_BODIES; ++q) {
+    F.t_index[q] = c.t_index[q];
+    F.flux_rate[q] = c.flux_rate[q];
+  }
+  F.dt = small;
+  F.t0 = t0;
+  F.t_out = static_cast<T *>(f->t);
+  F.dt_out = static_cast<T *>(f->dt);
+  F.coeffs = static_cast<T *>(f->coeffs);
+  F.heat_rate = thermal ? static_cast<T *>(f->heat_rate) : nullptr;
+  F.p = p_out;
+  F.status = status;
+  CUDA_TRY(aero::launch_finalize<T>(F, s));
+  CUDA_TRY(mark(18));
+  return AERO_OK;
+}
+
+template <typename T>
+int init_impl(const AeroNs3dPlan *p, unsigned char *ws, cudaStream_t s) {
+  CUDA_TRY(cudaMemsetAsync(ws, 0, p->total, s));
+  for (int a = 0; a < 3; ++a) {
+    const AxisInfo &x = p->ax[a];
+    CUDA_TRY(aero::launch_axis_tables<T>(x.n, x.kind, x.method == 1, p->cfg.h, reinterpret_cast<T *>(ws + x.off_tw),
+                                         reinterpret_cast<T *>(ws + x.off_post), reinterpret_cast<T *>(ws + x.off_cs),
+                                         reinterpret_cast<double *>(ws + x.off_lam),
+                                         x.method == 1 ? reinterpret_cast<T *>(ws + x.off_dense) : nullptr, s));
+  }
+  return AERO_OK;
+}
+
+template <typename T>
+int poisson_impl(const AeroNs3dPlan *p, const void *f, void *psi, unsigned char *ws, cudaStream_t s) {
+  return poisson_passes<T>(p, static_cast<const T *>(f), static_cast<T *>(psi), ws, s);
+}
+
+template <typename T>
+int project_impl(const AeroNs3dPlan *p, void *u, void *v, void *w, void *psi, unsigned char *ws, cudaStream_t s) {
+  const AeroNs3dConfig &c = p->cfg;
+  T *pa = reinterpret_cast<T *>(ws + p->off_pa);
+  T *upb = reinterpret_cast<T *>(ws + p->off_up), *vpb = reinterpret_cast<T *>(ws + p->off_vp),
+    *wpb = reinterpret_cast<T *>(ws + p->off_wp);
+  CUDA_TRY(aero::launch_divergence<T>(static_cast<T *>(u), static_cast<T *>(v), static_cast<T *>(w), c.nx, c.ny, c.nz,
+                                      c.periodic[0], c.periodic[1], c.periodic[2], T(1.0 / c.h), pa, s));
+  const int rc = poisson_passes<T>(p, pa, static_cast<T *>(psi), ws, s);
+  if (rc) return rc;
+  aero::CorrectParams<T> C{};
+  C.nx = c.nx;
+  C.ny = c.ny;
+  C.nz = c.nz;
+  C.px = c.periodic[0];
+  C.py = c.periodic[1];
+  C.pz = c.periodic[2];
+  C.inv_h = T(1.0 / c.h);
+  C.uh = static_cast<T *>(u);
+  C.vh = static_cast<T *>(v);
+  C.wh = static_cast<T *>(w);
+  C.psi = static_cast<T *>(psi);
+  C.u = upb;
+  C.v = vpb;
+  C.w = wpb;
+  CUDA_TRY(aero::launch_correct<T>(C, s));
+  CUDA_TRY(cudaMemcpyAsync(u, upb, p->nu * sizeof(T), cudaMemcpyDeviceToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(v, vpb, p->nv * sizeof(T), cudaMemcpyDeviceToDevice, s));
+  CUDA_TRY(cudaMemcpyAsync(w, wpb, p->nw * sizeof(T), cudaMemcpyDeviceToDevice, s));
+  return AERO_OK;
+}
+
+bool window_empty(const int32_t *w) { return w[1] <= w[0] || w[3] <= w[2] || w[5] <= w[4]; }
+
+}  // namespace
+
+extern "C" {
+
+int aero_abi_version(void) { return AERO_ABI_VERSION; }
+
+const char *aero_last_error(void) { return g_last_error.c_str(); }
+
+int aero_ns3d_plan_create(const AeroNs3dConfig *cfg, AeroNs3dPlan **plan) {
+  if (!cfg || !plan) return fail(AERO_EINVAL, "null argument");
+  *plan = nullptr;
+  const AeroNs3dConfig &c = *cfg;
+  if (c.abi_version != AERO_ABI_VERSION) return fail(AERO_EINVAL, "ABI version mismatch");
+  if (c.dtype != AERO_F32 && c.dtype != AERO_F64) return fail(AERO_EINVAL, "dtype must be float32 or float64");
+  if (c.nx < 4 || c.ny < 4 || c.nz < 4) return fail(AERO_EINVAL, "the grid needs at least 4 x 4 x 4 cells");
+  if (!(c.h > 0) || !std::isfinite(c.h)) return fail(AERO_EINVAL, "cell size h must be positive");
+  if (c.advection != AERO_ADV_UPWIND3 && c.advection != AERO_ADV_CENTRAL) return fail(AERO_EINVAL, "unknown advection");
+  if (c.les < AERO_LES_NONE || c.les > AERO_LES_VREMAN) return fail(AERO_EINVAL, "unknown turbulence model");
+  if (c.nbody < 0 || c.nbody > AERO_MAX_BODIES)
+    return fail(AERO_EUNSUPPORTED, "at most " + std::to_string(AERO_MAX_BODIES) + " bodies");
+  for (int comp = 0; comp < 3; ++comp)
+    for (int a = 0; a < 3; ++a)
+      for (int sd = 0; sd < 2; ++sd)
+        if (c.ghost_kind[comp][a][sd] < AERO_GHOST_EDGE || c.ghost_kind[comp][a][sd] > AERO_GHOST_PERIODIC_FACE)
+          return fail(AERO_EINVAL, "unknown ghost rule");
+  if (!window_empty(c.window)) {
+    if (c.window[0] < 0 || c.window[1] > c.nz || c.window[2] < 0 || c.window[3] > c.ny || c.window[4] < 0 ||
+        c.window[5] > c.nx)
+      return fail(AERO_EINVAL, "body window outside the domain");
+  }
+  if (c.thermal) {
+    if (c.n_tbody < 0 || c.n_tbody > c.nbody) return fail(AERO_EINVAL, "bad temperature-body count");
+    for (int q = 0; q < 6; ++q)
+      if (c.side_kind[q] < AERO_TH_PERIODIC || c.side_kind[q] > AERO_TH_HEAT_FLUX)
+        return fail(AERO_EINVAL, "unknown thermal side condition");
+    if (!(c.prt > 0) || !(c.eta_t > 0)) return fail(AERO_EINVAL, "bad thermal constants");
+  }
+  if (c.smoke && !window_empty(c.dye_window)) {
+    if (c.dye_window[0] < 0 || c.dye_window[1] > c.nz || c.dye_window[2] < 0 || c.dye_window[3] > c.ny ||
+        c.dye_window[4] < 0 || c.dye_window[5] > c.nx)
+      return fail(AERO_EINVAL, "smoke nozzle window outside the domain");
+  }
+  if (!(c.eta > 0)) return fail(AERO_EINVAL, "eta must be positive");
+  AeroNs3dPlan *p = new AeroNs3dPlan();
+  p->cfg = c;
+  p->esz = c.dtype == AERO_F64 ? 8 : 4;
+  const size_t nx = c.nx, ny = c.ny, nz = c.nz;
+  p->nu = nz * ny * (nx + 1);
+  p->nv = nz * (ny + 1) * nx;
+  p->nw = (nz + 1) * ny * nx;
+  p->nc = nz * ny * nx;
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t o = off;
+    off = align_up(off + bytes);
+    return o;
+  };
+  const size_t e = p->esz;
+  p->off_uh = take(p->nu * e);
+  p->off_vh = take(p->nv * e);
+  p->off_wh = take(p->nw * e);
+  p->off_up = take(p->nu * e);
+  p->off_vp = take(p->nv * e);
+  p->off_wp = take(p->nw * e);
+  p->off_tha = take(c.thermal ? p->nc * e : 0);
+  p->off_thb = take(c.thermal ? p->nc * e : 0);
+  p->off_pa = take(p->nc * e);
+  p->off_small = take(8 * e);
+  p->off_scalars = take(sizeof(double) * aero::SC_COUNT);
+  p->off_status = take(sizeof(int) * 4);
+  p->zc = c.nz <= 16 ? c.nz : 16;
+  p->nblocks = (int)(((nx + 31) / 32) * ((ny + 7) / 8) * ((nz + p->zc - 1) / p->zc));
+  p->nq = c.nbody * 9 + (c.thermal ? c.n_tbody : 0);
+  p->off_partials = take(sizeof(double) * 3 * (size_t)p->nblocks * std::max(p->nq, 1));
+  const int ns[3] = {c.nx, c.ny, c.nz};
+  for (int a = 0; a < 3; ++a) {
+    AxisInfo &x = p->ax[a];
+    x.n = ns[a];
+    x.kind = c.periodic[a] ? 1 : 0;
+    x.nfac = factor(x.n, x.fac);
+    x.method = x.nfac < 0 ? 1 : 0;
+    if (x.nfac < 0) x.nfac = 0;
+    // lines per block: keep the tile (3 n L elements) within ~48 KiB, even, 2..64
+    int L = (int)((48 * 1024) / (3 * e * (size_t)x.n));
+    L = std::max(2, std::min(64, L));
+    L &= ~1;
+    if (x.method == 1) L = std::max(2, std::min(L, 16));
+    x.L = L;
+    x.off_tw = take(2 * x.n * e);
+    x.off_post = take(2 * x.n * e);
+    x.off_cs = take(2 * x.n * e);
+    x.off_lam = take(sizeof(double) * x.n);
+    x.off_dense = take(x.method == 1 ? (size_t)x.n * x.n * e : 0);
+  }
+  p->total = off;
+  *plan = p;
+  return AERO_OK;
+}
+
+void aero_ns3d_plan_destroy(AeroNs3dPlan *plan) { delete plan; }
+
+size_t aero_ns3d_workspace_bytes(const AeroNs3dPlan *plan) { return plan ? plan->total : 0; }
+
+int aero_ns3d_workspace_init(const AeroNs3dPlan *plan, void *workspace, void *stream) {
+  if (!plan || !workspace) return fail(AERO_EINVAL, "null argument");
+  if (reinterpret_cast<uintptr_t>(workspace) % ALIGN) return fail(AERO_EINVAL, "workspace must be 256-byte aligned");
+  auto s = static_cast<cudaStream_t>(stream);
+  auto ws = static_cast<unsigned char *>(workspace);
+  return plan->cfg.dtype == AERO_F64 ? init_impl<double>(plan, ws, s) : init_impl<float>(plan, ws, s);
+}
+
+int aero_ns3d_step(const AeroNs3dPlan *plan, const AeroNs3dFields *f, const AeroNs3dGeom *g, const void *dt_in,
+                   void *workspace, void *stream) {
+  return aero_ns3d_step_traced(plan, f, g, dt_in, workspace, stream, nullptr, 0);
+}
+
+int aero_ns3d_step_traced(const AeroNs3dPlan *plan, const AeroNs3dFields *f, const AeroNs3dGeom *g,
+                          const void *dt_in, void *workspace, void *stream, void *const *events, int32_t nevents) {
+  if (!plan || !f || !g || !workspace) return fail(AERO_EINVAL, "null argument");
+  if (reinterpret_cast<uintptr_t>(workspace) % ALIGN) return fail(AERO_EINVAL, "workspace must be 256-byte aligned");
+  const AeroNs3dConfig &c = plan->cfg;
+  if (!f->u0 || !f->v0 || !f->w0 || !f->u || !f->v || !f->w || !f->p || !f->t0 || !f->t || !f->dt)
+    return fail(AERO_EINVAL, "missing state pointer");
+  if (c.thermal && (!f->theta0 || !f->theta)) return fail(AERO_EINVAL, "heat transfer needs theta pointers");
+  if (c.smoke && (!f->dye0 || !f->dye)) return fail(AERO_EINVAL, "smoke needs dye pointers");
+  if (c.smoke && f->dye0 == f->dye) return fail(AERO_EINVAL, "dye output must not alias dye input");
+  if (!c.periodic[0] && !c.closed && !g->u_inlet) return fail(AERO_EINVAL, "missing inlet profile");
+  if (!window_empty(c.window) && c.nbody > 0) {
+    if (!g->chi_u || !g->chi_v || !g->chi_w || !g->chi_c || !g->a_u || !g->a_v || !g->a_w || !g->k_u || !g->k_v ||
+        !g->k_w || !f->coeffs)
+      return fail(AERO_EINVAL, "missing body masks");
+    if (c.thermal && c.n_tbody > 0 && (!g->chi_t || !g->a_t || !g->w_t)) return fail(AERO_EINVAL, "missing thermal masks");
+    if (c.thermal && c.has_adia && (!g->adia_u || !g->adia_v || !g->adia_w))
+      return fail(AERO_EINVAL, "missing adiabatic masks");
+    if (c.thermal && c.has_skin && !g->skin) return fail(AERO_EINVAL, "missing heat-flux skin");
+  }
+  if (c.thermal && !f->heat_rate && c.nbody > 0) return fail(AERO_EINVAL, "missing heat-rate output");
+  auto s = static_cast<cudaStream_t>(stream);
+  auto ws = static_cast<unsigned char *>(workspace);
+  return c.dtype == AERO_F64 ? step_impl<double>(plan, f, g, dt_in, ws, s, events, nevents)
+                             : step_impl<float>(plan, f, g, dt_in, ws, s, events, nevents);
+}
+
+int aero_ns3d_smoke(const AeroNs3dPlan *plan, const AeroNs3dFields *f, const AeroNs3dGeom *g, void *stream) {
+  if (!plan || !f || !g) return fail(AERO_EINVAL, "null argument");
+  if (!plan->cfg.smoke) return fail(AERO_EINVAL, "the plan has no smoke");
+  if (!f->dye0 || !f->dye || !f->u || !f->v || !f->w || !f->t || !f->dt) return fail(AERO_EINVAL, "missing pointer");
+  if (f->dye0 == f->dye) return fail(AERO_EINVAL, "dye output must not alias dye input");
+  auto s = static_cast<cudaStream_t>(stream);
+  return plan->cfg.dtype == AERO_F64
+             ? smoke_impl<double>(plan, f, g, static_cast<const double *>(f->dt), static_cast<const double *>(f->t), s)
+             : smoke_impl<float>(plan, f, g, static_cast<const float *>(f->dt), static_cast<const float *>(f->t), s);
+}
+
+int aero_ns3d_poisson_solve(const AeroNs3dPlan *plan, const void *f, void *psi, void *workspace, void *stream) {
+  if (!plan || !f || !psi || !workspace) return fail(AERO_EINVAL, "null argument");
+  auto s = static_cast<cudaStream_t>(stream);
+  auto ws = static_cast<unsigned char *>(workspace);
+  return plan->cfg.dtype == AERO_F64 ? poisson_impl<double>(plan, f, psi, ws, s)
+                                     : poisson_impl<float>(plan, f, psi, ws, s);
+}
+
+int aero_ns3d_project(const AeroNs3dPlan *plan, void *u, void *v, void *w, void *psi, void *workspace, void *stream) {
+  if (!plan || !u || !v || !w || !psi || !workspace) return fail(AERO_EINVAL, "null argument");
+  auto s = static_cast<cudaStream_t>(stream);
+  auto ws = static_cast<unsigned char *>(workspace);
+  return plan->cfg.dtype == AERO_F64 ? project_impl<double>(plan, u, v, w, psi, ws, s)
+                                     : project_impl<float>(plan, u, v, w, psi, ws, s);
+}
+
+int aero_ns3d_read_status(const AeroNs3dPlan *plan, const void *workspace, int32_t *status, void *stream) {
+  if (!plan || !workspace || !status) return fail(AERO_EINVAL, "null argument");
+  auto s = static_cast<cudaStream_t>(stream);
+  int v = 0;
+  CUDA_TRY(cudaMemcpyAsync(&v, static_cast<const unsigned char *>(workspace) + plan->off_status, sizeof(int),
+                           cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  *status = v;
+  return AERO_OK;
+}
+
+}  // extern "C"

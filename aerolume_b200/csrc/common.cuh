@@ -1,0 +1,134 @@
+// Shared device helpers of the B200 Navier-Stokes kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/aero_b200.h"
+
+namespace aero {
+
+// Ghost-cell rules of Aerolume ns3d/core.py:147-246 as index maps.  A ghost entry g
+// (g < 0 or g >= n along an axis of n entries) takes the value s * x[map(g)] + c.
+// Rules of the three axes compose in the order x, then y, then z (core.py:249-272):
+//   value = sz * (sy * (sx * x + cx) + cy) + cz.
+template <typename T>
+__device__ __forceinline__ int ghost_map(int g, int n, int kind_lo, int kind_hi, T val_lo, T val_hi, T &s, T &c) {
+  s = T(1);
+  c = T(0);
+  if (g >= 0 && g < n) return g;
+  const bool lo = g < 0;
+  if (lo) {
+    if (g < -2) g = -2;
+  } else if (g > n + 1) {
+    g = n + 1;
+  }
+  const int kind = lo ? kind_lo : kind_hi;
+  int m;
+  switch (kind) {
+    case AERO_GHOST_EDGE: m = lo ? 0 : n - 1; break;
+    case AERO_GHOST_EVEN: m = lo ? -1 - g : 2 * n - 1 - g; break;
+    case AERO_GHOST_ODD: m = lo ? -1 - g : 2 * n - 1 - g; s = T(-1); break;
+    case AERO_GHOST_AFFINE:
+      m = lo ? -1 - g : 2 * n - 1 - g;
+      s = T(-1);
+      c = T(2) * (lo ? val_lo : val_hi);
+      break;
+    case AERO_GHOST_FACE_ODD: m = lo ? -g : 2 * (n - 1) - g; s = T(-1); break;
+    case AERO_GHOST_PERIODIC_CELL: m = lo ? g + n : g - n; break;
+    default: m = lo ? g + n - 1 : g - n + 1; break;  // periodic_face
+  }
+  if (m < 0) m = 0;
+  if (m > n - 1) m = n - 1;
+  return m;
+}
+
+// The rules of one staggered component on its (n2, n1, n0) = (z, y, x) array.
+template <typename T>
+struct CompRules {
+  int n0, n1, n2;
+  int kind[3][2];
+  T val[3][2];
+};
+
+// Value of the ghost-padded component at (k, j, i) (each index may lie up to two
+// entries outside the array).
+template <typename T>
+__device__ __forceinline__ T padded(const T *__restrict__ f, const CompRules<T> &r, int k, int j, int i) {
+  T sx, cx, sy, cy, sz, cz;
+  const int mi = ghost_map<T>(i, r.n0, r.kind[0][0], r.kind[0][1], r.val[0][0], r.val[0][1], sx, cx);
+  const int mj = ghost_map<T>(j, r.n1, r.kind[1][0], r.kind[1][1], r.val[1][0], r.val[1][1], sy, cy);
+  const int mk = ghost_map<T>(k, r.n2, r.kind[2][0], r.kind[2][1], r.val[2][0], r.val[2][1], sz, cz);
+  const T x = __ldg(f + ((size_t)mk * r.n1 + mj) * r.n0 + mi);
+  return sz * (sy * (sx * x + cx) + cy) + cz;
+}
+
+// Temperature ghosts of ns3d/physics.py:589-621: one side's rule on the six faces; edge
+// and corner ghosts are never read (the MUSCL stencil runs along one axis at a time).
+struct ThetaSides {
+  int kind[6];
+  double val[6];
+};
+
+template <typename T>
+__device__ __forceinline__ T theta_padded(const T *__restrict__ c, int nz, int ny, int nx, const ThetaSides &sd,
+                                          T h, int k, int j, int i) {
+  const bool ox = i < 0 || i >= nx, oy = j < 0 || j >= ny, oz = k < 0 || k >= nz;
+  if (!ox && !oy && !oz) return __ldg(c + ((size_t)k * ny + j) * nx + i);
+  if ((int)ox + (int)oy + (int)oz > 1) return T(0);
+  int g, n, side;
+  if (ox) {
+    g = i; n = nx; side = i < 0 ? 0 : 1;
+  } else if (oy) {
+    g = j; n = ny; side = j < 0 ? 2 : 3;
+  } else {
+    g = k; n = nz; side = k < 0 ? 4 : 5;
+  }
+  const bool lo = (side & 1) == 0;
+  if (lo && g < -2) g = -2;
+  if (!lo && g > n + 1) g = n + 1;
+  auto at = [&](int m) -> T {
+    if (m < 0) m = 0;
+    if (m > n - 1) m = n - 1;
+    if (ox) return __ldg(c + ((size_t)k * ny + j) * nx + m);
+    if (oy) return __ldg(c + ((size_t)k * ny + m) * nx + i);
+    return __ldg(c + ((size_t)m * ny + j) * nx + i);
+  };
+  const int kind = sd.kind[side];
+  const T val = T(sd.val[side]);
+  if (kind == AERO_TH_PERIODIC) return at(lo ? g + n : g - n);
+  if (kind == AERO_TH_OUTFLOW) return at(lo ? 0 : n - 1);
+  const T mirror = at(lo ? -1 - g : 2 * n - 1 - g);
+  switch (kind) {
+    case AERO_TH_ADIABATIC: return mirror;
+    case AERO_TH_INFLOW: return val;
+    case AERO_TH_TEMPERATURE: return T(2) * val - mirror;
+    default: {  // heat flux: + G h on the first layer, + 3 G h on the second
+      const T w = (lo ? (g == -2) : (g == n + 1)) ? T(3) : T(1);
+      return mirror + val * (w * h);
+    }
+  }
+}
+
+// torch.lerp's two-branch formula (the reference blends RK stages with it).
+template <typename T>
+__device__ __forceinline__ T lerp_t(T s, T e, T w) {
+  return (w < T(0.5)) ? s + w * (e - s) : e - (e - s) * (T(1) - w);
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Non-negative maxima through the ordered bit patterns of IEEE doubles (NaN wins,
+// which the status check then reports).
+__device__ __forceinline__ void atomic_max_nonneg(unsigned long long *addr, double v) {
+  atomicMax(addr, (unsigned long long)__double_as_longlong(v));
+}
+
+__device__ __forceinline__ double as_double(unsigned long long bits) { return __longlong_as_double((long long)bits); }
+
+}  // namespace aero

@@ -1,0 +1,138 @@
+// Kernel parameter blocks and launchers of the 3D step (internal to libaero_b200.so).
+#pragma once
+
+#include <algorithm>
+#include <cstddef>
+
+#include "common.cuh"
+
+namespace aero {
+
+// scalar slots of the workspace's double block
+enum : int {
+  SC_MAXU = 0,
+  SC_MAXV = 1,
+  SC_MAXW = 2,
+  SC_MAXT = 3,
+  SC_NUTMAX = 4,
+  SC_DT = 5,
+  SC_SUM_INLET = 6,
+  SC_SUM_U0 = 7,       // sum u0[..., nx]
+  SC_SUMS = 8,         // 3 stages x (sum up[nx], sum up[nx-1], spare)
+  SC_COUNT = 20
+};
+
+enum : int { MODE_STAGE = 0, MODE_NUT_ONLY = 1 };
+
+template <typename T>
+struct StageParams {
+  int nx, ny, nz, zc, mode;
+  T h, inv_h;
+  CompRules<T> ru, rv, rw;
+  int px, py, pz, closed;
+  int upwind, les;
+  T kadv, nu_h2, les_cd2;
+  // stage
+  T a, bdt_scale, wgt;
+  const T *dt;
+  const T *up, *vp, *wp;      // stage-start velocity (ghosts by rule)
+  const T *u0, *v0, *w0;      // step-start velocity (RK blend)
+  T *uh, *vh, *wh;            // stage value out
+  const T *u_inlet;
+  const T *outlet_corr;       // device scalar: the outlet mass-balance correction
+  // window
+  int has_win, win[6], wnx, wny, nbody, nq;
+  T eta;
+  const T *chi_u, *chi_v, *chi_w, *chi_c, *a_u, *a_v, *a_w, *k_u, *k_v, *k_w;
+  double *partials;           // [block][nq] (this stage's slice)
+  unsigned long long *nut_max;
+  // heat
+  int thermal, has_adia, n_tbody;
+  ThetaSides sides;
+  T kh, kprt, kappa, ri, eta_t;
+  const T *thp, *th0;
+  T *thh;
+  const T *chi_t, *a_t, *w_t, *adia_u, *adia_v, *adia_w, *vol_w, *skin;
+};
+
+struct DtParams {
+  double *scalars;
+  const void *dt_in;
+  void *dt_out;
+  int *status;
+  int has_dt_fixed, les, thermal, has_heat_max;
+  double dt_fixed, cfl, h, nu, viscous_dt, kappa, prt, ri, heat_max;
+};
+
+template <typename T>
+struct CorrectParams {
+  int nx, ny, nz, px, py, pz;
+  T inv_h;
+  const T *uh, *vh, *wh, *psi;
+  T *u, *v, *w;
+};
+
+template <typename T>
+struct SmokeParams {
+  int nx, ny, nz, px, py, pz;
+  T inv_h;
+  const T *c0, *u, *v, *w, *dt, *t0, *t_new;  // t_new NULL: t0 + dt
+  T *c;
+  const T *chi_c;
+  int win[6];
+  const T *weight;
+  int dwin[6];
+  double pulse_on, pulse_period;
+};
+
+template <typename T>
+struct FinalizeParams {
+  size_t ncell;
+  int nbody, nq, nblocks, n_tbody, symmetry;
+  const double *partials;
+  double h, pe, y0, moment_ref_y, ref_area, span_ref, length_ref;
+  int t_index[AERO_MAX_BODIES];
+  double flux_rate[AERO_MAX_BODIES];
+  const T *dt, *t0;
+  T *t_out, *dt_out, *coeffs, *heat_rate, *p;
+  int *status;
+};
+
+template <typename T>
+struct AxisTables {
+  int n, method, kind, nfac;
+  int fac[16];
+  const T *tw, *post, *cs, *dense;
+  const double *lam;
+  T s0, s1, rsqrt_n;
+};
+
+template <typename T>
+struct TransformParams {
+  const T *in;
+  T *out;
+  int nx, ny, nz, axis, mode, L;  // mode: 0 forward, 1 inverse, 2 forward-solve-inverse
+  AxisTables<T> A;
+  const double *lam_x, *lam_y;
+};
+
+template <typename T> size_t stage_smem_bytes();
+template <typename T> cudaError_t launch_stage(const StageParams<T> &, cudaStream_t);
+template <typename T> cudaError_t launch_absmax(const T *, size_t, unsigned long long *, cudaStream_t);
+template <typename T> cudaError_t launch_dt(const DtParams &, cudaStream_t);
+template <typename T> cudaError_t launch_outlet_sum(const T *, const T *, int, int, double *, cudaStream_t);
+template <typename T>
+cudaError_t launch_outlet_corr(const double *, const double *, const double *, const T *, double, double, double,
+                               double, T *, cudaStream_t);
+template <typename T>
+cudaError_t launch_divergence(const T *, const T *, const T *, int, int, int, int, int, int, T, T *, cudaStream_t);
+template <typename T> cudaError_t launch_correct(const CorrectParams<T> &, cudaStream_t);
+template <typename T> cudaError_t launch_smoke(const SmokeParams<T> &, cudaStream_t);
+template <typename T> cudaError_t launch_finalize(const FinalizeParams<T> &, cudaStream_t);
+template <typename T> cudaError_t launch_psi_accumulate(const T *, T *, size_t, T, int, cudaStream_t);
+template <typename T> size_t transform_smem_bytes(int, int);
+template <typename T> cudaError_t launch_transform(const TransformParams<T> &, cudaStream_t);
+template <typename T>
+cudaError_t launch_axis_tables(int, int, int, double, T *, T *, T *, double *, T *, cudaStream_t);
+
+}  // namespace aero

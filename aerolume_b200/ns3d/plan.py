@@ -1,0 +1,297 @@
+"""One 3D configuration bound to the C ABI: constants, device masks and the workspace.
+
+:class:`Ns3dPlan` reads the reference's objects by attribute (``Ops3D``, ``Geometry3D``,
+``ThermalOps``, ``DyeSources``: the containers of :mod:`aerolume_b200.ns3d.types` or the
+reference's own), validates what the B200 step supports, uploads the window masks once
+and owns the device workspace.  Unsupported physics (fans, ports, paint, heat sources, a
+PID step controller, more than eight bodies) raises ``RuntimeError``: there is no
+fallback to a CPU or plain-torch path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from .. import _lib
+from .._lib import ADV, F32, F64, GHOST, LES, MAX_BODIES, THETA_SIDE, check
+
+
+def _f(x) -> float:
+    return float(x.item() if torch.is_tensor(x) else x)
+
+
+def _torch_dtype(ops):
+    dt = getattr(ops, "dtype", "float32")
+    if isinstance(dt, torch.dtype):
+        return dt
+    return torch.float64 if str(dt) in ("float64", "torch.float64") else torch.float32
+
+
+def _window_empty(win) -> bool:
+    k0, k1, j0, j1, i0, i1 = win
+    return k1 <= k0 or j1 <= j0 or i1 <= i0
+
+
+class Ns3dPlan:
+    """Plan + device tensors for one (ops, geom, thermal, smoke) configuration.
+
+    ``thermal`` is a ``ThermalOps`` (or None); ``dye_src`` a ``DyeSources`` (or None);
+    ``smoke`` turns the smoke update on inside :meth:`step`.
+    """
+
+    def __init__(self, ops, geom, thermal=None, dye_src=None, *, smoke: bool = False, device=None):
+        self.device = torch.device(device) if device is not None else torch.device("cuda")
+        if self.device.type != "cuda":
+            raise RuntimeError("the B200 step runs on a CUDA device only (no CPU fallback)")
+        if not torch.cuda.is_available():
+            raise RuntimeError("CUDA is not available: the B200 step has no CPU fallback")
+        L = _lib.lib()
+        self.dtype = _torch_dtype(ops)
+        self.ops, self.geom, self.thermal, self.dye_src = ops, geom, thermal, dye_src
+        self.smoke = bool(smoke)
+        nx, ny, nz = int(ops.nx), int(ops.ny), int(ops.nz)
+        self.shape = (nz, ny, nx)
+        cfg = _lib.Ns3dConfig()
+        cfg.abi_version = _lib.ABI_VERSION
+        cfg.dtype = F64 if self.dtype == torch.float64 else F32
+        cfg.nx, cfg.ny, cfg.nz = nx, ny, nz
+        cfg.h = float(ops.h)
+        px, py, pz = (bool(x) for x in ops.periodic_axes)
+        cfg.periodic[0], cfg.periodic[1], cfg.periodic[2] = int(px), int(py), int(pz)
+        cfg.closed = int(bool(getattr(ops, "closed", False)))
+        cfg.symmetry = int(bool(getattr(ops, "symmetry", False)))
+        if ops.advection not in ADV:
+            raise RuntimeError(f"unsupported advection scheme {ops.advection!r}")
+        cfg.advection = ADV[ops.advection]
+        if ops.turbulence not in LES:
+            raise RuntimeError(f"unsupported turbulence model {ops.turbulence!r}")
+        cfg.les = LES[ops.turbulence]
+        cfg.les_c = float(ops.les_c)
+        cfg.nu = float(ops.nu_value)
+        cfg.eta = _f(ops.eta)
+        cfg.cfl = float(ops.cfl)
+        if getattr(ops, "dt_fixed", None) is not None:
+            cfg.has_dt_fixed = 1
+            cfg.dt_fixed = float(ops.dt_fixed)
+        for c, comp in enumerate("uvw"):
+            for a in range(3):
+                for s in range(2):
+                    kind, val = ops.ghost[comp][a][s]
+                    cfg.ghost_kind[c][a][s] = GHOST[kind]
+                    cfg.ghost_val[c][a][s] = float(val)
+        cfg.ref_area = float(ops.ref_area)
+        cfg.length_ref = float(ops.length_ref)
+        cfg.span_ref = float(ops.span_ref)
+        for q in range(3):
+            cfg.moment_ref[q] = float(ops.moment_ref[q])
+        cfg.y0 = float(ops.y0)
+        if getattr(ops, "forcing", None) is not None:
+            raise RuntimeError("a uniform body force (verification forcing) is not supported by the B200 step")
+        self.nbody = int(geom.nbody)
+        win = tuple(int(x) for x in geom.window)
+        self.has_win = not _window_empty(win) and self.nbody > 0
+        if self.nbody > MAX_BODIES:
+            raise RuntimeError(f"the B200 step supports at most {MAX_BODIES} bodies")
+        for q in range(6):
+            cfg.window[q] = win[q] if self.has_win else 0
+        cfg.nbody = self.nbody
+        self._keep = []
+        dev, dt = self.device, self.dtype
+
+        def up(x):
+            if x is None:
+                return None
+            t = torch.as_tensor(np.asarray(x) if not torch.is_tensor(x) else x)
+            t = t.to(device=dev, dtype=dt).contiguous()
+            self._keep.append(t)
+            return t
+
+        g = _lib.Ns3dGeom()
+        if self.has_win:
+            for name in ("chi_u", "chi_v", "chi_w", "chi_c", "a_u", "a_v", "a_w", "k_u", "k_v", "k_w"):
+                setattr(g, name, up(getattr(geom, name)).data_ptr())
+        u_in = getattr(ops, "u_inlet", None)
+        if u_in is not None:
+            g.u_inlet = up(torch.as_tensor(np.asarray(u_in) if not torch.is_tensor(u_in) else u_in)
+                           .reshape(nz, ny)).data_ptr()
+        if thermal is not None:
+            self._thermal_config(cfg, g, thermal, up)
+        if self.smoke:
+            cfg.smoke = 1
+            if dye_src is not None and not _window_empty(dye_src.window):
+                for q in range(6):
+                    cfg.dye_window[q] = int(dye_src.window[q])
+                g.dye_weight = up(dye_src.weight).data_ptr()
+                pulse = [_f(x) for x in (dye_src.pulse if not torch.is_tensor(dye_src.pulse) else dye_src.pulse.tolist())]
+                cfg.pulse_on, cfg.pulse_period = pulse[0], pulse[1]
+            else:
+                cfg.pulse_on, cfg.pulse_period = 2.0, 1.0
+        self.cfg = cfg
+        self.geom_c = g
+        handle = C.c_void_p()
+        check(L.aero_ns3d_plan_create(C.byref(cfg), C.byref(handle)), "aero_ns3d_plan_create")
+        self._handle = handle
+        nbytes = L.aero_ns3d_workspace_bytes(handle)
+        self._ws_raw = torch.empty(nbytes + 256, dtype=torch.uint8, device=dev)
+        base = self._ws_raw.data_ptr()
+        self.ws_ptr = (base + 255) & ~255
+        self.workspace_bytes = nbytes
+        check(L.aero_ns3d_workspace_init(handle, C.c_void_p(self.ws_ptr), self._stream()),
+              "aero_ns3d_workspace_init")
+
+    # -------------------------------------------------------------------- set-up
+    def _thermal_config(self, cfg, g, th, up):
+        srcs = getattr(th, "sources", None)
+        if srcs is not None and len(getattr(srcs, "items", [])):
+            raise RuntimeError("volumetric heat sources are not supported by the B200 step")
+        cfg.thermal = 1
+        cfg.kappa, cfg.pe, cfg.ri, cfg.prt = float(th.kappa), float(th.pe), float(th.ri), float(th.prt)
+        cfg.eta_t = _f(th.eta)
+        vals = th.side_vals.tolist() if torch.is_tensor(th.side_vals) else list(th.side_vals)
+        for q in range(6):
+            cfg.side_kind[q] = THETA_SIDE[th.side_kinds[q]]
+            cfg.side_val[q] = float(vals[q])
+        hm = getattr(th, "heat_max", None)
+        if hm is not None:
+            cfg.has_heat_max = 1
+            cfg.heat_max = _f(hm)
+        tg = th.geom
+        t_index = list(getattr(tg, "t_index", []) or [])
+        if self.has_win:
+            cfg.n_tbody = len(t_index)
+            for q, b in enumerate(t_index):
+                cfg.t_index[q] = int(b)
+            if tg.chi_t is not None:
+                g.chi_t = up(tg.chi_t).data_ptr()
+                g.a_t = up(tg.a_t).data_ptr()
+                g.w_t = up(tg.w_t).data_ptr()
+            if tg.adia is not None:
+                cfg.has_adia = 1
+                g.adia_u, g.adia_v, g.adia_w = (up(a).data_ptr() for a in tg.adia)
+            if tg.vol_w is not None:
+                g.vol_w = up(tg.vol_w).data_ptr()
+            if getattr(tg, "skin", None) is not None:
+                cfg.has_skin = 1
+                g.skin = up(tg.skin).data_ptr()
+        fr = getattr(tg, "flux_rate", None)
+        if fr is not None:
+            vals = fr.tolist() if torch.is_tensor(fr) else list(np.asarray(fr).reshape(-1))
+            for q, x in enumerate(vals[:MAX_BODIES]):
+                cfg.flux_rate[q] = float(x)
+
+    def _stream(self):
+        return C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+
+    def __del__(self):
+        h = getattr(self, "_handle", None)
+        if h is not None and h.value:
+            try:
+                _lib.lib().aero_ns3d_plan_destroy(h)
+            except Exception:  # pragma: no cover - interpreter shutdown
+                pass
+            self._handle = None
+
+    # -------------------------------------------------------------------- buffers
+    def empty_fields(self):
+        """Fresh device tensors for a step's outputs."""
+        nz, ny, nx = self.shape
+        kw = {"device": self.device, "dtype": self.dtype}
+        out = {"u": torch.empty(nz, ny, nx + 1, **kw), "v": torch.empty(nz, ny + 1, nx, **kw),
+               "w": torch.empty(nz + 1, ny, nx, **kw), "p": torch.empty(nz, ny, nx, **kw),
+               "t": torch.empty((), **kw), "dt": torch.empty((), **kw),
+               "coeffs": torch.zeros(max(self.nbody, 0), 6, **kw)}
+        if self.thermal is not None:
+            out["theta"] = torch.empty(nz, ny, nx, **kw)
+            out["heat_rate"] = torch.zeros(max(self.nbody, 0), **kw)
+        if self.smoke:
+            out["dye"] = torch.empty(nz, ny, nx, **kw)
+        return out
+
+    def _check(self, name, t, shape):
+        if not torch.is_tensor(t) or t.device != self.device or t.dtype != self.dtype or not t.is_contiguous():
+            raise RuntimeError(f"{name} must be a contiguous {self.dtype} tensor on {self.device}")
+        if tuple(t.shape) != tuple(shape):
+            raise RuntimeError(f"{name} has shape {tuple(t.shape)}, expected {tuple(shape)}")
+
+    # -------------------------------------------------------------------- calls
+    def step(self, u0, v0, w0, t0, *, theta0=None, dye0=None, out=None, dt=None, events=None):
+        """One step (plus the smoke update when the plan has smoke); returns the output dict.
+
+        ``out`` (from :meth:`empty_fields`) may hold ``u0 / v0 / w0 / theta0`` themselves
+        (in-place update); ``dt`` is None (CFL rule on the device) or a 0-d device tensor.
+        ``events``: a list of ``torch.cuda.Event(enable_timing=True)`` recorded at the step's
+        phase boundaries (``aero_ns3d_step_traced``)."""
+        nz, ny, nx = self.shape
+        self._check("u0", u0, (nz, ny, nx + 1))
+        self._check("v0", v0, (nz, ny + 1, nx))
+        self._check("w0", w0, (nz + 1, ny, nx))
+        self._check("t0", t0, ())
+        out = self.empty_fields() if out is None else out
+        f = _lib.Ns3dFields()
+        f.u0, f.v0, f.w0, f.t0 = u0.data_ptr(), v0.data_ptr(), w0.data_ptr(), t0.data_ptr()
+        for name in ("u", "v", "w", "p", "t", "dt", "coeffs"):
+            setattr(f, name, out[name].data_ptr())
+        if self.thermal is not None:
+            if theta0 is None:
+                raise RuntimeError("this plan has heat transfer: theta0 is required")
+            self._check("theta0", theta0, (nz, ny, nx))
+            f.theta0, f.theta, f.heat_rate = theta0.data_ptr(), out["theta"].data_ptr(), out["heat_rate"].data_ptr()
+        if self.smoke:
+            if dye0 is None:
+                raise RuntimeError("this plan has smoke: dye0 is required")
+            self._check("dye0", dye0, (nz, ny, nx))
+            f.dye0, f.dye = dye0.data_ptr(), out["dye"].data_ptr()
+        dtp = None
+        if dt is not None:
+            self._check("dt", dt, ())
+            dtp = C.c_void_p(dt.data_ptr())
+        L = _lib.lib()
+        if events is None:
+            check(L.aero_ns3d_step(self._handle, C.byref(f), C.byref(self.geom_c), dtp, C.c_void_p(self.ws_ptr),
+                                   self._stream()), "aero_ns3d_step")
+        else:
+            arr = (C.c_void_p * len(events))(*[C.c_void_p(e.cuda_event) for e in events])
+            check(L.aero_ns3d_step_traced(self._handle, C.byref(f), C.byref(self.geom_c), dtp, C.c_void_p(self.ws_ptr),
+                                          self._stream(), arr, len(events)), "aero_ns3d_step_traced")
+        return out
+
+    def smoke_step(self, dye0, u, v, w, t_new, dt, out=None):
+        """The smoke update alone with the given velocity, step and new time."""
+        if not self.smoke:
+            raise RuntimeError("this plan was built without smoke")
+        nz, ny, nx = self.shape
+        self._check("dye0", dye0, (nz, ny, nx))
+        out = torch.empty_like(dye0) if out is None else out
+        f = _lib.Ns3dFields()
+        f.dye0, f.dye = dye0.data_ptr(), out.data_ptr()
+        f.u, f.v, f.w, f.t, f.dt = u.data_ptr(), v.data_ptr(), w.data_ptr(), t_new.data_ptr(), dt.data_ptr()
+        check(_lib.lib().aero_ns3d_smoke(self._handle, C.byref(f), C.byref(self.geom_c), self._stream()),
+              "aero_ns3d_smoke")
+        return out
+
+    def poisson_solve(self, f, psi=None):
+        self._check("f", f, self.shape)
+        psi = torch.empty_like(f) if psi is None else psi
+        check(_lib.lib().aero_ns3d_poisson_solve(self._handle, C.c_void_p(f.data_ptr()), C.c_void_p(psi.data_ptr()),
+                                                 C.c_void_p(self.ws_ptr), self._stream()), "aero_ns3d_poisson_solve")
+        return psi
+
+    def project(self, u, v, w):
+        """In place (u, v, w) <- projection; returns psi."""
+        psi = torch.empty(self.shape, device=self.device, dtype=self.dtype)
+        check(_lib.lib().aero_ns3d_project(self._handle, C.c_void_p(u.data_ptr()), C.c_void_p(v.data_ptr()),
+                                           C.c_void_p(w.data_ptr()), C.c_void_p(psi.data_ptr()),
+                                           C.c_void_p(self.ws_ptr), self._stream()), "aero_ns3d_project")
+        return psi
+
+    def status(self) -> int:
+        """Device status word of the last step (synchronises): 0, or bit 0 = non-finite value."""
+        v = C.c_int32()
+        check(_lib.lib().aero_ns3d_read_status(self._handle, C.c_void_p(self.ws_ptr), C.byref(v), self._stream()),
+              "aero_ns3d_read_status")
+        return int(v.value)
+
+
+__all__ = ["Ns3dPlan"]

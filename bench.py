@@ -1,0 +1,348 @@
+"""Throughput of the B200 3D Navier-Stokes step (Mcell-steps/s) on the bluff-box workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: 256 x 128 x 128 FP32 cells (4.19 M), box 1 x 1 x 0.5 on a moving floor, WALE LES,
+Boussinesq temperature (body 10 K above the stream, Pr 0.71, Ri 0.1 on the body height),
+one 16-nozzle smoke rake; seeded N(0, 1e-3) noise on a uniform stream, projected.  One
+"step" is one SSP-RK3 time step with its three projections, the temperature stages, the
+forces and heat rates, and the smoke update.
+
+``value``: steps with the state resident in HBM, K steps captured in one CUDA graph and
+replayed once between a barrier and ``torch.cuda.synchronize()``, timed with CUDA events
+(max over ranks).  ``e2e``: the same step through the public plan API with host buffers --
+every step copies the state in from pinned host memory and the new state, coefficients and
+heat rates back out.  ``roofline``: the dominant kernel's algorithmic bytes per launch over
+its event-timed mean duration against the measured HBM copy bandwidth.  ``cpu_baseline``:
+the numpy oracle (a restatement of the reference's plain-torch step) on a bounded sample of
+the same workload on this host.
+
+With ``--gpus N`` (N > 1, launched by torch.distributed.run) every rank advances its own
+replica (no data-path collective: a single instance of this solver does not shard), and
+``value`` is the total over ranks.  ``--impl reference`` times the reference arm: the
+oracle's CPU step on rank 0 (other ranks exit without work).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Mcell-steps/s on 1 B200: plain vs batched vs learned closure, at stated error"
+UNIT = "Mcell-steps/s"
+SHAPE = (256, 128, 128)
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _config(nx, ny, nz, extra=None):
+    cfg = {"workload": f"box on moving floor {nx}x{ny}x{nz} FP32, WALE, Boussinesq heat, 1 smoke rake",
+           "cells": nx * ny * nz, "grid": [nx, ny, nz], "inputs_vs_l2": "working set ~1 GB > 126 MB L2 (no flush)",
+           "parallelism": "replicas"}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region (median SM clock, throttle reasons)."""
+
+    def __init__(self, index):
+        self.proc = None
+        self.path = ROOT / "gpurun_out" / f"clocks_{os.getpid()}.csv"
+        try:
+            self.path.parent.mkdir(exist_ok=True)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={index}",
+                 "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        rows = [r.split(",") for r in self.path.read_text().splitlines() if r.strip()]
+        try:
+            self.path.unlink()
+        except OSError:
+            pass
+        sm = [float(r[0]) for r in rows if r[0].strip().replace(".", "").isdigit()]
+        if not sm:
+            return None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if len(r) > 3 + i and "Active" in r[3 + i]})
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(rows[0][1]), "reasons": reasons,
+                "samples": len(sm)}
+
+
+def oracle_sample(nx, ny, nz, steps):
+    """Wall time of ``steps`` oracle steps (after one untimed step) on the full workload."""
+    from aerolume_b200.ns3d.workloads import box_on_moving_floor, initial_state
+    from oracle import ns3d as O
+    ops, geom, th, src, _ = box_on_moving_floor(nx, ny, nz, dtype="float32")
+    u, v, w = (x.numpy() for x in initial_state(ops, device="cpu"))
+    f32 = np.float32
+    ps = O.PoissonSolver3D(nx, ny, nz, ops.h, ops.periodic_axes, f32)
+    u, v, w, _ = O.project3d(u, v, w, ops, ps)
+    theta = np.zeros((nz, ny, nx), f32)
+    dye = np.zeros((nz, ny, nx), f32)
+    t = f32(0.0)
+
+    def one(u, v, w, t, theta, dye):
+        r = O.step3d_phys(u, v, w, t, geom, ops, ps, th=th, theta=theta)
+        c = O.apply_solids_and_sources(O.advect_dye3d(dye, r.u, r.v, r.w, r.dt, ops), r.t, geom, src)
+        return r.u, r.v, r.w, r.t, r.theta, c
+
+    u, v, w, t, theta, dye = one(u, v, w, t, theta, dye)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        u, v, w, t, theta, dye = one(u, v, w, t, theta, dye)
+    return time.perf_counter() - t0
+
+
+def _threads():
+    try:
+        from threadpoolctl import threadpool_info
+        return max([i.get("num_threads", 1) for i in threadpool_info()] + [1])
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def run_reference(args, rank):
+    nx, ny, nz = args.shape
+    if rank != 0:
+        return
+    steps = max(1, min(args.steps, 3))
+    secs = oracle_sample(nx, ny, nz, steps)
+    val = nx * ny * nz * steps / secs / 1e6
+    sample = f"{steps} full {nx}x{ny}x{nz} steps of the numpy oracle after 1 untimed step"
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": steps, "warmup": 1, "ms_per_step": 1e3 * secs / steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": _config(nx, ny, nz),
+            "cpu_baseline": {"value": val, "unit": UNIT, "cores": _threads(), "kind": "port", "sample": sample},
+            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def launches_per_step(plan):
+    """Kernels one aero_ns3d_step launches (the sequence in csrc/capi.cu)."""
+    c = plan.cfg
+    tunnel = not c.periodic[0] and not c.closed
+    n = 3 + (1 if c.thermal else 0)                # |u|, |v|, |w|, |theta| maxima
+    n += 1 if c.les else 0                          # eddy-viscosity pre-pass
+    n += 1                                          # dt
+    n += 1 if tunnel else 0                         # inlet / u0 outlet sums
+    per_stage = 1 + 1 + 5 + 1 + 1 + (2 if tunnel else 0)   # stage, divergence, 5 transforms, psi_w, correction
+    n += 3 * per_stage
+    n += 1 if c.smoke else 0
+    n += 1                                          # finalize
+    return n
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from aerolume_b200.ns3d.plan import Ns3dPlan
+    from aerolume_b200.ns3d.workloads import box_on_moving_floor, initial_state
+    from aerolume_b200 import _lib
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    nx, ny, nz = args.shape
+    cells = nx * ny * nz
+    ops, geom, th, src, _ = box_on_moving_floor(nx, ny, nz, dtype="float32", seed=0)
+    plan = Ns3dPlan(ops, geom, th, src, smoke=True, device=dev)
+    u, v, w = initial_state(ops, seed=rank, device=dev)
+    plan.project(u, v, w)
+    theta = torch.zeros(nz, ny, nx, device=dev)
+    dyes = [torch.zeros(nz, ny, nx, device=dev), torch.zeros(nz, ny, nx, device=dev)]
+    t = torch.zeros((), device=dev)
+    out = plan.empty_fields()
+    out["u"], out["v"], out["w"], out["theta"] = u, v, w, theta
+
+    def step(j, events=None):
+        out["dye"] = dyes[(j + 1) % 2]
+        plan.step(u, v, w, t, theta0=theta, dye0=dyes[j % 2], out=out, events=events)
+        t.copy_(out["t"])
+
+    # ---- warm-up (eager), then capture exactly K steps with phase events in one graph
+    for j in range(args.warmup):
+        step(j)
+    torch.cuda.synchronize()
+    K = args.steps
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(_lib.TRACE_EVENTS)] for _ in range(K)]
+    for row in ev:                          # torch creates the CUDA event on its first record
+        for e in row:
+            e.record()
+    torch.cuda.synchronize()
+    s = torch.cuda.Stream(device=dev)
+    s.wait_stream(torch.cuda.current_stream(dev))
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(s):
+        with torch.cuda.graph(g, stream=s):
+            for j in range(K):
+                step(args.warmup + j, ev[j])
+    torch.cuda.current_stream(dev).wait_stream(s)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    clocks = Clocks(local_rank) if rank == 0 else None
+    time.sleep(0.3 if clocks else 0.0)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    start.record()
+    g.replay()
+    end.record()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    ms = start.elapsed_time(end)
+    clk = clocks.stop() if clocks else None
+    status = plan.status()
+    if dist is not None:
+        tt = torch.tensor([ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    # ---- phase times from the events (mean over the K captured steps)
+    def span(j, a, b):
+        return ev[j][a].elapsed_time(ev[j][b])
+    stage_ms = [span(j, 2 + 5 * st, 3 + 5 * st) for j in range(K) for st in range(3)]
+    poisson_ms = [span(j, 4 + 5 * st, 5 + 5 * st) for j in range(K) for st in range(3)]
+    phases = {
+        "time_step": float(np.mean([span(j, 0, 1) for j in range(K)])),
+        "outlet_corr": float(np.mean([span(j, 1 + 5 * st if st else 1, 2 + 5 * st) for j in range(K) for st in range(3)])),
+        "stage_kernel": float(np.mean(stage_ms)),
+        "divergence": float(np.mean([span(j, 3 + 5 * st, 4 + 5 * st) for j in range(K) for st in range(3)])),
+        "poisson": float(np.mean(poisson_ms)),
+        "correct": float(np.mean([span(j, 5 + 5 * st, 6 + 5 * st) for j in range(K) for st in range(3)])),
+        "smoke": float(np.mean([span(j, 16, 17) for j in range(K)])),
+        "finalize": float(np.mean([span(j, 17, 18) for j in range(K)])),
+    }
+    # ---- e2e through the public API with host buffers
+    e2e = None
+    if rank == 0 or world > 1:
+        host_in = {k: torch.empty(x.shape, dtype=x.dtype, pin_memory=True)
+                   for k, x in (("u", u), ("v", v), ("w", w), ("theta", theta), ("dye", dyes[0]), ("t", t))}
+        for k, x in (("u", u), ("v", v), ("w", w), ("theta", theta), ("dye", dyes[0]), ("t", t)):
+            host_in[k].copy_(x)
+        host_out = {k: torch.empty(x.shape, dtype=x.dtype, pin_memory=True) for k, x in out.items()}
+        d_in = {k: torch.empty_like(x, device=dev) for k, x in host_in.items()}
+        o2 = plan.empty_fields()
+        h2d = sum(x.numel() * x.element_size() for x in host_in.values())
+        d2h = sum(x.numel() * x.element_size() for x in host_out.values())
+        torch.cuda.synchronize()
+        ke = max(3, min(K, 10))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(ke):
+            for k in host_in:
+                d_in[k].copy_(host_in[k], non_blocking=True)
+            plan.step(d_in["u"], d_in["v"], d_in["w"], d_in["t"], theta0=d_in["theta"], dye0=d_in["dye"], out=o2)
+            for k in host_out:
+                host_out[k].copy_(o2[k], non_blocking=True)
+            # the next step starts from this step's result, as a host caller's loop would
+            for k in ("u", "v", "w", "theta", "dye", "t"):
+                host_in[k], host_out[k] = host_out[k], host_in[k]
+        e1.record()
+        torch.cuda.synchronize()
+        ems = e0.elapsed_time(e1) / ke
+        if dist is not None:
+            tt = torch.tensor([ems], device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ems = float(tt.item())
+        e2e = {"value": world * cells / (ems * 1e-3) / 1e6, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "ms_per_step": ems, "steps": ke}
+    if rank != 0:
+        return
+    peak, peak_kind = _peaks()
+    # dominant kernel: the stage kernel.  Algorithmic bytes per launch, FP32 (4 B) per cell:
+    # reads stage-start u, v, w (3) and theta (1), the step-start u, v, w (3) and theta (1)
+    # at stages 2 and 3, writes the stage value u, v, w (3) and theta (1): 8, 12, 12 words.
+    alg = 4 * cells * (8 + 12 + 12) / 3.0
+    achieved = alg / (phases["stage_kernel"] * 1e-3) / 1e9
+    ms_step = ms / K
+    value = world * cells * K / (ms * 1e-3) / 1e6
+    sample_steps = 2
+    secs = oracle_sample(nx, ny, nz, sample_steps) if not args.no_cpu else float("nan")
+    cpu = {"value": cells * sample_steps / secs / 1e6, "unit": UNIT, "cores": _threads(), "kind": "port",
+           "sample": f"{sample_steps} full {nx}x{ny}x{nz} steps of the numpy oracle after 1 untimed step"}
+    traffic = None
+    tp = ROOT / "profiles" / "stage_kernel_traffic.json"
+    if tp.exists():
+        try:
+            traffic = json.loads(tp.read_text()).get("bytes_per_launch_full_size")
+        except Exception:
+            traffic = None
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup,
+            "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": _config(nx, ny, nz, {"plain_variant": "plain drop-in (WALE)", "graph": f"{K} steps, 1 replay"}),
+            "roofline": {"bound": "hbm", "kernel": "stage_kernel", "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                         "alg_bytes_per_launch": alg},
+            "phases_ms": phases, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches_per_step(plan) * K,
+            "clocks": clk, "status": status}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--shape", type=int, nargs=3, default=list(SHAPE), help="nx ny nz (2:1:1)")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

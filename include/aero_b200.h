@@ -1,0 +1,173 @@
+/*
+ * aero_b200.h -- C ABI of the B200-native Navier-Stokes step (libaero_b200.so).
+ *
+ * Plain pointers, sizes and a cudaStream_t (passed as void*): no torch types.  Every
+ * device buffer is owned by the caller; the library never allocates or frees device
+ * memory and never synchronises the stream, so every call can be captured in a CUDA
+ * graph.  Functions return AERO_OK (0) or a negative AERO_E* code; aero_last_error()
+ * gives a thread-local message for the last failure on the calling thread.
+ *
+ * The entry points replace these parts of the reference (Aerolume, src/aerolume/solvers):
+ *
+ *   aero_ns3d_plan_create      ns3d/fused.py:226 load_kernels (builds the per-config constants)
+ *   aero_ns3d_step             ns3d/fused.py:378 fast_step_phys (+ core.py:765 step3d_phys),
+ *                              followed by the smoke update of ns3d/solver.py:646
+ *                              _advance_tracers (ns3d/fused.py:553 fast_dye and
+ *                              ns3d/dye.py:301 apply_solids_and_sources)
+ *   aero_ns3d_smoke            ns3d/fused.py:553 fast_dye + ns3d/dye.py:301 apply_solids_and_sources
+ *   aero_ns3d_project          ns3d/core.py:604 project3d
+ *   aero_ns3d_poisson_solve    ns3d/poisson.py:152 PoissonSolver3D.solve
+ *   aero_ns3d_workspace_bytes  (no counterpart: the reference allocates inside torch)
+ */
+#ifndef AERO_B200_H
+#define AERO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AERO_ABI_VERSION 1
+
+#define AERO_OK 0
+#define AERO_EINVAL -1        /* invalid argument or inconsistent configuration     */
+#define AERO_EUNSUPPORTED -2  /* a feature this build does not implement: no fallback */
+#define AERO_ECUDA -3         /* a CUDA launch or runtime call failed                */
+
+#define AERO_MAX_BODIES 8
+
+enum { AERO_F32 = 0, AERO_F64 = 1 };
+enum { AERO_ADV_UPWIND3 = 0, AERO_ADV_CENTRAL = 1 };
+enum { AERO_LES_NONE = 0, AERO_LES_SMAGORINSKY = 1, AERO_LES_WALE = 2, AERO_LES_VREMAN = 3 };
+/* velocity ghost-cell rules of ns3d/core.py:147-181 */
+enum {
+  AERO_GHOST_EDGE = 0, AERO_GHOST_EVEN = 1, AERO_GHOST_ODD = 2, AERO_GHOST_AFFINE = 3,
+  AERO_GHOST_FACE_ODD = 4, AERO_GHOST_PERIODIC_CELL = 5, AERO_GHOST_PERIODIC_FACE = 6
+};
+/* temperature side conditions of ns3d/physics.py:589-607 (left, right, front, back, bottom, top) */
+enum {
+  AERO_TH_PERIODIC = 0, AERO_TH_OUTFLOW = 1, AERO_TH_ADIABATIC = 2, AERO_TH_INFLOW = 3,
+  AERO_TH_TEMPERATURE = 4, AERO_TH_HEAT_FLUX = 5
+};
+
+/* Everything static about one 3D solve: grid, rules, constants (ns3d/core.py:61-108,
+ * ns3d/physics.py:494-560, ns3d/dye.py:140-151).  Scalars are doubles whatever the
+ * field dtype; the kernels round them to the field type as the reference does. */
+typedef struct AeroNs3dConfig {
+  int32_t abi_version;          /* AERO_ABI_VERSION                                        */
+  int32_t dtype;                /* AERO_F32 or AERO_F64                                    */
+  int32_t nx, ny, nz;           /* cells                                                   */
+  double h;
+  int32_t periodic[3];          /* x, y, z                                                 */
+  int32_t closed;               /* walls at x0 and x1 (domain = "closed")                  */
+  int32_t symmetry;             /* y = y0 symmetry plane (forces doubled)                  */
+  int32_t advection;            /* AERO_ADV_*                                              */
+  int32_t les;                  /* AERO_LES_*                                              */
+  double les_c;                 /* model constant                                          */
+  double nu;                    /* 1 / Re                                                  */
+  double eta;                   /* Brinkman permeability                                   */
+  double cfl;
+  int32_t has_dt_fixed;
+  double dt_fixed;
+  int32_t ghost_kind[3][3][2];  /* [u, v, w][x, y, z][lo, hi] : AERO_GHOST_*               */
+  double ghost_val[3][3][2];    /* value of AFFINE rules (moving road)                     */
+  double ref_area, length_ref, span_ref;
+  double moment_ref[3];
+  double y0;
+  int32_t window[6];            /* body cell window k0, k1, j0, j1, i0, i1 (empty: none)   */
+  int32_t nbody;
+  /* heat transfer (thermal = 0: off) */
+  int32_t thermal;
+  double kappa, pe, ri, prt, eta_t;
+  int32_t side_kind[6];         /* AERO_TH_*                                               */
+  double side_val[6];
+  int32_t has_heat_max;
+  double heat_max;
+  int32_t n_tbody;              /* "temperature" bodies                                    */
+  int32_t t_index[AERO_MAX_BODIES];
+  int32_t has_adia, has_skin;
+  double flux_rate[AERO_MAX_BODIES];
+  /* smoke (smoke = 0: off) */
+  int32_t smoke;
+  int32_t dye_window[6];        /* nozzle window (empty: no nozzles)                       */
+  double pulse_on, pulse_period;
+} AeroNs3dConfig;
+
+/* Window masks and constant inputs (device pointers of the plan's dtype; NULL when absent).
+ * Shapes are those of ns3d/geometry.py:275-303 and ns3d/physics.py:314-461. */
+typedef struct AeroNs3dGeom {
+  const void *chi_u, *chi_v, *chi_w, *chi_c;
+  const void *a_u, *a_v, *a_w;
+  const void *k_u, *k_v, *k_w;  /* (nbody, 3, ...) force / moment weights                */
+  const void *chi_t, *a_t, *w_t;
+  const void *adia_u, *adia_v, *adia_w;
+  const void *vol_w, *skin;
+  const void *dye_weight;
+  const void *u_inlet;          /* (nz, ny)                                                */
+} AeroNs3dGeom;
+
+/* State in and out (device pointers of the plan's dtype).  u may alias u0, v v0, w w0 and
+ * theta theta0; dye must not alias dye0.  t0, t, dt are 0-d scalars; coeffs is
+ * (nbody, 6), heat_rate (nbody).  theta/dye pointers are ignored when the plan has no
+ * heat transfer / smoke. */
+typedef struct AeroNs3dFields {
+  const void *u0, *v0, *w0, *theta0, *dye0, *t0;
+  void *u, *v, *w, *p, *theta, *dye, *t, *dt;
+  void *coeffs, *heat_rate;
+} AeroNs3dFields;
+
+typedef struct AeroNs3dPlan AeroNs3dPlan;
+
+int aero_abi_version(void);
+const char *aero_last_error(void);
+
+/* Validate a configuration and build its host-side constants. */
+int aero_ns3d_plan_create(const AeroNs3dConfig *cfg, AeroNs3dPlan **plan);
+void aero_ns3d_plan_destroy(AeroNs3dPlan *plan);
+
+/* Device workspace the plan needs (bytes, 256-byte aligned base required). */
+size_t aero_ns3d_workspace_bytes(const AeroNs3dPlan *plan);
+
+/* Fill the plan's tables (twiddles, eigenvalues) in a fresh workspace; once per workspace. */
+int aero_ns3d_workspace_init(const AeroNs3dPlan *plan, void *workspace, void *stream);
+
+/* One SSP-RK3 step with the configured physics, then the smoke update.
+ * dt_in: NULL for the CFL / heat-equation rule evaluated on the device, else a device
+ * 0-d scalar with the step to take. */
+int aero_ns3d_step(const AeroNs3dPlan *plan, const AeroNs3dFields *f, const AeroNs3dGeom *g,
+                   const void *dt_in, void *workspace, void *stream);
+
+/* aero_ns3d_step that also records CUDA events (cudaEvent_t handles, created with timing
+ * enabled) at the phase boundaries of the step, as external events so that they work inside a
+ * captured CUDA graph.  Event i is recorded after phase i (up to nevents):
+ *   0 start; 1 time step (maxima, eddy-viscosity pre-pass, dt);
+ *   2 + 5 s .. 6 + 5 s for stage s = 0, 1, 2: outlet correction, stage kernel, divergence,
+ *   Poisson solve (five transform passes and the psi accumulation), gradient correction;
+ *   17 smoke; 18 end of step.  (No counterpart in the reference: a measurement hook.) */
+#define AERO_NS3D_TRACE_EVENTS 19
+int aero_ns3d_step_traced(const AeroNs3dPlan *plan, const AeroNs3dFields *f, const AeroNs3dGeom *g,
+                          const void *dt_in, void *workspace, void *stream, void *const *events, int32_t nevents);
+
+/* Smoke alone (the step's tracer update): dye <- MUSCL step of dye0 with (u, v, w) and dt,
+ * then solids cleared and nozzles relaxed at time t.  Fields of f used: u, v, w, dye0, dye,
+ * and dt and t as inputs (the step just taken and the new time).  dye must not alias dye0. */
+int aero_ns3d_smoke(const AeroNs3dPlan *plan, const AeroNs3dFields *f, const AeroNs3dGeom *g, void *stream);
+
+/* psi with L psi = f, zero mean (f and psi: (nz, ny, nx) device arrays; may alias). */
+int aero_ns3d_poisson_solve(const AeroNs3dPlan *plan, const void *f, void *psi, void *workspace,
+                            void *stream);
+
+/* In place: (u, v, w) <- (u, v, w) - grad psi with lap psi = div(u, v, w); psi written. */
+int aero_ns3d_project(const AeroNs3dPlan *plan, void *u, void *v, void *w, void *psi, void *workspace,
+                      void *stream);
+
+/* Device-side status word of the last step on this workspace (0 = fine; bit 0: a
+ * non-finite value reached a reduction).  Reads through a host copy: synchronises. */
+int aero_ns3d_read_status(const AeroNs3dPlan *plan, const void *workspace, int32_t *status, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AERO_B200_H */

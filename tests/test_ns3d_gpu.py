@@ -1,0 +1,155 @@
+"""The CUDA 3D step through the C ABI against the reference's golden vectors and the oracle."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from _golden import CASES_3D, GOLDEN, load_case
+from oracle import ns3d as O
+
+pytestmark = pytest.mark.gpu
+
+# per-step tolerances, relative to the field's max norm: float64 agrees with the reference's
+# float64 step to round-off; float32 to the stated 1e-5 of the FP32 step
+TOL = {"float64": 1e-10, "float32": 1e-5}
+
+
+def _rel(a, b):
+    a = a.detach().double().cpu().numpy() if torch.is_tensor(a) else np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
+
+
+def _dev(x, dt):
+    return torch.as_tensor(np.ascontiguousarray(x)).to("cuda", dt).contiguous()
+
+
+def _plan_and_inputs(name):
+    from aerolume_b200.ns3d.plan import Ns3dPlan
+    meta, ops, geom, th, src, arr = load_case(name)
+    dt = torch.float64 if meta["dtype"] == "float64" else torch.float32
+    plan = Ns3dPlan(ops, geom, th, src, smoke=True)
+    ins = {"u0": _dev(arr["in_u"], dt), "v0": _dev(arr["in_v"], dt), "w0": _dev(arr["in_w"], dt),
+           "t0": _dev(arr["in_t"], dt), "dye0": _dev(arr["in_dye"], dt)}
+    if th is not None:
+        ins["theta0"] = _dev(arr["in_theta"], dt)
+    return meta, plan, ins, arr
+
+
+@pytest.mark.parametrize("name", CASES_3D)
+def test_one_step_matches_reference(name):
+    meta, plan, ins, arr = _plan_and_inputs(name)
+    out = plan.step(ins["u0"], ins["v0"], ins["w0"], ins["t0"], theta0=ins.get("theta0"), dye0=ins["dye0"])
+    torch.cuda.synchronize()
+    tol = TOL[meta["dtype"]]
+    for f in ("u", "v", "w", "p", "dye"):
+        assert _rel(out[f], arr["out1_" + f]) < tol, (f, _rel(out[f], arr["out1_" + f]))
+    assert _rel(out["dt"], arr["out1_dt"]) < tol
+    assert _rel(out["t"], arr["out1_t"]) < tol
+    if arr["out1_coeffs"].size:
+        cref = arr["out1_coeffs"]
+        err = np.abs(out["coeffs"].double().cpu().numpy() - cref).max() / max(1.0, np.abs(cref).max())
+        assert err < (1e-9 if meta["dtype"] == "float64" else 2e-4), err
+    if "out1_theta" in arr:
+        assert _rel(out["theta"], arr["out1_theta"]) < tol
+        if arr["out1_heat_rate"].size:
+            hr = arr["out1_heat_rate"]
+            err = np.abs(out["heat_rate"].double().cpu().numpy() - hr).max() / max(1.0, np.abs(hr).max())
+            assert err < (1e-9 if meta["dtype"] == "float64" else 2e-4), err
+    assert plan.status() == 0
+
+
+@pytest.mark.parametrize("name", [n for n in CASES_3D if "tunnel" in n])
+def test_three_steps_in_place_match_reference(name):
+    """Three steps updating the state in place (u, v, w, theta outputs alias the inputs)."""
+    meta, plan, ins, arr = _plan_and_inputs(name)
+    u, v, w, t = ins["u0"], ins["v0"], ins["w0"], ins["t0"]
+    theta, dye = ins.get("theta0"), ins["dye0"]
+    out = plan.empty_fields()
+    for _ in range(3):
+        out["u"], out["v"], out["w"] = u, v, w
+        if theta is not None:
+            out["theta"] = theta
+        plan.step(u, v, w, t, theta0=theta, dye0=dye, out=out)
+        t = out["t"].clone()
+        dye = out["dye"].clone()
+    torch.cuda.synchronize()
+    tol = 10 * TOL[meta["dtype"]]
+    for f, x in (("u", u), ("v", v), ("w", w), ("p", out["p"]), ("theta", theta), ("dye", dye)):
+        assert _rel(x, arr["outN_" + f]) < tol, (f, _rel(x, arr["outN_" + f]))
+
+
+def _poisson_ops(nx, ny, nz, h, per, dtype):
+    from aerolume_b200.ns3d.setup import make_ops
+    ops = make_ops(nx, ny, nz, h, re=100.0, periodic=all(per), bc_y="periodic" if per[1] and not all(per) else "slip",
+                   dtype=dtype)
+    ops.periodic_axes = tuple(per)
+    return ops
+
+
+@pytest.mark.parametrize("dtype", ["float64", "float32"])
+def test_poisson_matches_reference_for_odd_shapes_and_all_bc_mixes(dtype):
+    from aerolume_b200.ns3d.plan import Ns3dPlan
+    from aerolume_b200.ns3d.types import Geometry3D
+    z = np.load(GOLDEN / "poisson3d.npz")
+    h = float(z["h"])
+    tdt = torch.float64 if dtype == "float64" else torch.float32
+    for n in range(int(z["count"])):
+        nx, ny, nz, px, py, pz = (int(x) for x in z[f"meta{n}"])
+        ops = _poisson_ops(nx, ny, nz, h, (bool(px), bool(py), bool(pz)), dtype)
+        plan = Ns3dPlan(ops, Geometry3D((0, 0, 0, 0, 0, 0)))
+        psi = plan.poisson_solve(_dev(z[f"f{n}"], tdt))
+        err = _rel(psi, z[f"psi{n}"])
+        assert err < (1e-12 if dtype == "float64" else 2e-6), (n, err)
+
+
+@pytest.mark.parametrize("n", [(64, 32, 32), (96, 48, 24), (128, 64, 64), (48, 40, 36)])
+def test_poisson_fft_sizes_solve_exactly(n):
+    """L psi = f to round-off on the FFT sizes (2^a 3^b) and the dense fallback (5, 7)."""
+    from aerolume_b200.ns3d.plan import Ns3dPlan
+    from aerolume_b200.ns3d.types import Geometry3D
+    nx, ny, nz = n
+    for per in ((False, False, False), (True, True, True), (False, True, False)):
+        ops = _poisson_ops(nx, ny, nz, 0.05, per, "float64")
+        plan = Ns3dPlan(ops, Geometry3D((0, 0, 0, 0, 0, 0)))
+        f = torch.randn(nz, ny, nx, dtype=torch.float64, generator=torch.Generator().manual_seed(1))
+        f = (f - f.mean()).cuda()
+        psi = plan.poisson_solve(f)
+        ps = O.PoissonSolver3D(nx, ny, nz, 0.05, per, np.float64)
+        lap = ps.laplacian(psi.cpu().numpy(), 0.05, per)
+        assert np.abs(lap - f.cpu().numpy()).max() < 1e-9 * f.abs().max().item()
+
+
+def test_bench_case_matches_oracle_float64_and_float32():
+    """The bench workload's builders (box on a moving floor, WALE, heat, smoke) at 32 x 16 x 16:
+    CUDA vs the oracle from the same inputs, one step."""
+    from aerolume_b200.ns3d.plan import Ns3dPlan
+    from aerolume_b200.ns3d.workloads import box_on_moving_floor, initial_state
+    for dtype, tol in (("float64", 1e-10), ("float32", 1e-5)):
+        ops, geom, th, src, _ = box_on_moving_floor(32, 16, 16, dtype=dtype, seed=3)
+        plan = Ns3dPlan(ops, geom, th, src, smoke=True)
+        u, v, w = initial_state(ops, seed=3, noise=0.05)
+        plan.project(u, v, w)
+        tdt = u.dtype
+        g = torch.Generator().manual_seed(4)
+        theta = (0.2 * torch.randn(16, 16, 32, generator=g, dtype=torch.float64)).to("cuda", tdt)
+        dye = torch.rand(16, 16, 32, generator=g, dtype=torch.float64).to("cuda", tdt)
+        t0 = torch.zeros((), device="cuda", dtype=tdt)
+        out = plan.step(u, v, w, t0, theta0=theta, dye0=dye)
+        npd = np.float64 if dtype == "float64" else np.float32
+        ps = O.PoissonSolver3D(32, 16, 16, ops.h, ops.periodic_axes, npd)
+        c = lambda x: x.cpu().numpy()
+        r = O.step3d_phys(c(u), c(v), c(w), npd(0.0), geom_np(geom, npd), ops, ps, th=th, theta=c(theta))
+        cd = O.apply_solids_and_sources(O.advect_dye3d(c(dye), r.u, r.v, r.w, r.dt, ops), r.t, geom_np(geom, npd), src)
+        for f, ref in (("u", r.u), ("v", r.v), ("w", r.w), ("p", r.p), ("theta", r.theta), ("dye", cd)):
+            assert _rel(out[f], ref) < tol, (dtype, f, _rel(out[f], ref))
+        assert np.abs(out["coeffs"].double().cpu().numpy() - r.coeffs).max() < (1e-9 if dtype == "float64" else 1e-3)
+
+
+def geom_np(geom, npd):
+    from aerolume_b200.ns3d.types import Geometry3D
+    g = Geometry3D(geom.window, nbody=geom.nbody)
+    for n in ("chi_u", "chi_v", "chi_w", "chi_c", "a_u", "a_v", "a_w", "k_u", "k_v", "k_w"):
+        setattr(g, n, np.asarray(getattr(geom, n), npd))
+    return g
