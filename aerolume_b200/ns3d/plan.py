@@ -47,6 +47,8 @@ class Ns3dPlan:
             raise RuntimeError("the B200 step runs on a CUDA device only (no CPU fallback)")
         if not torch.cuda.is_available():
             raise RuntimeError("CUDA is not available: the B200 step has no CPU fallback")
+        if self.device.index is None:
+            self.device = torch.device("cuda", torch.cuda.current_device())
         L = _lib.lib()
         self.dtype = _torch_dtype(ops)
         self.ops, self.geom, self.thermal, self.dye_src = ops, geom, thermal, dye_src

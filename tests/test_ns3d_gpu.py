@@ -22,7 +22,8 @@ def _rel(a, b):
 
 
 def _dev(x, dt):
-    return torch.as_tensor(np.ascontiguousarray(x)).to("cuda", dt).contiguous()
+    x = np.asarray(x)
+    return torch.as_tensor(np.ascontiguousarray(x).reshape(x.shape)).to("cuda", dt).contiguous()
 
 
 def _plan_and_inputs(name):
