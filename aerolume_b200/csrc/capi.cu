@@ -4,6 +4,8 @@
 #include <cstring>
 #include <string>
 
+#include <cudaTypedefs.h>
+
 #include "ns3d.cuh"
 
 namespace {
@@ -33,6 +35,39 @@ int factor(int n, int *fac) {
   return n == 1 ? k : -1;
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link)
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+// 3D tiled view (x, y, z extents, row pitch in elements) with a (bx, by, 1) box; false when
+// the view cannot be described (alignment) -- the kernels then load synchronously.
+bool encode3d(CUtensorMap *m, bool f64, const void *base, size_t nx, size_t ny, size_t nz, size_t pitch, int bx,
+              int by) {
+  auto fn = encode_fn();
+  if (!fn || !base) return false;
+  const size_t e = f64 ? 8 : 4;
+  if (reinterpret_cast<uintptr_t>(base) % 16 || (pitch * e) % 16 || (bx * e) % 16) return false;
+  cuuint64_t dims[3] = {nx, ny, nz};
+  cuuint64_t strides[2] = {pitch * e, pitch * ny * e};
+  cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult r = fn(m, f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<void *>(base),
+                  dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
+}
+
 struct AxisInfo {
   int n, kind, method, nfac, L;
   int fac[16];
@@ -45,10 +80,11 @@ struct AeroNs3dPlan {
   AeroNs3dConfig cfg;
   size_t esz;                     // bytes per element
   size_t nu, nv, nw, nc;          // element counts of u, v, w and cell arrays
-  size_t off_uh, off_vh, off_wh, off_up, off_vp, off_wp, off_tha, off_thb, off_pa;
+  size_t off_uh, off_vh, off_wh, off_up, off_vp, off_wp, off_tha, off_thb, off_pa, off_nu;
   size_t off_small, off_scalars, off_status, off_partials, total;
   AxisInfo ax[3];
   int zc, nblocks, nq;
+  int pu, pn;                     // row pitches of the stage-start u copy and of nu
 };
 
 namespace {
@@ -98,11 +134,12 @@ int poisson_passes(const AeroNs3dPlan *p, const T *f, T *psi, unsigned char *ws,
 }
 
 template <typename T>
-aero::CompRules<T> comp_rules(const AeroNs3dConfig &c, int comp) {
+aero::CompRules<T> comp_rules(const AeroNs3dConfig &c, int comp, int pitch = 0) {
   aero::CompRules<T> r{};
   r.n0 = c.nx + (comp == 0);
   r.n1 = c.ny + (comp == 1);
   r.n2 = c.nz + (comp == 2);
+  r.p0 = pitch > 0 ? pitch : r.n0;
   for (int a = 0; a < 3; ++a)
     for (int s = 0; s < 2; ++s) {
       r.kind[a][s] = c.ghost_kind[comp][a][s];
@@ -211,8 +248,9 @@ int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom
 
   // ---- time step
   const bool need_max = dt_in == nullptr && !c.has_dt_fixed;
+  // the stage-start u copy with a 16-byte row pitch (TMA), and max |u0| on the way
+  CUDA_TRY(aero::launch_copy_u<T>(u0, upb, nx, ny, nz, p->pu, need_max ? bits + aero::SC_MAXU : nullptr, s));
   if (need_max) {
-    CUDA_TRY(aero::launch_absmax<T>(u0, p->nu, bits + aero::SC_MAXU, s));
     CUDA_TRY(aero::launch_absmax<T>(v0, p->nv, bits + aero::SC_MAXV, s));
     CUDA_TRY(aero::launch_absmax<T>(w0, p->nw, bits + aero::SC_MAXW, s));
     if (thermal) CUDA_TRY(aero::launch_absmax<T>(th0, p->nc, bits + aero::SC_MAXT, s));
@@ -225,9 +263,11 @@ int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom
   S.zc = p->zc;
   S.h = T(c.h);
   S.inv_h = T(1.0 / c.h);
-  S.ru = comp_rules<T>(c, 0);
+  S.ru = comp_rules<T>(c, 0, p->pu);
   S.rv = comp_rules<T>(c, 1);
   S.rw = comp_rules<T>(c, 2);
+  S.status = status;
+  S.nu_pitch = p->pn;
   S.px = c.periodic[0];
   S.py = c.periodic[1];
   S.pz = c.periodic[2];
@@ -236,7 +276,45 @@ int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom
   S.les = c.les;
   S.kadv = T((c.advection == AERO_ADV_UPWIND3 ? 7.0 / 24.0 : 0.25) / c.h);
   S.nu_h2 = T(T(c.nu) * T(1.0 / (c.h * c.h)));
-  S.les_cd2 = T(c.les == AERO_LES_VREMAN ? c.les_c * c.h * c.h : c.les_c * c.les_c * c.h * c.h);
+  T *nu_buf = reinterpret_cast<T *>(ws + p->off_nu);
+  S.nu = nu_buf;
+  aero::NuParams<T> NP{};
+  NP.nx = nx;
+  NP.ny = ny;
+  NP.nz = nz;
+  NP.zc = p->zc;
+  NP.les = c.les;
+  NP.inv_h = T(1.0 / c.h);
+  NP.cd2 = T(c.les == AERO_LES_VREMAN ? c.les_c * c.h * c.h : c.les_c * c.les_c * c.h * c.h);
+  NP.ru = comp_rules<T>(c, 0, p->pu);
+  NP.rv = comp_rules<T>(c, 1);
+  NP.rw = comp_rules<T>(c, 2);
+  NP.status = status;
+  NP.nu_pitch = p->pn;
+  const bool f64 = sizeof(T) == 8;
+  // TMA views: stage-start u copy and nu are fixed workspace buffers; v, w, theta change by stage
+  CUtensorMap map_u_stage, map_u_nu, map_nu;
+  bool tma_ok = encode3d(&map_u_stage, f64, upb, nx + 1, ny, nz, p->pu, 40, 12) &&
+                encode3d(&map_u_nu, f64, upb, nx + 1, ny, nz, p->pu, 36, 10);
+  if (les) tma_ok = tma_ok && encode3d(&map_nu, f64, nu_buf, nx + 2, ny + 2, nz + 2, p->pn, 36, 10);
+  auto stage_views = [&](const T *vp, const T *wp, const T *thp, aero::StageParams<T> &P) {
+    P.use_tma = tma_ok && encode3d(&P.map_v, f64, vp, nx, ny + 1, nz, nx, 40, 12) &&
+                encode3d(&P.map_w, f64, wp, nx, ny, nz + 1, nx, 40, 12) &&
+                (!thermal || encode3d(&P.map_th, f64, thp, nx, ny, nz, nx, 40, 12));
+    P.map_u = map_u_stage;
+    if (les) P.map_nu = map_nu;
+  };
+  auto nu_views = [&](const T *vp, const T *wp, aero::NuParams<T> &N) {
+    N.use_tma = tma_ok && encode3d(&N.map_v, f64, vp, nx, ny + 1, nz, nx, 36, 10) &&
+                encode3d(&N.map_w, f64, wp, nx, ny, nz + 1, nx, 36, 10);
+    N.map_u = map_u_nu;
+  };
+  NP.has_win = has_win;
+  for (int q = 0; q < 6; ++q) NP.win[q] = has_win ? c.window[q] : 0;
+  NP.wnx = c.window[5] - c.window[4];
+  NP.wny = c.window[3] - c.window[2];
+  NP.chi_c = static_cast<const T *>(g->chi_c);
+  NP.nu = nu_buf;
   S.dt = small;
   S.u0 = u0;
   S.v0 = v0;
@@ -291,15 +369,14 @@ int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom
     }
   }
 
-  if (need_max && les) {
-    aero::StageParams<T> N = S;
-    N.mode = aero::MODE_NUT_ONLY;
-    N.up = u0;
+  if (les) {  // eddy viscosity of u0: the first stage's, and its maximum for the time step
+    aero::NuParams<T> N = NP;
+    N.up = upb;
     N.vp = v0;
     N.wp = w0;
-    N.thermal = 0;
-    N.nut_max = bits + aero::SC_NUTMAX;
-    CUDA_TRY(aero::launch_stage<T>(N, s));
+    nu_views(v0, w0, N);
+    N.nut_max = need_max ? bits + aero::SC_NUTMAX : nullptr;
+    CUDA_TRY(aero::launch_nu<T>(N, s));
   }
 
   aero::DtParams D{};
@@ -324,7 +401,7 @@ int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom
 
   const int rows = nz * ny;
   if (tunnel) {
-    plane_sum_kernel<T><<<1, 1024, 0, s>>>(u0, nx + 1, nx, sc + aero::SC_SUM_U0, S.u_inlet, 1, 0,
+    plane_sum_kernel<T><<<1, 1024, 0, s>>>(upb, p->pu, nx, sc + aero::SC_SUM_U0, S.u_inlet, 1, 0,
                                           sc + aero::SC_SUM_INLET, rows);
     CUDA_TRY(cudaGetLastError());
   }
@@ -333,17 +410,25 @@ int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom
   static const double RK[3][3] = {{0.0, 1.0, 1.0 / 6.0}, {0.75, 0.25, 2.0 / 3.0}, {1.0 / 3.0, 2.0 / 3.0, 1.0}};
   T *p_out = static_cast<T *>(f->p);
   for (int st = 0; st < 3; ++st) {
-    const T *up = st == 0 ? u0 : upb, *vp = st == 0 ? v0 : vpb, *wp = st == 0 ? w0 : wpb;
+    const T *up = upb, *vp = st == 0 ? v0 : vpb, *wp = st == 0 ? w0 : wpb;
     if (tunnel) {
       double *sums = sc + aero::SC_SUMS + 3 * st;
-      plane_sum_kernel<T><<<1, 1024, 0, s>>>(up, nx + 1, nx, sums, up, nx + 1, nx - 1, sums + 1, rows);
+      plane_sum_kernel<T><<<1, 1024, 0, s>>>(up, p->pu, nx, sums, up, p->pu, nx - 1, sums + 1, rows);
       CUDA_TRY(cudaGetLastError());
       CUDA_TRY(aero::launch_outlet_corr<T>(sums, sc + aero::SC_SUM_U0, sc + aero::SC_SUM_INLET, small, RK[st][0],
                                            RK[st][1], 1.0 / c.h, 1.0 / rows, small + 1, s));
     }
+    if (les && st > 0) {
+      aero::NuParams<T> N = NP;
+      N.up = up;
+      N.vp = vp;
+      N.wp = wp;
+      nu_views(vp, wp, N);
+      N.nut_max = nullptr;
+      CUDA_TRY(aero::launch_nu<T>(N, s));
+    }
     CUDA_TRY(mark(2 + 5 * st));
     aero::StageParams<T> P = S;
-    P.mode = aero::MODE_STAGE;
     P.a = T(RK[st][0]);
     P.bdt_scale = T(RK[st][1]);
     P.wgt = T(RK[st][2]);
@@ -351,11 +436,11 @@ int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom
     P.vp = vp;
     P.wp = wp;
     P.partials = has_win ? partials + (size_t)st * p->nblocks * p->nq : nullptr;
-    P.nut_max = nullptr;
     if (thermal) {
       P.thp = st == 0 ? th0 : (st == 1 ? tha : thb);
       P.thh = st == 0 ? tha : (st == 1 ? thb : static_cast<T *>(f->theta));
     }
+    stage_views(vp, wp, thermal ? P.thp : nullptr, P);
     CUDA_TRY(aero::launch_stage<T>(P, s));
     CUDA_TRY(mark(3 + 5 * st));
     CUDA_TRY(aero::launch_divergence<T>(uh, vh, wh, nx, ny, nz, c.periodic[0], c.periodic[1], c.periodic[2],
@@ -363,7 +448,7 @@ int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom
     CUDA_TRY(mark(4 + 5 * st));
     const int rc = poisson_passes<T>(p, pa, pa, ws, s);
     if (rc) return rc;
-    CUDA_TRY(aero::launch_psi_accumulate<T>(pa, p_out, p->nc, T(RK[st][2]), st == 0, s));
+    CUDA_TRY(aero::launch_psi_accumulate<T>(pa, p_out, p->nc, T(RK[st][2]), st == 0 ? 0 : (st == 1 ? 1 : 2), small, s));
     CUDA_TRY(mark(5 + 5 * st));
     aero::CorrectParams<T> C{};
     C.nx = nx;
@@ -378,6 +463,7 @@ int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom
     C.wh = wh;
     C.psi = pa;
     C.u = st == 2 ? static_cast<T *>(f->u) : upb;
+    C.pu_out = st == 2 ? nx + 1 : p->pu;
     C.v = st == 2 ? static_cast<T *>(f->v) : vpb;
     C.w = st == 2 ? static_cast<T *>(f->w) : wpb;
     CUDA_TRY(aero::launch_correct<T>(C, s));
@@ -399,6 +485,7 @@ int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom
   F.n_tbody = thermal && has_win ? c.n_tbody : 0;
   F.symmetry = c.symmetry;
   F.partials = partials;
+  F.tot = sc + aero::SC_TOT;
   F.h = c.h;
   F.pe = c.pe;
   F.y0 = c.y0;
@@ -445,8 +532,8 @@ template <typename T>
 int project_impl(const AeroNs3dPlan *p, void *u, void *v, void *w, void *psi, unsigned char *ws, cudaStream_t s) {
   const AeroNs3dConfig &c = p->cfg;
   T *pa = reinterpret_cast<T *>(ws + p->off_pa);
-  T *upb = reinterpret_cast<T *>(ws + p->off_up), *vpb = reinterpret_cast<T *>(ws + p->off_vp),
-    *wpb = reinterpret_cast<T *>(ws + p->off_wp);
+  T *upb = reinterpret_cast<T *>(ws + p->off_uh), *vpb = reinterpret_cast<T *>(ws + p->off_vh),
+    *wpb = reinterpret_cast<T *>(ws + p->off_wh);
   CUDA_TRY(aero::launch_divergence<T>(static_cast<T *>(u), static_cast<T *>(v), static_cast<T *>(w), c.nx, c.ny, c.nz,
                                       c.periodic[0], c.periodic[1], c.periodic[2], T(1.0 / c.h), pa, s));
   const int rc = poisson_passes<T>(p, pa, static_cast<T *>(psi), ws, s);
@@ -466,6 +553,7 @@ int project_impl(const AeroNs3dPlan *p, void *u, void *v, void *w, void *psi, un
   C.u = upb;
   C.v = vpb;
   C.w = wpb;
+  C.pu_out = c.nx + 1;
   CUDA_TRY(aero::launch_correct<T>(C, s));
   CUDA_TRY(cudaMemcpyAsync(u, upb, p->nu * sizeof(T), cudaMemcpyDeviceToDevice, s));
   CUDA_TRY(cudaMemcpyAsync(v, vpb, p->nv * sizeof(T), cudaMemcpyDeviceToDevice, s));
@@ -536,12 +624,15 @@ int aero_ns3d_plan_create(const AeroNs3dConfig *cfg, AeroNs3dPlan **plan) {
   p->off_uh = take(p->nu * e);
   p->off_vh = take(p->nv * e);
   p->off_wh = take(p->nw * e);
-  p->off_up = take(p->nu * e);
+  p->pu = (int)((nx + 1 + 3) / 4 * 4);
+  p->pn = (int)((nx + 2 + 3) / 4 * 4);
+  p->off_up = take(nz * ny * (size_t)p->pu * e);
   p->off_vp = take(p->nv * e);
   p->off_wp = take(p->nw * e);
   p->off_tha = take(c.thermal ? p->nc * e : 0);
   p->off_thb = take(c.thermal ? p->nc * e : 0);
   p->off_pa = take(p->nc * e);
+  p->off_nu = take(c.les != AERO_LES_NONE ? (nz + 2) * (ny + 2) * (size_t)p->pn * e : 0);
   p->off_small = take(8 * e);
   p->off_scalars = take(sizeof(double) * aero::SC_COUNT);
   p->off_status = take(sizeof(int) * 4);

@@ -46,7 +46,8 @@ __device__ __forceinline__ int ghost_map(int g, int n, int kind_lo, int kind_hi,
 // The rules of one staggered component on its (n2, n1, n0) = (z, y, x) array.
 template <typename T>
 struct CompRules {
-  int n0, n1, n2;
+  int n0, n1, n2;  // entries along x, y, z
+  int p0;          // row pitch (elements) of the array, >= n0
   int kind[3][2];
   T val[3][2];
 };
@@ -59,7 +60,7 @@ __device__ __forceinline__ T padded(const T *__restrict__ f, const CompRules<T> 
   const int mi = ghost_map<T>(i, r.n0, r.kind[0][0], r.kind[0][1], r.val[0][0], r.val[0][1], sx, cx);
   const int mj = ghost_map<T>(j, r.n1, r.kind[1][0], r.kind[1][1], r.val[1][0], r.val[1][1], sy, cy);
   const int mk = ghost_map<T>(k, r.n2, r.kind[2][0], r.kind[2][1], r.val[2][0], r.val[2][1], sz, cz);
-  const T x = __ldg(f + ((size_t)mk * r.n1 + mj) * r.n0 + mi);
+  const T x = __ldg(f + ((size_t)mk * r.n1 + mj) * r.p0 + mi);
   return sz * (sy * (sx * x + cx) + cy) + cz;
 }
 

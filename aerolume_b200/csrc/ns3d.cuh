@@ -4,6 +4,8 @@
 #include <algorithm>
 #include <cstddef>
 
+#include <cuda.h>
+
 #include "common.cuh"
 
 namespace aero {
@@ -19,19 +21,39 @@ enum : int {
   SC_SUM_INLET = 6,
   SC_SUM_U0 = 7,       // sum u0[..., nx]
   SC_SUMS = 8,         // 3 stages x (sum up[nx], sum up[nx-1], spare)
-  SC_COUNT = 20
+  SC_TOT = 20,         // reduced force / heat sums (AERO_MAX_BODIES * 10)
+  SC_COUNT = 20 + AERO_MAX_BODIES * 10
 };
 
-enum : int { MODE_STAGE = 0, MODE_NUT_ONLY = 1 };
+template <typename T>
+struct NuParams {
+  CUtensorMap map_u, map_v, map_w;  // TMA views of the stage-start velocity (use_tma)
+  int use_tma;
+  int *status;
+  int nu_pitch;
+  int nx, ny, nz, zc, les;
+  T inv_h, cd2;
+  CompRules<T> ru, rv, rw;
+  const T *up, *vp, *wp;
+  int has_win, win[6], wnx, wny;
+  const T *chi_c;
+  T *nu;                      // (nz+2, ny+2, nx+2): cells -1..n of every axis
+  unsigned long long *nut_max;  // or NULL
+};
 
 template <typename T>
 struct StageParams {
-  int nx, ny, nz, zc, mode;
+  CUtensorMap map_u, map_v, map_w, map_th, map_nu;  // TMA views (use_tma)
+  int use_tma;
+  int *status;
+  int nu_pitch;
+  int nx, ny, nz, zc;
   T h, inv_h;
   CompRules<T> ru, rv, rw;
   int px, py, pz, closed;
   int upwind, les;
-  T kadv, nu_h2, les_cd2;
+  T kadv, nu_h2;
+  const T *nu;                // eddy viscosity of the stage-start velocity (nu_kernel)
   // stage
   T a, bdt_scale, wgt;
   const T *dt;
@@ -45,7 +67,6 @@ struct StageParams {
   T eta;
   const T *chi_u, *chi_v, *chi_w, *chi_c, *a_u, *a_v, *a_w, *k_u, *k_v, *k_w;
   double *partials;           // [block][nq] (this stage's slice)
-  unsigned long long *nut_max;
   // heat
   int thermal, has_adia, n_tbody;
   ThetaSides sides;
@@ -67,6 +88,7 @@ struct DtParams {
 template <typename T>
 struct CorrectParams {
   int nx, ny, nz, px, py, pz;
+  int pu_out;                 // row pitch of the u output
   T inv_h;
   const T *uh, *vh, *wh, *psi;
   T *u, *v, *w;
@@ -90,6 +112,7 @@ struct FinalizeParams {
   size_t ncell;
   int nbody, nq, nblocks, n_tbody, symmetry;
   const double *partials;
+  double *tot;                // nq reduced sums (workspace)
   double h, pe, y0, moment_ref_y, ref_area, span_ref, length_ref;
   int t_index[AERO_MAX_BODIES];
   double flux_rate[AERO_MAX_BODIES];
@@ -118,7 +141,10 @@ struct TransformParams {
 
 template <typename T> size_t stage_smem_bytes();
 template <typename T> cudaError_t launch_stage(const StageParams<T> &, cudaStream_t);
+template <typename T> cudaError_t launch_nu(const NuParams<T> &, cudaStream_t);
 template <typename T> cudaError_t launch_absmax(const T *, size_t, unsigned long long *, cudaStream_t);
+template <typename T>
+cudaError_t launch_copy_u(const T *, T *, int, int, int, int, unsigned long long *, cudaStream_t);
 template <typename T> cudaError_t launch_dt(const DtParams &, cudaStream_t);
 template <typename T> cudaError_t launch_outlet_sum(const T *, const T *, int, int, double *, cudaStream_t);
 template <typename T>
@@ -129,7 +155,7 @@ cudaError_t launch_divergence(const T *, const T *, const T *, int, int, int, in
 template <typename T> cudaError_t launch_correct(const CorrectParams<T> &, cudaStream_t);
 template <typename T> cudaError_t launch_smoke(const SmokeParams<T> &, cudaStream_t);
 template <typename T> cudaError_t launch_finalize(const FinalizeParams<T> &, cudaStream_t);
-template <typename T> cudaError_t launch_psi_accumulate(const T *, T *, size_t, T, int, cudaStream_t);
+template <typename T> cudaError_t launch_psi_accumulate(const T *, T *, size_t, T, int, const T *, cudaStream_t);
 template <typename T> size_t transform_smem_bytes(int, int);
 template <typename T> cudaError_t launch_transform(const TransformParams<T> &, cudaStream_t);
 template <typename T>

@@ -1,0 +1,456 @@
+// Small kernels of the 3D step: maxima, time step, outlet sums, divergence, gradient
+// correction, smoke, partial-sum reduction and the end of the step.
+//
+// Arithmetic follows Aerolume ns3d/core.py:577-678, 875-883, physics.py:713-742, 1230-1262
+// and dye.py:232-312 operation by operation.
+#include "ns3d.cuh"
+#include "stencil.cuh"
+
+namespace aero {
+
+// --------------------------------------------------------------------------------------
+// pre-pass maxima, time step, outlet sums
+// --------------------------------------------------------------------------------------
+
+template <typename T>
+__global__ void absmax_kernel(const T *__restrict__ a, size_t n, unsigned long long *out) {
+  T m = T(0);
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    const T v = fabs(a[e]);
+    m = (v > m || v != v) ? v : m;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const T other = __shfl_xor_sync(0xffffffffu, m, o);
+    m = (other > m || other != other) ? other : m;
+  }
+  if ((threadIdx.x & 31) == 0) atomic_max_nonneg(out, (double)m);
+}
+
+// u0 (rows of nx + 1) into the stage-start buffer with a 16-byte row pitch, with max |u0|
+template <typename T>
+__global__ void copy_u_kernel(const T *__restrict__ u, T *__restrict__ out, int nx, int ny, int pitch,
+                              unsigned long long *mx) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+  T m = T(0);
+  if (i <= nx) {
+    const T v = u[((size_t)k * ny + j) * (nx + 1) + i];
+    out[((size_t)k * ny + j) * pitch + i] = v;
+    m = fabs(v);
+  }
+  if (mx) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const T other = __shfl_xor_sync(0xffffffffu, m, o);
+      m = (other > m || other != other) ? other : m;
+    }
+    if ((threadIdx.x & 31) == 0) atomic_max_nonneg(mx, (double)m);
+  }
+}
+
+// One thread: the step's dt from the maxima (core.py:637-646, physics.py:723-742, 1230-1262),
+// rounded through the field type as the reference computes it.
+template <typename T>
+__global__ void dt_kernel(const DtParams P) {
+  const double *sc = P.scalars;
+  const unsigned long long *bits = reinterpret_cast<const unsigned long long *>(sc);
+  T dt;
+  if (P.dt_in) {
+    dt = *reinterpret_cast<const T *>(P.dt_in);
+  } else if (P.has_dt_fixed) {
+    dt = T(P.dt_fixed);
+  } else {
+    const T mu = T(as_double(bits[SC_MAXU])), mv = T(as_double(bits[SC_MAXV])), mw = T(as_double(bits[SC_MAXW]));
+    T umax = (mu + mv) + mw;
+    umax = umax > T(1e-6) ? umax : T(1e-6);
+    if (umax != umax) umax = mu + mv + mw;  // keep NaN
+    dt = T(P.cfl * P.h) / umax;
+    const bool les = P.les != 0;
+    const T nut_max = T(as_double(bits[SC_NUTMAX]));
+    const T nu = les ? T(P.nu) + nut_max : T(P.nu);
+    const T dv = T(P.viscous_dt * P.h * P.h) / nu;
+    dt = dv < dt ? dv : dt;
+    if (P.thermal) {
+      const T kap = les ? T(P.kappa) + nut_max / T(P.prt) : T(P.kappa);
+      const T diff_rate = kap / T(P.viscous_dt * P.h * P.h);
+      const T lim = T(1) / (umax * T(1.0 / (0.5 * P.h)) + diff_rate);
+      dt = lim < dt ? lim : dt;
+      if (P.ri != 0.0) {
+        T acc = T(fabs(P.ri)) * T(as_double(bits[SC_MAXT]));
+        acc = acc > T(1e-12) ? acc : T(1e-12);
+        const T f = T(P.cfl) * sqrt(T(P.h) / acc);
+        dt = f < dt ? f : dt;
+      }
+      if (P.has_heat_max) {
+        T s = T(P.heat_max);
+        s = s > T(1e-12) ? s : T(1e-12);
+        const T l1 = T(1) / s;
+        dt = l1 < dt ? l1 : dt;
+        if (P.ri != 0.0) {
+          const T l2 = pow(T(6.0 * P.cfl * P.h) / (T(fabs(P.ri)) * s), T(1.0 / 3.0));
+          dt = l2 < dt ? l2 : dt;
+        }
+      }
+    }
+  }
+  *reinterpret_cast<T *>(P.dt_out) = dt;
+  P.scalars[SC_DT] = (double)dt;
+  if (!(dt == dt) || !(dt > T(0)) || isinf((double)dt)) atomicOr(P.status, 1);
+}
+
+// Outlet-plane sums in a fixed order (deterministic): one block of 1024 threads.
+// sums[0] = sum u[..., nx], sums[1] = sum u[..., nx-1] (and sums[2] = sum u0[..., nx] when
+// u0 is given).  The stage blends them into the outlet correction by linearity.
+template <typename T>
+__global__ void outlet_sum_kernel(const T *__restrict__ u, const T *__restrict__ u0, int nx, int rows,
+                                  double *sums) {
+  __shared__ double red[3][32];
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+  for (int r = threadIdx.x; r < rows; r += blockDim.x) {
+    const size_t base = (size_t)r * (nx + 1);
+    s0 += (double)u[base + nx];
+    s1 += (double)u[base + nx - 1];
+    if (u0) s2 += (double)u0[base + nx];
+  }
+  s0 = warp_sum(s0);
+  s1 = warp_sum(s1);
+  s2 = warp_sum(s2);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) {
+    red[0][w] = s0;
+    red[1][w] = s1;
+    red[2][w] = s2;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, b = 0.0, c = 0.0;
+    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) {
+      a += red[0][q];
+      b += red[1][q];
+      c += red[2][q];
+    }
+    sums[0] = a;
+    sums[1] = b;
+    if (u0) sums[2] = c;
+  }
+}
+
+// corr = (sum u_inlet - sum uh[..., nx]) / (ny nz) with sum uh[..., nx] blended from the
+// stage-start sums: sum lerp(up, u0, a) + b dt / h (sum up[nx-1] - sum up[nx]).
+template <typename T>
+__global__ void outlet_corr_kernel(const double *sums_p, const double *sum_u0, const double *sum_inlet, const T *dt,
+                                   double a, double bscale, double inv_h, double inv_rows, T *corr) {
+  const double bdt = (double)(T(bscale) * *dt);
+  const double so = sums_p[0], si = sums_p[1], s0 = *sum_u0;
+  const double out = (1.0 - a) * so + a * s0 + bdt * inv_h * (si - so);
+  *corr = T((*sum_inlet - out) * inv_rows);
+}
+
+// --------------------------------------------------------------------------------------
+// projection: divergence and gradient correction (core.py:577-601)
+// --------------------------------------------------------------------------------------
+
+template <typename T>
+__global__ void divergence_kernel(const T *__restrict__ u, const T *__restrict__ v, const T *__restrict__ w, int nx,
+                                  int ny, int nz, int px, int py, int pz, T inv_h, T *__restrict__ div) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+  if (i >= nx) return;
+  const size_t ru = ((size_t)k * ny + j) * (nx + 1);
+  const T ur = (px && i == nx - 1) ? u[ru] : u[ru + i + 1];
+  const T ul = u[ru + i];
+  const size_t rv = (size_t)k * (ny + 1) * nx;
+  const T vr = (py && j == ny - 1) ? v[rv + i] : v[rv + (size_t)(j + 1) * nx + i];
+  const T vl = v[rv + (size_t)j * nx + i];
+  const T wr = (pz && k == nz - 1) ? w[(size_t)j * nx + i] : w[((size_t)(k + 1) * ny + j) * nx + i];
+  const T wl = w[((size_t)k * ny + j) * nx + i];
+  div[((size_t)k * ny + j) * nx + i] = ((ur - ul) + (vr - vl) + (wr - wl)) * inv_h;
+}
+
+// u <- uh - grad psi on every face; boundary-normal faces keep uh (non-periodic), periodic
+// duplicate faces equal face 0.
+template <typename T>
+__global__ void correct_kernel(const CorrectParams<T> P) {
+  const int nx = P.nx, ny = P.ny, nz = P.nz;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+  const T inv = P.inv_h;
+  if (i <= nx && j < ny && k < nz) {  // u face (k, j, i)
+    const size_t e = ((size_t)k * ny + j) * (nx + 1) + i;
+    const size_t c = ((size_t)k * ny + j) * nx;
+    T val;
+    if (P.px) {
+      const int ii = (i == nx) ? 0 : i;
+      const int il = (ii == 0) ? nx - 1 : ii - 1;
+      val = P.uh[e - i + ii] - (P.psi[c + ii] - P.psi[c + il]) * inv;
+    } else if (i == 0 || i == nx) {
+      val = P.uh[e];
+    } else {
+      val = P.uh[e] - (P.psi[c + i] - P.psi[c + i - 1]) * inv;
+    }
+    P.u[((size_t)k * ny + j) * P.pu_out + i] = val;
+  }
+  if (i < nx && j <= ny && k < nz) {  // v face (k, j, i)
+    const size_t e = ((size_t)k * (ny + 1) + j) * nx + i;
+    T val;
+    if (P.py) {
+      const int jj = (j == ny) ? 0 : j;
+      const int jl = (jj == 0) ? ny - 1 : jj - 1;
+      val = P.vh[((size_t)k * (ny + 1) + jj) * nx + i] -
+            (P.psi[((size_t)k * ny + jj) * nx + i] - P.psi[((size_t)k * ny + jl) * nx + i]) * inv;
+    } else if (j == 0 || j == ny) {
+      val = P.vh[e];
+    } else {
+      val = P.vh[e] - (P.psi[((size_t)k * ny + j) * nx + i] - P.psi[((size_t)k * ny + j - 1) * nx + i]) * inv;
+    }
+    P.v[e] = val;
+  }
+  if (i < nx && j < ny && k <= nz) {  // w face (k, j, i)
+    const size_t e = ((size_t)k * ny + j) * nx + i;
+    T val;
+    if (P.pz) {
+      const int kk = (k == nz) ? 0 : k;
+      const int kl = (kk == 0) ? nz - 1 : kk - 1;
+      val = P.wh[((size_t)kk * ny + j) * nx + i] -
+            (P.psi[((size_t)kk * ny + j) * nx + i] - P.psi[((size_t)kl * ny + j) * nx + i]) * inv;
+    } else if (k == 0 || k == nz) {
+      val = P.wh[e];
+    } else {
+      val = P.wh[e] - (P.psi[e] - P.psi[e - (size_t)ny * nx]) * inv;
+    }
+    P.w[e] = val;
+  }
+}
+
+// --------------------------------------------------------------------------------------
+// smoke: MUSCL forward Euler, clip and floor, solids and nozzles (dye.py:232-312)
+// --------------------------------------------------------------------------------------
+
+template <typename T>
+__device__ __forceinline__ T dye_at(const T *__restrict__ c, int nz, int ny, int nx, int px, int py, int pz, int k,
+                                    int j, int i) {
+  // pad_dye ghosts (dye.py:232-263): inlet zeros, outlet zero-gradient, mirrored y / z
+  if (i < 0) {
+    if (!px) return T(0);
+    i += nx;
+  } else if (i >= nx) {
+    i = px ? i - nx : nx - 1;
+  }
+  if (j < 0) j = py ? j + ny : -1 - j;
+  else if (j >= ny) j = py ? j - ny : 2 * ny - 1 - j;
+  if (k < 0) k = pz ? k + nz : -1 - k;
+  else if (k >= nz) k = pz ? k - nz : 2 * nz - 1 - k;
+  return __ldg(c + ((size_t)k * ny + j) * nx + i);
+}
+
+template <typename T>
+__global__ void smoke_kernel(const SmokeParams<T> P) {
+  const int nx = P.nx, ny = P.ny, nz = P.nz;
+  const T dt = *P.dt;
+  const T kk = dt * P.inv_h;
+  const T t = P.t_new ? *P.t_new : *P.t0 + dt;
+  const T on = (fmod(t, T(P.pulse_period)) < T(P.pulse_on)) ? T(1) : T(0);
+  {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+    if (i >= nx) return;
+    const size_t e = ((size_t)k * ny + j) * nx + i;
+    auto C = [&](int dk, int dj, int di) { return dye_at<T>(P.c0, nz, ny, nx, P.px, P.py, P.pz, k + dk, j + dj, i + di); };
+    const T c = C(0, 0, 0);
+    const T fx0 = muscl_flux<T>(C(0, 0, -2), C(0, 0, -1), c, C(0, 0, 1), P.u[((size_t)k * ny + j) * (nx + 1) + i]);
+    const T fx1 = muscl_flux<T>(C(0, 0, -1), c, C(0, 0, 1), C(0, 0, 2), P.u[((size_t)k * ny + j) * (nx + 1) + i + 1]);
+    const T fy0 = muscl_flux<T>(C(0, -2, 0), C(0, -1, 0), c, C(0, 1, 0), P.v[((size_t)k * (ny + 1) + j) * nx + i]);
+    const T fy1 = muscl_flux<T>(C(0, -1, 0), c, C(0, 1, 0), C(0, 2, 0), P.v[((size_t)k * (ny + 1) + j + 1) * nx + i]);
+    const T fz0 = muscl_flux<T>(C(-2, 0, 0), C(-1, 0, 0), c, C(1, 0, 0), P.w[((size_t)k * ny + j) * nx + i]);
+    const T fz1 = muscl_flux<T>(C(-1, 0, 0), c, C(1, 0, 0), C(2, 0, 0), P.w[((size_t)(k + 1) * ny + j) * nx + i]);
+    T v = c - kk * (((fx1 - fx0) + (fy1 - fy0)) + (fz1 - fz0));
+    v = v > T(1) ? T(1) : v;
+    v = v < T(1e-8) ? T(0) : v;
+    if (P.chi_c && k >= P.win[0] && k < P.win[1] && j >= P.win[2] && j < P.win[3] && i >= P.win[4] && i < P.win[5]) {
+      const T chi = P.chi_c[((size_t)(k - P.win[0]) * (P.win[3] - P.win[2]) + (j - P.win[2])) * (P.win[5] - P.win[4]) +
+                            (i - P.win[4])];
+      if (chi > T(0.5)) v = T(0);
+    }
+    if (P.weight && k >= P.dwin[0] && k < P.dwin[1] && j >= P.dwin[2] && j < P.dwin[3] && i >= P.dwin[4] &&
+        i < P.dwin[5]) {
+      const T wgt = P.weight[((size_t)(k - P.dwin[0]) * (P.dwin[3] - P.dwin[2]) + (j - P.dwin[2])) * (P.dwin[5] - P.dwin[4]) +
+                             (i - P.dwin[4])];
+      v = v + wgt * on * (T(1) - v);
+    }
+    P.c[e] = v;
+  }
+}
+
+// --------------------------------------------------------------------------------------
+// end of step: p, coefficients, heat rates, t and dt (core.py:653-678, 875-883,
+// physics.py:713-721)
+// --------------------------------------------------------------------------------------
+
+// tot[q] = sum over stages and blocks of partials[stage][block][q]: one block per q, a
+// fixed thread-to-term mapping and tree, so the sum is the same on every run.
+__global__ void partials_reduce_kernel(const double *__restrict__ partials, int nblocks, int nq, double *tot) {
+  const int q = blockIdx.x;
+  double s = 0.0;
+  for (int e = threadIdx.x; e < 3 * nblocks; e += blockDim.x) s += partials[(size_t)e * nq + q];
+  s = warp_sum(s);
+  __shared__ double red[32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+    tot[q] = t;
+  }
+}
+
+template <typename T>
+__global__ void finalize_kernel(const FinalizeParams<T> P) {
+  const T dt = *P.dt;
+  *P.t_out = *P.t0 + dt;
+  *P.dt_out = dt;
+  const double *tot = P.tot;
+  const double ddt = (double)dt;
+  int bad = 0;
+  for (int b = 0; b < P.nbody; ++b) {
+    const double scale = -(P.h * P.h * P.h) / ddt;
+    const double *r = tot + b * 9;
+    double fx = r[0] * scale, fy = r[3] * scale, fz = r[6] * scale;
+    double mx = r[4] * scale + r[7] * scale, my = r[1] * scale + r[8] * scale, mz = r[2] * scale + r[5] * scale;
+    if (P.symmetry) {
+      const double dy = P.moment_ref_y - P.y0;
+      fx *= 2.0;
+      fz *= 2.0;
+      my *= 2.0;
+      fy = 0.0;
+      mx = -dy * fz;
+      mz = dy * fx;
+    }
+    const double qa = 0.5 * P.ref_area;
+    const double c6[6] = {fx / qa, fy / qa, fz / qa, mx / (qa * P.span_ref), my / (qa * P.length_ref),
+                          mz / (qa * P.span_ref)};
+    for (int c = 0; c < 6; ++c) {
+      P.coeffs[b * 6 + c] = T(c6[c]);
+      if (!(c6[c] == c6[c])) bad = 1;
+    }
+  }
+  if (P.heat_rate) {
+    const double sym = P.symmetry ? 2.0 : 1.0;
+    const double scale = sym * P.h * P.h * P.h * P.pe / ddt;
+    for (int b = 0; b < P.nbody; ++b) {
+      double q = 0.0;
+      for (int t = 0; t < P.n_tbody; ++t)
+        if (P.t_index[t] == b) q += tot[P.nbody * 9 + t];
+      q = q * scale + P.flux_rate[b] * sym;
+      P.heat_rate[b] = T(q);
+      if (!(q == q)) bad = 1;
+    }
+  }
+  if (bad || !(dt == dt)) atomicOr(P.status, 1);
+}
+
+// psi_w (in p) <- psi * wgt (mode 0), psi_w + wgt * psi (mode 1), or, at the last stage,
+// (psi_w + wgt * psi) * (1 / dt): the step-averaged pressure (core.py:874-875, mode 2)
+template <typename T>
+__global__ void psi_accumulate_kernel(const T *__restrict__ psi, T *__restrict__ pw, size_t n, T wgt, int mode,
+                                      const T *__restrict__ dt) {
+  const T rdt = mode == 2 ? T(1) / *dt : T(1);
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    if (mode == 0) {
+      pw[e] = psi[e] * wgt;
+    } else {
+      const T s = pw[e] + wgt * psi[e];
+      pw[e] = mode == 2 ? s * rdt : s;
+    }
+  }
+}
+
+// --------------------------------------------------------------------------------------
+// launchers
+// --------------------------------------------------------------------------------------
+
+template <typename T>
+cudaError_t launch_absmax(const T *a, size_t n, unsigned long long *out, cudaStream_t s) {
+  int blocks = (int)std::min<size_t>((n + 255) / 256, 148 * 8);
+  absmax_kernel<T><<<blocks, 256, 0, s>>>(a, n, out);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_copy_u(const T *u, T *out, int nx, int ny, int nz, int pitch, unsigned long long *mx,
+                          cudaStream_t s) {
+  copy_u_kernel<T><<<dim3((nx + 1 + 127) / 128, ny, nz), 128, 0, s>>>(u, out, nx, ny, pitch, mx);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_dt(const DtParams &P, cudaStream_t s) {
+  dt_kernel<T><<<1, 1, 0, s>>>(P);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_outlet_sum(const T *u, const T *u0, int nx, int rows, double *sums, cudaStream_t s) {
+  outlet_sum_kernel<T><<<1, 1024, 0, s>>>(u, u0, nx, rows, sums);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_outlet_corr(const double *sums_p, const double *sum_u0, const double *sum_inlet, const T *dt,
+                               double a, double b, double inv_h, double inv_rows, T *corr, cudaStream_t s) {
+  outlet_corr_kernel<T><<<1, 1, 0, s>>>(sums_p, sum_u0, sum_inlet, dt, a, b, inv_h, inv_rows, corr);
+  return cudaGetLastError();
+}
+
+static inline int grid_for(size_t n) { return (int)std::max<size_t>(1, std::min<size_t>((n + 255) / 256, 148 * 16)); }
+
+template <typename T>
+cudaError_t launch_divergence(const T *u, const T *v, const T *w, int nx, int ny, int nz, int px, int py, int pz,
+                              T inv_h, T *div, cudaStream_t s) {
+  divergence_kernel<T><<<dim3((nx + 127) / 128, ny, nz), 128, 0, s>>>(u, v, w, nx, ny, nz, px, py, pz, inv_h, div);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_correct(const CorrectParams<T> &P, cudaStream_t s) {
+  correct_kernel<T><<<dim3((P.nx + 1 + 127) / 128, P.ny + 1, P.nz + 1), 128, 0, s>>>(P);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_smoke(const SmokeParams<T> &P, cudaStream_t s) {
+  smoke_kernel<T><<<dim3((P.nx + 127) / 128, P.ny, P.nz), 128, 0, s>>>(P);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_finalize(const FinalizeParams<T> &P, cudaStream_t s) {
+  if (P.nq > 0) {
+    partials_reduce_kernel<<<P.nq, 256, 0, s>>>(P.partials, P.nblocks, P.nq, P.tot);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  finalize_kernel<T><<<1, 1, 0, s>>>(P);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_psi_accumulate(const T *psi, T *pw, size_t n, T wgt, int mode, const T *dt, cudaStream_t s) {
+  psi_accumulate_kernel<T><<<grid_for(n), 256, 0, s>>>(psi, pw, n, wgt, mode, dt);
+  return cudaGetLastError();
+}
+
+#define INSTANTIATE(T)                                                                                               \
+  template cudaError_t launch_absmax<T>(const T *, size_t, unsigned long long *, cudaStream_t);                     \
+  template cudaError_t launch_dt<T>(const DtParams &, cudaStream_t);                                                \
+  template cudaError_t launch_copy_u<T>(const T *, T *, int, int, int, int, unsigned long long *, cudaStream_t);                                                \
+  template cudaError_t launch_outlet_sum<T>(const T *, const T *, int, int, double *, cudaStream_t);                 \
+  template cudaError_t launch_outlet_corr<T>(const double *, const double *, const double *, const T *, double,      \
+                                             double, double, double, T *, cudaStream_t);                             \
+  template cudaError_t launch_divergence<T>(const T *, const T *, const T *, int, int, int, int, int, int, T, T *,    \
+                                            cudaStream_t);                                                           \
+  template cudaError_t launch_correct<T>(const CorrectParams<T> &, cudaStream_t);                                   \
+  template cudaError_t launch_smoke<T>(const SmokeParams<T> &, cudaStream_t);                                       \
+  template cudaError_t launch_finalize<T>(const FinalizeParams<T> &, cudaStream_t);                                 \
+  template cudaError_t launch_psi_accumulate<T>(const T *, T *, size_t, T, int, const T *, cudaStream_t);
+
+INSTANTIATE(float)
+INSTANTIATE(double)
+
+}  // namespace aero

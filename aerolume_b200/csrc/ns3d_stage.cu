@@ -1,5 +1,4 @@
-// The 3D SSP-RK3 stage kernel and its helpers (pre-pass, time step, outlet sums,
-// correction, smoke, end of step).
+// The eddy-viscosity kernel and the SSP-RK3 stage kernel of the 3D step.
 //
 // Arithmetic follows the reference's plain-torch step (Aerolume ns3d/core.py:765-883)
 // operation by operation, so float64 runs agree with it to round-off:
@@ -7,116 +6,187 @@
 //   LES         core.py:400-524      RK update  core.py:819-827
 //   boundaries  core.py:281-297, 527-543
 //   penalty     core.py:615-634      buoyancy   physics.py:744-790
-//   theta       physics.py:609-708   dt rule    core.py:637-646, physics.py:723-742,1230-1262
-//   smoke       dye.py:232-312
+//   theta       physics.py:609-708
 //
-// Layout: every field is a C-contiguous (z, y, x) array with the staggered shapes of
-// core.py:11-14.  The stage kernel tiles x-y in 32 x 8 columns and marches along z,
-// keeping five planes of each velocity component and of theta (two ghost layers) and
-// three planes of the eddy viscosity in shared memory.
+// Layout: C-contiguous (z, y, x) arrays with the staggered shapes of core.py:11-14; the
+// stage-start u is read from a copy with a 16-byte row pitch (the reference's u rows hold
+// nx + 1 values).  Both kernels tile x-y in 32 x 8 columns and march along z through a ring
+// of plane slots in shared memory.  One thread streams each new z-plane of every field into
+// its slot with TMA (cp.async.bulk.tensor, completion on the slot's mbarrier) one plane
+// ahead of the computation, so the copies overlap the arithmetic; tiles on the domain
+// boundary then overwrite their out-of-range entries with the ghost-cell rules.  Shapes
+// whose rows are not 16-byte multiples use a synchronous loader into the same slots.
+// What the z direction needs on both sides of a plane -- the z fluxes of the momentum
+// components and of theta, the x-z / y-z shear stresses and tau_33 -- is evaluated once
+// per interface and carried to the next plane in registers.
 #include "ns3d.cuh"
+#include "stencil.cuh"
+#include "tma.cuh"
 
 namespace aero {
 
+constexpr int TX = 32, TY = 8;
+// stage tile: x from i0 - 4 (a 16-byte aligned TMA start) to i0 + TX + 3, y from j0 - 2
+constexpr int PX = TX + 8, PY = TY + 4, PPL = PX * PY;
+// eddy-viscosity tile of the stage kernel: nu array columns i0 .. i0 + TX + 3, rows j0 .. j0 + TY + 1
+constexpr int NUX = TX + 4, NUY = TY + 2, NUPL = 384;  // 360 used, slots padded to 128 bytes
+constexpr int NSLOT = 6;
+// nu kernel tile: x from i0 - 4, y from j0 - 2, 36 x 10
+constexpr int QX = TX + 4, QY = TY + 2, QPL = 384;
+constexpr int QSLOT = 4;
+
 // --------------------------------------------------------------------------------------
-// small device helpers
+// eddy viscosity nu_t on cells -1..n of every axis (core.py:400-482, 498-504), written to
+// nu[k + 1][j + 1][i + 1] of an (nz+2, ny+2, nx+2) array, plus its maximum
 // --------------------------------------------------------------------------------------
 
-// 24/7 x the upwind3 flux, or 4 x the central flux (core.py:331-345).
 template <typename T>
-__device__ __forceinline__ T face_flux(T vsum, T a, T b, T c, T d, bool upwind) {
-  const T s = b + c;
-  if (!upwind) return vsum * s;
-  const T cen = s + T(-1.0 / 7.0) * (a + d);
-  const T dis = (b - c) + T(-1.0 / 3.0) * (a - d);
-  return vsum * cen + T(3.0 / 7.0) * fabs(vsum) * dis;
-}
-
-// MUSCL / van Leer upwind face value times the velocity (dye.py:266-277).
-template <typename T>
-__device__ __forceinline__ T van_leer(T p, T q) {
-  const T pq = p * q;
-  return pq > T(0) ? T(2) * pq / (p + q) : T(0);
-}
+struct NuSmem {
+  alignas(128) T vel[3][QSLOT][QPL];
+  uint64_t bar[QSLOT];
+};
 
 template <typename T>
-__device__ __forceinline__ T muscl_flux(T a, T b, T c, T d, T vel) {
-  const T up = b + T(0.5) * van_leer(b - a, c - b);
-  const T dn = c - T(0.5) * van_leer(c - b, d - c);
-  return vel * (vel > T(0) ? up : dn);
-}
-
-// Eddy viscosity from the traceless gradient (core.py:448-482); g[i][j] = du_i/dx_j.
-template <typename T>
-__device__ __forceinline__ T eddy_viscosity(const T g[3][3], int model, T cd2) {
-  T s[3][3];
-#pragma unroll
-  for (int i = 0; i < 3; ++i)
-#pragma unroll
-    for (int j = 0; j < 3; ++j) s[i][j] = T(0.5) * (g[i][j] + g[j][i]);
-  T ss = T(0);
-#pragma unroll
-  for (int i = 0; i < 3; ++i)
-#pragma unroll
-    for (int j = 0; j < 3; ++j) ss = ss + s[i][j] * s[i][j];
-  if (model == AERO_LES_SMAGORINSKY) return cd2 * sqrt(T(2) * ss + T(1e-30));
-  if (model == AERO_LES_WALE) {
-    T g2[3][3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-      for (int j = 0; j < 3; ++j) g2[i][j] = (g[i][0] * g[0][j] + g[i][1] * g[1][j]) + g[i][2] * g[2][j];
-    const T tr3 = (g2[0][0] + g2[1][1] + g2[2][2]) * T(1.0 / 3.0);
-    T sd = T(0);
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-      for (int j = 0; j < 3; ++j) {
-        T sdij = T(0.5) * (g2[i][j] + g2[j][i]);
-        if (i == j) sdij = sdij - tr3;
-        sd = sd + sdij * sdij;
-      }
-    const T sdp = sd > T(0) ? sd : T(0);
-    const T ssp = ss > T(0) ? ss : T(0);
-    const T num = pow(sdp, T(1.5));
-    const T den = pow(ssp, T(2.5)) + pow(sdp, T(1.25)) + T(1e-30);
-    return cd2 * num / den;
+__global__ void __launch_bounds__(TX *TY) nu_kernel(const __grid_constant__ NuParams<T> P) {
+  __shared__ NuSmem<T> S;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;  // cells of the tile: (j0-1+ty, i0-1+tx)
+  const int qb = blockIdx.z * P.zc, qe = min(qb + P.zc, P.nz + 2);
+  const int nx = P.nx, ny = P.ny, nz = P.nz;
+  const T inv = P.inv_h;
+  // tile entry (ly, lx) <-> x index i0 - 4 + lx (face for u, cell for v / w), y index j0 - 2 + ly
+  const bool interior_xy = i0 - 2 >= 0 && i0 + TX <= nx && j0 - 2 >= 0 && j0 + TY <= ny;
+  const uint32_t bytes = 3u * QX * QY * sizeof(T);
+  auto SL = [&](int kp) { return (kp - qb + 2) & (QSLOT - 1); };
+  auto issue = [&](int kp) {
+    const int s = SL(kp);
+    fence_proxy_async();
+    mbar_arrive_expect_tx(&S.bar[s], bytes);
+    tma_load_3d(S.vel[0][s], &P.map_u, i0 - 4, j0 - 2, kp, &S.bar[s]);
+    tma_load_3d(S.vel[1][s], &P.map_v, i0 - 4, j0 - 2, kp, &S.bar[s]);
+    tma_load_3d(S.vel[2][s], &P.map_w, i0 - 4, j0 - 2, kp, &S.bar[s]);
+  };
+  // entries outside an array get the ghost rule's value (all entries on the slow path)
+  auto fill = [&](int kp, bool all) {
+    const int s = SL(kp);
+    if (!all && interior_xy && kp >= 0 && kp < nz) return;
+    for (int e = tid; e < QX * QY; e += TX * TY) {
+      const int ly = e / QX, lx = e - ly * QX;
+      if (lx < 2) continue;
+      const int gj = j0 - 2 + ly, gi = i0 - 4 + lx;
+      if (all || gi < 0 || gi > nx || gj < 0 || gj >= ny || kp < 0 || kp >= nz)
+        S.vel[0][s][e] = padded<T>(P.up, P.ru, kp, gj, gi);
+      if (all || gi < 0 || gi >= nx || gj < 0 || gj > ny || kp < 0 || kp >= nz)
+        S.vel[1][s][e] = padded<T>(P.vp, P.rv, kp, gj, gi);
+      if (all || gi < 0 || gi >= nx || gj < 0 || gj >= ny || kp < 0 || kp > nz)
+        S.vel[2][s][e] = padded<T>(P.wp, P.rw, kp, gj, gi);
+    }
+  };
+  auto await_plane = [&](int kp) {
+    const int m = kp - qb + 2;
+    mbar_wait_bounded(&S.bar[SL(kp)], (uint32_t)((m / QSLOT) & 1), P.status);
+  };
+  if (tid == 0) {
+    for (int q = 0; q < QSLOT; ++q) mbar_init(&S.bar[q], 1);
+    mbar_fence_init();
   }
-  // Vreman: beta_ij = sum_m g[i][m] g[j][m]
-  T b[3][3];
+  __syncthreads();
+  // nu plane q holds cells k = q - 1, which need velocity planes q - 2 .. q
+  if (P.use_tma) {
+    if (tid == 0)
+      for (int kp = qb - 2; kp <= qb; ++kp) issue(kp);
+    for (int kp = qb - 2; kp <= qb; ++kp) {
+      await_plane(kp);
+      fill(kp, false);
+    }
+  } else {
+    for (int kp = qb - 2; kp <= qb; ++kp) fill(kp, true);
+  }
+  __syncthreads();
+#define V3(c, dz, yy, xx) S.vel[c][SL(kn + (dz))][(yy) * QX + (xx)]
+  T mx = T(0);
+  for (int q = qb; q < qe; ++q) {
+    const bool pre = q + 1 < qe;
+    if (P.use_tma && pre && tid == 0) issue(q + 1);
+    const int kn = q - 1;
+    const int cj = j0 - 1 + ty, ci = i0 - 1 + tx;  // this thread's cell
+    if (cj <= ny && ci <= nx) {
+      const int y = ty + 1, x = tx + 3;
+      const T qq = T(0.25);
+      T g[3][3];
+      g[0][0] = (V3(0, 0, y, x + 1) - V3(0, 0, y, x)) * inv;
+      g[1][1] = (V3(1, 0, y + 1, x) - V3(1, 0, y, x)) * inv;
+      g[0][1] = ((((V3(0, 0, y, x) - V3(0, 0, y - 1, x)) * inv + (V3(0, 0, y + 1, x) - V3(0, 0, y, x)) * inv) +
+                  (V3(0, 0, y, x + 1) - V3(0, 0, y - 1, x + 1)) * inv) +
+                 (V3(0, 0, y + 1, x + 1) - V3(0, 0, y, x + 1)) * inv) *
+                qq;
+      g[0][2] = ((((V3(0, 0, y, x) - V3(0, -1, y, x)) * inv + (V3(0, 1, y, x) - V3(0, 0, y, x)) * inv) +
+                  (V3(0, 0, y, x + 1) - V3(0, -1, y, x + 1)) * inv) +
+                 (V3(0, 1, y, x + 1) - V3(0, 0, y, x + 1)) * inv) *
+                qq;
+      g[1][0] = ((((V3(1, 0, y, x) - V3(1, 0, y, x - 1)) * inv + (V3(1, 0, y + 1, x) - V3(1, 0, y + 1, x - 1)) * inv) +
+                  (V3(1, 0, y, x + 1) - V3(1, 0, y, x)) * inv) +
+                 (V3(1, 0, y + 1, x + 1) - V3(1, 0, y + 1, x)) * inv) *
+                qq;
+      g[1][2] = ((((V3(1, 0, y, x) - V3(1, -1, y, x)) * inv + (V3(1, 1, y, x) - V3(1, 0, y, x)) * inv) +
+                  (V3(1, 0, y + 1, x) - V3(1, -1, y + 1, x)) * inv) +
+                 (V3(1, 1, y + 1, x) - V3(1, 0, y + 1, x)) * inv) *
+                qq;
+      g[2][0] = ((((V3(2, 0, y, x) - V3(2, 0, y, x - 1)) * inv + (V3(2, 1, y, x) - V3(2, 1, y, x - 1)) * inv) +
+                  (V3(2, 0, y, x + 1) - V3(2, 0, y, x)) * inv) +
+                 (V3(2, 1, y, x + 1) - V3(2, 1, y, x)) * inv) *
+                qq;
+      g[2][1] = ((((V3(2, 0, y, x) - V3(2, 0, y - 1, x)) * inv + (V3(2, 1, y, x) - V3(2, 1, y - 1, x)) * inv) +
+                  (V3(2, 0, y + 1, x) - V3(2, 0, y, x)) * inv) +
+                 (V3(2, 1, y + 1, x) - V3(2, 1, y, x)) * inv) *
+                qq;
+      g[2][2] = -(g[0][0] + g[1][1]);
+      T nu = eddy_viscosity<T>(g, P.les, P.cd2);
+      if (P.has_win && kn >= P.win[0] && kn < P.win[1] && cj >= P.win[2] && cj < P.win[3] && ci >= P.win[4] &&
+          ci < P.win[5]) {
+        const T chi = P.chi_c[((size_t)(kn - P.win[0]) * P.wny + (cj - P.win[2])) * P.wnx + (ci - P.win[4])];
+        nu = nu * (T(1) - chi);
+      }
+      P.nu[((size_t)q * (ny + 2) + (cj + 1)) * P.nu_pitch + (ci + 1)] = nu;
+      mx = (nu > mx || nu != nu) ? nu : mx;
+    }
+    if (pre) {
+      if (P.use_tma) {
+        await_plane(q + 1);
+        fill(q + 1, false);
+      } else {
+        fill(q + 1, true);
+      }
+    }
+    __syncthreads();
+  }
+#undef V3
+  if (P.nut_max) {
 #pragma unroll
-  for (int i = 0; i < 3; ++i)
-#pragma unroll
-    for (int j = 0; j < 3; ++j) b[i][j] = (g[i][0] * g[j][0] + g[i][1] * g[j][1]) + g[i][2] * g[j][2];
-  T bb = b[0][0] * b[1][1] - b[0][1] * b[0][1] + b[0][0] * b[2][2] - b[0][2] * b[0][2] + b[1][1] * b[2][2] -
-         b[1][2] * b[1][2];
-  bb = bb > T(0) ? bb : T(0);
-  T aa = T(0);
-#pragma unroll
-  for (int i = 0; i < 3; ++i)
-#pragma unroll
-    for (int j = 0; j < 3; ++j) aa = aa + g[i][j] * g[i][j];
-  return cd2 * sqrt(bb / (aa + T(1e-30)) + T(1e-30));
+    for (int o = 16; o > 0; o >>= 1) {
+      const T other = __shfl_xor_sync(0xffffffffu, mx, o);
+      mx = (other > mx || other != other) ? other : mx;
+    }
+    if ((tid & 31) == 0) atomic_max_nonneg(P.nut_max, (double)mx);
+  }
 }
 
 // --------------------------------------------------------------------------------------
 // the stage kernel
 // --------------------------------------------------------------------------------------
 
-constexpr int TX = 32, TY = 8, HX = TX + 4, HY = TY + 4, NPL = HX * HY;  // velocity / theta planes
-constexpr int NX2 = TX + 2, NY2 = TY + 2, NNU = NX2 * NY2;               // eddy-viscosity planes
-
 template <typename T>
 struct StageSmem {
-  T vel[3][5][NPL];
-  T th[5][NPL];
-  T nu[3][NNU];
+  alignas(128) T vel[3][NSLOT][PPL];
+  alignas(128) T th[NSLOT][PPL];
+  alignas(128) T nu[NSLOT][NUPL];
   double acc[8][AERO_MAX_BODIES * 10];  // per-warp force / heat sums
+  uint64_t bar[NSLOT];
 };
 
 template <typename T>
-__global__ void __launch_bounds__(TX *TY) stage_kernel(const StageParams<T> P) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+__global__ void __launch_bounds__(TX *TY, 2) stage_kernel(const __grid_constant__ StageParams<T> P) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   StageSmem<T> &S = *reinterpret_cast<StageSmem<T> *>(smem_raw);
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
   const int lane = tid & 31, warp = tid >> 5;
@@ -126,116 +196,141 @@ __global__ void __launch_bounds__(TX *TY) stage_kernel(const StageParams<T> P) {
   const int i = i0 + tx, j = j0 + ty;
   const bool les = P.les != AERO_LES_NONE;
   const bool upwind = P.upwind != 0;
+  const bool thermal = P.thermal != 0;
   const T inv = P.inv_h;
   const int nq = P.nq;
-  const bool nut_only = P.mode == MODE_NUT_ONLY;
 
-  if (!nut_only)
-    for (int q = tid; q < 8 * AERO_MAX_BODIES * 10; q += TX * TY) (&S.acc[0][0])[q] = 0.0;
+  for (int q = tid; q < 8 * AERO_MAX_BODIES * 10; q += TX * TY) (&S.acc[0][0])[q] = 0.0;
 
-  // ---- loaders -------------------------------------------------------------------
-  auto load_plane = [&](int kp) {
-    const int slot = ((kp % 5) + 5) % 5;
-    for (int e = tid; e < NPL; e += TX * TY) {
-      const int ly = e / HX, lx = e - ly * HX;
-      const int gj = j0 - 2 + ly, gi = i0 - 2 + lx;
-      S.vel[0][slot][e] = padded<T>(P.up, P.ru, kp, gj, gi);
-      S.vel[1][slot][e] = padded<T>(P.vp, P.rv, kp, gj, gi);
-      S.vel[2][slot][e] = padded<T>(P.wp, P.rw, kp, gj, gi);
-      if (P.thermal) S.th[slot][e] = theta_padded<T>(P.thp, nz, ny, nx, P.sides, P.h, kp, gj, gi);
-    }
+  // ---- plane slots: plane kp of every field (and nu cell plane kp - 1) lives in slot SL(kp)
+  // tile entry (ly, lx) <-> x index i0 - 4 + lx, y index j0 - 2 + ly
+  const bool interior_xy = i0 - 2 >= 0 && i0 + TX + 2 <= nx && j0 - 2 >= 0 && j0 + TY + 2 <= ny;
+  const uint32_t bytes = (uint32_t)sizeof(T) * ((3u + (thermal ? 1u : 0u)) * PPL + (les ? (uint32_t)(NUX * NUY) : 0u));
+  auto SL = [&](int kp) { return (kp - kb + 2) % NSLOT; };
+  auto issue = [&](int kp) {
+    const int s = SL(kp);
+    fence_proxy_async();
+    mbar_arrive_expect_tx(&S.bar[s], bytes);
+    tma_load_3d(S.vel[0][s], &P.map_u, i0 - 4, j0 - 2, kp, &S.bar[s]);
+    tma_load_3d(S.vel[1][s], &P.map_v, i0 - 4, j0 - 2, kp, &S.bar[s]);
+    tma_load_3d(S.vel[2][s], &P.map_w, i0 - 4, j0 - 2, kp, &S.bar[s]);
+    if (thermal) tma_load_3d(S.th[s], &P.map_th, i0 - 4, j0 - 2, kp, &S.bar[s]);
+    if (les) tma_load_3d(S.nu[s], &P.map_nu, i0, j0, kp, &S.bar[s]);
   };
-  // velocity at plane (kc + dz), local cell (ly, lx) of the halo-2 tile
-#define VEL(c, dz, ly, lx) S.vel[c][(((kc + (dz)) % 5) + 5) % 5][(ly) * HX + (lx)]
-#define TH(dz, ly, lx) S.th[(((kc + (dz)) % 5) + 5) % 5][(ly) * HX + (lx)]
-#define NU(dz, ly, lx) S.nu[(((kc + (dz)) % 3) + 3) % 3][(ly) * NX2 + (lx)]
-
-  // eddy viscosity of plane kn for the (TY+2) x (TX+2) cells of the tile and its ring
-  T nut_local_max = T(0);
-  auto compute_nu = [&](int kn) {
-    const int kc = kn;  // velocity offsets are relative to plane kn
-    const int slot = ((kn % 3) + 3) % 3;
-    for (int e = tid; e < NNU; e += TX * TY) {
-      const int ly = e / NX2, lx = e - ly * NX2;
-      const int cj = j0 - 1 + ly, ci = i0 - 1 + lx;
-      T nu = T(0);
-      if (cj >= -1 && cj <= ny && ci >= -1 && ci <= nx && kn >= -1 && kn <= nz) {
-        const int y = ly + 1, x = lx + 1;  // this cell in the halo-2 tile
-        T g[3][3];
-        g[0][0] = (VEL(0, 0, y, x + 1) - VEL(0, 0, y, x)) * inv;
-        g[1][1] = (VEL(1, 0, y + 1, x) - VEL(1, 0, y, x)) * inv;
-        const T q = T(0.25);
-        g[0][1] = ((((VEL(0, 0, y, x) - VEL(0, 0, y - 1, x)) * inv + (VEL(0, 0, y + 1, x) - VEL(0, 0, y, x)) * inv) +
-                    (VEL(0, 0, y, x + 1) - VEL(0, 0, y - 1, x + 1)) * inv) +
-                   (VEL(0, 0, y + 1, x + 1) - VEL(0, 0, y, x + 1)) * inv) *
-                  q;
-        g[0][2] = ((((VEL(0, 0, y, x) - VEL(0, -1, y, x)) * inv + (VEL(0, 1, y, x) - VEL(0, 0, y, x)) * inv) +
-                    (VEL(0, 0, y, x + 1) - VEL(0, -1, y, x + 1)) * inv) +
-                   (VEL(0, 1, y, x + 1) - VEL(0, 0, y, x + 1)) * inv) *
-                  q;
-        g[1][0] = ((((VEL(1, 0, y, x) - VEL(1, 0, y, x - 1)) * inv + (VEL(1, 0, y + 1, x) - VEL(1, 0, y + 1, x - 1)) * inv) +
-                    (VEL(1, 0, y, x + 1) - VEL(1, 0, y, x)) * inv) +
-                   (VEL(1, 0, y + 1, x + 1) - VEL(1, 0, y + 1, x)) * inv) *
-                  q;
-        g[1][2] = ((((VEL(1, 0, y, x) - VEL(1, -1, y, x)) * inv + (VEL(1, 1, y, x) - VEL(1, 0, y, x)) * inv) +
-                    (VEL(1, 0, y + 1, x) - VEL(1, -1, y + 1, x)) * inv) +
-                   (VEL(1, 1, y + 1, x) - VEL(1, 0, y + 1, x)) * inv) *
-                  q;
-        g[2][0] = ((((VEL(2, 0, y, x) - VEL(2, 0, y, x - 1)) * inv + (VEL(2, 1, y, x) - VEL(2, 1, y, x - 1)) * inv) +
-                    (VEL(2, 0, y, x + 1) - VEL(2, 0, y, x)) * inv) +
-                   (VEL(2, 1, y, x + 1) - VEL(2, 1, y, x)) * inv) *
-                  q;
-        g[2][1] = ((((VEL(2, 0, y, x) - VEL(2, 0, y - 1, x)) * inv + (VEL(2, 1, y, x) - VEL(2, 1, y - 1, x)) * inv) +
-                    (VEL(2, 0, y + 1, x) - VEL(2, 0, y, x)) * inv) +
-                   (VEL(2, 1, y + 1, x) - VEL(2, 1, y, x)) * inv) *
-                  q;
-        g[2][2] = -(g[0][0] + g[1][1]);
-        nu = eddy_viscosity<T>(g, P.les, P.les_cd2);
-        if (kn >= P.win[0] && kn < P.win[1] && cj >= P.win[2] && cj < P.win[3] && ci >= P.win[4] && ci < P.win[5]) {
-          const T chi = P.chi_c[((size_t)(kn - P.win[0]) * P.wny + (cj - P.win[2])) * P.wnx + (ci - P.win[4])];
-          nu = nu * (T(1) - chi);
-        }
-        nut_local_max = fmax(nut_local_max, nu);
+  // entries outside an array get the ghost rule's value (every entry on the slow path)
+  auto fill = [&](int kp, bool all) {
+    const int s = SL(kp);
+    if (!all && interior_xy && kp >= 0 && kp < nz) return;
+    for (int e = tid; e < PPL; e += TX * TY) {
+      const int ly = e / PX, lx = e - ly * PX;
+      if (lx < 2) continue;
+      const int gj = j0 - 2 + ly, gi = i0 - 4 + lx;
+      const bool oc = gi < 0 || gi >= nx || gj < 0 || gj >= ny || kp < 0 || kp >= nz;
+      if (all || oc || gi == nx) S.vel[0][s][e] = padded<T>(P.up, P.ru, kp, gj, gi);
+      if (all || oc || gj == ny) S.vel[1][s][e] = padded<T>(P.vp, P.rv, kp, gj, gi);
+      if (all || oc || kp == nz) S.vel[2][s][e] = padded<T>(P.wp, P.rw, kp, gj, gi);
+      if (thermal && (all || oc)) S.th[s][e] = theta_padded<T>(P.thp, nz, ny, nx, P.sides, P.h, kp, gj, gi);
+    }
+    if (all && les) {
+      const int q = min(max(kp, 0), nz + 1);
+      for (int e = tid; e < NUX * NUY; e += TX * TY) {
+        const int ly = e / NUX, lx = e - ly * NUX;
+        const int r = min(j0 + ly, ny + 1), c = min(i0 + lx, nx + 1);
+        S.nu[s][e] = __ldg(P.nu + ((size_t)q * (ny + 2) + r) * P.nu_pitch + c);
       }
-      S.nu[slot][e] = nu;
+    }
+  };
+  auto await_plane = [&](int kp) {
+    const int m = kp - kb + 2;
+    mbar_wait_bounded(&S.bar[SL(kp)], (uint32_t)((m / NSLOT) & 1), P.status);
+  };
+#define VEL(c, dz, yy, xx) S.vel[c][SL(kc + (dz))][(yy) * PX + (xx)]
+#define TH(dz, yy, xx) S.th[SL(kc + (dz))][(yy) * PX + (xx)]
+#define NU(dz, yy, xx) S.nu[SL(kc + (dz) + 1)][(yy) * NUX + (xx)]
+
+  const int y = ty + 2, x = tx + 4;      // this thread's cell / faces in the plane tile
+  const int ny2 = ty + 1, nx2 = tx + 1;  // ... in the eddy-viscosity tile
+  const bool valid = (i < nx) && (j < ny);
+  const int wk0 = P.win[0], wk1 = P.win[1], wj0 = P.win[2], wj1 = P.win[3], wi0 = P.win[4], wi1 = P.win[5];
+  const int wzn = wk1 - wk0, wyn = wj1 - wj0, wxn = wi1 - wi0;
+  const T two = T(2), qq = T(0.25);
+  const T kh = P.kh;
+  auto kface = [&](T n1, T n2, bool boundary) -> T {
+    if (!les || boundary) return kh;
+    return kh + P.kprt * (n1 + n2);
+  };
+
+  // ---- the z interface above plane kc (between kc and kc + 1), evaluated once and carried
+  T zu = T(0), zv = T(0), zw = T(0), z13 = T(0), z23 = T(0), z33 = T(0), zth = T(0);
+  auto z_interface = [&](const int kc) {
+    // u: z flux on the x-z edge (kc+1, i); v: on the y-z edge (kc+1, j); w: at the cell centre kc
+    zu = face_flux<T>(VEL(2, 1, y, x - 1) + VEL(2, 1, y, x), VEL(0, -1, y, x), VEL(0, 0, y, x), VEL(0, 1, y, x),
+                      VEL(0, 2, y, x), upwind);
+    zv = face_flux<T>(VEL(2, 1, y - 1, x) + VEL(2, 1, y, x), VEL(1, -1, y, x), VEL(1, 0, y, x), VEL(1, 1, y, x),
+                      VEL(1, 2, y, x), upwind);
+    zw = face_flux<T>(VEL(2, 0, y, x) + VEL(2, 1, y, x), VEL(2, -1, y, x), VEL(2, 0, y, x), VEL(2, 1, y, x),
+                      VEL(2, 2, y, x), upwind);
+    if (les) {  // tau_13, tau_23 on those edges; tau_33 at the cell centre kc
+      const T n13 = (((NU(0, ny2, nx2 - 1) + NU(1, ny2, nx2 - 1)) + NU(0, ny2, nx2)) + NU(1, ny2, nx2)) * qq;
+      const T s13 = (VEL(0, 1, y, x) - VEL(0, 0, y, x)) * inv + (VEL(2, 1, y, x) - VEL(2, 1, y, x - 1)) * inv;
+      z13 = n13 * s13;
+      const T n23 = (((NU(0, ny2 - 1, nx2) + NU(1, ny2 - 1, nx2)) + NU(0, ny2, nx2)) + NU(1, ny2, nx2)) * qq;
+      const T s23 = (VEL(1, 1, y, x) - VEL(1, 0, y, x)) * inv + (VEL(2, 1, y, x) - VEL(2, 1, y - 1, x)) * inv;
+      z23 = n23 * s23;
+      z33 = two * NU(0, ny2, nx2) * ((VEL(2, 1, y, x) - VEL(2, 0, y, x)) * inv);
+    }
+    if (thermal) {  // theta flux through the z face kc + 1 (between cells kc and kc + 1)
+      const T kz = kface(NU(0, ny2, nx2), NU(1, ny2, nx2), !P.pz && (kc + 1 == nz || kc + 1 == 0));
+      const T cb = TH(0, y, x), cc = TH(1, y, x);
+      T f = muscl_flux<T>(TH(-1, y, x), cb, cc, TH(2, y, x), VEL(2, 1, y, x)) - kz * (cc - cb);
+      if (P.has_adia && j >= wj0 && j < wj1 && i >= wi0 && i < wi1 && kc + 1 >= wk0 && kc + 1 <= wk1)
+        f += kz * P.adia_w[((size_t)(kc + 1 - wk0) * wyn + (j - wj0)) * wxn + (i - wi0)] * (cc - cb);
+      zth = f;
     }
   };
 
-  // ---- preload -----------------------------------------------------------------------
-  for (int kp = kb - 2; kp <= kb + 1; ++kp) load_plane(kp);
+  // ---- prologue: planes kb-2 .. kb+2 (nu cell planes kb-3 .. kb+1); the interface below kb
+  if (tid == 0) {
+    for (int q = 0; q < NSLOT; ++q) mbar_init(&S.bar[q], 1);
+    mbar_fence_init();
+  }
   __syncthreads();
-  if (les) {
-    compute_nu(kb - 1);
-    compute_nu(kb);
+  if (P.use_tma) {
+    if (tid == 0)
+      for (int kp = kb - 2; kp <= kb + 2; ++kp) issue(kp);
+    for (int kp = kb - 2; kp <= kb + 2; ++kp) {
+      await_plane(kp);
+      fill(kp, false);
+    }
+  } else {
+    for (int kp = kb - 2; kp <= kb + 2; ++kp) fill(kp, true);
+  }
+  __syncthreads();
+  {
+    const int kc = kb - 1;
+    if (valid) z_interface(kc);
   }
 
-  // per-thread register carry of theta / force sums
   for (int k = kb; k < ke; ++k) {
-    __syncthreads();
-    load_plane(k + 2);
-    __syncthreads();
-    if (les) {
-      compute_nu(k + 1);
-      __syncthreads();
-    }
-    if (nut_only) continue;
+    // stream plane k + 3 into the slot plane k - 3 used while this plane is computed
+    const bool pre = k + 3 <= ke + 1;
+    if (P.use_tma && pre && tid == 0) issue(k + 3);
     const int kc = k;
-    const int y = ty + 2, x = tx + 2;  // this thread's cell / faces in the halo-2 tile
-    const int ny2 = ty + 1, nx2 = tx + 1;  // ... in the eddy-viscosity tile
-    const bool valid = (i < nx) && (j < ny);
     const T bdt = P.bdt_scale * *P.dt;
     const T a = P.a;
 
     double cu = 0.0, cv = 0.0, cw = 0.0, ct = 0.0;  // weighted window increments
-    int fu_in = 0, fv_in = 0, fw_in = 0, ft_in = 0;  // which faces lie in the window
+    int fu_in = 0, fv_in = 0, fw_in = 0, ft_in = 0;
     size_t wu = 0, wv = 0, ww = 0, wt = 0;
 
     if (valid) {
-      // ================= momentum tendencies (core.py:353-397, 485-524) ===============
+      // the interface below this plane, carried from the previous plane
+      const T zu_l = zu, zv_l = zv, zw_l = zw, z13_l = z13, z23_l = z23, z33_l = z33, zth_l = zth;
+      z_interface(kc);
       const T kadv = P.kadv, nuh2 = P.nu_h2;
-      // ---- u face (k, j, i)
-      T lu;
-      {
+      // ================= momentum tendencies (core.py:353-397, 485-524) ===============
+      T lu, lv, lw;
+      {  // ---- u face (k, j, i)
         T au = face_flux<T>(VEL(0, 0, y, x - 1) + VEL(0, 0, y, x), VEL(0, 0, y, x - 2), VEL(0, 0, y, x - 1),
                             VEL(0, 0, y, x), VEL(0, 0, y, x + 1), upwind) -
                face_flux<T>(VEL(0, 0, y, x) + VEL(0, 0, y, x + 1), VEL(0, 0, y, x - 1), VEL(0, 0, y, x),
@@ -245,35 +340,23 @@ __global__ void __launch_bounds__(TX *TY) stage_kernel(const StageParams<T> P) {
         const T gyr = face_flux<T>(VEL(1, 0, y + 1, x - 1) + VEL(1, 0, y + 1, x), VEL(0, 0, y - 1, x), VEL(0, 0, y, x),
                                    VEL(0, 0, y + 1, x), VEL(0, 0, y + 2, x), upwind);
         au = au + (gyl - gyr);
-        const T gzl = face_flux<T>(VEL(2, 0, y, x - 1) + VEL(2, 0, y, x), VEL(0, -2, y, x), VEL(0, -1, y, x),
-                                   VEL(0, 0, y, x), VEL(0, 1, y, x), upwind);
-        const T gzr = face_flux<T>(VEL(2, 1, y, x - 1) + VEL(2, 1, y, x), VEL(0, -1, y, x), VEL(0, 0, y, x),
-                                   VEL(0, 1, y, x), VEL(0, 2, y, x), upwind);
-        au = (au + (gzl - gzr)) * kadv;
+        au = (au + (zu_l - zu)) * kadv;
         const T lap = ((VEL(0, 0, y, x + 1) + VEL(0, 0, y, x - 1)) + (VEL(0, 0, y + 1, x) + VEL(0, 0, y - 1, x)) +
                        (VEL(0, 1, y, x) + VEL(0, -1, y, x))) -
                       T(6) * VEL(0, 0, y, x);
         lu = au + nuh2 * lap;
         if (les) {
-          const T two = T(2), q = T(0.25);
           const T t11r = two * NU(0, ny2, nx2) * ((VEL(0, 0, y, x + 1) - VEL(0, 0, y, x)) * inv);
           const T t11l = two * NU(0, ny2, nx2 - 1) * ((VEL(0, 0, y, x) - VEL(0, 0, y, x - 1)) * inv);
-          const T n12l = (((NU(0, ny2 - 1, nx2 - 1) + NU(0, ny2, nx2 - 1)) + NU(0, ny2 - 1, nx2)) + NU(0, ny2, nx2)) * q;
+          const T n12l = (((NU(0, ny2 - 1, nx2 - 1) + NU(0, ny2, nx2 - 1)) + NU(0, ny2 - 1, nx2)) + NU(0, ny2, nx2)) * qq;
           const T s12l = (VEL(0, 0, y, x) - VEL(0, 0, y - 1, x)) * inv + (VEL(1, 0, y, x) - VEL(1, 0, y, x - 1)) * inv;
-          const T n12r = (((NU(0, ny2, nx2 - 1) + NU(0, ny2 + 1, nx2 - 1)) + NU(0, ny2, nx2)) + NU(0, ny2 + 1, nx2)) * q;
+          const T n12r = (((NU(0, ny2, nx2 - 1) + NU(0, ny2 + 1, nx2 - 1)) + NU(0, ny2, nx2)) + NU(0, ny2 + 1, nx2)) * qq;
           const T s12r =
               (VEL(0, 0, y + 1, x) - VEL(0, 0, y, x)) * inv + (VEL(1, 0, y + 1, x) - VEL(1, 0, y + 1, x - 1)) * inv;
-          const T n13l = (((NU(-1, ny2, nx2 - 1) + NU(0, ny2, nx2 - 1)) + NU(-1, ny2, nx2)) + NU(0, ny2, nx2)) * q;
-          const T s13l = (VEL(0, 0, y, x) - VEL(0, -1, y, x)) * inv + (VEL(2, 0, y, x) - VEL(2, 0, y, x - 1)) * inv;
-          const T n13r = (((NU(0, ny2, nx2 - 1) + NU(1, ny2, nx2 - 1)) + NU(0, ny2, nx2)) + NU(1, ny2, nx2)) * q;
-          const T s13r = (VEL(0, 1, y, x) - VEL(0, 0, y, x)) * inv + (VEL(2, 1, y, x) - VEL(2, 1, y, x - 1)) * inv;
-          const T fu = (((((t11r - t11l) + n12r * s12r) - n12l * s12l) + n13r * s13r) - n13l * s13l) * inv;
-          lu = lu + fu;
+          lu = lu + (((((t11r - t11l) + n12r * s12r) - n12l * s12l) + z13) - z13_l) * inv;
         }
       }
-      // ---- v face (k, j, i)
-      T lv;
-      {
+      {  // ---- v face (k, j, i)
         T av = face_flux<T>(VEL(0, 0, y - 1, x) + VEL(0, 0, y, x), VEL(1, 0, y, x - 2), VEL(1, 0, y, x - 1),
                             VEL(1, 0, y, x), VEL(1, 0, y, x + 1), upwind) -
                face_flux<T>(VEL(0, 0, y - 1, x + 1) + VEL(0, 0, y, x + 1), VEL(1, 0, y, x - 1), VEL(1, 0, y, x),
@@ -283,35 +366,23 @@ __global__ void __launch_bounds__(TX *TY) stage_kernel(const StageParams<T> P) {
         const T gyr = face_flux<T>(VEL(1, 0, y, x) + VEL(1, 0, y + 1, x), VEL(1, 0, y - 1, x), VEL(1, 0, y, x),
                                    VEL(1, 0, y + 1, x), VEL(1, 0, y + 2, x), upwind);
         av = av + (gyl - gyr);
-        const T gzl = face_flux<T>(VEL(2, 0, y - 1, x) + VEL(2, 0, y, x), VEL(1, -2, y, x), VEL(1, -1, y, x),
-                                   VEL(1, 0, y, x), VEL(1, 1, y, x), upwind);
-        const T gzr = face_flux<T>(VEL(2, 1, y - 1, x) + VEL(2, 1, y, x), VEL(1, -1, y, x), VEL(1, 0, y, x),
-                                   VEL(1, 1, y, x), VEL(1, 2, y, x), upwind);
-        av = (av + (gzl - gzr)) * kadv;
+        av = (av + (zv_l - zv)) * kadv;
         const T lap = ((VEL(1, 0, y, x + 1) + VEL(1, 0, y, x - 1)) + (VEL(1, 0, y + 1, x) + VEL(1, 0, y - 1, x)) +
                        (VEL(1, 1, y, x) + VEL(1, -1, y, x))) -
                       T(6) * VEL(1, 0, y, x);
         lv = av + nuh2 * lap;
         if (les) {
-          const T two = T(2), q = T(0.25);
-          const T n12l = (((NU(0, ny2 - 1, nx2 - 1) + NU(0, ny2, nx2 - 1)) + NU(0, ny2 - 1, nx2)) + NU(0, ny2, nx2)) * q;
+          const T n12l = (((NU(0, ny2 - 1, nx2 - 1) + NU(0, ny2, nx2 - 1)) + NU(0, ny2 - 1, nx2)) + NU(0, ny2, nx2)) * qq;
           const T s12l = (VEL(0, 0, y, x) - VEL(0, 0, y - 1, x)) * inv + (VEL(1, 0, y, x) - VEL(1, 0, y, x - 1)) * inv;
-          const T n12r = (((NU(0, ny2 - 1, nx2) + NU(0, ny2, nx2)) + NU(0, ny2 - 1, nx2 + 1)) + NU(0, ny2, nx2 + 1)) * q;
+          const T n12r = (((NU(0, ny2 - 1, nx2) + NU(0, ny2, nx2)) + NU(0, ny2 - 1, nx2 + 1)) + NU(0, ny2, nx2 + 1)) * qq;
           const T s12r =
               (VEL(0, 0, y, x + 1) - VEL(0, 0, y - 1, x + 1)) * inv + (VEL(1, 0, y, x + 1) - VEL(1, 0, y, x)) * inv;
           const T t22r = two * NU(0, ny2, nx2) * ((VEL(1, 0, y + 1, x) - VEL(1, 0, y, x)) * inv);
           const T t22l = two * NU(0, ny2 - 1, nx2) * ((VEL(1, 0, y, x) - VEL(1, 0, y - 1, x)) * inv);
-          const T n23l = (((NU(-1, ny2 - 1, nx2) + NU(0, ny2 - 1, nx2)) + NU(-1, ny2, nx2)) + NU(0, ny2, nx2)) * q;
-          const T s23l = (VEL(1, 0, y, x) - VEL(1, -1, y, x)) * inv + (VEL(2, 0, y, x) - VEL(2, 0, y - 1, x)) * inv;
-          const T n23r = (((NU(0, ny2 - 1, nx2) + NU(1, ny2 - 1, nx2)) + NU(0, ny2, nx2)) + NU(1, ny2, nx2)) * q;
-          const T s23r = (VEL(1, 1, y, x) - VEL(1, 0, y, x)) * inv + (VEL(2, 1, y, x) - VEL(2, 1, y - 1, x)) * inv;
-          const T fv = (((((n12r * s12r - n12l * s12l) + t22r) - t22l) + n23r * s23r) - n23l * s23l) * inv;
-          lv = lv + fv;
+          lv = lv + (((((n12r * s12r - n12l * s12l) + t22r) - t22l) + z23) - z23_l) * inv;
         }
       }
-      // ---- w face (k, j, i)
-      T lw;
-      {
+      {  // ---- w face (k, j, i)
         T aw = face_flux<T>(VEL(0, -1, y, x) + VEL(0, 0, y, x), VEL(2, 0, y, x - 2), VEL(2, 0, y, x - 1),
                             VEL(2, 0, y, x), VEL(2, 0, y, x + 1), upwind) -
                face_flux<T>(VEL(0, -1, y, x + 1) + VEL(0, 0, y, x + 1), VEL(2, 0, y, x - 1), VEL(2, 0, y, x),
@@ -321,31 +392,21 @@ __global__ void __launch_bounds__(TX *TY) stage_kernel(const StageParams<T> P) {
         const T gyr = face_flux<T>(VEL(1, -1, y + 1, x) + VEL(1, 0, y + 1, x), VEL(2, 0, y - 1, x), VEL(2, 0, y, x),
                                    VEL(2, 0, y + 1, x), VEL(2, 0, y + 2, x), upwind);
         aw = aw + (gyl - gyr);
-        const T gzl = face_flux<T>(VEL(2, -1, y, x) + VEL(2, 0, y, x), VEL(2, -2, y, x), VEL(2, -1, y, x),
-                                   VEL(2, 0, y, x), VEL(2, 1, y, x), upwind);
-        const T gzr = face_flux<T>(VEL(2, 0, y, x) + VEL(2, 1, y, x), VEL(2, -1, y, x), VEL(2, 0, y, x),
-                                   VEL(2, 1, y, x), VEL(2, 2, y, x), upwind);
-        aw = (aw + (gzl - gzr)) * kadv;
+        aw = (aw + (zw_l - zw)) * kadv;
         const T lap = ((VEL(2, 0, y, x + 1) + VEL(2, 0, y, x - 1)) + (VEL(2, 0, y + 1, x) + VEL(2, 0, y - 1, x)) +
                        (VEL(2, 1, y, x) + VEL(2, -1, y, x))) -
                       T(6) * VEL(2, 0, y, x);
         lw = aw + nuh2 * lap;
         if (les) {
-          const T two = T(2), q = T(0.25);
-          const T n13l = (((NU(-1, ny2, nx2 - 1) + NU(0, ny2, nx2 - 1)) + NU(-1, ny2, nx2)) + NU(0, ny2, nx2)) * q;
-          const T s13l = (VEL(0, 0, y, x) - VEL(0, -1, y, x)) * inv + (VEL(2, 0, y, x) - VEL(2, 0, y, x - 1)) * inv;
-          const T n13r = (((NU(-1, ny2, nx2) + NU(0, ny2, nx2)) + NU(-1, ny2, nx2 + 1)) + NU(0, ny2, nx2 + 1)) * q;
+          // tau_13 on the x-z edges (k, i) and (k, i+1), tau_23 on the y-z edges (k, j) and (k, j+1):
+          // the (k, i) and (k, j) ones are this thread's carried u / v interface values
+          const T n13r = (((NU(-1, ny2, nx2) + NU(0, ny2, nx2)) + NU(-1, ny2, nx2 + 1)) + NU(0, ny2, nx2 + 1)) * qq;
           const T s13r =
               (VEL(0, 0, y, x + 1) - VEL(0, -1, y, x + 1)) * inv + (VEL(2, 0, y, x + 1) - VEL(2, 0, y, x)) * inv;
-          const T n23l = (((NU(-1, ny2 - 1, nx2) + NU(0, ny2 - 1, nx2)) + NU(-1, ny2, nx2)) + NU(0, ny2, nx2)) * q;
-          const T s23l = (VEL(1, 0, y, x) - VEL(1, -1, y, x)) * inv + (VEL(2, 0, y, x) - VEL(2, 0, y - 1, x)) * inv;
-          const T n23r = (((NU(-1, ny2, nx2) + NU(0, ny2, nx2)) + NU(-1, ny2 + 1, nx2)) + NU(0, ny2 + 1, nx2)) * q;
+          const T n23r = (((NU(-1, ny2, nx2) + NU(0, ny2, nx2)) + NU(-1, ny2 + 1, nx2)) + NU(0, ny2 + 1, nx2)) * qq;
           const T s23r =
               (VEL(1, 0, y + 1, x) - VEL(1, -1, y + 1, x)) * inv + (VEL(2, 0, y + 1, x) - VEL(2, 0, y, x)) * inv;
-          const T t33r = two * NU(0, ny2, nx2) * ((VEL(2, 1, y, x) - VEL(2, 0, y, x)) * inv);
-          const T t33l = two * NU(-1, ny2, nx2) * ((VEL(2, 0, y, x) - VEL(2, -1, y, x)) * inv);
-          const T fw = (((((n13r * s13r - n13l * s13l) + n23r * s23r) - n23l * s23l) + t33r) - t33l) * inv;
-          lw = lw + fw;
+          lw = lw + (((((n13r * s13r - z13_l) + n23r * s23r) - z23_l) + z33) - z33_l) * inv;
         }
       }
 
@@ -360,9 +421,9 @@ __global__ void __launch_bounds__(TX *TY) stage_kernel(const StageParams<T> P) {
         vh = vp0 + lv * bdt;
         wh = wp0 + lw * bdt;
       } else {
-        uh = lerp_t<T>(up0, P.u0[iu], a) + lu * bdt;
-        vh = lerp_t<T>(vp0, P.v0[iv], a) + lv * bdt;
-        wh = lerp_t<T>(wp0, P.w0[iw], a) + lw * bdt;
+        uh = lerp_t<T>(up0, __ldg(P.u0 + iu), a) + lu * bdt;
+        vh = lerp_t<T>(vp0, __ldg(P.v0 + iv), a) + lv * bdt;
+        wh = lerp_t<T>(wp0, __ldg(P.w0 + iw), a) + lw * bdt;
       }
       if (!P.px && i == 0) uh = P.closed ? T(0) : P.u_inlet[(size_t)k * ny + j];
       if (!P.py && j == 0) vh = T(0);
@@ -372,23 +433,22 @@ __global__ void __launch_bounds__(TX *TY) stage_kernel(const StageParams<T> P) {
       const T kpen = bdt / P.eta;
       const T wg = P.wgt;
       if (P.has_win) {
-        const int k0 = P.win[0], k1 = P.win[1], wj0 = P.win[2], wj1 = P.win[3], wi0 = P.win[4], wi1 = P.win[5];
-        if (k >= k0 && k < k1 && j >= wj0 && j < wj1 && i >= wi0 && i <= wi1) {
-          wu = ((size_t)(k - k0) * (wj1 - wj0) + (j - wj0)) * (wi1 - wi0 + 1) + (i - wi0);
+        if (k >= wk0 && k < wk1 && j >= wj0 && j < wj1 && i >= wi0 && i <= wi1) {
+          wu = ((size_t)(k - wk0) * wyn + (j - wj0)) * (wxn + 1) + (i - wi0);
           const T un = (uh + kpen * P.a_u[wu]) / (T(1) + kpen * P.chi_u[wu]);
           cu = (double)((un - uh) * wg);
           uh = un;
           fu_in = 1;
         }
-        if (k >= k0 && k < k1 && j >= wj0 && j <= wj1 && i >= wi0 && i < wi1) {
-          wv = ((size_t)(k - k0) * (wj1 - wj0 + 1) + (j - wj0)) * (wi1 - wi0) + (i - wi0);
+        if (k >= wk0 && k < wk1 && j >= wj0 && j <= wj1 && i >= wi0 && i < wi1) {
+          wv = ((size_t)(k - wk0) * (wyn + 1) + (j - wj0)) * wxn + (i - wi0);
           const T vn = (vh + kpen * P.a_v[wv]) / (T(1) + kpen * P.chi_v[wv]);
           cv = (double)((vn - vh) * wg);
           vh = vn;
           fv_in = 1;
         }
-        if (k >= k0 && k <= k1 && j >= wj0 && j < wj1 && i >= wi0 && i < wi1) {
-          ww = ((size_t)(k - k0) * (wj1 - wj0) + (j - wj0)) * (wi1 - wi0) + (i - wi0);
+        if (k >= wk0 && k <= wk1 && j >= wj0 && j < wj1 && i >= wi0 && i < wi1) {
+          ww = ((size_t)(k - wk0) * wyn + (j - wj0)) * wxn + (i - wi0);
           const T wn = (wh + kpen * P.a_w[ww]) / (T(1) + kpen * P.chi_w[ww]);
           cw = (double)((wn - wh) * wg);
           wh = wn;
@@ -397,22 +457,18 @@ __global__ void __launch_bounds__(TX *TY) stage_kernel(const StageParams<T> P) {
       }
 
       // ================= buoyancy after the penalisation (physics.py:744-790) =========
-      if (P.thermal && P.ri != T(0)) {
-        if (k > 0 || P.pz) {
-          if (k > 0) {
-            const T tf = T(0.5) * (TH(0, y, x) + TH(-1, y, x));
-            wh = wh + tf * (bdt * P.ri);
-          } else {
-            const T edge = (TH(0, y, x) + TH(-1, y, x)) * (T(0.5) * P.ri) * bdt;
-            wh = wh + edge;
-          }
+      if (thermal && P.ri != T(0)) {
+        if (k > 0) {
+          const T tf = T(0.5) * (TH(0, y, x) + TH(-1, y, x));
+          wh = wh + tf * (bdt * P.ri);
+        } else if (P.pz) {
+          const T edge = (TH(0, y, x) + TH(-1, y, x)) * (T(0.5) * P.ri) * bdt;
+          wh = wh + edge;
         }
         if (fw_in && P.vol_w) {
           // theta on the w-face from the two cells around it (clamped / wrapped at the ends)
-          const int kl = (k == 0) ? (P.pz ? nz - 1 : 0) : k - 1;
-          const int kr = (k == nz) ? (P.pz ? 0 : nz - 1) : k;
-          const T tl = P.thp[((size_t)kl * ny + j) * nx + i], tr = P.thp[((size_t)kr * ny + j) * nx + i];
-          const T tw = T(0.5) * (tr + tl);
+          const T tl = (k == 0 && !P.pz) ? TH(0, y, x) : TH(-1, y, x);
+          const T tw = T(0.5) * (TH(0, y, x) + tl);
           const T share = (tw * P.vol_w[ww]) * (bdt * (P.ri * wg));
           cw += (double)share;
         }
@@ -422,8 +478,7 @@ __global__ void __launch_bounds__(TX *TY) stage_kernel(const StageParams<T> P) {
       P.uh[iu] = uh;
       P.vh[iv] = vh;
       P.wh[iw] = wh;
-      // the high boundary faces
-      if (i == nx - 1 && !P.px) {
+      if (i == nx - 1 && !P.px) {  // the outlet face (or the closed domain's wall)
         const size_t io = iu + 1;
         T uo;
         if (P.closed) {
@@ -431,23 +486,18 @@ __global__ void __launch_bounds__(TX *TY) stage_kernel(const StageParams<T> P) {
         } else {
           const T upo = VEL(0, 0, y, x + 1), upi = VEL(0, 0, y, x);
           const T lo = (upi - upo) * inv;
-          uo = (a == T(0) ? upo : lerp_t<T>(upo, P.u0[io], a)) + lo * bdt;
-          uo = uo + P.outlet_corr[0];
+          uo = (a == T(0) ? upo : lerp_t<T>(upo, __ldg(P.u0 + io), a)) + lo * bdt;
+          uo = uo + *P.outlet_corr;
         }
         P.uh[io] = uo;
       }
       if (j == ny - 1 && !P.py) P.vh[iv + nx] = T(0);
+      // the top w face is a boundary face (chi_w = vol_w = 0 there): zero normal velocity
       if (k == nz - 1 && !P.pz) P.wh[iw + (size_t)ny * nx] = T(0);
 
       // ================= theta stage (physics.py:647-708) ================================
-      if (P.thermal) {
-        const T kh = P.kh;
-        auto kface = [&](T n1, T n2, bool boundary) -> T {
-          if (!les || boundary) return kh;
-          return kh + P.kprt * (n1 + n2);
-        };
+      if (thermal) {
         const T c = TH(0, y, x);
-        // x faces i and i+1
         const T kxl = kface(NU(0, ny2, nx2 - 1), NU(0, ny2, nx2), !P.px && i == 0);
         const T kxr = kface(NU(0, ny2, nx2), NU(0, ny2, nx2 + 1), !P.px && i == nx - 1);
         T fxl = muscl_flux<T>(TH(0, y, x - 2), TH(0, y, x - 1), c, TH(0, y, x + 1), VEL(0, 0, y, x)) -
@@ -460,41 +510,27 @@ __global__ void __launch_bounds__(TX *TY) stage_kernel(const StageParams<T> P) {
                 kyl * (c - TH(0, y - 1, x));
         T fyr = muscl_flux<T>(TH(0, y - 1, x), c, TH(0, y + 1, x), TH(0, y + 2, x), VEL(1, 0, y + 1, x)) -
                 kyr * (TH(0, y + 1, x) - c);
-        const T kzl = kface(NU(-1, ny2, nx2), NU(0, ny2, nx2), !P.pz && k == 0);
-        const T kzr = kface(NU(0, ny2, nx2), NU(1, ny2, nx2), !P.pz && k == nz - 1);
-        T fzl = muscl_flux<T>(TH(-2, y, x), TH(-1, y, x), c, TH(1, y, x), VEL(2, 0, y, x)) - kzl * (c - TH(-1, y, x));
-        T fzr = muscl_flux<T>(TH(-1, y, x), c, TH(1, y, x), TH(2, y, x), VEL(2, 1, y, x)) - kzr * (TH(1, y, x) - c);
-        if (P.has_adia) {  // adiabatic bodies block conduction (physics.py:666-675)
-          const int k0 = P.win[0], k1 = P.win[1], wj0 = P.win[2], wj1 = P.win[3], wi0 = P.win[4], wi1 = P.win[5];
-          const int wzn = k1 - k0, wyn = wj1 - wj0, wxn = wi1 - wi0;
-          if (k >= k0 && k < k1 && j >= wj0 && j < wj1) {
+        if (P.has_adia && k >= wk0 && k < wk1) {  // adiabatic bodies block conduction (physics.py:666-675)
+          if (j >= wj0 && j < wj1) {
             if (i >= wi0 && i <= wi1)
-              fxl += kxl * P.adia_u[((size_t)(k - k0) * wyn + (j - wj0)) * (wxn + 1) + (i - wi0)] * (c - TH(0, y, x - 1));
+              fxl += kxl * P.adia_u[((size_t)(k - wk0) * wyn + (j - wj0)) * (wxn + 1) + (i - wi0)] * (c - TH(0, y, x - 1));
             if (i + 1 >= wi0 && i + 1 <= wi1)
-              fxr += kxr * P.adia_u[((size_t)(k - k0) * wyn + (j - wj0)) * (wxn + 1) + (i + 1 - wi0)] *
+              fxr += kxr * P.adia_u[((size_t)(k - wk0) * wyn + (j - wj0)) * (wxn + 1) + (i + 1 - wi0)] *
                      (TH(0, y, x + 1) - c);
           }
-          if (k >= k0 && k < k1 && i >= wi0 && i < wi1) {
+          if (i >= wi0 && i < wi1) {
             if (j >= wj0 && j <= wj1)
-              fyl += kyl * P.adia_v[((size_t)(k - k0) * (wyn + 1) + (j - wj0)) * wxn + (i - wi0)] * (c - TH(0, y - 1, x));
+              fyl += kyl * P.adia_v[((size_t)(k - wk0) * (wyn + 1) + (j - wj0)) * wxn + (i - wi0)] * (c - TH(0, y - 1, x));
             if (j + 1 >= wj0 && j + 1 <= wj1)
-              fyr += kyr * P.adia_v[((size_t)(k - k0) * (wyn + 1) + (j + 1 - wj0)) * wxn + (i - wi0)] *
+              fyr += kyr * P.adia_v[((size_t)(k - wk0) * (wyn + 1) + (j + 1 - wj0)) * wxn + (i - wi0)] *
                      (TH(0, y + 1, x) - c);
           }
-          if (j >= wj0 && j < wj1 && i >= wi0 && i < wi1) {
-            if (k >= k0 && k <= k1)
-              fzl += kzl * P.adia_w[((size_t)(k - k0) * wyn + (j - wj0)) * wxn + (i - wi0)] * (c - TH(-1, y, x));
-            if (k + 1 >= k0 && k + 1 <= k1)
-              fzr += kzr * P.adia_w[((size_t)(k + 1 - k0) * wyn + (j - wj0)) * wxn + (i - wi0)] * (TH(1, y, x) - c);
-          }
-          (void)wzn;
         }
-        const T D = ((fxr - fxl) + (fyr - fyl) + (fzr - fzl)) * inv;
+        const T D = ((fxr - fxl) + (fyr - fyl) + (zth - zth_l)) * inv;
         const size_t ic = ((size_t)k * ny + j) * nx + i;
-        T ch = (a == T(0) ? c : lerp_t<T>(c, P.th0[ic], a)) - bdt * D;
-        const int k0 = P.win[0], k1 = P.win[1], wj0 = P.win[2], wj1 = P.win[3], wi0 = P.win[4], wi1 = P.win[5];
-        if (P.has_win && k >= k0 && k < k1 && j >= wj0 && j < wj1 && i >= wi0 && i < wi1) {
-          wt = ((size_t)(k - k0) * (wj1 - wj0) + (j - wj0)) * (wi1 - wi0) + (i - wi0);
+        T ch = (a == T(0) ? c : lerp_t<T>(c, __ldg(P.th0 + ic), a)) - bdt * D;
+        if (P.has_win && k >= wk0 && k < wk1 && j >= wj0 && j < wj1 && i >= wi0 && i < wi1) {
+          wt = ((size_t)(k - wk0) * wyn + (j - wj0)) * wxn + (i - wi0);
           if (P.skin) ch = ch + (bdt * P.kappa) * P.skin[wt];
           if (P.chi_t) {
             const T kt = bdt / P.eta_t;
@@ -512,10 +548,10 @@ __global__ void __launch_bounds__(TX *TY) stage_kernel(const StageParams<T> P) {
     if (P.has_win) {
       const unsigned any = __ballot_sync(0xffffffffu, fu_in | fv_in | fw_in | ft_in);
       if (any) {
-        const size_t wsz_u = (size_t)(P.win[1] - P.win[0]) * (P.win[3] - P.win[2]) * (P.win[5] - P.win[4] + 1);
-        const size_t wsz_v = (size_t)(P.win[1] - P.win[0]) * (P.win[3] - P.win[2] + 1) * (P.win[5] - P.win[4]);
-        const size_t wsz_w = (size_t)(P.win[1] - P.win[0] + 1) * (P.win[3] - P.win[2]) * (P.win[5] - P.win[4]);
-        const size_t wsz_c = (size_t)(P.win[1] - P.win[0]) * (P.win[3] - P.win[2]) * (P.win[5] - P.win[4]);
+        const size_t wsz_u = (size_t)wzn * wyn * (wxn + 1);
+        const size_t wsz_v = (size_t)wzn * (wyn + 1) * wxn;
+        const size_t wsz_w = (size_t)(wzn + 1) * wyn * wxn;
+        const size_t wsz_c = (size_t)wzn * wyn * wxn;
         for (int b = 0; b < P.nbody; ++b) {
           for (int c3 = 0; c3 < 3; ++c3) {
             double xu = fu_in ? cu * (double)P.k_u[((size_t)b * 3 + c3) * wsz_u + wu] : 0.0;
@@ -538,24 +574,18 @@ __global__ void __launch_bounds__(TX *TY) stage_kernel(const StageParams<T> P) {
         }
       }
     }
+    if (pre) {
+      if (P.use_tma) {
+        await_plane(k + 3);
+        fill(k + 3, false);
+      } else {
+        fill(k + 3, true);
+      }
+    }
+    __syncthreads();
   }
 
-  if (les) {
-    // block max of nu_t, then one atomic per block
-    T m = nut_local_max;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    __syncthreads();
-    __shared__ double wmax[TX * TY / 32];
-    if (lane == 0) wmax[warp] = (double)m;
-    __syncthreads();
-    if (tid == 0 && P.nut_max) {
-      double mm = 0.0;
-      for (int w = 0; w < TX * TY / 32; ++w) mm = fmax(mm, wmax[w]);
-      atomic_max_nonneg(P.nut_max, mm);
-    }
-  }
-  if (!nut_only && P.has_win && P.partials) {
+  if (P.has_win && P.partials) {
     __syncthreads();
     const size_t blk = ((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
     for (int q = tid; q < nq; q += TX * TY) {
@@ -567,344 +597,6 @@ __global__ void __launch_bounds__(TX *TY) stage_kernel(const StageParams<T> P) {
 #undef VEL
 #undef TH
 #undef NU
-}
-
-// --------------------------------------------------------------------------------------
-// pre-pass maxima, time step, outlet sums
-// --------------------------------------------------------------------------------------
-
-template <typename T>
-__global__ void absmax_kernel(const T *__restrict__ a, size_t n, unsigned long long *out) {
-  T m = T(0);
-  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
-    const T v = fabs(a[e]);
-    m = (v > m || v != v) ? v : m;
-  }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    const T other = __shfl_xor_sync(0xffffffffu, m, o);
-    m = (other > m || other != other) ? other : m;
-  }
-  if ((threadIdx.x & 31) == 0) atomic_max_nonneg(out, (double)m);
-}
-
-// One thread: the step's dt from the maxima (core.py:637-646, physics.py:723-742, 1230-1262),
-// rounded through the field type as the reference computes it.
-template <typename T>
-__global__ void dt_kernel(const DtParams P) {
-  const double *sc = P.scalars;
-  const unsigned long long *bits = reinterpret_cast<const unsigned long long *>(sc);
-  T dt;
-  if (P.dt_in) {
-    dt = *reinterpret_cast<const T *>(P.dt_in);
-  } else if (P.has_dt_fixed) {
-    dt = T(P.dt_fixed);
-  } else {
-    const T mu = T(as_double(bits[SC_MAXU])), mv = T(as_double(bits[SC_MAXV])), mw = T(as_double(bits[SC_MAXW]));
-    T umax = (mu + mv) + mw;
-    umax = umax > T(1e-6) ? umax : T(1e-6);
-    if (umax != umax) umax = mu + mv + mw;  // keep NaN
-    dt = T(P.cfl * P.h) / umax;
-    const bool les = P.les != 0;
-    const T nut_max = T(as_double(bits[SC_NUTMAX]));
-    const T nu = les ? T(P.nu) + nut_max : T(P.nu);
-    const T dv = T(P.viscous_dt * P.h * P.h) / nu;
-    dt = dv < dt ? dv : dt;
-    if (P.thermal) {
-      const T kap = les ? T(P.kappa) + nut_max / T(P.prt) : T(P.kappa);
-      const T diff_rate = kap / T(P.viscous_dt * P.h * P.h);
-      const T lim = T(1) / (umax * T(1.0 / (0.5 * P.h)) + diff_rate);
-      dt = lim < dt ? lim : dt;
-      if (P.ri != 0.0) {
-        T acc = T(fabs(P.ri)) * T(as_double(bits[SC_MAXT]));
-        acc = acc > T(1e-12) ? acc : T(1e-12);
-        const T f = T(P.cfl) * sqrt(T(P.h) / acc);
-        dt = f < dt ? f : dt;
-      }
-      if (P.has_heat_max) {
-        T s = T(P.heat_max);
-        s = s > T(1e-12) ? s : T(1e-12);
-        const T l1 = T(1) / s;
-        dt = l1 < dt ? l1 : dt;
-        if (P.ri != 0.0) {
-          const T l2 = pow(T(6.0 * P.cfl * P.h) / (T(fabs(P.ri)) * s), T(1.0 / 3.0));
-          dt = l2 < dt ? l2 : dt;
-        }
-      }
-    }
-  }
-  *reinterpret_cast<T *>(P.dt_out) = dt;
-  P.scalars[SC_DT] = (double)dt;
-  if (!(dt == dt) || !(dt > T(0)) || isinf((double)dt)) atomicOr(P.status, 1);
-}
-
-// Outlet-plane sums in a fixed order (deterministic): one block of 1024 threads.
-// sums[0] = sum u[..., nx], sums[1] = sum u[..., nx-1] (and sums[2] = sum u0[..., nx] when
-// u0 is given).  The stage blends them into the outlet correction by linearity.
-template <typename T>
-__global__ void outlet_sum_kernel(const T *__restrict__ u, const T *__restrict__ u0, int nx, int rows,
-                                  double *sums) {
-  __shared__ double red[3][32];
-  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-  for (int r = threadIdx.x; r < rows; r += blockDim.x) {
-    const size_t base = (size_t)r * (nx + 1);
-    s0 += (double)u[base + nx];
-    s1 += (double)u[base + nx - 1];
-    if (u0) s2 += (double)u0[base + nx];
-  }
-  s0 = warp_sum(s0);
-  s1 = warp_sum(s1);
-  s2 = warp_sum(s2);
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  if (lane == 0) {
-    red[0][w] = s0;
-    red[1][w] = s1;
-    red[2][w] = s2;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double a = 0.0, b = 0.0, c = 0.0;
-    for (int q = 0; q < (int)(blockDim.x >> 5); ++q) {
-      a += red[0][q];
-      b += red[1][q];
-      c += red[2][q];
-    }
-    sums[0] = a;
-    sums[1] = b;
-    if (u0) sums[2] = c;
-  }
-}
-
-// corr = (sum u_inlet - sum uh[..., nx]) / (ny nz) with sum uh[..., nx] blended from the
-// stage-start sums: sum lerp(up, u0, a) + b dt / h (sum up[nx-1] - sum up[nx]).
-template <typename T>
-__global__ void outlet_corr_kernel(const double *sums_p, const double *sum_u0, const double *sum_inlet, const T *dt,
-                                   double a, double bscale, double inv_h, double inv_rows, T *corr) {
-  const double bdt = (double)(T(bscale) * *dt);
-  const double so = sums_p[0], si = sums_p[1], s0 = *sum_u0;
-  const double out = (1.0 - a) * so + a * s0 + bdt * inv_h * (si - so);
-  *corr = T((*sum_inlet - out) * inv_rows);
-}
-
-// --------------------------------------------------------------------------------------
-// projection: divergence and gradient correction (core.py:577-601)
-// --------------------------------------------------------------------------------------
-
-template <typename T>
-__global__ void divergence_kernel(const T *__restrict__ u, const T *__restrict__ v, const T *__restrict__ w, int nx,
-                                  int ny, int nz, int px, int py, int pz, T inv_h, T *__restrict__ div) {
-  const size_t n = (size_t)nx * ny * nz;
-  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
-    const int i = (int)(e % nx);
-    const size_t r = e / nx;
-    const int j = (int)(r % ny), k = (int)(r / ny);
-    const T ur = (px && i == nx - 1) ? u[((size_t)k * ny + j) * (nx + 1)] : u[((size_t)k * ny + j) * (nx + 1) + i + 1];
-    const T ul = u[((size_t)k * ny + j) * (nx + 1) + i];
-    const T vr = (py && j == ny - 1) ? v[((size_t)k * (ny + 1)) * nx + i] : v[((size_t)k * (ny + 1) + j + 1) * nx + i];
-    const T vl = v[((size_t)k * (ny + 1) + j) * nx + i];
-    const T wr = (pz && k == nz - 1) ? w[(size_t)j * nx + i] : w[((size_t)(k + 1) * ny + j) * nx + i];
-    const T wl = w[((size_t)k * ny + j) * nx + i];
-    div[e] = ((ur - ul) + (vr - vl) + (wr - wl)) * inv_h;
-  }
-}
-
-// u <- uh - grad psi on every face; boundary-normal faces keep uh (non-periodic), periodic
-// duplicate faces equal face 0.
-template <typename T>
-__global__ void correct_kernel(const CorrectParams<T> P) {
-  const int nx = P.nx, ny = P.ny, nz = P.nz;
-  const size_t nu = (size_t)nz * ny * (nx + 1), nv = (size_t)nz * (ny + 1) * nx, nw = (size_t)(nz + 1) * ny * nx;
-  const T inv = P.inv_h;
-  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < nu + nv + nw; e += (size_t)gridDim.x * blockDim.x) {
-    if (e < nu) {
-      int i = (int)(e % (nx + 1));
-      const size_t r = e / (nx + 1);
-      const int j = (int)(r % ny), k = (int)(r / ny);
-      T val;
-      if (P.px) {
-        const int ii = (i == nx) ? 0 : i;
-        const int il = (ii == 0) ? nx - 1 : ii - 1;
-        const size_t c = ((size_t)k * ny + j) * nx;
-        val = P.uh[((size_t)k * ny + j) * (nx + 1) + ii] - (P.psi[c + ii] - P.psi[c + il]) * inv;
-      } else if (i == 0 || i == nx) {
-        val = P.uh[e];
-      } else {
-        const size_t c = ((size_t)k * ny + j) * nx + i;
-        val = P.uh[e] - (P.psi[c] - P.psi[c - 1]) * inv;
-      }
-      P.u[e] = val;
-    } else if (e < nu + nv) {
-      const size_t f = e - nu;
-      const int i = (int)(f % nx);
-      const size_t r = f / nx;
-      int j = (int)(r % (ny + 1));
-      const int k = (int)(r / (ny + 1));
-      T val;
-      if (P.py) {
-        const int jj = (j == ny) ? 0 : j;
-        const int jl = (jj == 0) ? ny - 1 : jj - 1;
-        val = P.vh[((size_t)k * (ny + 1) + jj) * nx + i] -
-              (P.psi[((size_t)k * ny + jj) * nx + i] - P.psi[((size_t)k * ny + jl) * nx + i]) * inv;
-      } else if (j == 0 || j == ny) {
-        val = P.vh[f];
-      } else {
-        val = P.vh[f] - (P.psi[((size_t)k * ny + j) * nx + i] - P.psi[((size_t)k * ny + j - 1) * nx + i]) * inv;
-      }
-      P.v[f] = val;
-    } else {
-      const size_t f = e - nu - nv;
-      const int i = (int)(f % nx);
-      const size_t r = f / nx;
-      const int j = (int)(r % ny);
-      int k = (int)(r / ny);
-      T val;
-      if (P.pz) {
-        const int kk = (k == nz) ? 0 : k;
-        const int kl = (kk == 0) ? nz - 1 : kk - 1;
-        val = P.wh[((size_t)kk * ny + j) * nx + i] -
-              (P.psi[((size_t)kk * ny + j) * nx + i] - P.psi[((size_t)kl * ny + j) * nx + i]) * inv;
-      } else if (k == 0 || k == nz) {
-        val = P.wh[f];
-      } else {
-        val = P.wh[f] - (P.psi[((size_t)k * ny + j) * nx + i] - P.psi[((size_t)(k - 1) * ny + j) * nx + i]) * inv;
-      }
-      P.w[f] = val;
-    }
-  }
-}
-
-// --------------------------------------------------------------------------------------
-// smoke: MUSCL forward Euler, clip and floor, solids and nozzles (dye.py:232-312)
-// --------------------------------------------------------------------------------------
-
-template <typename T>
-__device__ __forceinline__ T dye_at(const T *__restrict__ c, int nz, int ny, int nx, int px, int py, int pz, int k,
-                                    int j, int i) {
-  // pad_dye ghosts (dye.py:232-263): inlet zeros, outlet zero-gradient, mirrored y / z
-  if (i < 0) {
-    if (!px) return T(0);
-    i += nx;
-  } else if (i >= nx) {
-    i = px ? i - nx : nx - 1;
-  }
-  if (j < 0) j = py ? j + ny : -1 - j;
-  else if (j >= ny) j = py ? j - ny : 2 * ny - 1 - j;
-  if (k < 0) k = pz ? k + nz : -1 - k;
-  else if (k >= nz) k = pz ? k - nz : 2 * nz - 1 - k;
-  return __ldg(c + ((size_t)k * ny + j) * nx + i);
-}
-
-template <typename T>
-__global__ void smoke_kernel(const SmokeParams<T> P) {
-  const int nx = P.nx, ny = P.ny, nz = P.nz;
-  const size_t n = (size_t)nx * ny * nz;
-  const T dt = *P.dt;
-  const T kk = dt * P.inv_h;
-  const T t = P.t_new ? *P.t_new : *P.t0 + dt;
-  const T on = (fmod(t, T(P.pulse_period)) < T(P.pulse_on)) ? T(1) : T(0);
-  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
-    const int i = (int)(e % nx);
-    const size_t r = e / nx;
-    const int j = (int)(r % ny), k = (int)(r / ny);
-    auto C = [&](int dk, int dj, int di) { return dye_at<T>(P.c0, nz, ny, nx, P.px, P.py, P.pz, k + dk, j + dj, i + di); };
-    const T c = C(0, 0, 0);
-    const T fx0 = muscl_flux<T>(C(0, 0, -2), C(0, 0, -1), c, C(0, 0, 1), P.u[((size_t)k * ny + j) * (nx + 1) + i]);
-    const T fx1 = muscl_flux<T>(C(0, 0, -1), c, C(0, 0, 1), C(0, 0, 2), P.u[((size_t)k * ny + j) * (nx + 1) + i + 1]);
-    const T fy0 = muscl_flux<T>(C(0, -2, 0), C(0, -1, 0), c, C(0, 1, 0), P.v[((size_t)k * (ny + 1) + j) * nx + i]);
-    const T fy1 = muscl_flux<T>(C(0, -1, 0), c, C(0, 1, 0), C(0, 2, 0), P.v[((size_t)k * (ny + 1) + j + 1) * nx + i]);
-    const T fz0 = muscl_flux<T>(C(-2, 0, 0), C(-1, 0, 0), c, C(1, 0, 0), P.w[((size_t)k * ny + j) * nx + i]);
-    const T fz1 = muscl_flux<T>(C(-1, 0, 0), c, C(1, 0, 0), C(2, 0, 0), P.w[((size_t)(k + 1) * ny + j) * nx + i]);
-    T v = c - kk * (((fx1 - fx0) + (fy1 - fy0)) + (fz1 - fz0));
-    v = v > T(1) ? T(1) : v;
-    v = v < T(1e-8) ? T(0) : v;
-    if (P.chi_c && k >= P.win[0] && k < P.win[1] && j >= P.win[2] && j < P.win[3] && i >= P.win[4] && i < P.win[5]) {
-      const T chi = P.chi_c[((size_t)(k - P.win[0]) * (P.win[3] - P.win[2]) + (j - P.win[2])) * (P.win[5] - P.win[4]) +
-                            (i - P.win[4])];
-      if (chi > T(0.5)) v = T(0);
-    }
-    if (P.weight && k >= P.dwin[0] && k < P.dwin[1] && j >= P.dwin[2] && j < P.dwin[3] && i >= P.dwin[4] &&
-        i < P.dwin[5]) {
-      const T wgt = P.weight[((size_t)(k - P.dwin[0]) * (P.dwin[3] - P.dwin[2]) + (j - P.dwin[2])) * (P.dwin[5] - P.dwin[4]) +
-                             (i - P.dwin[4])];
-      v = v + wgt * on * (T(1) - v);
-    }
-    P.c[e] = v;
-  }
-}
-
-// --------------------------------------------------------------------------------------
-// end of step: p, coefficients, heat rates, t and dt (core.py:653-678, 875-883,
-// physics.py:713-721)
-// --------------------------------------------------------------------------------------
-
-template <typename T>
-__global__ void finalize_kernel(const FinalizeParams<T> P) {
-  __shared__ double tot[AERO_MAX_BODIES * 10];
-  const T dt = *P.dt;
-  if (threadIdx.x == 0 && blockIdx.x == 0) {
-    *P.t_out = *P.t0 + dt;
-    *P.dt_out = dt;
-  }
-  if (blockIdx.x == 0) {
-    for (int q = threadIdx.x; q < P.nq; q += blockDim.x) {
-      double s = 0.0;
-      for (int st = 0; st < 3; ++st)
-        for (int b = 0; b < P.nblocks; ++b) s += P.partials[((size_t)st * P.nblocks + b) * P.nq + q];
-      tot[q] = s;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      const double ddt = (double)dt;
-      int bad = 0;
-      for (int b = 0; b < P.nbody; ++b) {
-        const double scale = -(P.h * P.h * P.h) / ddt;
-        const double *r = tot + b * 9;
-        double fx = r[0] * scale, fy = r[3] * scale, fz = r[6] * scale;
-        double mx = r[4] * scale + r[7] * scale, my = r[1] * scale + r[8] * scale, mz = r[2] * scale + r[5] * scale;
-        if (P.symmetry) {
-          const double dy = P.moment_ref_y - P.y0;
-          fx *= 2.0;
-          fz *= 2.0;
-          my *= 2.0;
-          fy = 0.0;
-          mx = -dy * fz;
-          mz = dy * fx;
-        }
-        const double qa = 0.5 * P.ref_area;
-        const double c6[6] = {fx / qa, fy / qa, fz / qa, mx / (qa * P.span_ref), my / (qa * P.length_ref),
-                              mz / (qa * P.span_ref)};
-        for (int c = 0; c < 6; ++c) {
-          P.coeffs[b * 6 + c] = T(c6[c]);
-          if (!(c6[c] == c6[c])) bad = 1;
-        }
-      }
-      if (P.heat_rate) {
-        const double sym = P.symmetry ? 2.0 : 1.0;
-        const double scale = sym * P.h * P.h * P.h * P.pe / (double)dt;
-        for (int b = 0; b < P.nbody; ++b) {
-          double q = 0.0;
-          for (int t = 0; t < P.n_tbody; ++t)
-            if (P.t_index[t] == b) q += tot[P.nbody * 9 + t];
-          q = q * scale + P.flux_rate[b] * sym;
-          P.heat_rate[b] = T(q);
-          if (!(q == q)) bad = 1;
-        }
-      }
-      if (bad) atomicOr(P.status, 1);
-    }
-  }
-  // p = psi_w / dt over the whole field
-  const size_t n = P.ncell;
-  const T rdt = T(1) / dt;
-  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
-    P.p[e] = P.p[e] * rdt;
-}
-
-// psi_w (in p) <- psi * wgt (first stage) or psi_w + wgt * psi
-template <typename T>
-__global__ void psi_accumulate_kernel(const T *__restrict__ psi, T *__restrict__ pw, size_t n, T wgt, int first) {
-  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
-    pw[e] = first ? psi[e] * wgt : pw[e] + wgt * psi[e];
 }
 
 // --------------------------------------------------------------------------------------
@@ -931,81 +623,17 @@ cudaError_t launch_stage(const StageParams<T> &P, cudaStream_t s) {
 }
 
 template <typename T>
-cudaError_t launch_absmax(const T *a, size_t n, unsigned long long *out, cudaStream_t s) {
-  int blocks = (int)std::min<size_t>((n + 255) / 256, 148 * 8);
-  absmax_kernel<T><<<blocks, 256, 0, s>>>(a, n, out);
+cudaError_t launch_nu(const NuParams<T> &P, cudaStream_t s) {
+  dim3 grid((P.nx + 2 + TX - 1) / TX, (P.ny + 2 + TY - 1) / TY, (P.nz + 2 + P.zc - 1) / P.zc);
+  nu_kernel<T><<<grid, dim3(TX, TY), 0, s>>>(P);
   return cudaGetLastError();
 }
 
-template <typename T>
-cudaError_t launch_dt(const DtParams &P, cudaStream_t s) {
-  dt_kernel<T><<<1, 1, 0, s>>>(P);
-  return cudaGetLastError();
-}
-
-template <typename T>
-cudaError_t launch_outlet_sum(const T *u, const T *u0, int nx, int rows, double *sums, cudaStream_t s) {
-  outlet_sum_kernel<T><<<1, 1024, 0, s>>>(u, u0, nx, rows, sums);
-  return cudaGetLastError();
-}
-
-template <typename T>
-cudaError_t launch_outlet_corr(const double *sums_p, const double *sum_u0, const double *sum_inlet, const T *dt,
-                               double a, double b, double inv_h, double inv_rows, T *corr, cudaStream_t s) {
-  outlet_corr_kernel<T><<<1, 1, 0, s>>>(sums_p, sum_u0, sum_inlet, dt, a, b, inv_h, inv_rows, corr);
-  return cudaGetLastError();
-}
-
-static inline int grid_for(size_t n) { return (int)std::max<size_t>(1, std::min<size_t>((n + 255) / 256, 148 * 16)); }
-
-template <typename T>
-cudaError_t launch_divergence(const T *u, const T *v, const T *w, int nx, int ny, int nz, int px, int py, int pz,
-                              T inv_h, T *div, cudaStream_t s) {
-  divergence_kernel<T><<<grid_for((size_t)nx * ny * nz), 256, 0, s>>>(u, v, w, nx, ny, nz, px, py, pz, inv_h, div);
-  return cudaGetLastError();
-}
-
-template <typename T>
-cudaError_t launch_correct(const CorrectParams<T> &P, cudaStream_t s) {
-  const size_t n = (size_t)P.nz * P.ny * (P.nx + 1) * 3 + (size_t)P.nx * P.ny;
-  correct_kernel<T><<<grid_for(n), 256, 0, s>>>(P);
-  return cudaGetLastError();
-}
-
-template <typename T>
-cudaError_t launch_smoke(const SmokeParams<T> &P, cudaStream_t s) {
-  smoke_kernel<T><<<grid_for((size_t)P.nx * P.ny * P.nz), 256, 0, s>>>(P);
-  return cudaGetLastError();
-}
-
-template <typename T>
-cudaError_t launch_finalize(const FinalizeParams<T> &P, cudaStream_t s) {
-  finalize_kernel<T><<<grid_for(P.ncell), 256, 0, s>>>(P);
-  return cudaGetLastError();
-}
-
-template <typename T>
-cudaError_t launch_psi_accumulate(const T *psi, T *pw, size_t n, T wgt, int first, cudaStream_t s) {
-  psi_accumulate_kernel<T><<<grid_for(n), 256, 0, s>>>(psi, pw, n, wgt, first);
-  return cudaGetLastError();
-}
-
-#define INSTANTIATE(T)                                                                                               \
-  template size_t stage_smem_bytes<T>();                                                                             \
-  template cudaError_t launch_stage<T>(const StageParams<T> &, cudaStream_t);                                       \
-  template cudaError_t launch_absmax<T>(const T *, size_t, unsigned long long *, cudaStream_t);                     \
-  template cudaError_t launch_dt<T>(const DtParams &, cudaStream_t);                                                \
-  template cudaError_t launch_outlet_sum<T>(const T *, const T *, int, int, double *, cudaStream_t);                 \
-  template cudaError_t launch_outlet_corr<T>(const double *, const double *, const double *, const T *, double,      \
-                                             double, double, double, T *, cudaStream_t);                             \
-  template cudaError_t launch_divergence<T>(const T *, const T *, const T *, int, int, int, int, int, int, T, T *,    \
-                                            cudaStream_t);                                                           \
-  template cudaError_t launch_correct<T>(const CorrectParams<T> &, cudaStream_t);                                   \
-  template cudaError_t launch_smoke<T>(const SmokeParams<T> &, cudaStream_t);                                       \
-  template cudaError_t launch_finalize<T>(const FinalizeParams<T> &, cudaStream_t);                                 \
-  template cudaError_t launch_psi_accumulate<T>(const T *, T *, size_t, T, int, cudaStream_t);
-
-INSTANTIATE(float)
-INSTANTIATE(double)
+template size_t stage_smem_bytes<float>();
+template size_t stage_smem_bytes<double>();
+template cudaError_t launch_stage<float>(const StageParams<float> &, cudaStream_t);
+template cudaError_t launch_stage<double>(const StageParams<double> &, cudaStream_t);
+template cudaError_t launch_nu<float>(const NuParams<float> &, cudaStream_t);
+template cudaError_t launch_nu<double>(const NuParams<double> &, cudaStream_t);
 
 }  // namespace aero

@@ -95,7 +95,7 @@ class Clocks:
         if not sm:
             return None
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if len(r) > 3 + i and "Active" in r[3 + i]})
+        reasons = sorted({names[i] for r in rows for i in range(4) if len(r) > 3 + i and r[3 + i].strip() == "Active"})
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(rows[0][1]), "reasons": reasons,
                 "samples": len(sm)}
 
@@ -154,13 +154,14 @@ def launches_per_step(plan):
     """Kernels one aero_ns3d_step launches (the sequence in csrc/capi.cu)."""
     c = plan.cfg
     tunnel = not c.periodic[0] and not c.closed
+    les = c.les != 0
     n = 3 + (1 if c.thermal else 0)                # |u|, |v|, |w|, |theta| maxima
-    n += 1 if c.les else 0                          # eddy-viscosity pre-pass
     n += 1                                          # dt
     n += 1 if tunnel else 0                         # inlet / u0 outlet sums
-    per_stage = 1 + 1 + 5 + 1 + 1 + (2 if tunnel else 0)   # stage, divergence, 5 transforms, psi_w, correction
-    n += 3 * per_stage
+    per_stage = 1 + 1 + 5 + 1 + 1 + (2 if tunnel else 0) + (1 if les else 0)
+    n += 3 * per_stage                              # [nu], [sums, corr], stage, div, 5 transforms, psi_w, correct
     n += 1 if c.smoke else 0
+    n += 1 if (c.nbody * 9 + (c.n_tbody if c.thermal else 0)) > 0 else 0   # partial-sum reduction
     n += 1                                          # finalize
     return n
 
