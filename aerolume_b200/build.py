@@ -16,6 +16,7 @@ PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 INCLUDE = PKG.parent / "include"
 LIB = PKG / "libaero_b200.so"
+LIB_CHECKED = PKG / "libaero_b200_checked.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC,-O3",
          "-Xptxas", "-O3"]
@@ -32,38 +33,44 @@ def sources() -> list[Path]:
     return sorted(CSRC.glob("*.cu"))
 
 
-def stale() -> bool:
-    if not LIB.exists():
+def stale(lib: Path = LIB) -> bool:
+    if not lib.exists():
         return True
-    t = LIB.stat().st_mtime
+    t = lib.stat().st_mtime
     deps = sources() + sorted(CSRC.glob("*.cuh")) + sorted(INCLUDE.glob("*.h")) + [Path(__file__)]
     return any(p.stat().st_mtime > t for p in deps)
 
 
-def build(force: bool = False, verbose: bool = False) -> Path:
-    if not force and not stale():
-        return LIB
-    build_dir = PKG / "_build"
+def build(force: bool = False, verbose: bool = False, checked: bool = False) -> Path:
+    """Compile the release library, or with ``checked`` the bounds-checked one
+    (AERO_BOUNDS_CHECK: every instrumented index is checked on the device)."""
+    lib = LIB_CHECKED if checked else LIB
+    if not force and not stale(lib):
+        return lib
+    build_dir = PKG / ("_build_checked" if checked else "_build")
     build_dir.mkdir(exist_ok=True)
     objs = []
     cc = nvcc()
     for src in sources():
         obj = build_dir / (src.stem + ".o")
         cmd = [cc, *ARCH, *FLAGS, "-I", str(INCLUDE), "-dc", "-c", str(src), "-o", str(obj)]
+        if checked:
+            cmd.append("-DAERO_BOUNDS_CHECK=1")
         if verbose:
             cmd += ["-Xptxas", "-v"]
         subprocess.run(cmd, check=True)
         objs.append(str(obj))
-    tmp = LIB.with_suffix(".so.tmp")
+    tmp = lib.with_suffix(".so.tmp")
     subprocess.run([cc, *ARCH, "-shared", "-Xcompiler", "-fPIC", *objs, "-o", str(tmp), "-lcudart"], check=True)
-    os.replace(tmp, LIB)
-    return LIB
+    os.replace(tmp, lib)
+    return lib
 
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--force", action="store_true")
     ap.add_argument("-v", "--verbose", action="store_true", help="print ptxas register / spill reports")
+    ap.add_argument("--checked", action="store_true", help="build libaero_b200_checked.so (device bounds checks)")
     a = ap.parse_args()
-    print(build(force=a.force, verbose=a.verbose))
+    print(build(force=a.force, verbose=a.verbose, checked=a.checked))
     sys.exit(0)

@@ -8,6 +8,12 @@
 
 #include "ns3d.cuh"
 
+#ifdef AERO_BOUNDS_CHECK
+namespace aero {
+__device__ long long aero_check_word[4];
+}
+#endif
+
 namespace {
 
 thread_local std::string g_last_error;
@@ -734,6 +740,20 @@ int aero_ns3d_project(const AeroNs3dPlan *plan, void *u, void *v, void *w, void 
   auto ws = static_cast<unsigned char *>(workspace);
   return plan->cfg.dtype == AERO_F64 ? project_impl<double>(plan, u, v, w, psi, ws, s)
                                      : project_impl<float>(plan, u, v, w, psi, ws, s);
+}
+
+int aero_debug_check(int64_t *out4) {
+#ifdef AERO_BOUNDS_CHECK
+  long long w[4];
+  CUDA_TRY(cudaMemcpyFromSymbol(w, aero::aero_check_word, sizeof(w)));
+  for (int q = 0; q < 4; ++q) out4[q] = w[q];
+  const long long zero[4] = {0, 0, 0, 0};
+  CUDA_TRY(cudaMemcpyToSymbol(aero::aero_check_word, zero, sizeof(zero)));
+  return AERO_OK;
+#else
+  (void)out4;
+  return fail(AERO_EUNSUPPORTED, "bounds checks are compiled only into libaero_b200_checked.so");
+#endif
 }
 
 int aero_ns3d_read_status(const AeroNs3dPlan *plan, const void *workspace, int32_t *status, void *stream) {

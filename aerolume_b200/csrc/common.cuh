@@ -8,6 +8,26 @@
 
 namespace aero {
 
+// Bounds checks of the checked build (-DAERO_BOUNDS_CHECK, libaero_b200_checked.so): a failed
+// check records (code, index, bound) once in aero_check_word and the access is skipped.  In the
+// release build every check is `true` and compiles away.
+#ifdef AERO_BOUNDS_CHECK
+extern __device__ long long aero_check_word[4];
+__device__ __forceinline__ bool aero_check(bool ok, int code, long long idx, long long bound) {
+  if (ok) return true;
+  if (atomicCAS(reinterpret_cast<unsigned long long *>(&aero_check_word[0]), 0ull, (unsigned long long)code) == 0ull) {
+    aero_check_word[1] = idx;
+    aero_check_word[2] = bound;
+    aero_check_word[3] = ((long long)blockIdx.x << 32) | threadIdx.x;
+  }
+  return false;
+}
+#define AERO_IN(idx, bound, code) \
+  aero::aero_check((long long)(idx) >= 0 && (long long)(idx) < (long long)(bound), (code), (long long)(idx), (long long)(bound))
+#else
+#define AERO_IN(idx, bound, code) true
+#endif
+
 // Ghost-cell rules of Aerolume ns3d/core.py:147-246 as index maps.  A ghost entry g
 // (g < 0 or g >= n along an axis of n entries) takes the value s * x[map(g)] + c.
 // Rules of the three axes compose in the order x, then y, then z (core.py:249-272):
@@ -128,6 +148,26 @@ __device__ __forceinline__ T warp_sum(T v) {
 // which the status check then reports).
 __device__ __forceinline__ void atomic_max_nonneg(unsigned long long *addr, double v) {
   atomicMax(addr, (unsigned long long)__double_as_longlong(v));
+}
+
+// Block-wide max of a non-negative value (NaN wins), then one atomic for the block.
+template <typename T>
+__device__ __forceinline__ void block_max_atomic(T m, unsigned long long *out) {
+  __shared__ double red[32];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const T other = __shfl_xor_sync(0xffffffffu, m, o);
+    m = (other > m || other != other) ? other : m;
+  }
+  const int nw = (blockDim.x * blockDim.y * blockDim.z + 31) >> 5;
+  const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  if ((tid & 31) == 0) red[tid >> 5] = (double)m;
+  __syncthreads();
+  if (tid == 0) {
+    double r = 0.0;
+    for (int w = 0; w < nw; ++w) r = (red[w] > r || red[w] != red[w]) ? red[w] : r;
+    atomic_max_nonneg(out, r);
+  }
 }
 
 __device__ __forceinline__ double as_double(unsigned long long bits) { return __longlong_as_double((long long)bits); }

@@ -12,6 +12,7 @@ namespace aero {
 // pre-pass maxima, time step, outlet sums
 // --------------------------------------------------------------------------------------
 
+// max |a| over an array: warp shuffles, then one atomic per block
 template <typename T>
 __global__ void absmax_kernel(const T *__restrict__ a, size_t n, unsigned long long *out) {
   T m = T(0);
@@ -19,12 +20,7 @@ __global__ void absmax_kernel(const T *__restrict__ a, size_t n, unsigned long l
     const T v = fabs(a[e]);
     m = (v > m || v != v) ? v : m;
   }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    const T other = __shfl_xor_sync(0xffffffffu, m, o);
-    m = (other > m || other != other) ? other : m;
-  }
-  if ((threadIdx.x & 31) == 0) atomic_max_nonneg(out, (double)m);
+  block_max_atomic<T>(m, out);
 }
 
 // u0 (rows of nx + 1) into the stage-start buffer with a 16-byte row pitch, with max |u0|
@@ -35,17 +31,11 @@ __global__ void copy_u_kernel(const T *__restrict__ u, T *__restrict__ out, int 
   T m = T(0);
   if (i <= nx) {
     const T v = u[((size_t)k * ny + j) * (nx + 1) + i];
-    out[((size_t)k * ny + j) * pitch + i] = v;
+    if (AERO_IN(((size_t)k * ny + j) * pitch + i, (long long)gridDim.z * ny * pitch, 201))
+      out[((size_t)k * ny + j) * pitch + i] = v;
     m = fabs(v);
   }
-  if (mx) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const T other = __shfl_xor_sync(0xffffffffu, m, o);
-      m = (other > m || other != other) ? other : m;
-    }
-    if ((threadIdx.x & 31) == 0) atomic_max_nonneg(mx, (double)m);
-  }
+  if (mx) block_max_atomic<T>(m, mx);
 }
 
 // One thread: the step's dt from the maxima (core.py:637-646, physics.py:723-742, 1230-1262),
@@ -367,8 +357,8 @@ __global__ void psi_accumulate_kernel(const T *__restrict__ psi, T *__restrict__
 
 template <typename T>
 cudaError_t launch_absmax(const T *a, size_t n, unsigned long long *out, cudaStream_t s) {
-  int blocks = (int)std::min<size_t>((n + 255) / 256, 148 * 8);
-  absmax_kernel<T><<<blocks, 256, 0, s>>>(a, n, out);
+  int blocks = (int)std::min<size_t>((n + 1023) / 1024, 148 * 2);
+  absmax_kernel<T><<<blocks, 1024, 0, s>>>(a, n, out);
   return cudaGetLastError();
 }
 

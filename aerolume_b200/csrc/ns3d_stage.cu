@@ -161,14 +161,7 @@ __global__ void __launch_bounds__(TX *TY) nu_kernel(const __grid_constant__ NuPa
     __syncthreads();
   }
 #undef V3
-  if (P.nut_max) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const T other = __shfl_xor_sync(0xffffffffu, mx, o);
-      mx = (other > mx || other != other) ? other : mx;
-    }
-    if ((tid & 31) == 0) atomic_max_nonneg(P.nut_max, (double)mx);
-  }
+  if (P.nut_max) block_max_atomic<T>(mx, P.nut_max);
 }
 
 // --------------------------------------------------------------------------------------

@@ -167,6 +167,12 @@ int aero_ns3d_project(const AeroNs3dPlan *plan, void *u, void *v, void *w, void 
  * non-finite value reached a reduction).  Reads through a host copy: synchronises. */
 int aero_ns3d_read_status(const AeroNs3dPlan *plan, const void *workspace, int32_t *status, void *stream);
 
+/* The checked build (libaero_b200_checked.so, compiled with AERO_BOUNDS_CHECK) records the
+ * first out-of-range shared- or global-memory index a kernel would have used -- (code, index,
+ * bound, block << 32 | thread) -- and skips that access.  Synchronising read that also clears
+ * the record; in the release library it returns AERO_EUNSUPPORTED.  (No counterpart in the reference: a debugging hook.) */
+int aero_debug_check(int64_t *out4);
+
 #ifdef __cplusplus
 }
 #endif
