@@ -29,7 +29,7 @@ EXPORTS = ("aero_abi_version", "aero_last_error", "aero_ns3d_plan_create", "aero
            "aero_ns3d_workspace_bytes", "aero_ns3d_workspace_init", "aero_ns3d_step", "aero_ns3d_step_traced",
            "aero_ns3d_smoke",
            "aero_ns3d_poisson_solve",
-           "aero_ns3d_project", "aero_ns3d_read_status", "aero_debug_check")
+           "aero_ns3d_project", "aero_ns3d_read_status", "aero_debug_check", "aero_ns3d_poisson_solve_static")
 
 
 class Ns3dConfig(C.Structure):
@@ -101,11 +101,12 @@ def lib() -> C.CDLL:
     L.aero_ns3d_project.argtypes = [C.c_void_p] + [C.c_void_p] * 6
     L.aero_ns3d_read_status.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_int32), C.c_void_p]
     L.aero_debug_check.argtypes = [C.POINTER(C.c_int64)]
+    L.aero_ns3d_poisson_solve_static.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.aero_debug_check.restype = C.c_int
     for name in ("aero_ns3d_plan_create", "aero_ns3d_workspace_init", "aero_ns3d_step", "aero_ns3d_step_traced",
                  "aero_ns3d_smoke",
                  "aero_ns3d_poisson_solve",
-                 "aero_ns3d_project", "aero_ns3d_read_status", "aero_debug_check"):
+                 "aero_ns3d_project", "aero_ns3d_read_status", "aero_debug_check", "aero_ns3d_poisson_solve_static"):
         getattr(L, name).restype = C.c_int
     if L.aero_abi_version() != ABI_VERSION:
         raise RuntimeError(f"{LIB_PATH.name} has ABI {L.aero_abi_version()}, expected {ABI_VERSION}; rebuild it")

@@ -2,6 +2,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 #include <cudaTypedefs.h>
@@ -567,6 +568,81 @@ int project_impl(const AeroNs3dPlan *p, void *u, void *v, void *w, void *psi, un
   return AERO_OK;
 }
 
+// ---- allocation-free Poisson solve -------------------------------------------------
+// The per-axis transform tables (twiddles, DCT post-twiddles, cos/sin, eigenvalues, dense
+// matrices) normally live in the caller's workspace.  aero_ns3d_poisson_solve_static keeps
+// them in this file-scope device array instead: every GPU that loads the library holds its
+// AERO_STATIC_SCRATCH_BYTES until the process exits, and no call allocates anything.  Every
+// call rewrites all of the tables it reads before reading them, so nothing in the array has
+// to start at zero; calls that overlap on the GPU (two streams, two host threads) share the
+// array and race.
+static __device__ __align__(256) unsigned char g_static_scratch[AERO_STATIC_SCRATCH_BYTES];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mutex;
+void *g_scratch_addr[kMaxDevices];  // device address of g_static_scratch, per device ordinal
+
+// Set-up, once per device and with that device current: g_static_scratch is a host-side
+// stand-in for the symbol, so its device address comes from cudaGetSymbolAddress.  On a
+// device's first call this may load the library's device code (lazy module loading).
+int static_scratch(unsigned char **out) {
+  int dev = -1;
+  CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return fail(AERO_EUNSUPPORTED, "device ordinal beyond 63");
+  std::lock_guard<std::mutex> lock(g_scratch_mutex);
+  if (!g_scratch_addr[dev]) {
+    void *ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_static_scratch);
+    if (e != cudaSuccess || !ptr)
+      return fail(AERO_ECUDA, std::string("cudaGetSymbolAddress(static scratch): ") + cudaGetErrorString(e));
+    g_scratch_addr[dev] = ptr;
+  }
+  *out = static_cast<unsigned char *>(g_scratch_addr[dev]);
+  return AERO_OK;
+}
+
+// The plan's tables re-laid out back to back (256-byte aligned) from offset 0; returns the bytes.
+size_t compact_tables(AeroNs3dPlan *q) {
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t at = off;
+    off += (bytes + ALIGN - 1) / ALIGN * ALIGN;
+    return at;
+  };
+  const size_t e = q->esz;
+  for (int a = 0; a < 3; ++a) {
+    AxisInfo &x = q->ax[a];
+    x.off_tw = take(2 * x.n * e);
+    x.off_post = take(2 * x.n * e);
+    x.off_cs = take(2 * x.n * e);
+    x.off_lam = take(sizeof(double) * x.n);
+    x.off_dense = take(x.method == 1 ? (size_t)x.n * x.n * e : 0);
+  }
+  return off;
+}
+
+template <typename T>
+int poisson_static_impl(const AeroNs3dPlan *plan, const void *f, void *psi, cudaStream_t s) {
+  AeroNs3dPlan q = *plan;  // host copy whose table offsets point into the static scratch
+  const size_t need = compact_tables(&q);
+  if (need > AERO_STATIC_SCRATCH_BYTES)
+    return fail(AERO_EINVAL, "the transform tables of this grid need " + std::to_string(need) +
+                                 " bytes; the static scratch holds " + std::to_string(AERO_STATIC_SCRATCH_BYTES) +
+                                 " (use aero_ns3d_poisson_solve with a workspace)");
+  unsigned char *scratch = nullptr;
+  const int rc = static_scratch(&scratch);
+  if (rc) return rc;
+  for (int a = 0; a < 3; ++a) {
+    const AxisInfo &x = q.ax[a];
+    CUDA_TRY(aero::launch_axis_tables<T>(x.n, x.kind, x.method == 1, q.cfg.h, reinterpret_cast<T *>(scratch + x.off_tw),
+                                         reinterpret_cast<T *>(scratch + x.off_post),
+                                         reinterpret_cast<T *>(scratch + x.off_cs),
+                                         reinterpret_cast<double *>(scratch + x.off_lam),
+                                         x.method == 1 ? reinterpret_cast<T *>(scratch + x.off_dense) : nullptr, s));
+  }
+  return poisson_passes<T>(&q, static_cast<const T *>(f), static_cast<T *>(psi), scratch, s);
+}
+
 bool window_empty(const int32_t *w) { return w[1] <= w[0] || w[3] <= w[2] || w[5] <= w[4]; }
 
 }  // namespace
@@ -732,6 +808,13 @@ int aero_ns3d_poisson_solve(const AeroNs3dPlan *plan, const void *f, void *psi, 
   auto ws = static_cast<unsigned char *>(workspace);
   return plan->cfg.dtype == AERO_F64 ? poisson_impl<double>(plan, f, psi, ws, s)
                                      : poisson_impl<float>(plan, f, psi, ws, s);
+}
+
+int aero_ns3d_poisson_solve_static(const AeroNs3dPlan *plan, const void *f, void *psi, void *stream) {
+  if (!plan || !f || !psi) return fail(AERO_EINVAL, "null argument");
+  auto s = static_cast<cudaStream_t>(stream);
+  return plan->cfg.dtype == AERO_F64 ? poisson_static_impl<double>(plan, f, psi, s)
+                                     : poisson_static_impl<float>(plan, f, psi, s);
 }
 
 int aero_ns3d_project(const AeroNs3dPlan *plan, void *u, void *v, void *w, void *psi, void *workspace, void *stream) {

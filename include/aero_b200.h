@@ -159,6 +159,21 @@ int aero_ns3d_smoke(const AeroNs3dPlan *plan, const AeroNs3dFields *f, const Aer
 int aero_ns3d_poisson_solve(const AeroNs3dPlan *plan, const void *f, void *psi, void *workspace,
                             void *stream);
 
+/* Allocation-free variant of aero_ns3d_poisson_solve.  No counterpart in the reference: it is
+ * for callers that cannot allocate device memory (a host that reserves the GPU's memory in its
+ * own arena, or a real-time loop in which cudaMalloc / cudaFree would synchronise the device).
+ * The transform tables go to a static device array of AERO_STATIC_SCRATCH_BYTES that every GPU
+ * which loads the library holds until exit; the caller passes no workspace.  The tables take
+ * 7n values per axis of n cells plus n * n for an axis whose length has a prime factor above 3
+ * (dense transform): FP64 fits three FFT axes of up to 2048 cells, or one dense axis of up to
+ * about 330 beside two FFT axes of 256.  Larger grids are rejected with AERO_EINVAL and a
+ * message naming the bytes they need.  The first call on a device looks up the array's device
+ * address (with that device current); make that first call before any stream capture.  Calls
+ * share the array: calls that overlap on the GPU race.  Allocates nothing (no cudaMalloc,
+ * cudaFree or allocating library routine). */
+#define AERO_STATIC_SCRATCH_BYTES (1u << 20)
+int aero_ns3d_poisson_solve_static(const AeroNs3dPlan *plan, const void *f, void *psi, void *stream);
+
 /* In place: (u, v, w) <- (u, v, w) - grad psi with lap psi = div(u, v, w); psi written. */
 int aero_ns3d_project(const AeroNs3dPlan *plan, void *u, void *v, void *w, void *psi, void *workspace,
                       void *stream);
