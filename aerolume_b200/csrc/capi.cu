@@ -157,13 +157,24 @@ aero::CompRules<T> comp_rules(const AeroNs3dConfig &c, int comp, int pitch = 0) 
 
 // sum of a[r * stride + off] over rows, in a fixed order, into out (double)
 template <typename T>
-__global__ void plane_sum_kernel(const T *a0, size_t stride0, size_t off0, double *out0, const T *a1, size_t stride1,
+__global__ void __launch_bounds__(512) plane_sum_kernel(const T *a0, size_t stride0, size_t off0, double *out0, const T *a1, size_t stride1,
                                  size_t off1, double *out1, int rows) {
   __shared__ double red[2][32];
+  constexpr int U = 16;  // rows in flight per thread: the loads of a chunk are independent
   double s0 = 0.0, s1 = 0.0;
-  for (int r = threadIdx.x; r < rows; r += blockDim.x) {
-    if (a0) s0 += (double)a0[(size_t)r * stride0 + off0];
-    if (a1) s1 += (double)a1[(size_t)r * stride1 + off1];
+  for (int base = 0; base < rows; base += U * (int)blockDim.x) {
+    T x0[U], x1[U];
+#pragma unroll
+    for (int q = 0; q < U; ++q) {
+      const int r = base + q * (int)blockDim.x + (int)threadIdx.x;
+      x0[q] = (a0 && r < rows) ? a0[(size_t)r * stride0 + off0] : T(0);
+      x1[q] = (a1 && r < rows) ? a1[(size_t)r * stride1 + off1] : T(0);
+    }
+#pragma unroll
+    for (int q = 0; q < U; ++q) {
+      s0 += (double)x0[q];
+      s1 += (double)x1[q];
+    }
   }
   s0 = aero::warp_sum(s0);
   s1 = aero::warp_sum(s1);
@@ -408,7 +419,7 @@ int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom
 
   const int rows = nz * ny;
   if (tunnel) {
-    plane_sum_kernel<T><<<1, 1024, 0, s>>>(upb, p->pu, nx, sc + aero::SC_SUM_U0, S.u_inlet, 1, 0,
+    plane_sum_kernel<T><<<1, 512, 0, s>>>(upb, p->pu, nx, sc + aero::SC_SUM_U0, S.u_inlet, 1, 0,
                                           sc + aero::SC_SUM_INLET, rows);
     CUDA_TRY(cudaGetLastError());
   }
@@ -420,7 +431,7 @@ int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom
     const T *up = upb, *vp = st == 0 ? v0 : vpb, *wp = st == 0 ? w0 : wpb;
     if (tunnel) {
       double *sums = sc + aero::SC_SUMS + 3 * st;
-      plane_sum_kernel<T><<<1, 1024, 0, s>>>(up, p->pu, nx, sums, up, p->pu, nx - 1, sums + 1, rows);
+      plane_sum_kernel<T><<<1, 512, 0, s>>>(up, p->pu, nx, sums, up, p->pu, nx - 1, sums + 1, rows);
       CUDA_TRY(cudaGetLastError());
       CUDA_TRY(aero::launch_outlet_corr<T>(sums, sc + aero::SC_SUM_U0, sc + aero::SC_SUM_INLET, small, RK[st][0],
                                            RK[st][1], 1.0 / c.h, 1.0 / rows, small + 1, s));

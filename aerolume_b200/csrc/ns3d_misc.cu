@@ -23,17 +23,30 @@ __global__ void absmax_kernel(const T *__restrict__ a, size_t n, unsigned long l
   block_max_atomic<T>(m, out);
 }
 
-// u0 (rows of nx + 1) into the stage-start buffer with a 16-byte row pitch, with max |u0|
+// u0 (rows of nx + 1) into the stage-start buffer with a 16-byte row pitch, with max |u0|.
+// A fixed grid strides over the rows (one max atomic per block, not per row); the thread of
+// x = nx - 1 also copies the last face, x = nx.
 template <typename T>
-__global__ void copy_u_kernel(const T *__restrict__ u, T *__restrict__ out, int nx, int ny, int pitch,
+__global__ void copy_u_kernel(const T *__restrict__ u, T *__restrict__ out, int nx, int ny, int nz, int pitch,
                               unsigned long long *mx) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int rows = ny * nz;
   T m = T(0);
-  if (i <= nx) {
-    const T v = u[((size_t)k * ny + j) * (nx + 1) + i];
-    if (AERO_IN(((size_t)k * ny + j) * pitch + i, (long long)gridDim.z * ny * pitch, 201))
-      out[((size_t)k * ny + j) * pitch + i] = v;
-    m = fabs(v);
+  if (i < nx) {
+    for (int r = blockIdx.y * blockDim.y + threadIdx.y; r < rows; r += gridDim.y * blockDim.y) {
+      const T *src = u + (size_t)r * (nx + 1);
+      T *dst = out + (size_t)r * pitch;
+      const T a = src[i];
+      if (AERO_IN((size_t)r * pitch + i, (long long)rows * pitch, 201)) dst[i] = a;
+      T ma = fabs(a);
+      if (i == nx - 1) {
+        const T b = src[nx];
+        if (AERO_IN((size_t)r * pitch + nx, (long long)rows * pitch, 202)) dst[nx] = b;
+        const T fb = fabs(b);
+        ma = (fb > ma || fb != fb) ? fb : ma;
+      }
+      m = (ma > m || ma != ma) ? ma : m;
+    }
   }
   if (mx) block_max_atomic<T>(m, mx);
 }
@@ -161,9 +174,11 @@ __global__ void divergence_kernel(const T *__restrict__ u, const T *__restrict__
 template <typename T>
 __global__ void correct_kernel(const CorrectParams<T> P) {
   const int nx = P.nx, ny = P.ny, nz = P.nz;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+  const int i0 = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
   const T inv = P.inv_h;
-  if (i <= nx && j < ny && k < nz) {  // u face (k, j, i)
+  // u faces (k, j, i): x = 0 .. nx; the thread of x = nx - 1 also does x = nx
+  const int ilast = (i0 < nx && j < ny && k < nz) ? (i0 == nx - 1 ? nx : i0) : i0 - 1;
+  for (int i = i0; i <= ilast; ++i) {
     const size_t e = ((size_t)k * ny + j) * (nx + 1) + i;
     const size_t c = ((size_t)k * ny + j) * nx;
     T val;
@@ -178,6 +193,7 @@ __global__ void correct_kernel(const CorrectParams<T> P) {
     }
     P.u[((size_t)k * ny + j) * P.pu_out + i] = val;
   }
+  const int i = i0;
   if (i < nx && j <= ny && k < nz) {  // v face (k, j, i)
     const size_t e = ((size_t)k * (ny + 1) + j) * nx + i;
     T val;
@@ -231,40 +247,101 @@ __device__ __forceinline__ T dye_at(const T *__restrict__ c, int nz, int ny, int
   return __ldg(c + ((size_t)k * ny + j) * nx + i);
 }
 
+// Smoke update (dye.py:265-312 advect_dye3d, solver.py:646-684): a 32 x 8 column of cells
+// marches up SMOKE_ZC planes.  Each plane of dye, with two ghost / halo cells on each side in
+// x and y, is loaded once into a 6-plane ring in shared memory (the plane three ahead is
+// fetched into registers while the current plane is computed), so every cell reads its
+// x / y / z stencil from shared memory and one barrier separates the planes.
+constexpr int SMOKE_TX = 32, SMOKE_TY = 8, SMOKE_ZC = 16;
+constexpr int SMOKE_PX = SMOKE_TX + 4, SMOKE_PY = SMOKE_TY + 4, SMOKE_PPL = SMOKE_PX * SMOKE_PY;  // 432
+constexpr int SMOKE_NSLOT = 6;
+constexpr int SMOKE_LOADS = (SMOKE_PPL + SMOKE_TX * SMOKE_TY - 1) / (SMOKE_TX * SMOKE_TY);      // 2
+
 template <typename T>
-__global__ void smoke_kernel(const SmokeParams<T> P) {
+__global__ void __launch_bounds__(SMOKE_TX *SMOKE_TY) smoke_kernel(const __grid_constant__ SmokeParams<T> P) {
+  __shared__ T ring[SMOKE_NSLOT][SMOKE_PPL];
   const int nx = P.nx, ny = P.ny, nz = P.nz;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * SMOKE_TX + tx;
+  const int i0 = blockIdx.x * SMOKE_TX, j0 = blockIdx.y * SMOKE_TY;
+  const int kb = blockIdx.z * SMOKE_ZC, ke = min(kb + SMOKE_ZC, nz);
   const T dt = *P.dt;
   const T kk = dt * P.inv_h;
   const T t = P.t_new ? *P.t_new : *P.t0 + dt;
   const T on = (fmod(t, T(P.pulse_period)) < T(P.pulse_on)) ? T(1) : T(0);
-  {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
-    if (i >= nx) return;
-    const size_t e = ((size_t)k * ny + j) * nx + i;
-    auto C = [&](int dk, int dj, int di) { return dye_at<T>(P.c0, nz, ny, nx, P.px, P.py, P.pz, k + dk, j + dj, i + di); };
-    const T c = C(0, 0, 0);
-    const T fx0 = muscl_flux<T>(C(0, 0, -2), C(0, 0, -1), c, C(0, 0, 1), P.u[((size_t)k * ny + j) * (nx + 1) + i]);
-    const T fx1 = muscl_flux<T>(C(0, 0, -1), c, C(0, 0, 1), C(0, 0, 2), P.u[((size_t)k * ny + j) * (nx + 1) + i + 1]);
-    const T fy0 = muscl_flux<T>(C(0, -2, 0), C(0, -1, 0), c, C(0, 1, 0), P.v[((size_t)k * (ny + 1) + j) * nx + i]);
-    const T fy1 = muscl_flux<T>(C(0, -1, 0), c, C(0, 1, 0), C(0, 2, 0), P.v[((size_t)k * (ny + 1) + j + 1) * nx + i]);
-    const T fz0 = muscl_flux<T>(C(-2, 0, 0), C(-1, 0, 0), c, C(1, 0, 0), P.w[((size_t)k * ny + j) * nx + i]);
-    const T fz1 = muscl_flux<T>(C(-1, 0, 0), c, C(1, 0, 0), C(2, 0, 0), P.w[((size_t)(k + 1) * ny + j) * nx + i]);
-    T v = c - kk * (((fx1 - fx0) + (fy1 - fy0)) + (fz1 - fz0));
-    v = v > T(1) ? T(1) : v;
-    v = v < T(1e-8) ? T(0) : v;
-    if (P.chi_c && k >= P.win[0] && k < P.win[1] && j >= P.win[2] && j < P.win[3] && i >= P.win[4] && i < P.win[5]) {
-      const T chi = P.chi_c[((size_t)(k - P.win[0]) * (P.win[3] - P.win[2]) + (j - P.win[2])) * (P.win[5] - P.win[4]) +
-                            (i - P.win[4])];
-      if (chi > T(0.5)) v = T(0);
+  auto slot = [&](int k) { return (k - kb + 2 + 2 * SMOKE_NSLOT) % SMOKE_NSLOT; };  // k >= kb - 2
+  // this thread's share of plane k (tile entry e = tid + q * 256 <-> (j0 - 2 + e / 36, i0 - 2 + e % 36))
+  auto fetch = [&](int k, T *r) {
+#pragma unroll
+    for (int q = 0; q < SMOKE_LOADS; ++q) {
+      const int e = tid + q * SMOKE_TX * SMOKE_TY;
+      if (e < SMOKE_PPL) {
+        // entries beyond the second ghost layer (x > nx + 1, y > ny + 1) feed no cell
+        const int ly = e / SMOKE_PX, lx = e - ly * SMOKE_PX;
+        const int gj = j0 - 2 + ly, gi = i0 - 2 + lx;
+        r[q] = (gi <= nx + 1 && gj <= ny + 1) ? dye_at<T>(P.c0, nz, ny, nx, P.px, P.py, P.pz, k, gj, gi) : T(0);
+      }
     }
-    if (P.weight && k >= P.dwin[0] && k < P.dwin[1] && j >= P.dwin[2] && j < P.dwin[3] && i >= P.dwin[4] &&
-        i < P.dwin[5]) {
-      const T wgt = P.weight[((size_t)(k - P.dwin[0]) * (P.dwin[3] - P.dwin[2]) + (j - P.dwin[2])) * (P.dwin[5] - P.dwin[4]) +
-                             (i - P.dwin[4])];
-      v = v + wgt * on * (T(1) - v);
+  };
+  auto store = [&](int k, const T *r) {
+    T *dst = ring[slot(k)];
+#pragma unroll
+    for (int q = 0; q < SMOKE_LOADS; ++q) {
+      const int e = tid + q * SMOKE_TX * SMOKE_TY;
+      if (e < SMOKE_PPL) dst[e] = r[q];
     }
-    P.c[e] = v;
+  };
+  T r[SMOKE_LOADS];
+  for (int k = kb - 2; k <= min(kb + 2, ke + 1); ++k) {
+    fetch(k, r);
+    store(k, r);
+  }
+  __syncthreads();
+  const int i = i0 + tx, j = j0 + ty;
+  const bool mine = i < nx && j < ny;
+  const int cx = tx + 2, cy = ty + 2, ce = cy * SMOKE_PX + cx;
+  T wlo = (mine && kb < nz) ? __ldg(P.w + ((size_t)kb * ny + j) * nx + i) : T(0);
+  for (int k = kb; k < ke; ++k) {
+    const bool more = k + 3 <= ke + 1;  // plane k + 3 is needed by the plane k + 1 stencil
+    if (more) fetch(k + 3, r);
+    if (mine) {
+      const T *S0 = ring[slot(k)];
+      const T c = S0[ce];
+      const T ul = __ldg(P.u + ((size_t)k * ny + j) * (nx + 1) + i);
+      const T ur = __ldg(P.u + ((size_t)k * ny + j) * (nx + 1) + i + 1);
+      const T vl = __ldg(P.v + ((size_t)k * (ny + 1) + j) * nx + i);
+      const T vr = __ldg(P.v + ((size_t)k * (ny + 1) + j + 1) * nx + i);
+      const T whi = __ldg(P.w + ((size_t)(k + 1) * ny + j) * nx + i);
+      const T fx0 = muscl_flux<T>(S0[ce - 2], S0[ce - 1], c, S0[ce + 1], ul);
+      const T fx1 = muscl_flux<T>(S0[ce - 1], c, S0[ce + 1], S0[ce + 2], ur);
+      const T fy0 = muscl_flux<T>(S0[ce - 2 * SMOKE_PX], S0[ce - SMOKE_PX], c, S0[ce + SMOKE_PX], vl);
+      const T fy1 = muscl_flux<T>(S0[ce - SMOKE_PX], c, S0[ce + SMOKE_PX], S0[ce + 2 * SMOKE_PX], vr);
+      const T zm2 = ring[slot(k - 2)][ce], zm1 = ring[slot(k - 1)][ce];
+      const T zp1 = ring[slot(k + 1)][ce], zp2 = ring[slot(k + 2)][ce];
+      const T fz0 = muscl_flux<T>(zm2, zm1, c, zp1, wlo);
+      const T fz1 = muscl_flux<T>(zm1, c, zp1, zp2, whi);
+      wlo = whi;
+      T v = c - kk * (((fx1 - fx0) + (fy1 - fy0)) + (fz1 - fz0));
+      v = v > T(1) ? T(1) : v;
+      v = v < T(1e-8) ? T(0) : v;
+      if (P.chi_c && k >= P.win[0] && k < P.win[1] && j >= P.win[2] && j < P.win[3] && i >= P.win[4] &&
+          i < P.win[5]) {
+        const T chi = P.chi_c[((size_t)(k - P.win[0]) * (P.win[3] - P.win[2]) + (j - P.win[2])) *
+                                  (P.win[5] - P.win[4]) +
+                              (i - P.win[4])];
+        if (chi > T(0.5)) v = T(0);
+      }
+      if (P.weight && k >= P.dwin[0] && k < P.dwin[1] && j >= P.dwin[2] && j < P.dwin[3] && i >= P.dwin[4] &&
+          i < P.dwin[5]) {
+        const T wgt = P.weight[((size_t)(k - P.dwin[0]) * (P.dwin[3] - P.dwin[2]) + (j - P.dwin[2])) *
+                                   (P.dwin[5] - P.dwin[4]) +
+                               (i - P.dwin[4])];
+        v = v + wgt * on * (T(1) - v);
+      }
+      P.c[((size_t)k * ny + j) * nx + i] = v;
+    }
+    // plane k + 3 goes into the slot of plane k - 3, which no thread reads from here on
+    if (more) store(k + 3, r);
+    __syncthreads();
   }
 }
 
@@ -365,7 +442,10 @@ cudaError_t launch_absmax(const T *a, size_t n, unsigned long long *out, cudaStr
 template <typename T>
 cudaError_t launch_copy_u(const T *u, T *out, int nx, int ny, int nz, int pitch, unsigned long long *mx,
                           cudaStream_t s) {
-  copy_u_kernel<T><<<dim3((nx + 1 + 127) / 128, ny, nz), 128, 0, s>>>(u, out, nx, ny, pitch, mx);
+  const unsigned gx = (unsigned)((nx + 127) / 128);
+  const unsigned rows = (unsigned)ny * (unsigned)nz;
+  const unsigned gy = std::max(1u, std::min((rows + 1) / 2, 2368u / gx));
+  copy_u_kernel<T><<<dim3(gx, gy), dim3(128, 2), 0, s>>>(u, out, nx, ny, nz, pitch, mx);
   return cudaGetLastError();
 }
 
@@ -399,13 +479,14 @@ cudaError_t launch_divergence(const T *u, const T *v, const T *w, int nx, int ny
 
 template <typename T>
 cudaError_t launch_correct(const CorrectParams<T> &P, cudaStream_t s) {
-  correct_kernel<T><<<dim3((P.nx + 1 + 127) / 128, P.ny + 1, P.nz + 1), 128, 0, s>>>(P);
+  correct_kernel<T><<<dim3((P.nx + 127) / 128, P.ny + 1, P.nz + 1), 128, 0, s>>>(P);
   return cudaGetLastError();
 }
 
 template <typename T>
 cudaError_t launch_smoke(const SmokeParams<T> &P, cudaStream_t s) {
-  smoke_kernel<T><<<dim3((P.nx + 127) / 128, P.ny, P.nz), 128, 0, s>>>(P);
+  const dim3 grid((P.nx + SMOKE_TX - 1) / SMOKE_TX, (P.ny + SMOKE_TY - 1) / SMOKE_TY, (P.nz + SMOKE_ZC - 1) / SMOKE_ZC);
+  smoke_kernel<T><<<grid, dim3(SMOKE_TX, SMOKE_TY), 0, s>>>(P);
   return cudaGetLastError();
 }
 

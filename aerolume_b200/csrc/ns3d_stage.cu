@@ -31,9 +31,14 @@ constexpr int PX = TX + 8, PY = TY + 4, PPL = PX * PY;
 // eddy-viscosity tile of the stage kernel: nu array columns i0 .. i0 + TX + 3, rows j0 .. j0 + TY + 1
 constexpr int NUX = TX + 4, NUY = TY + 2, NUPL = 384;  // 360 used, slots padded to 128 bytes
 constexpr int NSLOT = 6;
-// nu kernel tile: x from i0 - 4, y from j0 - 2, 36 x 10
+// nu kernel tile: x from i0 - 4, y from j0 - 2, 36 x 10; a ring of QSLOT planes per velocity
+// component, which lets the TMA copies run QSLOT - 3 planes ahead of the computation
 constexpr int QX = TX + 4, QY = TY + 2, QPL = 384;
-constexpr int QSLOT = 4;
+template <typename T>
+struct NuRing {
+  static constexpr int QSLOT = sizeof(T) == 4 ? 8 : 4;  // 36 KB (FP32) / 36 KB (FP64) of planes
+  static constexpr int AHEAD = QSLOT - 3;
+};
 
 // --------------------------------------------------------------------------------------
 // eddy viscosity nu_t on cells -1..n of every axis (core.py:400-482, 498-504), written to
@@ -42,13 +47,14 @@ constexpr int QSLOT = 4;
 
 template <typename T>
 struct NuSmem {
-  alignas(128) T vel[3][QSLOT][QPL];
-  uint64_t bar[QSLOT];
+  alignas(128) T vel[3][NuRing<T>::QSLOT][QPL];
+  uint64_t bar[NuRing<T>::QSLOT];
 };
 
 template <typename T>
 __global__ void __launch_bounds__(TX *TY) nu_kernel(const __grid_constant__ NuParams<T> P) {
   __shared__ NuSmem<T> S;
+  constexpr int QSLOT = NuRing<T>::QSLOT, AHEAD = NuRing<T>::AHEAD;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
   const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;  // cells of the tile: (j0-1+ty, i0-1+tx)
   const int qb = blockIdx.z * P.zc, qe = min(qb + P.zc, P.nz + 2);
@@ -91,10 +97,13 @@ __global__ void __launch_bounds__(TX *TY) nu_kernel(const __grid_constant__ NuPa
     mbar_fence_init();
   }
   __syncthreads();
-  // nu plane q holds cells k = q - 1, which need velocity planes q - 2 .. q
+  // nu plane q holds cells k = q - 1, which need velocity planes q - 2 .. q; the last plane
+  // any iteration needs is qe - 1.  Iteration q issues plane q + AHEAD, so the ring holds
+  // planes q - 2 .. q + AHEAD (QSLOT of them) and the slot it refills (plane q - 3) was last
+  // read in iteration q - 1, which ended with a barrier.
   if (P.use_tma) {
     if (tid == 0)
-      for (int kp = qb - 2; kp <= qb; ++kp) issue(kp);
+      for (int kp = qb - 2; kp <= min(qb + AHEAD - 1, qe - 1); ++kp) issue(kp);
     for (int kp = qb - 2; kp <= qb; ++kp) {
       await_plane(kp);
       fill(kp, false);
@@ -107,7 +116,7 @@ __global__ void __launch_bounds__(TX *TY) nu_kernel(const __grid_constant__ NuPa
   T mx = T(0);
   for (int q = qb; q < qe; ++q) {
     const bool pre = q + 1 < qe;
-    if (P.use_tma && pre && tid == 0) issue(q + 1);
+    if (P.use_tma && tid == 0 && q + AHEAD <= qe - 1) issue(q + AHEAD);
     const int kn = q - 1;
     const int cj = j0 - 1 + ty, ci = i0 - 1 + tx;  // this thread's cell
     if (cj <= ny && ci <= nx) {

@@ -26,6 +26,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import re
 import os
 import subprocess
 import sys
@@ -293,16 +294,19 @@ def run_ours(args, rank, world, local_rank):
     ms_step = ms / K
     value = world * cells * K / (ms * 1e-3) / 1e6
     sample_steps = 2
-    secs = oracle_sample(nx, ny, nz, sample_steps) if not args.no_cpu else float("nan")
-    cpu = {"value": cells * sample_steps / secs / 1e6, "unit": UNIT, "cores": _threads(), "kind": "port",
-           "sample": f"{sample_steps} full {nx}x{ny}x{nz} steps of the numpy oracle after 1 untimed step"}
+    if args.no_cpu:
+        cpu = None
+    else:
+        secs = oracle_sample(nx, ny, nz, sample_steps)
+        cpu = {"value": cells * sample_steps / secs / 1e6, "unit": UNIT, "cores": _threads(), "kind": "port",
+               "sample": f"{sample_steps} full {nx}x{ny}x{nz} steps of the numpy oracle after 1 untimed step"}
+    # DRAM bytes per stage_kernel launch (mean of the three stages) from the committed ncu
+    # summary of this workload; None for other shapes
     traffic = None
-    tp = ROOT / "profiles" / "stage_kernel_traffic.json"
-    if tp.exists():
-        try:
-            traffic = json.loads(tp.read_text()).get("bytes_per_launch_full_size")
-        except Exception:
-            traffic = None
+    tp = ROOT / "profiles" / "stage_kernel_256x128x128_dram.md"
+    if (nx, ny, nz) == SHAPE and tp.exists():
+        m = re.search(r"^traffic_bytes_per_launch_mean:\s*(\d+)", tp.read_text(), re.M)
+        traffic = int(m.group(1)) if m else None
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup,
             "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
