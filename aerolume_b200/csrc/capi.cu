@@ -119,16 +119,35 @@ aero::AxisTables<T> axis_tables(const AeroNs3dPlan *p, int a, unsigned char *ws)
 // psi = L^{-1} f through five passes: x, y forward; z forward-solve-inverse; y, x inverse.
 // Every pass owns whole lines per block, so after the first pass the solve runs in place.
 template <typename T>
-int poisson_passes(const AeroNs3dPlan *p, const T *f, T *psi, unsigned char *ws, cudaStream_t s) {
+// `fuse` (power-of-two x axes only, see fused_projection) supplies the divergence fusion
+// fields for the first pass and the pressure-accumulation fields for the last one.
+int poisson_passes(const AeroNs3dPlan *p, const T *f, T *psi, unsigned char *ws, cudaStream_t s,
+                   const aero::TransformParams<T> *fuse = nullptr) {
   const AeroNs3dConfig &c = p->cfg;
-  aero::TransformParams<T> P{};
-  P.nx = c.nx;
-  P.ny = c.ny;
-  P.nz = c.nz;
-  P.lam_x = reinterpret_cast<const double *>(ws + p->ax[0].off_lam);
-  P.lam_y = reinterpret_cast<const double *>(ws + p->ax[1].off_lam);
   const int axes[5] = {0, 1, 2, 1, 0}, modes[5] = {0, 0, 2, 1, 1};
   for (int q = 0; q < 5; ++q) {
+    aero::TransformParams<T> P{};
+    if (fuse && q == 0) {
+      P.fuse_div = fuse->fuse_div;
+      P.px = fuse->px;
+      P.py = fuse->py;
+      P.pz = fuse->pz;
+      P.uh = fuse->uh;
+      P.vh = fuse->vh;
+      P.wh = fuse->wh;
+      P.inv_h = fuse->inv_h;
+    }
+    if (fuse && q == 4) {
+      P.p_acc = fuse->p_acc;
+      P.wgt = fuse->wgt;
+      P.acc_mode = fuse->acc_mode;
+      P.dt = fuse->dt;
+    }
+    P.nx = c.nx;
+    P.ny = c.ny;
+    P.nz = c.nz;
+    P.lam_x = reinterpret_cast<const double *>(ws + p->ax[0].off_lam);
+    P.lam_y = reinterpret_cast<const double *>(ws + p->ax[1].off_lam);
     P.axis = axes[q];
     P.mode = modes[q];
     P.in = q == 0 ? f : psi;
@@ -461,12 +480,33 @@ int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom
     stage_views(vp, wp, thermal ? P.thp : nullptr, P);
     CUDA_TRY(aero::launch_stage<T>(P, s));
     CUDA_TRY(mark(3 + 5 * st));
-    CUDA_TRY(aero::launch_divergence<T>(uh, vh, wh, nx, ny, nz, c.periodic[0], c.periodic[1], c.periodic[2],
-                                        T(1.0 / c.h), pa, s));
-    CUDA_TRY(mark(4 + 5 * st));
-    const int rc = poisson_passes<T>(p, pa, pa, ws, s);
-    if (rc) return rc;
-    CUDA_TRY(aero::launch_psi_accumulate<T>(pa, p_out, p->nc, T(RK[st][2]), st == 0 ? 0 : (st == 1 ? 1 : 2), small, s));
+    const int acc_mode = st == 0 ? 0 : (st == 1 ? 1 : 2);
+    if (p->ax[0].method == 0 && aero::transform_pow2(nx)) {
+      // the first x pass forms div(u_hat) itself, the last one folds psi into p
+      aero::TransformParams<T> F{};
+      F.fuse_div = 1;
+      F.px = c.periodic[0];
+      F.py = c.periodic[1];
+      F.pz = c.periodic[2];
+      F.uh = uh;
+      F.vh = vh;
+      F.wh = wh;
+      F.inv_h = T(1.0 / c.h);
+      F.p_acc = p_out;
+      F.wgt = T(RK[st][2]);
+      F.acc_mode = acc_mode;
+      F.dt = small;
+      CUDA_TRY(mark(4 + 5 * st));
+      const int rc = poisson_passes<T>(p, nullptr, pa, ws, s, &F);
+      if (rc) return rc;
+    } else {
+      CUDA_TRY(aero::launch_divergence<T>(uh, vh, wh, nx, ny, nz, c.periodic[0], c.periodic[1], c.periodic[2],
+                                          T(1.0 / c.h), pa, s));
+      CUDA_TRY(mark(4 + 5 * st));
+      const int rc = poisson_passes<T>(p, pa, pa, ws, s);
+      if (rc) return rc;
+      CUDA_TRY(aero::launch_psi_accumulate<T>(pa, p_out, p->nc, T(RK[st][2]), acc_mode, small, s));
+    }
     CUDA_TRY(mark(5 + 5 * st));
     aero::CorrectParams<T> C{};
     C.nx = nx;

@@ -137,6 +137,16 @@ struct TransformParams {
   int nx, ny, nz, axis, mode, L;  // mode: 0 forward, 1 inverse, 2 forward-solve-inverse
   AxisTables<T> A;
   const double *lam_x, *lam_y;
+  // power-of-two x passes only: the forward pass may form div(uh, vh, wh) itself instead of
+  // reading `in`; the inverse pass may also fold psi into the step-averaged pressure
+  // (acc_mode 0: p = wgt psi; 1: p += wgt psi; 2: p = (p + wgt psi) / dt)
+  int fuse_div, px, py, pz;
+  const T *uh, *vh, *wh;
+  T inv_h;
+  T *p_acc;
+  T wgt;
+  int acc_mode;
+  const T *dt;
 };
 
 template <typename T> size_t stage_smem_bytes();
@@ -158,6 +168,9 @@ template <typename T> cudaError_t launch_finalize(const FinalizeParams<T> &, cud
 template <typename T> cudaError_t launch_psi_accumulate(const T *, T *, size_t, T, int, const T *, cudaStream_t);
 template <typename T> size_t transform_smem_bytes(int, int);
 template <typename T> cudaError_t launch_transform(const TransformParams<T> &, cudaStream_t);
+// true when an axis of n cells runs the compile-time power-of-two transform (8 <= n <= 2048),
+// which also takes the divergence / pressure fusions of TransformParams
+bool transform_pow2(int n);
 template <typename T>
 cudaError_t launch_axis_tables(int, int, int, double, T *, T *, T *, double *, T *, cudaStream_t);
 

@@ -15,6 +15,7 @@
 // length falls back to the dense orthonormal matrix in shared memory.  The z pass runs
 // forward transform, division by lambda_x + lambda_y + lambda_z (zero mode dropped) and
 // inverse transform in one kernel.
+#include "fft_tile.cuh"
 #include "ns3d.cuh"
 
 namespace aero {
@@ -266,6 +267,161 @@ __global__ void __launch_bounds__(256) line_transform_kernel(const TransformPara
   }
 }
 
+// --------------------------------------------------------------------------------------
+// Power-of-two axes: the compile-time tile transform of fft_tile.cuh
+// --------------------------------------------------------------------------------------
+
+struct BlockExec {
+  template <class F>
+  __device__ __forceinline__ void operator()(F &&f) {
+    f((int)threadIdx.x, (int)blockDim.x);
+    __syncthreads();
+  }
+};
+
+template <typename T, int N>
+struct Pow2Tile {
+  static constexpr int LOG2N = fft::ilog2(N);
+  static constexpr int LOG2L = fft::tile_log2L(N, (int)sizeof(T)), L = 1 << LOG2L, LD = L + 1;
+  static constexpr size_t TW = (size_t)N * 2 * sizeof(T);                        // twiddles
+  static constexpr size_t RB = ((size_t)N * LD * sizeof(T) + 15) & ~size_t(15);  // real tile
+  static constexpr size_t CB = (size_t)N * (L / 2) * 2 * sizeof(T);              // one complex buffer
+  static constexpr size_t SMEM = TW + RB + 2 * CB;
+};
+
+// One axis pass over L lines of N = 2^a cells: x lines are rows (r = k ny + j), y / z lines
+// are L consecutive x at fixed k / j.  Mode 0 forward, 1 inverse, 2 forward, division by
+// lambda_x + lambda_y + lambda_z (zero mode dropped) and inverse (z axis).
+template <typename T, int N>
+__global__ void __launch_bounds__(256) pow2_transform_kernel(const __grid_constant__ TransformParams<T> P) {
+  using G = Pow2Tile<T, N>;
+  constexpr int L = G::L, LD = G::LD, LOG2L = G::LOG2L, LOG2N = G::LOG2N;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  fft::Cx<T> *tw = reinterpret_cast<fft::Cx<T> *>(smem_raw);
+  T *R = reinterpret_cast<T *>(smem_raw + G::TW);
+  fft::Cx<T> *C0 = reinterpret_cast<fft::Cx<T> *>(smem_raw + G::TW + G::RB);
+  fft::Cx<T> *C1 = reinterpret_cast<fft::Cx<T> *>(smem_raw + G::TW + G::RB + G::CB);
+  __shared__ long long rowoff[5][L];  // fused divergence: u row, v rows j / j+1, w planes k / k+1
+  const int nx = P.nx, ny = P.ny, nz = P.nz;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  for (int m = tid; m < N; m += nthr) tw[m] = {P.A.tw[2 * m], P.A.tw[2 * m + 1]};
+  int nl;
+  size_t base, estride;
+  if (P.axis == 0) {
+    const size_t r0 = (size_t)blockIdx.x << LOG2L, rows = (size_t)nz * ny;
+    nl = (int)min((size_t)L, rows - r0);
+    base = r0 * N;
+    estride = 1;
+    if (P.fuse_div && tid < nl) {
+      const long long r = (long long)r0 + tid;
+      const int k = (int)(r / ny), j = (int)(r - (long long)k * ny);
+      rowoff[0][tid] = r * (nx + 1);
+      rowoff[1][tid] = ((long long)k * (ny + 1) + j) * nx;
+      rowoff[2][tid] = (P.py && j == ny - 1) ? (long long)k * (ny + 1) * nx : rowoff[1][tid] + nx;
+      rowoff[3][tid] = ((long long)k * ny + j) * nx;
+      rowoff[4][tid] = (P.pz && k == nz - 1) ? (long long)j * nx : rowoff[3][tid] + (long long)ny * nx;
+    }
+  } else {
+    const int i0 = blockIdx.x << LOG2L;
+    nl = min(L, nx - i0);
+    base = P.axis == 1 ? (size_t)blockIdx.y * ny * nx + i0 : (size_t)blockIdx.y * nx + i0;
+    estride = P.axis == 1 ? (size_t)nx : (size_t)ny * nx;
+  }
+  __syncthreads();
+  // ---- load (coalesced along whichever index is contiguous)
+  if (P.axis == 0) {
+    for (int e = tid; e < N * L; e += nthr) {
+      const int m = e & (N - 1), l = e >> LOG2N;
+      T val = T(0);
+      if (l < nl) {
+        if (P.fuse_div) {  // div(uh) of the stage velocity (core.py:577-579)
+          const T *ur = P.uh + rowoff[0][l];
+          const T u1 = (P.px && m == N - 1) ? ur[0] : ur[m + 1];
+          val = ((u1 - ur[m]) + (P.vh[rowoff[2][l] + m] - P.vh[rowoff[1][l] + m]) +
+                 (P.wh[rowoff[4][l] + m] - P.wh[rowoff[3][l] + m])) *
+                P.inv_h;
+        } else {
+          val = P.in[base + ((size_t)l << LOG2N) + m];
+        }
+      }
+      R[m * LD + l] = val;
+    }
+  } else {
+    for (int e = tid; e < N * L; e += nthr) {
+      const int l = e & (L - 1), m = e >> LOG2L;
+      R[m * LD + l] = (l < nl) ? P.in[base + l + (size_t)m * estride] : T(0);
+    }
+  }
+  __syncthreads();
+  const fft::AxisView<T> A{tw, reinterpret_cast<const fft::Cx<T> *>(P.A.post),
+                           reinterpret_cast<const fft::Cx<T> *>(P.A.cs), P.A.s0, P.A.s1, P.A.rsqrt_n, P.A.kind};
+  BlockExec ex;
+  if (P.mode == 2) {
+    fft::transform_tile<T, N, LOG2L>(R, C0, C1, tw, A, false, ex);
+    const int j = blockIdx.y, i0 = blockIdx.x << LOG2L;
+    for (int e = tid; e < N * L; e += nthr) {
+      const int l = e & (L - 1), k = e >> LOG2L;
+      const int i = i0 + l;
+      double inv = 0.0;
+      if (l < nl) {
+        const double lam = P.A.lam[k] + P.lam_y[j] + P.lam_x[i];
+        inv = (lam != 0.0) ? 1.0 / lam : 0.0;
+        if (k == 0 && j == 0 && i == 0) inv = 0.0;
+      }
+      R[k * LD + l] = R[k * LD + l] * T(inv);
+    }
+    __syncthreads();
+    fft::transform_tile<T, N, LOG2L>(R, C0, C1, tw, A, true, ex);
+  } else {
+    fft::transform_tile<T, N, LOG2L>(R, C0, C1, tw, A, P.mode == 1, ex);
+  }
+  // ---- store
+  if (P.axis == 0) {
+    const T rdt = (P.p_acc && P.acc_mode == 2) ? T(1) / *P.dt : T(1);
+    for (int e = tid; e < N * L; e += nthr) {
+      const int m = e & (N - 1), l = e >> LOG2N;
+      if (l >= nl) continue;
+      const size_t g = base + ((size_t)l << LOG2N) + m;
+      const T psi = R[m * LD + l];
+      P.out[g] = psi;
+      if (P.p_acc) {  // step-averaged pressure (core.py:874-875)
+        if (P.acc_mode == 0) {
+          P.p_acc[g] = psi * P.wgt;
+        } else {
+          const T sum = P.p_acc[g] + P.wgt * psi;
+          P.p_acc[g] = P.acc_mode == 2 ? sum * rdt : sum;
+        }
+      }
+    }
+  } else {
+    for (int e = tid; e < N * L; e += nthr) {
+      const int l = e & (L - 1), m = e >> LOG2L;
+      if (l < nl) P.out[base + l + (size_t)m * estride] = R[m * LD + l];
+    }
+  }
+}
+
+template <typename T, int N>
+cudaError_t launch_pow2(const TransformParams<T> &P, cudaStream_t s) {
+  using G = Pow2Tile<T, N>;
+  static bool configured = false;
+  if (!configured) {
+    const cudaError_t e = cudaFuncSetAttribute(pow2_transform_kernel<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)G::SMEM);
+    if (e != cudaSuccess) return e;
+    configured = true;
+  }
+  dim3 grid;
+  if (P.axis == 0)
+    grid = dim3((unsigned)(((size_t)P.nz * P.ny + G::L - 1) / G::L), 1, 1);
+  else
+    grid = dim3((unsigned)((P.nx + G::L - 1) / G::L), (unsigned)(P.axis == 1 ? P.nz : P.ny), 1);
+  pow2_transform_kernel<T, N><<<grid, 256, G::SMEM, s>>>(P);
+  return cudaGetLastError();
+}
+
+bool transform_pow2(int n) { return n >= 8 && n <= 2048 && (n & (n - 1)) == 0; }
+
 // Tables: twiddles e^{-2 pi i m / n}, DCT post-twiddles s_k e^{-i pi k / 2n}, cos / sin of
 // pi k / 2n, eigenvalues (2 cos(pi k / n) - 2) / h^2 or (2 cos(2 pi k / n) - 2) / h^2,
 // and the dense orthonormal matrix of poisson.py:74-90 for lengths the FFT does not take.
@@ -310,6 +466,20 @@ size_t transform_smem_bytes(int n, int L) {
 
 template <typename T>
 cudaError_t launch_transform(const TransformParams<T> &P, cudaStream_t s) {
+  if (P.A.method == 0 && transform_pow2(P.A.n)) {
+    switch (P.A.n) {
+      case 8: return launch_pow2<T, 8>(P, s);
+      case 16: return launch_pow2<T, 16>(P, s);
+      case 32: return launch_pow2<T, 32>(P, s);
+      case 64: return launch_pow2<T, 64>(P, s);
+      case 128: return launch_pow2<T, 128>(P, s);
+      case 256: return launch_pow2<T, 256>(P, s);
+      case 512: return launch_pow2<T, 512>(P, s);
+      case 1024: return launch_pow2<T, 1024>(P, s);
+      default: return launch_pow2<T, 2048>(P, s);
+    }
+  }
+  if (P.fuse_div || P.p_acc) return cudaErrorInvalidValue;  // fusions exist on power-of-two axes only
   const size_t smem = transform_smem_bytes<T>(P.A.n, P.L);
   static size_t set_to = 0;
   if (smem > set_to) {

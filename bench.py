@@ -159,8 +159,11 @@ def launches_per_step(plan):
     n = 3 + (1 if c.thermal else 0)                # |u|, |v|, |w|, |theta| maxima
     n += 1                                          # dt
     n += 1 if tunnel else 0                         # inlet / u0 outlet sums
-    per_stage = 1 + 1 + 5 + 1 + 1 + (2 if tunnel else 0) + (1 if les else 0)
-    n += 3 * per_stage                              # [nu], [sums, corr], stage, div, 5 transforms, psi_w, correct
+    # a power-of-two x axis folds the divergence into the first transform pass and the
+    # pressure accumulation into the last one
+    fused = 8 <= c.nx <= 2048 and (c.nx & (c.nx - 1)) == 0
+    per_stage = 1 + (0 if fused else 1) + 5 + (0 if fused else 1) + 1 + (2 if tunnel else 0) + (1 if les else 0)
+    n += 3 * per_stage                              # [nu], [sums, corr], stage, [div], 5 transforms, [psi_w], correct
     n += 1 if c.smoke else 0
     n += 1 if (c.nbody * 9 + (c.n_tbody if c.thermal else 0)) > 0 else 0   # partial-sum reduction
     n += 1                                          # finalize
