@@ -1,0 +1,66 @@
+"""Plain containers with the attribute names of the reference's 2D objects.
+
+``Ns2dPlan`` and the oracle read these attributes only, so the reference's own ``Ops`` /
+``Geometry`` (src/aerolume/solvers/ns2d/core.py:67-108, geometry.py:160-197) work as well.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+from typing import Any, NamedTuple
+
+
+class State2D(NamedTuple):
+    """Evolving state (core.py:111-130 without placed physics)."""
+    u: Any
+    v: Any
+    p: Any
+    dye: Any
+    t: Any
+    dt: Any
+
+
+@dataclass
+class Ops2D:
+    """Grid, boundaries and numerics of a 2D solve (core.py:67-108)."""
+    nx: int
+    ny: int
+    h: float
+    x0: float = 0.0
+    y0: float = 0.0
+    periodic: bool = False
+    closed: bool = False
+    bc_top: str = "slip"
+    bc_bottom: str = "slip"
+    bc_left: str = "noslip"
+    bc_right: str = "noslip"
+    ground_speed: float = 1.0
+    advection: str = "upwind3"
+    turbulence: str = "none"
+    les_c: float = 0.0
+    nu: float = 1e-3
+    eta: float = 1.0
+    cfl: float = 0.5
+    dt_fixed: float | None = None
+    u_inlet: Any = None          # (ny,) inlet u profile
+    dye_inlet: Any = None        # (ny,) inlet dye comb, or None without dye
+    force_ref: float = 1.0
+    moment_ref: tuple = (0.25, 0.0)
+    dtype: str = "float32"
+
+
+@dataclass
+class Geometry2D:
+    """Body masks on the cell window (j0, j1, i0, i1) (geometry.py:160-182)."""
+    window: tuple
+    chi_u: Any = None            # (wy, wx + 1)
+    chi_v: Any = None            # (wy + 1, wx)
+    chi_c: Any = None            # (wy, wx)
+    a_u: Any = None
+    a_v: Any = None
+    k_u: Any = None              # (nb, 2, wy, wx + 1): [Fx weight, moment weight]
+    k_v: Any = None              # (nb, 2, wy + 1, wx)
+    nbody: int = 0
+
+    @property
+    def empty(self) -> bool:
+        return self.window[1] <= self.window[0] or self.window[3] <= self.window[2]

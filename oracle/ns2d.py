@@ -1,0 +1,429 @@
+"""CPU oracle for the 2D staggered-grid Navier-Stokes step -- TEST INFRASTRUCTURE ONLY.
+
+This module is the checker, never the product: only ``tests/``, ``__graft_entry__.smoke()``
+and the CPU legs of ``bench.py`` may import it.  The CUDA path in ``aerolume_b200`` never
+calls into it.
+
+It restates, in numpy, the reference's plain 2D step (Aerolume ``src/aerolume/solvers/ns2d``)
+for the configurations the sm_100a kernels implement (tunnel, closed and periodic domains,
+slip / no-slip / moving walls, upwind3 or central advection, Smagorinsky / WALE / Vreman,
+immersed bodies, inlet-comb dye; no placed physics):
+
+* ``step2d``            core.py:815-969   SSP-RK3 with a projection after every stage
+* ``pad_u`` / ``pad_v`` core.py:284-325   two ghost layers
+* ``inlet_outlet``      core.py:328-359   inlet profile and outlet mass balance
+* ``advection2d``       core.py:366-414   upwind3 / central conservative advection
+* ``add_diffusion``     core.py:417-424
+* ``sgs_divergence2d``  core.py:427-520   eddy viscosity and div(2 nu_t S)
+* ``momentum_rhs2d``    core.py:571-613   tendencies with the boundary rows
+* ``project2d``         core.py:620-660   divergence, Poisson solve, u - grad psi
+* ``penalise2d``        core.py:663-682
+* ``cfl_dt2d``          core.py:685-696
+* ``advect_dye2d``      core.py:703-735, 779-792
+* ``PoissonSolver2D``   poisson.py:93-144 (the same exact solve in the orthonormal eigenbases)
+
+Parity is pinned: ``tests/test_oracle2d_golden.py`` checks this module against golden
+vectors that ``tests/golden/make_golden2d.py`` produced by running the reference itself.
+
+Inputs are duck-typed objects with the reference's attribute names (see
+``aerolume_b200.ns2d.types``); arrays are numpy, C order ``(ny, nx)`` with the staggered
+shapes of core.py:9-12: u (ny, nx + 1), v (ny + 1, nx), p (ny, nx).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from .ns3d import FORCE_WEIGHTS, SSP_RK3, face_flux, lerp, neumann_basis, periodic_basis
+
+_SQRT_EPS = 1e-30                                                  # ns2d/core.py:466
+DYE_ZERO = 1e-6                                                    # ns2d/core.py:735
+
+
+# ---------------------------------------------------------------------------
+# boundary conditions (core.py:271-359)
+# ---------------------------------------------------------------------------
+
+def _wall_ghost(rows, kind, speed):
+    if kind == "slip":
+        return rows
+    if kind == "noslip":
+        return -rows
+    return rows.dtype.type(2.0 * speed) - rows
+
+
+def pad_u(u, ops):
+    """(ny + 4, nx + 5): padded [j + 2, i + 2] = u[j, i] (core.py:284-305)."""
+    if ops.periodic:
+        up = u[:, :-1]
+        up = np.concatenate([up[:, -2:], up, up[:, :3]], axis=1)
+        return np.concatenate([up[-2:], up, up[:2]], axis=0)
+    if ops.closed:
+        ux = np.concatenate([-u[:, 1:3][:, ::-1], u, -u[:, -3:-1][:, ::-1]], axis=1)
+    else:
+        ux = np.concatenate([np.repeat(u[:, :1], 2, axis=1), u, np.repeat(u[:, -1:], 2, axis=1)], axis=1)
+    bot = _wall_ghost(ux[:2][::-1], ops.bc_bottom, ops.ground_speed)
+    top = _wall_ghost(ux[-2:][::-1], ops.bc_top, 0.0)
+    return np.concatenate([bot, ux, top], axis=0)
+
+
+def pad_v(v, ops):
+    """(ny + 5, nx + 4): padded [j + 2, i + 2] = v[j, i] (core.py:308-325)."""
+    if ops.periodic:
+        vp = v[:-1]
+        vp = np.concatenate([vp[-2:], vp, vp[:3]], axis=0)
+        return np.concatenate([vp[:, -2:], vp, vp[:, :2]], axis=1)
+    vy = np.concatenate([-v[1:3][::-1], v, -v[-3:-1][::-1]], axis=0)
+    if ops.closed:
+        sl = -1.0 if ops.bc_left == "noslip" else 1.0
+        sr = -1.0 if ops.bc_right == "noslip" else 1.0
+        T = v.dtype.type
+        return np.concatenate([T(sl) * vy[:, :2][:, ::-1], vy, T(sr) * vy[:, -2:][:, ::-1]], axis=1)
+    return np.concatenate([-vy[:, :2][:, ::-1], vy, np.repeat(vy[:, -1:], 2, axis=1)], axis=1)
+
+
+def inlet_outlet(u, ops):
+    """Inlet profile, outlet shifted so outflow = inflow (core.py:337-359)."""
+    u = u.copy()
+    if ops.closed:
+        u[:, 0] = 0
+        u[:, -1] = 0
+        return u
+    T = u.dtype.type
+    corr = (np.asarray(ops.u_inlet, dtype=u.dtype).sum(dtype=u.dtype) - u[:, -1].sum(dtype=u.dtype)) / T(ops.ny)
+    u[:, 0] = np.asarray(ops.u_inlet, dtype=u.dtype)
+    u[:, -1] = u[:, -1] + corr
+    return u
+
+
+def apply_boundary_values(u, v, ops):
+    """Dirichlet values and outlet balance; periodic duplicates (core.py:328-334)."""
+    if ops.periodic:
+        u = u.copy()
+        v = v.copy()
+        u[:, -1] = u[:, 0]
+        v[-1] = v[0]
+        return u, v
+    u = inlet_outlet(u, ops)
+    v = v.copy()
+    v[0] = 0
+    v[-1] = 0
+    return u, v
+
+
+# ---------------------------------------------------------------------------
+# right-hand side (core.py:366-613)
+# ---------------------------------------------------------------------------
+
+def advection_scale(ops):
+    return (7.0 / 24.0 if ops.advection == "upwind3" else 0.25) / ops.h       # core.py:369
+
+
+def advection2d(U, V, ops):
+    """-div(u u) at the u- and v-faces (core.py:366-383)."""
+    ny, nx = ops.ny, ops.nx
+    up = ops.advection == "upwind3"
+    k = U.dtype.type(advection_scale(ops))
+    fx = face_flux(None, U[2:-2, 0:nx + 2], U[2:-2, 1:nx + 3], U[2:-2, 2:nx + 4], U[2:-2, 3:nx + 5], up)
+    vs = V[2:ny + 3, 1:nx + 2] + V[2:ny + 3, 2:nx + 3]
+    gy = face_flux(vs, U[0:ny + 1, 2:-2], U[1:ny + 2, 2:-2], U[2:ny + 3, 2:-2], U[3:ny + 4, 2:-2], up)
+    au = (((fx[:, :-1] - fx[:, 1:]) + gy[:-1]) - gy[1:]) * k
+    us = U[1:ny + 2, 2:-2] + U[2:ny + 3, 2:-2]
+    fx = face_flux(us, V[2:-2, 0:nx + 1], V[2:-2, 1:nx + 2], V[2:-2, 2:nx + 3], V[2:-2, 3:nx + 4], up)
+    gy = face_flux(None, V[0:ny + 2, 2:-2], V[1:ny + 3, 2:-2], V[2:ny + 4, 2:-2], V[3:ny + 5, 2:-2], up)
+    av = (((fx[:, :-1] - fx[:, 1:]) + gy[:-1]) - gy[1:]) * k
+    return au, av
+
+
+def add_diffusion(acc, P, nu_h2):
+    """acc + nu / h^2 * 5-point Laplacian (core.py:417-424)."""
+    ring = (((P[2:-2, 3:-1] + P[2:-2, 1:-3]) + P[3:-1, 2:-2]) + P[1:-3, 2:-2])
+    ring = ring + P.dtype.type(-4.0) * P[2:-2, 2:-2]
+    return acc + ring * nu_h2
+
+
+def gradients2d(U, V, ops):
+    """(g11, g12, g21, g22) at cells -1..ny x -1..nx, shear at corners (core.py:427-444)."""
+    ny, nx = ops.ny, ops.nx
+    inv_h = U.dtype.type(1.0 / ops.h)
+    g11 = (U[1:ny + 3, 2:nx + 4] - U[1:ny + 3, 1:nx + 3]) * inv_h
+    g22 = (V[2:ny + 4, 1:nx + 3] - V[1:ny + 3, 1:nx + 3]) * inv_h
+    dudy = (U[1:ny + 4, 1:nx + 4] - U[0:ny + 3, 1:nx + 4]) * inv_h
+    dvdx = (V[1:ny + 4, 1:nx + 4] - V[1:ny + 4, 0:nx + 3]) * inv_h
+    q = U.dtype.type(0.25)
+
+    def avg(a):
+        return (((a[:-1, :-1] + a[1:, :-1]) + a[:-1, 1:]) + a[1:, 1:]) * q
+    return g11, avg(dudy), avg(dvdx), g22, dudy + dvdx
+
+
+def eddy_viscosity2d(g11, g12, g21, g22, ops):
+    """Smagorinsky / WALE / Vreman in 2D (core.py:469-500)."""
+    T = g11.dtype.type
+    delta2 = ops.h * ops.h
+    c = ops.les_c
+    s12 = T(0.5) * (g12 + g21)
+    ss = (g11 * g11 + g22 * g22) + T(2.0) * s12 * s12
+    if ops.turbulence == "smagorinsky":
+        return T(c * c * delta2) * np.sqrt(T(2.0) * ss + T(_SQRT_EPS))
+    if ops.turbulence == "wale":
+        q11 = g11 * g11 + g12 * g21
+        q22 = g21 * g12 + g22 * g22
+        q12 = T(0.5) * (((g11 * g12 + g12 * g22) + g21 * g11) + g22 * g21)
+        tr3 = (q11 + q22) * T(1.0 / 3.0)
+        sd = (((q11 - tr3) ** 2 + (q22 - tr3) ** 2) + T(2.0) * q12 * q12) + tr3 * tr3
+        num = np.maximum(sd, T(0)) ** T(1.5)
+        den = (np.maximum(ss, T(0)) ** T(2.5) + np.maximum(sd, T(0)) ** T(1.25)) + T(1e-30)
+        return T(c * c * delta2) * num / den
+    if ops.turbulence == "vreman":
+        b11 = g11 * g11 + g12 * g12
+        b22 = g21 * g21 + g22 * g22
+        b12 = g11 * g21 + g12 * g22
+        bb = np.maximum(b11 * b22 - b12 * b12, T(0))
+        aa = ((g11 * g11 + g12 * g12) + g21 * g21) + g22 * g22
+        return T(c * delta2) * np.sqrt(bb / (aa + T(1e-30)) + T(_SQRT_EPS))
+    raise ValueError(ops.turbulence)
+
+
+def sgs_divergence2d(U, V, geom, ops):
+    """div(2 nu_t S) at u- and v-faces and max nu_t (core.py:503-525)."""
+    ny, nx = ops.ny, ops.nx
+    T = U.dtype.type
+    inv_h = T(1.0 / ops.h)
+    g11, g12, g21, g22, shear_k = gradients2d(U, V, ops)
+    nut = eddy_viscosity2d(g11, g12, g21, g22, ops)
+    if not geom.empty:
+        j0, j1, i0, i1 = geom.window
+        nut = nut.copy()
+        nut[j0 + 1:j1 + 1, i0 + 1:i1 + 1] = nut[j0 + 1:j1 + 1, i0 + 1:i1 + 1] * (T(1.0) - geom.chi_c)
+    q = T(0.25)
+    nut_k = (((nut[:-1, :-1] + nut[1:, :-1]) + nut[:-1, 1:]) + nut[1:, 1:]) * q
+    txx = T(2.0) * nut[1:ny + 1] * g11[1:ny + 1]
+    tyy = T(2.0) * nut[:, 1:nx + 1] * g22[:, 1:nx + 1]
+    txy = nut_k * shear_k[1:ny + 2, 1:nx + 2]
+    fu = (((txx[:, 1:] - txx[:, :-1]) + txy[1:]) - txy[:-1]) * inv_h
+    fv = (((txy[:, 1:] - txy[:, :-1]) + tyy[1:]) - tyy[:-1]) * inv_h
+    return fu, fv, nut.max()
+
+
+def momentum_rhs2d(u, v, geom, ops):
+    """(Lu, Lv, nut_max) with the boundary rows / columns set (core.py:571-613)."""
+    T = u.dtype.type
+    U, V = pad_u(u, ops), pad_v(v, ops)
+    au, av = advection2d(U, V, ops)
+    nu_h2 = T(ops.nu) * T(1.0 / ops.h ** 2)
+    lu = add_diffusion(au, U, nu_h2)
+    lv = add_diffusion(av, V, nu_h2)
+    nut_max = None
+    if ops.turbulence != "none":
+        fu, fv, nut_max = sgs_divergence2d(U, V, geom, ops)
+        lu = lu + fu
+        lv = lv + fv
+    if ops.periodic:
+        return lu, lv, nut_max
+    lu = lu.copy()
+    lv = lv.copy()
+    lu[:, 0] = 0
+    lu[:, -1] = 0 if ops.closed else (u[:, -2] - u[:, -1]) * T(1.0 / ops.h)
+    lv[0] = 0
+    lv[-1] = 0
+    return lu, lv, nut_max
+
+
+# ---------------------------------------------------------------------------
+# projection, penalisation, time step (core.py:620-696)
+# ---------------------------------------------------------------------------
+
+def divergence2d(u, v, h):
+    """((u_{i+1} - u_i) + v_{j+1}) - v_j, over h (core.py:620-622)."""
+    return (((u[:, 1:] - u[:, :-1]) + v[1:]) - v[:-1]) * u.dtype.type(1.0 / h)
+
+
+class PoissonSolver2D:
+    """Exact ``L psi = f`` with zero mean (poisson.py:93-144), in the orthonormal DCT-II /
+    Hartley eigenbases (the same solution as the reference's packed real FFTs)."""
+
+    def __init__(self, nx, ny, h, periodic, dtype):
+        qx, lx = periodic_basis(nx) if periodic else neumann_basis(nx)
+        qy, ly = periodic_basis(ny) if periodic else neumann_basis(ny)
+        self.qx, self.qy = qx.astype(dtype), qy.astype(dtype)
+        lam = ly[:, None] / (h * h) + lx[None, :] / (h * h)
+        inv = np.where(lam != 0, 1.0 / np.where(lam != 0, lam, 1.0), 0.0)
+        inv[0, 0] = 0.0
+        self.inv_lam = inv.astype(dtype)
+
+    def solve(self, f):
+        a = f @ self.qx.T
+        a = self.qy @ a
+        a = a * self.inv_lam
+        a = self.qy.T @ a
+        return a @ self.qx
+
+    @staticmethod
+    def laplacian(psi, h, periodic):
+        """The discrete operator (poisson.py:136-144)."""
+        if periodic:
+            pe = np.concatenate([psi[:, -1:], psi, psi[:, :1]], axis=1)
+            pe = np.concatenate([pe[-1:], pe, pe[:1]], axis=0)
+        else:
+            pe = np.concatenate([psi[:, :1], psi, psi[:, -1:]], axis=1)
+            pe = np.concatenate([pe[:1], pe, pe[-1:]], axis=0)
+        return (pe[1:-1, 2:] + pe[1:-1, :-2] + pe[2:, 1:-1] + pe[:-2, 1:-1] - 4 * pe[1:-1, 1:-1]) / (h * h)
+
+
+def correct2d(u, v, psi, ops):
+    """u - grad psi; boundary-normal faces untouched (core.py:643-660)."""
+    T = psi.dtype.type
+    inv_h = T(1.0 / ops.h)
+    if ops.periodic:
+        gx = (psi - np.roll(psi, 1, axis=1)) * inv_h
+        gy = (psi - np.roll(psi, 1, axis=0)) * inv_h
+        return u - np.concatenate([gx, gx[:, :1]], axis=1), v - np.concatenate([gy, gy[:1]], axis=0)
+    gx = (psi[:, 1:] - psi[:, :-1]) * inv_h
+    gy = (psi[1:] - psi[:-1]) * inv_h
+    zc = np.zeros_like(psi[:, :1])
+    zr = np.zeros_like(psi[:1])
+    return u - np.concatenate([zc, gx, zc], axis=1), v - np.concatenate([zr, gy, zr], axis=0)
+
+
+def project2d(u, v, ops, poisson):
+    psi = poisson.solve(divergence2d(u, v, ops.h))
+    un, vn = correct2d(u, v, psi, ops)
+    return un, vn, psi
+
+
+def penalise2d(u, v, geom, ops, bdt):
+    """Implicit Brinkman on the window; returns (u, v, du, dv) (core.py:663-682)."""
+    T = u.dtype.type
+    j0, j1, i0, i1 = geom.window
+    k = bdt / T(ops.eta)
+    u = u.copy()
+    v = v.copy()
+    uw = u[j0:j1, i0:i1 + 1]
+    vw = v[j0:j1 + 1, i0:i1]
+    un = (uw + k * geom.a_u) / (T(1.0) + k * geom.chi_u)
+    vn = (vw + k * geom.a_v) / (T(1.0) + k * geom.chi_v)
+    du, dv = un - uw, vn - vw
+    u[j0:j1, i0:i1 + 1] = un
+    v[j0:j1 + 1, i0:i1] = vn
+    return u, v, du, dv
+
+
+def cfl_dt2d(u, v, ops, nut_max=None):
+    """min(cfl h / (max|u| + max|v|), 0.25 h^2 / (nu + max nu_t)) (core.py:685-696)."""
+    T = u.dtype.type
+    umax = max(np.abs(u).max() + np.abs(v).max(), T(1e-6))
+    dt = T(ops.cfl * ops.h) / umax
+    nu = T(ops.nu) if nut_max is None else T(ops.nu) + nut_max
+    return min(dt, T(0.25 * ops.h * ops.h) / nu)
+
+
+# ---------------------------------------------------------------------------
+# dye (core.py:703-735, 779-792)
+# ---------------------------------------------------------------------------
+
+def _van_leer(a, b):
+    ab = a * b
+    s = a + b
+    out = np.zeros_like(ab)
+    m = ab > 0
+    out[m] = a.dtype.type(2.0) * ab[m] / s[m]
+    return out
+
+
+def advect_dye2d(c, u, v, dt, ops):
+    """Forward-Euler MUSCL / van Leer step of the dye, cut below 1e-6, clamped at 1."""
+    T = c.dtype.type
+    if ops.periodic:
+        cx = np.concatenate([c[:, -2:], c, c[:, :2]], axis=1)
+        cy = np.concatenate([c[-2:], c, c[:2]], axis=0)
+    else:
+        inlet = np.asarray(ops.dye_inlet, dtype=c.dtype).reshape(-1, 1)
+        cx = np.concatenate([np.repeat(inlet, 2, axis=1), c, np.repeat(c[:, -1:], 2, axis=1)], axis=1)
+        cy = np.concatenate([np.repeat(c[:1], 2, axis=0), c, np.repeat(c[-1:], 2, axis=0)], axis=0)
+    half = T(0.5)
+    s = _van_leer(cx[:, 1:-1] - cx[:, :-2], cx[:, 2:] - cx[:, 1:-1])
+    left = cx[:, 1:-2] + half * s[:, :-1]
+    right = cx[:, 2:-1] - half * s[:, 1:]
+    fx = u * np.where(u > 0, left, right)
+    s = _van_leer(cy[1:-1] - cy[:-2], cy[2:] - cy[1:-1])
+    low = cy[1:-2] + half * s[:-1]
+    high = cy[2:-1] - half * s[1:]
+    fy = v * np.where(v > 0, low, high)
+    c = c - (dt * T(1.0 / ops.h)) * (((fx[:, 1:] - fx[:, :-1]) + fy[1:]) - fy[:-1])
+    c = np.where(c > T(DYE_ZERO), c, T(0))
+    return np.minimum(c, T(1.0))
+
+
+def zero_dye_in_solids(c, geom):
+    if geom.empty:
+        return c
+    c = c.copy()
+    j0, j1, i0, i1 = geom.window
+    c[j0:j1, i0:i1] = c[j0:j1, i0:i1] * (geom.chi_c <= 0.5).astype(c.dtype)
+    return c
+
+
+# ---------------------------------------------------------------------------
+# the step (core.py:815-969)
+# ---------------------------------------------------------------------------
+
+def force_coefficients2d(acc_u, acc_v, geom, ops, dt):
+    """[Cd, Cl, Cm] per body (core.py:943-949), reduced in float64."""
+    if geom.empty:
+        return np.zeros((geom.nbody, 3))
+    denom = float(dt * dt.dtype.type(0.5) * dt.dtype.type(ops.force_ref))
+    scale = -(ops.h * ops.h) / denom
+    ku = np.asarray(geom.k_u, np.float64)
+    kv = np.asarray(geom.k_v, np.float64)
+    ru = np.einsum("bkij,ij->bk", ku, np.asarray(acc_u, np.float64))
+    rv = np.einsum("bkij,ij->bk", kv, np.asarray(acc_v, np.float64))
+    return np.stack([ru[:, 0], rv[:, 0], ru[:, 1] + rv[:, 1]], axis=1) * scale
+
+
+@dataclass
+class StepResult2D:
+    u: np.ndarray
+    v: np.ndarray
+    p: np.ndarray
+    t: np.ndarray
+    dt: np.ndarray
+    coeffs: np.ndarray
+    dye: np.ndarray | None = None
+
+
+def step2d(u0, v0, t, geom, ops, poisson, *, dye=None, dt=None):
+    """One SSP-RK3 step (core.py:815-969 without placed physics)."""
+    T = u0.dtype.type
+    up, vp = u0, v0
+    acc_u = acc_v = psi_w = None
+    for s, ((a, b), w) in enumerate(zip(SSP_RK3, FORCE_WEIGHTS)):
+        lu, lv, nut_max = momentum_rhs2d(up, vp, geom, ops)
+        if s == 0 and dt is None:
+            dt = T(ops.dt_fixed) if ops.dt_fixed is not None else cfl_dt2d(u0, v0, ops, nut_max)
+        dt = T(dt)
+        bdt = dt * T(b)
+        if a == 0.0:
+            uh = up + lu * bdt
+            vh = vp + lv * bdt
+        else:
+            uh = lerp(up, u0, a) + lu * bdt
+            vh = lerp(vp, v0, a) + lv * bdt
+        if not ops.periodic:
+            uh = inlet_outlet(uh, ops)
+        if not geom.empty:
+            uh, vh, du, dv = penalise2d(uh, vh, geom, ops, bdt)
+            acc_u = du * T(w) if acc_u is None else acc_u + du * T(w)
+            acc_v = dv * T(w) if acc_v is None else acc_v + dv * T(w)
+            if ops.periodic:
+                uh, vh = apply_boundary_values(uh, vh, ops)
+        up, vp, psi = project2d(uh, vh, ops, poisson)
+        psi_w = psi * T(w) if psi_w is None else psi_w + T(w) * psi
+    p = psi_w * (T(1.0) / dt)
+    coeffs = force_coefficients2d(acc_u, acc_v, geom, ops, dt)
+    new_dye = None
+    if dye is not None:
+        new_dye = zero_dye_in_solids(advect_dye2d(dye, up, vp, dt, ops), geom)
+    return StepResult2D(up, vp, p, np.asarray(t + dt, dtype=u0.dtype), np.asarray(dt, dtype=u0.dtype), coeffs,
+                        new_dye)

@@ -45,3 +45,26 @@ def load_case(name):
     if "dye" in meta:
         src = DyeSources(tuple(meta["dye"]["window"]), arr["dye_weight"].astype(dt), tuple(meta["dye"]["pulse"]))
     return meta, ops, geom, th, src, arr
+
+
+CASES_2D = sorted(p.stem[len("ns2d_"):] for p in GOLDEN.glob("ns2d_*.npz"))
+
+
+def load_case2d(name):
+    from aerolume_b200.ns2d.types import Geometry2D, Ops2D
+    z = np.load(GOLDEN / f"ns2d_{name}.npz")
+    meta = json.loads(str(z["meta"]))
+    arr = {k: z[k] for k in z.files if k != "meta"}
+    dt = np.float64 if meta["dtype"] == "float64" else np.float32
+    ops = Ops2D(nx=meta["nx"], ny=meta["ny"], h=meta["h"], x0=meta["x0"], y0=meta["y0"], periodic=meta["periodic"],
+                closed=meta["closed"], bc_top=meta["bc_top"], bc_bottom=meta["bc_bottom"], bc_left=meta["bc_left"],
+                bc_right=meta["bc_right"], ground_speed=meta["ground_speed"], advection=meta["advection"],
+                turbulence=meta["turbulence"], les_c=meta["les_c"], nu=meta["nu"], eta=meta["eta"], cfl=meta["cfl"],
+                dt_fixed=meta["dt_fixed"], u_inlet=arr["u_inlet"].astype(dt),
+                dye_inlet=arr["dye_inlet"].astype(dt) if "dye_inlet" in arr else None,
+                force_ref=meta["force_ref"], moment_ref=tuple(meta["moment_ref"]), dtype=meta["dtype"])
+    geom = Geometry2D(tuple(meta["window"]), nbody=meta["nbody"])
+    if not geom.empty:
+        for n in ("chi_u", "chi_v", "chi_c", "a_u", "a_v", "k_u", "k_v"):
+            setattr(geom, n, arr[n].astype(dt))
+    return meta, ops, geom, arr

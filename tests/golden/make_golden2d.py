@@ -1,0 +1,164 @@
+"""Generate the golden vectors that pin the 2D oracle to the reference (run in the build container).
+
+Usage (the reference must be importable; it is read, never modified)::
+
+    PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden2d.py
+
+Each case builds a configuration with the reference's own 2D API (``SolverConfig``,
+``make_operators``, ``build_geometry``), starts from the reference's initial state plus seeded
+noise, imposes the boundary values and projects in FP64 (the pattern of the reference's
+tests/test_ns2d_core.py), then runs ``core.step_full`` on the CPU.  Every input the step reads
+and every output it returns is written to ``ns2d_<case>.npz`` beside this script; scalar
+parameters go into a JSON ``meta`` entry.  ``poisson2d.npz`` holds ``PoissonSolver.solve`` on
+seeded right-hand sides.  Nothing at test time needs the reference.
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+import sys
+from pathlib import Path
+
+import numpy as np
+import torch
+
+HERE = Path(__file__).resolve().parent
+REF = Path(os.environ.get("AEROLUME_REF", "/root/reference"))
+sys.path.insert(0, str(REF / "src"))
+
+from aerolume.solvers.ns2d import core  # noqa: E402
+from aerolume.solvers.ns2d.config import ImmersedBody, SolverConfig  # noqa: E402
+from aerolume.solvers.ns2d.geometry import build_geometry  # noqa: E402
+from aerolume.solvers.ns2d.poisson import PoissonSolver  # noqa: E402
+
+
+def circle(cx, cy, r, n):
+    a = 2.0 * math.pi * np.arange(n) / n
+    return np.stack([cx + r * np.cos(a), cy + r * np.sin(a)], axis=1)
+
+
+def square(cx, cy, s):
+    return np.array([[cx - s, cy - s], [cx + s, cy - s], [cx + s, cy + s], [cx - s, cy + s]])
+
+
+def _np(t):
+    return None if t is None else t.detach().cpu().numpy().copy()
+
+
+def extract(ops, geom):
+    meta = {
+        "nx": ops.nx, "ny": ops.ny, "h": ops.h, "x0": ops.x0, "y0": ops.y0, "periodic": bool(ops.periodic),
+        "closed": bool(ops.closed), "bc_top": ops.bc_top, "bc_bottom": ops.bc_bottom, "bc_left": ops.bc_left,
+        "bc_right": ops.bc_right, "ground_speed": float(ops.ground_speed), "advection": ops.advection,
+        "turbulence": ops.turbulence, "les_c": float(ops.les_c), "nu": float(ops.nu), "eta": float(ops.eta),
+        "cfl": float(ops.cfl), "dt_fixed": ops.dt_fixed, "force_ref": float(ops.force_ref),
+        "moment_ref": list(ops.moment_ref), "window": list(geom.window), "nbody": int(geom.nbody),
+        "dtype": "float64" if ops.dtype == torch.float64 else "float32",
+    }
+    arrays = {"u_inlet": _np(ops.u_inlet)[:, 0]}
+    if ops.dye_inlet is not None:
+        arrays["dye_inlet"] = _np(ops.dye_inlet)[:, 0]
+    if not geom.empty:
+        for name in ("chi_u", "chi_v", "chi_c", "a_u", "a_v", "k_u", "k_v"):
+            arrays[name] = _np(getattr(geom, name))
+    return meta, arrays
+
+
+def run_case(name, cfg_kw, *, dtype="float64", amp=0.1, seed=1, steps=1):
+    cfg64 = SolverConfig(**{**cfg_kw, "dtype": "float64", "device": "cpu", "perturb": False})
+    cfg = SolverConfig(**{**cfg_kw, "dtype": dtype, "device": "cpu", "perturb": False})
+    ops64 = core.make_operators(cfg64)
+    ops = core.make_operators(cfg)
+    geom = build_geometry(cfg.bodies, ops)
+    s64 = core.init_state(cfg64, ops64, perturb=False)
+    g = torch.Generator().manual_seed(seed)
+    u = s64.u + amp * torch.randn(s64.u.shape, generator=g, dtype=torch.float64)
+    v = s64.v + amp * torch.randn(s64.v.shape, generator=g, dtype=torch.float64)
+    u, v = core._apply_boundary_values(u, v, ops64)
+    u, v, _ = core.project(u, v, ops64)
+    tdt = ops.dtype
+    dye = None
+    if cfg.dye:
+        dye = torch.rand((cfg.ny, cfg.nx), generator=g, dtype=torch.float64)
+        dye[dye < 0.3] = 0.0
+        dye = dye.to(tdt)
+    zero = torch.zeros((), dtype=tdt)
+    state = core.State(u.to(tdt), v.to(tdt), torch.zeros(cfg.ny, cfg.nx, dtype=tdt), dye,
+                       torch.tensor(0.37, dtype=tdt), zero.clone())
+    meta, arrays = extract(ops, geom)
+    arrays.update({"in_u": _np(state.u), "in_v": _np(state.v), "in_t": _np(state.t)})
+    if dye is not None:
+        arrays["in_dye"] = _np(dye)
+    st = state
+    with torch.no_grad():
+        for k in range(steps):
+            st, coeffs = core.step_full(st, geom, ops)
+            if k == 0:
+                arrays.update({"out1_u": _np(st.u), "out1_v": _np(st.v), "out1_p": _np(st.p), "out1_t": _np(st.t),
+                               "out1_dt": _np(st.dt), "out1_coeffs": _np(coeffs)})
+                if st.dye is not None:
+                    arrays["out1_dye"] = _np(st.dye)
+    meta["steps"] = steps
+    if steps > 1:
+        arrays.update({"outN_u": _np(st.u), "outN_v": _np(st.v), "outN_p": _np(st.p), "outN_t": _np(st.t)})
+        if st.dye is not None:
+            arrays["outN_dye"] = _np(st.dye)
+    store = {k: (np.asarray(x, dtype=np.float32) if dtype == "float32" and np.asarray(x).dtype == np.float64
+                 else np.asarray(x)) for k, x in arrays.items()}
+    np.savez_compressed(HERE / f"ns2d_{name}.npz", meta=np.array(json.dumps(meta)), **store)
+    return meta
+
+
+def poisson_cases():
+    """Seeded right-hand sides and the reference's solutions (Neumann and periodic)."""
+    out = {}
+    g = torch.Generator().manual_seed(7)
+    shapes = [(7, 5), (8, 6), (12, 9), (16, 12), (20, 10), (32, 16)]
+    n = 0
+    for (nx, ny) in shapes:
+        for per in (False, True):
+            ps = PoissonSolver(nx, ny, 0.3, periodic=per, device=torch.device("cpu"), dtype=torch.float64)
+            f = torch.randn(ny, nx, generator=g, dtype=torch.float64)
+            f = f - f.mean()
+            out[f"f{n}"] = f.numpy()
+            out[f"psi{n}"] = ps.solve(f).numpy()
+            out[f"meta{n}"] = np.array([nx, ny, int(per)], dtype=np.int64)
+            n += 1
+    np.savez_compressed(HERE / "poisson2d.npz", h=np.array(0.3), count=np.array(n), **out)
+
+
+def main():
+    torch.set_num_threads(4)
+    # cylinder in a slip-walled tunnel (the shape of the 2D benchmark, coarser)
+    cyl = ImmersedBody(circle(2.0, 2.0, 0.5, 64), name="cylinder")
+    tunnel = {"nx": 64, "ny": 32, "h": 1.0 / 8.0, "x0": 0.0, "y0": 0.0, "re": 200.0, "bodies": [cyl],
+              "force_ref": 0.5, "moment_ref": (2.0, 2.0), "dye": True}
+    run_case("cylinder_upwind_f64", tunnel, dtype="float64", amp=0.05, seed=1, steps=3)
+    run_case("cylinder_upwind_f32", tunnel, dtype="float32", amp=0.05, seed=1, steps=3)
+    # periodic box, Smagorinsky, a spinning body
+    spin = ImmersedBody(square(1.0, 1.2, 0.3), name="spinner", omega=1.5, center=(1.0, 1.2))
+    run_case("periodic_smag_spin_f64", {"nx": 32, "ny": 24, "h": 2.5 / 32, "x0": 0.0, "y0": 0.0, "re": 800.0,
+                                        "bodies": [spin], "periodic": True, "turbulence": "smagorinsky",
+                                        "dye": True, "moment_ref": (1.0, 1.2)},
+             dtype="float64", amp=0.3, seed=2)
+    # closed cavity: moving bottom, slip left wall, WALE, a body
+    block = ImmersedBody(square(1.6, 1.0, 0.25), name="block")
+    run_case("closed_wale_f64", {"nx": 40, "ny": 24, "h": 0.1, "x0": 0.0, "y0": 0.0, "re": 2000.0,
+                                 "bodies": [block], "domain": "closed", "bc_bottom": "moving", "ground_speed": 1.0,
+                                 "bc_left": "slip", "bc_right": "noslip", "bc_top": "noslip",
+                                 "turbulence": "wale", "dye": True, "moment_ref": (1.6, 1.0)},
+             dtype="float64", amp=0.2, seed=3)
+    # no-slip top, moving floor, parabolic inlet, central advection, Vreman, two bodies
+    a = ImmersedBody(circle(1.2, 1.1, 0.3, 48), name="a")
+    b = ImmersedBody(square(2.3, 1.4, 0.22), name="b")
+    run_case("tunnel_two_bodies_vreman_f64", {"nx": 48, "ny": 24, "h": 0.1, "x0": 0.0, "y0": 0.0, "re": 500.0,
+                                              "bodies": [a, b], "inlet": "parabolic", "bc_top": "noslip",
+                                              "bc_bottom": "moving", "ground_speed": 0.5, "advection": "central",
+                                              "turbulence": "vreman", "dye": False, "moment_ref": (1.5, 1.0)},
+             dtype="float64", amp=0.05, seed=4)
+    poisson_cases()
+
+
+if __name__ == "__main__":
+    main()

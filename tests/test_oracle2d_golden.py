@@ -1,0 +1,62 @@
+"""The 2D oracle against golden vectors produced by the reference itself (make_golden2d.py)."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from _golden import CASES_2D, GOLDEN, load_case2d
+from oracle import ns2d as O2
+
+# float64: the restatement agrees with the reference to round-off; float32: to the FP32 step
+TOL = {"float64": 1e-12, "float32": 2e-6}
+
+
+def _rel(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
+
+
+def _run(name, steps=1):
+    meta, ops, geom, arr = load_case2d(name)
+    dt = np.float64 if meta["dtype"] == "float64" else np.float32
+    ps = O2.PoissonSolver2D(ops.nx, ops.ny, ops.h, ops.periodic, dt)
+    u, v, t = arr["in_u"], arr["in_v"], arr["in_t"]
+    dye = arr.get("in_dye")
+    outs = []
+    for _ in range(steps):
+        r = O2.step2d(u, v, t, geom, ops, ps, dye=dye)
+        outs.append(r)
+        u, v, t, dye = r.u, r.v, r.t, r.dye
+    return meta, arr, outs
+
+
+@pytest.mark.parametrize("name", CASES_2D)
+def test_oracle2d_one_step_matches_reference(name):
+    meta, arr, (r,) = _run(name)
+    tol = TOL[meta["dtype"]]
+    for k, got in (("u", r.u), ("v", r.v), ("p", r.p)):
+        assert _rel(got, arr[f"out1_{k}"]) < tol, (k, _rel(got, arr[f"out1_{k}"]))
+    assert _rel(r.dt, arr["out1_dt"]) < tol
+    assert _rel(r.t, arr["out1_t"]) < tol
+    if meta["nbody"]:
+        assert _rel(r.coeffs, arr["out1_coeffs"]) < (1e-10 if meta["dtype"] == "float64" else 1e-4)
+    if "out1_dye" in arr:
+        assert _rel(r.dye, arr["out1_dye"]) < tol
+
+
+@pytest.mark.parametrize("name", [c for c in CASES_2D if c.startswith("cylinder")])
+def test_oracle2d_three_steps_match_reference(name):
+    meta, arr, outs = _run(name, steps=3)
+    tol = 10 * TOL[meta["dtype"]]
+    r = outs[-1]
+    for k, got in (("u", r.u), ("v", r.v), ("p", r.p), ("dye", r.dye)):
+        assert _rel(got, arr[f"outN_{k}"]) < tol, (k, _rel(got, arr[f"outN_{k}"]))
+
+
+def test_poisson2d_matches_reference():
+    z = np.load(GOLDEN / "poisson2d.npz")
+    h = float(z["h"])
+    for n in range(int(z["count"])):
+        nx, ny, per = (int(x) for x in z[f"meta{n}"])
+        ps = O2.PoissonSolver2D(nx, ny, h, bool(per), np.float64)
+        assert _rel(ps.solve(z[f"f{n}"]), z[f"psi{n}"]) < 1e-12, n
