@@ -29,7 +29,9 @@ EXPORTS = ("aero_abi_version", "aero_last_error", "aero_ns3d_plan_create", "aero
            "aero_ns3d_workspace_bytes", "aero_ns3d_workspace_init", "aero_ns3d_step", "aero_ns3d_step_traced",
            "aero_ns3d_smoke",
            "aero_ns3d_poisson_solve",
-           "aero_ns3d_project", "aero_ns3d_read_status", "aero_debug_check", "aero_ns3d_poisson_solve_static")
+           "aero_ns3d_project", "aero_ns3d_read_status", "aero_debug_check", "aero_ns3d_poisson_solve_static",
+           "aero_ns2d_plan_create", "aero_ns2d_plan_destroy", "aero_ns2d_workspace_bytes",
+           "aero_ns2d_workspace_init", "aero_ns2d_step", "aero_ns2d_poisson_solve")
 
 
 class Ns3dConfig(C.Structure):
@@ -69,6 +71,27 @@ class Ns3dFields(C.Structure):
         "u", "v", "w", "p", "theta", "dye", "t", "dt", "coeffs", "heat_rate")]
 
 
+class Ns2dConfig(C.Structure):
+    _fields_ = [
+        ("abi_version", C.c_int32), ("dtype", C.c_int32), ("nx", C.c_int32), ("ny", C.c_int32),
+        ("h", C.c_double), ("periodic", C.c_int32), ("closed", C.c_int32),
+        ("advection", C.c_int32), ("les", C.c_int32), ("les_c", C.c_double),
+        ("nu", C.c_double), ("eta", C.c_double), ("cfl", C.c_double),
+        ("has_dt_fixed", C.c_int32), ("dt_fixed", C.c_double),
+        ("ghost_kind", ((C.c_int32 * 2) * 2) * 2), ("ghost_val", ((C.c_double * 2) * 2) * 2),
+        ("force_ref", C.c_double), ("window", C.c_int32 * 4), ("nbody", C.c_int32), ("dye", C.c_int32),
+    ]
+
+
+class Ns2dGeom(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in ("chi_u", "chi_v", "chi_c", "a_u", "a_v", "k_u", "k_v", "u_inlet",
+                                          "dye_inlet")]
+
+
+class Ns2dFields(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in ("u0", "v0", "t0", "dye0", "u", "v", "p", "t", "dt", "dye", "coeffs")]
+
+
 _LIB = None
 
 
@@ -102,11 +125,21 @@ def lib() -> C.CDLL:
     L.aero_ns3d_read_status.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_int32), C.c_void_p]
     L.aero_debug_check.argtypes = [C.POINTER(C.c_int64)]
     L.aero_ns3d_poisson_solve_static.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.aero_ns2d_plan_create.argtypes = [C.POINTER(Ns2dConfig), C.POINTER(C.c_void_p)]
+    L.aero_ns2d_plan_destroy.argtypes = [C.c_void_p]
+    L.aero_ns2d_plan_destroy.restype = None
+    L.aero_ns2d_workspace_bytes.argtypes = [C.c_void_p]
+    L.aero_ns2d_workspace_bytes.restype = C.c_size_t
+    L.aero_ns2d_workspace_init.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    L.aero_ns2d_step.argtypes = [C.c_void_p, C.POINTER(Ns2dFields), C.POINTER(Ns2dGeom), C.c_void_p, C.c_void_p,
+                                 C.c_void_p]
+    L.aero_ns2d_poisson_solve.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     L.aero_debug_check.restype = C.c_int
     for name in ("aero_ns3d_plan_create", "aero_ns3d_workspace_init", "aero_ns3d_step", "aero_ns3d_step_traced",
                  "aero_ns3d_smoke",
                  "aero_ns3d_poisson_solve",
-                 "aero_ns3d_project", "aero_ns3d_read_status", "aero_debug_check", "aero_ns3d_poisson_solve_static"):
+                 "aero_ns3d_project", "aero_ns3d_read_status", "aero_debug_check", "aero_ns3d_poisson_solve_static",
+                 "aero_ns2d_plan_create", "aero_ns2d_workspace_init", "aero_ns2d_step", "aero_ns2d_poisson_solve"):
         getattr(L, name).restype = C.c_int
     if L.aero_abi_version() != ABI_VERSION:
         raise RuntimeError(f"{LIB_PATH.name} has ABI {L.aero_abi_version()}, expected {ABI_VERSION}; rebuild it")

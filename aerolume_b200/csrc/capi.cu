@@ -7,6 +7,7 @@
 
 #include <cudaTypedefs.h>
 
+#include "host_common.cuh"
 #include "ns3d.cuh"
 
 #ifdef AERO_BOUNDS_CHECK
@@ -24,23 +25,17 @@ int fail(int code, const std::string &msg) {
   return code;
 }
 
+using aero_host::align_up;
+using aero_host::ALIGN;
+using aero_host::AxisInfo;
+using aero_host::factor;
+
 #define CUDA_TRY(expr)                                                                              \
   do {                                                                                              \
     cudaError_t e__ = (expr);                                                                       \
     if (e__ != cudaSuccess) return fail(AERO_ECUDA, std::string(#expr) + ": " + cudaGetErrorString(e__)); \
   } while (0)
 
-constexpr size_t ALIGN = 256;
-size_t align_up(size_t x) { return (x + ALIGN - 1) & ~(ALIGN - 1); }
-
-// radix sequence (4s, then 2, then 3s) for n = 2^a 3^b, else empty
-int factor(int n, int *fac) {
-  int k = 0;
-  while (n % 4 == 0) { fac[k++] = 4; n /= 4; }
-  while (n % 2 == 0) { fac[k++] = 2; n /= 2; }
-  while (n % 3 == 0) { fac[k++] = 3; n /= 3; }
-  return n == 1 ? k : -1;
-}
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link)
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
@@ -75,13 +70,9 @@ bool encode3d(CUtensorMap *m, bool f64, const void *base, size_t nx, size_t ny, 
   return r == CUDA_SUCCESS;
 }
 
-struct AxisInfo {
-  int n, kind, method, nfac, L;
-  int fac[16];
-  size_t off_tw, off_post, off_cs, off_lam, off_dense;
-};
-
 }  // namespace
+
+int aero_host::set_error(int code, const std::string &msg) { return fail(code, msg); }
 
 struct AeroNs3dPlan {
   AeroNs3dConfig cfg;
@@ -98,29 +89,14 @@ namespace {
 
 template <typename T>
 aero::AxisTables<T> axis_tables(const AeroNs3dPlan *p, int a, unsigned char *ws) {
-  const AxisInfo &x = p->ax[a];
-  aero::AxisTables<T> A{};
-  A.n = x.n;
-  A.method = x.method;
-  A.kind = x.kind;
-  A.nfac = x.nfac;
-  for (int i = 0; i < x.nfac; ++i) A.fac[i] = x.fac[i];
-  A.tw = reinterpret_cast<const T *>(ws + x.off_tw);
-  A.post = reinterpret_cast<const T *>(ws + x.off_post);
-  A.cs = reinterpret_cast<const T *>(ws + x.off_cs);
-  A.lam = reinterpret_cast<const double *>(ws + x.off_lam);
-  A.dense = x.method == 1 ? reinterpret_cast<const T *>(ws + x.off_dense) : nullptr;
-  A.s0 = T(std::sqrt(1.0 / x.n));
-  A.s1 = T(std::sqrt(2.0 / x.n));
-  A.rsqrt_n = T(1.0 / std::sqrt((double)x.n));
-  return A;
+  return aero_host::axis_view<T>(p->ax[a], ws);
 }
 
 // psi = L^{-1} f through five passes: x, y forward; z forward-solve-inverse; y, x inverse.
 // Every pass owns whole lines per block, so after the first pass the solve runs in place.
+// `fuse` (power-of-two x axes only) supplies the divergence fusion fields for the first
+// pass and the pressure-accumulation fields for the last one.
 template <typename T>
-// `fuse` (power-of-two x axes only, see fused_projection) supplies the divergence fusion
-// fields for the first pass and the pressure-accumulation fields for the last one.
 int poisson_passes(const AeroNs3dPlan *p, const T *f, T *psi, unsigned char *ws, cudaStream_t s,
                    const aero::TransformParams<T> *fuse = nullptr) {
   const AeroNs3dConfig &c = p->cfg;
@@ -571,13 +547,7 @@ int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom
 template <typename T>
 int init_impl(const AeroNs3dPlan *p, unsigned char *ws, cudaStream_t s) {
   CUDA_TRY(cudaMemsetAsync(ws, 0, p->total, s));
-  for (int a = 0; a < 3; ++a) {
-    const AxisInfo &x = p->ax[a];
-    CUDA_TRY(aero::launch_axis_tables<T>(x.n, x.kind, x.method == 1, p->cfg.h, reinterpret_cast<T *>(ws + x.off_tw),
-                                         reinterpret_cast<T *>(ws + x.off_post), reinterpret_cast<T *>(ws + x.off_cs),
-                                         reinterpret_cast<double *>(ws + x.off_lam),
-                                         x.method == 1 ? reinterpret_cast<T *>(ws + x.off_dense) : nullptr, s));
-  }
+  for (int a = 0; a < 3; ++a) CUDA_TRY(aero_host::axis_init<T>(p->ax[a], p->cfg.h, ws, s));
   return AERO_OK;
 }
 
@@ -660,15 +630,7 @@ size_t compact_tables(AeroNs3dPlan *q) {
     off += (bytes + ALIGN - 1) / ALIGN * ALIGN;
     return at;
   };
-  const size_t e = q->esz;
-  for (int a = 0; a < 3; ++a) {
-    AxisInfo &x = q->ax[a];
-    x.off_tw = take(2 * x.n * e);
-    x.off_post = take(2 * x.n * e);
-    x.off_cs = take(2 * x.n * e);
-    x.off_lam = take(sizeof(double) * x.n);
-    x.off_dense = take(x.method == 1 ? (size_t)x.n * x.n * e : 0);
-  }
+  for (int a = 0; a < 3; ++a) aero_host::axis_place(q->ax[a], q->esz, take);
   return off;
 }
 
@@ -683,14 +645,7 @@ int poisson_static_impl(const AeroNs3dPlan *plan, const void *f, void *psi, cuda
   unsigned char *scratch = nullptr;
   const int rc = static_scratch(&scratch);
   if (rc) return rc;
-  for (int a = 0; a < 3; ++a) {
-    const AxisInfo &x = q.ax[a];
-    CUDA_TRY(aero::launch_axis_tables<T>(x.n, x.kind, x.method == 1, q.cfg.h, reinterpret_cast<T *>(scratch + x.off_tw),
-                                         reinterpret_cast<T *>(scratch + x.off_post),
-                                         reinterpret_cast<T *>(scratch + x.off_cs),
-                                         reinterpret_cast<double *>(scratch + x.off_lam),
-                                         x.method == 1 ? reinterpret_cast<T *>(scratch + x.off_dense) : nullptr, s));
-  }
+  for (int a = 0; a < 3; ++a) CUDA_TRY(aero_host::axis_init<T>(q.ax[a], q.cfg.h, scratch, s));
   return poisson_passes<T>(&q, static_cast<const T *>(f), static_cast<T *>(psi), scratch, s);
 }
 
@@ -776,22 +731,8 @@ int aero_ns3d_plan_create(const AeroNs3dConfig *cfg, AeroNs3dPlan **plan) {
   const int ns[3] = {c.nx, c.ny, c.nz};
   for (int a = 0; a < 3; ++a) {
     AxisInfo &x = p->ax[a];
-    x.n = ns[a];
-    x.kind = c.periodic[a] ? 1 : 0;
-    x.nfac = factor(x.n, x.fac);
-    x.method = x.nfac < 0 ? 1 : 0;
-    if (x.nfac < 0) x.nfac = 0;
-    // lines per block: keep the tile (3 n L elements) within ~48 KiB, even, 2..64
-    int L = (int)((48 * 1024) / (3 * e * (size_t)x.n));
-    L = std::max(2, std::min(64, L));
-    L &= ~1;
-    if (x.method == 1) L = std::max(2, std::min(L, 16));
-    x.L = L;
-    x.off_tw = take(2 * x.n * e);
-    x.off_post = take(2 * x.n * e);
-    x.off_cs = take(2 * x.n * e);
-    x.off_lam = take(sizeof(double) * x.n);
-    x.off_dense = take(x.method == 1 ? (size_t)x.n * x.n * e : 0);
+    aero_host::axis_setup(x, ns[a], c.periodic[a] != 0, e);
+    aero_host::axis_place(x, e, take);
   }
   p->total = off;
   *plan = p;

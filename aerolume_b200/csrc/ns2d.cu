@@ -1,0 +1,775 @@
+// The 2D step of the C ABI: Aerolume ns2d/core.py:815-969 (step_full) without placed physics,
+// with the dye update of its lines 959-962.
+//
+// Arithmetic follows the reference's plain-torch step operation by operation, so float64
+// runs agree with it to round-off:
+//   ghosts     core.py:284-325     advection  core.py:366-383   diffusion core.py:417-424
+//   LES        core.py:427-525     boundaries core.py:571-613, 337-359
+//   penalty    core.py:663-682     projection core.py:620-660   dt        core.py:685-696
+//   dye        core.py:703-735, 779-792
+//
+// Layout: C-contiguous (y, x) arrays, u (ny, nx+1), v (ny+1, nx), cells (ny, nx).  One
+// launch per stage computes the tendencies of a 32 x 8 tile of u- and v-faces from shared-
+// memory tiles of the stage-start velocity (ghost values from the index maps of
+// common.cuh), the eddy viscosity and stresses of the tile's cells and corners, the RK
+// blend, the inlet / outlet balance, the implicit Brinkman penalisation and the bodies'
+// force partials.  The Poisson solve runs the transform kernels of poisson.cu on the grid
+// as (nz, ny, nx) = (ny, 1, nx): x forward, y forward-solve-inverse, x inverse.
+#include "host_common.cuh"
+#include "ns3d.cuh"
+#include "stencil.cuh"
+
+namespace aero {
+namespace ns2d {
+
+constexpr int TX = 32, TY = 8, NT = TX * TY;
+constexpr int UX = TX + 5, UY = TY + 4;  // u tile: faces i0-2 .. i0+TX+2, rows j0-2 .. j0+TY+1
+constexpr int VX = TX + 4, VY = TY + 5;  // v tile: columns i0-2 .. i0+TX+1, faces j0-2 .. j0+TY+2
+constexpr int CX = TX + 2, CY = TY + 2;  // cells i0-1 .. i0+TX, j0-1 .. j0+TY
+constexpr int KX = TX + 1, KY = TY + 1;  // corners i0 .. i0+TX, j0 .. j0+TY
+constexpr int MAXQ = 4 * AERO_MAX_BODIES;
+
+// Ghost rules of one component on its (n1, n0) = (y, x) array; rules compose x, then y.
+template <typename T>
+struct Rules2 {
+  int n0, n1, p0;  // entries along x and y (without a periodic duplicate), row pitch
+  int kind[2][2];
+  T val[2][2];
+};
+
+template <typename T>
+__device__ __forceinline__ T padded2(const T *__restrict__ f, const Rules2<T> &r, int j, int i) {
+  T sx, cx, sy, cy;
+  const int mi = ghost_map<T>(i, r.n0, r.kind[0][0], r.kind[0][1], r.val[0][0], r.val[0][1], sx, cx);
+  const int mj = ghost_map<T>(j, r.n1, r.kind[1][0], r.kind[1][1], r.val[1][0], r.val[1][1], sy, cy);
+  const T x = __ldg(f + (size_t)mj * r.p0 + mi);
+  return sy * (sx * x + cx) + cy;
+}
+
+// Eddy viscosity of the 2D gradient (core.py:469-500); cfac = c^2 h^2 (Smagorinsky, WALE)
+// or c h^2 (Vreman).
+template <typename T>
+__device__ __forceinline__ T eddy2d(T g11, T g12, T g21, T g22, int model, T cfac) {
+  const T s12 = T(0.5) * (g12 + g21);
+  const T ss = (g11 * g11 + g22 * g22) + T(2) * s12 * s12;
+  if (model == AERO_LES_SMAGORINSKY) return cfac * sqrt(T(2) * ss + T(1e-30));
+  if (model == AERO_LES_WALE) {
+    const T q11 = g11 * g11 + g12 * g21;
+    const T q22 = g21 * g12 + g22 * g22;
+    const T q12 = T(0.5) * (((g11 * g12 + g12 * g22) + g21 * g11) + g22 * g21);
+    const T tr3 = (q11 + q22) * T(1.0 / 3.0);
+    const T d1 = q11 - tr3, d2 = q22 - tr3;
+    const T sd = ((d1 * d1 + d2 * d2) + T(2) * q12 * q12) + tr3 * tr3;
+    const T sdp = sd > T(0) ? sd : T(0), ssp = ss > T(0) ? ss : T(0);
+    const T num = pow(sdp, T(1.5));
+    const T den = (pow(ssp, T(2.5)) + pow(sdp, T(1.25))) + T(1e-30);
+    return cfac * num / den;
+  }
+  // Vreman
+  const T b11 = g11 * g11 + g12 * g12;
+  const T b22 = g21 * g21 + g22 * g22;
+  const T b12 = g11 * g21 + g12 * g22;
+  T bb = b11 * b22 - b12 * b12;
+  bb = bb > T(0) ? bb : T(0);
+  const T aa = ((g11 * g11 + g12 * g12) + g21 * g21) + g22 * g22;
+  return cfac * sqrt(bb / (aa + T(1e-30)) + T(1e-30));
+}
+
+template <typename T>
+struct StageParams {
+  int nx, ny, periodic, closed, upwind, les;
+  T inv_h, kadv, nuh2, cfac;
+  Rules2<T> ru, rv;
+  const T *up, *vp, *u0, *v0;  // stage start, step start
+  T *uh, *vh;                  // stage value (after BCs and penalisation)
+  T a, b, w;                   // RK blend weight, tendency weight, force weight
+  const T *dt;
+  const T *u_inlet;
+  int has_win, win[4];         // j0, j1, i0, i1
+  const T *chi_u, *chi_v, *chi_c, *a_u, *a_v, *k_u, *k_v;
+  T eta;
+  int nbody;
+  double *partials;            // this stage's [block][4 nbody]
+  unsigned long long *nut_max; // nu-only pass: max nu_t (ordered bits)
+};
+
+// One RK stage of the u- and v-faces of a 32 x 8 tile; NU_ONLY: only the maximum eddy
+// viscosity of the tile's cells (the first stage's dt needs it before the update).
+template <typename T, bool NU_ONLY>
+__global__ void __launch_bounds__(NT) stage2d_kernel(const __grid_constant__ StageParams<T> P) {
+  __shared__ T U[UY][UX];
+  __shared__ T V[VY][VX];
+  __shared__ T NU[CY][CX], TXX[CY][CX], TYY[CY][CX];
+  __shared__ T TXY[KY][KX];
+  __shared__ double red[NT / 32][MAXQ];
+  __shared__ T corr_s;
+  const int nx = P.nx, ny = P.ny;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
+  const bool tunnel = !P.periodic && !P.closed;
+  const T dt = *P.dt;
+  const T bdt = dt * P.b;
+  // outlet balance (core.py:352-359): every block with outlet faces sums the whole outlet
+  // column of the stage value in the same fixed order, so all agree
+  if (!NU_ONLY && tunnel && i0 + TX >= nx && tid < 32) {
+    double s_in = 0.0, s_out = 0.0;
+    for (int j = tid; j < ny; j += 32) {
+      const T un = P.up[(size_t)j * (nx + 1) + nx];
+      const T lu = (P.up[(size_t)j * (nx + 1) + nx - 1] - un) * P.inv_h;
+      const T uo = P.a == T(0) ? un : lerp_t<T>(un, P.u0[(size_t)j * (nx + 1) + nx], P.a);
+      s_out += (double)(uo + lu * bdt);
+      s_in += (double)P.u_inlet[j];
+    }
+    s_in = warp_sum(s_in);
+    s_out = warp_sum(s_out);
+    if (tid == 0) corr_s = T((s_in - s_out) / (double)ny);
+  }
+  for (int e = tid; e < UY * UX; e += NT) {
+    const int r = e / UX, c = e - r * UX;
+    U[r][c] = padded2<T>(P.up, P.ru, j0 - 2 + r, i0 - 2 + c);
+  }
+  for (int e = tid; e < VY * VX; e += NT) {
+    const int r = e / VX, c = e - r * VX;
+    V[r][c] = padded2<T>(P.vp, P.rv, j0 - 2 + r, i0 - 2 + c);
+  }
+  __syncthreads();
+  // tile coordinates: u[j][i] -> U[j - j0 + 2][i - i0 + 2], v likewise in V
+  if (P.les) {
+    T mx = T(0);
+    const T q = T(0.25);
+    for (int e = tid; e < CY * CX; e += NT) {
+      const int r = e / CX, c = e - r * CX;  // cell (j0 - 1 + r, i0 - 1 + c)
+      const int jc = j0 - 1 + r, ic = i0 - 1 + c;
+      const int ju = r + 1, iu = c + 1;      // U / V index of u[jc][ic], v[jc][ic]
+      const T g11 = (U[ju][iu + 1] - U[ju][iu]) * P.inv_h;
+      const T g22 = (V[ju + 1][iu] - V[ju][iu]) * P.inv_h;
+      // du/dy and dv/dx at the corners (jc .. jc+1, ic .. ic+1), averaged in the
+      // reference's order: (c[j, i] + c[j+1, i]) + c[j, i+1] + c[j+1, i+1]
+      auto dudy = [&](int kr, int kc) { return (U[kr][kc] - U[kr - 1][kc]) * P.inv_h; };
+      auto dvdx = [&](int kr, int kc) { return (V[kr][kc] - V[kr][kc - 1]) * P.inv_h; };
+      const T g12 = (((dudy(ju, iu) + dudy(ju + 1, iu)) + dudy(ju, iu + 1)) + dudy(ju + 1, iu + 1)) * q;
+      const T g21 = (((dvdx(ju, iu) + dvdx(ju + 1, iu)) + dvdx(ju, iu + 1)) + dvdx(ju + 1, iu + 1)) * q;
+      T nu = eddy2d<T>(g11, g12, g21, g22, P.les, P.cfac);
+      if (P.has_win && jc >= P.win[0] && jc < P.win[1] && ic >= P.win[2] && ic < P.win[3]) {
+        const T chi = P.chi_c[(size_t)(jc - P.win[0]) * (P.win[3] - P.win[2]) + (ic - P.win[2])];
+        nu = nu * (T(1) - chi);
+      }
+      NU[r][c] = nu;
+      TXX[r][c] = T(2) * nu * g11;
+      TYY[r][c] = T(2) * nu * g22;
+      if (jc >= -1 && jc <= ny && ic >= -1 && ic <= nx) mx = (nu > mx || nu != nu) ? nu : mx;
+    }
+    if (NU_ONLY) {
+      block_max_atomic<T>(mx, P.nut_max);
+      return;
+    }
+    __syncthreads();
+    for (int e = tid; e < KY * KX; e += NT) {
+      const int r = e / KX, c = e - r * KX;  // corner (j0 + r, i0 + c)
+      const T nk = (((NU[r][c] + NU[r + 1][c]) + NU[r][c + 1]) + NU[r + 1][c + 1]) * q;
+      const int kr = r + 2, kc = c + 2;      // U / V index of the corner's u[j][i], v[j][i]
+      const T shear = (U[kr][kc] - U[kr - 1][kc]) * P.inv_h + (V[kr][kc] - V[kr][kc - 1]) * P.inv_h;
+      TXY[r][c] = nk * shear;
+    }
+    __syncthreads();
+  }
+  if (NU_ONLY) return;
+  const int j = j0 + ty, i = i0 + tx;
+  const bool in = j < ny && i < nx;
+  const T k_pen = bdt / P.eta;
+  const bool wblock = P.has_win && P.nbody > 0;
+  double fq[4] = {0.0, 0.0, 0.0, 0.0};  // this thread's force sums of body `bsel`
+  // ---- u-faces (j, i) and, for the last column, (j, nx)
+  auto u_face = [&](int fi, T &out, bool &pen, T &du, int &widx) {
+    const int r = j - j0 + 2, c = fi - i0 + 2;
+    const T *row = U[r];
+    const T fxl = face_flux<T>(row[c - 1] + row[c], row[c - 2], row[c - 1], row[c], row[c + 1], P.upwind != 0);
+    const T fxr = face_flux<T>(row[c] + row[c + 1], row[c - 1], row[c], row[c + 1], row[c + 2], P.upwind != 0);
+    const T vsb = V[r][c - 1] + V[r][c], vst = V[r + 1][c - 1] + V[r + 1][c];
+    const T gyb = face_flux<T>(vsb, U[r - 2][c], U[r - 1][c], U[r][c], U[r + 1][c], P.upwind != 0);
+    const T gyt = face_flux<T>(vst, U[r - 1][c], U[r][c], U[r + 1][c], U[r + 2][c], P.upwind != 0);
+    T lu = (((fxl - fxr) + gyb) - gyt) * P.kadv;
+    T ring = ((row[c + 1] + row[c - 1]) + U[r + 1][c]) + U[r - 1][c];
+    ring = ring + T(-4) * row[c];
+    lu = lu + ring * P.nuh2;
+    if (P.les) {
+      const int cc = fi - i0 + 1, cr = j - j0 + 1;  // cell fi in TXX, corner row j in TXY
+      lu = lu + (((TXX[cr][cc] - TXX[cr][cc - 1]) + TXY[cr][fi - i0]) - TXY[cr - 1][fi - i0]) * P.inv_h;
+    }
+    if (!P.periodic) {
+      if (fi == 0) lu = T(0);
+      if (fi == nx) lu = P.closed ? T(0) : (row[c - 1] - row[c]) * P.inv_h;
+    }
+    const T up = row[c];
+    const size_t g = (size_t)j * (nx + 1) + fi;
+    T uh = (P.a == T(0) ? up : lerp_t<T>(up, P.u0[g], P.a)) + lu * bdt;
+    if (!P.periodic) {
+      if (P.closed) {
+        if (fi == 0 || fi == nx) uh = T(0);
+      } else {
+        if (fi == 0) uh = P.u_inlet[j];
+        if (fi == nx) uh = uh + corr_s;
+      }
+    }
+    pen = false;
+    if (P.has_win && j >= P.win[0] && j < P.win[1] && fi >= P.win[2] && fi <= P.win[3]) {
+      widx = (j - P.win[0]) * (P.win[3] - P.win[2] + 1) + (fi - P.win[2]);
+      const T un = (uh + k_pen * P.a_u[widx]) / (T(1) + k_pen * P.chi_u[widx]);
+      du = un - uh;
+      uh = un;
+      pen = true;
+    }
+    out = uh;
+  };
+  auto v_face = [&](int fj, T &out, bool &pen, T &dv, int &widx) {
+    const int r = fj - j0 + 2, c = i - i0 + 2;
+    const T usl = U[r - 1][c] + U[r][c], usr = U[r - 1][c + 1] + U[r][c + 1];
+    const T *row = V[r];
+    const T fxl = face_flux<T>(usl, row[c - 2], row[c - 1], row[c], row[c + 1], P.upwind != 0);
+    const T fxr = face_flux<T>(usr, row[c - 1], row[c], row[c + 1], row[c + 2], P.upwind != 0);
+    const T gyb = face_flux<T>(V[r - 1][c] + V[r][c], V[r - 2][c], V[r - 1][c], V[r][c], V[r + 1][c], P.upwind != 0);
+    const T gyt = face_flux<T>(V[r][c] + V[r + 1][c], V[r - 1][c], V[r][c], V[r + 1][c], V[r + 2][c], P.upwind != 0);
+    T lv = (((fxl - fxr) + gyb) - gyt) * P.kadv;
+    T ring = ((row[c + 1] + row[c - 1]) + V[r + 1][c]) + V[r - 1][c];
+    ring = ring + T(-4) * row[c];
+    lv = lv + ring * P.nuh2;
+    if (P.les) {
+      const int cc = i - i0 + 1, cr = fj - j0 + 1;  // cell row fj in TYY, corner row fj in TXY
+      lv = lv + (((TXY[cr - 1][i - i0 + 1] - TXY[cr - 1][i - i0]) + TYY[cr][cc]) - TYY[cr - 1][cc]) * P.inv_h;
+    }
+    if (!P.periodic && (fj == 0 || fj == ny)) lv = T(0);
+    const T vp = row[c];
+    const size_t g = (size_t)fj * nx + i;
+    T vh = (P.a == T(0) ? vp : lerp_t<T>(vp, P.v0[g], P.a)) + lv * bdt;
+    pen = false;
+    if (P.has_win && fj >= P.win[0] && fj <= P.win[1] && i >= P.win[2] && i < P.win[3]) {
+      widx = (fj - P.win[0]) * (P.win[3] - P.win[2]) + (i - P.win[2]);
+      const T vn = (vh + k_pen * P.a_v[widx]) / (T(1) + k_pen * P.chi_v[widx]);
+      dv = vn - vh;
+      vh = vn;
+      pen = true;
+    }
+    out = vh;
+  };
+  // u faces of this thread: i, plus nx for the thread of i = nx - 1 (non-periodic)
+  T uv[2], du[2];
+  bool upen[2] = {false, false};
+  int uidx[2] = {0, 0}, nuf = 0;
+  T vv[2], dv[2];
+  bool vpen[2] = {false, false};
+  int vidx[2] = {0, 0}, nvf = 0;
+  if (in) {
+    // the last face of a row / column is computed everywhere; in a periodic domain its
+    // penalisation increment counts towards the force, but the face itself then takes the
+    // value of face 0 (core.py:330-331, 923-924)
+    u_face(i, uv[0], upen[0], du[0], uidx[0]);
+    nuf = 1;
+    if (i == nx - 1) {
+      u_face(nx, uv[1], upen[1], du[1], uidx[1]);
+      nuf = 2;
+    }
+    v_face(j, vv[0], vpen[0], dv[0], vidx[0]);
+    nvf = 1;
+    if (j == ny - 1) {
+      v_face(ny, vv[1], vpen[1], dv[1], vidx[1]);
+      nvf = 2;
+    }
+    P.uh[(size_t)j * (nx + 1) + i] = uv[0];
+    if (nuf == 2 && !P.periodic) P.uh[(size_t)j * (nx + 1) + nx] = uv[1];
+    if (P.periodic && i == 0) P.uh[(size_t)j * (nx + 1) + nx] = uv[0];
+    P.vh[(size_t)j * nx + i] = vv[0];
+    if (nvf == 2 && !P.periodic) P.vh[(size_t)ny * nx + i] = vv[1];
+    if (P.periodic && j == 0) P.vh[(size_t)ny * nx + i] = vv[0];
+  }
+  // ---- force partials of the bodies (core.py:943-949): per warp, then per block in order
+  if (wblock) {
+    const int warp = tid >> 5, lane = tid & 31;
+    const T wq = P.w;
+    const int wx = P.win[3] - P.win[2], wy = P.win[1] - P.win[0];
+    const size_t su = (size_t)wy * (wx + 1), sv = (size_t)(wy + 1) * wx;
+    for (int b = 0; b < P.nbody; ++b) {
+      fq[0] = fq[1] = fq[2] = fq[3] = 0.0;
+      for (int q = 0; q < nuf; ++q)
+        if (upen[q]) {
+          const double d = (double)(du[q] * wq);
+          fq[0] += (double)P.k_u[(size_t)(2 * b) * su + uidx[q]] * d;
+          fq[1] += (double)P.k_u[(size_t)(2 * b + 1) * su + uidx[q]] * d;
+        }
+      for (int q = 0; q < nvf; ++q)
+        if (vpen[q]) {
+          const double d = (double)(dv[q] * wq);
+          fq[2] += (double)P.k_v[(size_t)(2 * b) * sv + vidx[q]] * d;
+          fq[3] += (double)P.k_v[(size_t)(2 * b + 1) * sv + vidx[q]] * d;
+        }
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const double s = warp_sum(fq[q]);
+        if (lane == 0) red[warp][4 * b + q] = s;
+      }
+    }
+    __syncthreads();
+    const int nq = 4 * P.nbody;
+    if (tid < nq) {
+      double s = 0.0;
+      for (int wv = 0; wv < NT / 32; ++wv) s += red[wv][tid];
+      P.partials[(size_t)(blockIdx.y * gridDim.x + blockIdx.x) * nq + tid] = s;
+    }
+  }
+}
+
+// u <- uh - grad psi (core.py:643-660); one thread per cell column, the thread of the last
+// column also does the last u-face and the thread of the last row the last v-face
+template <typename T>
+__global__ void correct2d_kernel(int nx, int ny, int periodic, T inv_h, const T *__restrict__ uh,
+                                 const T *__restrict__ vh, const T *__restrict__ psi, T *__restrict__ u,
+                                 T *__restrict__ v) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+  if (i >= nx || j >= ny) return;
+  const size_t c = (size_t)j * nx;
+  for (int fi = i; fi <= (i == nx - 1 ? nx : i); ++fi) {
+    const size_t e = (size_t)j * (nx + 1) + fi;
+    T val;
+    if (periodic) {
+      const int ii = fi == nx ? 0 : fi, il = ii == 0 ? nx - 1 : ii - 1;
+      val = uh[e] - (psi[c + ii] - psi[c + il]) * inv_h;
+    } else if (fi == 0 || fi == nx) {
+      val = uh[e];
+    } else {
+      val = uh[e] - (psi[c + fi] - psi[c + fi - 1]) * inv_h;
+    }
+    u[e] = val;
+  }
+  for (int fj = j; fj <= (j == ny - 1 ? ny : j); ++fj) {
+    const size_t e = (size_t)fj * nx + i;
+    T val;
+    if (periodic) {
+      const int jj = fj == ny ? 0 : fj, jl = jj == 0 ? ny - 1 : jj - 1;
+      val = vh[e] - (psi[(size_t)jj * nx + i] - psi[(size_t)jl * nx + i]) * inv_h;
+    } else if (fj == 0 || fj == ny) {
+      val = vh[e];
+    } else {
+      val = vh[e] - (psi[(size_t)fj * nx + i] - psi[(size_t)(fj - 1) * nx + i]) * inv_h;
+    }
+    v[e] = val;
+  }
+}
+
+// ((u_{i+1} - u_i) + v_{j+1}) - v_j, over h (core.py:620-622)
+template <typename T>
+__global__ void divergence2d_kernel(int nx, int ny, T inv_h, const T *__restrict__ u, const T *__restrict__ v,
+                                    T *__restrict__ div) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+  if (i >= nx || j >= ny) return;
+  const size_t ru = (size_t)j * (nx + 1);
+  div[(size_t)j * nx + i] =
+      (((u[ru + i + 1] - u[ru + i]) + v[(size_t)(j + 1) * nx + i]) - v[(size_t)j * nx + i]) * inv_h;
+}
+
+template <typename T>
+struct DyeParams {
+  int nx, ny, periodic;
+  T inv_h;
+  const T *c0, *u, *v, *dt, *inlet;  // inlet may be NULL (zeros)
+  T *c;
+  int has_win, win[4];
+  const T *chi_c;
+};
+
+template <typename T>
+__device__ __forceinline__ T dye2d_at(const DyeParams<T> &P, int j, int i) {
+  // ghosts of core.py:716-721: inlet comb / zero-gradient outlet in x, zero gradient in y
+  if (P.periodic) {
+    i = i < 0 ? i + P.nx : (i >= P.nx ? i - P.nx : i);
+    j = j < 0 ? j + P.ny : (j >= P.ny ? j - P.ny : j);
+  } else {
+    j = j < 0 ? 0 : (j >= P.ny ? P.ny - 1 : j);
+    if (i < 0) return P.inlet ? P.inlet[j] : T(0);
+    if (i >= P.nx) i = P.nx - 1;
+  }
+  return __ldg(P.c0 + (size_t)j * P.nx + i);
+}
+
+// One forward-Euler MUSCL / van Leer step of the dye (core.py:703-735), cut below 1e-6,
+// clamped at 1, zero inside solids (core.py:779-792)
+template <typename T>
+__global__ void dye2d_kernel(const __grid_constant__ DyeParams<T> P) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+  const int nx = P.nx, ny = P.ny;
+  if (i >= nx || j >= ny) return;
+  auto C = [&](int dj, int di) { return dye2d_at<T>(P, j + dj, i + di); };
+  const T c = C(0, 0);
+  const T fx0 = muscl_flux<T>(C(0, -2), C(0, -1), c, C(0, 1), P.u[(size_t)j * (nx + 1) + i]);
+  const T fx1 = muscl_flux<T>(C(0, -1), c, C(0, 1), C(0, 2), P.u[(size_t)j * (nx + 1) + i + 1]);
+  const T fy0 = muscl_flux<T>(C(-2, 0), C(-1, 0), c, C(1, 0), P.v[(size_t)j * nx + i]);
+  const T fy1 = muscl_flux<T>(C(-1, 0), c, C(1, 0), C(2, 0), P.v[(size_t)(j + 1) * nx + i]);
+  T out = c - (*P.dt * P.inv_h) * (((fx1 - fx0) + fy1) - fy0);
+  out = out > T(1e-6) ? out : T(0);
+  out = out < T(1) ? out : T(1);
+  if (P.has_win && j >= P.win[0] && j < P.win[1] && i >= P.win[2] && i < P.win[3]) {
+    const T chi = P.chi_c[(size_t)(j - P.win[0]) * (P.win[3] - P.win[2]) + (i - P.win[2])];
+    out = out * (chi <= T(0.5) ? T(1) : T(0));
+  }
+  P.c[(size_t)j * nx + i] = out;
+}
+
+// dt (core.py:685-696): 0 CFL / viscous rule from the maxima, 1 fixed, 2 copied from dt_in
+template <typename T>
+__global__ void dt2d_kernel(int mode, const T *dt_in, double dt_fixed, const unsigned long long *bits, double cfl_h,
+                            double nu, double visc_h2, int les, T *dt_out) {
+  T dt;
+  if (mode == 2) {
+    dt = *dt_in;
+  } else if (mode == 1) {
+    dt = T(dt_fixed);
+  } else {
+    T umax = T(as_double(bits[SC_MAXU])) + T(as_double(bits[SC_MAXV]));
+    umax = umax > T(1e-6) || umax != umax ? umax : T(1e-6);
+    dt = T(cfl_h) / umax;
+    const T nut = les ? T(nu) + T(as_double(bits[SC_NUTMAX])) : T(nu);
+    const T dv = T(visc_h2) / nut;
+    dt = dv < dt ? dv : dt;
+  }
+  *dt_out = dt;
+}
+
+// Coefficients [Cd, Cl, Cm] per body from the stage partials in a fixed order, t + dt, dt
+template <typename T>
+__global__ void finalize2d_kernel(const double *__restrict__ partials, int nblocks, int nbody, double h,
+                                  double force_ref, const T *dt, const T *t0, T *t_out, T *dt_out, T *coeffs) {
+  __shared__ double tot[MAXQ];
+  const int nq = 4 * nbody;
+  for (int q = threadIdx.x >> 5; q < nq; q += blockDim.x >> 5) {
+    double s = 0.0;
+    for (int e = threadIdx.x & 31; e < 3 * nblocks; e += 32) s += partials[(size_t)e * nq + q];
+    s = warp_sum(s);
+    if ((threadIdx.x & 31) == 0) tot[q] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const T d = *dt;
+    *t_out = *t0 + d;
+    *dt_out = d;
+    const double denom = (double)((d * T(0.5)) * T(force_ref));
+    const double scale = -(h * h) / denom;
+    for (int b = 0; b < nbody; ++b) {
+      coeffs[3 * b + 0] = T(tot[4 * b + 0] * scale);
+      coeffs[3 * b + 1] = T(tot[4 * b + 2] * scale);
+      coeffs[3 * b + 2] = T((tot[4 * b + 1] + tot[4 * b + 3]) * scale);
+    }
+  }
+}
+
+}  // namespace ns2d
+}  // namespace aero
+
+// ---------------------------------------------------------------------------------------
+// plan and C ABI
+// ---------------------------------------------------------------------------------------
+
+using aero_host::AxisInfo;
+
+struct AeroNs2dPlan {
+  AeroNs2dConfig cfg;
+  size_t esz;
+  size_t nu, nv, nc;          // element counts of u, v and cells
+  size_t off_uh, off_vh, off_up, off_vp, off_pa, off_small, off_scalars, off_zero, off_partials, total;
+  AxisInfo ax[2];             // x (n = nx), y (n = ny)
+  int gx, gy, nblocks, nq;
+};
+
+namespace {
+
+using aero_host::set_error;
+
+template <typename T>
+aero::ns2d::Rules2<T> rules2(const AeroNs2dConfig &c, int comp) {
+  aero::ns2d::Rules2<T> r{};
+  r.n0 = c.nx + (comp == 0 && !c.periodic);
+  r.n1 = c.ny + (comp == 1 && !c.periodic);
+  r.p0 = c.nx + (comp == 0);
+  for (int a = 0; a < 2; ++a)
+    for (int s = 0; s < 2; ++s) {
+      r.kind[a][s] = c.ghost_kind[comp][a][s];
+      r.val[a][s] = T(c.ghost_val[comp][a][s]);
+    }
+  return r;
+}
+
+// psi = L^{-1} f: x forward, y forward-solve-inverse, x inverse on the (ny, 1, nx) view
+template <typename T>
+int poisson2d_passes(const AeroNs2dPlan *p, const T *f, T *psi, unsigned char *ws, cudaStream_t s,
+                     const aero::TransformParams<T> *fuse = nullptr) {
+  const AeroNs2dConfig &c = p->cfg;
+  const int axes[3] = {0, 2, 0}, modes[3] = {0, 2, 1};
+  for (int q = 0; q < 3; ++q) {
+    aero::TransformParams<T> P{};
+    if (fuse && q == 0) {
+      P.fuse_div = fuse->fuse_div;
+      P.uh = fuse->uh;
+      P.vh = fuse->vh;
+      P.inv_h = fuse->inv_h;
+    }
+    if (fuse && q == 2) {
+      P.p_acc = fuse->p_acc;
+      P.wgt = fuse->wgt;
+      P.acc_mode = fuse->acc_mode;
+      P.dt = fuse->dt;
+    }
+    P.nx = c.nx;
+    P.ny = 1;
+    P.nz = c.ny;
+    P.lam_x = reinterpret_cast<const double *>(ws + p->ax[0].off_lam);
+    P.lam_y = reinterpret_cast<const double *>(ws + p->off_zero);
+    P.axis = axes[q];
+    P.mode = modes[q];
+    P.in = q == 0 ? f : psi;
+    P.out = psi;
+    const AxisInfo &x = p->ax[axes[q] == 0 ? 0 : 1];
+    P.L = x.L;
+    P.A = aero_host::axis_view<T>(x, ws);
+    AERO_CUDA_TRY(aero::launch_transform<T>(P, s));
+  }
+  return AERO_OK;
+}
+
+template <typename T>
+int init2d_impl(const AeroNs2dPlan *p, unsigned char *ws, cudaStream_t s) {
+  AERO_CUDA_TRY(cudaMemsetAsync(ws, 0, p->total, s));
+  for (int a = 0; a < 2; ++a) AERO_CUDA_TRY(aero_host::axis_init<T>(p->ax[a], p->cfg.h, ws, s));
+  return AERO_OK;
+}
+
+template <typename T>
+int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGeom *g, const void *dt_in,
+                unsigned char *ws, cudaStream_t s) {
+  using namespace aero::ns2d;
+  const AeroNs2dConfig &c = p->cfg;
+  const int nx = c.nx, ny = c.ny;
+  const T *u0 = static_cast<const T *>(f->u0), *v0 = static_cast<const T *>(f->v0);
+  T *uh = reinterpret_cast<T *>(ws + p->off_uh), *vh = reinterpret_cast<T *>(ws + p->off_vh);
+  T *upb = reinterpret_cast<T *>(ws + p->off_up), *vpb = reinterpret_cast<T *>(ws + p->off_vp);
+  T *pa = reinterpret_cast<T *>(ws + p->off_pa);
+  T *small = reinterpret_cast<T *>(ws + p->off_small);
+  double *sc = reinterpret_cast<double *>(ws + p->off_scalars);
+  auto *bits = reinterpret_cast<unsigned long long *>(sc);
+  double *partials = reinterpret_cast<double *>(ws + p->off_partials);
+  const bool has_win = c.nbody > 0 && c.window[1] > c.window[0] && c.window[3] > c.window[2];
+  const bool les = c.les != AERO_LES_NONE;
+  // ---- dt
+  int dt_mode = dt_in ? 2 : (c.has_dt_fixed ? 1 : 0);
+  StageParams<T> S{};
+  S.nx = nx;
+  S.ny = ny;
+  S.periodic = c.periodic;
+  S.closed = c.closed;
+  S.upwind = c.advection == AERO_ADV_UPWIND3;
+  S.les = les ? c.les : 0;
+  S.inv_h = T(1.0 / c.h);
+  S.kadv = T((c.advection == AERO_ADV_UPWIND3 ? 7.0 / 24.0 : 0.25) / c.h);
+  S.nuh2 = T(c.nu) * T(1.0 / (c.h * c.h));
+  S.cfac = T(c.les == AERO_LES_VREMAN ? c.les_c * c.h * c.h : c.les_c * c.les_c * c.h * c.h);
+  S.ru = rules2<T>(c, 0);
+  S.rv = rules2<T>(c, 1);
+  S.u0 = u0;
+  S.v0 = v0;
+  S.uh = uh;
+  S.vh = vh;
+  S.dt = small;
+  S.u_inlet = static_cast<const T *>(g->u_inlet);
+  S.has_win = has_win;
+  for (int q = 0; q < 4; ++q) S.win[q] = c.window[q];
+  S.chi_u = static_cast<const T *>(g->chi_u);
+  S.chi_v = static_cast<const T *>(g->chi_v);
+  S.chi_c = static_cast<const T *>(g->chi_c);
+  S.a_u = static_cast<const T *>(g->a_u);
+  S.a_v = static_cast<const T *>(g->a_v);
+  S.k_u = static_cast<const T *>(g->k_u);
+  S.k_v = static_cast<const T *>(g->k_v);
+  S.eta = T(c.eta);
+  S.nbody = has_win ? c.nbody : 0;
+  const dim3 grid(p->gx, p->gy), block(TX, TY);
+  if (dt_mode == 0) {
+    AERO_CUDA_TRY(cudaMemsetAsync(sc, 0, 8 * sizeof(double), s));
+    AERO_CUDA_TRY(aero::launch_absmax<T>(u0, p->nu, bits + aero::SC_MAXU, s));
+    AERO_CUDA_TRY(aero::launch_absmax<T>(v0, p->nv, bits + aero::SC_MAXV, s));
+    if (les) {
+      StageParams<T> N = S;
+      N.up = u0;
+      N.vp = v0;
+      N.nut_max = bits + aero::SC_NUTMAX;
+      stage2d_kernel<T, true><<<grid, block, 0, s>>>(N);
+      AERO_CUDA_TRY(cudaGetLastError());
+    }
+  }
+  dt2d_kernel<T><<<1, 1, 0, s>>>(dt_mode, static_cast<const T *>(dt_in), c.dt_fixed, bits, c.cfl * c.h, c.nu,
+                                 0.25 * c.h * c.h, les ? 1 : 0, small);
+  AERO_CUDA_TRY(cudaGetLastError());
+  // ---- stages
+  static const double RK[3][3] = {{0.0, 1.0, 1.0 / 6.0}, {0.75, 0.25, 2.0 / 3.0}, {1.0 / 3.0, 2.0 / 3.0, 1.0}};
+  T *p_out = static_cast<T *>(f->p);
+  const bool fused = p->ax[0].method == 0 && aero::transform_pow2(nx);
+  for (int st = 0; st < 3; ++st) {
+    StageParams<T> P = S;
+    P.up = st == 0 ? u0 : upb;
+    P.vp = st == 0 ? v0 : vpb;
+    P.a = T(RK[st][0]);
+    P.b = T(RK[st][1]);
+    P.w = T(RK[st][2]);
+    P.partials = partials + (size_t)st * p->nblocks * std::max(p->nq, 1);
+    stage2d_kernel<T, false><<<grid, block, 0, s>>>(P);
+    AERO_CUDA_TRY(cudaGetLastError());
+    const int acc_mode = st == 0 ? 0 : (st == 1 ? 1 : 2);
+    if (fused) {
+      aero::TransformParams<T> F{};
+      F.fuse_div = 2;
+      F.uh = uh;
+      F.vh = vh;
+      F.inv_h = T(1.0 / c.h);
+      F.p_acc = p_out;
+      F.wgt = T(RK[st][2]);
+      F.acc_mode = acc_mode;
+      F.dt = small;
+      const int rc = poisson2d_passes<T>(p, nullptr, pa, ws, s, &F);
+      if (rc) return rc;
+    } else {
+      divergence2d_kernel<T><<<dim3((nx + 127) / 128, ny), 128, 0, s>>>(nx, ny, T(1.0 / c.h), uh, vh, pa);
+      AERO_CUDA_TRY(cudaGetLastError());
+      const int rc = poisson2d_passes<T>(p, pa, pa, ws, s);
+      if (rc) return rc;
+      AERO_CUDA_TRY(aero::launch_psi_accumulate<T>(pa, p_out, p->nc, T(RK[st][2]), acc_mode, small, s));
+    }
+    T *uo = st == 2 ? static_cast<T *>(f->u) : upb;
+    T *vo = st == 2 ? static_cast<T *>(f->v) : vpb;
+    correct2d_kernel<T><<<dim3((nx + 127) / 128, ny), 128, 0, s>>>(nx, ny, c.periodic, T(1.0 / c.h), uh, vh, pa, uo, vo);
+    AERO_CUDA_TRY(cudaGetLastError());
+  }
+  // ---- dye with the step's final velocity
+  if (c.dye) {
+    DyeParams<T> D{};
+    D.nx = nx;
+    D.ny = ny;
+    D.periodic = c.periodic;
+    D.inv_h = T(1.0 / c.h);
+    D.c0 = static_cast<const T *>(f->dye0);
+    D.u = static_cast<const T *>(f->u);
+    D.v = static_cast<const T *>(f->v);
+    D.dt = small;
+    D.inlet = static_cast<const T *>(g->dye_inlet);
+    D.c = static_cast<T *>(f->dye);
+    D.has_win = has_win;
+    for (int q = 0; q < 4; ++q) D.win[q] = c.window[q];
+    D.chi_c = static_cast<const T *>(g->chi_c);
+    dye2d_kernel<T><<<dim3((nx + 127) / 128, ny), 128, 0, s>>>(D);
+    AERO_CUDA_TRY(cudaGetLastError());
+  }
+  finalize2d_kernel<T><<<1, 256, 0, s>>>(partials, p->nblocks, S.nbody, c.h, c.force_ref, small,
+                                         static_cast<const T *>(f->t0), static_cast<T *>(f->t),
+                                         static_cast<T *>(f->dt), static_cast<T *>(f->coeffs));
+  AERO_CUDA_TRY(cudaGetLastError());
+  return AERO_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int aero_ns2d_plan_create(const AeroNs2dConfig *cfg, AeroNs2dPlan **plan) {
+  if (!cfg || !plan) return set_error(AERO_EINVAL, "null argument");
+  *plan = nullptr;
+  const AeroNs2dConfig &c = *cfg;
+  if (c.abi_version != AERO_ABI_VERSION) return set_error(AERO_EINVAL, "ABI version mismatch");
+  if (c.dtype != AERO_F32 && c.dtype != AERO_F64) return set_error(AERO_EINVAL, "dtype must be float32 or float64");
+  if (c.nx < 4 || c.ny < 4) return set_error(AERO_EINVAL, "the grid needs at least 4 x 4 cells");
+  if (!(c.h > 0) || !std::isfinite(c.h)) return set_error(AERO_EINVAL, "cell size h must be positive");
+  if (c.periodic && c.closed) return set_error(AERO_EINVAL, "a periodic domain cannot also be closed");
+  if (c.advection != AERO_ADV_UPWIND3 && c.advection != AERO_ADV_CENTRAL) return set_error(AERO_EINVAL, "unknown advection");
+  if (c.les < AERO_LES_NONE || c.les > AERO_LES_VREMAN) return set_error(AERO_EINVAL, "unknown turbulence model");
+  if (c.nbody < 0 || c.nbody > AERO_MAX_BODIES)
+    return set_error(AERO_EUNSUPPORTED, "at most " + std::to_string(AERO_MAX_BODIES) + " bodies");
+  for (int q = 0; q < 2; ++q)
+    for (int a = 0; a < 2; ++a)
+      for (int s = 0; s < 2; ++s)
+        if (c.ghost_kind[q][a][s] < AERO_GHOST_EDGE || c.ghost_kind[q][a][s] > AERO_GHOST_PERIODIC_FACE)
+          return set_error(AERO_EINVAL, "unknown ghost rule");
+  const bool has_win = c.window[1] > c.window[0] && c.window[3] > c.window[2];
+  if (has_win && (c.window[0] < 0 || c.window[1] > c.ny || c.window[2] < 0 || c.window[3] > c.nx))
+    return set_error(AERO_EINVAL, "body window outside the domain");
+  if (!(c.eta > 0)) return set_error(AERO_EINVAL, "eta must be positive");
+  auto *p = new AeroNs2dPlan();
+  p->cfg = c;
+  const size_t e = c.dtype == AERO_F64 ? 8 : 4;
+  p->esz = e;
+  const size_t nx = c.nx, ny = c.ny;
+  p->nu = ny * (nx + 1);
+  p->nv = (ny + 1) * nx;
+  p->nc = ny * nx;
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    const size_t at = off;
+    off += aero_host::align_up(bytes);
+    return at;
+  };
+  p->off_uh = take(p->nu * e);
+  p->off_vh = take(p->nv * e);
+  p->off_up = take(p->nu * e);
+  p->off_vp = take(p->nv * e);
+  p->off_pa = take(p->nc * e);
+  p->off_small = take(8 * e);
+  p->off_scalars = take(sizeof(double) * aero::SC_COUNT);
+  p->off_zero = take(sizeof(double));
+  p->gx = (int)((nx + aero::ns2d::TX - 1) / aero::ns2d::TX);
+  p->gy = (int)((ny + aero::ns2d::TY - 1) / aero::ns2d::TY);
+  p->nblocks = p->gx * p->gy;
+  p->nq = has_win ? 4 * c.nbody : 0;
+  p->off_partials = take(sizeof(double) * 3 * (size_t)p->nblocks * std::max(p->nq, 1));
+  aero_host::axis_setup(p->ax[0], c.nx, c.periodic != 0, e);
+  aero_host::axis_setup(p->ax[1], c.ny, c.periodic != 0, e);
+  for (int a = 0; a < 2; ++a) aero_host::axis_place(p->ax[a], e, take);
+  p->total = off;
+  *plan = p;
+  return AERO_OK;
+}
+
+void aero_ns2d_plan_destroy(AeroNs2dPlan *plan) { delete plan; }
+
+size_t aero_ns2d_workspace_bytes(const AeroNs2dPlan *plan) { return plan ? plan->total : 0; }
+
+int aero_ns2d_workspace_init(const AeroNs2dPlan *plan, void *workspace, void *stream) {
+  if (!plan || !workspace) return set_error(AERO_EINVAL, "null argument");
+  if (reinterpret_cast<uintptr_t>(workspace) % aero_host::ALIGN)
+    return set_error(AERO_EINVAL, "workspace must be 256-byte aligned");
+  auto s = static_cast<cudaStream_t>(stream);
+  auto ws = static_cast<unsigned char *>(workspace);
+  return plan->cfg.dtype == AERO_F64 ? init2d_impl<double>(plan, ws, s) : init2d_impl<float>(plan, ws, s);
+}
+
+int aero_ns2d_step(const AeroNs2dPlan *plan, const AeroNs2dFields *f, const AeroNs2dGeom *g, const void *dt_in,
+                   void *workspace, void *stream) {
+  if (!plan || !f || !g || !workspace) return set_error(AERO_EINVAL, "null argument");
+  if (reinterpret_cast<uintptr_t>(workspace) % aero_host::ALIGN)
+    return set_error(AERO_EINVAL, "workspace must be 256-byte aligned");
+  const AeroNs2dConfig &c = plan->cfg;
+  if (!f->u0 || !f->v0 || !f->t0 || !f->u || !f->v || !f->p || !f->t || !f->dt)
+    return set_error(AERO_EINVAL, "missing state pointer");
+  if (c.dye && (!f->dye0 || !f->dye)) return set_error(AERO_EINVAL, "dye needs dye pointers");
+  if (c.dye && f->dye0 == f->dye) return set_error(AERO_EINVAL, "dye output must not alias dye input");
+  if (!c.periodic && !c.closed && !g->u_inlet) return set_error(AERO_EINVAL, "missing inlet profile");
+  const bool has_win = c.nbody > 0 && c.window[1] > c.window[0] && c.window[3] > c.window[2];
+  if (has_win && (!g->chi_u || !g->chi_v || !g->chi_c || !g->a_u || !g->a_v || !g->k_u || !g->k_v || !f->coeffs))
+    return set_error(AERO_EINVAL, "missing body masks");
+  auto s = static_cast<cudaStream_t>(stream);
+  auto ws = static_cast<unsigned char *>(workspace);
+  return c.dtype == AERO_F64 ? step2d_impl<double>(plan, f, g, dt_in, ws, s)
+                             : step2d_impl<float>(plan, f, g, dt_in, ws, s);
+}
+
+int aero_ns2d_poisson_solve(const AeroNs2dPlan *plan, const void *f, void *psi, void *workspace, void *stream) {
+  if (!plan || !f || !psi || !workspace) return set_error(AERO_EINVAL, "null argument");
+  auto s = static_cast<cudaStream_t>(stream);
+  auto ws = static_cast<unsigned char *>(workspace);
+  return plan->cfg.dtype == AERO_F64
+             ? poisson2d_passes<double>(plan, static_cast<const double *>(f), static_cast<double *>(psi), ws, s)
+             : poisson2d_passes<float>(plan, static_cast<const float *>(f), static_cast<float *>(psi), ws, s);
+}
+
+}  // extern "C"

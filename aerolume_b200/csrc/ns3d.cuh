@@ -138,7 +138,8 @@ struct TransformParams {
   AxisTables<T> A;
   const double *lam_x, *lam_y;
   // power-of-two x passes only: the forward pass may form div(uh, vh, wh) itself instead of
-  // reading `in`; the inverse pass may also fold psi into the step-averaged pressure
+  // reading `in` (fuse_div 1: 3D; 2: the 2D grid viewed as (ny, 1, nx)); the inverse pass may
+  // also fold psi into the step-averaged pressure
   // (acc_mode 0: p = wgt psi; 1: p += wgt psi; 2: p = (p + wgt psi) / dt)
   int fuse_div, px, py, pz;
   const T *uh, *vh, *wh;

@@ -312,7 +312,12 @@ __global__ void __launch_bounds__(256) pow2_transform_kernel(const __grid_consta
     nl = (int)min((size_t)L, rows - r0);
     base = r0 * N;
     estride = 1;
-    if (P.fuse_div && tid < nl) {
+    if (P.fuse_div == 2 && tid < nl) {  // 2D: rows r of u (nx + 1 faces) and v (nx cells)
+      const long long r = (long long)r0 + tid;
+      rowoff[0][tid] = r * (nx + 1);
+      rowoff[1][tid] = r * nx;
+      rowoff[2][tid] = (r + 1) * nx;
+    } else if (P.fuse_div && tid < nl) {
       const long long r = (long long)r0 + tid;
       const int k = (int)(r / ny), j = (int)(r - (long long)k * ny);
       rowoff[0][tid] = r * (nx + 1);
@@ -334,7 +339,10 @@ __global__ void __launch_bounds__(256) pow2_transform_kernel(const __grid_consta
       const int m = e & (N - 1), l = e >> LOG2N;
       T val = T(0);
       if (l < nl) {
-        if (P.fuse_div) {  // div(uh) of the stage velocity (core.py:577-579)
+        if (P.fuse_div == 2) {  // 2D: ((u_{i+1} - u_i) + v_{j+1}) - v_j (ns2d/core.py:620-622)
+          const T *ur = P.uh + rowoff[0][l];
+          val = (((ur[m + 1] - ur[m]) + P.vh[rowoff[2][l] + m]) - P.vh[rowoff[1][l] + m]) * P.inv_h;
+        } else if (P.fuse_div) {  // div(uh) of the stage velocity (ns3d/core.py:577-579)
           const T *ur = P.uh + rowoff[0][l];
           const T u1 = (P.px && m == N - 1) ? ur[0] : ur[m + 1];
           val = ((u1 - ur[m]) + (P.vh[rowoff[2][l] + m] - P.vh[rowoff[1][l] + m]) +

@@ -1,0 +1,212 @@
+"""One 2D configuration bound to the C ABI: constants, device masks and the workspace.
+
+:class:`Ns2dPlan` reads the reference's 2D objects by attribute (``Ops`` and ``Geometry`` of
+src/aerolume/solvers/ns2d/core.py:67-108 and geometry.py:160-182, or the containers of
+:mod:`aerolume_b200.ns2d.types`), turns the boundary types into the ghost-cell rules of
+core.py:271-325, uploads the window masks once and owns the device workspace.  Placed
+physics (heat, fans, ports, emitters, the PID step controller), the wall model and body
+forcing raise ``RuntimeError``: there is no fallback to a CPU or plain-torch path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from .. import _lib
+from .._lib import ADV, F32, F64, GHOST, LES, MAX_BODIES, check
+
+
+def _f(x) -> float:
+    return float(x.item() if torch.is_tensor(x) else x)
+
+
+def _torch_dtype(ops):
+    dt = getattr(ops, "dtype", "float32")
+    if isinstance(dt, torch.dtype):
+        return dt
+    return torch.float64 if str(dt) in ("float64", "torch.float64") else torch.float32
+
+
+def ghost_rules(ops):
+    """[(u | v)][x | y][lo | hi] -> (kind, value): the padding of core.py:284-325."""
+    if ops.periodic:
+        per = (("periodic_cell", 0.0), ("periodic_cell", 0.0))
+        return ((per, per), (per, per))
+
+    def wall(kind, speed):
+        if kind == "slip":
+            return ("even", 0.0)
+        if kind == "noslip":
+            return ("odd", 0.0)
+        return ("affine", float(speed))          # moving: u = speed on the wall
+
+    uy = (wall(ops.bc_bottom, _f(ops.ground_speed)), wall(ops.bc_top, 0.0))
+    vy = (("face_odd", 0.0), ("face_odd", 0.0))
+    if ops.closed:
+        ux = (("face_odd", 0.0), ("face_odd", 0.0))
+        side = {"noslip": ("odd", 0.0), "slip": ("even", 0.0)}
+        vx = (side[ops.bc_left], side[ops.bc_right])
+    else:
+        ux = (("edge", 0.0), ("edge", 0.0))
+        vx = (("odd", 0.0), ("edge", 0.0))
+    return ((ux, uy), (vx, vy))
+
+
+class Ns2dPlan:
+    """Plan + device tensors for one 2D (ops, geom) configuration; ``dye`` turns on the dye
+    update after each step."""
+
+    def __init__(self, ops, geom, *, dye: bool = False, device=None):
+        self.device = torch.device(device) if device is not None else torch.device("cuda")
+        if self.device.type != "cuda":
+            raise RuntimeError("the B200 step runs on a CUDA device only (no CPU fallback)")
+        if not torch.cuda.is_available():
+            raise RuntimeError("CUDA is not available: the B200 step has no CPU fallback")
+        if self.device.index is None:
+            self.device = torch.device("cuda", torch.cuda.current_device())
+        if getattr(ops, "phys", None) is not None:
+            raise RuntimeError("placed physics (heat, fans, ports, emitters, PID dt) is not in the B200 2D step")
+        if getattr(ops, "forcing", None) is not None:
+            raise RuntimeError("a uniform body force (verification forcing) is not supported by the B200 step")
+        if getattr(ops, "wall_model", False):
+            raise RuntimeError("the Werner-Wengle wall model is not supported by the B200 step")
+        L = _lib.lib()
+        self.dtype = _torch_dtype(ops)
+        self.ops, self.geom = ops, geom
+        self.dye = bool(dye)
+        nx, ny = int(ops.nx), int(ops.ny)
+        self.shape = (ny, nx)
+        cfg = _lib.Ns2dConfig()
+        cfg.abi_version = _lib.ABI_VERSION
+        cfg.dtype = F64 if self.dtype == torch.float64 else F32
+        cfg.nx, cfg.ny = nx, ny
+        cfg.h = float(ops.h)
+        cfg.periodic = int(bool(ops.periodic))
+        cfg.closed = int(bool(getattr(ops, "closed", False)))
+        if ops.advection not in ADV:
+            raise RuntimeError(f"unsupported advection scheme {ops.advection!r}")
+        cfg.advection = ADV[ops.advection]
+        if ops.turbulence not in LES:
+            raise RuntimeError(f"unsupported turbulence model {ops.turbulence!r}")
+        cfg.les = LES[ops.turbulence]
+        cfg.les_c = float(ops.les_c)
+        cfg.nu = _f(ops.nu)
+        cfg.eta = _f(ops.eta)
+        cfg.cfl = float(ops.cfl)
+        if getattr(ops, "dt_fixed", None) is not None:
+            cfg.has_dt_fixed = 1
+            cfg.dt_fixed = float(ops.dt_fixed)
+        for c, comp in enumerate(ghost_rules(ops)):
+            for a in range(2):
+                for s in range(2):
+                    kind, val = comp[a][s]
+                    cfg.ghost_kind[c][a][s] = GHOST[kind]
+                    cfg.ghost_val[c][a][s] = val
+        cfg.force_ref = float(ops.force_ref)
+        self.nbody = int(geom.nbody)
+        if self.nbody > MAX_BODIES:
+            raise RuntimeError(f"the B200 step supports at most {MAX_BODIES} bodies")
+        win = tuple(int(x) for x in geom.window)
+        self.has_win = self.nbody > 0 and win[1] > win[0] and win[3] > win[2]
+        for q in range(4):
+            cfg.window[q] = win[q] if self.has_win else 0
+        cfg.nbody = self.nbody if self.has_win else 0
+        cfg.dye = int(self.dye)
+        self._keep = []
+        dev, dt = self.device, self.dtype
+
+        def up(x, shape=None):
+            t = torch.as_tensor(np.asarray(x) if not torch.is_tensor(x) else x)
+            t = t.to(device=dev, dtype=dt)
+            if shape is not None:
+                t = t.reshape(shape)
+            t = t.contiguous()
+            self._keep.append(t)
+            return t
+
+        g = _lib.Ns2dGeom()
+        if self.has_win:
+            for name in ("chi_u", "chi_v", "chi_c", "a_u", "a_v", "k_u", "k_v"):
+                setattr(g, name, up(getattr(geom, name)).data_ptr())
+        u_in = getattr(ops, "u_inlet", None)
+        if u_in is not None:
+            g.u_inlet = up(u_in, (ny,)).data_ptr()
+        d_in = getattr(ops, "dye_inlet", None)
+        if self.dye and d_in is not None:
+            g.dye_inlet = up(d_in, (ny,)).data_ptr()
+        self.cfg = cfg
+        self.geom_c = g
+        handle = C.c_void_p()
+        check(L.aero_ns2d_plan_create(C.byref(cfg), C.byref(handle)), "aero_ns2d_plan_create")
+        self._handle = handle
+        nbytes = L.aero_ns2d_workspace_bytes(handle)
+        self._ws_raw = torch.empty(nbytes + 256, dtype=torch.uint8, device=dev)
+        self.ws_ptr = (self._ws_raw.data_ptr() + 255) & ~255
+        self.workspace_bytes = nbytes
+        check(L.aero_ns2d_workspace_init(handle, C.c_void_p(self.ws_ptr), self._stream()), "aero_ns2d_workspace_init")
+
+    def _stream(self):
+        return C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+
+    def __del__(self):
+        h = getattr(self, "_handle", None)
+        if h is not None and h.value:
+            try:
+                _lib.lib().aero_ns2d_plan_destroy(h)
+            except Exception:  # pragma: no cover - interpreter shutdown
+                pass
+            self._handle = None
+
+    def empty_fields(self):
+        """Fresh device tensors for a step's outputs."""
+        ny, nx = self.shape
+        kw = dict(device=self.device, dtype=self.dtype)
+        out = {"u": torch.empty(ny, nx + 1, **kw), "v": torch.empty(ny + 1, nx, **kw), "p": torch.empty(ny, nx, **kw),
+               "t": torch.empty((), **kw), "dt": torch.empty((), **kw),
+               "coeffs": torch.zeros(max(self.nbody, 1), 3, **kw)[: self.nbody]}
+        if self.dye:
+            out["dye"] = torch.empty(ny, nx, **kw)
+        return out
+
+    def _check(self, name, t, shape):
+        if not (torch.is_tensor(t) and t.device == self.device and t.dtype == self.dtype and t.is_contiguous()):
+            raise RuntimeError(f"{name} must be a contiguous {self.dtype} tensor on {self.device}")
+        if tuple(t.shape) != tuple(shape):
+            raise RuntimeError(f"{name} has shape {tuple(t.shape)}, expected {tuple(shape)}")
+
+    def step(self, u0, v0, t0, *, dye0=None, out=None, dt=None):
+        """One step (plus the dye update when the plan has dye); returns the output dict.
+        ``out`` may hold u0 / v0 themselves (in-place update); ``dt`` is None (CFL rule on
+        the device) or a 0-d device tensor."""
+        ny, nx = self.shape
+        self._check("u0", u0, (ny, nx + 1))
+        self._check("v0", v0, (ny + 1, nx))
+        self._check("t0", t0, ())
+        out = self.empty_fields() if out is None else out
+        f = _lib.Ns2dFields()
+        f.u0, f.v0, f.t0 = u0.data_ptr(), v0.data_ptr(), t0.data_ptr()
+        for name in ("u", "v", "p", "t", "dt"):
+            setattr(f, name, out[name].data_ptr())
+        if self.nbody and self.has_win:
+            f.coeffs = out["coeffs"].data_ptr()
+        if self.dye:
+            if dye0 is None:
+                raise RuntimeError("this plan has dye: dye0 is required")
+            self._check("dye0", dye0, (ny, nx))
+            f.dye0, f.dye = dye0.data_ptr(), out["dye"].data_ptr()
+        dtp = None
+        if dt is not None:
+            self._check("dt", dt, ())
+            dtp = C.c_void_p(dt.data_ptr())
+        check(_lib.lib().aero_ns2d_step(self._handle, C.byref(f), C.byref(self.geom_c), dtp, C.c_void_p(self.ws_ptr),
+                                        self._stream()), "aero_ns2d_step")
+        return out
+
+    def poisson_solve(self, f, psi=None):
+        self._check("f", f, self.shape)
+        psi = torch.empty_like(f) if psi is None else psi
+        check(_lib.lib().aero_ns2d_poisson_solve(self._handle, C.c_void_p(f.data_ptr()), C.c_void_p(psi.data_ptr()),
+                                                 C.c_void_p(self.ws_ptr), self._stream()), "aero_ns2d_poisson_solve")
+        return psi

@@ -18,6 +18,11 @@
  *   aero_ns3d_project          ns3d/core.py:604 project3d
  *   aero_ns3d_poisson_solve    ns3d/poisson.py:152 PoissonSolver3D.solve
  *   aero_ns3d_workspace_bytes  (no counterpart: the reference allocates inside torch)
+ *   aero_ns2d_plan_create      ns2d/core.py:182 make_operators (the per-config constants)
+ *   aero_ns2d_step             ns2d/core.py:815 step_full (no placed physics), with the dye
+ *                              update of its lines 959-962 (core.py:703 advect_dye,
+ *                              core.py:779 _zero_dye_in_solids)
+ *   aero_ns2d_poisson_solve    ns2d/poisson.py:126 PoissonSolver.solve
  */
 #ifndef AERO_B200_H
 #define AERO_B200_H
@@ -187,6 +192,65 @@ int aero_ns3d_read_status(const AeroNs3dPlan *plan, const void *workspace, int32
  * bound, block << 32 | thread) -- and skips that access.  Synchronising read that also clears
  * the record; in the release library it returns AERO_EUNSUPPORTED.  (No counterpart in the reference: a debugging hook.) */
 int aero_debug_check(int64_t *out4);
+
+/* ---- 2D step ----------------------------------------------------------------------- */
+
+typedef struct AeroNs2dPlan AeroNs2dPlan;
+
+/* Everything a 2D step needs besides the fields (ns2d/core.py:67-108 Ops).  Arrays are
+ * C-contiguous (ny, nx) with the staggered shapes of ns2d/core.py:9-12: u (ny, nx+1),
+ * v (ny+1, nx), p / dye (ny, nx). */
+typedef struct {
+  int32_t abi_version;          /* AERO_ABI_VERSION                                        */
+  int32_t dtype;                /* AERO_F32 or AERO_F64                                    */
+  int32_t nx, ny;               /* cells, >= 4 each                                        */
+  double h;                     /* cell size                                               */
+  int32_t periodic;             /* both axes periodic (core.py:80)                         */
+  int32_t closed;               /* walls on all four sides (core.py:102)                   */
+  int32_t advection;            /* AERO_ADV_*                                              */
+  int32_t les;                  /* AERO_LES_*                                              */
+  double les_c;                 /* model constant                                          */
+  double nu;                    /* 1 / Re                                                  */
+  double eta;                   /* Brinkman permeability                                   */
+  double cfl;
+  int32_t has_dt_fixed;
+  double dt_fixed;
+  int32_t ghost_kind[2][2][2];  /* [u, v][x, y][lo, hi] : AERO_GHOST_* (core.py:284-325)    */
+  double ghost_val[2][2][2];    /* wall speed of AERO_GHOST_AFFINE                         */
+  double force_ref;             /* coefficients = F / (0.5 force_ref)                      */
+  int32_t window[4];            /* body cell window j0, j1, i0, i1 (empty: no bodies)      */
+  int32_t nbody;                /* <= AERO_MAX_BODIES                                      */
+  int32_t dye;                  /* advect the dye after the step                           */
+} AeroNs2dConfig;
+
+/* Window masks (geometry.py:160-178) and boundary profiles, device pointers. */
+typedef struct {
+  const void *chi_u, *chi_v, *chi_c;  /* (wy, wx+1), (wy+1, wx), (wy, wx)                  */
+  const void *a_u, *a_v;              /* solid velocity times chi                           */
+  const void *k_u, *k_v;              /* (nbody, 2, ...): [force weight, moment weight]     */
+  const void *u_inlet;                /* (ny) inlet u (tunnel)                              */
+  const void *dye_inlet;              /* (ny) inlet dye comb, or NULL for zeros             */
+} AeroNs2dGeom;
+
+/* Step inputs (u0, v0, t0, dye0) and outputs; u / v may alias u0 / v0. */
+typedef struct {
+  const void *u0, *v0, *t0, *dye0;
+  void *u, *v, *p, *t, *dt, *dye;
+  void *coeffs;                       /* (nbody, 3): Cd, Cl, Cm                             */
+} AeroNs2dFields;
+
+int aero_ns2d_plan_create(const AeroNs2dConfig *cfg, AeroNs2dPlan **plan);
+void aero_ns2d_plan_destroy(AeroNs2dPlan *plan);
+size_t aero_ns2d_workspace_bytes(const AeroNs2dPlan *plan);
+int aero_ns2d_workspace_init(const AeroNs2dPlan *plan, void *workspace, void *stream);
+
+/* One SSP-RK3 step (dt_in NULL: the CFL / viscous rule on the device, else a device scalar),
+ * then the dye update when the plan has dye. */
+int aero_ns2d_step(const AeroNs2dPlan *plan, const AeroNs2dFields *f, const AeroNs2dGeom *g, const void *dt_in,
+                   void *workspace, void *stream);
+
+/* psi with L psi = f, zero mean ((ny, nx) device arrays; may alias). */
+int aero_ns2d_poisson_solve(const AeroNs2dPlan *plan, const void *f, void *psi, void *workspace, void *stream);
 
 #ifdef __cplusplus
 }

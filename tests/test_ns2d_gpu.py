@@ -1,0 +1,106 @@
+"""The CUDA 2D step through the C ABI against the reference's golden vectors and the oracle."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from _golden import CASES_2D, GOLDEN, load_case2d
+from oracle import ns2d as O2
+
+pytestmark = pytest.mark.gpu
+
+# per-step tolerances relative to max |field|: FP64 agrees with the reference's FP64 step to
+# round-off; FP32 to the stated 1e-5 of the FP32 step
+TOL = {"float64": 1e-10, "float32": 1e-5}
+TOL_COEFF = {"float64": 1e-9, "float32": 1e-4}
+
+
+def _rel(a, b):
+    a = a.detach().double().cpu().numpy() if torch.is_tensor(a) else np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
+
+
+def _dev(x, dt):
+    x = np.asarray(x)
+    return torch.as_tensor(np.ascontiguousarray(x).reshape(x.shape)).to("cuda", dt).contiguous()
+
+
+def _setup(name):
+    from aerolume_b200.ns2d.plan import Ns2dPlan
+    meta, ops, geom, arr = load_case2d(name)
+    dt = torch.float64 if meta["dtype"] == "float64" else torch.float32
+    plan = Ns2dPlan(ops, geom, dye="in_dye" in arr)
+    ins = {"u0": _dev(arr["in_u"], dt), "v0": _dev(arr["in_v"], dt), "t0": _dev(arr["in_t"], dt)}
+    if "in_dye" in arr:
+        ins["dye0"] = _dev(arr["in_dye"], dt)
+    return meta, plan, ins, arr
+
+
+@pytest.mark.parametrize("name", CASES_2D)
+def test_step2d_matches_reference(name):
+    meta, plan, ins, arr = _setup(name)
+    out = plan.step(**ins)
+    torch.cuda.synchronize()
+    tol = TOL[meta["dtype"]]
+    for k in ("u", "v", "p"):
+        assert _rel(out[k], arr[f"out1_{k}"]) < tol, (k, _rel(out[k], arr[f"out1_{k}"]))
+    assert _rel(out["dt"], arr["out1_dt"]) < tol
+    assert _rel(out["t"], arr["out1_t"]) < tol
+    if meta["nbody"]:
+        assert _rel(out["coeffs"], arr["out1_coeffs"]) < TOL_COEFF[meta["dtype"]]
+    if "out1_dye" in arr:
+        assert _rel(out["dye"], arr["out1_dye"]) < tol
+
+
+@pytest.mark.parametrize("name", [c for c in CASES_2D if c.startswith("cylinder")])
+def test_three_steps_in_place_match_reference(name):
+    meta, plan, ins, arr = _setup(name)
+    u, v, t, dye = ins["u0"], ins["v0"], ins["t0"], ins.get("dye0")
+    out = plan.empty_fields()
+    for _ in range(3):
+        out["u"], out["v"] = u, v             # in-place velocity update
+        res = plan.step(u, v, t, dye0=dye, out=out)
+        t = res["t"].clone()
+        if dye is not None:
+            dye, res["dye"] = res["dye"], dye  # ping-pong the dye
+    torch.cuda.synchronize()
+    tol = 10 * TOL[meta["dtype"]]
+    for k, got in (("u", u), ("v", v), ("p", res["p"]), ("t", t)):
+        assert _rel(got, arr[f"outN_{k}"]) < tol, (k, _rel(got, arr[f"outN_{k}"]))
+    if dye is not None:
+        assert _rel(dye, arr["outN_dye"]) < tol
+
+
+def _poisson_plan(nx, ny, h, periodic, dtype):
+    from aerolume_b200.ns2d.plan import Ns2dPlan
+    from aerolume_b200.ns2d.types import Geometry2D, Ops2D
+    ops = Ops2D(nx=nx, ny=ny, h=h, periodic=periodic, u_inlet=np.ones(ny), dtype=dtype)
+    return Ns2dPlan(ops, Geometry2D((0, 0, 0, 0)))
+
+
+@pytest.mark.parametrize("dtype", ["float64", "float32"])
+def test_poisson2d_matches_reference(dtype):
+    z = np.load(GOLDEN / "poisson2d.npz")
+    h = float(z["h"])
+    tdt = torch.float64 if dtype == "float64" else torch.float32
+    for n in range(int(z["count"])):
+        nx, ny, per = (int(x) for x in z[f"meta{n}"])
+        if nx < 4 or ny < 4:
+            continue
+        plan = _poisson_plan(nx, ny, h, bool(per), dtype)
+        psi = plan.poisson_solve(_dev(z[f"f{n}"], tdt))
+        assert _rel(psi, z[f"psi{n}"]) < (1e-12 if dtype == "float64" else 2e-6), (n, _rel(psi, z[f"psi{n}"]))
+
+
+@pytest.mark.parametrize("shape", [(64, 32), (256, 128), (128, 128), (96, 40)])
+def test_poisson2d_solves_exactly(shape):
+    nx, ny = shape
+    for per in (False, True):
+        plan = _poisson_plan(nx, ny, 0.05, per, "float64")
+        f = torch.randn(ny, nx, dtype=torch.float64, generator=torch.Generator().manual_seed(3))
+        f = (f - f.mean()).cuda()
+        psi = plan.poisson_solve(f)
+        lap = O2.PoissonSolver2D.laplacian(psi.cpu().numpy(), 0.05, per)
+        assert np.abs(lap - f.cpu().numpy()).max() < 1e-9 * f.abs().max().item()
