@@ -17,6 +17,12 @@ its event-timed mean duration against the measured HBM copy bandwidth.  ``cpu_ba
 the numpy oracle (a restatement of the reference's plain-torch step) on a bounded sample of
 the same workload on this host.
 
+``--workload cylinder2d`` measures the 2D step instead (a D = 0.5 cylinder at Re_D 100 in an
+8 x 4 tunnel, 256 x 128 FP32, upwind3, CFL 0.5) and ``--workload sweep2d`` the batched sweep
+(64 NACA 4-digit airfoils on grids from 256 x 128 to 1024 x 512, all advanced by one CUDA
+graph that spreads the instances over 16 streams; the same plans looped one after another on
+a single stream are reported beside it).
+
 With ``--gpus N`` (N > 1, launched by torch.distributed.run) every rank advances its own
 replica (no data-path collective: a single instance of this solver does not shard), and
 ``value`` is the total over ranks.  ``--impl reference`` times the reference arm: the
@@ -322,20 +328,289 @@ def run_ours(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------------------
+# 2D workloads
+# ---------------------------------------------------------------------------------------
+
+def _launches_2d(plan):
+    c = plan.cfg
+    fused = 8 <= c.nx <= 2048 and (c.nx & (c.nx - 1)) == 0
+    n = 1                                              # dt
+    if not c.has_dt_fixed:
+        n += 2 + (1 if c.les else 0)                   # |u|, |v| maxima, nu_t of u0
+    n += 3 * (1 + 3 + 1 + (0 if fused else 2))         # stage, 3 transform passes, correct, [div, psi_w]
+    n += 1 if c.dye else 0
+    return n + 1                                       # finalize
+
+
+def _time_graph(g, dist, local_rank, rank, dev):
+    import torch
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    clocks = Clocks(local_rank) if rank == 0 else None
+    time.sleep(0.3 if clocks else 0.0)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    start.record()
+    g.replay()
+    end.record()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    ms = start.elapsed_time(end)
+    clk = clocks.stop() if clocks else None
+    if dist is not None:
+        tt = torch.tensor([ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    return ms, clk
+
+
+def oracle2d_sample(ops, geom, steps, seed=0):
+    """Wall time of ``steps`` 2D oracle steps (after one untimed step)."""
+    from oracle import ns2d as O2
+    f32 = np.float32
+    rng = np.random.default_rng(seed)
+    ps = O2.PoissonSolver2D(ops.nx, ops.ny, ops.h, ops.periodic, f32)
+    u = (np.ones((ops.ny, ops.nx + 1)) + 1e-3 * rng.standard_normal((ops.ny, ops.nx + 1))).astype(f32)
+    v = (1e-3 * rng.standard_normal((ops.ny + 1, ops.nx))).astype(f32)
+    u, v = O2.apply_boundary_values(u, v, ops)
+    u, v, _ = O2.project2d(u, v, ops, ps)
+    geom32 = type(geom)(geom.window, *[None if x is None else np.asarray(x, f32) for x in
+                                       (geom.chi_u, geom.chi_v, geom.chi_c, geom.a_u, geom.a_v, geom.k_u, geom.k_v)],
+                        geom.nbody)
+    t = f32(0.0)
+    r = O2.step2d(u, v, t, geom32, ops, ps)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        r = O2.step2d(r.u, r.v, r.t, geom32, ops, ps)
+    return time.perf_counter() - t0
+
+
+def run_2d(args, rank, world, local_rank):
+    import torch
+    from aerolume_b200.ns2d.plan import Ns2dPlan
+    from aerolume_b200.ns2d.workloads import cylinder_tunnel, initial_state
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    nx, ny = 256, 128
+    cells = nx * ny
+    ops, geom = cylinder_tunnel(nx, ny, "float32")
+    plan = Ns2dPlan(ops, geom, device=dev)
+    u, v = initial_state(ops, plan, seed=rank, noise=1e-3)
+    t = torch.zeros((), device=dev)
+    out = plan.empty_fields()
+    out["u"], out["v"] = u, v
+
+    def step():
+        plan.step(u, v, t, out=out)
+        t.copy_(out["t"])
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    K = args.steps
+    s = torch.cuda.Stream(device=dev)
+    s.wait_stream(torch.cuda.current_stream(dev))
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(s):
+        with torch.cuda.graph(g, stream=s):
+            for _ in range(K):
+                step()
+    torch.cuda.current_stream(dev).wait_stream(s)
+    ms, clk = _time_graph(g, dist, local_rank, rank, dev)
+    coeffs = out["coeffs"][0].tolist()
+    # e2e: state in from pinned host memory, step, state / coefficients / time out, every step
+    hu, hv = u.cpu().pin_memory(), v.cpu().pin_memory()
+    ho = {k: torch.empty(x.shape, dtype=x.dtype, pin_memory=True) for k, x in out.items()}
+    du, dv = torch.empty_like(u), torch.empty_like(v)
+    o2 = plan.empty_fields()
+    ke = max(10, min(K, 200))
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(ke):
+        du.copy_(hu, non_blocking=True)
+        dv.copy_(hv, non_blocking=True)
+        plan.step(du, dv, t, out=o2)
+        for k in ho:
+            ho[k].copy_(o2[k], non_blocking=True)
+        hu, ho["u"] = ho["u"], hu
+        hv, ho["v"] = ho["v"], hv
+    e1.record()
+    torch.cuda.synchronize()
+    ems = e0.elapsed_time(e1) / ke
+    if rank != 0:
+        return
+    h2d = u.numel() * 4 + v.numel() * 4
+    d2h = sum(x.numel() * x.element_size() for x in out.values())
+    peak, peak_kind = _peaks()
+    alg = 228.0 * cells                               # compulsory bytes per 2D cell-step, FP32
+    ms_step = ms / K
+    cpu = None
+    if not args.no_cpu:
+        steps_cpu = 20
+        secs = oracle2d_sample(ops, geom, steps_cpu)
+        cpu = {"value": cells * steps_cpu / secs / 1e6, "unit": UNIT, "cores": _threads(), "kind": "port",
+               "sample": f"{steps_cpu} full {nx}x{ny} steps of the numpy 2D oracle after 1 untimed step"}
+    line = {"metric": METRIC, "value": world * cells * K / (ms * 1e-3) / 1e6, "unit": UNIT, "n_gpus": world,
+            "steps": K, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "cylinder D=0.5 at (2,2), 256x128 FP32, Re_D 100, slip walls, upwind3, CFL 0.5",
+                       "cells": cells, "grid": [nx, ny],
+                       "inputs_vs_l2": "7.5 MB working set stays in the 126 MB L2 between steps (no flush)",
+                       "parallelism": "replicas", "graph": f"{K} steps, 1 replay"},
+            "roofline": {"bound": "hbm", "kernel": "whole step", "achieved": alg / (ms_step * 1e-3) / 1e9,
+                         "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                         "frac": alg / (ms_step * 1e-3) / 1e9 / peak, "traffic": None,
+                         "alg_bytes_per_step": alg},
+            "cpu_baseline": cpu,
+            "e2e": {"value": cells / (ems * 1e-3) / 1e6, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h), "ms_per_step": ems, "steps": ke},
+            "gpu_launches": _launches_2d(plan) * K, "clocks": clk, "coeffs_last": coeffs}
+    print(json.dumps(line), flush=True)
+
+
+def run_sweep(args, rank, world, local_rank):
+    import torch
+    from aerolume_b200.ns2d.plan import Ns2dPlan
+    from aerolume_b200.ns2d.workloads import initial_state, sweep_instances
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    insts = sweep_instances(64, seed=0)
+    plans, states = [], []
+    for k, (ops, geom, _) in enumerate(insts):
+        plan = Ns2dPlan(ops, geom, device=dev)
+        u, v = initial_state(ops, plan, seed=1000 * rank + k, noise=1e-3)
+        out = plan.empty_fields()
+        out["u"], out["v"] = u, v
+        plans.append(plan)
+        states.append((u, v, torch.zeros((), device=dev), out))
+    cells = sum(o.nx * o.ny for o, _, _ in insts)
+    nstream = 16
+    streams = [torch.cuda.Stream(device=dev) for _ in range(nstream)]
+
+    def one(k):
+        u, v, t, out = states[k]
+        plans[k].step(u, v, t, out=out)
+        t.copy_(out["t"])
+
+    def sweep_step(main):
+        for q in range(nstream):
+            streams[q].wait_stream(main)
+        for k in range(len(plans)):
+            with torch.cuda.stream(streams[k % nstream]):
+                one(k)
+        for q in range(nstream):
+            main.wait_stream(streams[q])
+
+    main = torch.cuda.current_stream(dev)
+    for _ in range(args.warmup):
+        sweep_step(main)
+    torch.cuda.synchronize()
+    K = args.steps
+    s = torch.cuda.Stream(device=dev)
+    s.wait_stream(main)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(s):
+        with torch.cuda.graph(g, stream=s):
+            for _ in range(K):
+                sweep_step(s)
+    main.wait_stream(s)
+    ms, clk = _time_graph(g, dist, local_rank, rank, dev)
+    # the same plans looped one instance after another on one stream
+    gl = torch.cuda.CUDAGraph()
+    s.wait_stream(main)
+    with torch.cuda.stream(s):
+        with torch.cuda.graph(gl, stream=s):
+            for _ in range(K):
+                for k in range(len(plans)):
+                    one(k)
+    main.wait_stream(s)
+    ms_loop, _ = _time_graph(gl, dist, local_rank, rank, dev)
+    if rank != 0:
+        return
+    peak, peak_kind = _peaks()
+    alg = 228.0 * cells
+    cpu = None
+    if not args.no_cpu:
+        ops0, geom0, _ = min(insts, key=lambda x: x[0].nx)
+        steps_cpu = 10
+        secs = oracle2d_sample(ops0, geom0, steps_cpu)
+        cpu = {"value": ops0.nx * ops0.ny * steps_cpu / secs / 1e6, "unit": UNIT, "cores": _threads(),
+               "kind": "port", "sample": f"{steps_cpu} steps of one {ops0.nx}x{ops0.ny} instance of the numpy 2D oracle"}
+    grids = {}
+    for o, _, _ in insts:
+        grids[f"{o.nx}x{o.ny}"] = grids.get(f"{o.nx}x{o.ny}", 0) + 1
+    line = {"metric": METRIC, "value": world * cells * K / (ms * 1e-3) / 1e6, "unit": UNIT, "n_gpus": world,
+            "steps": K, "warmup": args.warmup, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "batched sweep: 64 NACA 4-digit airfoils, seeded grids 256x128..1024x512 FP32, "
+                                   "upwind3, CFL 0.5, no LES", "cells": cells, "grids": grids,
+                       "inputs_vs_l2": f"{cells * 4 * 10 / 1e6:.0f} MB of state + workspace > 126 MB L2 (no flush)",
+                       "parallelism": "replicas", "graph": f"{K} sweep steps (64 instances each) over 16 streams, 1 replay"},
+            "looped": {"value": world * cells * K / (ms_loop * 1e-3) / 1e6, "unit": UNIT, "ms_per_step": ms_loop / K,
+                       "how": "the same plans one after another on one stream, one graph"},
+            "roofline": {"bound": "hbm", "kernel": "whole sweep step", "achieved": alg / (ms / K * 1e-3) / 1e9,
+                         "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                         "frac": alg / (ms / K * 1e-3) / 1e9 / peak, "traffic": None, "alg_bytes_per_step": alg},
+            "cpu_baseline": cpu, "e2e": None,
+            "gpu_launches": sum(_launches_2d(p) for p in plans) * K, "clocks": clk}
+    print(json.dumps(line), flush=True)
+
+
+def run_reference_2d(args, rank):
+    from aerolume_b200.ns2d.workloads import cylinder_tunnel, sweep_instances
+    if rank != 0:
+        return
+    if args.workload == "cylinder2d":
+        ops, geom = cylinder_tunnel(256, 128, "float32")
+        desc = "cylinder D=0.5 at (2,2), 256x128 FP32, Re_D 100, slip walls, upwind3, CFL 0.5"
+    else:
+        ops, geom, _ = min(sweep_instances(64, seed=0), key=lambda x: x[0].nx)
+        desc = f"one {ops.nx}x{ops.ny} instance of the batched NACA sweep"
+    steps = max(1, min(args.steps, 20))
+    secs = oracle2d_sample(ops, geom, steps)
+    val = ops.nx * ops.ny * steps / secs / 1e6
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
+            "warmup": 1, "ms_per_step": 1e3 * secs / steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": {"workload": desc},
+            "cpu_baseline": {"value": val, "unit": UNIT, "cores": _threads(), "kind": "port",
+                             "sample": f"{steps} steps of the numpy 2D oracle after 1 untimed step"},
+            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=None, help="timed steps (default 20; 400 for cylinder2d, "
+                                                             "10 for sweep2d)")
+    ap.add_argument("--workload", default="box3d", choices=["box3d", "cylinder2d", "sweep2d"])
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--shape", type=int, nargs=3, default=list(SHAPE), help="nx ny nz (2:1:1)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     args = ap.parse_args()
+    if args.steps is None:
+        args.steps = {"box3d": 20, "cylinder2d": 400, "sweep2d": 10}[args.workload]
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
-        run_reference(args, rank)
+        if args.workload == "box3d":
+            run_reference(args, rank)
+        else:
+            run_reference_2d(args, rank)
         return
     if world > 1:
         import datetime
@@ -345,7 +620,7 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     try:
-        run_ours(args, rank, world, local_rank)
+        {"box3d": run_ours, "cylinder2d": run_2d, "sweep2d": run_sweep}[args.workload](args, rank, world, local_rank)
     finally:
         if world > 1:
             import torch.distributed as dist
