@@ -38,15 +38,6 @@ __device__ __forceinline__ int ghost_map(int g, int n, int kind_lo, int kind_hi,
   c = T(0);
   if (g >= 0 && g < n) return g;
   const bool lo = g < 0;
-  // periodic rules wrap any index (a tile may reach past the second ghost layer)
-  if ((lo ? kind_lo : kind_hi) == AERO_GHOST_PERIODIC_CELL) {
-    int m = g % n;
-    return m < 0 ? m + n : m;
-  }
-  if ((lo ? kind_lo : kind_hi) == AERO_GHOST_PERIODIC_FACE) {  // n entries, period n - 1
-    int m = g % (n - 1);
-    return m < 0 ? m + n - 1 : m;
-  }
   if (lo) {
     if (g < -2) g = -2;
   } else if (g > n + 1) {

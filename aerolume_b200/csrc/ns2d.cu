@@ -32,7 +32,7 @@ constexpr int MAXQ = 4 * AERO_MAX_BODIES;
 // Ghost rules of one component on its (n1, n0) = (y, x) array; rules compose x, then y.
 template <typename T>
 struct Rules2 {
-  int n0, n1, p0;  // entries along x and y (without a periodic duplicate), row pitch
+  int n0, n1, p0;  // entries along x and y (face arrays: with the periodic duplicate), row pitch
   int kind[2][2];
   T val[2][2];
 };
@@ -484,8 +484,8 @@ using aero_host::set_error;
 template <typename T>
 aero::ns2d::Rules2<T> rules2(const AeroNs2dConfig &c, int comp) {
   aero::ns2d::Rules2<T> r{};
-  r.n0 = c.nx + (comp == 0 && !c.periodic);
-  r.n1 = c.ny + (comp == 1 && !c.periodic);
+  r.n0 = c.nx + (comp == 0);
+  r.n1 = c.ny + (comp == 1);
   r.p0 = c.nx + (comp == 0);
   for (int a = 0; a < 2; ++a)
     for (int s = 0; s < 2; ++s) {

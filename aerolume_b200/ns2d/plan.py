@@ -32,8 +32,10 @@ def _torch_dtype(ops):
 def ghost_rules(ops):
     """[(u | v)][x | y][lo | hi] -> (kind, value): the padding of core.py:284-325."""
     if ops.periodic:
-        per = (("periodic_cell", 0.0), ("periodic_cell", 0.0))
-        return ((per, per), (per, per))
+        # face arrays keep their duplicate entry (period n - 1), cell-centred ones wrap by n
+        face = (("periodic_face", 0.0), ("periodic_face", 0.0))
+        cell = (("periodic_cell", 0.0), ("periodic_cell", 0.0))
+        return ((face, cell), (cell, face))
 
     def wall(kind, speed):
         if kind == "slip":

@@ -1,0 +1,58 @@
+"""The reference's 2D step function (src/aerolume/solvers/ns2d/core.py:815 ``step_full``),
+served by the B200 step.
+
+``FlowSolver`` imports ``step_full`` at module import (ns2d/solver.py:44-57) and calls it as
+``step_full(state, geom, ops, None, out=..., diag=...)`` (solver.py:384-408); rebinding
+``aerolume.solvers.ns2d.solver.step_full`` to this function swaps the step.  It returns
+``(State, coeffs (nbody, 3))`` of new tensors like the reference.  Placed physics, the wall
+model, diagnostics rows and traces raise instead of being computed differently.
+"""
+from __future__ import annotations
+
+from typing import Any, NamedTuple
+
+import torch
+
+from .plan import Ns2dPlan
+
+
+class State(NamedTuple):
+    """The reference's 2D state (core.py:111-130); placed-physics fields stay None."""
+    u: Any
+    v: Any
+    p: Any
+    dye: Any
+    t: Any
+    dt: Any
+    theta: Any = None
+    dye_extra: Any = None
+    ctrl: Any = None
+
+
+_PLANS: dict = {}
+
+
+def _plan_for(ops, geom, dye, device):
+    key = (id(ops), id(geom), dye)
+    entry = _PLANS.get(key)
+    if entry is None:
+        entry = (Ns2dPlan(ops, geom, dye=dye, device=device), ops, geom)   # keeps ops / geom alive
+        _PLANS[key] = entry
+    return entry[0]
+
+
+def step_full(state, geom, ops, dt=None, *, out=None, diag=False, trace=None):
+    """One SSP-RK3 step (plus the dye update when the state carries dye)."""
+    if diag or trace is not None:
+        raise RuntimeError("diagnostics rows and stage traces are not produced by the B200 step")
+    for name in ("theta", "dye_extra", "ctrl"):
+        if getattr(state, name, None) is not None:
+            raise RuntimeError(f"placed-physics state {name!r} is not in the B200 2D step")
+    plan = _plan_for(ops, geom, state.dye is not None, state.u.device)
+    if dt is not None and not torch.is_tensor(dt):
+        dt = torch.tensor(float(dt), device=state.u.device, dtype=state.u.dtype)
+    res = plan.step(state.u, state.v, state.t, dye0=state.dye, dt=dt)
+    new = State(res["u"], res["v"], res["p"], res.get("dye"), res["t"], res["dt"])
+    coeffs = res["coeffs"] if plan.nbody and plan.has_win else torch.zeros(0, 3, device=state.u.device,
+                                                                          dtype=state.u.dtype)
+    return new, coeffs

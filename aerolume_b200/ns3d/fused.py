@@ -1,0 +1,100 @@
+"""The reference's fused-kernel seam of ``FlowSolver3D`` (src/aerolume/solvers/ns3d/fused.py),
+served by the B200 step.
+
+Same names, arguments and results as the reference module, so ``ns3d/solver.py`` can import
+these instead (solver.py:161-166 ``load_kernels``; solver.py:583-595 ``fast_step`` /
+``fast_step_phys``; solver.py:655-657 ``fast_dye``):
+
+* ``load_kernels(scheme, device, dtype)`` raises ``RuntimeError`` when the B200 library or a
+  CUDA device is missing (fused.py:226-235 raises the same way, so the solver records
+  ``fused_error``); it returns a handle that caches one plan per configuration.
+* ``fast_step`` / ``fast_step_phys`` return ``(State3D, coeffs)`` / ``StepOut3D`` of new
+  tensors, as fused.py:371 / 378-502 do.
+* ``fast_dye`` is the MUSCL advection of one smoke channel (fused.py:553-565).
+
+Placed physics that the B200 step does not implement (fans, ports, paint, the PID step
+controller, diagnostics rows) raises instead of being computed differently.
+"""
+from __future__ import annotations
+
+import torch
+
+from .plan import Ns3dPlan
+from .types import Geometry3D, State3D, StepOut3D
+
+
+class B200Kernels:
+    """What ``load_kernels`` returns: the scheme plus plans cached by configuration."""
+
+    def __init__(self, scheme, device, dtype):
+        self.scheme, self.device, self.dtype = scheme, device, dtype
+        self._plans = {}
+
+    def plan_for(self, geom, ops, phys=None):
+        thermal = getattr(phys, "thermal", None) if phys is not None else None
+        key = ("step", id(geom), id(ops), id(thermal))
+        entry = self._plans.get(key)
+        if entry is None:
+            if phys is not None:
+                for name in ("fans", "ports", "paint", "pid"):
+                    if getattr(phys, name, None) is not None:
+                        raise RuntimeError(f"placed physics {name!r} is not in the B200 step")
+            plan = Ns3dPlan(ops, geom, thermal, None, device=self.device)
+            entry = (plan, geom, ops, thermal)          # the objects stay alive with their plan
+            self._plans[key] = entry
+        return entry[0]
+
+    def dye_plan_for(self, ops):
+        key = ("dye", id(ops))
+        entry = self._plans.get(key)
+        if entry is None:
+            plan = Ns3dPlan(ops, Geometry3D((0, 0, 0, 0, 0, 0)), None, None, smoke=True, device=self.device)
+            entry = (plan, ops)
+            self._plans[key] = entry
+        return entry[0]
+
+
+def load_kernels(scheme: str, device: torch.device, dtype: torch.dtype) -> B200Kernels:
+    """The B200 kernels for ``scheme`` on ``device`` / ``dtype`` (raises when unavailable)."""
+    device = torch.device(device)
+    if device.type != "cuda":
+        raise RuntimeError("the B200 kernels need a CUDA device")
+    if not torch.cuda.is_available():
+        raise RuntimeError("CUDA is not available")
+    if scheme not in ("upwind3", "central"):
+        raise RuntimeError(f"unknown advection scheme {scheme!r}")
+    from .. import _lib
+    _lib.lib()                                           # raises when libaero_b200.so is missing
+    return B200Kernels(scheme, device, dtype)
+
+
+def _dt_arg(dt, like):
+    if dt is None or torch.is_tensor(dt):
+        return dt
+    return torch.tensor(float(dt), device=like.device, dtype=like.dtype)
+
+
+def fast_step(state, geom, ops, kern):
+    """One plain step: (State3D, coeffs (nbody, 6)) of new tensors."""
+    out = kern.plan_for(geom, ops).step(state.u, state.v, state.w, state.t)
+    return State3D(out["u"], out["v"], out["w"], out["p"], out["t"], out["dt"]), out["coeffs"]
+
+
+def fast_step_phys(state, geom, ops, kern, dt=None, *, phys=None, theta=None, diag=False, theta_kernels=True):
+    """One step with the placed physics the B200 step implements (heat transfer)."""
+    if diag:
+        raise RuntimeError("diagnostics rows are not produced by the B200 step")
+    plan = kern.plan_for(geom, ops, phys)
+    thermal = plan.thermal is not None and theta is not None
+    out = plan.step(state.u, state.v, state.w, state.t, theta0=theta if thermal else None,
+                    dt=_dt_arg(dt, state.t))
+    if thermal and torch.is_tensor(getattr(plan.thermal, "heat_rate", None)):
+        plan.thermal.heat_rate.copy_(out["heat_rate"])  # the reference leaves the rates there
+    new = State3D(out["u"], out["v"], out["w"], out["p"], out["t"], out["dt"])
+    return StepOut3D(new, out["coeffs"], out.get("theta") if thermal else None)
+
+
+def fast_dye(c, u, v, w, dt, ops, kern):
+    """MUSCL / van Leer advection of one smoke channel with the step's velocity and dt."""
+    dt = _dt_arg(dt, c)
+    return kern.dye_plan_for(ops).smoke_step(c, u, v, w, dt, dt, solids=False, sources=False)

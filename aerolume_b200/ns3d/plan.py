@@ -259,8 +259,10 @@ class Ns3dPlan:
                                           self._stream(), arr, len(events)), "aero_ns3d_step_traced")
         return out
 
-    def smoke_step(self, dye0, u, v, w, t_new, dt, out=None):
-        """The smoke update alone with the given velocity, step and new time."""
+    def smoke_step(self, dye0, u, v, w, t_new, dt, out=None, *, solids=True, sources=True):
+        """The smoke update alone with the given velocity, step and new time.  ``solids`` /
+        ``sources`` False leave out the clearing inside bodies / the nozzles (advection,
+        clipping and the floor only: the reference's fast_dye)."""
         if not self.smoke:
             raise RuntimeError("this plan was built without smoke")
         nz, ny, nx = self.shape
@@ -269,8 +271,14 @@ class Ns3dPlan:
         f = _lib.Ns3dFields()
         f.dye0, f.dye = dye0.data_ptr(), out.data_ptr()
         f.u, f.v, f.w, f.t, f.dt = u.data_ptr(), v.data_ptr(), w.data_ptr(), t_new.data_ptr(), dt.data_ptr()
-        check(_lib.lib().aero_ns3d_smoke(self._handle, C.byref(f), C.byref(self.geom_c), self._stream()),
-              "aero_ns3d_smoke")
+        g = self.geom_c
+        if not (solids and sources):
+            g = _lib.Ns3dGeom.from_buffer_copy(self.geom_c)
+            if not solids:
+                g.chi_c = None
+            if not sources:
+                g.dye_weight = None
+        check(_lib.lib().aero_ns3d_smoke(self._handle, C.byref(f), C.byref(g), self._stream()), "aero_ns3d_smoke")
         return out
 
     def poisson_solve(self, f, psi=None):

@@ -157,7 +157,9 @@ int aero_ns3d_step_traced(const AeroNs3dPlan *plan, const AeroNs3dFields *f, con
 
 /* Smoke alone (the step's tracer update): dye <- MUSCL step of dye0 with (u, v, w) and dt,
  * then solids cleared and nozzles relaxed at time t.  Fields of f used: u, v, w, dye0, dye,
- * and dt and t as inputs (the step just taken and the new time).  dye must not alias dye0. */
+ * and dt and t as inputs (the step just taken and the new time).  dye must not alias dye0.
+ * g->chi_c NULL skips the clearing inside solids and g->dye_weight NULL the nozzles, which
+ * leaves the advection alone (ns3d/fused.py:553 fast_dye). */
 int aero_ns3d_smoke(const AeroNs3dPlan *plan, const AeroNs3dFields *f, const AeroNs3dGeom *g, void *stream);
 
 /* psi with L psi = f, zero mean (f and psi: (nz, ny, nx) device arrays; may alias). */

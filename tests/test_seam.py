@@ -1,0 +1,77 @@
+"""The reference-named seams (aerolume_b200.ns3d.fused, aerolume_b200.ns2d.step) called the way
+the reference's solvers call them (ns3d/solver.py:583-595, 655-657; ns2d/solver.py:384-408)."""
+from __future__ import annotations
+
+import types
+
+import numpy as np
+import pytest
+import torch
+
+from _golden import load_case, load_case2d
+
+
+def _rel(a, b):
+    a = a.detach().double().cpu().numpy() if torch.is_tensor(a) else np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
+
+
+def test_load_kernels_refuses_a_cpu_device():
+    from aerolume_b200.ns3d.fused import load_kernels
+    with pytest.raises(RuntimeError):
+        load_kernels("upwind3", torch.device("cpu"), torch.float32)
+
+
+def test_step_full_refuses_diagnostics_and_placed_physics():
+    from aerolume_b200.ns2d.step import State, step_full
+    st = State(None, None, None, None, None, None)
+    with pytest.raises(RuntimeError):
+        step_full(st, None, None, diag=True)
+    with pytest.raises(RuntimeError):
+        step_full(st._replace(theta=1), None, None)
+
+
+def _dev(x, dt):
+    x = np.asarray(x)
+    return torch.as_tensor(np.ascontiguousarray(x).reshape(x.shape)).to("cuda", dt).contiguous()
+
+
+@pytest.mark.gpu
+def test_fast_step_phys_and_fast_dye_match_reference():
+    from aerolume_b200.ns3d.fused import fast_dye, fast_step_phys, load_kernels
+    from aerolume_b200.ns3d.types import State3D
+    from oracle import ns3d as O
+    meta, ops, geom, th, src, arr = load_case("tunnel_wale_heat_smoke_f64")
+    dt = torch.float64
+    kern = load_kernels(ops.advection, torch.device("cuda"), dt)
+    phys = types.SimpleNamespace(thermal=th, fans=None, ports=None, paint=None, pid=None)
+    nz, ny, nx = ops.nz, ops.ny, ops.nx
+    state = State3D(_dev(arr["in_u"], dt), _dev(arr["in_v"], dt), _dev(arr["in_w"], dt),
+                    torch.zeros(nz, ny, nx, device="cuda", dtype=dt), _dev(arr["in_t"], dt),
+                    torch.zeros((), device="cuda", dtype=dt))
+    out = fast_step_phys(state, geom, ops, kern, phys=phys, theta=_dev(arr["in_theta"], dt))
+    torch.cuda.synchronize()
+    for k, got in (("u", out.state.u), ("v", out.state.v), ("w", out.state.w), ("p", out.state.p),
+                   ("theta", out.theta)):
+        assert _rel(got, arr[f"out1_{k}"]) < 1e-10, k
+    assert _rel(out.coeffs, arr["out1_coeffs"]) < 1e-9
+    c = fast_dye(_dev(arr["in_dye"], dt), out.state.u, out.state.v, out.state.w, out.state.dt, ops, kern)
+    want = O.advect_dye3d(arr["in_dye"], *(x.cpu().numpy() for x in (out.state.u, out.state.v, out.state.w)),
+                          out.state.dt.cpu().numpy(), ops)
+    assert _rel(c, want) < 1e-12
+
+
+@pytest.mark.gpu
+def test_step_full_matches_reference():
+    from aerolume_b200.ns2d.step import State, step_full
+    meta, ops, geom, arr = load_case2d("cylinder_upwind_f64")
+    dt = torch.float64
+    ny, nx = ops.ny, ops.nx
+    st = State(_dev(arr["in_u"], dt), _dev(arr["in_v"], dt), torch.zeros(ny, nx, device="cuda", dtype=dt),
+               _dev(arr["in_dye"], dt), _dev(arr["in_t"], dt), torch.zeros((), device="cuda", dtype=dt))
+    new, coeffs = step_full(st, geom, ops, None)
+    torch.cuda.synchronize()
+    for k in ("u", "v", "p", "dye", "t", "dt"):
+        assert _rel(getattr(new, k), arr[f"out1_{k}"]) < 1e-10, k
+    assert _rel(coeffs, arr["out1_coeffs"]) < 1e-9
