@@ -187,7 +187,7 @@ struct StageSmem {
 };
 
 template <typename T>
-__global__ void __launch_bounds__(TX *TY, 2) stage_kernel(const __grid_constant__ StageParams<T> P) {
+__global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) stage_kernel(const __grid_constant__ StageParams<T> P) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   StageSmem<T> &S = *reinterpret_cast<StageSmem<T> *>(smem_raw);
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;

@@ -279,10 +279,11 @@ struct BlockExec {
   }
 };
 
-template <typename T, int N>
+// Tile of L = 2^LOG2L_ lines of N cells (LOG2L_ < 0: the widest tile within ~48 KiB).
+template <typename T, int N, int LOG2L_ = -1>
 struct Pow2Tile {
   static constexpr int LOG2N = fft::ilog2(N);
-  static constexpr int LOG2L = fft::tile_log2L(N, (int)sizeof(T)), L = 1 << LOG2L, LD = L + 1;
+  static constexpr int LOG2L = LOG2L_ >= 0 ? LOG2L_ : fft::tile_log2L(N, (int)sizeof(T)), L = 1 << LOG2L, LD = L + 1;
   static constexpr size_t TW = (size_t)N * 2 * sizeof(T);                        // twiddles
   static constexpr size_t RB = ((size_t)N * LD * sizeof(T) + 15) & ~size_t(15);  // real tile
   static constexpr size_t CB = (size_t)N * (L / 2) * 2 * sizeof(T);              // one complex buffer
@@ -292,9 +293,9 @@ struct Pow2Tile {
 // One axis pass over L lines of N = 2^a cells: x lines are rows (r = k ny + j), y / z lines
 // are L consecutive x at fixed k / j.  Mode 0 forward, 1 inverse, 2 forward, division by
 // lambda_x + lambda_y + lambda_z (zero mode dropped) and inverse (z axis).
-template <typename T, int N>
+template <typename T, int N, int LOG2L_>
 __global__ void __launch_bounds__(256) pow2_transform_kernel(const __grid_constant__ TransformParams<T> P) {
-  using G = Pow2Tile<T, N>;
+  using G = Pow2Tile<T, N, LOG2L_>;
   constexpr int L = G::L, LD = G::LD, LOG2L = G::LOG2L, LOG2N = G::LOG2N;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   fft::Cx<T> *tw = reinterpret_cast<fft::Cx<T> *>(smem_raw);
@@ -409,13 +410,13 @@ __global__ void __launch_bounds__(256) pow2_transform_kernel(const __grid_consta
   }
 }
 
-template <typename T, int N>
-cudaError_t launch_pow2(const TransformParams<T> &P, cudaStream_t s) {
-  using G = Pow2Tile<T, N>;
+template <typename T, int N, int LOG2L_>
+cudaError_t launch_pow2_tile(const TransformParams<T> &P, cudaStream_t s) {
+  using G = Pow2Tile<T, N, LOG2L_>;
   static bool configured = false;
   if (!configured) {
-    const cudaError_t e = cudaFuncSetAttribute(pow2_transform_kernel<T, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)G::SMEM);
+    const cudaError_t e = cudaFuncSetAttribute(pow2_transform_kernel<T, N, LOG2L_>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)G::SMEM);
     if (e != cudaSuccess) return e;
     configured = true;
   }
@@ -424,8 +425,19 @@ cudaError_t launch_pow2(const TransformParams<T> &P, cudaStream_t s) {
     grid = dim3((unsigned)(((size_t)P.nz * P.ny + G::L - 1) / G::L), 1, 1);
   else
     grid = dim3((unsigned)((P.nx + G::L - 1) / G::L), (unsigned)(P.axis == 1 ? P.nz : P.ny), 1);
-  pow2_transform_kernel<T, N><<<grid, 256, G::SMEM, s>>>(P);
+  pow2_transform_kernel<T, N, LOG2L_><<<grid, 256, G::SMEM, s>>>(P);
   return cudaGetLastError();
+}
+
+// The widest tile, unless that leaves the pass a handful of blocks (a 2D grid of 256 x 128
+// gets 8): then two-line tiles spread its lines over more SMs.  Larger grids keep the wide
+// tile, whose blocks do more work each (and concurrent solves fill the GPU anyway).
+template <typename T, int N>
+cudaError_t launch_pow2(const TransformParams<T> &P, cudaStream_t s) {
+  const size_t lines = P.axis == 0 ? (size_t)P.nz * P.ny : (size_t)P.nx * (P.axis == 1 ? P.nz : P.ny);
+  const size_t blocks = (lines + Pow2Tile<T, N>::L - 1) / Pow2Tile<T, N>::L;
+  if (blocks < 32 && Pow2Tile<T, N>::L > 2) return launch_pow2_tile<T, N, 1>(P, s);
+  return launch_pow2_tile<T, N, -1>(P, s);
 }
 
 bool transform_pow2(int n) { return n >= 8 && n <= 2048 && (n & (n - 1)) == 0; }

@@ -2,9 +2,9 @@
 // by thread (256 "threads", one phase after another) so the tests can compare the exact
 // device code path with scipy's orthonormal DCT / Hartley transforms on the CPU.
 //
-//   fft_tile_host <f32|f64> <N> <kind 0 DCT|1 DHT> <inverse 0|1>
-//   stdin: N * L doubles, row m of the tile then the next (L = the tile width for N), stdout
-//   the transformed tile in the same layout.
+//   fft_tile_host <f32|f64> <N> <kind 0 DCT|1 DHT> <inverse 0|1> [narrow 0|1]
+//   stdin: N * L doubles, row m of the tile then the next (L = the tile width for N, or 2 with
+//   narrow = 1), stdout the transformed tile in the same layout.
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -23,9 +23,9 @@ struct SerialExec {
   }
 };
 
-template <typename T, int N>
-int run(int kind, int inverse) {
-  constexpr int LOG2L = tile_log2L(N, (int)sizeof(T)), L = 1 << LOG2L, LD = L + 1;
+template <typename T, int N, int LOG2L>
+int run_tile(int kind, int inverse) {
+  constexpr int L = 1 << LOG2L, LD = L + 1;
   std::vector<double> in((size_t)N * L);
   if (fread(in.data(), sizeof(double), in.size(), stdin) != in.size()) return 2;
   std::vector<Cx<T>> tw(N), post(N), cs(N);
@@ -51,25 +51,32 @@ int run(int kind, int inverse) {
   return 0;
 }
 
+template <typename T, int N>
+int run(int kind, int inverse, int narrow) {
+  if (narrow) return run_tile<T, N, 1>(kind, inverse);
+  return run_tile<T, N, tile_log2L(N, (int)sizeof(T))>(kind, inverse);
+}
+
 template <typename T>
-int dispatch(int n, int kind, int inverse) {
+int dispatch(int n, int kind, int inverse, int narrow) {
   switch (n) {
-    case 8: return run<T, 8>(kind, inverse);
-    case 16: return run<T, 16>(kind, inverse);
-    case 32: return run<T, 32>(kind, inverse);
-    case 64: return run<T, 64>(kind, inverse);
-    case 128: return run<T, 128>(kind, inverse);
-    case 256: return run<T, 256>(kind, inverse);
-    case 512: return run<T, 512>(kind, inverse);
-    case 1024: return run<T, 1024>(kind, inverse);
-    case 2048: return run<T, 2048>(kind, inverse);
+    case 8: return run<T, 8>(kind, inverse, narrow);
+    case 16: return run<T, 16>(kind, inverse, narrow);
+    case 32: return run<T, 32>(kind, inverse, narrow);
+    case 64: return run<T, 64>(kind, inverse, narrow);
+    case 128: return run<T, 128>(kind, inverse, narrow);
+    case 256: return run<T, 256>(kind, inverse, narrow);
+    case 512: return run<T, 512>(kind, inverse, narrow);
+    case 1024: return run<T, 1024>(kind, inverse, narrow);
+    case 2048: return run<T, 2048>(kind, inverse, narrow);
   }
   return 3;
 }
 
 int main(int argc, char **argv) {
-  if (argc != 5) return 1;
+  if (argc != 5 && argc != 6) return 1;
   const bool f64 = std::strcmp(argv[1], "f64") == 0;
   const int n = std::atoi(argv[2]), kind = std::atoi(argv[3]), inverse = std::atoi(argv[4]);
-  return f64 ? dispatch<double>(n, kind, inverse) : dispatch<float>(n, kind, inverse);
+  const int narrow = argc == 6 ? std::atoi(argv[5]) : 0;
+  return f64 ? dispatch<double>(n, kind, inverse, narrow) : dispatch<float>(n, kind, inverse, narrow);
 }

@@ -36,9 +36,9 @@ def harness(tmp_path_factory):
     return exe
 
 
-def _run(exe, prec, n, kind, inverse, x):
-    r = subprocess.run([str(exe), prec, str(n), str(kind), str(int(inverse))], input=x.astype(np.float64).tobytes(),
-                       capture_output=True, check=True)
+def _run(exe, prec, n, kind, inverse, x, narrow=False):
+    r = subprocess.run([str(exe), prec, str(n), str(kind), str(int(inverse)), str(int(narrow))],
+                       input=x.astype(np.float64).tobytes(), capture_output=True, check=True)
     return np.frombuffer(r.stdout, dtype=np.float64).reshape(x.shape)
 
 
@@ -49,16 +49,17 @@ def _want(x, kind, inverse):
     return (f.real - f.imag) / np.sqrt(x.shape[0])
 
 
+@pytest.mark.parametrize("narrow", [False, True], ids=["wide", "two_lines"])
 @pytest.mark.parametrize("prec", ["f64", "f32"])
 @pytest.mark.parametrize("n", [8, 16, 32, 64, 128, 256, 512, 1024, 2048])
-def test_tile_transform_matches_orthonormal_bases(harness, prec, n):
+def test_tile_transform_matches_orthonormal_bases(harness, prec, n, narrow):
     rng = np.random.default_rng(n)
-    x = rng.standard_normal((n, _lines(n, 8 if prec == "f64" else 4)))
+    x = rng.standard_normal((n, 2 if narrow else _lines(n, 8 if prec == "f64" else 4)))
     if prec == "f32":
         x = x.astype(np.float32).astype(np.float64)
     for kind in (0, 1):
         for inverse in (False, True):
-            got = _run(harness, prec, n, kind, inverse, x)
+            got = _run(harness, prec, n, kind, inverse, x, narrow)
             want = _want(x, kind, inverse)
             err = np.abs(got - want).max() / np.abs(want).max()
             assert err < TOL[prec], (n, kind, inverse, err)
