@@ -79,7 +79,7 @@ struct AeroNs3dPlan {
   size_t esz;                     // bytes per element
   size_t nu, nv, nw, nc;          // element counts of u, v, w and cell arrays
   size_t off_uh, off_vh, off_wh, off_up, off_vp, off_wp, off_tha, off_thb, off_pa, off_nu;
-  size_t off_small, off_scalars, off_status, off_partials, total;
+  size_t off_small, off_scalars, off_status, off_partials, off_psum, total;
   AxisInfo ax[3];
   int zc, nblocks, nq;
   int pu, pn;                     // row pitches of the stage-start u copy and of nu
@@ -150,26 +150,22 @@ aero::CompRules<T> comp_rules(const AeroNs3dConfig &c, int comp, int pitch = 0) 
   return r;
 }
 
-// sum of a[r * stride + off] over rows, in a fixed order, into out (double)
+// Block b of the grid sums a[r * stride + off] over its contiguous slice of the rows, in a
+// fixed order, into out[b] (double); the consumer adds the PLANE_PARTS partials in order, so
+// the total is the same on every run.
+constexpr int PLANE_PARTS = 64;
+
 template <typename T>
-__global__ void __launch_bounds__(512) plane_sum_kernel(const T *a0, size_t stride0, size_t off0, double *out0, const T *a1, size_t stride1,
-                                 size_t off1, double *out1, int rows) {
-  __shared__ double red[2][32];
-  constexpr int U = 16;  // rows in flight per thread: the loads of a chunk are independent
+__global__ void __launch_bounds__(256) plane_sum_kernel(const T *a0, size_t stride0, size_t off0, double *out0,
+                                                        const T *a1, size_t stride1, size_t off1, double *out1,
+                                                        int rows) {
+  __shared__ double red[2][8];
+  const int per = (rows + gridDim.x - 1) / gridDim.x;
+  const int r0 = blockIdx.x * per, r1 = min(rows, r0 + per);
   double s0 = 0.0, s1 = 0.0;
-  for (int base = 0; base < rows; base += U * (int)blockDim.x) {
-    T x0[U], x1[U];
-#pragma unroll
-    for (int q = 0; q < U; ++q) {
-      const int r = base + q * (int)blockDim.x + (int)threadIdx.x;
-      x0[q] = (a0 && r < rows) ? a0[(size_t)r * stride0 + off0] : T(0);
-      x1[q] = (a1 && r < rows) ? a1[(size_t)r * stride1 + off1] : T(0);
-    }
-#pragma unroll
-    for (int q = 0; q < U; ++q) {
-      s0 += (double)x0[q];
-      s1 += (double)x1[q];
-    }
+  for (int r = r0 + (int)threadIdx.x; r < r1; r += blockDim.x) {
+    if (a0) s0 += (double)a0[(size_t)r * stride0 + off0];
+    if (a1) s1 += (double)a1[(size_t)r * stride1 + off1];
   }
   s0 = aero::warp_sum(s0);
   s1 = aero::warp_sum(s1);
@@ -184,8 +180,8 @@ __global__ void __launch_bounds__(512) plane_sum_kernel(const T *a0, size_t stri
       x += red[0][q];
       y += red[1][q];
     }
-    if (a0) *out0 = x;
-    if (a1) *out1 = y;
+    if (a0) out0[blockIdx.x] = x;
+    if (a1) out1[blockIdx.x] = y;
   }
 }
 
@@ -413,9 +409,10 @@ int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom
   CUDA_TRY(aero::launch_dt<T>(D, s));
 
   const int rows = nz * ny;
+  double *psum = reinterpret_cast<double *>(ws + p->off_psum);  // [u0 outlet | inlet | 3 stages x 2] x parts
   if (tunnel) {
-    plane_sum_kernel<T><<<1, 512, 0, s>>>(upb, p->pu, nx, sc + aero::SC_SUM_U0, S.u_inlet, 1, 0,
-                                          sc + aero::SC_SUM_INLET, rows);
+    plane_sum_kernel<T><<<PLANE_PARTS, 256, 0, s>>>(upb, p->pu, nx, psum, S.u_inlet, 1, 0, psum + PLANE_PARTS,
+                                                    rows);
     CUDA_TRY(cudaGetLastError());
   }
 
@@ -425,11 +422,12 @@ int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom
   for (int st = 0; st < 3; ++st) {
     const T *up = upb, *vp = st == 0 ? v0 : vpb, *wp = st == 0 ? w0 : wpb;
     if (tunnel) {
-      double *sums = sc + aero::SC_SUMS + 3 * st;
-      plane_sum_kernel<T><<<1, 512, 0, s>>>(up, p->pu, nx, sums, up, p->pu, nx - 1, sums + 1, rows);
+      double *sums = psum + (2 + 2 * st) * PLANE_PARTS;  // outlet column, the one before it
+      plane_sum_kernel<T><<<PLANE_PARTS, 256, 0, s>>>(up, p->pu, nx, sums, up, p->pu, nx - 1, sums + PLANE_PARTS,
+                                                      rows);
       CUDA_TRY(cudaGetLastError());
-      CUDA_TRY(aero::launch_outlet_corr<T>(sums, sc + aero::SC_SUM_U0, sc + aero::SC_SUM_INLET, small, RK[st][0],
-                                           RK[st][1], 1.0 / c.h, 1.0 / rows, small + 1, s));
+      CUDA_TRY(aero::launch_outlet_corr<T>(sums, sums + PLANE_PARTS, psum, psum + PLANE_PARTS, PLANE_PARTS, small,
+                                           RK[st][0], RK[st][1], 1.0 / c.h, 1.0 / rows, small + 1, s));
     }
     if (les && st > 0) {
       aero::NuParams<T> N = NP;
@@ -728,6 +726,7 @@ int aero_ns3d_plan_create(const AeroNs3dConfig *cfg, AeroNs3dPlan **plan) {
   p->nblocks = (int)(((nx + 31) / 32) * ((ny + 7) / 8) * ((nz + p->zc - 1) / p->zc));
   p->nq = c.nbody * 9 + (c.thermal ? c.n_tbody : 0);
   p->off_partials = take(sizeof(double) * 3 * (size_t)p->nblocks * std::max(p->nq, 1));
+  p->off_psum = take(sizeof(double) * 8 * PLANE_PARTS);
   const int ns[3] = {c.nx, c.ny, c.nz};
   for (int a = 0; a < 3; ++a) {
     AxisInfo &x = p->ax[a];

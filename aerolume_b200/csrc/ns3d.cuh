@@ -159,8 +159,8 @@ cudaError_t launch_copy_u(const T *, T *, int, int, int, int, unsigned long long
 template <typename T> cudaError_t launch_dt(const DtParams &, cudaStream_t);
 template <typename T> cudaError_t launch_outlet_sum(const T *, const T *, int, int, double *, cudaStream_t);
 template <typename T>
-cudaError_t launch_outlet_corr(const double *, const double *, const double *, const T *, double, double, double,
-                               double, T *, cudaStream_t);
+cudaError_t launch_outlet_corr(const double *, const double *, const double *, const double *, int, const T *, double,
+                               double, double, double, T *, cudaStream_t);
 template <typename T>
 cudaError_t launch_divergence(const T *, const T *, const T *, int, int, int, int, int, int, T, T *, cudaStream_t);
 template <typename T> cudaError_t launch_correct(const CorrectParams<T> &, cudaStream_t);

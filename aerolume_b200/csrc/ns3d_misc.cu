@@ -140,13 +140,23 @@ __global__ void outlet_sum_kernel(const T *__restrict__ u, const T *__restrict__
 
 // corr = (sum u_inlet - sum uh[..., nx]) / (ny nz) with sum uh[..., nx] blended from the
 // stage-start sums: sum lerp(up, u0, a) + b dt / h (sum up[nx-1] - sum up[nx]).
+// Outlet correction of a stage by linearity (core.py:281-297): the stage value's outlet sum is
+// (1 - a) sum up[nx] + a sum u0[nx] + b dt / h (sum up[nx-1] - sum up[nx]); every sum is the
+// in-order total of the plane-sum kernel's per-block partials.
 template <typename T>
-__global__ void outlet_corr_kernel(const double *sums_p, const double *sum_u0, const double *sum_inlet, const T *dt,
-                                   double a, double bscale, double inv_h, double inv_rows, T *corr) {
+__global__ void outlet_corr_kernel(const double *p_out, const double *p_in, const double *p_u0, const double *p_inlet,
+                                   int parts, const T *dt, double a, double bscale, double inv_h, double inv_rows,
+                                   T *corr) {
+  double so = 0.0, si = 0.0, s0 = 0.0, sn = 0.0;
+  for (int q = 0; q < parts; ++q) {
+    so += p_out[q];
+    si += p_in[q];
+    s0 += p_u0[q];
+    sn += p_inlet[q];
+  }
   const double bdt = (double)(T(bscale) * *dt);
-  const double so = sums_p[0], si = sums_p[1], s0 = *sum_u0;
   const double out = (1.0 - a) * so + a * s0 + bdt * inv_h * (si - so);
-  *corr = T((*sum_inlet - out) * inv_rows);
+  *corr = T((sn - out) * inv_rows);
 }
 
 // --------------------------------------------------------------------------------------
@@ -462,9 +472,10 @@ cudaError_t launch_outlet_sum(const T *u, const T *u0, int nx, int rows, double 
 }
 
 template <typename T>
-cudaError_t launch_outlet_corr(const double *sums_p, const double *sum_u0, const double *sum_inlet, const T *dt,
-                               double a, double b, double inv_h, double inv_rows, T *corr, cudaStream_t s) {
-  outlet_corr_kernel<T><<<1, 1, 0, s>>>(sums_p, sum_u0, sum_inlet, dt, a, b, inv_h, inv_rows, corr);
+cudaError_t launch_outlet_corr(const double *p_out, const double *p_in, const double *p_u0, const double *p_inlet,
+                               int parts, const T *dt, double a, double b, double inv_h, double inv_rows, T *corr,
+                               cudaStream_t s) {
+  outlet_corr_kernel<T><<<1, 1, 0, s>>>(p_out, p_in, p_u0, p_inlet, parts, dt, a, b, inv_h, inv_rows, corr);
   return cudaGetLastError();
 }
 
@@ -512,8 +523,8 @@ cudaError_t launch_psi_accumulate(const T *psi, T *pw, size_t n, T wgt, int mode
   template cudaError_t launch_dt<T>(const DtParams &, cudaStream_t);                                                \
   template cudaError_t launch_copy_u<T>(const T *, T *, int, int, int, int, unsigned long long *, cudaStream_t);                                                \
   template cudaError_t launch_outlet_sum<T>(const T *, const T *, int, int, double *, cudaStream_t);                 \
-  template cudaError_t launch_outlet_corr<T>(const double *, const double *, const double *, const T *, double,      \
-                                             double, double, double, T *, cudaStream_t);                             \
+  template cudaError_t launch_outlet_corr<T>(const double *, const double *, const double *, const double *, int,  \
+                                             const T *, double, double, double, double, T *, cudaStream_t);       \
   template cudaError_t launch_divergence<T>(const T *, const T *, const T *, int, int, int, int, int, int, T, T *,    \
                                             cudaStream_t);                                                           \
   template cudaError_t launch_correct<T>(const CorrectParams<T> &, cudaStream_t);                                   \
