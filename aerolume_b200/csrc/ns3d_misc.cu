@@ -268,7 +268,7 @@ constexpr int SMOKE_NSLOT = 6;
 constexpr int SMOKE_LOADS = (SMOKE_PPL + SMOKE_TX * SMOKE_TY - 1) / (SMOKE_TX * SMOKE_TY);      // 2
 
 template <typename T>
-__global__ void __launch_bounds__(SMOKE_TX *SMOKE_TY) smoke_kernel(const __grid_constant__ SmokeParams<T> P) {
+__global__ void __launch_bounds__(SMOKE_TX *SMOKE_TY, sizeof(T) == 4 ? 4 : 1) smoke_kernel(const __grid_constant__ SmokeParams<T> P) {
   __shared__ T ring[SMOKE_NSLOT][SMOKE_PPL];
   const int nx = P.nx, ny = P.ny, nz = P.nz;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * SMOKE_TX + tx;
