@@ -326,6 +326,16 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) stage_kernel(c
     size_t wu = 0, wv = 0, ww = 0, wt = 0;
 
     if (valid) {
+      // step-start values of this cell's faces for the RK blend, requested before the
+      // tendencies so that their DRAM latency hides behind the arithmetic
+      const size_t iu = ((size_t)k * ny + j) * (nx + 1) + i;
+      const size_t iv = ((size_t)k * (ny + 1) + j) * nx + i;
+      const size_t iw = ((size_t)k * ny + j) * nx + i;
+      const bool blend = a != T(0);
+      const T u0v = blend ? __ldg(P.u0 + iu) : T(0);
+      const T v0v = blend ? __ldg(P.v0 + iv) : T(0);
+      const T w0v = blend ? __ldg(P.w0 + iw) : T(0);
+      const T t0v = (blend && thermal) ? __ldg(P.th0 + iw) : T(0);
       // the interface below this plane, carried from the previous plane
       const T zu_l = zu, zv_l = zv, zw_l = zw, z13_l = z13, z23_l = z23, z33_l = z33, zth_l = zth;
       z_interface(kc);
@@ -413,9 +423,6 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) stage_kernel(c
       }
 
       // ================= boundary tendencies and RK update (core.py:527-543, 819-827) =
-      const size_t iu = ((size_t)k * ny + j) * (nx + 1) + i;
-      const size_t iv = ((size_t)k * (ny + 1) + j) * nx + i;
-      const size_t iw = ((size_t)k * ny + j) * nx + i;
       const T up0 = VEL(0, 0, y, x), vp0 = VEL(1, 0, y, x), wp0 = VEL(2, 0, y, x);
       T uh, vh, wh;
       if (a == T(0)) {
@@ -423,9 +430,9 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) stage_kernel(c
         vh = vp0 + lv * bdt;
         wh = wp0 + lw * bdt;
       } else {
-        uh = lerp_t<T>(up0, __ldg(P.u0 + iu), a) + lu * bdt;
-        vh = lerp_t<T>(vp0, __ldg(P.v0 + iv), a) + lv * bdt;
-        wh = lerp_t<T>(wp0, __ldg(P.w0 + iw), a) + lw * bdt;
+        uh = lerp_t<T>(up0, u0v, a) + lu * bdt;
+        vh = lerp_t<T>(vp0, v0v, a) + lv * bdt;
+        wh = lerp_t<T>(wp0, w0v, a) + lw * bdt;
       }
       if (!P.px && i == 0) uh = P.closed ? T(0) : P.u_inlet[(size_t)k * ny + j];
       if (!P.py && j == 0) vh = T(0);
@@ -530,7 +537,7 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) stage_kernel(c
         }
         const T D = ((fxr - fxl) + (fyr - fyl) + (zth - zth_l)) * inv;
         const size_t ic = ((size_t)k * ny + j) * nx + i;
-        T ch = (a == T(0) ? c : lerp_t<T>(c, __ldg(P.th0 + ic), a)) - bdt * D;
+        T ch = (a == T(0) ? c : lerp_t<T>(c, t0v, a)) - bdt * D;
         if (P.has_win && k >= wk0 && k < wk1 && j >= wj0 && j < wj1 && i >= wi0 && i < wi1) {
           wt = ((size_t)(k - wk0) * wyn + (j - wj0)) * wxn + (i - wi0);
           if (P.skin) ch = ch + (bdt * P.kappa) * P.skin[wt];
