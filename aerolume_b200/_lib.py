@@ -17,6 +17,8 @@ LIB_PATH = Path(__file__).resolve().parent / (
 ABI_VERSION = 1
 MAX_BODIES = 8
 TRACE_EVENTS = 19
+# output fields of aero_ns3d_fields, in its order
+FIELD_NAMES = ("uc", "vc", "wc", "speed", "vorticity", "q", "nut")
 
 F32, F64 = 0, 1
 ADV = {"upwind3": 0, "central": 1}
@@ -31,7 +33,8 @@ EXPORTS = ("aero_abi_version", "aero_last_error", "aero_ns3d_plan_create", "aero
            "aero_ns3d_poisson_solve",
            "aero_ns3d_project", "aero_ns3d_read_status", "aero_debug_check", "aero_ns3d_poisson_solve_static",
            "aero_ns2d_plan_create", "aero_ns2d_plan_destroy", "aero_ns2d_workspace_bytes",
-           "aero_ns2d_workspace_init", "aero_ns2d_step", "aero_ns2d_poisson_solve")
+           "aero_ns2d_workspace_init", "aero_ns2d_step", "aero_ns2d_poisson_solve", "aero_ns3d_fields",
+           "aero_ns3d_probe")
 
 
 class Ns3dConfig(C.Structure):
@@ -134,12 +137,17 @@ def lib() -> C.CDLL:
     L.aero_ns2d_step.argtypes = [C.c_void_p, C.POINTER(Ns2dFields), C.POINTER(Ns2dGeom), C.c_void_p, C.c_void_p,
                                  C.c_void_p]
     L.aero_ns2d_poisson_solve.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.aero_ns3d_fields.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(Ns3dGeom),
+                                   C.POINTER(C.c_void_p), C.c_void_p]
+    L.aero_ns3d_probe.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_double),
+                                  C.POINTER(C.c_double), C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]
     L.aero_debug_check.restype = C.c_int
     for name in ("aero_ns3d_plan_create", "aero_ns3d_workspace_init", "aero_ns3d_step", "aero_ns3d_step_traced",
                  "aero_ns3d_smoke",
                  "aero_ns3d_poisson_solve",
                  "aero_ns3d_project", "aero_ns3d_read_status", "aero_debug_check", "aero_ns3d_poisson_solve_static",
-                 "aero_ns2d_plan_create", "aero_ns2d_workspace_init", "aero_ns2d_step", "aero_ns2d_poisson_solve"):
+                 "aero_ns2d_plan_create", "aero_ns2d_workspace_init", "aero_ns2d_step", "aero_ns2d_poisson_solve",
+                 "aero_ns3d_fields", "aero_ns3d_probe"):
         getattr(L, name).restype = C.c_int
     if L.aero_abi_version() != ABI_VERSION:
         raise RuntimeError(f"{LIB_PATH.name} has ABI {L.aero_abi_version()}, expected {ABI_VERSION}; rebuild it")

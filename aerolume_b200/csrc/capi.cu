@@ -647,6 +647,36 @@ int poisson_static_impl(const AeroNs3dPlan *plan, const void *f, void *psi, cuda
   return poisson_passes<T>(&q, static_cast<const T *>(f), static_cast<T *>(psi), scratch, s);
 }
 
+template <typename T>
+int fields_impl(const AeroNs3dPlan *p, const void *u, const void *v, const void *w, const AeroNs3dGeom *g,
+                void *const *out, cudaStream_t s) {
+  const AeroNs3dConfig &c = p->cfg;
+  aero::FieldsParams<T> F{};
+  F.nx = c.nx;
+  F.ny = c.ny;
+  F.nz = c.nz;
+  F.les = c.les;
+  F.inv_h = T(1.0 / c.h);
+  F.cd2 = T(c.les == AERO_LES_VREMAN ? c.les_c * c.h * c.h : c.les_c * c.les_c * c.h * c.h);
+  F.ru = comp_rules<T>(c, 0);
+  F.rv = comp_rules<T>(c, 1);
+  F.rw = comp_rules<T>(c, 2);
+  F.u = static_cast<const T *>(u);
+  F.v = static_cast<const T *>(v);
+  F.w = static_cast<const T *>(w);
+  const bool has_win = !(c.window[1] <= c.window[0] || c.window[3] <= c.window[2] || c.window[5] <= c.window[4]) &&
+                       c.nbody > 0 && g && g->chi_c;
+  F.has_win = has_win;
+  for (int q = 0; q < 6; ++q) F.win[q] = has_win ? c.window[q] : 0;
+  F.wnx = c.window[5] - c.window[4];
+  F.wny = c.window[3] - c.window[2];
+  F.chi_c = has_win ? static_cast<const T *>(g->chi_c) : nullptr;
+  for (int q = 0; q < AERO_FIELD_COUNT; ++q) F.out[q] = static_cast<T *>(out[q]);
+  F.gradient = out[4] || out[5] || out[6];
+  CUDA_TRY(aero::launch_fields<T>(F, s));
+  return AERO_OK;
+}
+
 bool window_empty(const int32_t *w) { return w[1] <= w[0] || w[3] <= w[2] || w[5] <= w[4]; }
 
 }  // namespace
@@ -806,6 +836,31 @@ int aero_ns3d_poisson_solve_static(const AeroNs3dPlan *plan, const void *f, void
   auto s = static_cast<cudaStream_t>(stream);
   return plan->cfg.dtype == AERO_F64 ? poisson_static_impl<double>(plan, f, psi, s)
                                      : poisson_static_impl<float>(plan, f, psi, s);
+}
+
+int aero_ns3d_fields(const AeroNs3dPlan *plan, const void *u, const void *v, const void *w, const AeroNs3dGeom *g,
+                     void *const *out, void *stream) {
+  if (!plan || !u || !v || !w || !out) return fail(AERO_EINVAL, "null argument");
+  auto s = static_cast<cudaStream_t>(stream);
+  return plan->cfg.dtype == AERO_F64 ? fields_impl<double>(plan, u, v, w, g, out, s)
+                                     : fields_impl<float>(plan, u, v, w, g, out, s);
+}
+
+int aero_ns3d_probe(const AeroNs3dPlan *plan, const void *field, const int32_t shape[3], const double origin[3],
+                    const double off[3], const void *pts, int64_t npts, void *out, void *stream) {
+  if (!plan || !field || !shape || !origin || !off || (npts > 0 && (!pts || !out)))
+    return fail(AERO_EINVAL, "null argument");
+  if (npts < 0 || shape[0] < 1 || shape[1] < 1 || shape[2] < 1) return fail(AERO_EINVAL, "bad shape or point count");
+  auto s = static_cast<cudaStream_t>(stream);
+  if (plan->cfg.dtype == AERO_F64)
+    CUDA_TRY(aero::launch_probe<double>(static_cast<const double *>(field), shape[2], shape[1], shape[0], origin,
+                                        plan->cfg.h, off, static_cast<const double *>(pts), npts,
+                                        static_cast<double *>(out), s));
+  else
+    CUDA_TRY(aero::launch_probe<float>(static_cast<const float *>(field), shape[2], shape[1], shape[0], origin,
+                                       plan->cfg.h, off, static_cast<const float *>(pts), npts,
+                                       static_cast<float *>(out), s));
+  return AERO_OK;
 }
 
 int aero_ns3d_project(const AeroNs3dPlan *plan, void *u, void *v, void *w, void *psi, void *workspace, void *stream) {

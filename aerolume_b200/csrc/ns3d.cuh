@@ -150,6 +150,18 @@ struct TransformParams {
   const T *dt;
 };
 
+// output fields (fields3d.cu): out[0..6] = centred u, v, w, speed, vorticity, Q, nu_t (or NULL)
+template <typename T>
+struct FieldsParams {
+  int nx, ny, nz, les, gradient;
+  T inv_h, cd2;
+  CompRules<T> ru, rv, rw;
+  const T *u, *v, *w;
+  int has_win, win[6], wnx, wny;
+  const T *chi_c;
+  T *out[7];
+};
+
 template <typename T> size_t stage_smem_bytes();
 template <typename T> cudaError_t launch_stage(const StageParams<T> &, cudaStream_t);
 template <typename T> cudaError_t launch_nu(const NuParams<T> &, cudaStream_t);
@@ -172,6 +184,10 @@ template <typename T> cudaError_t launch_transform(const TransformParams<T> &, c
 // true when an axis of n cells runs the compile-time power-of-two transform (8 <= n <= 2048),
 // which also takes the divergence / pressure fusions of TransformParams
 bool transform_pow2(int n);
+template <typename T> cudaError_t launch_fields(const FieldsParams<T> &, cudaStream_t);
+template <typename T>
+cudaError_t launch_probe(const T *, int, int, int, const double *, double, const double *, const T *, long long, T *,
+                         cudaStream_t);
 template <typename T>
 cudaError_t launch_axis_tables(int, int, int, double, T *, T *, T *, double *, T *, cudaStream_t);
 

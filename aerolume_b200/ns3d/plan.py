@@ -10,6 +10,7 @@ fallback to a CPU or plain-torch path.
 from __future__ import annotations
 
 import ctypes as C
+import math
 
 import numpy as np
 import torch
@@ -279,6 +280,61 @@ class Ns3dPlan:
             if not sources:
                 g.dye_weight = None
         check(_lib.lib().aero_ns3d_smoke(self._handle, C.byref(f), C.byref(g), self._stream()), "aero_ns3d_smoke")
+        return out
+
+    def fields(self, u, v, w, names=_lib.FIELD_NAMES):
+        """Cell-centred output fields of the state (u, v, w): any of "uc", "vc", "wc" (centred
+        velocity), "speed", "vorticity", "q", "nut"; returns {name: (nz, ny, nx) tensor}."""
+        nz, ny, nx = self.shape
+        self._check("u", u, (nz, ny, nx + 1))
+        self._check("v", v, (nz, ny + 1, nx))
+        self._check("w", w, (nz + 1, ny, nx))
+        res = {}
+        ptrs = (C.c_void_p * len(_lib.FIELD_NAMES))()
+        for q, name in enumerate(_lib.FIELD_NAMES):
+            if name in names:
+                res[name] = torch.empty(self.shape, device=self.device, dtype=self.dtype)
+                ptrs[q] = res[name].data_ptr()
+        unknown = set(names) - set(_lib.FIELD_NAMES)
+        if unknown:
+            raise KeyError(f"unknown fields {sorted(unknown)}; available: {', '.join(_lib.FIELD_NAMES)}")
+        check(_lib.lib().aero_ns3d_fields(self._handle, C.c_void_p(u.data_ptr()), C.c_void_p(v.data_ptr()),
+                                          C.c_void_p(w.data_ptr()), C.byref(self.geom_c), ptrs, self._stream()),
+              "aero_ns3d_fields")
+        return res
+
+    def slice(self, u, v, w, name, axis, position):
+        """A planar cut of an output field at ``position`` normal to ``axis`` ("x", "y", "z"):
+        linear interpolation between the two nearest cell planes, clamped to the domain
+        (ns3d/solver.py:1505-1540); (nz, nx) for "y", (ny, nx) for "z", (nz, ny) for "x"."""
+        dim = {"z": 0, "y": 1, "x": 2}[axis]
+        n = self.shape[dim]
+        origin = float(getattr(self.ops, ("z0", "y0", "x0")[dim], 0.0))
+        f = min(max((position - origin) / float(self.ops.h) - 0.5, 0.0), n - 1.0)
+        i0 = min(math.floor(f), max(n - 2, 0))
+        t = f - i0
+        i1 = min(i0 + 1, n - 1)
+        full = self.fields(u, v, w, (name,))[name]
+        a, b = full.narrow(dim, i0, 1), full.narrow(dim, i1, 1)
+        return ((1.0 - t) * a + t * b).squeeze(dim)
+
+    def probe(self, field, pts, off=(0.5, 0.5, 0.5), origin=None):
+        """Trilinear samples of ``field`` at points (P, 3) = (x, y, z); entry (k, j, i) of the
+        field sits at origin + ((i, j, k) + off) h (off (0, .5, .5) for u-faces and so on)."""
+        if origin is None:
+            origin = (float(getattr(self.ops, "x0", 0.0)), float(getattr(self.ops, "y0", 0.0)),
+                      float(getattr(self.ops, "z0", 0.0)))
+        if not (torch.is_tensor(field) and field.device == self.device and field.dtype == self.dtype and field.dim() == 3
+                and field.is_contiguous()):
+            raise RuntimeError(f"field must be a contiguous 3D {self.dtype} tensor on {self.device}")
+        self._check("pts", pts, (pts.shape[0], 3))
+        out = torch.empty(pts.shape[0], device=self.device, dtype=self.dtype)
+        shape = (C.c_int32 * 3)(*field.shape)
+        o = (C.c_double * 3)(*origin)
+        f = (C.c_double * 3)(*off)
+        check(_lib.lib().aero_ns3d_probe(self._handle, C.c_void_p(field.data_ptr()), shape, o, f,
+                                         C.c_void_p(pts.data_ptr()), pts.shape[0], C.c_void_p(out.data_ptr()),
+                                         self._stream()), "aero_ns3d_probe")
         return out
 
     def poisson_solve(self, f, psi=None):

@@ -18,6 +18,8 @@
  *   aero_ns3d_project          ns3d/core.py:604 project3d
  *   aero_ns3d_poisson_solve    ns3d/poisson.py:152 PoissonSolver3D.solve
  *   aero_ns3d_workspace_bytes  (no counterpart: the reference allocates inside torch)
+ *   aero_ns3d_fields           ns3d/fields.py:45 gradient_field, ns3d/solver.py:1374 _centred
+ *   aero_ns3d_probe            ns3d/fields.py:78 trilinear (surface probes, slices, wake lines)
  *   aero_ns2d_plan_create      ns2d/core.py:182 make_operators (the per-config constants)
  *   aero_ns2d_step             ns2d/core.py:815 step_full (no placed physics), with the dye
  *                              update of its lines 959-962 (core.py:703 advect_dye,
@@ -184,6 +186,23 @@ int aero_ns3d_poisson_solve_static(const AeroNs3dPlan *plan, const void *f, void
 /* In place: (u, v, w) <- (u, v, w) - grad psi with lap psi = div(u, v, w); psi written. */
 int aero_ns3d_project(const AeroNs3dPlan *plan, void *u, void *v, void *w, void *psi, void *workspace,
                       void *stream);
+
+/* Cell-centred output fields of a state (u, v, w: the plan's staggered shapes), the B200 side of
+ * ns3d/fields.py:24-75 gradient_field and ns3d/solver.py:1374-1416 FlowSolver3D._centred:
+ * out[AERO_FIELD_U..AERO_FIELD_NUT] are (nz, ny, nx) device arrays, or NULL to skip one.  The
+ * eddy viscosity is switched off inside solids with g->chi_c (g may be NULL: no bodies). */
+enum {
+  AERO_FIELD_U = 0, AERO_FIELD_V = 1, AERO_FIELD_W = 2, AERO_FIELD_SPEED = 3,
+  AERO_FIELD_VORTICITY = 4, AERO_FIELD_Q = 5, AERO_FIELD_NUT = 6, AERO_FIELD_COUNT = 7
+};
+int aero_ns3d_fields(const AeroNs3dPlan *plan, const void *u, const void *v, const void *w, const AeroNs3dGeom *g,
+                     void *const *out, void *stream);
+
+/* Trilinear sampling (ns3d/fields.py:78 trilinear) of a (shape[0], shape[1], shape[2]) =
+ * (nz, ny, nx) field whose entry (k, j, i) sits at origin + ((i, j, k) + off) h, at npts
+ * points (x, y, z) (device, the plan's dtype); points outside are clamped to the edge. */
+int aero_ns3d_probe(const AeroNs3dPlan *plan, const void *field, const int32_t shape[3], const double origin[3],
+                    const double off[3], const void *pts, int64_t npts, void *out, void *stream);
 
 /* Device-side status word of the last step on this workspace (0 = fine; bit 0: a
  * non-finite value reached a reduction).  Reads through a host copy: synchronises. */

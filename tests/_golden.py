@@ -12,10 +12,8 @@ GOLDEN = Path(__file__).resolve().parent / "golden"
 CASES_3D = sorted(p.stem[len("ns3d_"):] for p in GOLDEN.glob("ns3d_*.npz"))
 
 
-def load_case(name):
-    z = np.load(GOLDEN / f"ns3d_{name}.npz")
-    meta = json.loads(str(z["meta"]))
-    arr = {k: z[k] for k in z.files if k != "meta"}
+def ops_from_meta(meta, arr):
+    """The Ops3D and Geometry3D of a golden case's metadata and arrays."""
     dt = np.float64 if meta["dtype"] == "float64" else np.float32
     ghost = {k: tuple(tuple((r[0], float(r[1])) for r in ax) for ax in v) for k, v in meta["ghost"].items()}
     ops = Ops3D(nx=meta["nx"], ny=meta["ny"], nz=meta["nz"], h=meta["h"], x0=meta["x0"], y0=meta["y0"],
@@ -30,6 +28,16 @@ def load_case(name):
     if not geom.empty:
         for n in ("chi_u", "chi_v", "chi_w", "chi_c", "a_u", "a_v", "a_w", "k_u", "k_v", "k_w"):
             setattr(geom, n, arr[n].astype(dt))
+    return ops, geom
+
+
+def load_case(name):
+    z = np.load(GOLDEN / f"ns3d_{name}.npz")
+    meta = json.loads(str(z["meta"]))
+    arr = {k: z[k] for k in z.files if k != "meta"}
+    ops, geom = ops_from_meta(meta, arr)
+    dt = np.float64 if meta["dtype"] == "float64" else np.float32
+    win = tuple(meta["window"])
     th = None
     if "thermal" in meta:
         t = meta["thermal"]
@@ -67,4 +75,14 @@ def load_case2d(name):
     if not geom.empty:
         for n in ("chi_u", "chi_v", "chi_c", "a_u", "a_v", "k_u", "k_v"):
             setattr(geom, n, arr[n].astype(dt))
+    return meta, ops, geom, arr
+
+
+def load_fields_case(tag):
+    """(ops, geom, arrays) of one case of fields3d.npz (arrays without the tag prefix)."""
+    z = np.load(GOLDEN / "fields3d.npz")
+    meta = json.loads(str(z[f"{tag}_meta"]))
+    arr = {k[len(tag) + 1:]: z[k] for k in z.files if k.startswith(tag + "_") and k != f"{tag}_meta"}
+    ops, geom = ops_from_meta(meta, arr)
+    ops.x0, ops.y0, ops.z0 = meta["origin"]
     return meta, ops, geom, arr
