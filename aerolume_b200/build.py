@@ -10,6 +10,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
@@ -49,8 +50,8 @@ def build(force: bool = False, verbose: bool = False, checked: bool = False) -> 
         return lib
     build_dir = PKG / ("_build_checked" if checked else "_build")
     build_dir.mkdir(exist_ok=True)
-    objs = []
     cc = nvcc()
+    cmds, objs = [], []
     for src in sources():
         obj = build_dir / (src.stem + ".o")
         cmd = [cc, *ARCH, *FLAGS, "-I", str(INCLUDE), "-dc", "-c", str(src), "-o", str(obj)]
@@ -58,8 +59,13 @@ def build(force: bool = False, verbose: bool = False, checked: bool = False) -> 
             cmd.append("-DAERO_BOUNDS_CHECK=1")
         if verbose:
             cmd += ["-Xptxas", "-v"]
-        subprocess.run(cmd, check=True)
+        cmds.append(cmd)
         objs.append(str(obj))
+    # one nvcc per translation unit, in parallel
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        for r in list(ex.map(lambda c: subprocess.run(c, capture_output=not verbose, text=True), cmds)):
+            if r.returncode != 0:
+                raise RuntimeError(f"nvcc failed: {' '.join(r.args)}\n{r.stdout or ''}{r.stderr or ''}")
     tmp = lib.with_suffix(".so.tmp")
     subprocess.run([cc, *ARCH, "-shared", "-Xcompiler", "-fPIC", *objs, "-o", str(tmp), "-lcudart"], check=True)
     os.replace(tmp, lib)

@@ -51,7 +51,7 @@ struct NuSmem {
   uint64_t bar[NuRing<T>::QSLOT];
 };
 
-template <typename T>
+template <typename T, int MODEL>
 __global__ void __launch_bounds__(TX *TY) nu_kernel(const __grid_constant__ NuParams<T> P) {
   __shared__ NuSmem<T> S;
   constexpr int QSLOT = NuRing<T>::QSLOT, AHEAD = NuRing<T>::AHEAD;
@@ -150,7 +150,7 @@ __global__ void __launch_bounds__(TX *TY) nu_kernel(const __grid_constant__ NuPa
                  (V3(2, 1, y + 1, x) - V3(2, 1, y, x)) * inv) *
                 qq;
       g[2][2] = -(g[0][0] + g[1][1]);
-      T nu = eddy_viscosity<T>(g, P.les, P.cd2);
+      T nu = eddy_viscosity<T>(g, MODEL, P.cd2);
       if (P.has_win && kn >= P.win[0] && kn < P.win[1] && cj >= P.win[2] && cj < P.win[3] && ci >= P.win[4] &&
           ci < P.win[5]) {
         const T chi = P.chi_c[((size_t)(kn - P.win[0]) * P.wny + (cj - P.win[2])) * P.wnx + (ci - P.win[4])];
@@ -186,7 +186,9 @@ struct StageSmem {
   uint64_t bar[NSLOT];
 };
 
-template <typename T>
+// UPWIND, LES and THERMAL are the plan's advection scheme, LES switch and heat switch, fixed at
+// compile time so that each configuration's body is straight-line code
+template <typename T, bool UPWIND, bool LES, bool THERMAL>
 __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) stage_kernel(const __grid_constant__ StageParams<T> P) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   StageSmem<T> &S = *reinterpret_cast<StageSmem<T> *>(smem_raw);
@@ -196,9 +198,7 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) stage_kernel(c
   const int kb = blockIdx.z * P.zc, ke = min(kb + P.zc, P.nz);
   const int nx = P.nx, ny = P.ny, nz = P.nz;
   const int i = i0 + tx, j = j0 + ty;
-  const bool les = P.les != AERO_LES_NONE;
-  const bool upwind = P.upwind != 0;
-  const bool thermal = P.thermal != 0;
+  constexpr bool les = LES, upwind = UPWIND, thermal = THERMAL;
   const T inv = P.inv_h;
   const int nq = P.nq;
 
@@ -617,24 +617,43 @@ size_t stage_smem_bytes() {
   return sizeof(StageSmem<T>);
 }
 
-template <typename T>
-cudaError_t launch_stage(const StageParams<T> &P, cudaStream_t s) {
+template <typename T, bool UPWIND, bool LES, bool THERMAL>
+cudaError_t launch_stage_cfg(const StageParams<T> &P, cudaStream_t s) {
   const size_t smem = sizeof(StageSmem<T>);
   static bool attr = false;
   if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(stage_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(stage_kernel<T, UPWIND, LES, THERMAL>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     attr = true;
   }
   dim3 grid((P.nx + TX - 1) / TX, (P.ny + TY - 1) / TY, (P.nz + P.zc - 1) / P.zc);
-  stage_kernel<T><<<grid, dim3(TX, TY), smem, s>>>(P);
+  stage_kernel<T, UPWIND, LES, THERMAL><<<grid, dim3(TX, TY), smem, s>>>(P);
   return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_stage(const StageParams<T> &P, cudaStream_t s) {
+  using Launch = cudaError_t (*)(const StageParams<T> &, cudaStream_t);
+  // index: upwind x 4 + les x 2 + thermal
+  static const Launch table[8] = {
+      launch_stage_cfg<T, false, false, false>, launch_stage_cfg<T, false, false, true>,
+      launch_stage_cfg<T, false, true, false>,  launch_stage_cfg<T, false, true, true>,
+      launch_stage_cfg<T, true, false, false>,  launch_stage_cfg<T, true, false, true>,
+      launch_stage_cfg<T, true, true, false>,   launch_stage_cfg<T, true, true, true>};
+  const int idx = (P.upwind ? 4 : 0) + (P.les != AERO_LES_NONE ? 2 : 0) + (P.thermal ? 1 : 0);
+  return table[idx](P, s);
 }
 
 template <typename T>
 cudaError_t launch_nu(const NuParams<T> &P, cudaStream_t s) {
   dim3 grid((P.nx + 2 + TX - 1) / TX, (P.ny + 2 + TY - 1) / TY, (P.nz + 2 + P.zc - 1) / P.zc);
-  nu_kernel<T><<<grid, dim3(TX, TY), 0, s>>>(P);
+  switch (P.les) {
+    case AERO_LES_SMAGORINSKY: nu_kernel<T, AERO_LES_SMAGORINSKY><<<grid, dim3(TX, TY), 0, s>>>(P); break;
+    case AERO_LES_WALE: nu_kernel<T, AERO_LES_WALE><<<grid, dim3(TX, TY), 0, s>>>(P); break;
+    case AERO_LES_VREMAN: nu_kernel<T, AERO_LES_VREMAN><<<grid, dim3(TX, TY), 0, s>>>(P); break;
+    default: return cudaErrorInvalidValue;
+  }
   return cudaGetLastError();
 }
 
