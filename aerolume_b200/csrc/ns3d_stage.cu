@@ -255,6 +255,15 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) stage_kernel(c
   const bool valid = (i < nx) && (j < ny);
   const int wk0 = P.win[0], wk1 = P.win[1], wj0 = P.win[2], wj1 = P.win[3], wi0 = P.win[4], wi1 = P.win[5];
   const int wzn = wk1 - wk0, wyn = wj1 - wj0, wxn = wi1 - wi0;
+  // which of the window's face / cell columns this thread's (j, i) lies in, evaluated once:
+  // bit 0 u faces (i), 1 v faces (j), 2 cells and w faces, 3 u face i + 1, 4 v face j + 1
+  int wcol = 0;
+  if (P.has_win && valid) {
+    const bool jc = j >= wj0 && j < wj1, ic = i >= wi0 && i < wi1;
+    wcol = ((jc && i >= wi0 && i <= wi1) ? 1 : 0) | ((ic && j >= wj0 && j <= wj1) ? 2 : 0) | ((jc && ic) ? 4 : 0) |
+           ((jc && i + 1 >= wi0 && i + 1 <= wi1) ? 8 : 0) | ((ic && j + 1 >= wj0 && j + 1 <= wj1) ? 16 : 0);
+  }
+  const bool warp_win = __any_sync(0xffffffffu, wcol != 0);  // warp-uniform
   const T two = T(2), qq = T(0.25);
   const T kh = P.kh;
   auto kface = [&](T n1, T n2, bool boundary) -> T {
@@ -285,7 +294,7 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) stage_kernel(c
       const T kz = kface(NU(0, ny2, nx2), NU(1, ny2, nx2), !P.pz && (kc + 1 == nz || kc + 1 == 0));
       const T cb = TH(0, y, x), cc = TH(1, y, x);
       T f = muscl_flux<T>(TH(-1, y, x), cb, cc, TH(2, y, x), VEL(2, 1, y, x)) - kz * (cc - cb);
-      if (P.has_adia && j >= wj0 && j < wj1 && i >= wi0 && i < wi1 && kc + 1 >= wk0 && kc + 1 <= wk1)
+      if ((wcol & 4) && P.has_adia && kc + 1 >= wk0 && kc + 1 <= wk1)
         f += kz * P.adia_w[((size_t)(kc + 1 - wk0) * wyn + (j - wj0)) * wxn + (i - wi0)] * (cc - cb);
       zth = f;
     }
@@ -441,22 +450,22 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) stage_kernel(c
       // ================= window penalisation (core.py:615-634) =========================
       const T kpen = bdt / P.eta;
       const T wg = P.wgt;
-      if (P.has_win) {
-        if (k >= wk0 && k < wk1 && j >= wj0 && j < wj1 && i >= wi0 && i <= wi1) {
+      if (wcol) {
+        if ((wcol & 1) && k >= wk0 && k < wk1) {
           wu = ((size_t)(k - wk0) * wyn + (j - wj0)) * (wxn + 1) + (i - wi0);
           const T un = (uh + kpen * P.a_u[wu]) / (T(1) + kpen * P.chi_u[wu]);
           cu = (double)((un - uh) * wg);
           uh = un;
           fu_in = 1;
         }
-        if (k >= wk0 && k < wk1 && j >= wj0 && j <= wj1 && i >= wi0 && i < wi1) {
+        if ((wcol & 2) && k >= wk0 && k < wk1) {
           wv = ((size_t)(k - wk0) * (wyn + 1) + (j - wj0)) * wxn + (i - wi0);
           const T vn = (vh + kpen * P.a_v[wv]) / (T(1) + kpen * P.chi_v[wv]);
           cv = (double)((vn - vh) * wg);
           vh = vn;
           fv_in = 1;
         }
-        if (k >= wk0 && k <= wk1 && j >= wj0 && j < wj1 && i >= wi0 && i < wi1) {
+        if ((wcol & 4) && k >= wk0 && k <= wk1) {
           ww = ((size_t)(k - wk0) * wyn + (j - wj0)) * wxn + (i - wi0);
           const T wn = (wh + kpen * P.a_w[ww]) / (T(1) + kpen * P.chi_w[ww]);
           cw = (double)((wn - wh) * wg);
@@ -519,18 +528,18 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) stage_kernel(c
                 kyl * (c - TH(0, y - 1, x));
         T fyr = muscl_flux<T>(TH(0, y - 1, x), c, TH(0, y + 1, x), TH(0, y + 2, x), VEL(1, 0, y + 1, x)) -
                 kyr * (TH(0, y + 1, x) - c);
-        if (P.has_adia && k >= wk0 && k < wk1) {  // adiabatic bodies block conduction (physics.py:666-675)
-          if (j >= wj0 && j < wj1) {
-            if (i >= wi0 && i <= wi1)
+        if ((wcol & 27) && P.has_adia && k >= wk0 && k < wk1) {  // adiabatic bodies block conduction (physics.py:666-675)
+          {
+            if (wcol & 1)
               fxl += kxl * P.adia_u[((size_t)(k - wk0) * wyn + (j - wj0)) * (wxn + 1) + (i - wi0)] * (c - TH(0, y, x - 1));
-            if (i + 1 >= wi0 && i + 1 <= wi1)
+            if (wcol & 8)
               fxr += kxr * P.adia_u[((size_t)(k - wk0) * wyn + (j - wj0)) * (wxn + 1) + (i + 1 - wi0)] *
                      (TH(0, y, x + 1) - c);
           }
-          if (i >= wi0 && i < wi1) {
-            if (j >= wj0 && j <= wj1)
+          {
+            if (wcol & 2)
               fyl += kyl * P.adia_v[((size_t)(k - wk0) * (wyn + 1) + (j - wj0)) * wxn + (i - wi0)] * (c - TH(0, y - 1, x));
-            if (j + 1 >= wj0 && j + 1 <= wj1)
+            if (wcol & 16)
               fyr += kyr * P.adia_v[((size_t)(k - wk0) * (wyn + 1) + (j + 1 - wj0)) * wxn + (i - wi0)] *
                      (TH(0, y + 1, x) - c);
           }
@@ -538,7 +547,7 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) stage_kernel(c
         const T D = ((fxr - fxl) + (fyr - fyl) + (zth - zth_l)) * inv;
         const size_t ic = ((size_t)k * ny + j) * nx + i;
         T ch = (a == T(0) ? c : lerp_t<T>(c, t0v, a)) - bdt * D;
-        if (P.has_win && k >= wk0 && k < wk1 && j >= wj0 && j < wj1 && i >= wi0 && i < wi1) {
+        if ((wcol & 4) && k >= wk0 && k < wk1) {
           wt = ((size_t)(k - wk0) * wyn + (j - wj0)) * wxn + (i - wi0);
           if (P.skin) ch = ch + (bdt * P.kappa) * P.skin[wt];
           if (P.chi_t) {
@@ -554,7 +563,7 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) stage_kernel(c
     }
 
     // ================= force / heat sums: per-warp, fixed order (deterministic) ===========
-    if (P.has_win) {
+    if (warp_win) {
       const unsigned any = __ballot_sync(0xffffffffu, fu_in | fv_in | fw_in | ft_in);
       if (any) {
         const size_t wsz_u = (size_t)wzn * wyn * (wxn + 1);
