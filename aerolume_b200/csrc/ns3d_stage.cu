@@ -448,9 +448,9 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) stage_kernel(c
       if (!P.pz && k == 0) wh = T(0);
 
       // ================= window penalisation (core.py:615-634) =========================
-      const T kpen = bdt / P.eta;
       const T wg = P.wgt;
       if (wcol) {
+        const T kpen = bdt / P.eta;
         if ((wcol & 1) && k >= wk0 && k < wk1) {
           wu = ((size_t)(k - wk0) * wyn + (j - wj0)) * (wxn + 1) + (i - wi0);
           const T un = (uh + kpen * P.a_u[wu]) / (T(1) + kpen * P.chi_u[wu]);
