@@ -1,4 +1,5 @@
-// The eddy-viscosity kernel and the SSP-RK3 stage kernel of the 3D step.
+// The eddy-viscosity kernel and the SSP-RK3 stage kernel of the 3D step (templates; each
+// precision is instantiated in its own translation unit, ns3d_stage_f32.cu / ns3d_stage_f64.cu).
 //
 // Arithmetic follows the reference's plain-torch step (Aerolume ns3d/core.py:765-883)
 // operation by operation, so float64 runs agree with it to round-off:
@@ -19,6 +20,8 @@
 // What the z direction needs on both sides of a plane -- the z fluxes of the momentum
 // components and of theta, the x-z / y-z shear stresses and tau_33 -- is evaluated once
 // per interface and carried to the next plane in registers.
+#pragma once
+
 #include "ns3d.cuh"
 #include "stencil.cuh"
 #include "tma.cuh"
@@ -666,11 +669,5 @@ cudaError_t launch_nu(const NuParams<T> &P, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-template size_t stage_smem_bytes<float>();
-template size_t stage_smem_bytes<double>();
-template cudaError_t launch_stage<float>(const StageParams<float> &, cudaStream_t);
-template cudaError_t launch_stage<double>(const StageParams<double> &, cudaStream_t);
-template cudaError_t launch_nu<float>(const NuParams<float> &, cudaStream_t);
-template cudaError_t launch_nu<double>(const NuParams<double> &, cudaStream_t);
 
 }  // namespace aero
