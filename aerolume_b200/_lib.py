@@ -14,7 +14,7 @@ import os
 
 LIB_PATH = Path(__file__).resolve().parent / (
     "libaero_b200_checked.so" if os.environ.get("AERO_B200_CHECKED") == "1" else "libaero_b200.so")
-ABI_VERSION = 1
+ABI_VERSION = 2
 MAX_BODIES = 8
 TRACE_EVENTS = 19
 # output fields of aero_ns3d_fields, in its order
@@ -59,19 +59,21 @@ class Ns3dConfig(C.Structure):
         ("flux_rate", C.c_double * MAX_BODIES),
         ("smoke", C.c_int32), ("dye_window", C.c_int32 * 6),
         ("pulse_on", C.c_double), ("pulse_period", C.c_double),
+        ("u_floor", C.c_double), ("pid", C.c_int32), ("pid_target", C.c_double), ("paint", C.c_int32),
     ]
 
 
 class Ns3dGeom(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in (
         "chi_u", "chi_v", "chi_w", "chi_c", "a_u", "a_v", "a_w", "k_u", "k_v", "k_w",
-        "chi_t", "a_t", "w_t", "adia_u", "adia_v", "adia_w", "vol_w", "skin", "dye_weight", "u_inlet")]
+        "chi_t", "a_t", "w_t", "adia_u", "adia_v", "adia_w", "vol_w", "skin", "dye_weight", "u_inlet",
+        "paint_u", "paint_v", "paint_w", "paint_c")]
 
 
 class Ns3dFields(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in (
         "u0", "v0", "w0", "theta0", "dye0", "t0",
-        "u", "v", "w", "p", "theta", "dye", "t", "dt", "coeffs", "heat_rate")]
+        "u", "v", "w", "p", "theta", "dye", "t", "dt", "coeffs", "heat_rate", "pid_dt_prev", "pid_e1", "pid_e2")]
 
 
 class Ns2dConfig(C.Structure):

@@ -217,6 +217,7 @@ int smoke_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeo
   M.weight = dye_src ? static_cast<const T *>(g->dye_weight) : nullptr;
   M.pulse_on = c.pulse_on;
   M.pulse_period = c.pulse_period;
+  M.paint_c = c.paint ? static_cast<const T *>(g->paint_c) : nullptr;
   CUDA_TRY(aero::launch_smoke<T>(M, s));
   return AERO_OK;
 }
@@ -344,6 +345,11 @@ int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom
   S.chi_v = static_cast<const T *>(g->chi_v);
   S.chi_w = static_cast<const T *>(g->chi_w);
   S.chi_c = static_cast<const T *>(g->chi_c);
+  if (c.paint) {
+    S.paint_u = static_cast<const T *>(g->paint_u);
+    S.paint_v = static_cast<const T *>(g->paint_v);
+    S.paint_w = static_cast<const T *>(g->paint_w);
+  }
   S.a_u = static_cast<const T *>(g->a_u);
   S.a_v = static_cast<const T *>(g->a_v);
   S.a_w = static_cast<const T *>(g->a_w);
@@ -406,6 +412,12 @@ int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom
   D.prt = c.prt;
   D.ri = c.ri;
   D.heat_max = c.heat_max;
+  D.u_floor = c.u_floor;
+  D.pid = c.pid;
+  D.pid_target = c.pid_target;
+  D.pid_dt_prev = f->pid_dt_prev;
+  D.pid_e1 = f->pid_e1;
+  D.pid_e2 = f->pid_e2;
   CUDA_TRY(aero::launch_dt<T>(D, s));
 
   const int rows = nz * ny;
@@ -722,6 +734,8 @@ int aero_ns3d_plan_create(const AeroNs3dConfig *cfg, AeroNs3dPlan **plan) {
       return fail(AERO_EINVAL, "smoke nozzle window outside the domain");
   }
   if (!(c.eta > 0)) return fail(AERO_EINVAL, "eta must be positive");
+  if (!(c.u_floor >= 0) || !std::isfinite(c.u_floor)) return fail(AERO_EINVAL, "u_floor must be >= 0");
+  if (c.pid && !(c.pid_target >= 0.1 && c.pid_target <= 1.0)) return fail(AERO_EINVAL, "pid_target must be in [0.1, 1]");
   AeroNs3dPlan *p = new AeroNs3dPlan();
   p->cfg = c;
   p->esz = c.dtype == AERO_F64 ? 8 : 4;
@@ -806,6 +820,9 @@ int aero_ns3d_step_traced(const AeroNs3dPlan *plan, const AeroNs3dFields *f, con
     if (c.thermal && c.has_skin && !g->skin) return fail(AERO_EINVAL, "missing heat-flux skin");
   }
   if (c.thermal && !f->heat_rate && c.nbody > 0) return fail(AERO_EINVAL, "missing heat-rate output");
+  if (c.paint && (!g->paint_u || !g->paint_v || !g->paint_w || (c.smoke && !g->paint_c)))
+    return fail(AERO_EINVAL, "missing paint masks");
+  if (c.pid && (!f->pid_dt_prev || !f->pid_e1 || !f->pid_e2)) return fail(AERO_EINVAL, "missing PID state");
   auto s = static_cast<cudaStream_t>(stream);
   auto ws = static_cast<unsigned char *>(workspace);
   return c.dtype == AERO_F64 ? step_impl<double>(plan, f, g, dt_in, ws, s, events, nevents)

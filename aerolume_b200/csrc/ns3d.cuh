@@ -74,6 +74,7 @@ struct StageParams {
   const T *thp, *th0;
   T *thh;
   const T *chi_t, *a_t, *w_t, *adia_u, *adia_v, *adia_w, *vol_w, *skin;
+  const T *paint_u, *paint_v, *paint_w;  // painted solid fractions (whole grid) or NULL
 };
 
 struct DtParams {
@@ -83,6 +84,10 @@ struct DtParams {
   int *status;
   int has_dt_fixed, les, thermal, has_heat_max;
   double dt_fixed, cfl, h, nu, viscous_dt, kappa, prt, ri, heat_max;
+  double u_floor;             // sources' speed scale (0: none)
+  int pid;                    // PID controller on the rule's dt
+  double pid_target;
+  void *pid_dt_prev, *pid_e1, *pid_e2;  // its state (plan dtype), updated in place
 };
 
 template <typename T>
@@ -105,6 +110,7 @@ struct SmokeParams {
   const T *weight;
   int dwin[6];
   double pulse_on, pulse_period;
+  const T *paint_c;           // painted solid fraction of the cells (whole grid) or NULL
 };
 
 template <typename T>

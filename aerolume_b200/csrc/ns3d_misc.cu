@@ -73,6 +73,11 @@ __global__ void dt_kernel(const DtParams P) {
     const T nu = les ? T(P.nu) + nut_max : T(P.nu);
     const T dv = T(P.viscous_dt * P.h * P.h) / nu;
     dt = dv < dt ? dv : dt;
+    if (P.u_floor > 0.0) {  // the sources' speed scale bounds dt from rest (physics.py:1239-1241)
+      const T cap = T(P.cfl * P.h / P.u_floor);
+      dt = dt > cap ? cap : dt;
+      umax = umax < T(P.u_floor) ? T(P.u_floor) : umax;
+    }
     if (P.thermal) {
       const T kap = les ? T(P.kappa) + nut_max / T(P.prt) : T(P.kappa);
       const T diff_rate = kap / T(P.viscous_dt * P.h * P.h);
@@ -94,6 +99,24 @@ __global__ void dt_kernel(const DtParams P) {
           dt = l2 < dt ? l2 : dt;
         }
       }
+    }
+    if (P.pid) {
+      // PID control towards pid_target x the limit on e = log(want / dt_prev)
+      // (physics.py:1161-1173): gains (kI, kP, kD) = (0.3, 0.4, 0.05), the growth factor
+      // within [0.5, 1.2], never above the limit; the first step takes the target itself
+      T *dprev = static_cast<T *>(P.pid_dt_prev), *e1p = static_cast<T *>(P.pid_e1), *e2p = static_cast<T *>(P.pid_e2);
+      const T want = dt * T(P.pid_target);
+      const bool first = *dprev <= T(0);
+      const T prev = first ? want : *dprev;
+      const T e = log(want / prev);
+      const T e1 = *e1p, e2 = *e2p;
+      T fac = exp((T(0.3) * e + T(0.4) * (e - e1)) + T(0.05) * ((e - T(2) * e1) + e2));
+      fac = fac < T(0.5) ? T(0.5) : (fac > T(1.2) ? T(1.2) : fac);
+      const T d = first ? want : prev * fac;
+      dt = (d < dt || d != d) ? d : dt;
+      *e2p = e1;
+      *e1p = first ? T(0) : e;
+      *dprev = dt;
     }
   }
   *reinterpret_cast<T *>(P.dt_out) = dt;
@@ -347,6 +370,8 @@ __global__ void __launch_bounds__(SMOKE_TX *SMOKE_TY, sizeof(T) == 4 ? 4 : 1) sm
                                (i - P.dwin[4])];
         v = v + wgt * on * (T(1) - v);
       }
+      // painted solids hold no smoke, after the sources (ns3d/solver.py:642-644)
+      if (P.paint_c && P.paint_c[((size_t)k * ny + j) * nx + i] > T(0.5)) v = T(0);
       P.c[((size_t)k * ny + j) * nx + i] = v;
     }
     // plane k + 3 goes into the slot of plane k - 3, which no thread reads from here on

@@ -477,6 +477,14 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) stage_kernel(c
         }
       }
 
+      // ================= painted solids, after the bodies (physics.py:1132-1137) =========
+      if (P.paint_u) {
+        const T kpen = bdt / P.eta;
+        uh = uh / (T(1) + kpen * P.paint_u[iu]);
+        vh = vh / (T(1) + kpen * P.paint_v[iv]);
+        wh = wh / (T(1) + kpen * P.paint_w[iw]);
+      }
+
       // ================= buoyancy after the penalisation (physics.py:744-790) =========
       if (thermal && P.ri != T(0)) {
         if (k > 0) {
@@ -509,6 +517,7 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) stage_kernel(c
           const T lo = (upi - upo) * inv;
           uo = (a == T(0) ? upo : lerp_t<T>(upo, __ldg(P.u0 + io), a)) + lo * bdt;
           uo = uo + *P.outlet_corr;
+          if (P.paint_u) uo = uo / (T(1) + (bdt / P.eta) * P.paint_u[io]);
         }
         P.uh[io] = uo;
       }

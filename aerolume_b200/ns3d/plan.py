@@ -39,10 +39,14 @@ class Ns3dPlan:
     """Plan + device tensors for one (ops, geom, thermal, smoke) configuration.
 
     ``thermal`` is a ``ThermalOps`` (or None); ``dye_src`` a ``DyeSources`` (or None);
-    ``smoke`` turns the smoke update on inside :meth:`step`.
+    ``smoke`` turns the smoke update on inside :meth:`step`.  ``paint`` (``chi_u / chi_v /
+    chi_w / chi_c`` tensors, a ``PaintLayer``), ``pid`` (``target`` and the ``dt_prev / e1 /
+    e2`` state tensors, a ``PidDt``) and ``u_floor`` (the sources' speed scale) are the step
+    controls of the placed physics (physics.py:1074-1262).
     """
 
-    def __init__(self, ops, geom, thermal=None, dye_src=None, *, smoke: bool = False, device=None):
+    def __init__(self, ops, geom, thermal=None, dye_src=None, *, smoke: bool = False, device=None, paint=None,
+                 pid=None, u_floor: float = 0.0):
         self.device = torch.device(device) if device is not None else torch.device("cuda")
         if self.device.type != "cuda":
             raise RuntimeError("the B200 step runs on a CUDA device only (no CPU fallback)")
@@ -131,6 +135,19 @@ class Ns3dPlan:
                 cfg.pulse_on, cfg.pulse_period = pulse[0], pulse[1]
             else:
                 cfg.pulse_on, cfg.pulse_period = 2.0, 1.0
+        self.paint, self.pid = paint, pid
+        cfg.u_floor = float(u_floor)
+        if pid is not None:
+            cfg.pid, cfg.pid_target = 1, float(pid.target)
+            for name in ("dt_prev", "e1", "e2"):
+                self._check("pid." + name, getattr(pid, name), ())
+        if paint is not None:
+            cfg.paint = 1
+            shapes = {"u": (nz, ny, nx + 1), "v": (nz, ny + 1, nx), "w": (nz + 1, ny, nx), "c": (nz, ny, nx)}
+            for gname, shape in shapes.items():
+                t = getattr(paint, "chi_" + gname)
+                self._check("paint.chi_" + gname, t, shape)
+                setattr(g, "paint_" + gname, t.data_ptr())
         self.cfg = cfg
         self.geom_c = g
         handle = C.c_void_p()
@@ -246,6 +263,8 @@ class Ns3dPlan:
                 raise RuntimeError("this plan has smoke: dye0 is required")
             self._check("dye0", dye0, (nz, ny, nx))
             f.dye0, f.dye = dye0.data_ptr(), out["dye"].data_ptr()
+        if self.pid is not None:
+            f.pid_dt_prev, f.pid_e1, f.pid_e2 = (getattr(self.pid, n).data_ptr() for n in ("dt_prev", "e1", "e2"))
         dtp = None
         if dt is not None:
             self._check("dt", dt, ())
@@ -277,6 +296,7 @@ class Ns3dPlan:
             g = _lib.Ns3dGeom.from_buffer_copy(self.geom_c)
             if not solids:
                 g.chi_c = None
+                g.paint_c = None
             if not sources:
                 g.dye_weight = None
         check(_lib.lib().aero_ns3d_smoke(self._handle, C.byref(f), C.byref(g), self._stream()), "aero_ns3d_smoke")

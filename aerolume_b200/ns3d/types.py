@@ -9,6 +9,9 @@ accepts either these containers or the reference's own objects:
   ``aerolume.solvers.ns3d.physics.ThermalOps`` / ``ThermalGeometry`` the step reads
   (physics.py:314-461, 494-560)
 * :class:`DyeSources` -- ``aerolume.solvers.ns3d.dye.DyeSources`` (dye.py:140-151)
+* :class:`PaintLayer3D` / :class:`PidState3D` -- the parts of
+  ``aerolume.solvers.ns3d.physics.PaintLayer`` / ``PidDt`` the step reads and updates
+  (physics.py:1074-1181)
 * :class:`State3D`, :class:`StepOut3D` -- core.py:111-119, 745-750
 
 Arrays may be numpy arrays or torch tensors; the step uploads what is not already on the
@@ -143,3 +146,25 @@ class DyeSources:
     def empty(self) -> bool:
         k0, k1, j0, j1, i0, i1 = self.window
         return k1 <= k0 or j1 <= j0 or i1 <= i0
+
+
+@dataclass
+class PaintLayer3D:
+    """Painted solid fractions on the whole grid (physics.py:1074-1141): chi_u (nz, ny, nx+1),
+    chi_v (nz, ny+1, nx), chi_w (nz+1, ny, nx), chi_c (nz, ny, nx), device tensors of the
+    plan's dtype.  The step reads them at every call, so edits in place take effect."""
+    chi_u: Any
+    chi_v: Any
+    chi_w: Any
+    chi_c: Any
+
+
+@dataclass
+class PidState3D:
+    """The PID step controller (physics.py:1144-1181): the target fraction of the stability
+    limit and its state, 0-d device tensors dt_prev (<= 0: no step yet), e1, e2 that the
+    step updates in place."""
+    target: float
+    dt_prev: Any
+    e1: Any
+    e2: Any

@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define AERO_ABI_VERSION 1
+#define AERO_ABI_VERSION 2
 
 #define AERO_OK 0
 #define AERO_EINVAL -1        /* invalid argument or inconsistent configuration     */
@@ -100,6 +100,11 @@ typedef struct AeroNs3dConfig {
   int32_t smoke;
   int32_t dye_window[6];        /* nozzle window (empty: no nozzles)                       */
   double pulse_on, pulse_period;
+  /* step controls of the placed physics (ns3d/physics.py:1144-1181, 1230-1262) */
+  double u_floor;               /* speed scale of the momentum sources (0: none)           */
+  int32_t pid;                  /* PID control of dt towards pid_target x the limit         */
+  double pid_target;
+  int32_t paint;                /* painted solids (geom paint_*; physics.py:1074-1141)      */
 } AeroNs3dConfig;
 
 /* Window masks and constant inputs (device pointers of the plan's dtype; NULL when absent).
@@ -113,6 +118,9 @@ typedef struct AeroNs3dGeom {
   const void *vol_w, *skin;
   const void *dye_weight;
   const void *u_inlet;          /* (nz, ny)                                                */
+  /* painted solid fractions on the whole grid (u, v, w faces and cells; read at every step,
+   * so strokes between steps take effect) */
+  const void *paint_u, *paint_v, *paint_w, *paint_c;
 } AeroNs3dGeom;
 
 /* State in and out (device pointers of the plan's dtype).  u may alias u0, v v0, w w0 and
@@ -123,6 +131,9 @@ typedef struct AeroNs3dFields {
   const void *u0, *v0, *w0, *theta0, *dye0, *t0;
   void *u, *v, *w, *p, *theta, *dye, *t, *dt;
   void *coeffs, *heat_rate;
+  /* PID controller state (0-d scalars of the plan's dtype, read and updated in place by a
+   * step whose dt comes from the rule; dt_prev <= 0 means "first step") */
+  void *pid_dt_prev, *pid_e1, *pid_e2;
 } AeroNs3dFields;
 
 typedef struct AeroNs3dPlan AeroNs3dPlan;

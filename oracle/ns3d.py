@@ -15,7 +15,9 @@ the sm_100a kernels implement (Aerolume ``src/aerolume/solvers/ns3d``):
 * ``force_coefficients`` core.py:653-678
 * ``PoissonSolver3D``    poisson.py:74-157 exact solve in the per-axis eigenbases
 * ``ThermalOps``         physics.py:494-790 heat equation, buoyancy, heat rates
-* ``Physics3D.dt_rule``  physics.py:1230-1262
+* ``Physics3D.dt_rule``  physics.py:1230-1262 (with the sources' speed floor and ``PidDt``,
+                         physics.py:1144-1181)
+* ``PaintLayer``         physics.py:1074-1141 painted solids, penalised after the bodies
 * smoke                  dye.py:232-312    MUSCL / van Leer advection, solids, nozzles
 
 Parity is pinned: ``tests/test_oracle_golden.py`` checks this module against golden
@@ -693,10 +695,45 @@ def thermal_dt_limit(th, nut_max, ops, umax):
     return T(1.0) / (umax * T(1.0 / (THETA_COURANT_MAX * ops.h)) + diff_rate)
 
 
-def dt_rule(u0, v0, w0, ops, nut_max, th, theta):
-    """Physics3D.dt_rule without fans, ports or PID (physics.py:1230-1262)."""
+PID_GAINS = (0.3, 0.4, 0.05)                                      # ns3d/physics.py:79 (kI, kP, kD)
+PID_LIMITS = (0.5, 1.2)                                           # ns3d/physics.py:81
+
+
+class PidState:
+    """The PID controller's state (physics.py:1144-1181): 0-d arrays dt_prev, e1, e2
+    (dt_prev <= 0: no step yet) and the target fraction of the limit."""
+
+    def __init__(self, target, dtype):
+        self.target = float(target)
+        self.dt_prev, self.e1, self.e2 = (np.zeros((), dtype) for _ in range(3))
+
+
+def pid_dt(pid, dt_cap):
+    """PidDt.__call__ (physics.py:1161-1173): updates the state, returns dt."""
+    T = np.asarray(dt_cap).dtype.type
+    ki, kp, kd = PID_GAINS
+    want = T(dt_cap * T(pid.target))
+    first = pid.dt_prev <= 0
+    prev = want if first else T(pid.dt_prev)
+    with np.errstate(all="ignore"):
+        e = T(np.log(T(want / prev)))
+        fac = T(np.exp(T(T(T(T(ki) * e) + T(T(kp) * T(e - pid.e1))) + T(T(kd) * T(T(e - T(2.0) * pid.e1) + pid.e2)))))
+    fac = T(min(max(fac, T(PID_LIMITS[0])), T(PID_LIMITS[1])))
+    dt = T(np.minimum(want if first else T(prev * fac), dt_cap))
+    pid.e2 = np.asarray(pid.e1).copy()
+    pid.e1 = np.asarray(T(0.0) if first else e)
+    pid.dt_prev = np.asarray(dt)
+    return dt
+
+
+def dt_rule(u0, v0, w0, ops, nut_max, th, theta, u_floor=0.0, pid=None):
+    """Physics3D.dt_rule without fans and ports (physics.py:1230-1262); ``u_floor`` is the
+    sources' speed scale, ``pid`` a :class:`PidState` (or None)."""
     T = u0.dtype.type
     dt, umax = cfl_dt3d(u0, v0, w0, ops, nut_max)
+    if u_floor > 0.0:
+        dt = np.minimum(dt, T(ops.cfl * ops.h / u_floor))
+        umax = np.maximum(umax, T(u_floor))
     if th is not None:
         dt = np.minimum(dt, thermal_dt_limit(th, nut_max, ops, umax))
         if th.ri != 0.0 and theta is not None:
@@ -707,6 +744,8 @@ def dt_rule(u0, v0, w0, ops, nut_max, th, theta):
             dt = np.minimum(dt, T(1.0) / s_max)
             if th.ri != 0.0:
                 dt = np.minimum(dt, (T(6.0 * ops.cfl * ops.h) / (T(abs(th.ri)) * s_max)) ** T(1.0 / 3.0))
+    if pid is not None:
+        dt = pid_dt(pid, T(dt))
     return T(dt)
 
 
@@ -722,8 +761,11 @@ class StepResult:
         self.__dict__.update(kw)
 
 
-def step3d_phys(u0, v0, w0, t, geom, ops, poisson, *, th=None, theta=None, dt=None, trace=False):
-    """One SSP-RK3 step (core.py:765-883, fixed physics: thermal, buoyancy; no fans/ports/paint)."""
+def step3d_phys(u0, v0, w0, t, geom, ops, poisson, *, th=None, theta=None, dt=None, trace=False, paint=None,
+                pid=None, u_floor=0.0):
+    """One SSP-RK3 step (core.py:765-883) with heat transfer, buoyancy, painted solids
+    (``paint``: (chi_u, chi_v, chi_w) on the whole grid) and the PID / speed-floor dt rule;
+    no fans or ports."""
     T = u0.dtype.type
     up, vp, wp = u0, v0, w0
     acc = None
@@ -740,8 +782,8 @@ def step3d_phys(u0, v0, w0, t, geom, ops, poisson, *, th=None, theta=None, dt=No
             if dt is None:
                 if ops.dt_fixed is not None:
                     dt = T(ops.dt_fixed)
-                elif thermal or th is not None:
-                    dt = dt_rule(u0, v0, w0, ops, nut_max, th, t0)
+                elif thermal or th is not None or pid is not None or u_floor > 0.0:
+                    dt = dt_rule(u0, v0, w0, ops, nut_max, th, t0, u_floor, pid)
                 else:
                     dt = cfl_dt3d(u0, v0, w0, ops, nut_max)[0]
             dt = T(dt)
@@ -759,6 +801,11 @@ def step3d_phys(u0, v0, w0, t, geom, ops, poisson, *, th=None, theta=None, dt=No
             wg = T(wgt)
             acc = [du * wg, dv * wg, dw * wg] if acc is None else [acc[0] + du * wg, acc[1] + dv * wg,
                                                                     acc[2] + dw * wg]
+            if any(ops.periodic_axes):
+                uh, vh, wh = sync_periodic(uh, vh, wh, ops)
+        if paint is not None:  # PaintLayer.penalise (physics.py:1132-1137), after the bodies
+            k = T(bdt / T(ops.eta))
+            uh, vh, wh = (x / (T(1.0) + k * chi) for x, chi in zip((uh, vh, wh), paint))
             if any(ops.periodic_axes):
                 uh, vh, wh = sync_periodic(uh, vh, wh, ops)
         if thermal and th.ri != 0.0:

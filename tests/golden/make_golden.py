@@ -2,7 +2,9 @@
 
 Usage (the reference must be importable; it is read, never modified)::
 
-    PYTHONPATH=/root/reference/src PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden.py
+    PYTHONPATH=/root/reference/src PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden.py [case ...]
+
+(no case names: every case and the Poisson fixtures).
 
 Each case builds a configuration with the reference's own API (``SolverConfig3D``,
 ``make_operators3d``, ``build_geometry3d``, ``Physics3D``, ``build_dye_sources``), starts
@@ -32,7 +34,7 @@ from aerolume.solvers.ns3d import core  # noqa: E402
 from aerolume.solvers.ns3d.config import DyeRake, ImmersedMesh, SolverConfig3D, ThermalConfig3D  # noqa: E402
 from aerolume.solvers.ns3d.dye import advect_dye3d, apply_solids_and_sources, build_dye_sources  # noqa: E402
 from aerolume.solvers.ns3d.geometry import body_window3d, build_geometry3d  # noqa: E402
-from aerolume.solvers.ns3d.physics import Physics3D  # noqa: E402
+from aerolume.solvers.ns3d.physics import PaintLayer, Physics3D  # noqa: E402
 from aerolume.solvers.ns3d.poisson import PoissonSolver3D  # noqa: E402
 
 
@@ -107,10 +109,18 @@ def extract(ops, geom, phys, src):
     if src is not None and not src.empty:
         meta["dye"] = {"window": list(src.window), "pulse": [float(x) for x in src.pulse]}
         arrays["dye_weight"] = _np(src.weight)
+    if phys is not None and phys.pid is not None:
+        meta["pid"] = {"target": phys.pid.target}
+    if phys is not None:
+        meta["u_floor"] = float(phys.u_floor)
+    if phys is not None and phys.paint is not None:
+        for g in "uvwc":
+            arrays["paint_" + g] = _np(getattr(phys.paint, "chi_" + g))
     return meta, arrays
 
 
-def run_case(name, cfg_kw, *, dtype="float64", amp=0.1, seed=1, rake=None, steps=1):
+def _run_case(name, cfg_kw, *, dtype="float64", amp=0.1, seed=1, rake=None, steps=1, strokes=()):
+    """One fixture; ``strokes`` are PaintLayer.stroke keyword sets (painted solids)."""
     base = dict(cfg_kw)
     cfg64 = SolverConfig3D(**{**base, "dtype": "float64", "device": "cpu", "perturb": False})
     cfg = SolverConfig3D(**{**base, "dtype": dtype, "device": "cpu", "perturb": False})
@@ -118,6 +128,10 @@ def run_case(name, cfg_kw, *, dtype="float64", amp=0.1, seed=1, rake=None, steps
     window = body_window3d([b.vertices_numpy() for b in cfg.bodies], ops) if cfg.bodies else (0, 0, 0, 0, 0, 0)
     geom = build_geometry3d(cfg.bodies, ops, window=window)
     phys = Physics3D(cfg, ops, geom, cfg.bodies) if cfg.has_placed_physics else None
+    if strokes:
+        phys.paint = PaintLayer(ops)
+        for kw in strokes:
+            assert phys.paint.stroke(ops, **kw)
     src = build_dye_sources(rake, ops) if rake is not None else None
     u, v, w, theta, dye = _random_state(cfg64, amp, seed)
     tdt = ops.dtype
@@ -137,7 +151,11 @@ def run_case(name, cfg_kw, *, dtype="float64", amp=0.1, seed=1, rake=None, steps
             new = out.state
             c = advect_dye3d(c, new.u, new.v, new.w, new.dt, ops)
             apply_solids_and_sources(c, new.t, geom, src)
+            if phys is not None and phys.paint is not None:   # FlowSolver3D._solid_cleanup
+                c.masked_fill_(phys.paint.chi_c > 0.5, 0.0)
             st, th = new, out.theta
+            if phys is not None and phys.pid is not None:
+                arrays[f"pid{k + 1}"] = np.array([float(phys.pid.dt_prev), float(phys.pid.e1), float(phys.pid.e2)])
             if k == 0:
                 arrays.update({"out1_u": _np(new.u), "out1_v": _np(new.v), "out1_w": _np(new.w),
                                "out1_p": _np(new.p), "out1_t": _np(new.t), "out1_dt": _np(new.dt),
@@ -176,6 +194,11 @@ def poisson_cases():
 
 def main():
     torch.set_num_threads(4)
+    names = sys.argv[1:]
+
+    def run_case(name, *a, **kw):
+        if not names or name in names:
+            _run_case(name, *a, **kw)
     h = 1.0 / 6.0
     box = ImmersedMesh(*box_mesh(0.5, 0.5, 0.25, (1.25, 1.0, 0.125)), name="box", thermal="temperature",
                        thermal_value=1.0)
@@ -214,7 +237,18 @@ def main():
     run_case("yperiodic_two_bodies_heatflux_f64", yper, dtype="float64", seed=6, amp=0.1)
     run_case("plain_upwind_f64", dict(grid, re=200.0, bodies=[ImmersedMesh(*box_mesh(0.5, 0.5, 0.5, (1.2, 1.0, 0.8)))],
                                       ref_area=0.25), dtype="float64", seed=7, amp=0.1)
-    poisson_cases()
+    # painted solids (a ball and a box, one of them across the body window) and the PID step
+    # controller, over three steps so that the controller runs past its first step
+    strokes = (dict(center=(2.6, 1.0, 0.6), radius=0.35), dict(center=(1.6, 1.3, 0.4), radius=0.2, shape="box",
+                                                               size=(0.3, 0.4, 0.5)))
+    paint_pid = dict(tunnel, adaptive_dt="pid", pid_target=0.7)
+    run_case("tunnel_paint_pid_f64", paint_pid, dtype="float64", rake=rake, steps=3, strokes=strokes, seed=8)
+    run_case("tunnel_paint_pid_f32", paint_pid, dtype="float32", rake=rake, steps=3, strokes=strokes, seed=8)
+    plain_pid = dict(grid, re=500.0, adaptive_dt="pid", pid_target=0.9)
+    run_case("plain_pid_paint_f64", plain_pid, dtype="float64", steps=3, seed=9, amp=0.3,
+             strokes=(dict(center=(2.0, 1.0, 0.8), radius=0.4),))
+    if not names or "poisson" in names:
+        poisson_cases()
     for p in sorted(HERE.glob("*.npz")):
         print(f"{p.name}: {p.stat().st_size / 1024:.0f} KiB")
 

@@ -28,14 +28,23 @@ def _dev(x, dt):
 
 def _plan_and_inputs(name):
     from aerolume_b200.ns3d.plan import Ns3dPlan
+    from aerolume_b200.ns3d.types import PaintLayer3D, PidState3D
     meta, ops, geom, th, src, arr = load_case(name)
     dt = torch.float64 if meta["dtype"] == "float64" else torch.float32
-    plan = Ns3dPlan(ops, geom, th, src, smoke=True)
+    paint = PaintLayer3D(*(_dev(arr["paint_" + g], dt) for g in "uvwc")) if "paint_u" in arr else None
+    pid = None
+    if "pid" in meta:
+        pid = PidState3D(meta["pid"]["target"], *(torch.zeros((), device="cuda", dtype=dt) for _ in range(3)))
+    plan = Ns3dPlan(ops, geom, th, src, smoke=True, paint=paint, pid=pid, u_floor=meta.get("u_floor", 0.0))
     ins = {"u0": _dev(arr["in_u"], dt), "v0": _dev(arr["in_v"], dt), "w0": _dev(arr["in_w"], dt),
            "t0": _dev(arr["in_t"], dt), "dye0": _dev(arr["in_dye"], dt)}
     if th is not None:
         ins["theta0"] = _dev(arr["in_theta"], dt)
     return meta, plan, ins, arr
+
+
+def _pid_state(plan):
+    return np.array([float(getattr(plan.pid, n)) for n in ("dt_prev", "e1", "e2")])
 
 
 @pytest.mark.parametrize("name", CASES_3D)
@@ -58,16 +67,20 @@ def test_one_step_matches_reference(name):
             hr = arr["out1_heat_rate"]
             err = np.abs(out["heat_rate"].double().cpu().numpy() - hr).max() / max(1.0, np.abs(hr).max())
             assert err < (1e-9 if meta["dtype"] == "float64" else 2e-4), err
+    if "pid" in meta:
+        ref = arr["pid1"]
+        assert np.abs(_pid_state(plan) - ref).max() <= TOL[meta["dtype"]] * max(1.0, np.abs(ref).max())
     assert plan.status() == 0
 
 
-@pytest.mark.parametrize("name", [n for n in CASES_3D if "tunnel" in n])
+@pytest.mark.parametrize("name", [n for n in CASES_3D if "tunnel" in n or "pid" in n])
 def test_three_steps_in_place_match_reference(name):
     """Three steps updating the state in place (u, v, w, theta outputs alias the inputs)."""
     meta, plan, ins, arr = _plan_and_inputs(name)
     u, v, w, t = ins["u0"], ins["v0"], ins["w0"], ins["t0"]
     theta, dye = ins.get("theta0"), ins["dye0"]
     out = plan.empty_fields()
+    pids = []
     for _ in range(3):
         out["u"], out["v"], out["w"] = u, v, w
         if theta is not None:
@@ -75,10 +88,16 @@ def test_three_steps_in_place_match_reference(name):
         plan.step(u, v, w, t, theta0=theta, dye0=dye, out=out)
         t = out["t"].clone()
         dye = out["dye"].clone()
+        if "pid" in meta:
+            pids.append(_pid_state(plan))
     torch.cuda.synchronize()
     tol = 10 * TOL[meta["dtype"]]
     for f, x in (("u", u), ("v", v), ("w", w), ("p", out["p"]), ("theta", theta), ("dye", dye)):
-        assert _rel(x, arr["outN_" + f]) < tol, (f, _rel(x, arr["outN_" + f]))
+        if "outN_" + f in arr:
+            assert _rel(x, arr["outN_" + f]) < tol, (f, _rel(x, arr["outN_" + f]))
+    for k, got in enumerate(pids):  # the PID state after every step
+        ref = arr[f"pid{k + 1}"]
+        assert np.abs(got - ref).max() <= tol * max(1.0, np.abs(ref).max()), k
 
 
 def _poisson_ops(nx, ny, nz, h, per, dtype):

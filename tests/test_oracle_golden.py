@@ -15,13 +15,19 @@ def _run(name, steps=1):
     u, v, w, t = arr["in_u"], arr["in_v"], arr["in_w"], dt(arr["in_t"])
     theta = arr.get("in_theta")
     c = arr["in_dye"]
+    paint = tuple(arr["paint_" + g] for g in "uvw") if "paint_u" in arr else None
+    pid = O.PidState(meta["pid"]["target"], dt) if "pid" in meta else None
     outs = []
     for _ in range(steps):
-        r = O.step3d_phys(u, v, w, t, geom, ops, ps, th=th, theta=theta)
+        r = O.step3d_phys(u, v, w, t, geom, ops, ps, th=th, theta=theta, paint=paint, pid=pid,
+                          u_floor=meta.get("u_floor", 0.0))
         c = O.advect_dye3d(c, r.u, r.v, r.w, r.dt, ops)
         c = O.apply_solids_and_sources(c, r.t, geom, src)
+        if "paint_c" in arr:                         # painted cells hold no smoke
+            c = np.where(arr["paint_c"] > 0.5, c.dtype.type(0.0), c)
         u, v, w, t, theta = r.u, r.v, r.w, r.t, r.theta
         r.dye = c
+        r.pid = None if pid is None else np.array([float(pid.dt_prev), float(pid.e1), float(pid.e2)])
         outs.append(r)
     return meta, arr, outs
 
@@ -49,14 +55,19 @@ def test_oracle_matches_reference_one_step(name):
     assert _rel(r.dye, arr["out1_dye"]) < tol
 
 
-@pytest.mark.parametrize("name", [n for n in CASES_3D if "tunnel" in n])
+@pytest.mark.parametrize("name", [n for n in CASES_3D if "tunnel" in n or "pid" in n])
 def test_oracle_matches_reference_three_steps(name):
     meta, arr, outs = _run(name, steps=3)
     r = outs[-1]
     tol = 1e-11 if meta["dtype"] == "float64" else 1e-4
     for f in ("u", "v", "w", "p", "theta"):
-        assert _rel(getattr(r, f), arr["outN_" + f]) < tol, f
+        if "outN_" + f in arr:
+            assert _rel(getattr(r, f), arr["outN_" + f]) < tol, f
     assert _rel(r.dye, arr["outN_dye"]) < tol
+    if "pid" in meta:  # the controller's state after every step: dt_prev, e1, e2
+        for k, rk in enumerate(outs):
+            ref = arr[f"pid{k + 1}"]
+            assert np.abs(rk.pid - ref).max() <= (1e-12 if meta["dtype"] == "float64" else 1e-5) * max(1.0, np.abs(ref).max()), k
 
 
 def test_oracle_poisson_matches_reference():
@@ -70,3 +81,17 @@ def test_oracle_poisson_matches_reference():
         # and the solve is exact: L psi = f (the reference's tests/test_ns3d_core.py:79-91)
         lap = ps.laplacian(psi, h, (bool(px), bool(py), bool(pz)))
         assert np.abs(lap - z[f"f{n}"]).max() < 1e-10 * np.abs(z[f"f{n}"]).max()
+
+
+def test_paint_and_pid_fixtures_exercise_both():
+    """Leaving out the painted solids, or the controller, moves the step far outside the
+    tolerances above: the fixtures pin both features, not a step they do not touch."""
+    meta, ops, geom, th, src, arr = load_case("tunnel_paint_pid_f64")
+    ps = O.PoissonSolver3D(ops.nx, ops.ny, ops.nz, ops.h, ops.periodic_axes, np.float64)
+    paint = tuple(arr["paint_" + g] for g in "uvw")
+    args = (arr["in_u"], arr["in_v"], arr["in_w"], np.float64(arr["in_t"]), geom, ops, ps)
+    kw = dict(th=th, theta=arr["in_theta"])
+    no_paint = O.step3d_phys(*args, **kw, pid=O.PidState(meta["pid"]["target"], np.float64))
+    assert _rel(no_paint.u, arr["out1_u"]) > 1e-4
+    no_pid = O.step3d_phys(*args, **kw, paint=paint)
+    assert abs(float(no_pid.dt) - float(arr["out1_dt"])) > 1e-3 * float(arr["out1_dt"])
