@@ -350,6 +350,21 @@ int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom
     S.paint_v = static_cast<const T *>(g->paint_v);
     S.paint_w = static_cast<const T *>(g->paint_w);
   }
+  S.nfan = c.nfan;
+  S.fan_swirl = c.fan_swirl;
+  for (int q = 0; q < c.nfan; ++q) {
+    const AeroNs3dFan &F = g->fans[q];
+    auto &d = S.fan[q];
+    for (int e = 0; e < 6; ++e) d.win[e] = F.window[e];
+    d.f[0] = static_cast<const T *>(F.f_u);
+    d.f[1] = static_cast<const T *>(F.f_v);
+    d.f[2] = static_cast<const T *>(F.f_w);
+    d.s[0] = static_cast<const T *>(F.s_u);
+    d.s[1] = static_cast<const T *>(F.s_v);
+    d.s[2] = static_cast<const T *>(F.s_w);
+    d.thrust = static_cast<const T *>(F.thrust);
+    d.swirl_amp = static_cast<const T *>(F.swirl_amp);
+  }
   S.a_u = static_cast<const T *>(g->a_u);
   S.a_v = static_cast<const T *>(g->a_v);
   S.a_w = static_cast<const T *>(g->a_w);
@@ -419,6 +434,39 @@ int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom
   D.pid_e1 = f->pid_e1;
   D.pid_e2 = f->pid_e2;
   CUDA_TRY(aero::launch_dt<T>(D, s));
+
+  // fans: disc velocities of the step-start state and the PI thrust, before any stage
+  if (c.nfan > 0) {
+    aero::FanBeginParams<T> FB{};
+    FB.nfan = c.nfan;
+    FB.any_swirl = c.fan_swirl;
+    FB.nx = nx;
+    FB.ny = ny;
+    FB.nz = nz;
+    FB.u0 = u0;
+    FB.v0 = v0;
+    FB.w0 = w0;
+    FB.dt = small;
+    for (int q = 0; q < c.nfan; ++q) {
+      const AeroNs3dFan &F = g->fans[q];
+      auto &d = FB.fan[q];
+      for (int e = 0; e < 6; ++e) d.win[e] = F.window[e];
+      d.velocity_mode = F.velocity_mode;
+      d.target = F.target;
+      d.kp = F.kp;
+      d.ki = F.ki;
+      d.tmax = F.tmax;
+      d.swirl = F.swirl;
+      d.m[0] = static_cast<const T *>(F.m_u);
+      d.m[1] = static_cast<const T *>(F.m_v);
+      d.m[2] = static_cast<const T *>(F.m_w);
+      d.thrust = static_cast<T *>(F.thrust);
+      d.ud = static_cast<T *>(F.ud);
+      d.e_prev = static_cast<T *>(F.e_prev);
+      d.swirl_amp = static_cast<T *>(F.swirl_amp);
+    }
+    CUDA_TRY(aero::launch_fan_begin<T>(FB, s));
+  }
 
   const int rows = nz * ny;
   double *psum = reinterpret_cast<double *>(ws + p->off_psum);  // [u0 outlet | inlet | 3 stages x 2] x parts
@@ -736,6 +784,8 @@ int aero_ns3d_plan_create(const AeroNs3dConfig *cfg, AeroNs3dPlan **plan) {
   if (!(c.eta > 0)) return fail(AERO_EINVAL, "eta must be positive");
   if (!(c.u_floor >= 0) || !std::isfinite(c.u_floor)) return fail(AERO_EINVAL, "u_floor must be >= 0");
   if (c.pid && !(c.pid_target >= 0.1 && c.pid_target <= 1.0)) return fail(AERO_EINVAL, "pid_target must be in [0.1, 1]");
+  if (c.nfan < 0 || c.nfan > AERO_MAX_FANS)
+    return fail(AERO_EUNSUPPORTED, "at most " + std::to_string(AERO_MAX_FANS) + " fans");
   AeroNs3dPlan *p = new AeroNs3dPlan();
   p->cfg = c;
   p->esz = c.dtype == AERO_F64 ? 8 : 4;
@@ -823,6 +873,18 @@ int aero_ns3d_step_traced(const AeroNs3dPlan *plan, const AeroNs3dFields *f, con
   if (c.paint && (!g->paint_u || !g->paint_v || !g->paint_w || (c.smoke && !g->paint_c)))
     return fail(AERO_EINVAL, "missing paint masks");
   if (c.pid && (!f->pid_dt_prev || !f->pid_e1 || !f->pid_e2)) return fail(AERO_EINVAL, "missing PID state");
+  if (c.nfan > 0) {
+    if (!g->fans) return fail(AERO_EINVAL, "missing fan descriptors");
+    for (int q = 0; q < c.nfan; ++q) {
+      const AeroNs3dFan &F = g->fans[q];
+      if (window_empty(F.window) || F.window[0] < 0 || F.window[1] > c.nz || F.window[2] < 0 || F.window[3] > c.ny ||
+          F.window[4] < 0 || F.window[5] > c.nx)
+        return fail(AERO_EINVAL, "fan window empty or outside the domain");
+      if (!F.f_u || !F.f_v || !F.f_w || !F.m_u || !F.m_v || !F.m_w || !F.thrust || !F.ud || !F.e_prev ||
+          !F.swirl_amp || (c.fan_swirl && (!F.s_u || !F.s_v || !F.s_w)))
+        return fail(AERO_EINVAL, "missing fan weights or state");
+    }
+  }
   auto s = static_cast<cudaStream_t>(stream);
   auto ws = static_cast<unsigned char *>(workspace);
   return c.dtype == AERO_F64 ? step_impl<double>(plan, f, g, dt_in, ws, s, events, nevents)

@@ -1,8 +1,8 @@
 // Output fields of a 3D state (Aerolume ns3d/fields.py:24-102, ns3d/solver.py:1374-1416):
 // cell-centred velocity and speed, vorticity magnitude, Q-criterion and eddy viscosity from the
 // velocity-gradient tensor, and trilinear sampling of any (staggered) field at points.  These
-// are outputs (per frame, not per step): one thread per cell, the 3 x 3 x 3 neighbourhood read
-// through L1 / L2, interior cells with plain loads and boundary cells through the ghost rules.
+// are outputs (per frame, not per step): one thread per cell, the 3 x 3 x 3 neighbourhood
+// staged per block in shared memory with the ghost rules applied while staging.
 #include "ns3d.cuh"
 #include "stencil.cuh"
 
@@ -85,38 +85,46 @@ __device__ __forceinline__ void write_fields(const FieldsParams<T> &P, const T g
   }
 }
 
+// One block per 32 x 8 cells of a z-plane.  The block first stages the three face arrays on
+// the tile's neighbourhood -- entries (k-1..k+1, j0-1..j0+8, i0-1..i0+32) of each -- in shared
+// memory, reading in-range entries directly and applying the ghost rules only to the entries
+// outside an array, so no thread diverges into the rules while the fields are computed.
+constexpr int FTX = 32, FTY = 8, FSX = FTX + 2, FSY = FTY + 2;
+
 template <typename T>
-__global__ void __launch_bounds__(256) fields_kernel(const __grid_constant__ FieldsParams<T> P) {
+__global__ void __launch_bounds__(FTX *FTY) fields_kernel(const __grid_constant__ FieldsParams<T> P) {
+  __shared__ T sm[3][3][FSY][FSX];  // [component][dz + 1][y][x]
   const int nx = P.nx, ny = P.ny, nz = P.nz;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y, k = blockIdx.z;
+  const int i0 = blockIdx.x * FTX, j0 = blockIdx.y * FTY, k = blockIdx.z;
+  const int tid = threadIdx.y * FTX + threadIdx.x;
+  for (int e = tid; e < 3 * 3 * FSY * FSX; e += FTX * FTY) {
+    const int x = e % FSX, y = (e / FSX) % FSY, z = (e / (FSX * FSY)) % 3, comp = e / (FSX * FSY * 3);
+    const int gi = i0 - 1 + x, gj = j0 - 1 + y, gk = k - 1 + z;
+    T val;
+    if (comp == 0) {
+      val = (gi >= 0 && gi <= nx && gj >= 0 && gj < ny && gk >= 0 && gk < nz)
+                ? __ldg(P.u + ((size_t)gk * ny + gj) * (nx + 1) + gi)
+                : padded<T>(P.u, P.ru, gk, gj, gi);
+    } else if (comp == 1) {
+      val = (gi >= 0 && gi < nx && gj >= 0 && gj <= ny && gk >= 0 && gk < nz)
+                ? __ldg(P.v + ((size_t)gk * (ny + 1) + gj) * nx + gi)
+                : padded<T>(P.v, P.rv, gk, gj, gi);
+    } else {
+      val = (gi >= 0 && gi < nx && gj >= 0 && gj < ny && gk >= 0 && gk <= nz)
+                ? __ldg(P.w + ((size_t)gk * ny + gj) * nx + gi)
+                : padded<T>(P.w, P.rw, gk, gj, gi);
+    }
+    sm[comp][z][y][x] = val;
+  }
+  __syncthreads();
+  const int tx = threadIdx.x, ty = threadIdx.y, i = i0 + tx, j = j0 + ty;
   if (i >= nx || j >= ny) return;
-  const size_t su = (size_t)ny * (nx + 1), sv = (size_t)(ny + 1) * nx, sw = (size_t)ny * nx;
-  const T *bu = P.u + (size_t)k * su + (size_t)j * (nx + 1) + i;
-  const T *bv = P.v + (size_t)k * sv + (size_t)j * nx + i;
-  const T *bw = P.w + (size_t)k * sw + (size_t)j * nx + i;
-  const T uc = T(0.5) * (bu[1] + bu[0]), vc = T(0.5) * (bv[nx] + bv[0]), wc = T(0.5) * (bw[sw] + bw[0]);
+  auto L = [&](int comp, int dz, int dy, int dx) -> T { return sm[comp][1 + dz][1 + ty + dy][1 + tx + dx]; };
+  const T uc = T(0.5) * (L(0, 0, 0, 1) + L(0, 0, 0, 0)), vc = T(0.5) * (L(1, 0, 1, 0) + L(1, 0, 0, 0)),
+          wc = T(0.5) * (L(2, 1, 0, 0) + L(2, 0, 0, 0));
   const size_t c = ((size_t)k * ny + j) * nx + i;
-  if (!P.gradient) {
-    const T g[3][3] = {{T(0), T(0), T(0)}, {T(0), T(0), T(0)}, {T(0), T(0), T(0)}};
-    write_fields<T>(P, g, c, k, j, i, uc, vc, wc);
-    return;
-  }
-  T g[3][3];
-  if (k >= 1 && k <= nz - 2 && j >= 1 && j <= ny - 2 && i >= 1 && i <= nx - 2) {
-    auto L = [&](int comp, int dz, int dy, int dx) -> T {
-      if (comp == 0) return __ldg(bu + dz * (ptrdiff_t)su + dy * (ptrdiff_t)(nx + 1) + dx);
-      if (comp == 1) return __ldg(bv + dz * (ptrdiff_t)sv + dy * (ptrdiff_t)nx + dx);
-      return __ldg(bw + dz * (ptrdiff_t)sw + dy * (ptrdiff_t)nx + dx);
-    };
-    cell_gradient<T>(L, P.inv_h, g);
-  } else {
-    auto L = [&](int comp, int dz, int dy, int dx) -> T {
-      if (comp == 0) return padded<T>(P.u, P.ru, k + dz, j + dy, i + dx);
-      if (comp == 1) return padded<T>(P.v, P.rv, k + dz, j + dy, i + dx);
-      return padded<T>(P.w, P.rw, k + dz, j + dy, i + dx);
-    };
-    cell_gradient<T>(L, P.inv_h, g);
-  }
+  T g[3][3] = {{T(0), T(0), T(0)}, {T(0), T(0), T(0)}, {T(0), T(0), T(0)}};
+  if (P.gradient) cell_gradient<T>(L, P.inv_h, g);
   write_fields<T>(P, g, c, k, j, i, uc, vc, wc);
 }
 
@@ -156,7 +164,7 @@ __global__ void probe_kernel(const T *__restrict__ f, int fnx, int fny, int fnz,
 
 template <typename T>
 cudaError_t launch_fields(const FieldsParams<T> &P, cudaStream_t s) {
-  fields_kernel<T><<<dim3((P.nx + 31) / 32, (P.ny + 7) / 8, P.nz), dim3(32, 8), 0, s>>>(P);
+  fields_kernel<T><<<dim3((P.nx + FTX - 1) / FTX, (P.ny + FTY - 1) / FTY, P.nz), dim3(FTX, FTY), 0, s>>>(P);
   return cudaGetLastError();
 }
 

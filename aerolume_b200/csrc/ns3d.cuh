@@ -41,6 +41,28 @@ struct NuParams {
   unsigned long long *nut_max;  // or NULL
 };
 
+// An actuator disc as the stage kernel sees it: its window, force and swirl weights on the
+// window's u, v, w faces, and its thrust / swirl amplitude (device scalars of this step).
+template <typename T>
+struct FanForce {
+  int win[6];
+  const T *f[3], *s[3];
+  const T *thrust, *swirl_amp;
+};
+
+// The fans' begin-of-step update (physics.py:922-942): disc velocities and the PI thrust.
+template <typename T>
+struct FanBeginParams {
+  int nfan, any_swirl, nx, ny, nz;
+  const T *u0, *v0, *w0, *dt;
+  struct {
+    int win[6], velocity_mode;
+    double target, kp, ki, tmax, swirl;
+    const T *m[3];
+    T *thrust, *ud, *e_prev, *swirl_amp;
+  } fan[AERO_MAX_FANS];
+};
+
 template <typename T>
 struct StageParams {
   CUtensorMap map_u, map_v, map_w, map_th, map_nu;  // TMA views (use_tma)
@@ -75,6 +97,8 @@ struct StageParams {
   T *thh;
   const T *chi_t, *a_t, *w_t, *adia_u, *adia_v, *adia_w, *vol_w, *skin;
   const T *paint_u, *paint_v, *paint_w;  // painted solid fractions (whole grid) or NULL
+  int nfan, fan_swirl;
+  FanForce<T> fan[AERO_MAX_FANS];
 };
 
 struct DtParams {
@@ -175,6 +199,7 @@ template <typename T> cudaError_t launch_absmax(const T *, size_t, unsigned long
 template <typename T>
 cudaError_t launch_copy_u(const T *, T *, int, int, int, int, unsigned long long *, cudaStream_t);
 template <typename T> cudaError_t launch_dt(const DtParams &, cudaStream_t);
+template <typename T> cudaError_t launch_fan_begin(const FanBeginParams<T> &, cudaStream_t);
 template <typename T> cudaError_t launch_outlet_sum(const T *, const T *, int, int, double *, cudaStream_t);
 template <typename T>
 cudaError_t launch_outlet_corr(const double *, const double *, const double *, const double *, int, const T *, double,

@@ -51,6 +51,56 @@ __global__ void copy_u_kernel(const T *__restrict__ u, T *__restrict__ out, int 
   if (mx) block_max_atomic<T>(m, mx);
 }
 
+// One block per fan (physics.py:922-942): the disc-averaged axial velocity of the step-start
+// state, sum(m_u u) + sum(m_v v) + sum(m_w w) over the fan's faces (each sum in FP64 in a
+// fixed order, rounded to the field type), then the PI update of a velocity-mode fan's thrust
+// T <- clamp(T + kP (e - e_prev) + kI dt e, -tmax, tmax) with e = target - ud, and the swirl
+// amplitude swirl ud |ud|.
+template <typename T>
+__global__ void __launch_bounds__(256) fan_begin_kernel(const __grid_constant__ FanBeginParams<T> P) {
+  __shared__ double red[3][8];
+  const auto &F = P.fan[blockIdx.x];
+  const int nx = P.nx, ny = P.ny;
+  const int k0 = F.win[0], j0 = F.win[2], i0 = F.win[4];
+  const int wz = F.win[1] - k0, wy = F.win[3] - j0, wx = F.win[5] - i0;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int c = 0; c < 3; ++c) {
+    // face window of component c: (wz + [c == 2]) x (wy + [c == 1]) x (wx + [c == 0])
+    const int ez = wz + (c == 2), ey = wy + (c == 1), ex = wx + (c == 0);
+    const size_t n = (size_t)ez * ey * ex;
+    const T *vel = c == 0 ? P.u0 : (c == 1 ? P.v0 : P.w0);
+    const int rowlen = c == 0 ? nx + 1 : nx, rows = c == 1 ? ny + 1 : ny;
+    double acc = 0.0;
+    for (size_t e = tid; e < n; e += blockDim.x) {
+      const int x = (int)(e % ex), y = (int)((e / ex) % ey), z = (int)(e / ((size_t)ex * ey));
+      acc += (double)F.m[c][e] * (double)vel[((size_t)(k0 + z) * rows + (j0 + y)) * rowlen + (i0 + x)];
+    }
+    acc = warp_sum(acc);
+    if (lane == 0) red[c][warp] = acc;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    T part[3];
+    for (int c = 0; c < 3; ++c) {
+      double t = 0.0;
+      for (int w = 0; w < (int)(blockDim.x / 32); ++w) t += red[c][w];
+      part[c] = T(t);
+    }
+    const T ud = (part[0] + part[1]) + part[2];
+    *F.ud = ud;
+    const T e = T(F.target) - ud;
+    if (F.velocity_mode) {
+      T nw = (*F.thrust + T(F.kp) * (e - *F.e_prev)) + (T(F.ki) * *P.dt) * e;
+      const T tm = T(F.tmax);
+      nw = nw > tm ? tm : nw;  // NaN passes through, as torch.minimum / maximum
+      nw = nw < -tm ? -tm : nw;
+      *F.thrust = nw;
+      *F.e_prev = e;
+    }
+    if (P.any_swirl) *F.swirl_amp = (T(F.swirl) * ud) * fabs(ud);
+  }
+}
+
 // One thread: the step's dt from the maxima (core.py:637-646, physics.py:723-742, 1230-1262),
 // rounded through the field type as the reference computes it.
 template <typename T>
@@ -485,6 +535,13 @@ cudaError_t launch_copy_u(const T *u, T *out, int nx, int ny, int nz, int pitch,
 }
 
 template <typename T>
+cudaError_t launch_fan_begin(const FanBeginParams<T> &P, cudaStream_t s) {
+  if (P.nfan <= 0) return cudaSuccess;
+  fan_begin_kernel<T><<<P.nfan, 256, 0, s>>>(P);
+  return cudaGetLastError();
+}
+
+template <typename T>
 cudaError_t launch_dt(const DtParams &P, cudaStream_t s) {
   dt_kernel<T><<<1, 1, 0, s>>>(P);
   return cudaGetLastError();
@@ -546,6 +603,7 @@ cudaError_t launch_psi_accumulate(const T *psi, T *pw, size_t n, T wgt, int mode
 #define INSTANTIATE(T)                                                                                               \
   template cudaError_t launch_absmax<T>(const T *, size_t, unsigned long long *, cudaStream_t);                     \
   template cudaError_t launch_dt<T>(const DtParams &, cudaStream_t);                                                \
+  template cudaError_t launch_fan_begin<T>(const FanBeginParams<T> &, cudaStream_t);                                \
   template cudaError_t launch_copy_u<T>(const T *, T *, int, int, int, int, unsigned long long *, cudaStream_t);                                                \
   template cudaError_t launch_outlet_sum<T>(const T *, const T *, int, int, double *, cudaStream_t);                 \
   template cudaError_t launch_outlet_corr<T>(const double *, const double *, const double *, const double *, int,  \

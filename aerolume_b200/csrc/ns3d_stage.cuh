@@ -434,6 +434,36 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) stage_kernel(c
         }
       }
 
+      // ================= actuator discs (physics.py:944-952): + f T (+ s amp), fan by fan
+      for (int q = 0; q < P.nfan; ++q) {
+        const FanForce<T> &F = P.fan[q];
+        // this cell's u / v / w faces inside the fan's window (faces i..i1 / j..j1 / k..k1)
+        const bool jc = j >= F.win[2] && j < F.win[3], ic = i >= F.win[4] && i < F.win[5];
+        const bool kc = k >= F.win[0] && k < F.win[1];
+        const bool in_u = kc && jc && i >= F.win[4] && i <= F.win[5];
+        const bool in_v = kc && ic && j >= F.win[2] && j <= F.win[3];
+        const bool in_w = jc && ic && k >= F.win[0] && k <= F.win[1];
+        if (in_u || in_v || in_w) {
+          const int fwy = F.win[3] - F.win[2], fwx = F.win[5] - F.win[4];
+          const T thrust = *F.thrust, amp = P.fan_swirl ? *F.swirl_amp : T(0);
+          if (in_u) {
+            const size_t e = ((size_t)(k - F.win[0]) * fwy + (j - F.win[2])) * (fwx + 1) + (i - F.win[4]);
+            lu = lu + F.f[0][e] * thrust;
+            if (P.fan_swirl) lu = lu + F.s[0][e] * amp;
+          }
+          if (in_v) {
+            const size_t e = ((size_t)(k - F.win[0]) * (fwy + 1) + (j - F.win[2])) * fwx + (i - F.win[4]);
+            lv = lv + F.f[1][e] * thrust;
+            if (P.fan_swirl) lv = lv + F.s[1][e] * amp;
+          }
+          if (in_w) {
+            const size_t e = ((size_t)(k - F.win[0]) * fwy + (j - F.win[2])) * fwx + (i - F.win[4]);
+            lw = lw + F.f[2][e] * thrust;
+            if (P.fan_swirl) lw = lw + F.s[2][e] * amp;
+          }
+        }
+      }
+
       // ================= boundary tendencies and RK update (core.py:527-543, 819-827) =
       const T up0 = VEL(0, 0, y, x), vp0 = VEL(1, 0, y, x), wp0 = VEL(2, 0, y, x);
       T uh, vh, wh;

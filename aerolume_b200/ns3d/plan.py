@@ -16,7 +16,7 @@ import numpy as np
 import torch
 
 from .. import _lib
-from .._lib import ADV, F32, F64, GHOST, LES, MAX_BODIES, THETA_SIDE, check
+from .._lib import ADV, F32, F64, GHOST, LES, MAX_BODIES, MAX_FANS, THETA_SIDE, check
 
 
 def _f(x) -> float:
@@ -41,12 +41,13 @@ class Ns3dPlan:
     ``thermal`` is a ``ThermalOps`` (or None); ``dye_src`` a ``DyeSources`` (or None);
     ``smoke`` turns the smoke update on inside :meth:`step`.  ``paint`` (``chi_u / chi_v /
     chi_w / chi_c`` tensors, a ``PaintLayer``), ``pid`` (``target`` and the ``dt_prev / e1 /
-    e2`` state tensors, a ``PidDt``) and ``u_floor`` (the sources' speed scale) are the step
-    controls of the placed physics (physics.py:1074-1262).
+    e2`` state tensors, a ``PidDt``), ``u_floor`` (the sources' speed scale) and ``fans`` (a
+    ``FanSet``: actuator discs with their PI thrust state) are the placed physics of
+    physics.py:831-1262 the step runs.
     """
 
     def __init__(self, ops, geom, thermal=None, dye_src=None, *, smoke: bool = False, device=None, paint=None,
-                 pid=None, u_floor: float = 0.0):
+                 pid=None, u_floor: float = 0.0, fans=None):
         self.device = torch.device(device) if device is not None else torch.device("cuda")
         if self.device.type != "cuda":
             raise RuntimeError("the B200 step runs on a CUDA device only (no CPU fallback)")
@@ -148,6 +149,9 @@ class Ns3dPlan:
                 t = getattr(paint, "chi_" + gname)
                 self._check("paint.chi_" + gname, t, shape)
                 setattr(g, "paint_" + gname, t.data_ptr())
+        self.fans = fans if fans is not None and len(fans) else None
+        if self.fans is not None:
+            self._fan_config(cfg, g, self.fans, up)
         self.cfg = cfg
         self.geom_c = g
         handle = C.c_void_p()
@@ -200,6 +204,48 @@ class Ns3dPlan:
             vals = fr.tolist() if torch.is_tensor(fr) else list(np.asarray(fr).reshape(-1))
             for q, x in enumerate(vals[:MAX_BODIES]):
                 cfg.flux_rate[q] = float(x)
+
+    def _fan_config(self, cfg, g, fans, up):
+        n = len(fans.items)
+        if n > MAX_FANS:
+            raise RuntimeError(f"the B200 step supports at most {MAX_FANS} fans")
+
+        def host(x):
+            return [float(v) for v in (x.tolist() if torch.is_tensor(x) else np.asarray(x).reshape(-1))]
+        consts = {name: host(getattr(fans, name)) for name in ("target", "kp", "ki", "tmax", "swirl")}
+        vmode = host(fans.velocity_mode)
+        cfg.nfan, cfg.fan_swirl = n, int(bool(fans.any_swirl))
+        arr = (_lib.Ns3dFan * n)()
+        nz, ny, nx = self.shape
+        for q, it in enumerate(fans.items):
+            d = arr[q]
+            win = tuple(int(x) for x in it["win"])
+            if _window_empty(win):
+                raise RuntimeError("a fan window is empty")
+            for e in range(6):
+                d.window[e] = win[e]
+            k0, k1, j0, j1, i0, i1 = win
+            shapes = {"u": (k1 - k0, j1 - j0, i1 - i0 + 1), "v": (k1 - k0, j1 - j0 + 1, i1 - i0),
+                      "w": (k1 - k0 + 1, j1 - j0, i1 - i0)}
+            d.velocity_mode = int(bool(vmode[q]))
+            for name in ("target", "kp", "ki", "tmax", "swirl"):
+                setattr(d, name, consts[name][q])
+            for kind in "fsm":
+                for comp in "uvw":
+                    a = it.get(kind + comp)
+                    if a is None:
+                        continue
+                    t = up(a)
+                    if tuple(t.shape) != shapes[comp]:
+                        raise RuntimeError(f"fan {q} weights {kind}{comp} have shape {tuple(t.shape)}, "
+                                           f"expected {shapes[comp]}")
+                    setattr(d, f"{kind}_{comp}", t.data_ptr())
+            for name in ("thrust", "ud", "e_prev", "swirl_amp"):
+                t = getattr(fans, name)
+                self._check("fans." + name, t, (n,))
+                setattr(d, name, t.data_ptr() + q * t.element_size())
+        self._fan_arr = arr
+        g.fans = C.cast(arr, C.c_void_p)
 
     def _stream(self):
         return C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)

@@ -9,9 +9,9 @@ accepts either these containers or the reference's own objects:
   ``aerolume.solvers.ns3d.physics.ThermalOps`` / ``ThermalGeometry`` the step reads
   (physics.py:314-461, 494-560)
 * :class:`DyeSources` -- ``aerolume.solvers.ns3d.dye.DyeSources`` (dye.py:140-151)
-* :class:`PaintLayer3D` / :class:`PidState3D` -- the parts of
-  ``aerolume.solvers.ns3d.physics.PaintLayer`` / ``PidDt`` the step reads and updates
-  (physics.py:1074-1181)
+* :class:`PaintLayer3D` / :class:`PidState3D` / :class:`FanSet3D` -- the parts of
+  ``aerolume.solvers.ns3d.physics.PaintLayer`` / ``PidDt`` / ``FanSet`` the step reads and
+  updates (physics.py:831-979, 1074-1181)
 * :class:`State3D`, :class:`StepOut3D` -- core.py:111-119, 745-750
 
 Arrays may be numpy arrays or torch tensors; the step uploads what is not already on the
@@ -168,3 +168,29 @@ class PidState3D:
     dt_prev: Any
     e1: Any
     e2: Any
+
+
+@dataclass
+class FanSet3D:
+    """Actuator discs (physics.py:831-979), the attributes the step reads and updates.
+
+    ``items[q]``: ``win`` (the fan's cell window) and its weights on the window's faces,
+    ``fu / fv / fw`` (force), ``su / sv / sw`` (swirl), ``mu / mv / mw`` (disc average).
+    Per-fan constants ``target, kp, ki, tmax, swirl`` and ``velocity_mode`` (nfan,), and the
+    state tensors ``thrust, ud, e_prev, swirl_amp`` (nfan,) on the device, updated in place.
+    """
+    items: list
+    target: Any
+    kp: Any
+    ki: Any
+    tmax: Any
+    velocity_mode: Any
+    swirl: Any
+    any_swirl: bool
+    thrust: Any
+    ud: Any
+    e_prev: Any
+    swirl_amp: Any
+
+    def __len__(self) -> int:
+        return len(self.items)

@@ -23,6 +23,11 @@ the same workload on this host.
 graph that spreads the instances over 16 streams; the same plans looped one after another on
 a single stream are reported beside it).
 
+``--workload fields3d`` measures the field outputs of the same 3D state (ns3d/solver.py:
+1374-1416, fields.py:45-102): one pass writes all seven cell fields (centred u, v, w, speed,
+vorticity magnitude, Q-criterion, eddy viscosity) from the staggered velocity, and a
+million trilinear probes of the speed field are timed beside it.
+
 With ``--gpus N`` (N > 1, launched by torch.distributed.run) every rank advances its own
 replica (no data-path collective: a single instance of this solver does not shard), and
 ``value`` is the total over ranks.  ``--impl reference`` times the reference arm: the
@@ -568,6 +573,146 @@ def run_sweep(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+FIELDS_METRIC = "Mcell/s of field outputs (7 cell fields per pass) on 1 B200"
+FIELDS_UNIT = "Mcell/s"
+
+
+def _fields_oracle(u, v, w, ops, geom):
+    """The oracle's seven fields of one state (chi_c on the body window as the eddy-viscosity mask)."""
+    from oracle import fields3d as F
+    mask = None
+    if not geom.empty:
+        k0, k1, j0, j1, i0, i1 = geom.window
+        mask = np.zeros(u[..., 1:].shape, u.dtype)
+        mask[k0:k1, j0:j1, i0:i1] = geom.chi_c
+    return [F.centre_u(u), F.centre_v(v), F.centre_w(w), F.speed(u, v, w)] + \
+        [F.gradient_field(n, u, v, w, ops, mask) for n in ("vorticity", "q", "nut")]
+
+
+def _fields_setup(shape, device):
+    from aerolume_b200.ns3d.workloads import box_on_moving_floor, initial_state
+    nx, ny, nz = shape
+    ops, geom, th, src, _ = box_on_moving_floor(nx, ny, nz, dtype="float32")
+    u, v, w = initial_state(ops, device=device)
+    return ops, geom, th, src, u, v, w
+
+
+def run_fields(args, rank, world, local_rank):
+    import torch
+    from aerolume_b200 import _lib
+    from aerolume_b200.ns3d.plan import Ns3dPlan
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    nx, ny, nz = args.shape
+    cells = nx * ny * nz
+    ops, geom, th, src, u, v, w = _fields_setup(args.shape, dev)
+    plan = Ns3dPlan(ops, geom, th, src, smoke=True, device=dev)
+    names = _lib.FIELD_NAMES
+    for _ in range(args.warmup):
+        plan.fields(u, v, w, names)
+    torch.cuda.synchronize()
+    K = args.steps
+    s = torch.cuda.Stream(device=dev)
+    s.wait_stream(torch.cuda.current_stream(dev))
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(s):
+        with torch.cuda.graph(g, stream=s):
+            for _ in range(K):
+                plan.fields(u, v, w, names)
+    torch.cuda.current_stream(dev).wait_stream(s)
+    ms, clk = _time_graph(g, dist, local_rank, rank, dev)
+    # probes: a million seeded points in the domain, trilinear samples of the speed field
+    speed = plan.fields(u, v, w, ("speed",))["speed"]
+    gen = torch.Generator(device="cpu").manual_seed(0)
+    ext = torch.tensor([nx, ny, nz], dtype=torch.float32) * float(ops.h)
+    pts = (torch.rand(1 << 20, 3, generator=gen) * ext).to(dev).contiguous()
+    for _ in range(3):
+        plan.probe(speed, pts)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(K):
+        plan.probe(speed, pts)
+    e1.record()
+    torch.cuda.synchronize()
+    probe_ms = e0.elapsed_time(e1) / K
+    # e2e: state in from pinned host memory, the seven fields back out
+    host_in = [torch.empty(x.shape, dtype=x.dtype, pin_memory=True).copy_(x) for x in (u, v, w)]
+    host_out = [torch.empty((nz, ny, nx), dtype=u.dtype, pin_memory=True) for _ in names]
+    d_in = [torch.empty_like(x) for x in (u, v, w)]
+    torch.cuda.synchronize()
+    ke = max(3, min(K, 10))
+    e0.record()
+    for _ in range(ke):
+        for d, h in zip(d_in, host_in):
+            d.copy_(h, non_blocking=True)
+        res = plan.fields(*d_in, names)
+        for h, n in zip(host_out, names):
+            h.copy_(res[n], non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    ems = e0.elapsed_time(e1) / ke
+    if rank != 0:
+        return
+    peak, peak_kind = _peaks()
+    # algorithmic bytes per pass, FP32: the three face arrays read once, seven cell fields written
+    alg = 4 * (u.numel() + v.numel() + w.numel() + len(names) * cells)
+    achieved = alg / (ms / K * 1e-3) / 1e9
+    cpu = None
+    if not args.no_cpu:
+        un, vn, wn = (x.cpu().numpy() for x in (u, v, w))
+        _fields_oracle(un, vn, wn, ops, geom)
+        t0 = time.perf_counter()
+        _fields_oracle(un, vn, wn, ops, geom)
+        secs = time.perf_counter() - t0
+        cpu = {"value": cells / secs / 1e6, "unit": FIELDS_UNIT, "cores": _threads(), "kind": "port",
+               "sample": f"one full {nx}x{ny}x{nz} pass of the numpy field oracle after 1 untimed pass"}
+    line = {"metric": FIELDS_METRIC, "value": world * cells * K / (ms * 1e-3) / 1e6, "unit": FIELDS_UNIT,
+            "n_gpus": world, "steps": K, "warmup": args.warmup, "ms_per_step": ms / K, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"field outputs of the box-on-moving-floor state {nx}x{ny}x{nz} FP32 (WALE)",
+                       "fields": list(names), "inputs_vs_l2": "67 MB in + 117 MB out per pass > 126 MB L2",
+                       "parallelism": "replicas", "graph": f"{K} passes, 1 replay"},
+            "roofline": {"bound": "hbm", "kernel": "fields_kernel", "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                         "alg_bytes_per_launch": alg},
+            "probes": {"value": (1 << 20) / (probe_ms * 1e-3) / 1e6, "unit": "Mpoints/s", "ms": probe_ms,
+                       "points": 1 << 20, "field": "speed"},
+            "cpu_baseline": cpu,
+            "e2e": {"value": world * cells / (ems * 1e-3) / 1e6, "unit": FIELDS_UNIT,
+                    "h2d_bytes_per_step": int(sum(x.numel() * x.element_size() for x in host_in)),
+                    "d2h_bytes_per_step": int(sum(x.numel() * x.element_size() for x in host_out)),
+                    "ms_per_step": ems, "steps": ke},
+            "gpu_launches": K, "clocks": clk, "status": plan.status()}
+    print(json.dumps(line), flush=True)
+
+
+def run_reference_fields(args, rank):
+    if rank != 0:
+        return
+    nx, ny, nz = args.shape
+    ops, geom, _, _, u, v, w = _fields_setup(args.shape, "cpu")
+    un, vn, wn = (x.numpy() for x in (u, v, w))
+    _fields_oracle(un, vn, wn, ops, geom)
+    steps = max(1, min(args.steps, 3))
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        _fields_oracle(un, vn, wn, ops, geom)
+    secs = time.perf_counter() - t0
+    val = nx * ny * nz * steps / secs / 1e6
+    line = {"impl": "reference", "metric": FIELDS_METRIC, "value": val, "unit": FIELDS_UNIT, "n_gpus": args.gpus,
+            "steps": steps, "warmup": 1, "ms_per_step": 1e3 * secs / steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"field outputs of the box-on-moving-floor state {nx}x{ny}x{nz} FP32 (WALE)"},
+            "cpu_baseline": {"value": val, "unit": FIELDS_UNIT, "cores": _threads(), "kind": "port",
+                             "sample": f"{steps} full passes of the numpy field oracle after 1 untimed pass"},
+            "e2e": {"value": val, "unit": FIELDS_UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
 def run_reference_2d(args, rank):
     from aerolume_b200.ns2d.workloads import cylinder_tunnel, sweep_instances
     if rank != 0:
@@ -595,20 +740,22 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=None, help="timed steps (default 20; 400 for cylinder2d, "
                                                              "10 for sweep2d)")
-    ap.add_argument("--workload", default="box3d", choices=["box3d", "cylinder2d", "sweep2d"])
+    ap.add_argument("--workload", default="box3d", choices=["box3d", "cylinder2d", "sweep2d", "fields3d"])
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--shape", type=int, nargs=3, default=list(SHAPE), help="nx ny nz (2:1:1)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     args = ap.parse_args()
     if args.steps is None:
-        args.steps = {"box3d": 20, "cylinder2d": 400, "sweep2d": 10}[args.workload]
+        args.steps = {"box3d": 20, "cylinder2d": 400, "sweep2d": 10, "fields3d": 20}[args.workload]
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         if args.workload == "box3d":
             run_reference(args, rank)
+        elif args.workload == "fields3d":
+            run_reference_fields(args, rank)
         else:
             run_reference_2d(args, rank)
         return
@@ -620,7 +767,8 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     try:
-        {"box3d": run_ours, "cylinder2d": run_2d, "sweep2d": run_sweep}[args.workload](args, rank, world, local_rank)
+        {"box3d": run_ours, "cylinder2d": run_2d, "sweep2d": run_sweep, "fields3d": run_fields}[args.workload](
+            args, rank, world, local_rank)
     finally:
         if world > 1:
             import torch.distributed as dist

@@ -44,6 +44,7 @@ extern "C" {
 #define AERO_ECUDA -3         /* a CUDA launch or runtime call failed                */
 
 #define AERO_MAX_BODIES 8
+#define AERO_MAX_FANS 4
 
 enum { AERO_F32 = 0, AERO_F64 = 1 };
 enum { AERO_ADV_UPWIND3 = 0, AERO_ADV_CENTRAL = 1 };
@@ -105,7 +106,24 @@ typedef struct AeroNs3dConfig {
   int32_t pid;                  /* PID control of dt towards pid_target x the limit         */
   double pid_target;
   int32_t paint;                /* painted solids (geom paint_*; physics.py:1074-1141)      */
+  int32_t nfan;                 /* actuator discs (geom fans; physics.py:831-979)           */
+  int32_t fan_swirl;            /* any fan with swirl                                       */
 } AeroNs3dConfig;
+
+/* One actuator disc (ns3d/physics.py:831-979): its cell window, the force, swirl and
+ * disc-average weights on the window's u, v, w faces (the shapes of the body window's
+ * masks, over the fan's own window), the PI constants, and its state: 0-d scalars of the
+ * plan's dtype that every step updates in place (thrust T, disc velocity ud, PI error
+ * e_prev, swirl amplitude). */
+typedef struct AeroNs3dFan {
+  int32_t window[6];            /* k0, k1, j0, j1, i0, i1                                  */
+  int32_t velocity_mode;        /* 1: PI on the thrust towards target; 0: fixed thrust     */
+  double target, kp, ki, tmax, swirl;
+  const void *f_u, *f_v, *f_w;  /* n_g phi_g / (sum phi h^3)                               */
+  const void *s_u, *s_v, *s_w;  /* swirl weights                                           */
+  const void *m_u, *m_v, *m_w;  /* disc-average weights                                    */
+  void *thrust, *ud, *e_prev, *swirl_amp;
+} AeroNs3dFan;
 
 /* Window masks and constant inputs (device pointers of the plan's dtype; NULL when absent).
  * Shapes are those of ns3d/geometry.py:275-303 and ns3d/physics.py:314-461. */
@@ -121,6 +139,7 @@ typedef struct AeroNs3dGeom {
   /* painted solid fractions on the whole grid (u, v, w faces and cells; read at every step,
    * so strokes between steps take effect) */
   const void *paint_u, *paint_v, *paint_w, *paint_c;
+  const AeroNs3dFan *fans;      /* host array of cfg.nfan descriptors, read at every step  */
 } AeroNs3dGeom;
 
 /* State in and out (device pointers of the plan's dtype).  u may alias u0, v v0, w w0 and

@@ -18,6 +18,7 @@ the sm_100a kernels implement (Aerolume ``src/aerolume/solvers/ns3d``):
 * ``Physics3D.dt_rule``  physics.py:1230-1262 (with the sources' speed floor and ``PidDt``,
                          physics.py:1144-1181)
 * ``PaintLayer``         physics.py:1074-1141 painted solids, penalised after the bodies
+* ``FanSet``             physics.py:831-979 actuator discs: disc velocity, PI thrust, forces
 * smoke                  dye.py:232-312    MUSCL / van Leer advection, solids, nozzles
 
 Parity is pinned: ``tests/test_oracle_golden.py`` checks this module against golden
@@ -342,8 +343,9 @@ def boundary_tendencies(u, lu, lv, lw, ops):
     return lu, lv, lw
 
 
-def momentum_rhs3d(u, v, w, geom, ops):
-    """Explicit tendencies, nu_t field and max (core.py:546-570)."""
+def momentum_rhs3d(u, v, w, geom, ops, sources=None):
+    """Explicit tendencies, nu_t field and max (core.py:546-570); ``sources`` (lu, lv, lw) ->
+    (lu, lv, lw) adds the placed physics' forces before the boundary tendencies."""
     T = u.dtype.type
     U, V, W = pad_velocity(u, v, w, ops)
     au, av, aw = advection3(U, V, W, ops)
@@ -355,6 +357,8 @@ def momentum_rhs3d(u, v, w, geom, ops):
     if ops.turbulence != "none":
         fu, fv, fw, nut, nut_max = sgs_divergence3d(U, V, W, geom, ops)
         lu, lv, lw = lu + fu, lv + fv, lw + fw
+    if sources is not None:
+        lu, lv, lw = sources(lu, lv, lw)
     lu, lv, lw = boundary_tendencies(u, lu, lv, lw, ops)
     return lu, lv, lw, nut, nut_max
 
@@ -726,6 +730,51 @@ def pid_dt(pid, dt_cap):
     return dt
 
 
+class FanState:
+    """FanSet (physics.py:831-979) in numpy.  ``items[q]``: ``win`` and the weight triples
+    ``f`` (force), ``s`` (swirl), ``m`` (disc average) on the window's u, v, w faces;
+    per-fan constants (nfan,) and the state ``thrust, ud, e_prev, swirl_amp`` (nfan,)."""
+
+    def __init__(self, items, target, kp, ki, tmax, velocity_mode, swirl, any_swirl, thrust, dtype):
+        T = np.dtype(dtype).type
+        self.items = items
+        self.target, self.kp, self.ki, self.tmax, self.swirl = (np.asarray(x, dtype) for x in
+                                                                 (target, kp, ki, tmax, swirl))
+        self.velocity_mode = np.asarray(velocity_mode, bool)
+        self.any_swirl = bool(any_swirl)
+        self.thrust = np.asarray(thrust, dtype).copy()
+        self.ud, self.e_prev, self.swirl_amp = (np.zeros(len(items), dtype) for _ in range(3))
+        self.T = T
+
+
+def fan_begin_step(fans, u0, v0, w0, dt):
+    """FanSet.measure + begin_step (physics.py:922-942)."""
+    T = fans.T
+    ud = np.array([T(T(T(np.sum(it["m"][0] * u0[_face_slices(it["win"], "u")])) +
+                       T(np.sum(it["m"][1] * v0[_face_slices(it["win"], "v")]))) +
+                     T(np.sum(it["m"][2] * w0[_face_slices(it["win"], "w")]))) for it in fans.items], fans.thrust.dtype)
+    fans.ud = ud
+    e = fans.target - ud
+    new = (fans.thrust + fans.kp * (e - fans.e_prev)) + (fans.ki * T(dt)) * e
+    new = np.maximum(np.minimum(new, fans.tmax), -fans.tmax)
+    fans.thrust = np.where(fans.velocity_mode, new, fans.thrust)
+    fans.e_prev = np.where(fans.velocity_mode, e, fans.e_prev)
+    if fans.any_swirl:
+        fans.swirl_amp = (fans.swirl * ud) * np.abs(ud)
+
+
+def fan_forces(fans, lu, lv, lw):
+    """FanSet.add_forces (physics.py:944-952): + f T (+ s amp) on each fan's faces."""
+    out = [lu.copy(), lv.copy(), lw.copy()]
+    for q, it in enumerate(fans.items):
+        for c, g in enumerate("uvw"):
+            sl = _face_slices(it["win"], g)
+            out[c][sl] = out[c][sl] + it["f"][c] * fans.thrust[q]
+            if fans.any_swirl:
+                out[c][sl] = out[c][sl] + it["s"][c] * fans.swirl_amp[q]
+    return tuple(out)
+
+
 def dt_rule(u0, v0, w0, ops, nut_max, th, theta, u_floor=0.0, pid=None):
     """Physics3D.dt_rule without fans and ports (physics.py:1230-1262); ``u_floor`` is the
     sources' speed scale, ``pid`` a :class:`PidState` (or None)."""
@@ -762,10 +811,10 @@ class StepResult:
 
 
 def step3d_phys(u0, v0, w0, t, geom, ops, poisson, *, th=None, theta=None, dt=None, trace=False, paint=None,
-                pid=None, u_floor=0.0):
+                pid=None, u_floor=0.0, fans=None):
     """One SSP-RK3 step (core.py:765-883) with heat transfer, buoyancy, painted solids
-    (``paint``: (chi_u, chi_v, chi_w) on the whole grid) and the PID / speed-floor dt rule;
-    no fans or ports."""
+    (``paint``: (chi_u, chi_v, chi_w) on the whole grid), the PID / speed-floor dt rule and
+    fans (a :class:`FanState`, updated in place); no ports."""
     T = u0.dtype.type
     up, vp, wp = u0, v0, w0
     acc = None
@@ -775,18 +824,25 @@ def step3d_phys(u0, v0, w0, t, geom, ops, poisson, *, th=None, theta=None, dt=No
     heat_acc = np.zeros(geom.nbody if not geom.empty else max(geom.nbody, 0), dtype=np.float64)
     stages = []
     nut_stage1 = None
+    placed = th is not None or pid is not None or u_floor > 0.0 or fans is not None
     for s, ((a, b), wgt) in enumerate(zip(SSP_RK3, FORCE_WEIGHTS)):
-        lu, lv, lw, nut, nut_max = momentum_rhs3d(up, vp, wp, geom, ops)
         if s == 0:
+            # the dt rule and the fans' controllers act before any source is evaluated
+            lu, lv, lw, nut, nut_max = momentum_rhs3d(up, vp, wp, geom, ops)
             nut_stage1 = nut
             if dt is None:
                 if ops.dt_fixed is not None:
                     dt = T(ops.dt_fixed)
-                elif thermal or th is not None or pid is not None or u_floor > 0.0:
+                elif placed:
                     dt = dt_rule(u0, v0, w0, ops, nut_max, th, t0, u_floor, pid)
                 else:
                     dt = cfl_dt3d(u0, v0, w0, ops, nut_max)[0]
             dt = T(dt)
+            if fans is not None:
+                fan_begin_step(fans, u0, v0, w0, dt)
+        if s > 0 or fans is not None:
+            lu, lv, lw, nut, nut_max = momentum_rhs3d(
+                up, vp, wp, geom, ops, sources=None if fans is None else (lambda a, b_, c: fan_forces(fans, a, b_, c)))
         bdt = T(dt * T(b))
         if a == 0.0:
             uh, vh, wh = up + lu * bdt, vp + lv * bdt, wp + lw * bdt

@@ -55,6 +55,20 @@ def load_case(name):
     return meta, ops, geom, th, src, arr
 
 
+def fan_items(meta, arr):
+    """Per-fan windows and weights of a golden case (numpy, the case dtype):
+    [{"win", "fu".."fw", "su".."sw", "mu".."mw"}]."""
+    dt = np.float64 if meta["dtype"] == "float64" else np.float32
+    out = []
+    for q, win in enumerate(meta["fans"]["win"]):
+        it = {"win": tuple(win)}
+        for kind in "fsm":
+            for g in "uvw":
+                it[kind + g] = arr[f"fan{q}_{kind}{g}"].astype(dt)
+        out.append(it)
+    return out
+
+
 CASES_2D = sorted(p.stem[len("ns2d_"):] for p in GOLDEN.glob("ns2d_*.npz"))
 
 

@@ -31,7 +31,7 @@ REF = Path(os.environ.get("AEROLUME_REF", "/root/reference"))
 sys.path.insert(0, str(REF / "src"))
 
 from aerolume.solvers.ns3d import core  # noqa: E402
-from aerolume.solvers.ns3d.config import DyeRake, ImmersedMesh, SolverConfig3D, ThermalConfig3D  # noqa: E402
+from aerolume.solvers.ns3d.config import DyeRake, Fan3D, ImmersedMesh, SolverConfig3D, ThermalConfig3D  # noqa: E402
 from aerolume.solvers.ns3d.dye import advect_dye3d, apply_solids_and_sources, build_dye_sources  # noqa: E402
 from aerolume.solvers.ns3d.geometry import body_window3d, build_geometry3d  # noqa: E402
 from aerolume.solvers.ns3d.physics import PaintLayer, Physics3D  # noqa: E402
@@ -116,6 +116,16 @@ def extract(ops, geom, phys, src):
     if phys is not None and phys.paint is not None:
         for g in "uvwc":
             arrays["paint_" + g] = _np(getattr(phys.paint, "chi_" + g))
+    if phys is not None and phys.fans is not None:
+        fs = phys.fans
+        meta["fans"] = {"any_swirl": bool(fs.any_swirl), "win": [list(it["win"]) for it in fs.items],
+                        **{k: [float(x) for x in getattr(fs, k).tolist()]
+                           for k in ("target", "kp", "ki", "tmax", "swirl", "thrust")},
+                        "velocity_mode": [bool(x) for x in fs.velocity_mode.tolist()]}
+        for q, it in enumerate(fs.items):
+            for kind in "fsm":
+                for g in "uvw":
+                    arrays[f"fan{q}_{kind}{g}"] = _np(it[kind + g])
     return meta, arrays
 
 
@@ -156,6 +166,10 @@ def _run_case(name, cfg_kw, *, dtype="float64", amp=0.1, seed=1, rake=None, step
             st, th = new, out.theta
             if phys is not None and phys.pid is not None:
                 arrays[f"pid{k + 1}"] = np.array([float(phys.pid.dt_prev), float(phys.pid.e1), float(phys.pid.e2)])
+            if phys is not None and phys.fans is not None:   # thrust, ud, e_prev, swirl_amp after the step
+                f = phys.fans
+                arrays[f"fans{k + 1}"] = np.stack([_np(x).astype(np.float64) for x in (f.thrust, f.ud, f.e_prev,
+                                                                                       f.swirl_amp)])
             if k == 0:
                 arrays.update({"out1_u": _np(new.u), "out1_v": _np(new.v), "out1_w": _np(new.w),
                                "out1_p": _np(new.p), "out1_t": _np(new.t), "out1_dt": _np(new.dt),
@@ -247,6 +261,19 @@ def main():
     plain_pid = dict(grid, re=500.0, adaptive_dt="pid", pid_target=0.9)
     run_case("plain_pid_paint_f64", plain_pid, dtype="float64", steps=3, seed=9, amp=0.3,
              strokes=(dict(center=(2.0, 1.0, 0.8), radius=0.4),))
+    # two fans: a velocity-regulated one with swirl and a fixed-thrust one at an angle, three
+    # steps so that the PI controller acts on its own output
+    fans = [Fan3D(center=(1.1, 1.0, 0.85), direction=(1.0, 0.0, 0.0), diameter=0.9, mode="velocity", value=1.4,
+                  swirl=0.5, name="a"),
+            Fan3D(center=(2.7, 1.1, 0.8), direction=(0.6, 0.8, 0.0), diameter=0.7, mode="thrust", value=0.08, name="b")]
+    fan_case = dict(grid, re=600.0, fans=fans, turbulence="wale")
+    run_case("fans_swirl_f64", fan_case, dtype="float64", steps=3, seed=10, amp=0.1)
+    run_case("fans_swirl_f32", fan_case, dtype="float32", steps=3, seed=10, amp=0.1)
+    closed_fan = dict(grid, nx=14, ny=10, nz=10, re=300.0, domain="closed", bc_x="noslip", bc_y="noslip",
+                      bc_zmin="noslip", bc_zmax="noslip",
+                      fans=[Fan3D(center=(1.2, 0.8, 0.8), direction=(0.0, 0.0, 1.0), diameter=0.8,
+                                  mode="pressure_jump", value=0.3, name="up")])
+    run_case("closed_fan_pressure_f64", closed_fan, dtype="float64", steps=3, seed=11, amp=0.05)
     if not names or "poisson" in names:
         poisson_cases()
     for p in sorted(HERE.glob("*.npz")):

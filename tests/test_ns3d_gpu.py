@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 import torch
 
-from _golden import CASES_3D, GOLDEN, load_case
+from _golden import CASES_3D, GOLDEN, fan_items, load_case
 from oracle import ns3d as O
 
 pytestmark = pytest.mark.gpu
@@ -28,14 +28,23 @@ def _dev(x, dt):
 
 def _plan_and_inputs(name):
     from aerolume_b200.ns3d.plan import Ns3dPlan
-    from aerolume_b200.ns3d.types import PaintLayer3D, PidState3D
+    from aerolume_b200.ns3d.types import FanSet3D, PaintLayer3D, PidState3D
     meta, ops, geom, th, src, arr = load_case(name)
     dt = torch.float64 if meta["dtype"] == "float64" else torch.float32
     paint = PaintLayer3D(*(_dev(arr["paint_" + g], dt) for g in "uvwc")) if "paint_u" in arr else None
     pid = None
     if "pid" in meta:
         pid = PidState3D(meta["pid"]["target"], *(torch.zeros((), device="cuda", dtype=dt) for _ in range(3)))
-    plan = Ns3dPlan(ops, geom, th, src, smoke=True, paint=paint, pid=pid, u_floor=meta.get("u_floor", 0.0))
+    fans = None
+    if "fans" in meta:
+        fm = meta["fans"]
+        items = [{k: (_dev(x, dt) if k != "win" else x) for k, x in it.items()} for it in fan_items(meta, arr)]
+        n = len(items)
+        fans = FanSet3D(items, *(fm[k] for k in ("target", "kp", "ki", "tmax", "velocity_mode", "swirl")),
+                        fm["any_swirl"], torch.tensor(fm["thrust"], device="cuda", dtype=dt),
+                        *(torch.zeros(n, device="cuda", dtype=dt) for _ in range(3)))
+    plan = Ns3dPlan(ops, geom, th, src, smoke=True, paint=paint, pid=pid, u_floor=meta.get("u_floor", 0.0),
+                    fans=fans)
     ins = {"u0": _dev(arr["in_u"], dt), "v0": _dev(arr["in_v"], dt), "w0": _dev(arr["in_w"], dt),
            "t0": _dev(arr["in_t"], dt), "dye0": _dev(arr["in_dye"], dt)}
     if th is not None:
@@ -45,6 +54,10 @@ def _plan_and_inputs(name):
 
 def _pid_state(plan):
     return np.array([float(getattr(plan.pid, n)) for n in ("dt_prev", "e1", "e2")])
+
+
+def _fan_state(plan):
+    return np.stack([getattr(plan.fans, n).double().cpu().numpy() for n in ("thrust", "ud", "e_prev", "swirl_amp")])
 
 
 @pytest.mark.parametrize("name", CASES_3D)
@@ -70,17 +83,20 @@ def test_one_step_matches_reference(name):
     if "pid" in meta:
         ref = arr["pid1"]
         assert np.abs(_pid_state(plan) - ref).max() <= TOL[meta["dtype"]] * max(1.0, np.abs(ref).max())
+    if "fans" in meta:
+        ref = arr["fans1"]
+        assert np.abs(_fan_state(plan) - ref).max() <= TOL[meta["dtype"]] * max(1.0, np.abs(ref).max())
     assert plan.status() == 0
 
 
-@pytest.mark.parametrize("name", [n for n in CASES_3D if "tunnel" in n or "pid" in n])
+@pytest.mark.parametrize("name", [n for n in CASES_3D if "tunnel" in n or "pid" in n or "fan" in n])
 def test_three_steps_in_place_match_reference(name):
     """Three steps updating the state in place (u, v, w, theta outputs alias the inputs)."""
     meta, plan, ins, arr = _plan_and_inputs(name)
     u, v, w, t = ins["u0"], ins["v0"], ins["w0"], ins["t0"]
     theta, dye = ins.get("theta0"), ins["dye0"]
     out = plan.empty_fields()
-    pids = []
+    pids, fan_states = [], []
     for _ in range(3):
         out["u"], out["v"], out["w"] = u, v, w
         if theta is not None:
@@ -90,6 +106,8 @@ def test_three_steps_in_place_match_reference(name):
         dye = out["dye"].clone()
         if "pid" in meta:
             pids.append(_pid_state(plan))
+        if "fans" in meta:
+            fan_states.append(_fan_state(plan))
     torch.cuda.synchronize()
     tol = 10 * TOL[meta["dtype"]]
     for f, x in (("u", u), ("v", v), ("w", w), ("p", out["p"]), ("theta", theta), ("dye", dye)):
@@ -97,6 +115,9 @@ def test_three_steps_in_place_match_reference(name):
             assert _rel(x, arr["outN_" + f]) < tol, (f, _rel(x, arr["outN_" + f]))
     for k, got in enumerate(pids):  # the PID state after every step
         ref = arr[f"pid{k + 1}"]
+        assert np.abs(got - ref).max() <= tol * max(1.0, np.abs(ref).max()), k
+    for k, got in enumerate(fan_states):  # thrust, disc velocity, PI error, swirl amplitude
+        ref = arr[f"fans{k + 1}"]
         assert np.abs(got - ref).max() <= tol * max(1.0, np.abs(ref).max()), k
 
 

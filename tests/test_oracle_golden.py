@@ -4,7 +4,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from _golden import CASES_3D, GOLDEN, load_case
+from _golden import CASES_3D, GOLDEN, fan_items, load_case
 from oracle import ns3d as O
 
 
@@ -17,10 +17,17 @@ def _run(name, steps=1):
     c = arr["in_dye"]
     paint = tuple(arr["paint_" + g] for g in "uvw") if "paint_u" in arr else None
     pid = O.PidState(meta["pid"]["target"], dt) if "pid" in meta else None
+    fans = None
+    if "fans" in meta:
+        fm = meta["fans"]
+        items = [{"win": it["win"], "f": tuple(it["f" + g] for g in "uvw"), "s": tuple(it["s" + g] for g in "uvw"),
+                  "m": tuple(it["m" + g] for g in "uvw")} for it in fan_items(meta, arr)]
+        fans = O.FanState(items, fm["target"], fm["kp"], fm["ki"], fm["tmax"], fm["velocity_mode"], fm["swirl"],
+                          fm["any_swirl"], fm["thrust"], dt)
     outs = []
     for _ in range(steps):
         r = O.step3d_phys(u, v, w, t, geom, ops, ps, th=th, theta=theta, paint=paint, pid=pid,
-                          u_floor=meta.get("u_floor", 0.0))
+                          u_floor=meta.get("u_floor", 0.0), fans=fans)
         c = O.advect_dye3d(c, r.u, r.v, r.w, r.dt, ops)
         c = O.apply_solids_and_sources(c, r.t, geom, src)
         if "paint_c" in arr:                         # painted cells hold no smoke
@@ -28,6 +35,7 @@ def _run(name, steps=1):
         u, v, w, t, theta = r.u, r.v, r.w, r.t, r.theta
         r.dye = c
         r.pid = None if pid is None else np.array([float(pid.dt_prev), float(pid.e1), float(pid.e2)])
+        r.fans = None if fans is None else np.stack([fans.thrust, fans.ud, fans.e_prev, fans.swirl_amp]).astype(np.float64)
         outs.append(r)
     return meta, arr, outs
 
@@ -55,7 +63,7 @@ def test_oracle_matches_reference_one_step(name):
     assert _rel(r.dye, arr["out1_dye"]) < tol
 
 
-@pytest.mark.parametrize("name", [n for n in CASES_3D if "tunnel" in n or "pid" in n])
+@pytest.mark.parametrize("name", [n for n in CASES_3D if "tunnel" in n or "pid" in n or "fan" in n])
 def test_oracle_matches_reference_three_steps(name):
     meta, arr, outs = _run(name, steps=3)
     r = outs[-1]
@@ -68,6 +76,10 @@ def test_oracle_matches_reference_three_steps(name):
         for k, rk in enumerate(outs):
             ref = arr[f"pid{k + 1}"]
             assert np.abs(rk.pid - ref).max() <= (1e-12 if meta["dtype"] == "float64" else 1e-5) * max(1.0, np.abs(ref).max()), k
+    if "fans" in meta:  # thrust, disc velocity, PI error, swirl amplitude after every step
+        for k, rk in enumerate(outs):
+            ref = arr[f"fans{k + 1}"]
+            assert np.abs(rk.fans - ref).max() <= (1e-11 if meta["dtype"] == "float64" else 1e-5) * max(1.0, np.abs(ref).max()), k
 
 
 def test_oracle_poisson_matches_reference():
@@ -95,3 +107,16 @@ def test_paint_and_pid_fixtures_exercise_both():
     assert _rel(no_paint.u, arr["out1_u"]) > 1e-4
     no_pid = O.step3d_phys(*args, **kw, paint=paint)
     assert abs(float(no_pid.dt) - float(arr["out1_dt"])) > 1e-3 * float(arr["out1_dt"])
+
+
+def test_fan_fixtures_exercise_the_fans():
+    """The fans move the flow and the controller moves the thrust: leaving them out, or
+    freezing the thrust, is far outside the tolerances."""
+    meta, ops, geom, th, src, arr = load_case("fans_swirl_f64")
+    ps = O.PoissonSolver3D(ops.nx, ops.ny, ops.nz, ops.h, ops.periodic_axes, np.float64)
+    r = O.step3d_phys(arr["in_u"], arr["in_v"], arr["in_w"], np.float64(arr["in_t"]), geom, ops, ps,
+                      u_floor=meta["u_floor"])
+    assert _rel(r.u, arr["out1_u"]) > 1e-3
+    thrust = arr["fans3"][0]
+    assert abs(thrust[0] - meta["fans"]["thrust"][0]) > 1e-3 * abs(meta["fans"]["thrust"][0])  # regulated
+    assert thrust[1] == meta["fans"]["thrust"][1]                                             # fixed
