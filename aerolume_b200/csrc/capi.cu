@@ -365,6 +365,19 @@ int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom
     d.thrust = static_cast<const T *>(F.thrust);
     d.swirl_amp = static_cast<const T *>(F.swirl_amp);
   }
+  S.nport = c.nport;
+  S.port_leak = T(c.port_leak);
+  for (int q = 0; q < c.nport; ++q) {
+    const AeroNs3dPort &Q = g->ports[q];
+    auto &d = S.port[q];
+    for (int e = 0; e < 6; ++e) d.win[e] = Q.window[e];
+    d.vent = Q.vent;
+    d.theta = T(Q.theta);
+    d.f[0] = static_cast<const T *>(Q.f_u);
+    d.f[1] = static_cast<const T *>(Q.f_v);
+    d.f[2] = static_cast<const T *>(Q.f_w);
+    d.m = static_cast<const T *>(Q.m);
+  }
   S.a_u = static_cast<const T *>(g->a_u);
   S.a_v = static_cast<const T *>(g->a_v);
   S.a_w = static_cast<const T *>(g->a_w);
@@ -487,7 +500,8 @@ int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom
                                                       rows);
       CUDA_TRY(cudaGetLastError());
       CUDA_TRY(aero::launch_outlet_corr<T>(sums, sums + PLANE_PARTS, psum, psum + PLANE_PARTS, PLANE_PARTS, small,
-                                           RK[st][0], RK[st][1], 1.0 / c.h, 1.0 / rows, small + 1, s));
+                                           RK[st][0], RK[st][1], 1.0 / c.h, 1.0 / rows,
+                                           c.nport > 0 ? c.port_source : 0.0, small + 1, s));
     }
     if (les && st > 0) {
       aero::NuParams<T> N = NP;
@@ -515,7 +529,7 @@ int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom
     CUDA_TRY(aero::launch_stage<T>(P, s));
     CUDA_TRY(mark(3 + 5 * st));
     const int acc_mode = st == 0 ? 0 : (st == 1 ? 1 : 2);
-    if (p->ax[0].method == 0 && aero::transform_pow2(nx)) {
+    if (p->ax[0].method == 0 && aero::transform_pow2(nx) && c.nport == 0) {
       // the first x pass forms div(u_hat) itself, the last one folds psi into p
       aero::TransformParams<T> F{};
       F.fuse_div = 1;
@@ -536,6 +550,7 @@ int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom
     } else {
       CUDA_TRY(aero::launch_divergence<T>(uh, vh, wh, nx, ny, nz, c.periodic[0], c.periodic[1], c.periodic[2],
                                           T(1.0 / c.h), pa, s));
+      CUDA_TRY(aero::launch_port_continuity<T>(pa, nx, ny, S.nport, S.port, s));  // div - m (jets, vents)
       CUDA_TRY(mark(4 + 5 * st));
       const int rc = poisson_passes<T>(p, pa, pa, ws, s);
       if (rc) return rc;
@@ -786,6 +801,11 @@ int aero_ns3d_plan_create(const AeroNs3dConfig *cfg, AeroNs3dPlan **plan) {
   if (c.pid && !(c.pid_target >= 0.1 && c.pid_target <= 1.0)) return fail(AERO_EINVAL, "pid_target must be in [0.1, 1]");
   if (c.nfan < 0 || c.nfan > AERO_MAX_FANS)
     return fail(AERO_EUNSUPPORTED, "at most " + std::to_string(AERO_MAX_FANS) + " fans");
+  if (c.nport < 0 || c.nport > AERO_MAX_PORTS)
+    return fail(AERO_EUNSUPPORTED, "at most " + std::to_string(AERO_MAX_PORTS) + " jets and vents");
+  if (c.nport > 0 && c.smoke)
+    return fail(AERO_EUNSUPPORTED, "jets and vents with the smoke update inside the step: run the step without "
+                                   "smoke and apply their smoke sources after aero_ns3d_smoke");
   AeroNs3dPlan *p = new AeroNs3dPlan();
   p->cfg = c;
   p->esz = c.dtype == AERO_F64 ? 8 : 4;
@@ -873,6 +893,16 @@ int aero_ns3d_step_traced(const AeroNs3dPlan *plan, const AeroNs3dFields *f, con
   if (c.paint && (!g->paint_u || !g->paint_v || !g->paint_w || (c.smoke && !g->paint_c)))
     return fail(AERO_EINVAL, "missing paint masks");
   if (c.pid && (!f->pid_dt_prev || !f->pid_e1 || !f->pid_e2)) return fail(AERO_EINVAL, "missing PID state");
+  if (c.nport > 0) {
+    if (!g->ports) return fail(AERO_EINVAL, "missing port descriptors");
+    for (int q = 0; q < c.nport; ++q) {
+      const AeroNs3dPort &Q = g->ports[q];
+      if (window_empty(Q.window) || Q.window[0] < 0 || Q.window[1] > c.nz || Q.window[2] < 0 || Q.window[3] > c.ny ||
+          Q.window[4] < 0 || Q.window[5] > c.nx)
+        return fail(AERO_EINVAL, "port window empty or outside the domain");
+      if (!Q.f_u || !Q.f_v || !Q.f_w || !Q.m) return fail(AERO_EINVAL, "missing port weights");
+    }
+  }
   if (c.nfan > 0) {
     if (!g->fans) return fail(AERO_EINVAL, "missing fan descriptors");
     for (int q = 0; q < c.nfan; ++q) {

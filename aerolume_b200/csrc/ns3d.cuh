@@ -50,6 +50,19 @@ struct FanForce {
   const T *thrust, *swirl_amp;
 };
 
+// A jet or vent as the stage kernel sees it (physics.py:1033-1072).
+template <typename T>
+struct PortSource {
+  int win[6], vent;
+  T theta;
+  const T *f[3], *m;
+};
+
+template <typename T>
+struct PortParamsBlock {
+  PortSource<T> port[AERO_MAX_PORTS];
+};
+
 // The fans' begin-of-step update (physics.py:922-942): disc velocities and the PI thrust.
 template <typename T>
 struct FanBeginParams {
@@ -99,6 +112,9 @@ struct StageParams {
   const T *paint_u, *paint_v, *paint_w;  // painted solid fractions (whole grid) or NULL
   int nfan, fan_swirl;
   FanForce<T> fan[AERO_MAX_FANS];
+  int nport;
+  T port_leak;
+  PortSource<T> port[AERO_MAX_PORTS];
 };
 
 struct DtParams {
@@ -200,10 +216,13 @@ template <typename T>
 cudaError_t launch_copy_u(const T *, T *, int, int, int, int, unsigned long long *, cudaStream_t);
 template <typename T> cudaError_t launch_dt(const DtParams &, cudaStream_t);
 template <typename T> cudaError_t launch_fan_begin(const FanBeginParams<T> &, cudaStream_t);
+// div -= m on every port's cells (physics.py:1043-1047)
+template <typename T>
+cudaError_t launch_port_continuity(T *div, int nx, int ny, int nport, const PortSource<T> *ports, cudaStream_t s);
 template <typename T> cudaError_t launch_outlet_sum(const T *, const T *, int, int, double *, cudaStream_t);
 template <typename T>
 cudaError_t launch_outlet_corr(const double *, const double *, const double *, const double *, int, const T *, double,
-                               double, double, double, T *, cudaStream_t);
+                               double, double, double, double, T *, cudaStream_t);
 template <typename T>
 cudaError_t launch_divergence(const T *, const T *, const T *, int, int, int, int, int, int, T, T *, cudaStream_t);
 template <typename T> cudaError_t launch_correct(const CorrectParams<T> &, cudaStream_t);

@@ -219,7 +219,7 @@ __global__ void outlet_sum_kernel(const T *__restrict__ u, const T *__restrict__
 template <typename T>
 __global__ void outlet_corr_kernel(const double *p_out, const double *p_in, const double *p_u0, const double *p_inlet,
                                    int parts, const T *dt, double a, double bscale, double inv_h, double inv_rows,
-                                   T *corr) {
+                                   double source, T *corr) {
   double so = 0.0, si = 0.0, s0 = 0.0, sn = 0.0;
   for (int q = 0; q < parts; ++q) {
     so += p_out[q];
@@ -229,7 +229,27 @@ __global__ void outlet_corr_kernel(const double *p_out, const double *p_in, cons
   }
   const double bdt = (double)(T(bscale) * *dt);
   const double out = (1.0 - a) * so + a * s0 + bdt * inv_h * (si - so);
-  *corr = T((sn - out) * inv_rows);
+  T c = T((sn - out) * inv_rows);
+  // the ports' net mass flux leaves through the outlet too (core.py:294-296)
+  if (source != 0.0) c = c + T(source) * T(inv_rows);
+  *corr = c;
+}
+
+// div -= m on the cells of each port's window, one port after the other as the reference
+// applies them (physics.py:1043-1047); one block, the windows are small
+template <typename T>
+__global__ void port_continuity_kernel(T *div, int nx, int ny, int nport, PortParamsBlock<T> P) {
+  for (int q = 0; q < nport; ++q) {
+    const PortSource<T> &Q = P.port[q];
+    const int wz = Q.win[1] - Q.win[0], wy = Q.win[3] - Q.win[2], wx = Q.win[5] - Q.win[4];
+    const size_t n = (size_t)wz * wy * wx;
+    for (size_t e = threadIdx.x; e < n; e += blockDim.x) {
+      const int x = (int)(e % wx), y = (int)((e / wx) % wy), z = (int)(e / ((size_t)wx * wy));
+      T &d = div[((size_t)(Q.win[0] + z) * ny + (Q.win[2] + y)) * nx + (Q.win[4] + x)];
+      d = d - Q.m[e];
+    }
+    __syncthreads();
+  }
 }
 
 // --------------------------------------------------------------------------------------
@@ -555,9 +575,18 @@ cudaError_t launch_outlet_sum(const T *u, const T *u0, int nx, int rows, double 
 
 template <typename T>
 cudaError_t launch_outlet_corr(const double *p_out, const double *p_in, const double *p_u0, const double *p_inlet,
-                               int parts, const T *dt, double a, double b, double inv_h, double inv_rows, T *corr,
-                               cudaStream_t s) {
-  outlet_corr_kernel<T><<<1, 1, 0, s>>>(p_out, p_in, p_u0, p_inlet, parts, dt, a, b, inv_h, inv_rows, corr);
+                               int parts, const T *dt, double a, double b, double inv_h, double inv_rows,
+                               double source, T *corr, cudaStream_t s) {
+  outlet_corr_kernel<T><<<1, 1, 0, s>>>(p_out, p_in, p_u0, p_inlet, parts, dt, a, b, inv_h, inv_rows, source, corr);
+  return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_port_continuity(T *div, int nx, int ny, int nport, const PortSource<T> *ports, cudaStream_t s) {
+  if (nport <= 0) return cudaSuccess;
+  PortParamsBlock<T> P{};
+  for (int q = 0; q < nport; ++q) P.port[q] = ports[q];
+  port_continuity_kernel<T><<<1, 1024, 0, s>>>(div, nx, ny, nport, P);
   return cudaGetLastError();
 }
 
@@ -607,7 +636,8 @@ cudaError_t launch_psi_accumulate(const T *psi, T *pw, size_t n, T wgt, int mode
   template cudaError_t launch_copy_u<T>(const T *, T *, int, int, int, int, unsigned long long *, cudaStream_t);                                                \
   template cudaError_t launch_outlet_sum<T>(const T *, const T *, int, int, double *, cudaStream_t);                 \
   template cudaError_t launch_outlet_corr<T>(const double *, const double *, const double *, const double *, int,  \
-                                             const T *, double, double, double, double, T *, cudaStream_t);       \
+                                             const T *, double, double, double, double, double, T *, cudaStream_t); \
+  template cudaError_t launch_port_continuity<T>(T *, int, int, int, const PortSource<T> *, cudaStream_t);           \
   template cudaError_t launch_divergence<T>(const T *, const T *, const T *, int, int, int, int, int, int, T, T *,    \
                                             cudaStream_t);                                                           \
   template cudaError_t launch_correct<T>(const CorrectParams<T> &, cudaStream_t);                                   \

@@ -190,8 +190,10 @@ struct StageSmem {
 };
 
 // UPWIND, LES and THERMAL are the plan's advection scheme, LES switch and heat switch, fixed at
-// compile time so that each configuration's body is straight-line code
-template <typename T, bool UPWIND, bool LES, bool THERMAL>
+// compile time so that each configuration's body is straight-line code; PLACED adds the placed
+// physics that acts inside a stage (fans, jets and vents, painted solids), which the other instantiations
+// leave out entirely.
+template <typename T, bool UPWIND, bool LES, bool THERMAL, bool PLACED>
 __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) stage_kernel(const __grid_constant__ StageParams<T> P) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   StageSmem<T> &S = *reinterpret_cast<StageSmem<T> *>(smem_raw);
@@ -435,13 +437,13 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) stage_kernel(c
       }
 
       // ================= actuator discs (physics.py:944-952): + f T (+ s amp), fan by fan
-      for (int q = 0; q < P.nfan; ++q) {
+      for (int q = 0; q < (PLACED ? P.nfan : 0); ++q) {
         const FanForce<T> &F = P.fan[q];
         // this cell's u / v / w faces inside the fan's window (faces i..i1 / j..j1 / k..k1)
         const bool jc = j >= F.win[2] && j < F.win[3], ic = i >= F.win[4] && i < F.win[5];
-        const bool kc = k >= F.win[0] && k < F.win[1];
-        const bool in_u = kc && jc && i >= F.win[4] && i <= F.win[5];
-        const bool in_v = kc && ic && j >= F.win[2] && j <= F.win[3];
+        const bool kin = k >= F.win[0] && k < F.win[1];
+        const bool in_u = kin && jc && i >= F.win[4] && i <= F.win[5];
+        const bool in_v = kin && ic && j >= F.win[2] && j <= F.win[3];
         const bool in_w = jc && ic && k >= F.win[0] && k <= F.win[1];
         if (in_u || in_v || in_w) {
           const int fwy = F.win[3] - F.win[2], fwx = F.win[5] - F.win[4];
@@ -461,6 +463,26 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) stage_kernel(c
             lw = lw + F.f[2][e] * thrust;
             if (P.fan_swirl) lw = lw + F.s[2][e] * amp;
           }
+        }
+      }
+
+      // ================= jets and vents (physics.py:1033-1041): + f, or + f u for a vent =====
+      for (int q = 0; q < (PLACED ? P.nport : 0); ++q) {
+        const PortSource<T> &Q = P.port[q];
+        const bool jc = j >= Q.win[2] && j < Q.win[3], ic = i >= Q.win[4] && i < Q.win[5];
+        const bool kin = k >= Q.win[0] && k < Q.win[1];  // (kc names the plane)
+        const int fwy = Q.win[3] - Q.win[2], fwx = Q.win[5] - Q.win[4];
+        if (kin && jc && i >= Q.win[4] && i <= Q.win[5]) {
+          const T f = Q.f[0][((size_t)(k - Q.win[0]) * fwy + (j - Q.win[2])) * (fwx + 1) + (i - Q.win[4])];
+          lu = lu + (Q.vent ? f * VEL(0, 0, y, x) : f);
+        }
+        if (kin && ic && j >= Q.win[2] && j <= Q.win[3]) {
+          const T f = Q.f[1][((size_t)(k - Q.win[0]) * (fwy + 1) + (j - Q.win[2])) * fwx + (i - Q.win[4])];
+          lv = lv + (Q.vent ? f * VEL(1, 0, y, x) : f);
+        }
+        if (jc && ic && k >= Q.win[0] && k <= Q.win[1]) {
+          const T f = Q.f[2][((size_t)(k - Q.win[0]) * fwy + (j - Q.win[2])) * fwx + (i - Q.win[4])];
+          lw = lw + (Q.vent ? f * VEL(2, 0, y, x) : f);
         }
       }
 
@@ -508,7 +530,7 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) stage_kernel(c
       }
 
       // ================= painted solids, after the bodies (physics.py:1132-1137) =========
-      if (P.paint_u) {
+      if (PLACED && P.paint_u) {
         const T kpen = bdt / P.eta;
         uh = uh / (T(1) + kpen * P.paint_u[iu]);
         vh = vh / (T(1) + kpen * P.paint_v[iv]);
@@ -547,7 +569,7 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) stage_kernel(c
           const T lo = (upi - upo) * inv;
           uo = (a == T(0) ? upo : lerp_t<T>(upo, __ldg(P.u0 + io), a)) + lo * bdt;
           uo = uo + *P.outlet_corr;
-          if (P.paint_u) uo = uo / (T(1) + (bdt / P.eta) * P.paint_u[io]);
+          if (PLACED && P.paint_u) uo = uo / (T(1) + (bdt / P.eta) * P.paint_u[io]);
         }
         P.uh[io] = uo;
       }
@@ -589,9 +611,29 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) stage_kernel(c
         const T D = ((fxr - fxl) + (fyr - fyl) + (zth - zth_l)) * inv;
         const size_t ic = ((size_t)k * ny + j) * nx + i;
         T ch = (a == T(0) ? c : lerp_t<T>(c, t0v, a)) - bdt * D;
-        if ((wcol & 4) && k >= wk0 && k < wk1) {
+        const bool in_body = (wcol & 4) && k >= wk0 && k < wk1;
+        if (in_body) {
           wt = ((size_t)(k - wk0) * wyn + (j - wj0)) * wxn + (i - wi0);
           if (P.skin) ch = ch + (bdt * P.kappa) * P.skin[wt];
+        }
+        if (PLACED) {
+          // jets and vents (physics.py:1049-1072): a vent takes the local value out with its
+          // fluid, a jet brings its own; then an unbalanced closed box's uniform leak
+          for (int q = 0; q < P.nport; ++q) {
+            const PortSource<T> &Q = P.port[q];
+            if (k >= Q.win[0] && k < Q.win[1] && j >= Q.win[2] && j < Q.win[3] && i >= Q.win[4] && i < Q.win[5]) {
+              const T m = Q.m[((size_t)(k - Q.win[0]) * (Q.win[3] - Q.win[2]) + (j - Q.win[2])) *
+                                  (Q.win[5] - Q.win[4]) +
+                              (i - Q.win[4])];
+              if (Q.vent)
+                ch = ch + (bdt * m) * c;
+              else if (Q.theta != T(0))
+                ch = ch + (bdt * Q.theta) * m;
+            }
+          }
+          if (P.port_leak != T(0)) ch = ch - c * (bdt * P.port_leak);
+        }
+        if (in_body) {
           if (P.chi_t) {
             const T kt = bdt / P.eta_t;
             const T nw = (ch + kt * P.a_t[wt]) / (T(1) + kt * P.chi_t[wt]);
@@ -668,31 +710,36 @@ size_t stage_smem_bytes() {
   return sizeof(StageSmem<T>);
 }
 
-template <typename T, bool UPWIND, bool LES, bool THERMAL>
+template <typename T, bool UPWIND, bool LES, bool THERMAL, bool PLACED>
 cudaError_t launch_stage_cfg(const StageParams<T> &P, cudaStream_t s) {
   const size_t smem = sizeof(StageSmem<T>);
   static bool attr = false;
   if (!attr) {
-    cudaError_t e = cudaFuncSetAttribute(stage_kernel<T, UPWIND, LES, THERMAL>,
+    cudaError_t e = cudaFuncSetAttribute(stage_kernel<T, UPWIND, LES, THERMAL, PLACED>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     attr = true;
   }
   dim3 grid((P.nx + TX - 1) / TX, (P.ny + TY - 1) / TY, (P.nz + P.zc - 1) / P.zc);
-  stage_kernel<T, UPWIND, LES, THERMAL><<<grid, dim3(TX, TY), smem, s>>>(P);
+  stage_kernel<T, UPWIND, LES, THERMAL, PLACED><<<grid, dim3(TX, TY), smem, s>>>(P);
   return cudaGetLastError();
 }
 
 template <typename T>
 cudaError_t launch_stage(const StageParams<T> &P, cudaStream_t s) {
   using Launch = cudaError_t (*)(const StageParams<T> &, cudaStream_t);
-  // index: upwind x 4 + les x 2 + thermal
-  static const Launch table[8] = {
-      launch_stage_cfg<T, false, false, false>, launch_stage_cfg<T, false, false, true>,
-      launch_stage_cfg<T, false, true, false>,  launch_stage_cfg<T, false, true, true>,
-      launch_stage_cfg<T, true, false, false>,  launch_stage_cfg<T, true, false, true>,
-      launch_stage_cfg<T, true, true, false>,   launch_stage_cfg<T, true, true, true>};
-  const int idx = (P.upwind ? 4 : 0) + (P.les != AERO_LES_NONE ? 2 : 0) + (P.thermal ? 1 : 0);
+  // index: placed x 8 + upwind x 4 + les x 2 + thermal
+  static const Launch table[16] = {
+      launch_stage_cfg<T, false, false, false, false>, launch_stage_cfg<T, false, false, true, false>,
+      launch_stage_cfg<T, false, true, false, false>,  launch_stage_cfg<T, false, true, true, false>,
+      launch_stage_cfg<T, true, false, false, false>,  launch_stage_cfg<T, true, false, true, false>,
+      launch_stage_cfg<T, true, true, false, false>,   launch_stage_cfg<T, true, true, true, false>,
+      launch_stage_cfg<T, false, false, false, true>,  launch_stage_cfg<T, false, false, true, true>,
+      launch_stage_cfg<T, false, true, false, true>,   launch_stage_cfg<T, false, true, true, true>,
+      launch_stage_cfg<T, true, false, false, true>,   launch_stage_cfg<T, true, false, true, true>,
+      launch_stage_cfg<T, true, true, false, true>,    launch_stage_cfg<T, true, true, true, true>};
+  const bool placed = P.paint_u != nullptr || P.nfan > 0 || P.nport > 0;
+  const int idx = (placed ? 8 : 0) + (P.upwind ? 4 : 0) + (P.les != AERO_LES_NONE ? 2 : 0) + (P.thermal ? 1 : 0);
   return table[idx](P, s);
 }
 

@@ -12,9 +12,9 @@ these instead (solver.py:161-166 ``load_kernels``; solver.py:583-595 ``fast_step
   tensors, as fused.py:371 / 378-502 do.
 * ``fast_dye`` is the MUSCL advection of one smoke channel (fused.py:553-565).
 
-Placed physics that the B200 step does not implement (ports, diagnostics rows) raises instead
-of being computed differently; heat transfer, fans, painted solids and the PID step
-controller run in the step.
+Placed physics that the B200 step does not implement (volumetric heat sources, diagnostics
+rows) raises instead of being computed differently; heat transfer, fans, jets and vents,
+painted solids and the PID step controller run in the step.
 """
 from __future__ import annotations
 
@@ -36,16 +36,13 @@ class B200Kernels:
         paint = getattr(phys, "paint", None) if phys is not None else None
         pid = getattr(phys, "pid", None) if phys is not None else None
         fans = getattr(phys, "fans", None) if phys is not None else None
-        key = ("step", id(geom), id(ops), id(thermal), id(paint), id(pid), id(fans))
+        ports = getattr(phys, "ports", None) if phys is not None else None
+        key = ("step", id(geom), id(ops), id(thermal), id(paint), id(pid), id(fans), id(ports))
         entry = self._plans.get(key)
         if entry is None:
-            if phys is not None:
-                for name in ("ports",):
-                    if getattr(phys, name, None) is not None:
-                        raise RuntimeError(f"placed physics {name!r} is not in the B200 step")
-            plan = Ns3dPlan(ops, geom, thermal, None, device=self.device, paint=paint, pid=pid, fans=fans,
+            plan = Ns3dPlan(ops, geom, thermal, None, device=self.device, paint=paint, pid=pid, fans=fans, ports=ports,
                             u_floor=float(getattr(phys, "u_floor", 0.0) or 0.0) if phys is not None else 0.0)
-            entry = (plan, geom, ops, thermal, paint, pid, fans)   # the objects stay alive with their plan
+            entry = (plan, geom, ops, thermal, paint, pid, fans, ports)   # the objects stay alive with their plan
             self._plans[key] = entry
         return entry[0]
 
@@ -86,8 +83,8 @@ def fast_step(state, geom, ops, kern):
 
 
 def fast_step_phys(state, geom, ops, kern, dt=None, *, phys=None, theta=None, diag=False, theta_kernels=True):
-    """One step with the placed physics the B200 step implements (heat transfer, fans, painted
-    solids, the PID step controller)."""
+    """One step with the placed physics the B200 step implements (heat transfer, fans, jets and
+    vents, painted solids, the PID step controller)."""
     if diag:
         raise RuntimeError("diagnostics rows are not produced by the B200 step")
     plan = kern.plan_for(geom, ops, phys)

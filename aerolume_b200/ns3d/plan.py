@@ -16,7 +16,7 @@ import numpy as np
 import torch
 
 from .. import _lib
-from .._lib import ADV, F32, F64, GHOST, LES, MAX_BODIES, MAX_FANS, THETA_SIDE, check
+from .._lib import ADV, F32, F64, GHOST, LES, MAX_BODIES, MAX_FANS, MAX_PORTS, THETA_SIDE, check
 
 
 def _f(x) -> float:
@@ -42,12 +42,12 @@ class Ns3dPlan:
     ``smoke`` turns the smoke update on inside :meth:`step`.  ``paint`` (``chi_u / chi_v /
     chi_w / chi_c`` tensors, a ``PaintLayer``), ``pid`` (``target`` and the ``dt_prev / e1 /
     e2`` state tensors, a ``PidDt``), ``u_floor`` (the sources' speed scale) and ``fans`` (a
-    ``FanSet``: actuator discs with their PI thrust state) are the placed physics of
-    physics.py:831-1262 the step runs.
+    ``FanSet``: actuator discs with their PI thrust state) and ``ports`` (a ``PortSet``: jets
+    and vents) are the placed physics of physics.py:831-1262 the step runs.
     """
 
     def __init__(self, ops, geom, thermal=None, dye_src=None, *, smoke: bool = False, device=None, paint=None,
-                 pid=None, u_floor: float = 0.0, fans=None):
+                 pid=None, u_floor: float = 0.0, fans=None, ports=None):
         self.device = torch.device(device) if device is not None else torch.device("cuda")
         if self.device.type != "cuda":
             raise RuntimeError("the B200 step runs on a CUDA device only (no CPU fallback)")
@@ -152,6 +152,9 @@ class Ns3dPlan:
         self.fans = fans if fans is not None and len(fans) else None
         if self.fans is not None:
             self._fan_config(cfg, g, self.fans, up)
+        self.ports = ports if ports is not None and len(ports) else None
+        if self.ports is not None:
+            self._port_config(cfg, g, self.ports, up)
         self.cfg = cfg
         self.geom_c = g
         handle = C.c_void_p()
@@ -246,6 +249,38 @@ class Ns3dPlan:
                 setattr(d, name, t.data_ptr() + q * t.element_size())
         self._fan_arr = arr
         g.fans = C.cast(arr, C.c_void_p)
+
+    def _port_config(self, cfg, g, ports, up):
+        n = len(ports.items)
+        if n > MAX_PORTS:
+            raise RuntimeError(f"the B200 step supports at most {MAX_PORTS} jets and vents")
+        if self.smoke:
+            raise RuntimeError("jets and vents: build the plan without smoke and apply their smoke sources after "
+                               "smoke_step (as FlowSolver3D does)")
+        mf = ports.mass_flux
+        cfg.nport = n
+        cfg.port_source = float(mf.item() if torch.is_tensor(mf) else mf)
+        cfg.port_leak = float(getattr(ports, "leak", 0.0) or 0.0)
+        arr = (_lib.Ns3dPort * n)()
+        for q, it in enumerate(ports.items):
+            d = arr[q]
+            win = tuple(int(x) for x in it["win"])
+            if _window_empty(win):
+                raise RuntimeError("a port window is empty")
+            for e in range(6):
+                d.window[e] = win[e]
+            k0, k1, j0, j1, i0, i1 = win
+            d.vent = int(it["kind"] == "vent")
+            d.theta = float(it.get("theta", 0.0) or 0.0)
+            shapes = {"fu": ("f_u", (k1 - k0, j1 - j0, i1 - i0 + 1)), "fv": ("f_v", (k1 - k0, j1 - j0 + 1, i1 - i0)),
+                      "fw": ("f_w", (k1 - k0 + 1, j1 - j0, i1 - i0)), "m": ("m", (k1 - k0, j1 - j0, i1 - i0))}
+            for name, (field, shape) in shapes.items():
+                t = up(it[name])
+                if tuple(t.shape) != shape:
+                    raise RuntimeError(f"port {q} weights {name} have shape {tuple(t.shape)}, expected {shape}")
+                setattr(d, field, t.data_ptr())
+        self._port_arr = arr
+        g.ports = C.cast(arr, C.c_void_p)
 
     def _stream(self):
         return C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)

@@ -9,9 +9,9 @@ accepts either these containers or the reference's own objects:
   ``aerolume.solvers.ns3d.physics.ThermalOps`` / ``ThermalGeometry`` the step reads
   (physics.py:314-461, 494-560)
 * :class:`DyeSources` -- ``aerolume.solvers.ns3d.dye.DyeSources`` (dye.py:140-151)
-* :class:`PaintLayer3D` / :class:`PidState3D` / :class:`FanSet3D` -- the parts of
-  ``aerolume.solvers.ns3d.physics.PaintLayer`` / ``PidDt`` / ``FanSet`` the step reads and
-  updates (physics.py:831-979, 1074-1181)
+* :class:`PaintLayer3D` / :class:`PidState3D` / :class:`FanSet3D` / :class:`PortSet3D` -- the
+  parts of ``aerolume.solvers.ns3d.physics.PaintLayer`` / ``PidDt`` / ``FanSet`` / ``PortSet``
+  the step reads and updates (physics.py:831-1181)
 * :class:`State3D`, :class:`StepOut3D` -- core.py:111-119, 745-750
 
 Arrays may be numpy arrays or torch tensors; the step uploads what is not already on the
@@ -191,6 +191,22 @@ class FanSet3D:
     ud: Any
     e_prev: Any
     swirl_amp: Any
+
+    def __len__(self) -> int:
+        return len(self.items)
+
+
+@dataclass
+class PortSet3D:
+    """Jets and vents (physics.py:981-1072), the attributes the step reads.
+
+    ``items[q]``: ``win`` (cell window), ``kind`` ("jet" / "vent"), ``m`` (mass source on the
+    window's cells), ``fu / fv / fw`` (momentum weights on its faces; a vent's are multiplied
+    by the local velocity), ``theta`` (a jet's temperature).  ``mass_flux``: the net source in
+    outlet-face units; ``leak``: the uniform scalar leak of an unbalanced closed box."""
+    items: list
+    mass_flux: Any
+    leak: float = 0.0
 
     def __len__(self) -> int:
         return len(self.items)

@@ -45,6 +45,7 @@ extern "C" {
 
 #define AERO_MAX_BODIES 8
 #define AERO_MAX_FANS 4
+#define AERO_MAX_PORTS 4
 
 enum { AERO_F32 = 0, AERO_F64 = 1 };
 enum { AERO_ADV_UPWIND3 = 0, AERO_ADV_CENTRAL = 1 };
@@ -108,6 +109,9 @@ typedef struct AeroNs3dConfig {
   int32_t paint;                /* painted solids (geom paint_*; physics.py:1074-1141)      */
   int32_t nfan;                 /* actuator discs (geom fans; physics.py:831-979)           */
   int32_t fan_swirl;            /* any fan with swirl                                       */
+  int32_t nport;                /* jets and vents (geom ports; physics.py:981-1072)         */
+  double port_source;           /* their net mass flux in outlet-face units (h sum m)       */
+  double port_leak;             /* uniform scalar leak of an unbalanced closed box (Q / V)  */
 } AeroNs3dConfig;
 
 /* One actuator disc (ns3d/physics.py:831-979): its cell window, the force, swirl and
@@ -125,6 +129,18 @@ typedef struct AeroNs3dFan {
   void *thrust, *ud, *e_prev, *swirl_amp;
 } AeroNs3dFan;
 
+/* One jet or vent (ns3d/physics.py:981-1072): a mass source m = Q phi_c on the cells of its
+ * window (taken out of the projection's right-hand side), momentum on the window's faces
+ * (a jet: f = Q speed n_g phi_g; a vent: f = Q phi_g times the local velocity), and the
+ * temperature it carries (a jet's theta; a vent takes the local value out). */
+typedef struct AeroNs3dPort {
+  int32_t window[6];            /* k0, k1, j0, j1, i0, i1                                  */
+  int32_t vent;                 /* 1: vent, 0: jet                                         */
+  double theta;                 /* a jet's temperature                                     */
+  const void *f_u, *f_v, *f_w;  /* face weights over the window (body-mask shapes)         */
+  const void *m;                /* cell weights over the window                            */
+} AeroNs3dPort;
+
 /* Window masks and constant inputs (device pointers of the plan's dtype; NULL when absent).
  * Shapes are those of ns3d/geometry.py:275-303 and ns3d/physics.py:314-461. */
 typedef struct AeroNs3dGeom {
@@ -140,6 +156,7 @@ typedef struct AeroNs3dGeom {
    * so strokes between steps take effect) */
   const void *paint_u, *paint_v, *paint_w, *paint_c;
   const AeroNs3dFan *fans;      /* host array of cfg.nfan descriptors, read at every step  */
+  const AeroNs3dPort *ports;    /* host array of cfg.nport descriptors                     */
 } AeroNs3dGeom;
 
 /* State in and out (device pointers of the plan's dtype).  u may alias u0, v v0, w w0 and

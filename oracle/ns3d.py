@@ -19,6 +19,7 @@ the sm_100a kernels implement (Aerolume ``src/aerolume/solvers/ns3d``):
                          physics.py:1144-1181)
 * ``PaintLayer``         physics.py:1074-1141 painted solids, penalised after the bodies
 * ``FanSet``             physics.py:831-979 actuator discs: disc velocity, PI thrust, forces
+* ``PortSet``            physics.py:981-1072 jets and vents: forces, mass sources, theta sources
 * smoke                  dye.py:232-312    MUSCL / van Leer advection, solids, nozzles
 
 Parity is pinned: ``tests/test_oracle_golden.py`` checks this module against golden
@@ -112,8 +113,9 @@ def pad_velocity(u, v, w, ops):
     return pad3(u, g["u"]), pad3(v, g["v"]), pad3(w, g["w"])
 
 
-def inlet_outlet(u, ops):
-    """Inlet profile and outlet mass balance (core.py:281-297)."""
+def inlet_outlet(u, ops, source=None):
+    """Inlet profile and outlet mass balance (core.py:281-297); ``source`` is the ports' net
+    mass flux in outlet-face units (or None)."""
     u = u.copy()
     if ops.closed:
         u[..., 0] = 0.0
@@ -121,6 +123,8 @@ def inlet_outlet(u, ops):
         return u
     T = u.dtype.type
     corr = (ops.u_inlet.sum(dtype=u.dtype) - u[..., -1].sum(dtype=u.dtype)) * T(1.0 / (ops.nz * ops.ny))
+    if source is not None:
+        corr = T(corr + T(T(source) * T(1.0 / (ops.nz * ops.ny))))
     u[..., -1] = u[..., -1] + corr
     u[..., 0] = ops.u_inlet
     return u
@@ -639,8 +643,9 @@ def theta_fluxes(th, c, u, v, w, ops, nut):
     return out
 
 
-def theta_stage(th, c_prev, c0, up, vp, wp, a, bdt, wgt, ops, nut, heat_acc):
-    """One RK stage of theta with the body penalisation (physics.py:678-708)."""
+def theta_stage(th, c_prev, c0, up, vp, wp, a, bdt, wgt, ops, nut, heat_acc, ports=None):
+    """One RK stage of theta with the ports' sources and the body penalisation
+    (physics.py:678-708)."""
     T = c_prev.dtype.type
     fx, fy, fz = theta_fluxes(th, c_prev, up, vp, wp, ops, nut)
     D = ((fx[..., 1:] - fx[..., :-1]) + (fy[:, 1:] - fy[:, :-1]) + (fz[1:] - fz[:-1])) * T(1.0 / ops.h)
@@ -650,6 +655,8 @@ def theta_stage(th, c_prev, c0, up, vp, wp, a, bdt, wgt, ops, nut, heat_acc):
     g = th.geom
     if g.skin is not None:
         ch[_face_slices(g.window, "c")] += bk * g.skin
+    if ports is not None:
+        ch = port_scalar_sources(ports, ch, c_prev, bdt)
     if g.chi_t is not None:
         sl = _face_slices(g.window, "c")
         win = ch[sl]
@@ -763,6 +770,51 @@ def fan_begin_step(fans, u0, v0, w0, dt):
         fans.swirl_amp = (fans.swirl * ud) * np.abs(ud)
 
 
+class PortState:
+    """PortSet (physics.py:981-1072) in numpy: ``items[q]`` with ``win``, ``kind`` ("jet" /
+    "vent"), ``m`` (cells), ``f`` (the u, v, w face weights) and ``theta``; the net mass flux
+    in outlet-face units and the uniform leak of an unbalanced closed box."""
+
+    def __init__(self, items, mass_flux, leak):
+        self.items, self.mass_flux, self.leak = items, mass_flux, float(leak)
+
+
+def port_forces(ports, lu, lv, lw, u, v, w):
+    """PortSet.add_forces (physics.py:1033-1041): + f (jet) or + f u (vent)."""
+    out = [lu.copy(), lv.copy(), lw.copy()]
+    for it in ports.items:
+        for c, (g, vel) in enumerate(zip("uvw", (u, v, w))):
+            sl = _face_slices(it["win"], g)
+            out[c][sl] = out[c][sl] + (it["f"][c] if it["kind"] == "jet" else it["f"][c] * vel[sl])
+    return tuple(out)
+
+
+def port_continuity(ports, div):
+    """PortSet.continuity (physics.py:1043-1047): div - m on each port's cells."""
+    div = div.copy()
+    for it in ports.items:
+        sl = _face_slices(it["win"], "c")
+        div[sl] = div[sl] - it["m"]
+    return div
+
+
+def port_scalar_sources(ports, ch, c_prev, bdt):
+    """PortSet.scalar_sources for theta (physics.py:1049-1072)."""
+    T = ch.dtype.type
+    ch = ch.copy()
+    for it in ports.items:
+        sl = _face_slices(it["win"], "c")
+        if it["kind"] == "vent":
+            ch[sl] = ch[sl] + (bdt * it["m"]) * c_prev[sl]
+            continue
+        val = float(it.get("theta", 0.0) or 0.0)
+        if val != 0.0:
+            ch[sl] = ch[sl] + T(bdt * T(val)) * it["m"]
+    if ports.leak:
+        ch = ch - c_prev * T(bdt * T(ports.leak))
+    return ch
+
+
 def fan_forces(fans, lu, lv, lw):
     """FanSet.add_forces (physics.py:944-952): + f T (+ s amp) on each fan's faces."""
     out = [lu.copy(), lv.copy(), lw.copy()]
@@ -811,10 +863,10 @@ class StepResult:
 
 
 def step3d_phys(u0, v0, w0, t, geom, ops, poisson, *, th=None, theta=None, dt=None, trace=False, paint=None,
-                pid=None, u_floor=0.0, fans=None):
+                pid=None, u_floor=0.0, fans=None, ports=None):
     """One SSP-RK3 step (core.py:765-883) with heat transfer, buoyancy, painted solids
     (``paint``: (chi_u, chi_v, chi_w) on the whole grid), the PID / speed-floor dt rule and
-    fans (a :class:`FanState`, updated in place); no ports."""
+    fans (a :class:`FanState`, updated in place) and jets / vents (a :class:`PortState`)."""
     T = u0.dtype.type
     up, vp, wp = u0, v0, w0
     acc = None
@@ -824,7 +876,14 @@ def step3d_phys(u0, v0, w0, t, geom, ops, poisson, *, th=None, theta=None, dt=No
     heat_acc = np.zeros(geom.nbody if not geom.empty else max(geom.nbody, 0), dtype=np.float64)
     stages = []
     nut_stage1 = None
-    placed = th is not None or pid is not None or u_floor > 0.0 or fans is not None
+    placed = th is not None or pid is not None or u_floor > 0.0 or fans is not None or ports is not None
+
+    def sources(lu_, lv_, lw_):  # Physics3D.momentum_sources: fans, then jets and vents
+        if fans is not None:
+            lu_, lv_, lw_ = fan_forces(fans, lu_, lv_, lw_)
+        if ports is not None:
+            lu_, lv_, lw_ = port_forces(ports, lu_, lv_, lw_, up, vp, wp)
+        return lu_, lv_, lw_
     for s, ((a, b), wgt) in enumerate(zip(SSP_RK3, FORCE_WEIGHTS)):
         if s == 0:
             # the dt rule and the fans' controllers act before any source is evaluated
@@ -840,9 +899,9 @@ def step3d_phys(u0, v0, w0, t, geom, ops, poisson, *, th=None, theta=None, dt=No
             dt = T(dt)
             if fans is not None:
                 fan_begin_step(fans, u0, v0, w0, dt)
-        if s > 0 or fans is not None:
+        if s > 0 or fans is not None or ports is not None:
             lu, lv, lw, nut, nut_max = momentum_rhs3d(
-                up, vp, wp, geom, ops, sources=None if fans is None else (lambda a, b_, c: fan_forces(fans, a, b_, c)))
+                up, vp, wp, geom, ops, sources=None if fans is None and ports is None else sources)
         bdt = T(dt * T(b))
         if a == 0.0:
             uh, vh, wh = up + lu * bdt, vp + lv * bdt, wp + lw * bdt
@@ -851,7 +910,7 @@ def step3d_phys(u0, v0, w0, t, geom, ops, poisson, *, th=None, theta=None, dt=No
             vh = lerp(vp, v0, a) + lv * bdt
             wh = lerp(wp, w0, a) + lw * bdt
         if not ops.periodic_axes[0]:
-            uh = inlet_outlet(uh, ops)
+            uh = inlet_outlet(uh, ops, None if ports is None else ports.mass_flux)
         if not geom.empty:
             uh, vh, wh, du, dv, dw = penalise3d(uh, vh, wh, geom, ops, bdt)
             wg = T(wgt)
@@ -870,8 +929,10 @@ def step3d_phys(u0, v0, w0, t, geom, ops, poisson, *, th=None, theta=None, dt=No
                 acc[2] = acc[2] + share
         if thermal:
             tp_new = theta_stage(th, tp, t0, up, vp, wp, a, bdt, wgt, ops,
-                                 nut if ops.turbulence != "none" else None, heat_acc)
+                                 nut if ops.turbulence != "none" else None, heat_acc, ports)
         div = divergence3d(uh, vh, wh, ops.h)
+        if ports is not None:
+            div = port_continuity(ports, div)
         psi = poisson.solve(div)
         gx, gy, gz = pressure_gradient(psi, ops)
         if trace:

@@ -69,6 +69,19 @@ def fan_items(meta, arr):
     return out
 
 
+def port_items(meta, arr):
+    """Per-port windows, kinds, temperatures and weights of a golden case (numpy, the case
+    dtype): [{"win", "kind", "theta", "m", "fu", "fv", "fw"}]."""
+    dt = np.float64 if meta["dtype"] == "float64" else np.float32
+    out = []
+    for q, it in enumerate(meta["ports"]["items"]):
+        d = {"win": tuple(it["win"]), "kind": it["kind"], "theta": it["theta"], "m": arr[f"port{q}_m"].astype(dt)}
+        for g in "uvw":
+            d["f" + g] = arr[f"port{q}_f{g}"].astype(dt)
+        out.append(d)
+    return out
+
+
 CASES_2D = sorted(p.stem[len("ns2d_"):] for p in GOLDEN.glob("ns2d_*.npz"))
 
 

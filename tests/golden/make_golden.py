@@ -31,7 +31,8 @@ REF = Path(os.environ.get("AEROLUME_REF", "/root/reference"))
 sys.path.insert(0, str(REF / "src"))
 
 from aerolume.solvers.ns3d import core  # noqa: E402
-from aerolume.solvers.ns3d.config import DyeRake, Fan3D, ImmersedMesh, SolverConfig3D, ThermalConfig3D  # noqa: E402
+from aerolume.solvers.ns3d.config import (DyeRake, Fan3D, ImmersedMesh, Port3D, SolverConfig3D,  # noqa: E402
+                                          ThermalConfig3D)
 from aerolume.solvers.ns3d.dye import advect_dye3d, apply_solids_and_sources, build_dye_sources  # noqa: E402
 from aerolume.solvers.ns3d.geometry import body_window3d, build_geometry3d  # noqa: E402
 from aerolume.solvers.ns3d.physics import PaintLayer, Physics3D  # noqa: E402
@@ -126,6 +127,15 @@ def extract(ops, geom, phys, src):
             for kind in "fsm":
                 for g in "uvw":
                     arrays[f"fan{q}_{kind}{g}"] = _np(it[kind + g])
+    if phys is not None and phys.ports is not None:
+        ps = phys.ports
+        meta["ports"] = {"mass_flux": float(ps.mass_flux), "leak": float(ps.leak),
+                         "items": [{"win": list(it["win"]), "kind": it["kind"], "theta": float(it["theta"])}
+                                   for it in ps.items]}
+        for q, it in enumerate(ps.items):
+            arrays[f"port{q}_m"] = _np(it["m"])
+            for g in "uvw":
+                arrays[f"port{q}_f{g}"] = _np(it["f" + g])
     return meta, arrays
 
 
@@ -274,6 +284,21 @@ def main():
                       fans=[Fan3D(center=(1.2, 0.8, 0.8), direction=(0.0, 0.0, 1.0), diameter=0.8,
                                   mode="pressure_jump", value=0.3, name="up")])
     run_case("closed_fan_pressure_f64", closed_fan, dtype="float64", steps=3, seed=11, amp=0.05)
+    # jets and vents: a warm jet up from the floor and a vent downstream in the heated tunnel,
+    # and an unbalanced jet in a closed heated box (its uniform leak carries heat out)
+    ports = [Port3D(kind="jet", center=(1.0, 1.0, 0.35), direction=(0.0, 0.0, 1.0), diameter=0.6, speed=0.8,
+                    theta=0.7, name="jet"),
+             Port3D(kind="vent", center=(3.0, 0.9, 0.9), diameter=0.5, speed=0.5, name="vent")]
+    port_case = dict(grid, re=800.0, ports=ports, turbulence="wale",
+                     thermal=ThermalConfig3D(prandtl=0.71, richardson=0.2))
+    run_case("ports_heat_f64", port_case, dtype="float64", steps=3, seed=12, amp=0.1)
+    run_case("ports_heat_f32", port_case, dtype="float32", steps=3, seed=12, amp=0.1)
+    closed_jet = dict(grid, nx=14, ny=10, nz=10, re=300.0, domain="closed", bc_x="noslip", bc_y="noslip",
+                      bc_zmin="noslip", bc_zmax="noslip",
+                      ports=[Port3D(kind="jet", center=(1.1, 0.8, 0.5), direction=(0.6, 0.0, 0.8), diameter=0.5,
+                                    speed=0.6, theta=1.0, name="inflow")],
+                      thermal=ThermalConfig3D(prandtl=0.71, richardson=0.5))
+    run_case("closed_jet_leak_f64", closed_jet, dtype="float64", steps=3, seed=13, amp=0.05)
     if not names or "poisson" in names:
         poisson_cases()
     for p in sorted(HERE.glob("*.npz")):

@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 import torch
 
-from _golden import CASES_3D, GOLDEN, fan_items, load_case
+from _golden import CASES_3D, GOLDEN, fan_items, load_case, port_items
 from oracle import ns3d as O
 
 pytestmark = pytest.mark.gpu
@@ -28,7 +28,7 @@ def _dev(x, dt):
 
 def _plan_and_inputs(name):
     from aerolume_b200.ns3d.plan import Ns3dPlan
-    from aerolume_b200.ns3d.types import FanSet3D, PaintLayer3D, PidState3D
+    from aerolume_b200.ns3d.types import FanSet3D, PaintLayer3D, PidState3D, PortSet3D
     meta, ops, geom, th, src, arr = load_case(name)
     dt = torch.float64 if meta["dtype"] == "float64" else torch.float32
     paint = PaintLayer3D(*(_dev(arr["paint_" + g], dt) for g in "uvwc")) if "paint_u" in arr else None
@@ -43,12 +43,19 @@ def _plan_and_inputs(name):
         fans = FanSet3D(items, *(fm[k] for k in ("target", "kp", "ki", "tmax", "velocity_mode", "swirl")),
                         fm["any_swirl"], torch.tensor(fm["thrust"], device="cuda", dtype=dt),
                         *(torch.zeros(n, device="cuda", dtype=dt) for _ in range(3)))
-    plan = Ns3dPlan(ops, geom, th, src, smoke=True, paint=paint, pid=pid, u_floor=meta.get("u_floor", 0.0),
-                    fans=fans)
+    ports = None
+    if "ports" in meta:
+        ports = PortSet3D([{k: (_dev(x, dt) if isinstance(x, np.ndarray) else x) for k, x in it.items()}
+                           for it in port_items(meta, arr)], meta["ports"]["mass_flux"], meta["ports"]["leak"])
+    # with jets and vents the caller applies their smoke sources itself: no smoke in the step
+    plan = Ns3dPlan(ops, geom, th, src, smoke=ports is None, paint=paint, pid=pid, u_floor=meta.get("u_floor", 0.0),
+                    fans=fans, ports=ports)
     ins = {"u0": _dev(arr["in_u"], dt), "v0": _dev(arr["in_v"], dt), "w0": _dev(arr["in_w"], dt),
            "t0": _dev(arr["in_t"], dt), "dye0": _dev(arr["in_dye"], dt)}
     if th is not None:
         ins["theta0"] = _dev(arr["in_theta"], dt)
+    if not plan.smoke:
+        ins["dye0"] = None
     return meta, plan, ins, arr
 
 
@@ -66,7 +73,7 @@ def test_one_step_matches_reference(name):
     out = plan.step(ins["u0"], ins["v0"], ins["w0"], ins["t0"], theta0=ins.get("theta0"), dye0=ins["dye0"])
     torch.cuda.synchronize()
     tol = TOL[meta["dtype"]]
-    for f in ("u", "v", "w", "p", "dye"):
+    for f in ("u", "v", "w", "p") + (("dye",) if plan.smoke else ()):
         assert _rel(out[f], arr["out1_" + f]) < tol, (f, _rel(out[f], arr["out1_" + f]))
     assert _rel(out["dt"], arr["out1_dt"]) < tol
     assert _rel(out["t"], arr["out1_t"]) < tol
@@ -89,7 +96,8 @@ def test_one_step_matches_reference(name):
     assert plan.status() == 0
 
 
-@pytest.mark.parametrize("name", [n for n in CASES_3D if "tunnel" in n or "pid" in n or "fan" in n])
+@pytest.mark.parametrize("name", [n for n in CASES_3D if "tunnel" in n or "pid" in n or "fan" in n or "port" in n
+                                  or "jet" in n])
 def test_three_steps_in_place_match_reference(name):
     """Three steps updating the state in place (u, v, w, theta outputs alias the inputs)."""
     meta, plan, ins, arr = _plan_and_inputs(name)
@@ -103,7 +111,7 @@ def test_three_steps_in_place_match_reference(name):
             out["theta"] = theta
         plan.step(u, v, w, t, theta0=theta, dye0=dye, out=out)
         t = out["t"].clone()
-        dye = out["dye"].clone()
+        dye = out["dye"].clone() if plan.smoke else None
         if "pid" in meta:
             pids.append(_pid_state(plan))
         if "fans" in meta:
@@ -111,7 +119,7 @@ def test_three_steps_in_place_match_reference(name):
     torch.cuda.synchronize()
     tol = 10 * TOL[meta["dtype"]]
     for f, x in (("u", u), ("v", v), ("w", w), ("p", out["p"]), ("theta", theta), ("dye", dye)):
-        if "outN_" + f in arr:
+        if "outN_" + f in arr and x is not None:
             assert _rel(x, arr["outN_" + f]) < tol, (f, _rel(x, arr["outN_" + f]))
     for k, got in enumerate(pids):  # the PID state after every step
         ref = arr[f"pid{k + 1}"]

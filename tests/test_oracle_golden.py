@@ -4,7 +4,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from _golden import CASES_3D, GOLDEN, fan_items, load_case
+from _golden import CASES_3D, GOLDEN, fan_items, load_case, port_items
 from oracle import ns3d as O
 
 
@@ -24,10 +24,14 @@ def _run(name, steps=1):
                   "m": tuple(it["m" + g] for g in "uvw")} for it in fan_items(meta, arr)]
         fans = O.FanState(items, fm["target"], fm["kp"], fm["ki"], fm["tmax"], fm["velocity_mode"], fm["swirl"],
                           fm["any_swirl"], fm["thrust"], dt)
+    ports = None
+    if "ports" in meta:
+        items = [dict(it, f=tuple(it["f" + g] for g in "uvw")) for it in port_items(meta, arr)]
+        ports = O.PortState(items, meta["ports"]["mass_flux"], meta["ports"]["leak"])
     outs = []
     for _ in range(steps):
         r = O.step3d_phys(u, v, w, t, geom, ops, ps, th=th, theta=theta, paint=paint, pid=pid,
-                          u_floor=meta.get("u_floor", 0.0), fans=fans)
+                          u_floor=meta.get("u_floor", 0.0), fans=fans, ports=ports)
         c = O.advect_dye3d(c, r.u, r.v, r.w, r.dt, ops)
         c = O.apply_solids_and_sources(c, r.t, geom, src)
         if "paint_c" in arr:                         # painted cells hold no smoke
@@ -63,7 +67,8 @@ def test_oracle_matches_reference_one_step(name):
     assert _rel(r.dye, arr["out1_dye"]) < tol
 
 
-@pytest.mark.parametrize("name", [n for n in CASES_3D if "tunnel" in n or "pid" in n or "fan" in n])
+@pytest.mark.parametrize("name", [n for n in CASES_3D if "tunnel" in n or "pid" in n or "fan" in n or "port" in n
+                                  or "jet" in n])
 def test_oracle_matches_reference_three_steps(name):
     meta, arr, outs = _run(name, steps=3)
     r = outs[-1]
@@ -120,3 +125,16 @@ def test_fan_fixtures_exercise_the_fans():
     thrust = arr["fans3"][0]
     assert abs(thrust[0] - meta["fans"]["thrust"][0]) > 1e-3 * abs(meta["fans"]["thrust"][0])  # regulated
     assert thrust[1] == meta["fans"]["thrust"][1]                                             # fixed
+
+
+def test_port_fixtures_exercise_the_ports():
+    """Leaving the jets and vents out moves the step far outside the tolerances, and the
+    closed box's jet is unbalanced (its leak term is live)."""
+    meta, ops, geom, th, src, arr = load_case("ports_heat_f64")
+    ps = O.PoissonSolver3D(ops.nx, ops.ny, ops.nz, ops.h, ops.periodic_axes, np.float64)
+    r = O.step3d_phys(arr["in_u"], arr["in_v"], arr["in_w"], np.float64(arr["in_t"]), geom, ops, ps, th=th,
+                      theta=arr["in_theta"], u_floor=meta["u_floor"])
+    assert _rel(r.u, arr["out1_u"]) > 1e-3
+    assert _rel(r.theta, arr["out1_theta"]) > 1e-4
+    meta, *_ = load_case("closed_jet_leak_f64")
+    assert meta["ports"]["leak"] > 0
