@@ -75,3 +75,50 @@ def test_step_full_matches_reference():
     for k in ("u", "v", "p", "dye", "t", "dt"):
         assert _rel(getattr(new, k), arr[f"out1_{k}"]) < 1e-10, k
     assert _rel(coeffs, arr["out1_coeffs"]) < 1e-9
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["fans_swirl_f64", "ports_heat_f64", "tunnel_paint_pid_f64"])
+def test_fast_step_phys_runs_the_placed_physics(name):
+    """fast_step_phys with a Physics3D-shaped object carrying fans, jets / vents, paint and the
+    PID controller: the step matches the reference and the objects' state tensors are the ones
+    updated (FanSet.thrust, PidDt.dt_prev, ...), as the reference's solver expects."""
+    from _golden import fan_items, port_items
+    from aerolume_b200.ns3d.fused import fast_step_phys, load_kernels
+    from aerolume_b200.ns3d.types import FanSet3D, PaintLayer3D, PidState3D, PortSet3D, State3D
+    meta, ops, geom, th, src, arr = load_case(name)
+    dt = torch.float64
+    fans = ports = paint = pid = None
+    if "fans" in meta:
+        fm = meta["fans"]
+        items = [{k: (_dev(x, dt) if k != "win" else x) for k, x in it.items()} for it in fan_items(meta, arr)]
+        fans = FanSet3D(items, *(fm[k] for k in ("target", "kp", "ki", "tmax", "velocity_mode", "swirl")),
+                        fm["any_swirl"], torch.tensor(fm["thrust"], device="cuda", dtype=dt),
+                        *(torch.zeros(len(items), device="cuda", dtype=dt) for _ in range(3)))
+    if "ports" in meta:
+        ports = PortSet3D([{k: (_dev(x, dt) if isinstance(x, np.ndarray) else x) for k, x in it.items()}
+                           for it in port_items(meta, arr)], meta["ports"]["mass_flux"], meta["ports"]["leak"])
+    if "paint_u" in arr:
+        paint = PaintLayer3D(*(_dev(arr["paint_" + g], dt) for g in "uvwc"))
+    if "pid" in meta:
+        pid = PidState3D(meta["pid"]["target"], *(torch.zeros((), device="cuda", dtype=dt) for _ in range(3)))
+    phys = types.SimpleNamespace(thermal=th, fans=fans, ports=ports, paint=paint, pid=pid,
+                                 u_floor=meta.get("u_floor", 0.0))
+    kern = load_kernels(ops.advection, torch.device("cuda"), dt)
+    nz, ny, nx = ops.nz, ops.ny, ops.nx
+    state = State3D(_dev(arr["in_u"], dt), _dev(arr["in_v"], dt), _dev(arr["in_w"], dt),
+                    torch.zeros(nz, ny, nx, device="cuda", dtype=dt), _dev(arr["in_t"], dt),
+                    torch.zeros((), device="cuda", dtype=dt))
+    theta = _dev(arr["in_theta"], dt) if "in_theta" in arr else None
+    out = fast_step_phys(state, geom, ops, kern, phys=phys, theta=theta)
+    torch.cuda.synchronize()
+    for k, got in (("u", out.state.u), ("v", out.state.v), ("w", out.state.w), ("p", out.state.p)):
+        assert _rel(got, arr[f"out1_{k}"]) < 1e-10, k
+    if theta is not None:
+        assert _rel(out.theta, arr["out1_theta"]) < 1e-10
+    if fans is not None:
+        got = np.stack([x.cpu().numpy() for x in (fans.thrust, fans.ud, fans.e_prev, fans.swirl_amp)])
+        assert np.abs(got - arr["fans1"]).max() <= 1e-10 * max(1.0, np.abs(arr["fans1"]).max())
+    if pid is not None:
+        got = np.array([float(pid.dt_prev), float(pid.e1), float(pid.e2)])
+        assert np.abs(got - arr["pid1"]).max() <= 1e-10 * max(1.0, np.abs(arr["pid1"]).max())
