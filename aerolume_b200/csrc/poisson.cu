@@ -274,7 +274,7 @@ __global__ void __launch_bounds__(256) line_transform_kernel(const TransformPara
 struct BlockExec {
   template <class F>
   __device__ __forceinline__ void operator()(F &&f) {
-    f((int)threadIdx.x, (int)blockDim.x);
+    f((int)threadIdx.x, 256);  // every launch of the transform kernel uses 256 threads
     __syncthreads();
   }
 };
@@ -304,7 +304,8 @@ __global__ void __launch_bounds__(256) pow2_transform_kernel(const __grid_consta
   fft::Cx<T> *C1 = reinterpret_cast<fft::Cx<T> *>(smem_raw + G::TW + G::RB + G::CB);
   __shared__ long long rowoff[5][L];  // fused divergence: u row, v rows j / j+1, w planes k / k+1
   const int nx = P.nx, ny = P.ny, nz = P.nz;
-  const int tid = threadIdx.x, nthr = blockDim.x;
+  const int tid = threadIdx.x;
+  constexpr int nthr = 256;  // the launch's block size: loop trip counts are compile-time
   for (int m = tid; m < N; m += nthr) tw[m] = {P.A.tw[2 * m], P.A.tw[2 * m + 1]};
   int nl;
   size_t base, estride;
