@@ -159,6 +159,7 @@ template <typename T>
 __global__ void __launch_bounds__(256) plane_sum_kernel(const T *a0, size_t stride0, size_t off0, double *out0,
                                                         const T *a1, size_t stride1, size_t off1, double *out1,
                                                         int rows) {
+  aero::pdl_wait();
   __shared__ double red[2][8];
   const int per = (rows + gridDim.x - 1) / gridDim.x;
   const int r0 = blockIdx.x * per, r1 = min(rows, r0 + per);
@@ -484,7 +485,7 @@ int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom
   const int rows = nz * ny;
   double *psum = reinterpret_cast<double *>(ws + p->off_psum);  // [u0 outlet | inlet | 3 stages x 2] x parts
   if (tunnel) {
-    plane_sum_kernel<T><<<PLANE_PARTS, 256, 0, s>>>(upb, p->pu, nx, psum, S.u_inlet, 1, 0, psum + PLANE_PARTS,
+    (void)aero::launch_k(plane_sum_kernel<T>, PLANE_PARTS, 256, 0, s, upb, p->pu, nx, psum, S.u_inlet, 1, 0, psum + PLANE_PARTS,
                                                     rows);
     CUDA_TRY(cudaGetLastError());
   }
@@ -496,7 +497,7 @@ int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom
     const T *up = upb, *vp = st == 0 ? v0 : vpb, *wp = st == 0 ? w0 : wpb;
     if (tunnel) {
       double *sums = psum + (2 + 2 * st) * PLANE_PARTS;  // outlet column, the one before it
-      plane_sum_kernel<T><<<PLANE_PARTS, 256, 0, s>>>(up, p->pu, nx, sums, up, p->pu, nx - 1, sums + PLANE_PARTS,
+      (void)aero::launch_k(plane_sum_kernel<T>, PLANE_PARTS, 256, 0, s, up, p->pu, nx, sums, up, p->pu, nx - 1, sums + PLANE_PARTS,
                                                       rows);
       CUDA_TRY(cudaGetLastError());
       CUDA_TRY(aero::launch_outlet_corr<T>(sums, sums + PLANE_PARTS, psum, psum + PLANE_PARTS, PLANE_PARTS, small,

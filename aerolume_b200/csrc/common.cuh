@@ -2,11 +2,35 @@
 #pragma once
 
 #include <cstdint>
+#include <utility>
 #include <cuda_runtime.h>
 
 #include "../../include/aero_b200.h"
 
 namespace aero {
+
+// Programmatic dependent launch: every kernel of the library is launched with programmatic
+// stream serialisation, so its launch and block scheduling overlap the tail of the kernel
+// before it, and every kernel's first statement waits (griddepcontrol.wait) until that kernel
+// has completed and its writes are visible.  Launched without the attribute, the wait returns
+// at once.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_k(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                            Args &&...args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 // Bounds checks of the checked build (-DAERO_BOUNDS_CHECK, libaero_b200_checked.so): a failed
 // check records (code, index, bound) once in aero_check_word and the access is skipped.  In the

@@ -93,6 +93,7 @@ constexpr int FTX = 32, FTY = 8, FSX = FTX + 2, FSY = FTY + 2;
 
 template <typename T>
 __global__ void __launch_bounds__(FTX *FTY) fields_kernel(const __grid_constant__ FieldsParams<T> P) {
+  aero::pdl_wait();
   __shared__ T sm[3][3][FSY][FSX];  // [component][dz + 1][y][x]
   const int nx = P.nx, ny = P.ny, nz = P.nz;
   const int i0 = blockIdx.x * FTX, j0 = blockIdx.y * FTY, k = blockIdx.z;
@@ -132,6 +133,7 @@ __global__ void __launch_bounds__(FTX *FTY) fields_kernel(const __grid_constant_
 template <typename T>
 __global__ void probe_kernel(const T *__restrict__ f, int fnx, int fny, int fnz, T x0, T y0, T z0, T h, T ox, T oy,
                              T oz, const T *__restrict__ pts, long long npts, T *__restrict__ out) {
+  aero::pdl_wait();
   const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (p >= npts) return;
   auto axis = [&](T x, T origin, T off, int n, int &i0, T &t, int &s) {
@@ -164,7 +166,7 @@ __global__ void probe_kernel(const T *__restrict__ f, int fnx, int fny, int fnz,
 
 template <typename T>
 cudaError_t launch_fields(const FieldsParams<T> &P, cudaStream_t s) {
-  fields_kernel<T><<<dim3((P.nx + FTX - 1) / FTX, (P.ny + FTY - 1) / FTY, P.nz), dim3(FTX, FTY), 0, s>>>(P);
+  (void)aero::launch_k(fields_kernel<T>, dim3((P.nx + FTX - 1) / FTX, (P.ny + FTY - 1) / FTY, P.nz), dim3(FTX, FTY), 0, s, P);
   return cudaGetLastError();
 }
 
@@ -173,7 +175,7 @@ cudaError_t launch_probe(const T *f, int fnx, int fny, int fnz, const double ori
                          const T *pts, long long npts, T *out, cudaStream_t s) {
   if (npts <= 0) return cudaSuccess;
   const unsigned blocks = (unsigned)((npts + 255) / 256);
-  probe_kernel<T><<<blocks, 256, 0, s>>>(f, fnx, fny, fnz, T(origin[0]), T(origin[1]), T(origin[2]), T(h), T(off[0]),
+  (void)aero::launch_k(probe_kernel<T>, blocks, 256, 0, s, f, fnx, fny, fnz, T(origin[0]), T(origin[1]), T(origin[2]), T(h), T(off[0]),
                                          T(off[1]), T(off[2]), pts, npts, out);
   return cudaGetLastError();
 }

@@ -97,6 +97,7 @@ struct StageParams {
 // viscosity of the tile's cells (the first stage's dt needs it before the update).
 template <typename T, bool NU_ONLY>
 __global__ void __launch_bounds__(NT) stage2d_kernel(const __grid_constant__ StageParams<T> P) {
+  aero::pdl_wait();
   __shared__ T U[UY][UX];
   __shared__ T V[VY][VX];
   __shared__ T NU[CY][CX], TXX[CY][CX], TYY[CY][CX];
@@ -323,6 +324,7 @@ template <typename T>
 __global__ void correct2d_kernel(int nx, int ny, int periodic, T inv_h, const T *__restrict__ uh,
                                  const T *__restrict__ vh, const T *__restrict__ psi, T *__restrict__ u,
                                  T *__restrict__ v) {
+  aero::pdl_wait();
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
   if (i >= nx || j >= ny) return;
   const size_t c = (size_t)j * nx;
@@ -358,6 +360,7 @@ __global__ void correct2d_kernel(int nx, int ny, int periodic, T inv_h, const T 
 template <typename T>
 __global__ void divergence2d_kernel(int nx, int ny, T inv_h, const T *__restrict__ u, const T *__restrict__ v,
                                     T *__restrict__ div) {
+  aero::pdl_wait();
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
   if (i >= nx || j >= ny) return;
   const size_t ru = (size_t)j * (nx + 1);
@@ -393,6 +396,7 @@ __device__ __forceinline__ T dye2d_at(const DyeParams<T> &P, int j, int i) {
 // clamped at 1, zero inside solids (core.py:779-792)
 template <typename T>
 __global__ void dye2d_kernel(const __grid_constant__ DyeParams<T> P) {
+  aero::pdl_wait();
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
   const int nx = P.nx, ny = P.ny;
   if (i >= nx || j >= ny) return;
@@ -416,6 +420,7 @@ __global__ void dye2d_kernel(const __grid_constant__ DyeParams<T> P) {
 template <typename T>
 __global__ void dt2d_kernel(int mode, const T *dt_in, double dt_fixed, const unsigned long long *bits, double cfl_h,
                             double nu, double visc_h2, int les, T *dt_out) {
+  aero::pdl_wait();
   T dt;
   if (mode == 2) {
     dt = *dt_in;
@@ -436,6 +441,7 @@ __global__ void dt2d_kernel(int mode, const T *dt_in, double dt_fixed, const uns
 template <typename T>
 __global__ void finalize2d_kernel(const double *__restrict__ partials, int nblocks, int nbody, double h,
                                   double force_ref, const T *dt, const T *t0, T *t_out, T *dt_out, T *coeffs) {
+  aero::pdl_wait();
   __shared__ double tot[MAXQ];
   const int nq = 4 * nbody;
   for (int q = threadIdx.x >> 5; q < nq; q += blockDim.x >> 5) {
@@ -597,11 +603,11 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
       N.up = u0;
       N.vp = v0;
       N.nut_max = bits + aero::SC_NUTMAX;
-      stage2d_kernel<T, true><<<grid, block, 0, s>>>(N);
+      (void)aero::launch_k(stage2d_kernel<T, true>, grid, block, 0, s, N);
       AERO_CUDA_TRY(cudaGetLastError());
     }
   }
-  dt2d_kernel<T><<<1, 1, 0, s>>>(dt_mode, static_cast<const T *>(dt_in), c.dt_fixed, bits, c.cfl * c.h, c.nu,
+  (void)aero::launch_k(dt2d_kernel<T>, 1, 1, 0, s, dt_mode, static_cast<const T *>(dt_in), c.dt_fixed, bits, c.cfl * c.h, c.nu,
                                  0.25 * c.h * c.h, les ? 1 : 0, small);
   AERO_CUDA_TRY(cudaGetLastError());
   // ---- stages
@@ -616,7 +622,7 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
     P.b = T(RK[st][1]);
     P.w = T(RK[st][2]);
     P.partials = partials + (size_t)st * p->nblocks * std::max(p->nq, 1);
-    stage2d_kernel<T, false><<<grid, block, 0, s>>>(P);
+    (void)aero::launch_k(stage2d_kernel<T, false>, grid, block, 0, s, P);
     AERO_CUDA_TRY(cudaGetLastError());
     const int acc_mode = st == 0 ? 0 : (st == 1 ? 1 : 2);
     if (fused) {
@@ -632,7 +638,7 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
       const int rc = poisson2d_passes<T>(p, nullptr, pa, ws, s, &F);
       if (rc) return rc;
     } else {
-      divergence2d_kernel<T><<<dim3((nx + 127) / 128, ny), 128, 0, s>>>(nx, ny, T(1.0 / c.h), uh, vh, pa);
+      (void)aero::launch_k(divergence2d_kernel<T>, dim3((nx + 127) / 128, ny), 128, 0, s, nx, ny, T(1.0 / c.h), uh, vh, pa);
       AERO_CUDA_TRY(cudaGetLastError());
       const int rc = poisson2d_passes<T>(p, pa, pa, ws, s);
       if (rc) return rc;
@@ -640,7 +646,7 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
     }
     T *uo = st == 2 ? static_cast<T *>(f->u) : upb;
     T *vo = st == 2 ? static_cast<T *>(f->v) : vpb;
-    correct2d_kernel<T><<<dim3((nx + 127) / 128, ny), 128, 0, s>>>(nx, ny, c.periodic, T(1.0 / c.h), uh, vh, pa, uo, vo);
+    (void)aero::launch_k(correct2d_kernel<T>, dim3((nx + 127) / 128, ny), 128, 0, s, nx, ny, c.periodic, T(1.0 / c.h), uh, vh, pa, uo, vo);
     AERO_CUDA_TRY(cudaGetLastError());
   }
   // ---- dye with the step's final velocity
@@ -659,10 +665,10 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
     D.has_win = has_win;
     for (int q = 0; q < 4; ++q) D.win[q] = c.window[q];
     D.chi_c = static_cast<const T *>(g->chi_c);
-    dye2d_kernel<T><<<dim3((nx + 127) / 128, ny), 128, 0, s>>>(D);
+    (void)aero::launch_k(dye2d_kernel<T>, dim3((nx + 127) / 128, ny), 128, 0, s, D);
     AERO_CUDA_TRY(cudaGetLastError());
   }
-  finalize2d_kernel<T><<<1, 256, 0, s>>>(partials, p->nblocks, S.nbody, c.h, c.force_ref, small,
+  (void)aero::launch_k(finalize2d_kernel<T>, 1, 256, 0, s, partials, p->nblocks, S.nbody, c.h, c.force_ref, small,
                                          static_cast<const T *>(f->t0), static_cast<T *>(f->t),
                                          static_cast<T *>(f->dt), static_cast<T *>(f->coeffs));
   AERO_CUDA_TRY(cudaGetLastError());

@@ -15,6 +15,7 @@ namespace aero {
 // max |a| over an array: warp shuffles, then one atomic per block
 template <typename T>
 __global__ void absmax_kernel(const T *__restrict__ a, size_t n, unsigned long long *out) {
+  aero::pdl_wait();
   T m = T(0);
   for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
     const T v = fabs(a[e]);
@@ -29,6 +30,7 @@ __global__ void absmax_kernel(const T *__restrict__ a, size_t n, unsigned long l
 template <typename T>
 __global__ void copy_u_kernel(const T *__restrict__ u, T *__restrict__ out, int nx, int ny, int nz, int pitch,
                               unsigned long long *mx) {
+  aero::pdl_wait();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int rows = ny * nz;
   T m = T(0);
@@ -58,6 +60,7 @@ __global__ void copy_u_kernel(const T *__restrict__ u, T *__restrict__ out, int 
 // amplitude swirl ud |ud|.
 template <typename T>
 __global__ void __launch_bounds__(256) fan_begin_kernel(const __grid_constant__ FanBeginParams<T> P) {
+  aero::pdl_wait();
   __shared__ double red[3][8];
   const auto &F = P.fan[blockIdx.x];
   const int nx = P.nx, ny = P.ny;
@@ -105,6 +108,7 @@ __global__ void __launch_bounds__(256) fan_begin_kernel(const __grid_constant__ 
 // rounded through the field type as the reference computes it.
 template <typename T>
 __global__ void dt_kernel(const DtParams P) {
+  aero::pdl_wait();
   const double *sc = P.scalars;
   const unsigned long long *bits = reinterpret_cast<const unsigned long long *>(sc);
   T dt;
@@ -180,6 +184,7 @@ __global__ void dt_kernel(const DtParams P) {
 template <typename T>
 __global__ void outlet_sum_kernel(const T *__restrict__ u, const T *__restrict__ u0, int nx, int rows,
                                   double *sums) {
+  aero::pdl_wait();
   __shared__ double red[3][32];
   double s0 = 0.0, s1 = 0.0, s2 = 0.0;
   for (int r = threadIdx.x; r < rows; r += blockDim.x) {
@@ -220,6 +225,7 @@ template <typename T>
 __global__ void outlet_corr_kernel(const double *p_out, const double *p_in, const double *p_u0, const double *p_inlet,
                                    int parts, const T *dt, double a, double bscale, double inv_h, double inv_rows,
                                    double source, T *corr) {
+  aero::pdl_wait();
   double so = 0.0, si = 0.0, s0 = 0.0, sn = 0.0;
   for (int q = 0; q < parts; ++q) {
     so += p_out[q];
@@ -239,6 +245,7 @@ __global__ void outlet_corr_kernel(const double *p_out, const double *p_in, cons
 // applies them (physics.py:1043-1047); one block, the windows are small
 template <typename T>
 __global__ void port_continuity_kernel(T *div, int nx, int ny, int nport, PortParamsBlock<T> P) {
+  aero::pdl_wait();
   for (int q = 0; q < nport; ++q) {
     const PortSource<T> &Q = P.port[q];
     const int wz = Q.win[1] - Q.win[0], wy = Q.win[3] - Q.win[2], wx = Q.win[5] - Q.win[4];
@@ -259,6 +266,7 @@ __global__ void port_continuity_kernel(T *div, int nx, int ny, int nport, PortPa
 template <typename T>
 __global__ void divergence_kernel(const T *__restrict__ u, const T *__restrict__ v, const T *__restrict__ w, int nx,
                                   int ny, int nz, int px, int py, int pz, T inv_h, T *__restrict__ div) {
+  aero::pdl_wait();
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
   if (i >= nx) return;
   const size_t ru = ((size_t)k * ny + j) * (nx + 1);
@@ -276,6 +284,7 @@ __global__ void divergence_kernel(const T *__restrict__ u, const T *__restrict__
 // duplicate faces equal face 0.
 template <typename T>
 __global__ void correct_kernel(const CorrectParams<T> P) {
+  aero::pdl_wait();
   const int nx = P.nx, ny = P.ny, nz = P.nz;
   const int i0 = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
   const T inv = P.inv_h;
@@ -362,6 +371,7 @@ constexpr int SMOKE_LOADS = (SMOKE_PPL + SMOKE_TX * SMOKE_TY - 1) / (SMOKE_TX * 
 
 template <typename T>
 __global__ void __launch_bounds__(SMOKE_TX *SMOKE_TY, sizeof(T) == 4 ? 4 : 1) smoke_kernel(const __grid_constant__ SmokeParams<T> P) {
+  aero::pdl_wait();
   __shared__ T ring[SMOKE_NSLOT][SMOKE_PPL];
   const int nx = P.nx, ny = P.ny, nz = P.nz;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * SMOKE_TX + tx;
@@ -458,6 +468,7 @@ __global__ void __launch_bounds__(SMOKE_TX *SMOKE_TY, sizeof(T) == 4 ? 4 : 1) sm
 // tot[q] = sum over stages and blocks of partials[stage][block][q]: one block per q, a
 // fixed thread-to-term mapping and tree, so the sum is the same on every run.
 __global__ void partials_reduce_kernel(const double *__restrict__ partials, int nblocks, int nq, double *tot) {
+  aero::pdl_wait();
   const int q = blockIdx.x;
   double s = 0.0;
   for (int e = threadIdx.x; e < 3 * nblocks; e += blockDim.x) s += partials[(size_t)e * nq + q];
@@ -474,6 +485,7 @@ __global__ void partials_reduce_kernel(const double *__restrict__ partials, int 
 
 template <typename T>
 __global__ void finalize_kernel(const FinalizeParams<T> P) {
+  aero::pdl_wait();
   const T dt = *P.dt;
   *P.t_out = *P.t0 + dt;
   *P.dt_out = dt;
@@ -522,6 +534,7 @@ __global__ void finalize_kernel(const FinalizeParams<T> P) {
 template <typename T>
 __global__ void psi_accumulate_kernel(const T *__restrict__ psi, T *__restrict__ pw, size_t n, T wgt, int mode,
                                       const T *__restrict__ dt) {
+  aero::pdl_wait();
   const T rdt = mode == 2 ? T(1) / *dt : T(1);
   for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
     if (mode == 0) {
@@ -540,7 +553,7 @@ __global__ void psi_accumulate_kernel(const T *__restrict__ psi, T *__restrict__
 template <typename T>
 cudaError_t launch_absmax(const T *a, size_t n, unsigned long long *out, cudaStream_t s) {
   int blocks = (int)std::min<size_t>((n + 1023) / 1024, 148 * 2);
-  absmax_kernel<T><<<blocks, 1024, 0, s>>>(a, n, out);
+  (void)aero::launch_k(absmax_kernel<T>, blocks, 1024, 0, s, a, n, out);
   return cudaGetLastError();
 }
 
@@ -550,26 +563,26 @@ cudaError_t launch_copy_u(const T *u, T *out, int nx, int ny, int nz, int pitch,
   const unsigned gx = (unsigned)((nx + 127) / 128);
   const unsigned rows = (unsigned)ny * (unsigned)nz;
   const unsigned gy = std::max(1u, std::min((rows + 1) / 2, 2368u / gx));
-  copy_u_kernel<T><<<dim3(gx, gy), dim3(128, 2), 0, s>>>(u, out, nx, ny, nz, pitch, mx);
+  (void)aero::launch_k(copy_u_kernel<T>, dim3(gx, gy), dim3(128, 2), 0, s, u, out, nx, ny, nz, pitch, mx);
   return cudaGetLastError();
 }
 
 template <typename T>
 cudaError_t launch_fan_begin(const FanBeginParams<T> &P, cudaStream_t s) {
   if (P.nfan <= 0) return cudaSuccess;
-  fan_begin_kernel<T><<<P.nfan, 256, 0, s>>>(P);
+  (void)aero::launch_k(fan_begin_kernel<T>, P.nfan, 256, 0, s, P);
   return cudaGetLastError();
 }
 
 template <typename T>
 cudaError_t launch_dt(const DtParams &P, cudaStream_t s) {
-  dt_kernel<T><<<1, 1, 0, s>>>(P);
+  (void)aero::launch_k(dt_kernel<T>, 1, 1, 0, s, P);
   return cudaGetLastError();
 }
 
 template <typename T>
 cudaError_t launch_outlet_sum(const T *u, const T *u0, int nx, int rows, double *sums, cudaStream_t s) {
-  outlet_sum_kernel<T><<<1, 1024, 0, s>>>(u, u0, nx, rows, sums);
+  (void)aero::launch_k(outlet_sum_kernel<T>, 1, 1024, 0, s, u, u0, nx, rows, sums);
   return cudaGetLastError();
 }
 
@@ -577,7 +590,7 @@ template <typename T>
 cudaError_t launch_outlet_corr(const double *p_out, const double *p_in, const double *p_u0, const double *p_inlet,
                                int parts, const T *dt, double a, double b, double inv_h, double inv_rows,
                                double source, T *corr, cudaStream_t s) {
-  outlet_corr_kernel<T><<<1, 1, 0, s>>>(p_out, p_in, p_u0, p_inlet, parts, dt, a, b, inv_h, inv_rows, source, corr);
+  (void)aero::launch_k(outlet_corr_kernel<T>, 1, 1, 0, s, p_out, p_in, p_u0, p_inlet, parts, dt, a, b, inv_h, inv_rows, source, corr);
   return cudaGetLastError();
 }
 
@@ -586,7 +599,7 @@ cudaError_t launch_port_continuity(T *div, int nx, int ny, int nport, const Port
   if (nport <= 0) return cudaSuccess;
   PortParamsBlock<T> P{};
   for (int q = 0; q < nport; ++q) P.port[q] = ports[q];
-  port_continuity_kernel<T><<<1, 1024, 0, s>>>(div, nx, ny, nport, P);
+  (void)aero::launch_k(port_continuity_kernel<T>, 1, 1024, 0, s, div, nx, ny, nport, P);
   return cudaGetLastError();
 }
 
@@ -595,37 +608,37 @@ static inline int grid_for(size_t n) { return (int)std::max<size_t>(1, std::min<
 template <typename T>
 cudaError_t launch_divergence(const T *u, const T *v, const T *w, int nx, int ny, int nz, int px, int py, int pz,
                               T inv_h, T *div, cudaStream_t s) {
-  divergence_kernel<T><<<dim3((nx + 127) / 128, ny, nz), 128, 0, s>>>(u, v, w, nx, ny, nz, px, py, pz, inv_h, div);
+  (void)aero::launch_k(divergence_kernel<T>, dim3((nx + 127) / 128, ny, nz), 128, 0, s, u, v, w, nx, ny, nz, px, py, pz, inv_h, div);
   return cudaGetLastError();
 }
 
 template <typename T>
 cudaError_t launch_correct(const CorrectParams<T> &P, cudaStream_t s) {
-  correct_kernel<T><<<dim3((P.nx + 127) / 128, P.ny + 1, P.nz + 1), 128, 0, s>>>(P);
+  (void)aero::launch_k(correct_kernel<T>, dim3((P.nx + 127) / 128, P.ny + 1, P.nz + 1), 128, 0, s, P);
   return cudaGetLastError();
 }
 
 template <typename T>
 cudaError_t launch_smoke(const SmokeParams<T> &P, cudaStream_t s) {
   const dim3 grid((P.nx + SMOKE_TX - 1) / SMOKE_TX, (P.ny + SMOKE_TY - 1) / SMOKE_TY, (P.nz + SMOKE_ZC - 1) / SMOKE_ZC);
-  smoke_kernel<T><<<grid, dim3(SMOKE_TX, SMOKE_TY), 0, s>>>(P);
+  (void)aero::launch_k(smoke_kernel<T>, grid, dim3(SMOKE_TX, SMOKE_TY), 0, s, P);
   return cudaGetLastError();
 }
 
 template <typename T>
 cudaError_t launch_finalize(const FinalizeParams<T> &P, cudaStream_t s) {
   if (P.nq > 0) {
-    partials_reduce_kernel<<<P.nq, 256, 0, s>>>(P.partials, P.nblocks, P.nq, P.tot);
+    (void)aero::launch_k(partials_reduce_kernel, P.nq, 256, 0, s, P.partials, P.nblocks, P.nq, P.tot);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
   }
-  finalize_kernel<T><<<1, 1, 0, s>>>(P);
+  (void)aero::launch_k(finalize_kernel<T>, 1, 1, 0, s, P);
   return cudaGetLastError();
 }
 
 template <typename T>
 cudaError_t launch_psi_accumulate(const T *psi, T *pw, size_t n, T wgt, int mode, const T *dt, cudaStream_t s) {
-  psi_accumulate_kernel<T><<<grid_for(n), 256, 0, s>>>(psi, pw, n, wgt, mode, dt);
+  (void)aero::launch_k(psi_accumulate_kernel<T>, grid_for(n), 256, 0, s, psi, pw, n, wgt, mode, dt);
   return cudaGetLastError();
 }
 

@@ -56,6 +56,7 @@ struct NuSmem {
 
 template <typename T, int MODEL>
 __global__ void __launch_bounds__(TX *TY) nu_kernel(const __grid_constant__ NuParams<T> P) {
+  aero::pdl_wait();
   __shared__ NuSmem<T> S;
   constexpr int QSLOT = NuRing<T>::QSLOT, AHEAD = NuRing<T>::AHEAD;
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
@@ -195,6 +196,7 @@ struct StageSmem {
 // leave out entirely.
 template <typename T, bool UPWIND, bool LES, bool THERMAL, bool PLACED>
 __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) stage_kernel(const __grid_constant__ StageParams<T> P) {
+  aero::pdl_wait();
   extern __shared__ __align__(128) unsigned char smem_raw[];
   StageSmem<T> &S = *reinterpret_cast<StageSmem<T> *>(smem_raw);
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
@@ -721,7 +723,7 @@ cudaError_t launch_stage_cfg(const StageParams<T> &P, cudaStream_t s) {
     attr = true;
   }
   dim3 grid((P.nx + TX - 1) / TX, (P.ny + TY - 1) / TY, (P.nz + P.zc - 1) / P.zc);
-  stage_kernel<T, UPWIND, LES, THERMAL, PLACED><<<grid, dim3(TX, TY), smem, s>>>(P);
+  (void)aero::launch_k(stage_kernel<T, UPWIND, LES, THERMAL, PLACED>, grid, dim3(TX, TY), smem, s, P);
   return cudaGetLastError();
 }
 
@@ -747,9 +749,9 @@ template <typename T>
 cudaError_t launch_nu(const NuParams<T> &P, cudaStream_t s) {
   dim3 grid((P.nx + 2 + TX - 1) / TX, (P.ny + 2 + TY - 1) / TY, (P.nz + 2 + P.zc - 1) / P.zc);
   switch (P.les) {
-    case AERO_LES_SMAGORINSKY: nu_kernel<T, AERO_LES_SMAGORINSKY><<<grid, dim3(TX, TY), 0, s>>>(P); break;
-    case AERO_LES_WALE: nu_kernel<T, AERO_LES_WALE><<<grid, dim3(TX, TY), 0, s>>>(P); break;
-    case AERO_LES_VREMAN: nu_kernel<T, AERO_LES_VREMAN><<<grid, dim3(TX, TY), 0, s>>>(P); break;
+    case AERO_LES_SMAGORINSKY: (void)aero::launch_k(nu_kernel<T, AERO_LES_SMAGORINSKY>, grid, dim3(TX, TY), 0, s, P); break;
+    case AERO_LES_WALE: (void)aero::launch_k(nu_kernel<T, AERO_LES_WALE>, grid, dim3(TX, TY), 0, s, P); break;
+    case AERO_LES_VREMAN: (void)aero::launch_k(nu_kernel<T, AERO_LES_VREMAN>, grid, dim3(TX, TY), 0, s, P); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();

@@ -191,6 +191,7 @@ __device__ void transform_tile(T *R, int ld, Cx<T> *C0, Cx<T> *C1, int n, int L,
 
 template <typename T>
 __global__ void __launch_bounds__(256) line_transform_kernel(const TransformParams<T> P) {
+  aero::pdl_wait();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int n = P.A.n, L = P.L, ld = L + 1;
   T *R = reinterpret_cast<T *>(smem_raw);
@@ -295,6 +296,7 @@ struct Pow2Tile {
 // lambda_x + lambda_y + lambda_z (zero mode dropped) and inverse (z axis).
 template <typename T, int N, int LOG2L_>
 __global__ void __launch_bounds__(256) pow2_transform_kernel(const __grid_constant__ TransformParams<T> P) {
+  aero::pdl_wait();
   using G = Pow2Tile<T, N, LOG2L_>;
   constexpr int L = G::L, LD = G::LD, LOG2L = G::LOG2L, LOG2N = G::LOG2N;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -426,7 +428,7 @@ cudaError_t launch_pow2_tile(const TransformParams<T> &P, cudaStream_t s) {
     grid = dim3((unsigned)(((size_t)P.nz * P.ny + G::L - 1) / G::L), 1, 1);
   else
     grid = dim3((unsigned)((P.nx + G::L - 1) / G::L), (unsigned)(P.axis == 1 ? P.nz : P.ny), 1);
-  pow2_transform_kernel<T, N, LOG2L_><<<grid, 256, G::SMEM, s>>>(P);
+  (void)aero::launch_k(pow2_transform_kernel<T, N, LOG2L_>, grid, 256, G::SMEM, s, P);
   return cudaGetLastError();
 }
 
@@ -448,6 +450,7 @@ bool transform_pow2(int n) { return n >= 8 && n <= 2048 && (n & (n - 1)) == 0; }
 // and the dense orthonormal matrix of poisson.py:74-90 for lengths the FFT does not take.
 template <typename T>
 __global__ void axis_tables_kernel(int n, int kind, int dense, double h, T *tw, T *post, T *cs, double *lam, T *mat) {
+  aero::pdl_wait();
   const int tid = blockIdx.x * blockDim.x + threadIdx.x, nthr = gridDim.x * blockDim.x;
   for (int m = tid; m < n; m += nthr) {
     double s, c;
@@ -515,14 +518,14 @@ cudaError_t launch_transform(const TransformParams<T> &P, cudaStream_t s) {
   } else {
     grid = dim3((unsigned)((P.nx + P.L - 1) / P.L), (unsigned)(P.axis == 1 ? P.nz : P.ny), 1);
   }
-  line_transform_kernel<T><<<grid, 256, smem, s>>>(P);
+  (void)aero::launch_k(line_transform_kernel<T>, grid, 256, smem, s, P);
   return cudaGetLastError();
 }
 
 template <typename T>
 cudaError_t launch_axis_tables(int n, int kind, int dense, double h, T *tw, T *post, T *cs, double *lam, T *mat,
                                cudaStream_t s) {
-  axis_tables_kernel<T><<<64, 256, 0, s>>>(n, kind, dense, h, tw, post, cs, lam, mat);
+  (void)aero::launch_k(axis_tables_kernel<T>, 64, 256, 0, s, n, kind, dense, h, tw, post, cs, lam, mat);
   return cudaGetLastError();
 }
 
