@@ -75,6 +75,21 @@ __device__ __forceinline__ T eddy2d(T g11, T g12, T g21, T g22, int model, T cfa
   return cfac * sqrt(bb / (aa + T(1e-30)) + T(1e-30));
 }
 
+// The step's dt (ns2d/core.py:686-695): given (mode 2), fixed (mode 1), or the CFL / viscous rule
+// on the maxima in the scalar block (mode 0), rounded through the field type as the reference.
+template <typename T>
+__device__ __forceinline__ T dt2d_value(int mode, const T *dt_in, double dt_fixed, const unsigned long long *bits,
+                                        double cfl_h, double nu, double visc_h2, int les) {
+  if (mode == 2) return *dt_in;
+  if (mode == 1) return T(dt_fixed);
+  T umax = T(as_double(bits[SC_MAXU])) + T(as_double(bits[SC_MAXV]));
+  umax = umax > T(1e-6) || umax != umax ? umax : T(1e-6);
+  T dt = T(cfl_h) / umax;
+  const T nut = les ? T(nu) + T(as_double(bits[SC_NUTMAX])) : T(nu);
+  const T dv = T(visc_h2) / nut;
+  return dv < dt ? dv : dt;
+}
+
 template <typename T>
 struct StageParams {
   int nx, ny, periodic, closed, upwind, les;
@@ -91,6 +106,13 @@ struct StageParams {
   int nbody;
   double *partials;            // this stage's [block][4 nbody]
   unsigned long long *nut_max; // nu-only pass: max nu_t (ordered bits)
+  // first stage: every block derives the step's dt (dt2d_value) and block (0, 0) stores it
+  // in *dt_store for the kernels after it; otherwise dt is read from *dt
+  int dt_here, dt_mode, dt_les;
+  const T *dt_in;
+  const unsigned long long *dt_bits;
+  double dt_fixed, dt_cfl_h, dt_nu, dt_visc_h2;
+  T *dt_store;
 };
 
 // One RK stage of the u- and v-faces of a 32 x 8 tile; NU_ONLY: only the maximum eddy
@@ -108,7 +130,10 @@ __global__ void __launch_bounds__(NT) stage2d_kernel(const __grid_constant__ Sta
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
   const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
   const bool tunnel = !P.periodic && !P.closed;
-  const T dt = *P.dt;
+  const T dt = P.dt_here ? dt2d_value<T>(P.dt_mode, P.dt_in, P.dt_fixed, P.dt_bits, P.dt_cfl_h, P.dt_nu, P.dt_visc_h2,
+                                         P.dt_les)
+                         : *P.dt;
+  if (P.dt_here && blockIdx.x == 0 && blockIdx.y == 0 && tid == 0) *P.dt_store = dt;
   const T bdt = dt * P.b;
   // outlet balance (core.py:352-359): every block with outlet faces sums the whole outlet
   // column of the stage value in the same fixed order, so all agree
@@ -416,27 +441,6 @@ __global__ void dye2d_kernel(const __grid_constant__ DyeParams<T> P) {
   P.c[(size_t)j * nx + i] = out;
 }
 
-// dt (core.py:685-696): 0 CFL / viscous rule from the maxima, 1 fixed, 2 copied from dt_in
-template <typename T>
-__global__ void dt2d_kernel(int mode, const T *dt_in, double dt_fixed, const unsigned long long *bits, double cfl_h,
-                            double nu, double visc_h2, int les, T *dt_out) {
-  aero::pdl_wait();
-  T dt;
-  if (mode == 2) {
-    dt = *dt_in;
-  } else if (mode == 1) {
-    dt = T(dt_fixed);
-  } else {
-    T umax = T(as_double(bits[SC_MAXU])) + T(as_double(bits[SC_MAXV]));
-    umax = umax > T(1e-6) || umax != umax ? umax : T(1e-6);
-    dt = T(cfl_h) / umax;
-    const T nut = les ? T(nu) + T(as_double(bits[SC_NUTMAX])) : T(nu);
-    const T dv = T(visc_h2) / nut;
-    dt = dv < dt ? dv : dt;
-  }
-  *dt_out = dt;
-}
-
 // Coefficients [Cd, Cl, Cm] per body from the stage partials in a fixed order, t + dt, dt
 template <typename T>
 __global__ void finalize2d_kernel(const double *__restrict__ partials, int nblocks, int nbody, double h,
@@ -596,8 +600,7 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
   const dim3 grid(p->gx, p->gy), block(TX, TY);
   if (dt_mode == 0) {
     AERO_CUDA_TRY(cudaMemsetAsync(sc, 0, 8 * sizeof(double), s));
-    AERO_CUDA_TRY(aero::launch_absmax<T>(u0, p->nu, bits + aero::SC_MAXU, s));
-    AERO_CUDA_TRY(aero::launch_absmax<T>(v0, p->nv, bits + aero::SC_MAXV, s));
+    AERO_CUDA_TRY(aero::launch_absmax2<T>(u0, p->nu, bits + aero::SC_MAXU, v0, p->nv, bits + aero::SC_MAXV, s));
     if (les) {
       StageParams<T> N = S;
       N.up = u0;
@@ -607,9 +610,16 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
       AERO_CUDA_TRY(cudaGetLastError());
     }
   }
-  (void)aero::launch_k(dt2d_kernel<T>, 1, 1, 0, s, dt_mode, static_cast<const T *>(dt_in), c.dt_fixed, bits, c.cfl * c.h, c.nu,
-                                 0.25 * c.h * c.h, les ? 1 : 0, small);
-  AERO_CUDA_TRY(cudaGetLastError());
+  // the time step itself is derived by the first stage kernel (dt2d_value), which stores it
+  S.dt_mode = dt_mode;
+  S.dt_in = static_cast<const T *>(dt_in);
+  S.dt_bits = bits;
+  S.dt_fixed = c.dt_fixed;
+  S.dt_cfl_h = c.cfl * c.h;
+  S.dt_nu = c.nu;
+  S.dt_visc_h2 = 0.25 * c.h * c.h;
+  S.dt_les = les ? 1 : 0;
+  S.dt_store = small;
   // ---- stages
   static const double RK[3][3] = {{0.0, 1.0, 1.0 / 6.0}, {0.75, 0.25, 2.0 / 3.0}, {1.0 / 3.0, 2.0 / 3.0, 1.0}};
   T *p_out = static_cast<T *>(f->p);
@@ -622,6 +632,7 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
     P.b = T(RK[st][1]);
     P.w = T(RK[st][2]);
     P.partials = partials + (size_t)st * p->nblocks * std::max(p->nq, 1);
+    P.dt_here = st == 0;
     (void)aero::launch_k(stage2d_kernel<T, false>, grid, block, 0, s, P);
     AERO_CUDA_TRY(cudaGetLastError());
     const int acc_mode = st == 0 ? 0 : (st == 1 ? 1 : 2);

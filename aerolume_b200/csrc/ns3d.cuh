@@ -215,6 +215,9 @@ template <typename T> cudaError_t launch_absmax(const T *, size_t, unsigned long
 template <typename T>
 cudaError_t launch_copy_u(const T *, T *, int, int, int, int, unsigned long long *, cudaStream_t);
 template <typename T> cudaError_t launch_dt(const DtParams &, cudaStream_t);
+template <typename T>
+cudaError_t launch_absmax2(const T *, size_t, unsigned long long *, const T *, size_t, unsigned long long *,
+                           cudaStream_t);
 template <typename T> cudaError_t launch_fan_begin(const FanBeginParams<T> &, cudaStream_t);
 // div -= m on every port's cells (physics.py:1043-1047)
 template <typename T>

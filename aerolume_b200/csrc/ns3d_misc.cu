@@ -24,6 +24,21 @@ __global__ void absmax_kernel(const T *__restrict__ a, size_t n, unsigned long l
   block_max_atomic<T>(m, out);
 }
 
+// max |a| and max |b| in one launch (blockIdx.y selects the array)
+template <typename T>
+__global__ void absmax2_kernel(const T *__restrict__ a, size_t na, unsigned long long *out_a, const T *__restrict__ b,
+                               size_t nb, unsigned long long *out_b) {
+  aero::pdl_wait();
+  const T *x = blockIdx.y == 0 ? a : b;
+  const size_t n = blockIdx.y == 0 ? na : nb;
+  T m = T(0);
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    const T v = fabs(x[e]);
+    m = (v > m || v != v) ? v : m;
+  }
+  block_max_atomic<T>(m, blockIdx.y == 0 ? out_a : out_b);
+}
+
 // u0 (rows of nx + 1) into the stage-start buffer with a 16-byte row pitch, with max |u0|.
 // A fixed grid strides over the rows (one max atomic per block, not per row); the thread of
 // x = nx - 1 also copies the last face, x = nx.
@@ -558,6 +573,15 @@ cudaError_t launch_absmax(const T *a, size_t n, unsigned long long *out, cudaStr
 }
 
 template <typename T>
+cudaError_t launch_absmax2(const T *a, size_t na, unsigned long long *out_a, const T *b, size_t nb,
+                           unsigned long long *out_b, cudaStream_t s) {
+  const size_t n = na > nb ? na : nb;
+  const int blocks = (int)std::min<size_t>((n + 1023) / 1024, 148);
+  (void)aero::launch_k(absmax2_kernel<T>, dim3(blocks, 2), 1024, 0, s, a, na, out_a, b, nb, out_b);
+  return cudaGetLastError();
+}
+
+template <typename T>
 cudaError_t launch_copy_u(const T *u, T *out, int nx, int ny, int nz, int pitch, unsigned long long *mx,
                           cudaStream_t s) {
   const unsigned gx = (unsigned)((nx + 127) / 128);
@@ -644,6 +668,8 @@ cudaError_t launch_psi_accumulate(const T *psi, T *pw, size_t n, T wgt, int mode
 
 #define INSTANTIATE(T)                                                                                               \
   template cudaError_t launch_absmax<T>(const T *, size_t, unsigned long long *, cudaStream_t);                     \
+  template cudaError_t launch_absmax2<T>(const T *, size_t, unsigned long long *, const T *, size_t,                 \
+                                         unsigned long long *, cudaStream_t);                                        \
   template cudaError_t launch_dt<T>(const DtParams &, cudaStream_t);                                                \
   template cudaError_t launch_fan_begin<T>(const FanBeginParams<T> &, cudaStream_t);                                \
   template cudaError_t launch_copy_u<T>(const T *, T *, int, int, int, int, unsigned long long *, cudaStream_t);                                                \

@@ -340,9 +340,9 @@ def run_ours(args, rank, world, local_rank):
 def _launches_2d(plan):
     c = plan.cfg
     fused = 8 <= c.nx <= 2048 and (c.nx & (c.nx - 1)) == 0
-    n = 1                                              # dt
+    n = 0                                              # (dt is derived inside the first stage kernel)
     if not c.has_dt_fixed:
-        n += 2 + (1 if c.les else 0)                   # |u|, |v| maxima, nu_t of u0
+        n += 1 + (1 if c.les else 0)                   # |u| and |v| maxima (one launch), nu_t of u0
     n += 3 * (1 + 3 + 1 + (0 if fused else 2))         # stage, 3 transform passes, correct, [div, psi_w]
     n += 1 if c.dye else 0
     return n + 1                                       # finalize
