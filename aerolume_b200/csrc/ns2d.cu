@@ -37,13 +37,47 @@ struct Rules2 {
   T val[2][2];
 };
 
-template <typename T>
-__device__ __forceinline__ T padded2(const T *__restrict__ f, const Rules2<T> &r, int j, int i) {
+// value at (j, i) of a field with its ghost rules; load(mj, mi) gives the in-range entries
+template <typename T, class Load>
+__device__ __forceinline__ T padded2f(const Rules2<T> &r, int j, int i, const Load &load) {
   T sx, cx, sy, cy;
   const int mi = ghost_map<T>(i, r.n0, r.kind[0][0], r.kind[0][1], r.val[0][0], r.val[0][1], sx, cx);
   const int mj = ghost_map<T>(j, r.n1, r.kind[1][0], r.kind[1][1], r.val[1][0], r.val[1][1], sy, cy);
-  const T x = __ldg(f + (size_t)mj * r.p0 + mi);
+  const T x = load(mj, mi);
   return sy * (sx * x + cx) + cy;
+}
+
+template <typename T>
+__device__ __forceinline__ T padded2(const T *__restrict__ f, const Rules2<T> &r, int j, int i) {
+  return padded2f<T>(r, j, i, [&](int mj, int mi) { return __ldg(f + (size_t)mj * r.p0 + mi); });
+}
+
+// The projected velocity u = u_hat - grad psi on the u-face (j, fi) and the v-face (fj, i),
+// the correction of ns2d/core.py:632-646 (boundary-normal faces of a bounded domain keep
+// u_hat; a periodic domain wraps psi); correct2d_kernel writes the same values.
+template <typename T>
+__device__ __forceinline__ T projected_u(const T *__restrict__ uh, const T *__restrict__ psi, int nx, int periodic,
+                                         T inv_h, int j, int fi) {
+  const size_t c = (size_t)j * nx;
+  const T x = __ldg(uh + (size_t)j * (nx + 1) + fi);
+  if (periodic) {
+    const int ii = fi == nx ? 0 : fi, il = ii == 0 ? nx - 1 : ii - 1;
+    return x - (__ldg(psi + c + ii) - __ldg(psi + c + il)) * inv_h;
+  }
+  if (fi == 0 || fi == nx) return x;
+  return x - (__ldg(psi + c + fi) - __ldg(psi + c + fi - 1)) * inv_h;
+}
+
+template <typename T>
+__device__ __forceinline__ T projected_v(const T *__restrict__ vh, const T *__restrict__ psi, int nx, int ny,
+                                         int periodic, T inv_h, int fj, int i) {
+  const T x = __ldg(vh + (size_t)fj * nx + i);
+  if (periodic) {
+    const int jj = fj == ny ? 0 : fj, jl = jj == 0 ? ny - 1 : jj - 1;
+    return x - (__ldg(psi + (size_t)jj * nx + i) - __ldg(psi + (size_t)jl * nx + i)) * inv_h;
+  }
+  if (fj == 0 || fj == ny) return x;
+  return x - (__ldg(psi + (size_t)fj * nx + i) - __ldg(psi + (size_t)(fj - 1) * nx + i)) * inv_h;
 }
 
 // Eddy viscosity of the 2D gradient (core.py:469-500); cfac = c^2 h^2 (Smagorinsky, WALE)
@@ -95,7 +129,8 @@ struct StageParams {
   int nx, ny, periodic, closed, upwind, les;
   T inv_h, kadv, nuh2, cfac;
   Rules2<T> ru, rv;
-  const T *up, *vp, *u0, *v0;  // stage start, step start
+  const T *up, *vp, *u0, *v0;  // stage start (or, with psi, the previous stage value), step start
+  const T *psi;                // non-NULL: the stage start is up / vp projected with this psi
   T *uh, *vh;                  // stage value (after BCs and penalisation)
   T a, b, w;                   // RK blend weight, tendency weight, force weight
   const T *dt;
@@ -140,8 +175,10 @@ __global__ void __launch_bounds__(NT) stage2d_kernel(const __grid_constant__ Sta
   if (!NU_ONLY && tunnel && i0 + TX >= nx && tid < 32) {
     double s_in = 0.0, s_out = 0.0;
     for (int j = tid; j < ny; j += 32) {
-      const T un = P.up[(size_t)j * (nx + 1) + nx];
-      const T lu = (P.up[(size_t)j * (nx + 1) + nx - 1] - un) * P.inv_h;
+      const T un = P.psi ? projected_u<T>(P.up, P.psi, nx, P.periodic, P.inv_h, j, nx) : P.up[(size_t)j * (nx + 1) + nx];
+      const T un1 = P.psi ? projected_u<T>(P.up, P.psi, nx, P.periodic, P.inv_h, j, nx - 1)
+                          : P.up[(size_t)j * (nx + 1) + nx - 1];
+      const T lu = (un1 - un) * P.inv_h;
       const T uo = P.a == T(0) ? un : lerp_t<T>(un, P.u0[(size_t)j * (nx + 1) + nx], P.a);
       s_out += (double)(uo + lu * bdt);
       s_in += (double)P.u_inlet[j];
@@ -150,13 +187,28 @@ __global__ void __launch_bounds__(NT) stage2d_kernel(const __grid_constant__ Sta
     s_out = warp_sum(s_out);
     if (tid == 0) corr_s = T((s_in - s_out) / (double)ny);
   }
-  for (int e = tid; e < UY * UX; e += NT) {
-    const int r = e / UX, c = e - r * UX;
-    U[r][c] = padded2<T>(P.up, P.ru, j0 - 2 + r, i0 - 2 + c);
-  }
-  for (int e = tid; e < VY * VX; e += NT) {
-    const int r = e / VX, c = e - r * VX;
-    V[r][c] = padded2<T>(P.vp, P.rv, j0 - 2 + r, i0 - 2 + c);
+  if (P.psi) {  // the previous stage's projection, applied while staging the tile
+    for (int e = tid; e < UY * UX; e += NT) {
+      const int r = e / UX, c = e - r * UX;
+      U[r][c] = padded2f<T>(P.ru, j0 - 2 + r, i0 - 2 + c, [&](int mj, int mi) {
+        return projected_u<T>(P.up, P.psi, nx, P.periodic, P.inv_h, mj, mi);
+      });
+    }
+    for (int e = tid; e < VY * VX; e += NT) {
+      const int r = e / VX, c = e - r * VX;
+      V[r][c] = padded2f<T>(P.rv, j0 - 2 + r, i0 - 2 + c, [&](int mj, int mi) {
+        return projected_v<T>(P.vp, P.psi, nx, ny, P.periodic, P.inv_h, mj, mi);
+      });
+    }
+  } else {
+    for (int e = tid; e < UY * UX; e += NT) {
+      const int r = e / UX, c = e - r * UX;
+      U[r][c] = padded2<T>(P.up, P.ru, j0 - 2 + r, i0 - 2 + c);
+    }
+    for (int e = tid; e < VY * VX; e += NT) {
+      const int r = e / VX, c = e - r * VX;
+      V[r][c] = padded2<T>(P.vp, P.rv, j0 - 2 + r, i0 - 2 + c);
+    }
   }
   __syncthreads();
   // tile coordinates: u[j][i] -> U[j - j0 + 2][i - i0 + 2], v likewise in V
@@ -624,10 +676,17 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
   static const double RK[3][3] = {{0.0, 1.0, 1.0 / 6.0}, {0.75, 0.25, 2.0 / 3.0}, {1.0 / 3.0, 2.0 / 3.0, 1.0}};
   T *p_out = static_cast<T *>(f->p);
   const bool fused = p->ax[0].method == 0 && aero::transform_pow2(nx);
+  // stage values alternate between two buffer pairs; stages 2 and 3 project the previous
+  // stage's value themselves while staging it (P.psi), so only the last stage runs
+  // correct2d_kernel, into the caller's u, v
+  T *ub[2] = {uh, upb}, *vb[2] = {vh, vpb};
   for (int st = 0; st < 3; ++st) {
     StageParams<T> P = S;
-    P.up = st == 0 ? u0 : upb;
-    P.vp = st == 0 ? v0 : vpb;
+    P.up = st == 0 ? u0 : ub[(st + 1) % 2];
+    P.vp = st == 0 ? v0 : vb[(st + 1) % 2];
+    P.psi = st == 0 ? nullptr : pa;
+    P.uh = ub[st % 2];
+    P.vh = vb[st % 2];
     P.a = T(RK[st][0]);
     P.b = T(RK[st][1]);
     P.w = T(RK[st][2]);
@@ -639,8 +698,8 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
     if (fused) {
       aero::TransformParams<T> F{};
       F.fuse_div = 2;
-      F.uh = uh;
-      F.vh = vh;
+      F.uh = ub[st % 2];
+      F.vh = vb[st % 2];
       F.inv_h = T(1.0 / c.h);
       F.p_acc = p_out;
       F.wgt = T(RK[st][2]);
@@ -649,16 +708,18 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
       const int rc = poisson2d_passes<T>(p, nullptr, pa, ws, s, &F);
       if (rc) return rc;
     } else {
-      (void)aero::launch_k(divergence2d_kernel<T>, dim3((nx + 127) / 128, ny), 128, 0, s, nx, ny, T(1.0 / c.h), uh, vh, pa);
+      (void)aero::launch_k(divergence2d_kernel<T>, dim3((nx + 127) / 128, ny), 128, 0, s, nx, ny, T(1.0 / c.h),
+                           ub[st % 2], vb[st % 2], pa);
       AERO_CUDA_TRY(cudaGetLastError());
       const int rc = poisson2d_passes<T>(p, pa, pa, ws, s);
       if (rc) return rc;
       AERO_CUDA_TRY(aero::launch_psi_accumulate<T>(pa, p_out, p->nc, T(RK[st][2]), acc_mode, small, s));
     }
-    T *uo = st == 2 ? static_cast<T *>(f->u) : upb;
-    T *vo = st == 2 ? static_cast<T *>(f->v) : vpb;
-    (void)aero::launch_k(correct2d_kernel<T>, dim3((nx + 127) / 128, ny), 128, 0, s, nx, ny, c.periodic, T(1.0 / c.h), uh, vh, pa, uo, vo);
-    AERO_CUDA_TRY(cudaGetLastError());
+    if (st == 2) {
+      (void)aero::launch_k(correct2d_kernel<T>, dim3((nx + 127) / 128, ny), 128, 0, s, nx, ny, c.periodic,
+                           T(1.0 / c.h), ub[st % 2], vb[st % 2], pa, static_cast<T *>(f->u), static_cast<T *>(f->v));
+      AERO_CUDA_TRY(cudaGetLastError());
+    }
   }
   // ---- dye with the step's final velocity
   if (c.dye) {

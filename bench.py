@@ -343,7 +343,7 @@ def _launches_2d(plan):
     n = 0                                              # (dt is derived inside the first stage kernel)
     if not c.has_dt_fixed:
         n += 1 + (1 if c.les else 0)                   # |u| and |v| maxima (one launch), nu_t of u0
-    n += 3 * (1 + 3 + 1 + (0 if fused else 2))         # stage, 3 transform passes, correct, [div, psi_w]
+    n += 3 * (1 + 3 + (0 if fused else 2)) + 1         # stage, 3 transform passes, [div, psi_w]; one correct
     n += 1 if c.dye else 0
     return n + 1                                       # finalize
 
