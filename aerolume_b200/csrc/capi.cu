@@ -261,10 +261,12 @@ int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom
   const bool need_max = dt_in == nullptr && !c.has_dt_fixed;
   // the stage-start u copy with a 16-byte row pitch (TMA), and max |u0| on the way
   CUDA_TRY(aero::launch_copy_u<T>(u0, upb, nx, ny, nz, p->pu, need_max ? bits + aero::SC_MAXU : nullptr, s));
-  if (need_max) {
-    CUDA_TRY(aero::launch_absmax<T>(v0, p->nv, bits + aero::SC_MAXV, s));
-    CUDA_TRY(aero::launch_absmax<T>(w0, p->nw, bits + aero::SC_MAXW, s));
-    if (thermal) CUDA_TRY(aero::launch_absmax<T>(th0, p->nc, bits + aero::SC_MAXT, s));
+  if (need_max) {  // max |v0|, |w0| (and |theta0|) in one launch
+    aero::MaxJobs<T> J{};
+    J.job[0] = {v0, p->nv, bits + aero::SC_MAXV};
+    J.job[1] = {w0, p->nw, bits + aero::SC_MAXW};
+    if (thermal) J.job[2] = {th0, p->nc, bits + aero::SC_MAXT};
+    CUDA_TRY(aero::launch_absmax_multi<T>(J, thermal ? 3 : 2, s));
   }
 
   aero::StageParams<T> S{};

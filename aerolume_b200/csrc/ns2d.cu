@@ -652,7 +652,10 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
   const dim3 grid(p->gx, p->gy), block(TX, TY);
   if (dt_mode == 0) {
     AERO_CUDA_TRY(cudaMemsetAsync(sc, 0, 8 * sizeof(double), s));
-    AERO_CUDA_TRY(aero::launch_absmax2<T>(u0, p->nu, bits + aero::SC_MAXU, v0, p->nv, bits + aero::SC_MAXV, s));
+    aero::MaxJobs<T> J{};
+    J.job[0] = {u0, p->nu, bits + aero::SC_MAXU};
+    J.job[1] = {v0, p->nv, bits + aero::SC_MAXV};
+    AERO_CUDA_TRY(aero::launch_absmax_multi<T>(J, 2, s));
     if (les) {
       StageParams<T> N = S;
       N.up = u0;

@@ -216,8 +216,18 @@ template <typename T>
 cudaError_t launch_copy_u(const T *, T *, int, int, int, int, unsigned long long *, cudaStream_t);
 template <typename T> cudaError_t launch_dt(const DtParams &, cudaStream_t);
 template <typename T>
-cudaError_t launch_absmax2(const T *, size_t, unsigned long long *, const T *, size_t, unsigned long long *,
-                           cudaStream_t);
+struct MaxJob {
+  const T *a;
+  size_t n;
+  unsigned long long *out;
+};
+template <typename T>
+struct MaxJobs {
+  MaxJob<T> job[3];
+  int vec;
+};
+// max |a| of up to three arrays (ordered bit patterns, atomics), one launch
+template <typename T> cudaError_t launch_absmax_multi(const MaxJobs<T> &, int njobs, cudaStream_t);
 template <typename T> cudaError_t launch_fan_begin(const FanBeginParams<T> &, cudaStream_t);
 // div -= m on every port's cells (physics.py:1043-1047)
 template <typename T>

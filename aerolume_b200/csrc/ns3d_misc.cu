@@ -24,19 +24,40 @@ __global__ void absmax_kernel(const T *__restrict__ a, size_t n, unsigned long l
   block_max_atomic<T>(m, out);
 }
 
-// max |a| and max |b| in one launch (blockIdx.y selects the array)
+// max |a| of up to three arrays in one launch (blockIdx.y selects the array), 16-byte vector
+// loads when every array starts on a 16-byte boundary
 template <typename T>
-__global__ void absmax2_kernel(const T *__restrict__ a, size_t na, unsigned long long *out_a, const T *__restrict__ b,
-                               size_t nb, unsigned long long *out_b) {
+__global__ void __launch_bounds__(512) absmax_multi_kernel(const MaxJobs<T> J) {
   aero::pdl_wait();
-  const T *x = blockIdx.y == 0 ? a : b;
-  const size_t n = blockIdx.y == 0 ? na : nb;
+  const MaxJob<T> &q = J.job[blockIdx.y];
+  const size_t stride = (size_t)gridDim.x * blockDim.x, start = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   T m = T(0);
-  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
-    const T v = fabs(x[e]);
+  auto take = [&](T x) {
+    const T v = fabs(x);
     m = (v > m || v != v) ? v : m;
+  };
+  size_t done = 0;
+  if (J.vec) {
+    if constexpr (sizeof(T) == 4) {
+      const float4 *a4 = reinterpret_cast<const float4 *>(q.a);
+      const size_t nv = q.n / 4;
+      for (size_t e = start; e < nv; e += stride) {
+        const float4 x = __ldg(a4 + e);
+        take(x.x), take(x.y), take(x.z), take(x.w);
+      }
+      done = nv * 4;
+    } else {
+      const double2 *a2 = reinterpret_cast<const double2 *>(q.a);
+      const size_t nv = q.n / 2;
+      for (size_t e = start; e < nv; e += stride) {
+        const double2 x = __ldg(a2 + e);
+        take(x.x), take(x.y);
+      }
+      done = nv * 2;
+    }
   }
-  block_max_atomic<T>(m, blockIdx.y == 0 ? out_a : out_b);
+  for (size_t e = done + start; e < q.n; e += stride) take(__ldg(q.a + e));
+  block_max_atomic<T>(m, q.out);
 }
 
 // u0 (rows of nx + 1) into the stage-start buffer with a 16-byte row pitch, with max |u0|.
@@ -573,11 +594,18 @@ cudaError_t launch_absmax(const T *a, size_t n, unsigned long long *out, cudaStr
 }
 
 template <typename T>
-cudaError_t launch_absmax2(const T *a, size_t na, unsigned long long *out_a, const T *b, size_t nb,
-                           unsigned long long *out_b, cudaStream_t s) {
-  const size_t n = na > nb ? na : nb;
-  const int blocks = (int)std::min<size_t>((n + 1023) / 1024, 148);
-  (void)aero::launch_k(absmax2_kernel<T>, dim3(blocks, 2), 1024, 0, s, a, na, out_a, b, nb, out_b);
+cudaError_t launch_absmax_multi(const MaxJobs<T> &J, int njobs, cudaStream_t s) {
+  if (njobs <= 0) return cudaSuccess;
+  size_t n = 0;
+  MaxJobs<T> K = J;
+  K.vec = 1;
+  for (int q = 0; q < njobs; ++q) {
+    n = std::max(n, J.job[q].n);
+    if (reinterpret_cast<uintptr_t>(J.job[q].a) % 16) K.vec = 0;
+  }
+  const size_t per = K.vec ? 512 * (16 / sizeof(T)) : 512;
+  const int blocks = (int)std::max<size_t>(1, std::min<size_t>((n + per - 1) / per, 148 * 4 / (size_t)njobs));
+  (void)aero::launch_k(absmax_multi_kernel<T>, dim3(blocks, njobs), 512, 0, s, K);
   return cudaGetLastError();
 }
 
@@ -668,8 +696,7 @@ cudaError_t launch_psi_accumulate(const T *psi, T *pw, size_t n, T wgt, int mode
 
 #define INSTANTIATE(T)                                                                                               \
   template cudaError_t launch_absmax<T>(const T *, size_t, unsigned long long *, cudaStream_t);                     \
-  template cudaError_t launch_absmax2<T>(const T *, size_t, unsigned long long *, const T *, size_t,                 \
-                                         unsigned long long *, cudaStream_t);                                        \
+  template cudaError_t launch_absmax_multi<T>(const MaxJobs<T> &, int, cudaStream_t);                              \
   template cudaError_t launch_dt<T>(const DtParams &, cudaStream_t);                                                \
   template cudaError_t launch_fan_begin<T>(const FanBeginParams<T> &, cudaStream_t);                                \
   template cudaError_t launch_copy_u<T>(const T *, T *, int, int, int, int, unsigned long long *, cudaStream_t);                                                \

@@ -167,7 +167,7 @@ def launches_per_step(plan):
     c = plan.cfg
     tunnel = not c.periodic[0] and not c.closed
     les = c.les != 0
-    n = 3 + (1 if c.thermal else 0)                # |u|, |v|, |w|, |theta| maxima
+    n = 2                                           # u copy with max |u|; max |v|, |w| (|theta|) in one launch
     n += 1                                          # dt
     n += 1 if tunnel else 0                         # inlet / u0 outlet sums
     # a power-of-two x axis folds the divergence into the first transform pass and the
