@@ -202,3 +202,24 @@ def geom_np(geom, npd):
     for n in ("chi_u", "chi_v", "chi_w", "chi_c", "a_u", "a_v", "a_w", "k_u", "k_v", "k_w"):
         setattr(g, n, np.asarray(getattr(geom, n), npd))
     return g
+
+
+def _unaligned(x):
+    """A contiguous copy of x whose storage starts 4 bytes past a 16-byte boundary."""
+    buf = torch.empty(x.numel() + 4, device=x.device, dtype=x.dtype)
+    y = buf[1:1 + x.numel()].view(x.shape)
+    y.copy_(x)
+    return y
+
+
+def test_inputs_off_a_16_byte_boundary_give_the_same_step():
+    """Caller tensors that do not start on a 16-byte boundary take the synchronous plane
+    loader and the scalar maxima instead of TMA and vector loads; the step is the same."""
+    meta, plan, ins, arr = _plan_and_inputs("tunnel_wale_heat_smoke_f32")
+    a = plan.step(ins["u0"], ins["v0"], ins["w0"], ins["t0"], theta0=ins["theta0"], dye0=ins["dye0"])
+    un = {k: _unaligned(v) for k, v in ins.items() if k in ("u0", "v0", "w0", "theta0", "dye0")}
+    assert all(t.data_ptr() % 16 for t in un.values())
+    b = plan.step(un["u0"], un["v0"], un["w0"], ins["t0"], theta0=un["theta0"], dye0=un["dye0"])
+    torch.cuda.synchronize()
+    for f in ("u", "v", "w", "p", "theta", "dye", "dt"):
+        assert _rel(b[f], a[f].double().cpu().numpy()) < 1e-6, f
