@@ -49,6 +49,8 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
+from aerolume_b200.replicas import gather_results, max_over_ranks, shard_instances  # noqa: E402
+
 METRIC = "Mcell-steps/s on 1 B200: plain vs batched vs learned closure, at stated error"
 UNIT = "Mcell-steps/s"
 SHAPE = (256, 128, 128)
@@ -244,10 +246,7 @@ def run_ours(args, rank, world, local_rank):
     ms = start.elapsed_time(end)
     clk = clocks.stop() if clocks else None
     status = plan.status()
-    if dist is not None:
-        tt = torch.tensor([ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
+    ms = max_over_ranks(ms, dist, dev)
     # ---- phase times from the events (mean over the K captured steps)
     def span(j, a, b):
         return ev[j][a].elapsed_time(ev[j][b])
@@ -290,11 +289,7 @@ def run_ours(args, rank, world, local_rank):
                 host_in[k], host_out[k] = host_out[k], host_in[k]
         e1.record()
         torch.cuda.synchronize()
-        ems = e0.elapsed_time(e1) / ke
-        if dist is not None:
-            tt = torch.tensor([ems], device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            ems = float(tt.item())
+        ems = max_over_ranks(e0.elapsed_time(e1) / ke, dist, dev)
         e2e = {"value": world * cells / (ems * 1e-3) / 1e6, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "ms_per_step": ems, "steps": ke}
     if rank != 0:
@@ -367,11 +362,7 @@ def _time_graph(g, dist, local_rank, rank, dev):
         dist.barrier()
     ms = start.elapsed_time(end)
     clk = clocks.stop() if clocks else None
-    if dist is not None:
-        tt = torch.tensor([ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
-    return ms, clk
+    return max_over_ranks(ms, dist, dev), clk
 
 
 def oracle2d_sample(ops, geom, steps, seed=0):
@@ -491,7 +482,12 @@ def run_sweep(args, rank, world, local_rank):
         import torch.distributed as dist
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    insts = sweep_instances(64, seed=0)
+    all_insts = sweep_instances(64, seed=0)
+    if args.shard:  # the 64 instances split over the ranks (strong scaling), else every rank runs all 64
+        mine = shard_instances([o.nx * o.ny for o, _, _ in all_insts], world)[rank]
+    else:
+        mine = list(range(len(all_insts)))
+    insts = [all_insts[k] for k in mine]
     plans, states = [], []
     for k, (ops, geom, _) in enumerate(insts):
         plan = Ns2dPlan(ops, geom, device=dev)
@@ -542,6 +538,10 @@ def run_sweep(args, rank, world, local_rank):
                     one(k)
     main.wait_stream(s)
     ms_loop, _ = _time_graph(gl, dist, local_rank, rank, dev)
+    # per-instance results (lift and drag after the timed steps) gathered to rank 0
+    coeffs = {mine[k]: [float(x) for x in states[k][3]["coeffs"].reshape(-1)[:2].tolist()] for k in range(len(plans))}
+    coeffs = gather_results(coeffs, dist)
+    total_cells = sum(o.nx * o.ny for o, _, _ in all_insts) if args.shard else world * cells
     if rank != 0:
         return
     peak, peak_kind = _peaks()
@@ -556,14 +556,17 @@ def run_sweep(args, rank, world, local_rank):
     grids = {}
     for o, _, _ in insts:
         grids[f"{o.nx}x{o.ny}"] = grids.get(f"{o.nx}x{o.ny}", 0) + 1
-    line = {"metric": METRIC, "value": world * cells * K / (ms * 1e-3) / 1e6, "unit": UNIT, "n_gpus": world,
-            "steps": K, "warmup": args.warmup, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
+    line = {"metric": METRIC, "value": total_cells * K / (ms * 1e-3) / 1e6, "unit": UNIT, "n_gpus": world,
+            "steps": K, "warmup": args.warmup, "ms_per_step": ms / K, "higher_is_better": True,
+            "scaling": "strong" if args.shard else "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "batched sweep: 64 NACA 4-digit airfoils, seeded grids 256x128..1024x512 FP32, "
                                    "upwind3, CFL 0.5, no LES", "cells": cells, "grids": grids,
                        "inputs_vs_l2": f"{cells * 4 * 10 / 1e6:.0f} MB of state + workspace > 126 MB L2 (no flush)",
-                       "parallelism": "replicas", "graph": f"{K} sweep steps (64 instances each) over 16 streams, 1 replay"},
-            "looped": {"value": world * cells * K / (ms_loop * 1e-3) / 1e6, "unit": UNIT, "ms_per_step": ms_loop / K,
+                       "parallelism": "instances sharded over the ranks" if args.shard else "replicas",
+                       "graph": f"{K} sweep steps (64 instances each) over 16 streams, 1 replay"},
+            "instances": len(coeffs), "instances_per_rank": len(mine) if not args.shard else "size-balanced shard",
+            "looped": {"value": total_cells * K / (ms_loop * 1e-3) / 1e6, "unit": UNIT, "ms_per_step": ms_loop / K,
                        "how": "the same plans one after another on one stream, one graph"},
             "roofline": {"bound": "hbm", "kernel": "whole sweep step", "achieved": alg / (ms / K * 1e-3) / 1e9,
                          "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
@@ -745,6 +748,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--shape", type=int, nargs=3, default=list(SHAPE), help="nx ny nz (2:1:1)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--shard", action="store_true",
+                    help="sweep2d with N > 1: split the 64 instances over the ranks instead of replicating them")
     args = ap.parse_args()
     if args.steps is None:
         args.steps = {"box3d": 20, "cylinder2d": 400, "sweep2d": 10, "fields3d": 20}[args.workload]
