@@ -7,7 +7,7 @@ calls into it.
 It restates, in numpy, the reference's plain 2D step (Aerolume ``src/aerolume/solvers/ns2d``)
 for the configurations the sm_100a kernels implement (tunnel, closed and periodic domains,
 slip / no-slip / moving walls, upwind3 or central advection, Smagorinsky / WALE / Vreman,
-immersed bodies, inlet-comb dye; no placed physics):
+immersed bodies, inlet-comb dye) and heat transfer (no other placed physics):
 
 * ``step2d``            core.py:815-969   SSP-RK3 with a projection after every stage
 * ``pad_u`` / ``pad_v`` core.py:284-325   two ghost layers
@@ -21,6 +21,9 @@ immersed bodies, inlet-comb dye; no placed physics):
 * ``cfl_dt2d``          core.py:685-696
 * ``advect_dye2d``      core.py:703-735, 779-792
 * ``PoissonSolver2D``   poisson.py:93-144 (the same exact solve in the orthonormal eigenbases)
+* heat transfer         physics.py:623-639, 696-794, 833-923; scalar.py:34-183; core.py:774-813,
+                        974-1000: bounded theta transport, diffusion with wall modes, insulated and
+                        heat-flux bodies, temperature-body penalisation, buoyancy, dt limit, report
 
 Parity is pinned: ``tests/test_oracle2d_golden.py`` checks this module against golden
 vectors that ``tests/golden/make_golden2d.py`` produced by running the reference itself.
@@ -198,6 +201,7 @@ def sgs_divergence2d(U, V, geom, ops):
         nut = nut.copy()
         nut[j0 + 1:j1 + 1, i0 + 1:i1 + 1] = nut[j0 + 1:j1 + 1, i0 + 1:i1 + 1] * (T(1.0) - geom.chi_c)
     q = T(0.25)
+    sgs_divergence2d.nut = nut                     # the field, for the heat equation's diffusivity
     nut_k = (((nut[:-1, :-1] + nut[1:, :-1]) + nut[:-1, 1:]) + nut[1:, 1:]) * q
     txx = T(2.0) * nut[1:ny + 1] * g11[1:ny + 1]
     tyy = T(2.0) * nut[:, 1:nx + 1] * g22[:, 1:nx + 1]
@@ -427,3 +431,299 @@ def step2d(u0, v0, t, geom, ops, poisson, *, dye=None, dt=None):
         new_dye = zero_dye_in_solids(advect_dye2d(dye, up, vp, dt, ops), geom)
     return StepResult2D(up, vp, p, np.asarray(t + dt, dtype=u0.dtype), np.asarray(dt, dtype=u0.dtype), coeffs,
                         new_dye)
+
+
+# ---------------------------------------------------------------------------
+# heat transfer (physics.py:623-923, scalar.py:34-183, core.py:774-1000)
+# ---------------------------------------------------------------------------
+
+@dataclass
+class Thermal2D:
+    """The thermal part of the reference's 2D ``Physics`` (physics.py:305-322) and the
+    bodies' ``ThermalGeometry`` (geometry.py:120-158); arrays on the body window."""
+    kappa: float
+    ri: float
+    prt: float
+    gravity: tuple
+    eta_t: float
+    theta_in: float
+    wall_modes: tuple
+    wall_values: tuple
+    diff_coef: float
+    temp_ids: tuple = ()
+    flux_ids: tuple = ()
+    chi_t: np.ndarray | None = None
+    a_t: np.ndarray | None = None
+    w_t: np.ndarray | None = None
+    ins_u: np.ndarray | None = None
+    ins_v: np.ndarray | None = None
+    q_skin: np.ndarray | None = None
+    w_f: np.ndarray | None = None
+    vol_u: np.ndarray | None = None
+    vol_v: np.ndarray | None = None
+
+
+def _van_leer_scalar(a, b):
+    """scalar.py:34-39: 2ab / (a + b) where ab > 0, else 0."""
+    ab = a * b
+    out = np.zeros_like(ab)
+    m = ab > 0
+    out[m] = a.dtype.type(2.0) * ab[m] / (a + b)[m]
+    return out
+
+
+def tvd_fluxes(c, u, v, ops, inflow):
+    """MUSCL / van Leer advective fluxes u c, v c (scalar.py:63-84)."""
+    T = c.dtype.type
+    half = T(0.5)
+    if ops.periodic:
+        cx = np.concatenate([c[:, -2:], c, c[:, :2]], axis=1)
+        cy = np.concatenate([c[-2:], c, c[:2]], axis=0)
+    else:
+        right = np.repeat(c[:, -1:], 2, axis=1)
+        left = np.repeat(c[:, :1], 2, axis=1) if ops.closed else np.full_like(right, T(inflow))
+        cx = np.concatenate([left, c, right], axis=1)
+        cy = np.concatenate([np.repeat(c[:1], 2, axis=0), c, np.repeat(c[-1:], 2, axis=0)], axis=0)
+    s = _van_leer_scalar(cx[:, 1:-1] - cx[:, :-2], cx[:, 2:] - cx[:, 1:-1])
+    left = cx[:, 1:-2] + half * s[:, :-1]
+    right = cx[:, 2:-1] - half * s[:, 1:]
+    fx = u * np.where(u > 0, left, right)
+    s = _van_leer_scalar(cy[1:-1] - cy[:-2], cy[2:] - cy[1:-1])
+    low = cy[1:-2] + half * s[:-1]
+    high = cy[2:-1] - half * s[1:]
+    fy = v * np.where(v > 0, low, high)
+    return fx, fy
+
+
+def flux_divergence(fx, fy, h):
+    """-(div F) at the cells (scalar.py:87-89)."""
+    return (((fx[:, :-1] - fx[:, 1:]) + fy[:-1]) - fy[1:]) * fx.dtype.type(1.0 / h)
+
+
+def face_average_x(q, ops):
+    T = q.dtype.type
+    mid = T(0.5) * (q[:, 1:] + q[:, :-1])
+    if ops.periodic:
+        w = T(0.5) * (q[:, :1] + q[:, -1:])
+        return np.concatenate([w, mid, w], axis=1)
+    return np.concatenate([q[:, :1], mid, q[:, -1:]], axis=1)
+
+
+def face_average_y(q, ops):
+    T = q.dtype.type
+    mid = T(0.5) * (q[1:] + q[:-1])
+    if ops.periodic:
+        w = T(0.5) * (q[:1] + q[-1:])
+        return np.concatenate([w, mid, w], axis=0)
+    return np.concatenate([q[:1], mid, q[-1:]], axis=0)
+
+
+def diffusive_fluxes(c, kx, ky, ops, modes, values):
+    """F = -kappa grad c with the wall conditions on the boundary faces (scalar.py:100-146)."""
+    T = c.dtype.type
+    inv_h, inv_half = T(1.0 / ops.h), T(2.0 / ops.h)
+    kx_a, ky_a = np.ndim(kx) > 0, np.ndim(ky) > 0
+    kxi = kx[:, 1:-1] if kx_a else kx
+    kyi = ky[1:-1] if ky_a else ky
+    fxi = -(kxi * (c[:, 1:] - c[:, :-1])) * inv_h
+    fyi = -(kyi * (c[1:] - c[:-1])) * inv_h
+    kl = kx[:, :1] if kx_a else kx
+    kr = kx[:, -1:] if kx_a else kx
+    kb = ky[:1] if ky_a else ky
+    kt = ky[-1:] if ky_a else ky
+    first_x, last_x, first_y, last_y = c[:, :1], c[:, -1:], c[:1], c[-1:]
+
+    def side(mode, k, inner, value, sign, wrap):
+        if mode in ("temperature", "inlet"):
+            return (T(-sign) * inv_half) * k * (inner - T(value))
+        if mode == "heat_flux":
+            return (T(sign) * k) * T(value) * np.ones_like(inner)
+        if mode == "periodic":
+            return wrap
+        return np.zeros_like(inner)
+
+    wrap_x = -(kl * (first_x - last_x)) * inv_h if modes[0] == "periodic" else None
+    wrap_y = -(kb * (first_y - last_y)) * inv_h if modes[2] == "periodic" else None
+    fl = side(modes[0], kl, first_x, values[0], 1.0, wrap_x)
+    fr = side(modes[1], kr, last_x, values[1], -1.0, wrap_x)
+    fb = side(modes[2], kb, first_y, values[2], 1.0, wrap_y)
+    ft = side(modes[3], kt, last_y, values[3], -1.0, wrap_y)
+    fl, fr = (np.broadcast_to(x, (c.shape[0], 1)) for x in (fl, fr))
+    fb, ft = (np.broadcast_to(x, (1, c.shape[1])) for x in (fb, ft))
+    return np.concatenate([fl, fxi, fr], axis=1), np.concatenate([fb, fyi, ft], axis=0)
+
+
+def theta_rhs2d(th, u, v, nut, geom, tp, ops):
+    """Tendency of theta: bounded advection, diffusion with kappa (+ nu_t / Pr_t), insulated
+    bodies, wall conditions, heat-flux skins (physics.py:696-730, without heaters or vents)."""
+    T = th.dtype.type
+    ny, nx = th.shape
+    fx, fy = tvd_fluxes(th, u, v, ops, tp.theta_in)
+    lt = flux_divergence(fx, fy, ops.h)
+    kappa = T(tp.kappa)
+    insulated = tp.ins_u is not None and not geom.empty
+    if nut is not None:
+        nc = nut[1:-1, 1:-1] * T(1.0 / tp.prt)
+        kx = kappa + face_average_x(nc, ops)
+        ky = kappa + face_average_y(nc, ops)
+    elif insulated:
+        kx = np.full((ny, nx + 1), kappa, dtype=th.dtype)
+        ky = np.full((ny + 1, nx), kappa, dtype=th.dtype)
+    else:
+        kx = ky = kappa
+    if insulated:
+        j0, j1, i0, i1 = geom.window
+        kx = kx.copy()
+        ky = ky.copy()
+        kx[j0:j1, i0:i1 + 1] = kx[j0:j1, i0:i1 + 1] * tp.ins_u
+        ky[j0:j1 + 1, i0:i1] = ky[j0:j1 + 1, i0:i1] * tp.ins_v
+    Fx, Fy = diffusive_fluxes(th, kx, ky, ops, tp.wall_modes, tp.wall_values)
+    lt = lt + flux_divergence(Fx, Fy, ops.h)
+    if tp.flux_ids and not geom.empty:
+        j0, j1, i0, i1 = geom.window
+        lt = lt.copy()
+        lt[j0:j1, i0:i1] = lt[j0:j1, i0:i1] + kappa * tp.q_skin
+    return lt
+
+
+def penalise_theta2d(th, geom, tp, bdt):
+    """Implicit penalisation toward the temperature bodies; their heat (physics.py:733-757)."""
+    T = th.dtype.type
+    if not tp.temp_ids or geom.empty:
+        return th, None
+    k = T(bdt / T(tp.eta_t))
+    j0, j1, i0, i1 = geom.window
+    tw = th[j0:j1, i0:i1]
+    tn = (tw + k * tp.a_t) / (T(1.0) + k * tp.chi_t)
+    heat = np.einsum("bij,ij->b", tp.w_t.astype(np.float64), (tn - tw).astype(np.float64))
+    th = th.copy()
+    th[j0:j1, i0:i1] = tn
+    return th, heat
+
+
+def buoyancy2d(theta, tp, ops):
+    """-Ri theta g on the faces, zero on the boundary faces of a bounded domain (physics.py:623-637)."""
+    T = theta.dtype.type
+    gx, gy = tp.gravity
+    fu = fv = None
+    if gy != 0.0:
+        tv = face_average_y(theta, ops)
+        if not ops.periodic:
+            tv = tv.copy()
+            tv[0] = 0
+            tv[-1] = 0
+        fv = tv * T(T(tp.ri) * T(-gy))
+    if gx != 0.0:
+        tu = face_average_x(theta, ops)
+        if not ops.periodic:
+            tu = tu.copy()
+            tu[:, 0] = 0
+            tu[:, -1] = 0
+        fu = tu * T(T(tp.ri) * T(-gx))
+    return fu, fv
+
+
+def physics_dt_limit2d(dt, u, v, theta, nut_max, tp, ops):
+    """The bounded temperature step and the buoyant free-fall limit (physics.py:851-884)."""
+    T = u.dtype.type
+    kap = T(tp.kappa) if nut_max is None else T(tp.kappa) + nut_max * T(1.0 / tp.prt)
+    speed = max(np.abs(u).max() + np.abs(v).max(), T(0.0))
+    rate = speed * T(2.0 / ops.h) + kap * T(tp.diff_coef / (ops.h * ops.h))
+    dt = min(dt, T(1.0) / rate)
+    acc = T(abs(tp.ri)) * np.abs(theta).max()
+    return min(dt, T(ops.cfl) * np.sqrt(T(ops.h) / max(acc, T(1e-12))))
+
+
+def heat_report2d(old_theta, new_theta, new_u, heat_acc, geom, tp, ops, dt):
+    """The step's heat outputs (core.py:974-995, physics.py:760-794)."""
+    T = new_theta.dtype.type
+    h = ops.h
+    h2 = T(h * h)
+    out = {}
+    if tp.temp_ids and not geom.empty:
+        out["heat"] = heat_acc * float(h2 / dt)
+    if tp.flux_ids and not geom.empty:
+        j0, j1, i0, i1 = geom.window
+        out["theta_wall"] = np.einsum("bij,ij->b", tp.w_f.astype(np.float64), new_theta[j0:j1, i0:i1].astype(np.float64))
+    k = T(tp.kappa)
+    first = (new_theta[:, 0], new_theta[:, -1], new_theta[0, :], new_theta[-1, :])
+    rates = []
+    for i, mode in enumerate(tp.wall_modes):
+        if mode in ("temperature", "inlet"):
+            rates.append(float((T(2.0) * k) * (T(tp.wall_values[i]) - first[i]).sum()))
+        elif mode == "heat_flux":
+            rates.append(float(k * T(tp.wall_values[i]) * T(first[i].size * h)))
+        else:
+            rates.append(0.0)
+    out["wall_heat"] = np.array(rates)
+    out["heat_storage"] = np.array([float((new_theta.sum() - old_theta.sum()) * (h2 / dt))])
+    if ops.periodic or ops.closed:
+        out["flow_heat"] = np.zeros(2)
+    else:
+        out["flow_heat"] = np.array([float((new_u[:, 0] * T(tp.theta_in)).sum() * T(h)),
+                                     float((new_u[:, -1] * new_theta[:, -1]).sum() * T(h))])
+    return out
+
+
+def step2d_thermal(u0, v0, t, theta0, geom, ops, poisson, tp, *, dt=None):
+    """One SSP-RK3 step with heat transfer (core.py:815-969 with a thermal Physics): the
+    momentum of step2d plus theta transport, buoyancy after the penalisation (its solid share
+    booked against the body force), theta penalisation, and the heat report."""
+    T = u0.dtype.type
+    up, vp, thp = u0, v0, theta0
+    acc_u = acc_v = psi_w = heat_acc = None
+    les = ops.turbulence != "none"
+    for s, ((a, b), w) in enumerate(zip(SSP_RK3, FORCE_WEIGHTS)):
+        lu, lv, nut_max = momentum_rhs2d(up, vp, geom, ops)
+        nut = sgs_divergence2d.nut if les else None
+        if s == 0 and dt is None:
+            if ops.dt_fixed is not None:
+                dt = T(ops.dt_fixed)
+            else:
+                dt = cfl_dt2d(u0, v0, ops, nut_max)
+                dt = physics_dt_limit2d(dt, u0, v0, theta0, nut_max, tp, ops)
+        dt = T(dt)
+        lt = theta_rhs2d(thp, up, vp, nut, geom, tp, ops)
+        bdt = dt * T(b)
+        if a == 0.0:
+            uh = up + lu * bdt
+            vh = vp + lv * bdt
+            thh = thp + lt * bdt
+        else:
+            uh = lerp(up, u0, a) + lu * bdt
+            vh = lerp(vp, v0, a) + lv * bdt
+            thh = lerp(thp, theta0, a) + lt * bdt
+        if not ops.periodic:
+            uh = inlet_outlet(uh, ops)
+        if not geom.empty:
+            uh, vh, du, dv = penalise2d(uh, vh, geom, ops, bdt)
+            acc_u = du * T(w) if acc_u is None else acc_u + du * T(w)
+            acc_v = dv * T(w) if acc_v is None else acc_v + dv * T(w)
+        if tp.ri != 0.0:  # core.py:774-813
+            fu, fv = buoyancy2d(thp, tp, ops)
+            if fu is not None:
+                uh = uh + bdt * fu
+            if fv is not None:
+                vh = vh + bdt * fv
+            if not geom.empty:
+                j0, j1, i0, i1 = geom.window
+                vu = tp.vol_u if tp.vol_u is not None else geom.chi_u
+                vv = tp.vol_v if tp.vol_v is not None else geom.chi_v
+                if fu is not None:
+                    acc_u = acc_u + fu[j0:j1, i0:i1 + 1] * vu * T(bdt * T(w))
+                if fv is not None:
+                    acc_v = acc_v + fv[j0:j1 + 1, i0:i1] * vv * T(bdt * T(w))
+        if ops.periodic and not geom.empty:
+            uh, vh = apply_boundary_values(uh, vh, ops)
+        thh, heat = penalise_theta2d(thh, geom, tp, bdt)
+        if heat is not None:
+            heat_acc = heat * float(T(w)) if heat_acc is None else heat_acc + heat * float(T(w))
+        thp = thh
+        up, vp, psi = project2d(uh, vh, ops, poisson)
+        psi_w = psi * T(w) if psi_w is None else psi_w + T(w) * psi
+    p = psi_w * (T(1.0) / dt)
+    coeffs = force_coefficients2d(acc_u, acc_v, geom, ops, dt)
+    res = StepResult2D(up, vp, p, np.asarray(t + dt, dtype=u0.dtype), np.asarray(dt, dtype=u0.dtype), coeffs)
+    res.theta = thp
+    res.report = heat_report2d(theta0, thp, up, heat_acc, geom, tp, ops, dt)
+    return res

@@ -113,3 +113,18 @@ def load_fields_case(tag):
     ops, geom = ops_from_meta(meta, arr)
     ops.x0, ops.y0, ops.z0 = meta["origin"]
     return meta, ops, geom, arr
+
+
+def thermal2d_from_case(meta, arr):
+    """The oracle's Thermal2D of a 2D golden case with heat transfer (None without)."""
+    from oracle.ns2d import Thermal2D
+    t = meta.get("thermal")
+    if t is None:
+        return None
+    dt = np.float64 if meta["dtype"] == "float64" else np.float32
+    g = {n: (arr["th_" + n].astype(dt) if "th_" + n in arr else None)
+         for n in ("chi_t", "a_t", "w_t", "ins_u", "ins_v", "q_skin", "w_f", "vol_u", "vol_v")}
+    return Thermal2D(kappa=t["kappa"], ri=t["ri"], prt=t["prt"], gravity=tuple(t["gravity"]), eta_t=t["eta_t"],
+                     theta_in=t["theta_in"], wall_modes=tuple(t["wall_modes"]), wall_values=tuple(t["wall_values"]),
+                     diff_coef=t["diff_coef"], temp_ids=tuple(t.get("temp_ids", ())),
+                     flux_ids=tuple(t.get("flux_ids", ())), **g)

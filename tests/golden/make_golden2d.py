@@ -28,7 +28,7 @@ REF = Path(os.environ.get("AEROLUME_REF", "/root/reference"))
 sys.path.insert(0, str(REF / "src"))
 
 from aerolume.solvers.ns2d import core  # noqa: E402
-from aerolume.solvers.ns2d.config import ImmersedBody, SolverConfig  # noqa: E402
+from aerolume.solvers.ns2d.config import ImmersedBody, SolverConfig, ThermalConfig, WallBC  # noqa: E402
 from aerolume.solvers.ns2d.geometry import build_geometry  # noqa: E402
 from aerolume.solvers.ns2d.poisson import PoissonSolver  # noqa: E402
 
@@ -62,10 +62,24 @@ def extract(ops, geom):
     if not geom.empty:
         for name in ("chi_u", "chi_v", "chi_c", "a_u", "a_v", "k_u", "k_v"):
             arrays[name] = _np(getattr(geom, name))
+    ph = ops.phys
+    if ph is not None and ph.thermal:
+        meta["thermal"] = {"kappa": float(ph.kappa), "ri": float(ph.ri), "prt": ph.prt, "gravity": list(ph.gravity),
+                           "eta_t": float(ph.eta_t), "theta_in": float(ph.theta_in),
+                           "wall_modes": list(ph.wall_modes), "wall_values": [float(x) for x in ph.wall_values],
+                           "diff_coef": ph.diff_coef}
+        tg = geom.thermal
+        if tg is not None and not geom.empty:
+            meta["thermal"]["temp_ids"] = list(tg.temp_ids)
+            meta["thermal"]["flux_ids"] = list(tg.flux_ids)
+            for name in ("chi_t", "a_t", "w_t", "ins_u", "ins_v", "q_skin", "w_f", "vol_u", "vol_v"):
+                val = getattr(tg, name)
+                if val is not None:
+                    arrays["th_" + name] = _np(val)
     return meta, arrays
 
 
-def run_case(name, cfg_kw, *, dtype="float64", amp=0.1, seed=1, steps=1):
+def _run_case(name, cfg_kw, *, dtype="float64", amp=0.1, seed=1, steps=1):
     cfg64 = SolverConfig(**{**cfg_kw, "dtype": "float64", "device": "cpu", "perturb": False})
     cfg = SolverConfig(**{**cfg_kw, "dtype": dtype, "device": "cpu", "perturb": False})
     ops64 = core.make_operators(cfg64)
@@ -84,26 +98,38 @@ def run_case(name, cfg_kw, *, dtype="float64", amp=0.1, seed=1, steps=1):
         dye[dye < 0.3] = 0.0
         dye = dye.to(tdt)
     zero = torch.zeros((), dtype=tdt)
+    theta = None
+    if cfg.thermal is not None:
+        theta = (0.3 * torch.randn((cfg.ny, cfg.nx), generator=g, dtype=torch.float64)).to(tdt)
     state = core.State(u.to(tdt), v.to(tdt), torch.zeros(cfg.ny, cfg.nx, dtype=tdt), dye,
-                       torch.tensor(0.37, dtype=tdt), zero.clone())
+                       torch.tensor(0.37, dtype=tdt), zero.clone(), theta)
     meta, arrays = extract(ops, geom)
     arrays.update({"in_u": _np(state.u), "in_v": _np(state.v), "in_t": _np(state.t)})
     if dye is not None:
         arrays["in_dye"] = _np(dye)
+    if theta is not None:
+        arrays["in_theta"] = _np(theta)
     st = state
     with torch.no_grad():
         for k in range(steps):
-            st, coeffs = core.step_full(st, geom, ops)
+            rep = {}
+            st, coeffs = core.step_full(st, geom, ops, out=rep)
             if k == 0:
                 arrays.update({"out1_u": _np(st.u), "out1_v": _np(st.v), "out1_p": _np(st.p), "out1_t": _np(st.t),
                                "out1_dt": _np(st.dt), "out1_coeffs": _np(coeffs)})
                 if st.dye is not None:
                     arrays["out1_dye"] = _np(st.dye)
+                if st.theta is not None:
+                    arrays["out1_theta"] = _np(st.theta)
+                    for key, val in rep.items():
+                        arrays["out1_rep_" + key] = _np(val)
     meta["steps"] = steps
     if steps > 1:
         arrays.update({"outN_u": _np(st.u), "outN_v": _np(st.v), "outN_p": _np(st.p), "outN_t": _np(st.t)})
         if st.dye is not None:
             arrays["outN_dye"] = _np(st.dye)
+        if st.theta is not None:
+            arrays["outN_theta"] = _np(st.theta)
     store = {k: (np.asarray(x, dtype=np.float32) if dtype == "float32" and np.asarray(x).dtype == np.float64
                  else np.asarray(x)) for k, x in arrays.items()}
     np.savez_compressed(HERE / f"ns2d_{name}.npz", meta=np.array(json.dumps(meta)), **store)
@@ -130,6 +156,11 @@ def poisson_cases():
 
 def main():
     torch.set_num_threads(4)
+    names = sys.argv[1:]
+
+    def run_case(name, *a, **kw):
+        if not names or name in names:
+            _run_case(name, *a, **kw)
     # cylinder in a slip-walled tunnel (the shape of the 2D benchmark, coarser)
     cyl = ImmersedBody(circle(2.0, 2.0, 0.5, 64), name="cylinder")
     tunnel = {"nx": 64, "ny": 32, "h": 1.0 / 8.0, "x0": 0.0, "y0": 0.0, "re": 200.0, "bodies": [cyl],
@@ -157,7 +188,28 @@ def main():
                                               "bc_bottom": "moving", "ground_speed": 0.5, "advection": "central",
                                               "turbulence": "vreman", "dye": False, "moment_ref": (1.5, 1.0)},
              dtype="float64", amp=0.05, seed=4)
-    poisson_cases()
+    # heat transfer: a hot cylinder in a tunnel with buoyancy; a differentially heated cavity
+    # with an insulated block, a heat-flux body and WALE; a periodic box with a cold body
+    hot = ImmersedBody(circle(2.0, 2.0, 0.5, 64), name="hot", thermal="temperature", thermal_value=1.0)
+    heated = dict(tunnel, bodies=[hot], dye=False, thermal=ThermalConfig(prandtl=0.71, richardson=0.5))
+    run_case("cylinder_heated_f64", heated, dtype="float64", amp=0.05, seed=5, steps=3)
+    run_case("cylinder_heated_f32", heated, dtype="float32", amp=0.05, seed=5, steps=3)
+    ins = ImmersedBody(square(1.2, 1.2, 0.3), name="insulated", thermal="adiabatic")
+    flux = ImmersedBody(circle(2.8, 1.0, 0.25, 48), name="flux", thermal="heat_flux", thermal_value=0.8)
+    cavity = {"nx": 40, "ny": 24, "h": 0.1, "x0": 0.0, "y0": 0.0, "re": 1500.0, "bodies": [ins, flux],
+              "domain": "closed", "bc_bottom": "noslip", "bc_left": "noslip", "bc_right": "noslip",
+              "bc_top": "noslip", "turbulence": "wale", "dye": False, "moment_ref": (2.0, 1.2),
+              "thermal": ThermalConfig(prandtl=0.9, richardson=1.0, gravity=(0.3, -1.0),
+                                       walls=[WallBC("left", "temperature", 0.5), WallBC("right", "temperature", -0.5),
+                                              WallBC("bottom", "heat_flux", 0.3)])}
+    run_case("cavity_heated_wale_f64", cavity, dtype="float64", amp=0.1, seed=6, steps=3)
+    cold = ImmersedBody(square(1.0, 1.2, 0.4), name="cold", thermal="temperature", thermal_value=-0.5)
+    run_case("periodic_cold_body_f64", {"nx": 32, "ny": 24, "h": 2.5 / 32, "x0": 0.0, "y0": 0.0, "re": 600.0,
+                                        "bodies": [cold], "periodic": True, "dye": False, "moment_ref": (1.0, 1.2),
+                                        "thermal": ThermalConfig(prandtl=0.71, richardson=0.8)},
+             dtype="float64", amp=0.2, seed=7, steps=3)
+    if not names or "poisson" in names:
+        poisson_cases()
 
 
 if __name__ == "__main__":

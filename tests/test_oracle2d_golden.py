@@ -4,7 +4,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from _golden import CASES_2D, GOLDEN, load_case2d
+from _golden import CASES_2D, GOLDEN, load_case2d, thermal2d_from_case
 from oracle import ns2d as O2
 
 # float64: the restatement agrees with the reference to round-off; float32: to the FP32 step
@@ -22,9 +22,15 @@ def _run(name, steps=1):
     ps = O2.PoissonSolver2D(ops.nx, ops.ny, ops.h, ops.periodic, dt)
     u, v, t = arr["in_u"], arr["in_v"], arr["in_t"]
     dye = arr.get("in_dye")
+    tp = thermal2d_from_case(meta, arr)
+    theta = arr.get("in_theta")
     outs = []
     for _ in range(steps):
-        r = O2.step2d(u, v, t, geom, ops, ps, dye=dye)
+        if tp is not None:
+            r = O2.step2d_thermal(u, v, t, theta, geom, ops, ps, tp)
+            theta = r.theta
+        else:
+            r = O2.step2d(u, v, t, geom, ops, ps, dye=dye)
         outs.append(r)
         u, v, t, dye = r.u, r.v, r.t, r.dye
     return meta, arr, outs
@@ -34,6 +40,8 @@ def _run(name, steps=1):
 def test_oracle2d_one_step_matches_reference(name):
     meta, arr, (r,) = _run(name)
     tol = TOL[meta["dtype"]]
+    if "thermal" in meta and meta["dtype"] == "float32":
+        tol = 1e-5  # numpy's FP32 sums and limiter against torch's: round-off of the FP32 step
     for k, got in (("u", r.u), ("v", r.v), ("p", r.p)):
         assert _rel(got, arr[f"out1_{k}"]) < tol, (k, _rel(got, arr[f"out1_{k}"]))
     assert _rel(r.dt, arr["out1_dt"]) < tol
@@ -42,6 +50,12 @@ def test_oracle2d_one_step_matches_reference(name):
         assert _rel(r.coeffs, arr["out1_coeffs"]) < (1e-10 if meta["dtype"] == "float64" else 1e-4)
     if "out1_dye" in arr:
         assert _rel(r.dye, arr["out1_dye"]) < tol
+    if "out1_theta" in arr:
+        assert _rel(r.theta, arr["out1_theta"]) < tol, _rel(r.theta, arr["out1_theta"])
+        for key in [k[len("out1_rep_"):] for k in arr if k.startswith("out1_rep_")]:
+            ref = arr["out1_rep_" + key]
+            err = np.abs(np.asarray(r.report[key], np.float64) - ref).max() / max(1.0, np.abs(ref).max())
+            assert err < (1e-10 if meta["dtype"] == "float64" else 1e-4), (key, err)
 
 
 @pytest.mark.parametrize("name", [c for c in CASES_2D if c.startswith("cylinder")])
@@ -49,8 +63,9 @@ def test_oracle2d_three_steps_match_reference(name):
     meta, arr, outs = _run(name, steps=3)
     tol = 10 * TOL[meta["dtype"]]
     r = outs[-1]
-    for k, got in (("u", r.u), ("v", r.v), ("p", r.p), ("dye", r.dye)):
-        assert _rel(got, arr[f"outN_{k}"]) < tol, (k, _rel(got, arr[f"outN_{k}"]))
+    for k, got in (("u", r.u), ("v", r.v), ("p", r.p), ("dye", r.dye), ("theta", getattr(r, "theta", None))):
+        if f"outN_{k}" in arr:
+            assert _rel(got, arr[f"outN_{k}"]) < tol, (k, _rel(got, arr[f"outN_{k}"]))
 
 
 def test_poisson2d_matches_reference():
