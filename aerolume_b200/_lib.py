@@ -14,7 +14,7 @@ import os
 
 LIB_PATH = Path(__file__).resolve().parent / (
     "libaero_b200_checked.so" if os.environ.get("AERO_B200_CHECKED") == "1" else "libaero_b200.so")
-ABI_VERSION = 2
+ABI_VERSION = 3
 MAX_BODIES = 8
 MAX_FANS = 4
 MAX_PORTS = 4
@@ -27,6 +27,7 @@ ADV = {"upwind3": 0, "central": 1}
 LES = {"none": 0, "laminar": 0, "smagorinsky": 1, "wale": 2, "vreman": 3}
 GHOST = {"edge": 0, "even": 1, "odd": 2, "affine": 3, "face_odd": 4, "periodic_cell": 5, "periodic_face": 6}
 THETA_SIDE = {"periodic": 0, "outflow": 1, "adiabatic": 2, "inflow": 3, "temperature": 4, "heat_flux": 5}
+THETA2_MODE = {"adiabatic": 0, "temperature": 1, "heat_flux": 2, "inlet": 3, "outlet": 4, "periodic": 5}
 
 # every symbol include/aero_b200.h declares
 EXPORTS = ("aero_abi_version", "aero_last_error", "aero_ns3d_plan_create", "aero_ns3d_plan_destroy",
@@ -103,16 +104,23 @@ class Ns2dConfig(C.Structure):
         ("has_dt_fixed", C.c_int32), ("dt_fixed", C.c_double),
         ("ghost_kind", ((C.c_int32 * 2) * 2) * 2), ("ghost_val", ((C.c_double * 2) * 2) * 2),
         ("force_ref", C.c_double), ("window", C.c_int32 * 4), ("nbody", C.c_int32), ("dye", C.c_int32),
+        ("thermal", C.c_int32), ("kappa", C.c_double), ("ri", C.c_double), ("prt", C.c_double),
+        ("gravity", C.c_double * 2), ("eta_t", C.c_double), ("theta_in", C.c_double),
+        ("wall_mode", C.c_int32 * 4), ("wall_value", C.c_double * 4), ("diff_coef", C.c_double),
+        ("n_temp", C.c_int32), ("n_flux", C.c_int32), ("has_ins", C.c_int32), ("has_vol", C.c_int32),
     ]
 
 
 class Ns2dGeom(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in ("chi_u", "chi_v", "chi_c", "a_u", "a_v", "k_u", "k_v", "u_inlet",
-                                          "dye_inlet")]
+                                          "dye_inlet", "chi_t", "a_t", "w_t", "ins_u", "ins_v", "q_skin", "w_f",
+                                          "vol_u", "vol_v")]
 
 
 class Ns2dFields(C.Structure):
-    _fields_ = [(n, C.c_void_p) for n in ("u0", "v0", "t0", "dye0", "u", "v", "p", "t", "dt", "dye", "coeffs")]
+    _fields_ = [(n, C.c_void_p) for n in ("u0", "v0", "t0", "dye0", "u", "v", "p", "t", "dt", "dye", "coeffs",
+                                          "theta0", "theta", "heat", "theta_wall", "wall_heat", "heat_storage",
+                                          "flow_heat")]
 
 
 _LIB = None

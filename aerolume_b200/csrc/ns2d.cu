@@ -111,17 +111,38 @@ __device__ __forceinline__ T eddy2d(T g11, T g12, T g21, T g22, int model, T cfa
 
 // The step's dt (ns2d/core.py:686-695): given (mode 2), fixed (mode 1), or the CFL / viscous rule
 // on the maxima in the scalar block (mode 0), rounded through the field type as the reference.
+// Heat transfer's limits on dt (physics.py:851-884): the bounded temperature step and the
+// buoyant free-fall limit; on == 0 leaves dt alone.
+struct Dt2dThermal {
+  int on;
+  double kappa, inv_prt, two_over_h, diff_over_h2, abs_ri, cfl, h;
+};
+
 template <typename T>
 __device__ __forceinline__ T dt2d_value(int mode, const T *dt_in, double dt_fixed, const unsigned long long *bits,
-                                        double cfl_h, double nu, double visc_h2, int les) {
+                                        double cfl_h, double nu, double visc_h2, int les, const Dt2dThermal &th) {
   if (mode == 2) return *dt_in;
   if (mode == 1) return T(dt_fixed);
-  T umax = T(as_double(bits[SC_MAXU])) + T(as_double(bits[SC_MAXV]));
+  const T usum = T(as_double(bits[SC_MAXU])) + T(as_double(bits[SC_MAXV]));
+  T umax = usum;
   umax = umax > T(1e-6) || umax != umax ? umax : T(1e-6);
   T dt = T(cfl_h) / umax;
-  const T nut = les ? T(nu) + T(as_double(bits[SC_NUTMAX])) : T(nu);
+  const T nut_max = T(as_double(bits[SC_NUTMAX]));
+  const T nut = les ? T(nu) + nut_max : T(nu);
   const T dv = T(visc_h2) / nut;
-  return dv < dt ? dv : dt;
+  dt = dv < dt ? dv : dt;
+  if (th.on) {
+    const T kap = les ? T(th.kappa) + nut_max * T(th.inv_prt) : T(th.kappa);
+    const T speed = usum > T(0) || usum != usum ? usum : T(0);
+    const T rate = speed * T(th.two_over_h) + kap * T(th.diff_over_h2);
+    const T l1 = T(1) / rate;
+    dt = l1 < dt ? l1 : dt;
+    T acc = T(th.abs_ri) * T(as_double(bits[SC_MAXT]));
+    acc = acc > T(1e-12) || acc != acc ? acc : T(1e-12);
+    const T l2 = T(th.cfl) * sqrt(T(th.h) / acc);
+    dt = l2 < dt ? l2 : dt;
+  }
+  return dt;
 }
 
 template <typename T>
@@ -138,12 +159,21 @@ struct StageParams {
   int has_win, win[4];         // j0, j1, i0, i1
   const T *chi_u, *chi_v, *chi_c, *a_u, *a_v, *k_u, *k_v;
   T eta;
+  // heat transfer: buoyancy -Ri theta g on the faces from the stage-start theta, after the
+  // penalisation (core.py:774-813), with the solids' share (vol_u / vol_v, else chi) booked
+  // against the body force; nut_out (ny, nx) receives nu_t of the stage for the heat equation
+  const T *thp;
+  T ri_gx, ri_gy;              // Ri (-g_x), Ri (-g_y); 0: no buoyancy on that component
+  int buoy_u, buoy_v;
+  const T *vol_u, *vol_v;
+  T *nut_out;
   int nbody;
   double *partials;            // this stage's [block][4 nbody]
   unsigned long long *nut_max; // nu-only pass: max nu_t (ordered bits)
   // first stage: every block derives the step's dt (dt2d_value) and block (0, 0) stores it
   // in *dt_store for the kernels after it; otherwise dt is read from *dt
   int dt_here, dt_mode, dt_les;
+  Dt2dThermal dt_th;
   const T *dt_in;
   const unsigned long long *dt_bits;
   double dt_fixed, dt_cfl_h, dt_nu, dt_visc_h2;
@@ -166,7 +196,7 @@ __global__ void __launch_bounds__(NT) stage2d_kernel(const __grid_constant__ Sta
   const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
   const bool tunnel = !P.periodic && !P.closed;
   const T dt = P.dt_here ? dt2d_value<T>(P.dt_mode, P.dt_in, P.dt_fixed, P.dt_bits, P.dt_cfl_h, P.dt_nu, P.dt_visc_h2,
-                                         P.dt_les)
+                                         P.dt_les, P.dt_th)
                          : *P.dt;
   if (P.dt_here && blockIdx.x == 0 && blockIdx.y == 0 && tid == 0) *P.dt_store = dt;
   const T bdt = dt * P.b;
@@ -233,6 +263,8 @@ __global__ void __launch_bounds__(NT) stage2d_kernel(const __grid_constant__ Sta
         nu = nu * (T(1) - chi);
       }
       NU[r][c] = nu;
+      if (!NU_ONLY && P.nut_out && r >= 1 && r <= TY && c >= 1 && c <= TX && jc < ny && ic < nx)
+        P.nut_out[(size_t)jc * nx + ic] = nu;
       TXX[r][c] = T(2) * nu * g11;
       TYY[r][c] = T(2) * nu * g22;
       if (jc >= -1 && jc <= ny && ic >= -1 && ic <= nx) mx = (nu > mx || nu != nu) ? nu : mx;
@@ -258,7 +290,7 @@ __global__ void __launch_bounds__(NT) stage2d_kernel(const __grid_constant__ Sta
   const bool wblock = P.has_win && P.nbody > 0;
   double fq[4] = {0.0, 0.0, 0.0, 0.0};  // this thread's force sums of body `bsel`
   // ---- u-faces (j, i) and, for the last column, (j, nx)
-  auto u_face = [&](int fi, T &out, bool &pen, T &du, int &widx) {
+  auto u_face = [&](int fi, T &out, bool &pen, T &du, int &widx, T &sh) {
     const int r = j - j0 + 2, c = fi - i0 + 2;
     const T *row = U[r];
     const T fxl = face_flux<T>(row[c - 1] + row[c], row[c - 2], row[c - 1], row[c], row[c + 1], P.upwind != 0);
@@ -297,9 +329,18 @@ __global__ void __launch_bounds__(NT) stage2d_kernel(const __grid_constant__ Sta
       uh = un;
       pen = true;
     }
+    if (P.buoy_u) {  // face average of theta (0 on boundary faces of a bounded domain)
+      T tf;
+      const size_t tr = (size_t)j * nx;
+      if (fi > 0 && fi < nx) tf = T(0.5) * (P.thp[tr + fi] + P.thp[tr + fi - 1]);
+      else tf = P.periodic ? T(0.5) * (P.thp[tr] + P.thp[tr + nx - 1]) : T(0);
+      const T fu = tf * P.ri_gx;
+      uh = uh + bdt * fu;
+      if (pen) sh = fu * (P.vol_u ? P.vol_u[widx] : P.chi_u[widx]) * (bdt * P.w);
+    }
     out = uh;
   };
-  auto v_face = [&](int fj, T &out, bool &pen, T &dv, int &widx) {
+  auto v_face = [&](int fj, T &out, bool &pen, T &dv, int &widx, T &sh) {
     const int r = fj - j0 + 2, c = i - i0 + 2;
     const T usl = U[r - 1][c] + U[r][c], usr = U[r - 1][c + 1] + U[r][c + 1];
     const T *row = V[r];
@@ -327,29 +368,37 @@ __global__ void __launch_bounds__(NT) stage2d_kernel(const __grid_constant__ Sta
       vh = vn;
       pen = true;
     }
+    if (P.buoy_v) {
+      T tf;
+      if (fj > 0 && fj < ny) tf = T(0.5) * (P.thp[(size_t)fj * nx + i] + P.thp[(size_t)(fj - 1) * nx + i]);
+      else tf = P.periodic ? T(0.5) * (P.thp[i] + P.thp[(size_t)(ny - 1) * nx + i]) : T(0);
+      const T fv = tf * P.ri_gy;
+      vh = vh + bdt * fv;
+      if (pen) sh = fv * (P.vol_v ? P.vol_v[widx] : P.chi_v[widx]) * (bdt * P.w);
+    }
     out = vh;
   };
   // u faces of this thread: i, plus nx for the thread of i = nx - 1 (non-periodic)
-  T uv[2], du[2];
+  T uv[2], du[2], ush[2] = {T(0), T(0)};
   bool upen[2] = {false, false};
   int uidx[2] = {0, 0}, nuf = 0;
-  T vv[2], dv[2];
+  T vv[2], dv[2], vsh[2] = {T(0), T(0)};
   bool vpen[2] = {false, false};
   int vidx[2] = {0, 0}, nvf = 0;
   if (in) {
     // the last face of a row / column is computed everywhere; in a periodic domain its
     // penalisation increment counts towards the force, but the face itself then takes the
     // value of face 0 (core.py:330-331, 923-924)
-    u_face(i, uv[0], upen[0], du[0], uidx[0]);
+    u_face(i, uv[0], upen[0], du[0], uidx[0], ush[0]);
     nuf = 1;
     if (i == nx - 1) {
-      u_face(nx, uv[1], upen[1], du[1], uidx[1]);
+      u_face(nx, uv[1], upen[1], du[1], uidx[1], ush[1]);
       nuf = 2;
     }
-    v_face(j, vv[0], vpen[0], dv[0], vidx[0]);
+    v_face(j, vv[0], vpen[0], dv[0], vidx[0], vsh[0]);
     nvf = 1;
     if (j == ny - 1) {
-      v_face(ny, vv[1], vpen[1], dv[1], vidx[1]);
+      v_face(ny, vv[1], vpen[1], dv[1], vidx[1], vsh[1]);
       nvf = 2;
     }
     P.uh[(size_t)j * (nx + 1) + i] = uv[0];
@@ -369,13 +418,13 @@ __global__ void __launch_bounds__(NT) stage2d_kernel(const __grid_constant__ Sta
       fq[0] = fq[1] = fq[2] = fq[3] = 0.0;
       for (int q = 0; q < nuf; ++q)
         if (upen[q]) {
-          const double d = (double)(du[q] * wq);
+          const double d = (double)(du[q] * wq) + (double)ush[q];
           fq[0] += (double)P.k_u[(size_t)(2 * b) * su + uidx[q]] * d;
           fq[1] += (double)P.k_u[(size_t)(2 * b + 1) * su + uidx[q]] * d;
         }
       for (int q = 0; q < nvf; ++q)
         if (vpen[q]) {
-          const double d = (double)(dv[q] * wq);
+          const double d = (double)(dv[q] * wq) + (double)vsh[q];
           fq[2] += (double)P.k_v[(size_t)(2 * b) * sv + vidx[q]] * d;
           fq[3] += (double)P.k_v[(size_t)(2 * b + 1) * sv + vidx[q]] * d;
         }
@@ -493,6 +542,280 @@ __global__ void dye2d_kernel(const __grid_constant__ DyeParams<T> P) {
   P.c[(size_t)j * nx + i] = out;
 }
 
+
+// ---------------------------------------------------------------------------------------
+// heat transfer (ns2d/physics.py:623-923 with scalar.py:34-146)
+// ---------------------------------------------------------------------------------------
+constexpr int MAXR = 2 * AERO_MAX_BODIES + 2;  // per-block partials: heat, then sums and wall weights
+
+template <typename T>
+struct ThetaParams {
+  int nx, ny, periodic, closed;
+  T inv_h, inv_half;          // 1 / h, 2 / h
+  T kappa, inv_prt, theta_in, eta_t;
+  const T *thp, *th0;         // stage-start and step-start theta (ny, nx)
+  T *th;                      // the stage's theta
+  const T *up, *vp, *psi;     // stage-start velocity: u_hat and the previous psi, or u0 / v0
+  const T *nut;               // (ny, nx) nu_t of the stage, NULL without LES
+  int mode[4];                // AERO_TH2_* of left, right, bottom, top
+  T wval[4];
+  int has_win, win[4];
+  const T *ins_u, *ins_v, *q_skin, *chi_t, *a_t, *w_t, *w_f;  // NULL: absent
+  int n_temp, n_flux;
+  T a, b;
+  const T *dt;
+  double *heat_part;          // (nblocks, n_temp) of this stage
+  double *rep_part;           // last stage: (nblocks, 2 + n_flux) = sum theta, sum theta0, wall weights
+};
+
+// theta at (j, i) with the ghosts of scalar.py:63-78: periodic wrap; else the first / last
+// cell repeated, except the inflow value left of a tunnel.  The tile staging reaches up to
+// TX + 2 cells past the last one, more than a period of a small grid: the wrap is a modulo.
+template <typename T>
+__device__ __forceinline__ T theta_at(const ThetaParams<T> &P, int j, int i) {
+  if (P.periodic) {
+    i = ((i % P.nx) + P.nx) % P.nx;
+    j = ((j % P.ny) + P.ny) % P.ny;
+  } else {
+    j = j < 0 ? 0 : (j >= P.ny ? P.ny - 1 : j);
+    if (i < 0) {
+      if (!P.closed) return P.theta_in;
+      i = 0;
+    }
+    if (i >= P.nx) i = P.nx - 1;
+  }
+  return __ldg(P.thp + (size_t)j * P.nx + i);
+}
+
+// diffusivity on the x-face (j, f): kappa (+ the face average of nu_t / Pr_t), times the
+// insulation factor inside the window (physics.py:700-718)
+template <typename T>
+__device__ __forceinline__ T kx_face(const ThetaParams<T> &P, int j, int f) {
+  T k = P.kappa;
+  const int nx = P.nx;
+  if (P.nut) {
+    const T *row = P.nut + (size_t)j * nx;
+    T avg;
+    if (f > 0 && f < nx) avg = T(0.5) * (__ldg(row + f) * P.inv_prt + __ldg(row + f - 1) * P.inv_prt);
+    else if (P.periodic) avg = T(0.5) * (__ldg(row) * P.inv_prt + __ldg(row + nx - 1) * P.inv_prt);
+    else avg = __ldg(row + (f == 0 ? 0 : nx - 1)) * P.inv_prt;
+    k = P.kappa + avg;
+  }
+  if (P.ins_u && j >= P.win[0] && j < P.win[1] && f >= P.win[2] && f <= P.win[3])
+    k = k * __ldg(P.ins_u + (size_t)(j - P.win[0]) * (P.win[3] - P.win[2] + 1) + (f - P.win[2]));
+  return k;
+}
+
+template <typename T>
+__device__ __forceinline__ T ky_face(const ThetaParams<T> &P, int f, int i) {
+  T k = P.kappa;
+  const int nx = P.nx, ny = P.ny;
+  if (P.nut) {
+    T avg;
+    if (f > 0 && f < ny)
+      avg = T(0.5) * (__ldg(P.nut + (size_t)f * nx + i) * P.inv_prt + __ldg(P.nut + (size_t)(f - 1) * nx + i) * P.inv_prt);
+    else if (P.periodic)
+      avg = T(0.5) * (__ldg(P.nut + i) * P.inv_prt + __ldg(P.nut + (size_t)(ny - 1) * nx + i) * P.inv_prt);
+    else
+      avg = __ldg(P.nut + (size_t)(f == 0 ? 0 : ny - 1) * nx + i) * P.inv_prt;
+    k = P.kappa + avg;
+  }
+  if (P.ins_v && f >= P.win[0] && f <= P.win[1] && i >= P.win[2] && i < P.win[3])
+    k = k * __ldg(P.ins_v + (size_t)(f - P.win[0]) * (P.win[3] - P.win[2]) + (i - P.win[2]));
+  return k;
+}
+
+// diffusive flux -k dtheta/dn of a boundary face (scalar.py:112-146); sign +1 on the low side
+template <typename T>
+__device__ __forceinline__ T wall_flux(int mode, T k, T inner, T value, T inv_half, T sign) {
+  if (mode == AERO_TH2_TEMPERATURE || mode == AERO_TH2_INLET) return ((-sign * inv_half) * k) * (inner - value);
+  if (mode == AERO_TH2_HEAT_FLUX) return (sign * k) * value;
+  return T(0);
+}
+
+// One RK stage of theta on a 32 x 8 tile of cells: bounded advection with the stage-start
+// velocity, diffusion with the wall conditions, heat-flux skins, the RK blend and the
+// implicit penalisation toward the temperature bodies with their heat partials.
+template <typename T>
+__global__ void __launch_bounds__(NT) theta2d_kernel(const __grid_constant__ ThetaParams<T> P) {
+  aero::pdl_wait();
+  __shared__ T S[TY + 4][TX + 4];
+  __shared__ double red[NT / 32][MAXR];
+  const int nx = P.nx, ny = P.ny;
+  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
+  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
+  for (int e = tid; e < (TY + 4) * (TX + 4); e += NT) {
+    const int r = e / (TX + 4), c = e - r * (TX + 4);
+    S[r][c] = theta_at<T>(P, j0 - 2 + r, i0 - 2 + c);
+  }
+  __syncthreads();
+  const int j = j0 + ty, i = i0 + tx;
+  const bool in = j < ny && i < nx;
+  const int nh = P.n_temp, nr = P.rep_part ? 2 + P.n_flux : 0;
+  double acc[MAXR];
+#pragma unroll
+  for (int q = 0; q < MAXR; ++q) acc[q] = 0.0;
+  if (in) {
+    const int r = ty + 2, c = tx + 2;
+    const T ctr = S[r][c];
+    auto uface = [&](int f) {
+      return P.psi ? projected_u<T>(P.up, P.psi, nx, P.periodic, P.inv_h, j, f) : __ldg(P.up + (size_t)j * (nx + 1) + f);
+    };
+    auto vface = [&](int f) {
+      return P.psi ? projected_v<T>(P.vp, P.psi, nx, ny, P.periodic, P.inv_h, f, i) : __ldg(P.vp + (size_t)f * nx + i);
+    };
+    const T fx0 = muscl_flux<T>(S[r][c - 2], S[r][c - 1], ctr, S[r][c + 1], uface(i));
+    const T fx1 = muscl_flux<T>(S[r][c - 1], ctr, S[r][c + 1], S[r][c + 2], uface(i + 1));
+    const T fy0 = muscl_flux<T>(S[r - 2][c], S[r - 1][c], ctr, S[r + 1][c], vface(j));
+    const T fy1 = muscl_flux<T>(S[r - 1][c], ctr, S[r + 1][c], S[r + 2][c], vface(j + 1));
+    T lt = (((fx0 - fx1) + fy0) - fy1) * P.inv_h;
+    // diffusive fluxes of the four faces
+    auto dfx = [&](int f) {
+      if (f > 0 && f < nx) return -(kx_face<T>(P, j, f) * (S[r][f - i0 + 2] - S[r][f - i0 + 1])) * P.inv_h;
+      if (P.periodic)   // both ends carry the wrap flux with the first face's diffusivity
+        return -(kx_face<T>(P, j, 0) * (__ldg(P.thp + (size_t)j * nx) - __ldg(P.thp + (size_t)j * nx + nx - 1))) *
+               P.inv_h;
+      const int side = f == 0 ? 0 : 1;
+      const T inner = __ldg(P.thp + (size_t)j * nx + (f == 0 ? 0 : nx - 1));
+      return wall_flux<T>(P.mode[side], kx_face<T>(P, j, f), inner, P.wval[side], P.inv_half,
+                          side == 0 ? T(1) : T(-1));
+    };
+    auto dfy = [&](int f) {
+      if (f > 0 && f < ny) return -(ky_face<T>(P, f, i) * (S[f - j0 + 2][c] - S[f - j0 + 1][c])) * P.inv_h;
+      if (P.periodic)
+        return -(ky_face<T>(P, 0, i) * (__ldg(P.thp + i) - __ldg(P.thp + (size_t)(ny - 1) * nx + i))) * P.inv_h;
+      const int side = f == 0 ? 2 : 3;
+      const T inner = __ldg(P.thp + (size_t)(f == 0 ? 0 : ny - 1) * nx + i);
+      return wall_flux<T>(P.mode[side], ky_face<T>(P, f, i), inner, P.wval[side], P.inv_half,
+                          side == 2 ? T(1) : T(-1));
+    };
+    const T ld = (((dfx(i) - dfx(i + 1)) + dfy(j)) - dfy(j + 1)) * P.inv_h;
+    lt = lt + ld;
+    const bool inwin = P.has_win && j >= P.win[0] && j < P.win[1] && i >= P.win[2] && i < P.win[3];
+    const size_t widx = inwin ? (size_t)(j - P.win[0]) * (P.win[3] - P.win[2]) + (i - P.win[2]) : 0;
+    const size_t wsz = (size_t)(P.win[1] - P.win[0]) * (P.win[3] - P.win[2]);
+    if (inwin && P.q_skin) lt = lt + P.kappa * __ldg(P.q_skin + widx);
+    const T bdt = *P.dt * P.b;
+    const size_t g = (size_t)j * nx + i;
+    const T t0 = __ldg(P.th0 + g);
+    T th = (P.a == T(0) ? ctr : lerp_t<T>(ctr, t0, P.a)) + lt * bdt;
+    if (inwin && nh > 0) {
+      const T kt = bdt / P.eta_t;
+      const T tn = (th + kt * __ldg(P.a_t + widx)) / (T(1) + kt * __ldg(P.chi_t + widx));
+      const double d = (double)(tn - th);
+      for (int b = 0; b < nh; ++b) acc[b] = (double)__ldg(P.w_t + (size_t)b * wsz + widx) * d;
+      th = tn;
+    }
+    if (nr) {
+      acc[nh] = (double)th;
+      acc[nh + 1] = (double)t0;
+      if (inwin)
+        for (int b = 0; b < P.n_flux; ++b) acc[nh + 2 + b] = (double)__ldg(P.w_f + (size_t)b * wsz + widx) * (double)th;
+    }
+    P.th[g] = th;
+  }
+  const int nq = nh + nr;
+  if (nq == 0) return;
+  const int warp = tid >> 5, lane = tid & 31;
+  for (int q = 0; q < nq; ++q) {
+    const double v = warp_sum(acc[q]);
+    if (lane == 0) red[warp][q] = v;
+  }
+  __syncthreads();
+  if (tid < nq) {
+    double t = 0.0;
+    for (int w = 0; w < NT / 32; ++w) t += red[w][tid];
+    const size_t blk = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
+    if (tid < nh) P.heat_part[blk * nh + tid] = t;
+    else P.rep_part[blk * nr + (tid - nh)] = t;
+  }
+}
+
+template <typename T>
+struct ReportParams {
+  int nx, ny, periodic, closed, nblocks, n_temp, n_flux;
+  T h, h2, kappa, theta_in;
+  double hd;
+  int mode[4];
+  T wval[4];
+  T wgt[3];
+  const double *heat_part;    // (3, nblocks, n_temp)
+  const double *rep_part;     // (nblocks, 2 + n_flux)
+  const T *theta, *u, *dt;
+  double *heat, *theta_wall, *wall_heat, *heat_storage, *flow_heat;
+};
+
+// block-wide sum in a fixed order (every thread gets it)
+__device__ __forceinline__ double block_sum_fixed(double v, double *sh) {
+  v = warp_sum(v);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double t = 0.0;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
+  return t;
+}
+
+// The step's heat report (core.py:974-995, physics.py:760-794): one block of 256 threads.
+template <typename T>
+__global__ void heat_report2d_kernel(const __grid_constant__ ReportParams<T> P) {
+  aero::pdl_wait();
+  __shared__ double sh[32];
+  const int nx = P.nx, ny = P.ny, tid = threadIdx.x, nt = blockDim.x;
+  const T dt = *P.dt;
+  const double per_dt = (double)(P.h2 / dt);
+  const int nh = P.n_temp, nr = 2 + P.n_flux;
+  for (int b = 0; b < nh; ++b) {
+    double tot = 0.0;
+    for (int st = 0; st < 3; ++st) {
+      double s = 0.0;
+      for (int e = tid; e < P.nblocks; e += nt) s += P.heat_part[((size_t)st * P.nblocks + e) * nh + b];
+      s = block_sum_fixed(s, sh);
+      tot = st == 0 ? s * (double)P.wgt[0] : tot + s * (double)P.wgt[st];
+    }
+    if (tid == 0) P.heat[b] = tot * per_dt;
+  }
+  double sums[2];
+  for (int q = 0; q < nr; ++q) {
+    double s = 0.0;
+    for (int e = tid; e < P.nblocks; e += nt) s += P.rep_part[(size_t)e * nr + q];
+    s = block_sum_fixed(s, sh);
+    if (q < 2) sums[q] = s;
+    else if (tid == 0) P.theta_wall[q - 2] = s;
+  }
+  if (tid == 0) P.heat_storage[0] = (sums[0] - sums[1]) * per_dt;
+  for (int side = 0; side < 4; ++side) {
+    const int mode = P.mode[side];
+    const int n = side < 2 ? ny : nx;
+    double rate = 0.0;
+    if (mode == AERO_TH2_TEMPERATURE || mode == AERO_TH2_INLET) {
+      double s = 0.0;
+      for (int e = tid; e < n; e += nt) {
+        const size_t g = side == 0 ? (size_t)e * nx : side == 1 ? (size_t)e * nx + nx - 1
+                                                    : side == 2 ? (size_t)e : (size_t)(ny - 1) * nx + e;
+        s += (double)(P.wval[side] - P.theta[g]);
+      }
+      rate = (double)(T(2) * P.kappa) * block_sum_fixed(s, sh);
+    } else if (mode == AERO_TH2_HEAT_FLUX) {
+      rate = (double)((P.kappa * P.wval[side]) * T((double)n * P.hd));
+    }
+    if (tid == 0) P.wall_heat[side] = rate;
+  }
+  double fin = 0.0, fout = 0.0;
+  if (!P.periodic && !P.closed) {
+    for (int e = tid; e < ny; e += nt) {
+      fin += (double)(P.u[(size_t)e * (nx + 1)] * P.theta_in);
+      fout += (double)(P.u[(size_t)e * (nx + 1) + nx] * P.theta[(size_t)e * nx + nx - 1]);
+    }
+    fin = block_sum_fixed(fin, sh) * (double)P.h;
+    fout = block_sum_fixed(fout, sh) * (double)P.h;
+  }
+  if (tid == 0) {
+    P.flow_heat[0] = fin;
+    P.flow_heat[1] = fout;
+  }
+}
+
 // Coefficients [Cd, Cl, Cm] per body from the stage partials in a fixed order, t + dt, dt
 template <typename T>
 __global__ void finalize2d_kernel(const double *__restrict__ partials, int nblocks, int nbody, double h,
@@ -535,6 +858,7 @@ struct AeroNs2dPlan {
   size_t esz;
   size_t nu, nv, nc;          // element counts of u, v and cells
   size_t off_uh, off_vh, off_up, off_vp, off_pa, off_small, off_scalars, off_zero, off_partials, total;
+  size_t off_nut, off_tb0, off_tb1, off_hpart, off_rpart;  // heat transfer only
   AxisInfo ax[2];             // x (n = nx), y (n = ny)
   int gx, gy, nblocks, nq;
 };
@@ -617,6 +941,7 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
   double *partials = reinterpret_cast<double *>(ws + p->off_partials);
   const bool has_win = c.nbody > 0 && c.window[1] > c.window[0] && c.window[3] > c.window[2];
   const bool les = c.les != AERO_LES_NONE;
+  const bool thermal = c.thermal != 0;
   // ---- dt
   int dt_mode = dt_in ? 2 : (c.has_dt_fixed ? 1 : 0);
   StageParams<T> S{};
@@ -655,7 +980,8 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
     aero::MaxJobs<T> J{};
     J.job[0] = {u0, p->nu, bits + aero::SC_MAXU};
     J.job[1] = {v0, p->nv, bits + aero::SC_MAXV};
-    AERO_CUDA_TRY(aero::launch_absmax_multi<T>(J, 2, s));
+    if (thermal) J.job[2] = {static_cast<const T *>(f->theta0), p->nc, bits + aero::SC_MAXT};
+    AERO_CUDA_TRY(aero::launch_absmax_multi<T>(J, thermal ? 3 : 2, s));
     if (les) {
       StageParams<T> N = S;
       N.up = u0;
@@ -675,6 +1001,50 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
   S.dt_visc_h2 = 0.25 * c.h * c.h;
   S.dt_les = les ? 1 : 0;
   S.dt_store = small;
+  if (thermal && dt_mode == 0)
+    S.dt_th = Dt2dThermal{1, c.kappa, 1.0 / c.prt, 2.0 / c.h, c.diff_coef / (c.h * c.h), std::fabs(c.ri), c.cfl, c.h};
+  // heat transfer: buoyancy in the stage kernel, theta in its own kernel after it
+  T *nutb = thermal ? reinterpret_cast<T *>(ws + p->off_nut) : nullptr;
+  T *tb[2] = {thermal ? reinterpret_cast<T *>(ws + p->off_tb0) : nullptr,
+              thermal ? reinterpret_cast<T *>(ws + p->off_tb1) : nullptr};
+  ThetaParams<T> TP{};
+  if (thermal) {
+    S.ri_gx = T(T(c.ri) * T(-c.gravity[0]));
+    S.ri_gy = T(T(c.ri) * T(-c.gravity[1]));
+    S.buoy_u = c.ri != 0.0 && c.gravity[0] != 0.0;
+    S.buoy_v = c.ri != 0.0 && c.gravity[1] != 0.0;
+    S.vol_u = c.has_vol ? static_cast<const T *>(g->vol_u) : nullptr;
+    S.vol_v = c.has_vol ? static_cast<const T *>(g->vol_v) : nullptr;
+    S.nut_out = les ? nutb : nullptr;
+    TP.nx = nx;
+    TP.ny = ny;
+    TP.periodic = c.periodic;
+    TP.closed = c.closed;
+    TP.inv_h = T(1.0 / c.h);
+    TP.inv_half = T(2.0 / c.h);
+    TP.kappa = T(c.kappa);
+    TP.inv_prt = T(1.0 / c.prt);
+    TP.theta_in = T(c.theta_in);
+    TP.eta_t = T(c.eta_t);
+    TP.th0 = static_cast<const T *>(f->theta0);
+    TP.nut = les ? nutb : nullptr;
+    for (int q = 0; q < 4; ++q) {
+      TP.mode[q] = c.wall_mode[q];
+      TP.wval[q] = T(c.wall_value[q]);
+      TP.win[q] = c.window[q];
+    }
+    TP.has_win = has_win;
+    TP.ins_u = c.has_ins ? static_cast<const T *>(g->ins_u) : nullptr;
+    TP.ins_v = c.has_ins ? static_cast<const T *>(g->ins_v) : nullptr;
+    TP.q_skin = c.n_flux ? static_cast<const T *>(g->q_skin) : nullptr;
+    TP.chi_t = static_cast<const T *>(g->chi_t);
+    TP.a_t = static_cast<const T *>(g->a_t);
+    TP.w_t = static_cast<const T *>(g->w_t);
+    TP.w_f = static_cast<const T *>(g->w_f);
+    TP.n_temp = has_win ? c.n_temp : 0;
+    TP.n_flux = has_win ? c.n_flux : 0;
+    TP.dt = small;
+  }
   // ---- stages
   static const double RK[3][3] = {{0.0, 1.0, 1.0 / 6.0}, {0.75, 0.25, 2.0 / 3.0}, {1.0 / 3.0, 2.0 / 3.0, 1.0}};
   T *p_out = static_cast<T *>(f->p);
@@ -695,8 +1065,24 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
     P.w = T(RK[st][2]);
     P.partials = partials + (size_t)st * p->nblocks * std::max(p->nq, 1);
     P.dt_here = st == 0;
+    const T *th_in = st == 0 ? static_cast<const T *>(f->theta0) : tb[(st - 1) % 2];
+    if (thermal) P.thp = th_in;
     (void)aero::launch_k(stage2d_kernel<T, false>, grid, block, 0, s, P);
     AERO_CUDA_TRY(cudaGetLastError());
+    if (thermal) {  // before the transforms overwrite the previous psi
+      ThetaParams<T> Q = TP;
+      Q.thp = th_in;
+      Q.th = st == 2 ? static_cast<T *>(f->theta) : tb[st % 2];
+      Q.up = P.up;
+      Q.vp = P.vp;
+      Q.psi = P.psi;
+      Q.a = P.a;
+      Q.b = P.b;
+      Q.heat_part = reinterpret_cast<double *>(ws + p->off_hpart) + (size_t)st * p->nblocks * std::max(c.n_temp, 1);
+      Q.rep_part = st == 2 ? reinterpret_cast<double *>(ws + p->off_rpart) : nullptr;
+      (void)aero::launch_k(theta2d_kernel<T>, grid, block, 0, s, Q);
+      AERO_CUDA_TRY(cudaGetLastError());
+    }
     const int acc_mode = st == 0 ? 0 : (st == 1 ? 1 : 2);
     if (fused) {
       aero::TransformParams<T> F{};
@@ -723,6 +1109,38 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
                            T(1.0 / c.h), ub[st % 2], vb[st % 2], pa, static_cast<T *>(f->u), static_cast<T *>(f->v));
       AERO_CUDA_TRY(cudaGetLastError());
     }
+  }
+  if (thermal) {
+    ReportParams<T> R{};
+    R.nx = nx;
+    R.ny = ny;
+    R.periodic = c.periodic;
+    R.closed = c.closed;
+    R.nblocks = p->nblocks;
+    R.n_temp = TP.n_temp;
+    R.n_flux = TP.n_flux;
+    R.h = T(c.h);
+    R.hd = c.h;
+    R.h2 = T(c.h * c.h);
+    R.kappa = T(c.kappa);
+    R.theta_in = T(c.theta_in);
+    for (int q = 0; q < 4; ++q) {
+      R.mode[q] = c.wall_mode[q];
+      R.wval[q] = T(c.wall_value[q]);
+    }
+    for (int q = 0; q < 3; ++q) R.wgt[q] = T(RK[q][2]);
+    R.heat_part = reinterpret_cast<const double *>(ws + p->off_hpart);
+    R.rep_part = reinterpret_cast<const double *>(ws + p->off_rpart);
+    R.theta = static_cast<const T *>(f->theta);
+    R.u = static_cast<const T *>(f->u);
+    R.dt = small;
+    R.heat = static_cast<double *>(f->heat);
+    R.theta_wall = static_cast<double *>(f->theta_wall);
+    R.wall_heat = static_cast<double *>(f->wall_heat);
+    R.heat_storage = static_cast<double *>(f->heat_storage);
+    R.flow_heat = static_cast<double *>(f->flow_heat);
+    (void)aero::launch_k(heat_report2d_kernel<T>, 1, 256, 0, s, R);
+    AERO_CUDA_TRY(cudaGetLastError());
   }
   // ---- dye with the step's final velocity
   if (c.dye) {
@@ -776,6 +1194,19 @@ int aero_ns2d_plan_create(const AeroNs2dConfig *cfg, AeroNs2dPlan **plan) {
   if (has_win && (c.window[0] < 0 || c.window[1] > c.ny || c.window[2] < 0 || c.window[3] > c.nx))
     return set_error(AERO_EINVAL, "body window outside the domain");
   if (!(c.eta > 0)) return set_error(AERO_EINVAL, "eta must be positive");
+  if (c.thermal) {
+    if (c.n_temp < 0 || c.n_temp > AERO_MAX_BODIES || c.n_flux < 0 || c.n_flux > AERO_MAX_BODIES)
+      return set_error(AERO_EUNSUPPORTED, "at most " + std::to_string(AERO_MAX_BODIES) + " temperature / heat-flux bodies");
+    if ((c.n_temp || c.n_flux || c.has_ins || c.has_vol) && !has_win)
+      return set_error(AERO_EINVAL, "thermal body masks need a body window");
+    for (int q = 0; q < 4; ++q)
+      if (c.wall_mode[q] < AERO_TH2_ADIABATIC || c.wall_mode[q] > AERO_TH2_PERIODIC)
+        return set_error(AERO_EINVAL, "unknown temperature boundary mode");
+    if (c.periodic != (c.wall_mode[0] == AERO_TH2_PERIODIC))
+      return set_error(AERO_EINVAL, "temperature boundary modes disagree with the periodicity of the domain");
+    if (!(c.prt > 0)) return set_error(AERO_EINVAL, "turbulent Prandtl number must be positive");
+    if (c.n_temp && !(c.eta_t > 0)) return set_error(AERO_EINVAL, "eta_t must be positive");
+  }
   auto *p = new AeroNs2dPlan();
   p->cfg = c;
   const size_t e = c.dtype == AERO_F64 ? 8 : 4;
@@ -803,6 +1234,13 @@ int aero_ns2d_plan_create(const AeroNs2dConfig *cfg, AeroNs2dPlan **plan) {
   p->nblocks = p->gx * p->gy;
   p->nq = has_win ? 4 * c.nbody : 0;
   p->off_partials = take(sizeof(double) * 3 * (size_t)p->nblocks * std::max(p->nq, 1));
+  if (c.thermal) {
+    p->off_nut = take(p->nc * e);
+    p->off_tb0 = take(p->nc * e);
+    p->off_tb1 = take(p->nc * e);
+    p->off_hpart = take(sizeof(double) * 3 * (size_t)p->nblocks * std::max(c.n_temp, 1));
+    p->off_rpart = take(sizeof(double) * (size_t)p->nblocks * (2 + c.n_flux));
+  }
   aero_host::axis_setup(p->ax[0], c.nx, c.periodic != 0, e);
   aero_host::axis_setup(p->ax[1], c.ny, c.periodic != 0, e);
   for (int a = 0; a < 2; ++a) aero_host::axis_place(p->ax[a], e, take);
@@ -838,6 +1276,13 @@ int aero_ns2d_step(const AeroNs2dPlan *plan, const AeroNs2dFields *f, const Aero
   const bool has_win = c.nbody > 0 && c.window[1] > c.window[0] && c.window[3] > c.window[2];
   if (has_win && (!g->chi_u || !g->chi_v || !g->chi_c || !g->a_u || !g->a_v || !g->k_u || !g->k_v || !f->coeffs))
     return set_error(AERO_EINVAL, "missing body masks");
+  if (c.thermal) {
+    if (!f->theta0 || !f->theta || !f->wall_heat || !f->heat_storage || !f->flow_heat)
+      return set_error(AERO_EINVAL, "heat transfer needs theta and report pointers");
+    if ((c.n_temp && (!f->heat || !g->chi_t || !g->a_t || !g->w_t)) || (c.n_flux && (!f->theta_wall || !g->q_skin || !g->w_f)) ||
+        (c.has_ins && (!g->ins_u || !g->ins_v)) || (c.has_vol && (!g->vol_u || !g->vol_v)))
+      return set_error(AERO_EINVAL, "missing thermal body masks or report pointers");
+  }
   auto s = static_cast<cudaStream_t>(stream);
   auto ws = static_cast<unsigned char *>(workspace);
   return c.dtype == AERO_F64 ? step2d_impl<double>(plan, f, g, dt_in, ws, s)

@@ -3,9 +3,12 @@
 :class:`Ns2dPlan` reads the reference's 2D objects by attribute (``Ops`` and ``Geometry`` of
 src/aerolume/solvers/ns2d/core.py:67-108 and geometry.py:160-182, or the containers of
 :mod:`aerolume_b200.ns2d.types`), turns the boundary types into the ghost-cell rules of
-core.py:271-325, uploads the window masks once and owns the device workspace.  Placed
-physics (heat, fans, ports, emitters, the PID step controller), the wall model and body
-forcing raise ``RuntimeError``: there is no fallback to a CPU or plain-torch path.
+core.py:271-325, uploads the window masks once and owns the device workspace.  Heat
+transfer comes from ``thermal=`` (a :class:`~aerolume_b200.ns2d.types.Thermal2D`) or from the
+reference's ``ops.phys`` with ``geom.thermal`` when heat transfer is all it places; other
+placed physics (heat sources, fans, ports, paint, emitters, the PID step controller), the
+wall model and body forcing raise ``RuntimeError``: there is no fallback to a CPU or
+plain-torch path.
 """
 from __future__ import annotations
 
@@ -15,7 +18,8 @@ import numpy as np
 import torch
 
 from .. import _lib
-from .._lib import ADV, F32, F64, GHOST, LES, MAX_BODIES, check
+from .._lib import ADV, F32, F64, GHOST, LES, MAX_BODIES, THETA2_MODE, check
+from .types import Thermal2D
 
 
 def _f(x) -> float:
@@ -56,11 +60,37 @@ def ghost_rules(ops):
     return ((ux, uy), (vx, vy))
 
 
+def thermal_from_physics(ph, geom) -> Thermal2D:
+    """The heat transfer of the reference's 2D ``Physics`` (physics.py:291-345) and
+    ``geom.thermal``; raises when the physics places anything the B200 step does not run."""
+    others = [n for n, on in (("heat sources", getattr(ph, "heat", None) is not None),
+                              ("ports", bool(getattr(ph, "ports", None))), ("paint", bool(getattr(ph, "paint", False))),
+                              ("fans", int(getattr(ph, "nfan", 0) or 0) > 0),
+                              ("smoke groups", int(getattr(ph, "n_dye", 0) or 0) > 0 or bool(getattr(ph, "comb", False))),
+                              ("the PID step controller", bool(getattr(ph, "pid", False)))) if on]
+    if others:
+        raise RuntimeError("placed physics (" + ", ".join(others) + ") is not in the B200 2D step")
+    if not getattr(ph, "thermal", False):
+        raise RuntimeError("placed physics without heat transfer is not in the B200 2D step")
+    tg = getattr(geom, "thermal", None)
+    kw = {}
+    if tg is not None and not geom.empty:
+        kw = {n: getattr(tg, n, None) for n in ("chi_t", "a_t", "w_t", "ins_u", "ins_v", "q_skin", "w_f", "vol_u",
+                                                 "vol_v")}
+        kw["temp_ids"] = tuple(getattr(tg, "temp_ids", ()) or ())
+        kw["flux_ids"] = tuple(getattr(tg, "flux_ids", ()) or ())
+    vals = ph.wall_values
+    vals = vals.detach().cpu().tolist() if torch.is_tensor(vals) else list(vals)
+    return Thermal2D(kappa=_f(ph.kappa), ri=_f(ph.ri), prt=float(ph.prt), gravity=tuple(float(g) for g in ph.gravity),
+                     eta_t=_f(ph.eta_t), theta_in=_f(ph.theta_in), wall_modes=tuple(ph.wall_modes),
+                     wall_values=tuple(float(x) for x in vals), diff_coef=float(ph.diff_coef), **kw)
+
+
 class Ns2dPlan:
     """Plan + device tensors for one 2D (ops, geom) configuration; ``dye`` turns on the dye
-    update after each step."""
+    update after each step, ``thermal`` (a :class:`Thermal2D`) heat transfer."""
 
-    def __init__(self, ops, geom, *, dye: bool = False, device=None):
+    def __init__(self, ops, geom, *, dye: bool = False, thermal=None, device=None):
         self.device = torch.device(device) if device is not None else torch.device("cuda")
         if self.device.type != "cuda":
             raise RuntimeError("the B200 step runs on a CUDA device only (no CPU fallback)")
@@ -69,7 +99,9 @@ class Ns2dPlan:
         if self.device.index is None:
             self.device = torch.device("cuda", torch.cuda.current_device())
         if getattr(ops, "phys", None) is not None:
-            raise RuntimeError("placed physics (heat, fans, ports, emitters, PID dt) is not in the B200 2D step")
+            if thermal is not None:
+                raise RuntimeError("heat transfer comes either from ops.phys or from thermal=, not both")
+            thermal = thermal_from_physics(ops.phys, geom)
         if getattr(ops, "forcing", None) is not None:
             raise RuntimeError("a uniform body force (verification forcing) is not supported by the B200 step")
         if getattr(ops, "wall_model", False):
@@ -116,6 +148,8 @@ class Ns2dPlan:
             cfg.window[q] = win[q] if self.has_win else 0
         cfg.nbody = self.nbody if self.has_win else 0
         cfg.dye = int(self.dye)
+        self.thermal = thermal
+        self.n_temp = self.n_flux = 0
         self._keep = []
         dev, dt = self.device, self.dtype
 
@@ -138,6 +172,8 @@ class Ns2dPlan:
         d_in = getattr(ops, "dye_inlet", None)
         if self.dye and d_in is not None:
             g.dye_inlet = up(d_in, (ny,)).data_ptr()
+        if thermal is not None:
+            self._thermal_config(cfg, g, thermal, up)
         self.cfg = cfg
         self.geom_c = g
         handle = C.c_void_p()
@@ -148,6 +184,40 @@ class Ns2dPlan:
         self.ws_ptr = (self._ws_raw.data_ptr() + 255) & ~255
         self.workspace_bytes = nbytes
         check(L.aero_ns2d_workspace_init(handle, C.c_void_p(self.ws_ptr), self._stream()), "aero_ns2d_workspace_init")
+
+    def _thermal_config(self, cfg, g, th, up):
+        cfg.thermal = 1
+        cfg.kappa, cfg.ri, cfg.prt = float(th.kappa), float(th.ri), float(th.prt)
+        cfg.gravity[0], cfg.gravity[1] = (float(x) for x in th.gravity)
+        cfg.eta_t, cfg.theta_in = float(th.eta_t), float(th.theta_in)
+        modes = tuple(th.wall_modes)
+        if len(modes) != 4 or any(m not in THETA2_MODE for m in modes):
+            raise RuntimeError(f"unsupported temperature boundary modes {modes!r}")
+        for q in range(4):
+            cfg.wall_mode[q] = THETA2_MODE[modes[q]]
+            cfg.wall_value[q] = float(th.wall_values[q])
+        cfg.diff_coef = float(th.diff_coef)
+        if self.has_win:
+            self.n_temp, self.n_flux = len(th.temp_ids), len(th.flux_ids)
+            if self.n_temp > MAX_BODIES or self.n_flux > MAX_BODIES:
+                raise RuntimeError(f"the B200 step supports at most {MAX_BODIES} temperature / heat-flux bodies")
+            wy, wx = cfg.window[1] - cfg.window[0], cfg.window[3] - cfg.window[2]
+            if self.n_temp:
+                g.chi_t = up(th.chi_t, (wy, wx)).data_ptr()
+                g.a_t = up(th.a_t, (wy, wx)).data_ptr()
+                g.w_t = up(th.w_t, (self.n_temp, wy, wx)).data_ptr()
+            if self.n_flux:
+                g.q_skin = up(th.q_skin, (wy, wx)).data_ptr()
+                g.w_f = up(th.w_f, (self.n_flux, wy, wx)).data_ptr()
+            if th.ins_u is not None:
+                cfg.has_ins = 1
+                g.ins_u = up(th.ins_u, (wy, wx + 1)).data_ptr()
+                g.ins_v = up(th.ins_v, (wy + 1, wx)).data_ptr()
+            if th.vol_u is not None:
+                cfg.has_vol = 1
+                g.vol_u = up(th.vol_u, (wy, wx + 1)).data_ptr()
+                g.vol_v = up(th.vol_v, (wy + 1, wx)).data_ptr()
+        cfg.n_temp, cfg.n_flux = self.n_temp, self.n_flux
 
     def _stream(self):
         return C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
@@ -170,6 +240,11 @@ class Ns2dPlan:
                "coeffs": torch.zeros(max(self.nbody, 1), 3, **kw)[: self.nbody]}
         if self.dye:
             out["dye"] = torch.empty(ny, nx, **kw)
+        if self.thermal is not None:
+            d64 = dict(device=self.device, dtype=torch.float64)
+            out.update(theta=torch.empty(ny, nx, **kw), heat=torch.zeros(self.n_temp, **d64),
+                       theta_wall=torch.zeros(self.n_flux, **d64), wall_heat=torch.zeros(4, **d64),
+                       heat_storage=torch.zeros(1, **d64), flow_heat=torch.zeros(2, **d64))
         return out
 
     def _check(self, name, t, shape):
@@ -178,10 +253,11 @@ class Ns2dPlan:
         if tuple(t.shape) != tuple(shape):
             raise RuntimeError(f"{name} has shape {tuple(t.shape)}, expected {tuple(shape)}")
 
-    def step(self, u0, v0, t0, *, dye0=None, out=None, dt=None):
-        """One step (plus the dye update when the plan has dye); returns the output dict.
-        ``out`` may hold u0 / v0 themselves (in-place update); ``dt`` is None (CFL rule on
-        the device) or a 0-d device tensor."""
+    def step(self, u0, v0, t0, *, dye0=None, theta0=None, out=None, dt=None):
+        """One step (plus the dye update when the plan has dye, theta and the heat report
+        (float64: heat, theta_wall, wall_heat, heat_storage, flow_heat) with heat transfer);
+        returns the output dict.  ``out`` may hold u0 / v0 / theta0 themselves (in-place
+        update); ``dt`` is None (CFL rule on the device) or a 0-d device tensor."""
         ny, nx = self.shape
         self._check("u0", u0, (ny, nx + 1))
         self._check("v0", v0, (ny + 1, nx))
@@ -198,6 +274,19 @@ class Ns2dPlan:
                 raise RuntimeError("this plan has dye: dye0 is required")
             self._check("dye0", dye0, (ny, nx))
             f.dye0, f.dye = dye0.data_ptr(), out["dye"].data_ptr()
+        if self.thermal is not None:
+            if theta0 is None:
+                raise RuntimeError("this plan has heat transfer: theta0 is required")
+            self._check("theta0", theta0, (ny, nx))
+            f.theta0, f.theta = theta0.data_ptr(), out["theta"].data_ptr()
+            for name in ("heat", "theta_wall", "wall_heat", "heat_storage", "flow_heat"):
+                t = out[name]
+                if not (t.device == self.device and t.dtype == torch.float64 and t.is_contiguous()):
+                    raise RuntimeError(f"{name} must be a contiguous float64 tensor on {self.device}")
+                if t.numel():
+                    setattr(f, name, t.data_ptr())
+        elif theta0 is not None:
+            raise RuntimeError("theta0 given to a plan without heat transfer")
         dtp = None
         if dt is not None:
             self._check("dt", dt, ())

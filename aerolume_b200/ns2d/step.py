@@ -4,8 +4,10 @@ served by the B200 step.
 ``FlowSolver`` imports ``step_full`` at module import (ns2d/solver.py:44-57) and calls it as
 ``step_full(state, geom, ops, None, out=..., diag=...)`` (solver.py:384-408); rebinding
 ``aerolume.solvers.ns2d.solver.step_full`` to this function swaps the step.  It returns
-``(State, coeffs (nbody, 3))`` of new tensors like the reference.  Placed physics, the wall
-model, diagnostics rows and traces raise instead of being computed differently.
+``(State, coeffs (nbody, 3))`` of new tensors like the reference.  With heat transfer
+(``ops.phys`` placing heat transfer only) theta advances too and ``out`` receives the heat
+report of core.py:974-995.  Other placed physics, the wall model, diagnostics rows and
+traces raise instead of being computed differently.
 """
 from __future__ import annotations
 
@@ -17,7 +19,7 @@ from .plan import Ns2dPlan
 
 
 class State(NamedTuple):
-    """The reference's 2D state (core.py:111-130); placed-physics fields stay None."""
+    """The reference's 2D state (core.py:111-130); dye_extra and ctrl stay None."""
     u: Any
     v: Any
     p: Any
@@ -45,14 +47,24 @@ def step_full(state, geom, ops, dt=None, *, out=None, diag=False, trace=None):
     """One SSP-RK3 step (plus the dye update when the state carries dye)."""
     if diag or trace is not None:
         raise RuntimeError("diagnostics rows and stage traces are not produced by the B200 step")
-    for name in ("theta", "dye_extra", "ctrl"):
+    for name in ("dye_extra", "ctrl"):
         if getattr(state, name, None) is not None:
             raise RuntimeError(f"placed-physics state {name!r} is not in the B200 2D step")
+    theta = getattr(state, "theta", None)
+    if theta is not None and getattr(ops, "phys", None) is None:
+        raise RuntimeError("state.theta without heat transfer in ops.phys")
     plan = _plan_for(ops, geom, state.dye is not None, state.u.device)
+    if (plan.thermal is None) != (theta is None):
+        raise RuntimeError("state.theta must be given exactly when ops.phys has heat transfer")
     if dt is not None and not torch.is_tensor(dt):
         dt = torch.tensor(float(dt), device=state.u.device, dtype=state.u.dtype)
-    res = plan.step(state.u, state.v, state.t, dye0=state.dye, dt=dt)
-    new = State(res["u"], res["v"], res["p"], res.get("dye"), res["t"], res["dt"])
+    res = plan.step(state.u, state.v, state.t, dye0=state.dye, theta0=theta, dt=dt)
+    new = State(res["u"], res["v"], res["p"], res.get("dye"), res["t"], res["dt"], res.get("theta"))
+    if out is not None and plan.thermal is not None:
+        keys = (["heat"] if plan.n_temp else []) + (["theta_wall"] if plan.n_flux else []) + [
+            "wall_heat", "heat_storage", "flow_heat"]
+        for k in keys:
+            out[k] = res[k].to(state.u.dtype)
     coeffs = res["coeffs"] if plan.nbody and plan.has_win else torch.zeros(0, 3, device=state.u.device,
                                                                           dtype=state.u.dtype)
     return new, coeffs

@@ -64,3 +64,32 @@ class Geometry2D:
     @property
     def empty(self) -> bool:
         return self.window[1] <= self.window[0] or self.window[3] <= self.window[2]
+
+
+@dataclass
+class Thermal2D:
+    """Heat transfer of a 2D solve: the thermal part of the reference's ``Physics``
+    (src/aerolume/solvers/ns2d/physics.py:305-322) with the bodies' ``ThermalGeometry``
+    (geometry.py:120-158) on the body window.  ``wall_modes`` are the side modes of
+    scalar.py:96-146 (left, right, bottom, top); ``temp_ids`` / ``flux_ids`` only count the
+    temperature and heat-flux bodies."""
+    kappa: float
+    ri: float
+    prt: float
+    gravity: tuple
+    eta_t: float
+    theta_in: float
+    wall_modes: tuple
+    wall_values: tuple
+    diff_coef: float
+    temp_ids: tuple = ()
+    flux_ids: tuple = ()
+    chi_t: Any = None            # (wy, wx) temperature-body mask
+    a_t: Any = None              # (wy, wx) chi_t * body temperature
+    w_t: Any = None              # (n_temp, wy, wx) heat shares
+    ins_u: Any = None            # (wy, wx + 1) insulation factors of the x-faces
+    ins_v: Any = None            # (wy + 1, wx)
+    q_skin: Any = None           # (wy, wx) heat-flux skin source / kappa
+    w_f: Any = None              # (n_flux, wy, wx) wall-temperature weights
+    vol_u: Any = None            # (wy, wx + 1) solid area fractions for the buoyancy share
+    vol_v: Any = None            # (wy + 1, wx)

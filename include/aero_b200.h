@@ -36,7 +36,7 @@
 extern "C" {
 #endif
 
-#define AERO_ABI_VERSION 2
+#define AERO_ABI_VERSION 3
 
 #define AERO_OK 0
 #define AERO_EINVAL -1        /* invalid argument or inconsistent configuration     */
@@ -289,7 +289,21 @@ typedef struct {
   int32_t window[4];            /* body cell window j0, j1, i0, i1 (empty: no bodies)      */
   int32_t nbody;                /* <= AERO_MAX_BODIES                                      */
   int32_t dye;                  /* advect the dye after the step                           */
+  /* heat transfer (ns2d/physics.py:305-322, 623-923; thermal = 0: off) */
+  int32_t thermal;
+  double kappa, ri, prt;        /* 1 / Pe, Richardson number, turbulent Prandtl number    */
+  double gravity[2];            /* unit gravity direction (x, y)                           */
+  double eta_t, theta_in;       /* thermal permeability, inlet temperature                 */
+  int32_t wall_mode[4];         /* AERO_TH2_* of the left, right, bottom, top sides        */
+  double wall_value[4];         /* wall temperature (TEMPERATURE / INLET) or gradient G    */
+  double diff_coef;             /* largest diffusion coefficient (physics.py:833-848)      */
+  int32_t n_temp, n_flux;       /* temperature bodies, heat-flux bodies                    */
+  int32_t has_ins, has_vol;     /* insulation factors / area fractions present             */
 } AeroNs2dConfig;
+
+/* temperature boundary modes of a 2D side (ns2d/scalar.py:96-146) */
+enum { AERO_TH2_ADIABATIC = 0, AERO_TH2_TEMPERATURE = 1, AERO_TH2_HEAT_FLUX = 2, AERO_TH2_INLET = 3,
+       AERO_TH2_OUTLET = 4, AERO_TH2_PERIODIC = 5 };
 
 /* Window masks (geometry.py:160-178) and boundary profiles, device pointers. */
 typedef struct {
@@ -298,6 +312,11 @@ typedef struct {
   const void *k_u, *k_v;              /* (nbody, 2, ...): [force weight, moment weight]     */
   const void *u_inlet;                /* (ny) inlet u (tunnel)                              */
   const void *dye_inlet;              /* (ny) inlet dye comb, or NULL for zeros             */
+  /* heat transfer on the same window (ns2d/geometry.py:120-158): temperature bodies'
+   * chi_t, a_t (wy, wx) and shares w_t (n_temp, wy, wx); insulation ins_u (wy, wx+1),
+   * ins_v (wy+1, wx); heat-flux skins q_skin (wy, wx) and weights w_f (n_flux, wy, wx);
+   * area fractions vol_u, vol_v for the buoyancy share */
+  const void *chi_t, *a_t, *w_t, *ins_u, *ins_v, *q_skin, *w_f, *vol_u, *vol_v;
 } AeroNs2dGeom;
 
 /* Step inputs (u0, v0, t0, dye0) and outputs; u / v may alias u0 / v0. */
@@ -305,6 +324,12 @@ typedef struct {
   const void *u0, *v0, *t0, *dye0;
   void *u, *v, *p, *t, *dt, *dye;
   void *coeffs;                       /* (nbody, 3): Cd, Cl, Cm                             */
+  /* heat transfer: theta in / out (ny, nx; may alias) and the step's heat report
+   * (ns2d/core.py:974-995), all double: heat of each temperature body (n_temp), wall
+   * temperature of each heat-flux body (n_flux), wall heat of the left, right, bottom and
+   * top sides (4), heat storage (1), flow heat in at the inlet / out at the outlet (2) */
+  const void *theta0;
+  void *theta, *heat, *theta_wall, *wall_heat, *heat_storage, *flow_heat;
 } AeroNs2dFields;
 
 int aero_ns2d_plan_create(const AeroNs2dConfig *cfg, AeroNs2dPlan **plan);

@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 import torch
 
-from _golden import CASES_2D, GOLDEN, load_case2d
+from _golden import CASES_2D, GOLDEN, load_case2d, thermal2d_from_case
 from oracle import ns2d as O2
 
 pytestmark = pytest.mark.gpu
@@ -31,11 +31,32 @@ def _setup(name):
     from aerolume_b200.ns2d.plan import Ns2dPlan
     meta, ops, geom, arr = load_case2d(name)
     dt = torch.float64 if meta["dtype"] == "float64" else torch.float32
-    plan = Ns2dPlan(ops, geom, dye="in_dye" in arr)
+    plan = Ns2dPlan(ops, geom, dye="in_dye" in arr, thermal=thermal2d_from_case(meta, arr))
     ins = {"u0": _dev(arr["in_u"], dt), "v0": _dev(arr["in_v"], dt), "t0": _dev(arr["in_t"], dt)}
     if "in_dye" in arr:
         ins["dye0"] = _dev(arr["in_dye"], dt)
+    if "in_theta" in arr:
+        ins["theta0"] = _dev(arr["in_theta"], dt)
     return meta, plan, ins, arr
+
+
+def _check_report(out, arr, meta):
+    """The heat report against the reference's: each entry within TOL_COEFF of the larger of
+    its own magnitude and the scale of the sums it is made of (heat storage is a difference
+    of two sums over the grid, so its scale is sum |theta| h^2 / dt)."""
+    tol = TOL_COEFF[meta["dtype"]]
+    h2_dt = meta["h"] ** 2 / float(arr["out1_dt"])
+    for key in ("heat", "theta_wall", "wall_heat", "heat_storage", "flow_heat"):
+        ref_key = f"out1_rep_{key}"
+        if ref_key not in arr:
+            continue
+        got = out[key].cpu().numpy()
+        ref = np.asarray(arr[ref_key], np.float64)
+        scale = max(np.abs(ref).max(), 1e-30)
+        if key == "heat_storage":
+            scale = max(scale, (np.abs(arr["in_theta"]).sum() + np.abs(arr["out1_theta"]).sum()) * h2_dt)
+        assert got.shape == ref.shape, key
+        assert np.abs(got - ref).max() <= tol * scale, (key, got, ref)
 
 
 @pytest.mark.parametrize("name", CASES_2D)
@@ -52,16 +73,21 @@ def test_step2d_matches_reference(name):
         assert _rel(out["coeffs"], arr["out1_coeffs"]) < TOL_COEFF[meta["dtype"]]
     if "out1_dye" in arr:
         assert _rel(out["dye"], arr["out1_dye"]) < tol
+    if "out1_theta" in arr:
+        assert _rel(out["theta"], arr["out1_theta"]) < tol, _rel(out["theta"], arr["out1_theta"])
+        _check_report(out, arr, meta)
 
 
-@pytest.mark.parametrize("name", [c for c in CASES_2D if c.startswith("cylinder")])
+@pytest.mark.parametrize("name", [c for c in CASES_2D if c.startswith("cylinder") or "heated" in c or "cold" in c])
 def test_three_steps_in_place_match_reference(name):
     meta, plan, ins, arr = _setup(name)
-    u, v, t, dye = ins["u0"], ins["v0"], ins["t0"], ins.get("dye0")
+    u, v, t, dye, theta = ins["u0"], ins["v0"], ins["t0"], ins.get("dye0"), ins.get("theta0")
     out = plan.empty_fields()
     for _ in range(3):
         out["u"], out["v"] = u, v             # in-place velocity update
-        res = plan.step(u, v, t, dye0=dye, out=out)
+        if theta is not None:
+            out["theta"] = theta              # and theta in place
+        res = plan.step(u, v, t, dye0=dye, theta0=theta, out=out)
         t = res["t"].clone()
         if dye is not None:
             dye, res["dye"] = res["dye"], dye  # ping-pong the dye
@@ -71,6 +97,8 @@ def test_three_steps_in_place_match_reference(name):
         assert _rel(got, arr[f"outN_{k}"]) < tol, (k, _rel(got, arr[f"outN_{k}"]))
     if dye is not None:
         assert _rel(dye, arr["outN_dye"]) < tol
+    if theta is not None:
+        assert _rel(theta, arr["outN_theta"]) < tol, _rel(theta, arr["outN_theta"])
 
 
 def _poisson_plan(nx, ny, h, periodic, dtype):

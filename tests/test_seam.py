@@ -32,6 +32,28 @@ def test_step_full_refuses_diagnostics_and_placed_physics():
         step_full(st._replace(theta=1), None, None)
 
 
+def test_thermal_from_physics_takes_heat_only():
+    """The 2D plan reads heat transfer off the reference's Physics and refuses the rest."""
+    from aerolume_b200.ns2d.plan import thermal_from_physics
+    from aerolume_b200.ns2d.types import Geometry2D
+    geom = Geometry2D((2, 6, 3, 9), nbody=1)
+    geom.thermal = types.SimpleNamespace(temp_ids=(0,), flux_ids=(), chi_t=np.ones((4, 6)), a_t=np.ones((4, 6)),
+                                         w_t=np.ones((1, 4, 6)), ins_u=None, ins_v=None, q_skin=None, w_f=None,
+                                         vol_u=None, vol_v=None)
+    ph = types.SimpleNamespace(thermal=True, kappa=torch.tensor(0.01), ri=torch.tensor(0.5), prt=0.85,
+                               gravity=(0.0, -1.0), eta_t=torch.tensor(0.005), theta_in=torch.tensor(0.0),
+                               wall_modes=("inlet", "outlet", "adiabatic", "adiabatic"),
+                               wall_values=torch.zeros(4), diff_coef=5.0, heat=None, ports=[], paint=False, nfan=0,
+                               n_dye=0, comb=False, pid=False)
+    th = thermal_from_physics(ph, geom)
+    assert th.temp_ids == (0,) and th.wall_modes[0] == "inlet" and abs(th.kappa - 0.01) < 1e-9
+    assert th.a_t is geom.thermal.a_t and th.wall_values == (0.0, 0.0, 0.0, 0.0)
+    for name, val in (("nfan", 1), ("pid", True), ("paint", True), ("ports", [1]), ("heat", torch.ones(2)),
+                      ("n_dye", 2), ("thermal", False)):
+        with pytest.raises(RuntimeError):
+            thermal_from_physics(types.SimpleNamespace(**{**vars(ph), name: val}), geom)
+
+
 def _dev(x, dt):
     x = np.asarray(x)
     return torch.as_tensor(np.ascontiguousarray(x).reshape(x.shape)).to("cuda", dt).contiguous()
@@ -75,6 +97,37 @@ def test_step_full_matches_reference():
     for k in ("u", "v", "p", "dye", "t", "dt"):
         assert _rel(getattr(new, k), arr[f"out1_{k}"]) < 1e-10, k
     assert _rel(coeffs, arr["out1_coeffs"]) < 1e-9
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["cavity_heated_wale_f64", "cylinder_heated_f64"])
+def test_step_full_heat_matches_reference(name):
+    """step_full with ops.phys carrying heat transfer (the attributes of the reference's 2D
+    Physics) and geom.thermal: velocity, theta and the heat report in ``out``."""
+    from _golden import thermal2d_from_case
+    from aerolume_b200.ns2d.step import State, step_full
+    meta, ops, geom, arr = load_case2d(name)
+    th = thermal2d_from_case(meta, arr)
+    dt = torch.float64
+    ops.phys = types.SimpleNamespace(thermal=True, kappa=th.kappa, ri=th.ri, prt=th.prt, gravity=th.gravity,
+                                     eta_t=th.eta_t, theta_in=th.theta_in, wall_modes=th.wall_modes,
+                                     wall_values=th.wall_values, diff_coef=th.diff_coef, heat=None, ports=[],
+                                     paint=False, nfan=0, n_dye=0, comb=False, pid=False)
+    geom.thermal = th
+    ny, nx = ops.ny, ops.nx
+    st = State(_dev(arr["in_u"], dt), _dev(arr["in_v"], dt), torch.zeros(ny, nx, device="cuda", dtype=dt), None,
+               _dev(arr["in_t"], dt), torch.zeros((), device="cuda", dtype=dt), _dev(arr["in_theta"], dt))
+    out = {}
+    new, coeffs = step_full(st, geom, ops, None, out=out)
+    torch.cuda.synchronize()
+    for k in ("u", "v", "p", "t", "dt", "theta"):
+        assert _rel(getattr(new, k), arr[f"out1_{k}"]) < 1e-10, k
+    assert _rel(coeffs, arr["out1_coeffs"]) < 1e-9
+    for k in ("heat", "theta_wall", "wall_heat", "flow_heat"):
+        assert (k in out) == (f"out1_rep_{k}" in arr), k
+        if k in out:
+            ref = arr[f"out1_rep_{k}"]
+            assert np.abs(out[k].cpu().numpy() - ref).max() <= 1e-9 * max(np.abs(ref).max(), 1e-30), k
 
 
 @pytest.mark.gpu
