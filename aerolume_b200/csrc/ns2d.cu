@@ -1,5 +1,6 @@
-// The 2D step of the C ABI: Aerolume ns2d/core.py:815-969 (step_full) without placed physics,
-// with the dye update of its lines 959-962.
+// The 2D step of the C ABI: Aerolume ns2d/core.py:815-969 (step_full) with heat transfer as
+// its only placed physics (physics.py:623-884, core.py:774-813, 974-995), and the dye update
+// of its lines 959-962.
 //
 // Arithmetic follows the reference's plain-torch step operation by operation, so float64
 // runs agree with it to round-off:

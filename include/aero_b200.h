@@ -21,9 +21,10 @@
  *   aero_ns3d_fields           ns3d/fields.py:45 gradient_field, ns3d/solver.py:1374 _centred
  *   aero_ns3d_probe            ns3d/fields.py:78 trilinear (surface probes, slices, wake lines)
  *   aero_ns2d_plan_create      ns2d/core.py:182 make_operators (the per-config constants)
- *   aero_ns2d_step             ns2d/core.py:815 step_full (no placed physics), with the dye
- *                              update of its lines 959-962 (core.py:703 advect_dye,
- *                              core.py:779 _zero_dye_in_solids)
+ *   aero_ns2d_step             ns2d/core.py:815 step_full (heat transfer its only placed
+ *                              physics: physics.py:623-884, the report of core.py:974
+ *                              _report), with the dye update of its lines 959-962
+ *                              (core.py:703 advect_dye, core.py:779 _zero_dye_in_solids)
  *   aero_ns2d_poisson_solve    ns2d/poisson.py:126 PoissonSolver.solve
  */
 #ifndef AERO_B200_H
