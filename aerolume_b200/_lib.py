@@ -37,7 +37,8 @@ EXPORTS = ("aero_abi_version", "aero_last_error", "aero_ns3d_plan_create", "aero
            "aero_ns3d_project", "aero_ns3d_read_status", "aero_debug_check", "aero_ns3d_poisson_solve_static",
            "aero_ns2d_plan_create", "aero_ns2d_plan_destroy", "aero_ns2d_workspace_bytes",
            "aero_ns2d_workspace_init", "aero_ns2d_step", "aero_ns2d_poisson_solve", "aero_ns3d_fields",
-           "aero_ns3d_probe")
+           "aero_ns3d_probe", "aero_ns3d_masks_workspace_bytes", "aero_ns3d_build_masks",
+           "aero_mesh_sdf_workspace_bytes", "aero_mesh_signed_distance")
 
 
 class Ns3dConfig(C.Structure):
@@ -123,6 +124,25 @@ class Ns2dFields(C.Structure):
                                           "flow_heat")]
 
 
+class MaskConfig(C.Structure):
+    _fields_ = [
+        ("abi_version", C.c_int32), ("dtype", C.c_int32), ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+        ("h", C.c_double), ("x0", C.c_double), ("y0", C.c_double), ("z0", C.c_double),
+        ("periodic", C.c_int32 * 3), ("window", C.c_int32 * 6), ("mask_width", C.c_double),
+        ("mask_shift", C.c_double), ("moment_ref", C.c_double * 3), ("nbody", C.c_int32),
+    ]
+
+
+class MaskBody(C.Structure):
+    _fields_ = [("vertices", C.c_void_p), ("nvert", C.c_int32), ("faces", C.c_void_p), ("nface", C.c_int32),
+                ("omega", C.c_double), ("center", C.c_double * 3), ("axis", C.c_double * 3)]
+
+
+class MaskOut(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in ("chi_u", "chi_v", "chi_w", "chi_c", "a_u", "a_v", "a_w", "k_u", "k_v",
+                                          "k_w")]
+
+
 _LIB = None
 
 
@@ -169,6 +189,16 @@ def lib() -> C.CDLL:
                                    C.POINTER(C.c_void_p), C.c_void_p]
     L.aero_ns3d_probe.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_double),
                                   C.POINTER(C.c_double), C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]
+    L.aero_ns3d_masks_workspace_bytes.argtypes = [C.POINTER(MaskConfig), C.POINTER(MaskBody)]
+    L.aero_ns3d_masks_workspace_bytes.restype = C.c_size_t
+    L.aero_ns3d_build_masks.argtypes = [C.POINTER(MaskConfig), C.POINTER(MaskBody), C.POINTER(MaskOut), C.c_void_p,
+                                        C.c_void_p]
+    L.aero_ns3d_build_masks.restype = C.c_int
+    L.aero_mesh_sdf_workspace_bytes.argtypes = [C.c_int32, C.c_int32, C.c_int64]
+    L.aero_mesh_sdf_workspace_bytes.restype = C.c_size_t
+    L.aero_mesh_signed_distance.argtypes = [C.c_int32, C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p,
+                                            C.c_int64, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.aero_mesh_signed_distance.restype = C.c_int
     L.aero_debug_check.restype = C.c_int
     for name in ("aero_ns3d_plan_create", "aero_ns3d_workspace_init", "aero_ns3d_step", "aero_ns3d_step_traced",
                  "aero_ns3d_smoke",

@@ -20,6 +20,9 @@
  *   aero_ns3d_workspace_bytes  (no counterpart: the reference allocates inside torch)
  *   aero_ns3d_fields           ns3d/fields.py:45 gradient_field, ns3d/solver.py:1374 _centred
  *   aero_ns3d_probe            ns3d/fields.py:78 trilinear (surface probes, slices, wake lines)
+ *   aero_ns3d_build_masks      ns3d/geometry.py:385 build_geometry3d with its exact signed
+ *                              distance (geometry.py:229 grid_signed_distance, use_shared=False)
+ *   aero_mesh_signed_distance  ns3d/geometry.py:126 mesh_signed_distance
  *   aero_ns2d_plan_create      ns2d/core.py:182 make_operators (the per-config constants)
  *   aero_ns2d_step             ns2d/core.py:815 step_full (heat transfer its only placed
  *                              physics: physics.py:623-884, the report of core.py:974
@@ -251,6 +254,50 @@ int aero_ns3d_fields(const AeroNs3dPlan *plan, const void *u, const void *v, con
  * points (x, y, z) (device, the plan's dtype); points outside are clamped to the edge. */
 int aero_ns3d_probe(const AeroNs3dPlan *plan, const void *field, const int32_t shape[3], const double origin[3],
                     const double off[3], const void *pts, int64_t npts, void *out, void *stream);
+
+/* ---- mask construction (ns3d/geometry.py:385-495) ---------------------------------- */
+
+/* The operator fields build_geometry3d reads, and the body window the caller chose
+ * (geometry.py:323 body_window3d, or a fixed one for live attitude edits). */
+typedef struct {
+  int32_t abi_version;          /* AERO_ABI_VERSION                                        */
+  int32_t dtype;                /* AERO_F32 or AERO_F64 (masks and mesh coordinates)       */
+  int32_t nx, ny, nz;
+  double h, x0, y0, z0;
+  int32_t periodic[3];          /* x, y, z: periodic axes keep their boundary faces        */
+  int32_t window[6];            /* k0, k1, j0, j1, i0, i1 (non-empty, inside the domain)   */
+  double mask_width, mask_shift;/* ramp half-width and wall shift, in cells                */
+  double moment_ref[3];
+  int32_t nbody;                /* 1 .. AERO_MAX_BODIES                                    */
+} AeroMaskConfig;
+
+/* One immersed mesh (ns3d/config.py:81 ImmersedMesh): device vertices (nvert, 3) in the
+ * config dtype, device faces (nface, 3) of vertex indices in 0 .. nvert-1, rigid spin. */
+typedef struct {
+  const void *vertices;
+  int32_t nvert;
+  const int32_t *faces;
+  int32_t nface;
+  double omega, center[3], axis[3];
+} AeroMaskBody;
+
+/* Outputs on the window (geometry.py:275-303 Geometry3D): chi_u (wz, wy, wx+1), chi_v
+ * (wz, wy+1, wx), chi_w (wz+1, wy, wx), chi_c (wz, wy, wx), a_* like chi_*, k_u (nbody, 3,
+ * wz, wy, wx+1) and likewise k_v, k_w. */
+typedef struct {
+  void *chi_u, *chi_v, *chi_w, *chi_c, *a_u, *a_v, *a_w, *k_u, *k_v, *k_w;
+} AeroMaskOut;
+
+size_t aero_ns3d_masks_workspace_bytes(const AeroMaskConfig *cfg, const AeroMaskBody *bodies);
+int aero_ns3d_build_masks(const AeroMaskConfig *cfg, const AeroMaskBody *bodies, const AeroMaskOut *out,
+                          void *workspace, void *stream);
+
+/* Exact signed distance (negative inside) of npoints device points (x, y, z) to one mesh,
+ * with the face plane distance within plane_zone of a face (geometry.py:126-196). */
+size_t aero_mesh_sdf_workspace_bytes(int32_t dtype, int32_t nface, int64_t npoints);
+int aero_mesh_signed_distance(int32_t dtype, const void *vertices, int32_t nvert, const int32_t *faces, int32_t nface,
+                              const void *points, int64_t npoints, double plane_zone, void *out, void *workspace,
+                              void *stream);
 
 /* Device-side status word of the last step on this workspace (0 = fine; bit 0: a
  * non-finite value reached a reduction).  Reads through a host copy: synchronises. */

@@ -128,3 +128,22 @@ def thermal2d_from_case(meta, arr):
                      theta_in=t["theta_in"], wall_modes=tuple(t["wall_modes"]), wall_values=tuple(t["wall_values"]),
                      diff_coef=t["diff_coef"], temp_ids=tuple(t.get("temp_ids", ())),
                      flux_ids=tuple(t.get("flux_ids", ())), **g)
+
+
+def load_masks():
+    """(npz, case tags) of masks3d.npz."""
+    z = np.load(GOLDEN / "masks3d.npz")
+    return z, json.loads(str(z["cases"]))
+
+
+def masks_case(z, tag):
+    """(meta, ops namespace with the reference's attribute names, bodies) of one mask case."""
+    from types import SimpleNamespace
+    meta = json.loads(str(z[f"{tag}_meta"]))
+    ops = SimpleNamespace(nx=meta["nx"], ny=meta["ny"], nz=meta["nz"], h=meta["h"], x0=meta["origin"][0],
+                          y0=meta["origin"][1], z0=meta["origin"][2], periodic_axes=tuple(meta["periodic_axes"]),
+                          moment_ref=tuple(meta["moment_ref"]), mask_width=meta["mask_width"],
+                          mask_shift=meta["mask_shift"], dtype=meta["dtype"])
+    bodies = [SimpleNamespace(vertices=z[f"{tag}_v{q}"], faces=z[f"{tag}_f{q}"], omega=b["omega"],
+                              center=tuple(b["center"]), axis=tuple(b["axis"])) for q, b in enumerate(meta["bodies"])]
+    return meta, ops, bodies
