@@ -6,6 +6,10 @@ LES, no dye; and 64 NACA 4-digit airfoils (chord 1, quarter chord at (2, 2)) on 
 from {256x128, 384x192, 512x256, 768x384, 1024x512} with seeded thickness, camber, camber
 position, angle of attack and Reynolds number.  Initial fields: the inlet profile plus seeded
 N(0, noise) on u and v, boundary values imposed, then projected.
+
+``heated_cylinder`` is the cylinder wake with heat transfer: the cylinder held at theta = 1
+in a stream at theta = 0, Pr 0.71, Ri 0.5 with gravity along -y, inlet / outlet temperature
+sides and adiabatic walls (the reference's heated-cylinder validation set-up).
 """
 from __future__ import annotations
 
@@ -14,7 +18,8 @@ import math
 import numpy as np
 import torch
 
-from .setup import build_geometry, make_ops
+from .setup import build_geometry, make_ops, polygon_sdf, smooth_step
+from .types import Thermal2D
 
 SWEEP_GRIDS = ((256, 128), (384, 192), (512, 256), (768, 384), (1024, 512))
 
@@ -93,3 +98,35 @@ def initial_state(ops, plan, seed=0, noise=1e-3):
     u[:, 1:-1] -= (psi[:, 1:] - psi[:, :-1]) * (1.0 / ops.h)
     v[1:-1] -= (psi[1:] - psi[:-1]) * (1.0 / ops.h)
     return u.contiguous(), v.contiguous()
+
+
+def heated_cylinder(nx=256, ny=128, dtype="float32", vertices=256, prandtl=0.71, richardson=0.5):
+    """(ops, geom, thermal) of the cylinder tunnel with the cylinder held at theta = 1: the
+    thermal masks of ns2d/geometry.py:385-419 for one temperature body (chi_t = the cell
+    mask, a_t = chi_t, unit share, no insulated or heat-flux body) and the face area
+    fractions without the wall offset for the buoyancy share; kappa = 1 / (Re Pr), the
+    thermal permeability and diffusion coefficient of physics.py:263-288, 833-848."""
+    ops, geom = cylinder_tunnel(nx, ny, dtype, vertices)
+    h = ops.h
+    poly = circle(2.0, 2.0, 0.25, vertices)
+    j0, j1, i0, i1 = geom.window
+    wy, wx = j1 - j0, i1 - i0
+
+    def grid(nr, nc, xoff, yoff):
+        ys = ops.y0 + (np.arange(nr) + j0 + yoff) * h
+        xs = ops.x0 + (np.arange(nc) + i0 + xoff) * h
+        return np.meshgrid(ys, xs, indexing="ij")
+
+    yu, xu = grid(wy, wx + 1, 0.0, 0.5)
+    yv, xv = grid(wy + 1, wx, 0.5, 0.0)
+    vol_u = smooth_step(polygon_sdf(poly, xu, yu), h)
+    vol_v = smooth_step(polygon_sdf(poly, xv, yv), h)
+    chi_t = np.asarray(geom.chi_c, np.float64)
+    pe = 200.0 * prandtl                                   # Re 200 per unit length
+    eta_t = min(0.05 * h, h * h * pe / 60.0)
+    th = Thermal2D(kappa=1.0 / pe, ri=richardson, prt=0.85, gravity=(0.0, -1.0), eta_t=eta_t, theta_in=0.0,
+                   wall_modes=("inlet", "outlet", "adiabatic", "adiabatic"), wall_values=(0.0, 0.0, 0.0, 0.0),
+                   diff_coef=5.0, temp_ids=(0,), flux_ids=(), chi_t=chi_t, a_t=chi_t * 1.0,
+                   w_t=np.ones((1, wy, wx)), ins_u=np.ones((wy, wx + 1)), ins_v=np.ones((wy + 1, wx)),
+                   vol_u=vol_u, vol_v=vol_v)
+    return ops, geom, th

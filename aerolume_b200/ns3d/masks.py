@@ -101,10 +101,10 @@ def body_window3d(vertex_sets, ops, margin_cells=None, *, pitch_deg=0.0, yaw_deg
 
 
 def _upload_mesh(v, f, dev, dt):
-    if len(f) and (f.min() < 0 or f.max() >= len(_vertices_numpy(v))):
-        raise ValueError("a face names a vertex that does not exist")
     vt = (v.detach() if torch.is_tensor(v) else torch.as_tensor(_vertices_numpy(v)))
     vt = vt.reshape(-1, 3).to(device=dev, dtype=dt).contiguous()
+    if len(f) and (f.min() < 0 or f.max() >= vt.shape[0]):
+        raise ValueError("a face names a vertex that does not exist")
     ft = torch.as_tensor(f.astype(np.int32)).to(dev).contiguous()
     return vt, ft
 

@@ -6,6 +6,9 @@ box height (1e4 per unit length), WALE LES, Boussinesq temperature with the body
 theta = 1 (10 K above the stream), Pr = 0.71, Ri = 0.1 on the body height (0.2 per unit
 length), one smoke rake of 16 seeded nozzles upstream; initial field uniform U = 1 plus
 seeded N(0, 1e-3) noise on u, v, w, made divergence-free by the step's own projection.
+
+``sphere_mesh``: a closed latitude-longitude triangulation of a sphere, wound outward, the
+body of the mask-construction workload (a live attitude edit rebuilds its masks).
 """
 from __future__ import annotations
 
@@ -58,3 +61,26 @@ def initial_state(ops, *, seed=0, noise=1e-3, device="cuda"):
 
 
 __all__ = ["box_on_moving_floor", "initial_state"]
+
+
+def sphere_mesh(center, radius, n_lat=48, n_lon=96):
+    """(vertices (N, 3) float64, faces (M, 3) int64) of a closed sphere: two poles and
+    n_lat - 1 rings of n_lon vertices, 2 n_lon (n_lat - 1) triangles wound outward."""
+    c = np.asarray(center, dtype=np.float64)
+    th = np.pi * np.arange(1, n_lat) / n_lat                    # polar angle of each ring
+    ph = 2.0 * np.pi * np.arange(n_lon) / n_lon
+    st, ct = np.sin(th)[:, None], np.cos(th)[:, None]
+    ring = np.stack([st * np.cos(ph)[None, :], st * np.sin(ph)[None, :], np.broadcast_to(ct, (n_lat - 1, n_lon))],
+                    axis=-1).reshape(-1, 3)
+    v = np.vstack([[0.0, 0.0, 1.0], ring, [0.0, 0.0, -1.0]]) * radius + c
+    south = len(v) - 1
+    idx = lambda r, k: 1 + r * n_lon + (k % n_lon)              # noqa: E731
+    f = []
+    for k in range(n_lon):
+        f.append((0, idx(0, k), idx(0, k + 1)))
+        f.append((south, idx(n_lat - 2, k + 1), idx(n_lat - 2, k)))
+        for r in range(n_lat - 2):
+            a, b, c2, d = idx(r, k), idx(r, k + 1), idx(r + 1, k + 1), idx(r + 1, k)
+            f.append((a, d, c2))
+            f.append((a, c2, b))
+    return v, np.asarray(f, dtype=np.int64)

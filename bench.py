@@ -18,7 +18,8 @@ the numpy oracle (a restatement of the reference's plain-torch step) on a bounde
 the same workload on this host.
 
 ``--workload cylinder2d`` measures the 2D step instead (a D = 0.5 cylinder at Re_D 100 in an
-8 x 4 tunnel, 256 x 128 FP32, upwind3, CFL 0.5) and ``--workload sweep2d`` the batched sweep
+8 x 4 tunnel, 256 x 128 FP32, upwind3, CFL 0.5; ``heated2d``: the same with heat transfer,
+the cylinder held at theta = 1, Pr 0.71, Ri 0.5) and ``--workload sweep2d`` the batched sweep
 (64 NACA 4-digit airfoils on grids from 256 x 128 to 1024 x 512, all advanced by one CUDA
 graph that spreads the instances over 16 streams; the same plans looped one after another on
 a single stream are reported beside it).
@@ -27,6 +28,10 @@ a single stream are reported beside it).
 1374-1416, fields.py:45-102): one pass writes all seven cell fields (centred u, v, w, speed,
 vorticity magnitude, Q-criterion, eddy viscosity) from the staggered velocity, and a
 million trilinear probes of the speed field are timed beside it.
+
+``--workload masks3d`` measures mask construction (ns3d/geometry.py:385-495 with the exact
+signed distance): the masks, solid velocity and force weights of a closed 9024-triangle
+sphere of diameter 1 at 32 cells per diameter, rebuilt as a live attitude edit does.
 
 With ``--gpus N`` (N > 1, launched by torch.distributed.run) every rank advances its own
 replica (no data-path collective: a single instance of this solver does not shard), and
@@ -340,6 +345,7 @@ def _launches_2d(plan):
         n += 1 + (1 if c.les else 0)                   # |u| and |v| maxima (one launch), nu_t of u0
     n += 3 * (1 + 3 + (0 if fused else 2)) + 1         # stage, 3 transform passes, [div, psi_w]; one correct
     n += 1 if c.dye else 0
+    n += 3 + 1 if c.thermal else 0                     # a theta stage per RK stage, the heat report
     return n + 1                                       # finalize
 
 
@@ -365,8 +371,9 @@ def _time_graph(g, dist, local_rank, rank, dev):
     return max_over_ranks(ms, dist, dev), clk
 
 
-def oracle2d_sample(ops, geom, steps, seed=0):
-    """Wall time of ``steps`` 2D oracle steps (after one untimed step)."""
+def oracle2d_sample(ops, geom, steps, seed=0, thermal=None):
+    """Wall time of ``steps`` 2D oracle steps (after one untimed step); with ``thermal`` the
+    heat-transfer step, theta starting at 0."""
     from oracle import ns2d as O2
     f32 = np.float32
     rng = np.random.default_rng(seed)
@@ -379,6 +386,18 @@ def oracle2d_sample(ops, geom, steps, seed=0):
                                        (geom.chi_u, geom.chi_v, geom.chi_c, geom.a_u, geom.a_v, geom.k_u, geom.k_v)],
                         geom.nbody)
     t = f32(0.0)
+    if thermal is not None:
+        import dataclasses
+        tp = O2.Thermal2D(**{f.name: getattr(thermal, f.name) for f in dataclasses.fields(O2.Thermal2D)})
+        for f in ("chi_t", "a_t", "w_t", "ins_u", "ins_v", "q_skin", "w_f", "vol_u", "vol_v"):
+            if getattr(tp, f) is not None:
+                setattr(tp, f, np.asarray(getattr(tp, f), f32))
+        theta = np.zeros((ops.ny, ops.nx), f32)
+        r = O2.step2d_thermal(u, v, t, theta, geom32, ops, ps, tp)
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            r = O2.step2d_thermal(r.u, r.v, r.t, r.theta, geom32, ops, ps, tp)
+        return time.perf_counter() - t0
     r = O2.step2d(u, v, t, geom32, ops, ps)
     t0 = time.perf_counter()
     for _ in range(steps):
@@ -386,10 +405,14 @@ def oracle2d_sample(ops, geom, steps, seed=0):
     return time.perf_counter() - t0
 
 
+HEATED_2D = ("heated cylinder D=0.5 at (2,2) held at theta 1, 256x128 FP32, Re_D 100, Pr 0.71, Ri 0.5, "
+             "slip adiabatic walls, upwind3, CFL 0.5")
+
+
 def run_2d(args, rank, world, local_rank):
     import torch
     from aerolume_b200.ns2d.plan import Ns2dPlan
-    from aerolume_b200.ns2d.workloads import cylinder_tunnel, initial_state
+    from aerolume_b200.ns2d.workloads import cylinder_tunnel, heated_cylinder, initial_state
     dist = None
     if world > 1:
         import torch.distributed as dist
@@ -397,15 +420,23 @@ def run_2d(args, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     nx, ny = 256, 128
     cells = nx * ny
-    ops, geom = cylinder_tunnel(nx, ny, "float32")
-    plan = Ns2dPlan(ops, geom, device=dev)
+    heated = args.workload == "heated2d"
+    thermal = None
+    if heated:
+        ops, geom, thermal = heated_cylinder(nx, ny, "float32")
+    else:
+        ops, geom = cylinder_tunnel(nx, ny, "float32")
+    plan = Ns2dPlan(ops, geom, thermal=thermal, device=dev)
     u, v = initial_state(ops, plan, seed=rank, noise=1e-3)
     t = torch.zeros((), device=dev)
+    theta = torch.zeros(ny, nx, device=dev) if heated else None
     out = plan.empty_fields()
     out["u"], out["v"] = u, v
+    if heated:
+        out["theta"] = theta
 
     def step():
-        plan.step(u, v, t, out=out)
+        plan.step(u, v, t, theta0=theta, out=out)
         t.copy_(out["t"])
 
     for _ in range(args.warmup):
@@ -424,8 +455,10 @@ def run_2d(args, rank, world, local_rank):
     coeffs = out["coeffs"][0].tolist()
     # e2e: state in from pinned host memory, step, state / coefficients / time out, every step
     hu, hv = u.cpu().pin_memory(), v.cpu().pin_memory()
+    hth = theta.cpu().pin_memory() if heated else None
     ho = {k: torch.empty(x.shape, dtype=x.dtype, pin_memory=True) for k, x in out.items()}
     du, dv = torch.empty_like(u), torch.empty_like(v)
+    dth = torch.empty_like(theta) if heated else None
     o2 = plan.empty_fields()
     ke = max(10, min(K, 200))
     torch.cuda.synchronize()
@@ -434,31 +467,38 @@ def run_2d(args, rank, world, local_rank):
     for _ in range(ke):
         du.copy_(hu, non_blocking=True)
         dv.copy_(hv, non_blocking=True)
-        plan.step(du, dv, t, out=o2)
+        if heated:
+            dth.copy_(hth, non_blocking=True)
+        plan.step(du, dv, t, theta0=dth, out=o2)
         for k in ho:
             ho[k].copy_(o2[k], non_blocking=True)
         hu, ho["u"] = ho["u"], hu
         hv, ho["v"] = ho["v"], hv
+        if heated:
+            hth, ho["theta"] = ho["theta"], hth
     e1.record()
     torch.cuda.synchronize()
     ems = e0.elapsed_time(e1) / ke
     if rank != 0:
         return
-    h2d = u.numel() * 4 + v.numel() * 4
+    h2d = u.numel() * 4 + v.numel() * 4 + (theta.numel() * 4 if heated else 0)
     d2h = sum(x.numel() * x.element_size() for x in out.values())
     peak, peak_kind = _peaks()
-    alg = 228.0 * cells                               # compulsory bytes per 2D cell-step, FP32
+    # compulsory bytes per 2D cell-step, FP32; heat transfer adds theta_p (3 stages), theta_0
+    # (stages 2, 3) and the stage writes: 8 F
+    alg = (228.0 + (32.0 if heated else 0.0)) * cells
     ms_step = ms / K
     cpu = None
     if not args.no_cpu:
         steps_cpu = 20
-        secs = oracle2d_sample(ops, geom, steps_cpu)
+        secs = oracle2d_sample(ops, geom, steps_cpu, thermal=thermal)
         cpu = {"value": cells * steps_cpu / secs / 1e6, "unit": UNIT, "cores": _threads(), "kind": "port",
                "sample": f"{steps_cpu} full {nx}x{ny} steps of the numpy 2D oracle after 1 untimed step"}
     line = {"metric": METRIC, "value": world * cells * K / (ms * 1e-3) / 1e6, "unit": UNIT, "n_gpus": world,
             "steps": K, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "cylinder D=0.5 at (2,2), 256x128 FP32, Re_D 100, slip walls, upwind3, CFL 0.5",
+            "config": {"workload": HEATED_2D if heated else
+                       "cylinder D=0.5 at (2,2), 256x128 FP32, Re_D 100, slip walls, upwind3, CFL 0.5",
                        "cells": cells, "grid": [nx, ny],
                        "inputs_vs_l2": "7.5 MB working set stays in the 126 MB L2 between steps (no flush)",
                        "parallelism": "replicas", "graph": f"{K} steps, 1 replay"},
@@ -716,18 +756,156 @@ def run_reference_fields(args, rank):
     print(json.dumps(line), flush=True)
 
 
-def run_reference_2d(args, rank):
-    from aerolume_b200.ns2d.workloads import cylinder_tunnel, sweep_instances
+
+# ---------------------------------------------------------------------------------------
+# mask construction
+# ---------------------------------------------------------------------------------------
+MASKS_METRIC = "mask rebuilds/s of a 9024-triangle sphere on the 256x128x128 grid on 1 B200"
+MASKS_UNIT = "rebuilds/s"
+# FP32 operations of one point-triangle pair in the search kernel, counted from its source:
+# squared distance 148 (edges, normal, three edge-side tests, three segment distances) and
+# solid angle 85 (three norms, triple product, denominator), plus 3 square roots and 1 atan2
+# counted as one operation each
+FLOP_PER_PAIR = 148 + 85 + 4
+FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12   # SMs x FP32 lanes x FMA x max clock
+
+
+def _masks_setup(shape):
+    from aerolume_b200.ns3d.masks import body_window3d
+    from aerolume_b200.ns3d.workloads import box_on_moving_floor, sphere_mesh
+    nx, ny, nz = shape
+    ops = box_on_moving_floor(nx, ny, nz, dtype="float32")[0]
+    v, f = sphere_mesh((2.5, 2.0, 1.0), 0.5)
+    win = body_window3d([v], ops)
+    wz, wy, wx = win[1] - win[0], win[3] - win[2], win[5] - win[4]
+    npts = (wx + 1) * wy * wz + wx * (wy + 1) * wz + wx * wy * (wz + 1) + wx * wy * wz
+    return ops, v, f, win, npts
+
+
+def run_masks(args, rank, world, local_rank):
+    import torch
+    from aerolume_b200.ns3d.masks import build_geometry3d
+    from aerolume_b200.ns3d.types import Geometry3D
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    ops, v, f, win, npts = _masks_setup(args.shape)
+    pairs = npts * len(f)
+    body = (torch.as_tensor(v, dtype=torch.float32).to(dev), f)     # vertices resident on the device
+    # a live attitude edit keeps its window (and the graphs captured on it): pass it in
+    for _ in range(args.warmup):
+        build_geometry3d([body], ops, window=win, device=dev)
+    torch.cuda.synchronize()
+    K = args.steps
+    mon = Clocks(local_rank)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(K):
+        g = build_geometry3d([body], ops, window=win, device=dev)
+    e1.record()
+    torch.cuda.synchronize()
+    clk = mon.stop()
+    ms = e0.elapsed_time(e1) / K
+    if dist is not None:
+        from aerolume_b200.replicas import max_over_ranks
+        ms = max_over_ranks(ms, dist, dev)
+    # e2e: the mesh from host memory each time, the ten mask arrays back to pinned host memory
+    names = [n for n in Geometry3D.__dataclass_fields__ if n.startswith(("chi_", "a_", "k_"))]
+    host_out = {n: torch.empty(getattr(g, n).shape, dtype=g.chi_c.dtype, pin_memory=True) for n in names}
+    ke = max(3, min(K, 10))
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(ke):
+        gh = build_geometry3d([(v, f)], ops, window=win, device=dev)
+        for n in names:
+            host_out[n].copy_(getattr(gh, n), non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    ems = e0.elapsed_time(e1) / ke
     if rank != 0:
         return
+    achieved = pairs * FLOP_PER_PAIR / (ms * 1e-3) / 1e12
+    cpu = None
+    if not args.no_cpu:
+        cpu = _masks_cpu_sample(v, f, ops, win, pairs)
+    line = {"metric": MASKS_METRIC, "value": world * 1e3 / ms, "unit": MASKS_UNIT, "n_gpus": world, "steps": K,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "masks of a closed sphere D = 1 (48 x 96 latitude-longitude mesh, 9024 triangles) "
+                                   "at 32 cells per diameter in the 256x128x128 tunnel, exact signed distance",
+                       "window": list(win), "points": npts, "triangles": len(f), "pairs_per_rebuild": pairs,
+                       "inputs_vs_l2": "compute-bound search; 0.1 MB mesh, 5 MB of masks", "parallelism": "replicas"},
+            "pairs_per_s": pairs * 1e3 / ms,
+            "roofline": {"bound": "fp32", "kernel": "sdf_search_kernel", "achieved": achieved,
+                         "peak": FP32_NOMINAL_TFLOPS, "peak_kind": "nominal FP32 CUDA-core rate", "unit": "TFLOP/s",
+                         "frac": achieved / FP32_NOMINAL_TFLOPS, "traffic": None,
+                         "flop_per_pair": FLOP_PER_PAIR},
+            "cpu_baseline": cpu,
+            "e2e": {"value": world * 1e3 / ems, "unit": MASKS_UNIT,
+                    "h2d_bytes_per_step": int(v.size * 4 + f.size * 4),
+                    "d2h_bytes_per_step": int(sum(x.numel() * x.element_size() for x in host_out.values())),
+                    "ms_per_step": ems, "steps": ke},
+            "gpu_launches": K * 16, "clocks": clk}
+    print(json.dumps(line), flush=True)
+
+
+def _masks_cpu_sample(v, f, ops, win, pairs, npoint=4096):
+    """The numpy oracle's signed distance at npoint seeded window points (rebuilds/s scaled by
+    the pairs of a full rebuild)."""
+    from oracle import masks3d as M
+    rng = np.random.default_rng(0)
+    k0, k1, j0, j1, i0, i1 = win
+    lo = np.array([ops.x0 + i0 * ops.h, ops.y0 + j0 * ops.h, ops.z0 + k0 * ops.h])
+    hi = np.array([ops.x0 + i1 * ops.h, ops.y0 + j1 * ops.h, ops.z0 + k1 * ops.h])
+    p = rng.uniform(lo, hi, size=(npoint, 3)).astype(np.float32)
+    vf = v.astype(np.float32)
+    M.mesh_signed_distance(vf, f, p[:256], chunk=128)
+    t0 = time.perf_counter()
+    M.mesh_signed_distance(vf, f, p, chunk=128)
+    secs = time.perf_counter() - t0
+    rate = npoint * len(f) / secs
+    return {"value": rate / pairs, "unit": MASKS_UNIT, "cores": _threads(), "kind": "port",
+            "sample": f"numpy signed distance of {npoint} seeded window points to the {len(f)} triangles "
+                      f"({npoint * len(f) / 1e6:.0f} M pairs), scaled to a full rebuild of {pairs / 1e9:.2f} G pairs"}
+
+
+def run_reference_masks(args, rank):
+    if rank != 0:
+        return
+    ops, v, f, win, npts = _masks_setup(args.shape)
+    cpu = _masks_cpu_sample(v, f, ops, win, npts * len(f))
+    val = cpu["value"]
+    line = {"impl": "reference", "metric": MASKS_METRIC, "value": val, "unit": MASKS_UNIT, "n_gpus": args.gpus,
+            "steps": 1, "warmup": 1, "ms_per_step": 1e3 / val, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "masks of a closed sphere D = 1 (9024 triangles) at 32 cells per diameter in the "
+                                   "256x128x128 tunnel, exact signed distance"},
+            "cpu_baseline": cpu,
+            "e2e": {"value": val, "unit": MASKS_UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_reference_2d(args, rank):
+    from aerolume_b200.ns2d.workloads import cylinder_tunnel, heated_cylinder, sweep_instances
+    if rank != 0:
+        return
+    thermal = None
     if args.workload == "cylinder2d":
         ops, geom = cylinder_tunnel(256, 128, "float32")
         desc = "cylinder D=0.5 at (2,2), 256x128 FP32, Re_D 100, slip walls, upwind3, CFL 0.5"
+    elif args.workload == "heated2d":
+        ops, geom, thermal = heated_cylinder(256, 128, "float32")
+        desc = HEATED_2D
     else:
         ops, geom, _ = min(sweep_instances(64, seed=0), key=lambda x: x[0].nx)
         desc = f"one {ops.nx}x{ops.ny} instance of the batched NACA sweep"
     steps = max(1, min(args.steps, 20))
-    secs = oracle2d_sample(ops, geom, steps)
+    secs = oracle2d_sample(ops, geom, steps, thermal=thermal)
     val = ops.nx * ops.ny * steps / secs / 1e6
     line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
             "warmup": 1, "ms_per_step": 1e3 * secs / steps, "higher_is_better": True, "scaling": "weak",
@@ -743,7 +921,8 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=None, help="timed steps (default 20; 400 for cylinder2d, "
                                                              "10 for sweep2d)")
-    ap.add_argument("--workload", default="box3d", choices=["box3d", "cylinder2d", "sweep2d", "fields3d"])
+    ap.add_argument("--workload", default="box3d",
+                    choices=["box3d", "cylinder2d", "heated2d", "sweep2d", "fields3d", "masks3d"])
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--shape", type=int, nargs=3, default=list(SHAPE), help="nx ny nz (2:1:1)")
@@ -752,7 +931,8 @@ def main():
                     help="sweep2d with N > 1: split the 64 instances over the ranks instead of replicating them")
     args = ap.parse_args()
     if args.steps is None:
-        args.steps = {"box3d": 20, "cylinder2d": 400, "sweep2d": 10, "fields3d": 20}[args.workload]
+        args.steps = {"box3d": 20, "cylinder2d": 400, "heated2d": 400, "sweep2d": 10, "fields3d": 20,
+                      "masks3d": 10}[args.workload]
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
@@ -761,6 +941,8 @@ def main():
             run_reference(args, rank)
         elif args.workload == "fields3d":
             run_reference_fields(args, rank)
+        elif args.workload == "masks3d":
+            run_reference_masks(args, rank)
         else:
             run_reference_2d(args, rank)
         return
@@ -772,7 +954,8 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     try:
-        {"box3d": run_ours, "cylinder2d": run_2d, "sweep2d": run_sweep, "fields3d": run_fields}[args.workload](
+        {"box3d": run_ours, "cylinder2d": run_2d, "heated2d": run_2d, "sweep2d": run_sweep, "fields3d": run_fields,
+         "masks3d": run_masks}[args.workload](
             args, rank, world, local_rank)
     finally:
         if world > 1:
