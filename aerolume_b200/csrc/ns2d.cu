@@ -746,74 +746,84 @@ struct ReportParams {
   double *heat, *theta_wall, *wall_heat, *heat_storage, *flow_heat;
 };
 
-// block-wide sum in a fixed order (every thread gets it)
-__device__ __forceinline__ double block_sum_fixed(double v, double *sh) {
-  v = warp_sum(v);
-  __syncthreads();
-  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
-  __syncthreads();
-  double t = 0.0;
-  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += sh[w];
-  return t;
-}
-
-// The step's heat report (core.py:974-995, physics.py:760-794): one block of 256 threads.
+// The step's heat report (core.py:974-995, physics.py:760-794): one block, each warp takes
+// whole sums (a body's heat over the three stages, the two grid sums of the heat storage, a
+// heat-flux body's wall temperature, one side's wall heat, the two flow-heat sums) in a fixed
+// lane order, so the sums are deterministic and no block barrier is needed.
 template <typename T>
 __global__ void heat_report2d_kernel(const __grid_constant__ ReportParams<T> P) {
   aero::pdl_wait();
-  __shared__ double sh[32];
-  const int nx = P.nx, ny = P.ny, tid = threadIdx.x, nt = blockDim.x;
+  const int nx = P.nx, ny = P.ny, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
   const T dt = *P.dt;
   const double per_dt = (double)(P.h2 / dt);
-  const int nh = P.n_temp, nr = 2 + P.n_flux;
-  for (int b = 0; b < nh; ++b) {
-    double tot = 0.0;
-    for (int st = 0; st < 3; ++st) {
-      double s = 0.0;
-      for (int e = tid; e < P.nblocks; e += nt) s += P.heat_part[((size_t)st * P.nblocks + e) * nh + b];
-      s = block_sum_fixed(s, sh);
-      tot = st == 0 ? s * (double)P.wgt[0] : tot + s * (double)P.wgt[st];
-    }
-    if (tid == 0) P.heat[b] = tot * per_dt;
-  }
-  double sums[2];
-  for (int q = 0; q < nr; ++q) {
-    double s = 0.0;
-    for (int e = tid; e < P.nblocks; e += nt) s += P.rep_part[(size_t)e * nr + q];
-    s = block_sum_fixed(s, sh);
-    if (q < 2) sums[q] = s;
-    else if (tid == 0) P.theta_wall[q - 2] = s;
-  }
-  if (tid == 0) P.heat_storage[0] = (sums[0] - sums[1]) * per_dt;
-  for (int side = 0; side < 4; ++side) {
-    const int mode = P.mode[side];
-    const int n = side < 2 ? ny : nx;
-    double rate = 0.0;
-    if (mode == AERO_TH2_TEMPERATURE || mode == AERO_TH2_INLET) {
-      double s = 0.0;
-      for (int e = tid; e < n; e += nt) {
-        const size_t g = side == 0 ? (size_t)e * nx : side == 1 ? (size_t)e * nx + nx - 1
-                                                    : side == 2 ? (size_t)e : (size_t)(ny - 1) * nx + e;
-        s += (double)(P.wval[side] - P.theta[g]);
+  const int nh = P.n_temp, nr = 2 + P.n_flux, nb = P.nblocks;
+  const int ntask = nh + 1 + P.n_flux + 4 + 1;
+  for (int task = threadIdx.x >> 5; task < ntask; task += nwarp) {
+    if (task < nh) {  // heat of temperature body `task`
+      const int b = task;
+      double tot = 0.0;
+      for (int st = 0; st < 3; ++st) {
+        double s = 0.0;
+        for (int e = lane; e < nb; e += 32) s += P.heat_part[((size_t)st * nb + e) * nh + b];
+        s = warp_sum(s);
+        tot = st == 0 ? s * (double)P.wgt[0] : tot + s * (double)P.wgt[st];
       }
-      rate = (double)(T(2) * P.kappa) * block_sum_fixed(s, sh);
-    } else if (mode == AERO_TH2_HEAT_FLUX) {
-      rate = (double)((P.kappa * P.wval[side]) * T((double)n * P.hd));
+      if (lane == 0) P.heat[b] = tot * per_dt;
+      continue;
     }
-    if (tid == 0) P.wall_heat[side] = rate;
-  }
-  double fin = 0.0, fout = 0.0;
-  if (!P.periodic && !P.closed) {
-    for (int e = tid; e < ny; e += nt) {
-      fin += (double)(P.u[(size_t)e * (nx + 1)] * P.theta_in);
-      fout += (double)(P.u[(size_t)e * (nx + 1) + nx] * P.theta[(size_t)e * nx + nx - 1]);
+    int t = task - nh;
+    if (t == 0) {  // heat storage: (sum theta - sum theta0) h^2 / dt
+      double s1 = 0.0, s0 = 0.0;
+      for (int e = lane; e < nb; e += 32) {
+        s1 += P.rep_part[(size_t)e * nr];
+        s0 += P.rep_part[(size_t)e * nr + 1];
+      }
+      s1 = warp_sum(s1);
+      s0 = warp_sum(s0);
+      if (lane == 0) P.heat_storage[0] = (s1 - s0) * per_dt;
+      continue;
     }
-    fin = block_sum_fixed(fin, sh) * (double)P.h;
-    fout = block_sum_fixed(fout, sh) * (double)P.h;
-  }
-  if (tid == 0) {
-    P.flow_heat[0] = fin;
-    P.flow_heat[1] = fout;
+    t -= 1;
+    if (t < P.n_flux) {  // wall temperature of heat-flux body t
+      double s = 0.0;
+      for (int e = lane; e < nb; e += 32) s += P.rep_part[(size_t)e * nr + 2 + t];
+      s = warp_sum(s);
+      if (lane == 0) P.theta_wall[t] = s;
+      continue;
+    }
+    t -= P.n_flux;
+    if (t < 4) {  // wall heat of side t (left, right, bottom, top)
+      const int side = t, mode = P.mode[side];
+      const int n = side < 2 ? ny : nx;
+      double rate = 0.0;
+      if (mode == AERO_TH2_TEMPERATURE || mode == AERO_TH2_INLET) {
+        double s = 0.0;
+        for (int e = lane; e < n; e += 32) {
+          const size_t g = side == 0 ? (size_t)e * nx : side == 1 ? (size_t)e * nx + nx - 1
+                                                      : side == 2 ? (size_t)e : (size_t)(ny - 1) * nx + e;
+          s += (double)(P.wval[side] - P.theta[g]);
+        }
+        rate = (double)(T(2) * P.kappa) * warp_sum(s);
+      } else if (mode == AERO_TH2_HEAT_FLUX) {
+        rate = (double)((P.kappa * P.wval[side]) * T((double)n * P.hd));
+      }
+      if (lane == 0) P.wall_heat[side] = rate;
+      continue;
+    }
+    // flow heat in at the inlet and out at the outlet of a tunnel
+    double fin = 0.0, fout = 0.0;
+    if (!P.periodic && !P.closed) {
+      for (int e = lane; e < ny; e += 32) {
+        fin += (double)(P.u[(size_t)e * (nx + 1)] * P.theta_in);
+        fout += (double)(P.u[(size_t)e * (nx + 1) + nx] * P.theta[(size_t)e * nx + nx - 1]);
+      }
+      fin = warp_sum(fin) * (double)P.h;
+      fout = warp_sum(fout) * (double)P.h;
+    }
+    if (lane == 0) {
+      P.flow_heat[0] = fin;
+      P.flow_heat[1] = fout;
+    }
   }
 }
 
