@@ -81,7 +81,7 @@ struct AeroNs3dPlan {
   size_t off_uh, off_vh, off_wh, off_up, off_vp, off_wp, off_tha, off_thb, off_pa, off_nu;
   size_t off_small, off_scalars, off_status, off_partials, off_psum, total;
   AxisInfo ax[3];
-  int zc, nblocks, nq;
+  int zc, zc_nu, nblocks, nq;    // z-planes per CTA of the stage and eddy-viscosity kernels
   int pu, pn;                     // row pitches of the stage-start u copy and of nu
 };
 
@@ -295,7 +295,7 @@ int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom
   NP.nx = nx;
   NP.ny = ny;
   NP.nz = nz;
-  NP.zc = p->zc;
+  NP.zc = p->zc_nu;
   NP.les = c.les;
   NP.inv_h = T(1.0 / c.h);
   NP.cd2 = T(c.les == AERO_LES_VREMAN ? c.les_c * c.h * c.h : c.les_c * c.les_c * c.h * c.h);
@@ -839,7 +839,12 @@ int aero_ns3d_plan_create(const AeroNs3dConfig *cfg, AeroNs3dPlan **plan) {
   p->off_small = take(8 * e);
   p->off_scalars = take(sizeof(double) * aero::SC_COUNT);
   p->off_status = take(sizeof(int) * 4);
-  p->zc = c.nz <= 16 ? c.nz : 16;
+  // planes per CTA: the stage kernel in chunks of about 19 planes (at 256 x 128 x 128: 896
+  // CTAs, two full waves at 3 CTAs per SM on 148 SMs; 16 planes gave 1024 CTAs, 2.3 waves, and
+  // a 4 % slower stage), the eddy-viscosity kernel (5 CTAs per SM) in chunks of 16
+  const int nch = std::max(1, (int)std::lround(c.nz / 19.0));
+  p->zc = (c.nz + nch - 1) / nch;
+  p->zc_nu = c.nz <= 16 ? c.nz : 16;
   p->nblocks = (int)(((nx + 31) / 32) * ((ny + 7) / 8) * ((nz + p->zc - 1) / p->zc));
   p->nq = c.nbody * 9 + (c.thermal ? c.n_tbody : 0);
   p->off_partials = take(sizeof(double) * 3 * (size_t)p->nblocks * std::max(p->nq, 1));
