@@ -29,6 +29,10 @@ a single stream are reported beside it).
 vorticity magnitude, Q-criterion, eddy viscosity) from the staggered velocity, and a
 million trilinear probes of the speed field are timed beside it.
 
+``--workload placed3d`` measures the box case with the placed physics in the step (a swirling
+velocity-regulated fan, a warm jet and a vent, a painted block, the PID step controller; no
+smoke, which jets and vents leave to the caller), with the same plan without them beside it.
+
 ``--workload masks3d`` measures mask construction (ns3d/geometry.py:385-495 with the exact
 signed distance): the masks, solid velocity and force weights of a closed 9024-triangle
 sphere of diameter 1 at 32 cells per diameter, rebuilt as a live attitude edit does.
@@ -178,10 +182,13 @@ def launches_per_step(plan):
     n += 1                                          # dt
     n += 1 if tunnel else 0                         # inlet / u0 outlet sums
     # a power-of-two x axis folds the divergence into the first transform pass and the
-    # pressure accumulation into the last one
-    fused = 8 <= c.nx <= 2048 and (c.nx & (c.nx - 1)) == 0
+    # pressure accumulation into the last one (not with jets / vents, whose mass sources enter
+    # the divergence in their own launch)
+    fused = 8 <= c.nx <= 2048 and (c.nx & (c.nx - 1)) == 0 and c.nport == 0
     per_stage = 1 + (0 if fused else 1) + 5 + (0 if fused else 1) + 1 + (2 if tunnel else 0) + (1 if les else 0)
+    per_stage += 1 if c.nport else 0                # div -= m of the jets and vents
     n += 3 * per_stage                              # [nu], [sums, corr], stage, [div], 5 transforms, [psi_w], correct
+    n += 1 if c.nfan else 0                         # disc velocities and PI thrust, once per step
     n += 1 if c.smoke else 0
     n += 1 if (c.nbody * 9 + (c.n_tbody if c.thermal else 0)) > 0 else 0   # partial-sum reduction
     n += 1                                          # finalize
@@ -890,6 +897,167 @@ def run_reference_masks(args, rank):
     print(json.dumps(line), flush=True)
 
 
+
+# ---------------------------------------------------------------------------------------
+# placed physics in the 3D step
+# ---------------------------------------------------------------------------------------
+PLACED_DESC = ("box on moving floor {}x{}x{} FP32, WALE, Boussinesq heat, with a swirling velocity-regulated fan, "
+               "a warm jet and a vent, a painted block and the PID step controller (no smoke)")
+
+
+def _placed_cpu(shape, steps=1):
+    """Seconds of ``steps`` oracle steps (after one untimed step) of the placed-physics case."""
+    from aerolume_b200.ns3d.workloads import placed_box
+    from oracle import ns3d as O
+    nx, ny, nz = shape
+    f32 = np.float32
+    ops, geom, th, fans, ports, paint, pid_target, u_floor = placed_box(nx, ny, nz, dtype="float32")
+    g32 = type(geom)(geom.window, nbody=geom.nbody)
+    for n in ("chi_u", "chi_v", "chi_w", "chi_c", "a_u", "a_v", "a_w", "k_u", "k_v", "k_w"):
+        setattr(g32, n, np.asarray(getattr(geom, n), f32))
+    items = [{"win": it["win"], "f": tuple(np.asarray(it["f" + g], f32) for g in "uvw"),
+              "s": tuple(np.asarray(it["s" + g], f32) for g in "uvw"),
+              "m": tuple(np.asarray(it["m" + g], f32) for g in "uvw")} for it in fans["items"]]
+    fs = O.FanState(items, fans["target"], fans["kp"], fans["ki"], fans["tmax"], fans["velocity_mode"], fans["swirl"],
+                    fans["any_swirl"], fans["thrust"], f32)
+    pitems = [{"win": it["win"], "kind": it["kind"], "theta": it["theta"], "m": np.asarray(it["m"], f32),
+               "f": tuple(np.asarray(it["f" + g], f32) for g in "uvw")} for it in ports["items"]]
+    ps_ = O.PortState(pitems, ports["mass_flux"], ports["leak"])
+    pnt = tuple(np.asarray(paint[g], f32) for g in "uvw")
+    pid = O.PidState(pid_target, f32)
+    ps = O.PoissonSolver3D(nx, ny, nz, ops.h, ops.periodic_axes, f32)
+    rng = np.random.default_rng(0)
+    u = (np.ones((nz, ny, nx + 1)) + 1e-3 * rng.standard_normal((nz, ny, nx + 1))).astype(f32)
+    v = (1e-3 * rng.standard_normal((nz, ny + 1, nx))).astype(f32)
+    w = (1e-3 * rng.standard_normal((nz + 1, ny, nx))).astype(f32)
+    theta = np.zeros((nz, ny, nx), f32)
+    kw = dict(th=th, paint=pnt, pid=pid, u_floor=u_floor, fans=fs, ports=ps_)
+    r = O.step3d_phys(u, v, w, f32(0), g32, ops, ps, theta=theta, **kw)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        r = O.step3d_phys(r.u, r.v, r.w, r.t, g32, ops, ps, theta=r.theta, **kw)
+    return time.perf_counter() - t0
+
+
+def run_reference_placed(args, rank):
+    if rank != 0:
+        return
+    nx, ny, nz = args.shape
+    steps = max(1, min(args.steps, 2))
+    secs = _placed_cpu(args.shape, steps)
+    val = nx * ny * nz * steps / secs / 1e6
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
+            "warmup": 1, "ms_per_step": 1e3 * secs / steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": PLACED_DESC.format(nx, ny, nz)},
+            "cpu_baseline": {"value": val, "unit": UNIT, "cores": _threads(), "kind": "port",
+                             "sample": f"{steps} full steps of the numpy oracle after 1 untimed step"},
+            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_placed(args, rank, world, local_rank):
+    import torch
+    from aerolume_b200.ns3d.plan import Ns3dPlan
+    from aerolume_b200.ns3d.workloads import initial_state, placed_box, placed_state
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    nx, ny, nz = args.shape
+    cells = nx * ny * nz
+    ops, geom, th, fans, ports, paint, pid_target, u_floor = placed_box(nx, ny, nz, dtype="float32")
+    fs, ps, pl, pid = placed_state(fans, ports, paint, pid_target, dev, "float32")
+    plan = Ns3dPlan(ops, geom, th, None, device=dev, paint=pl, pid=pid, u_floor=u_floor, fans=fs, ports=ps)
+    plain = Ns3dPlan(ops, geom, th, None, device=dev)
+    u, v, w = initial_state(ops, seed=rank, device=dev)
+    plan.project(u, v, w)
+    theta = torch.zeros(nz, ny, nx, device=dev)
+    t = torch.zeros((), device=dev)
+    state0 = [x.clone() for x in (u, v, w, theta)]
+
+    def runner(pl_):
+        out = pl_.empty_fields()
+        out["u"], out["v"], out["w"], out["theta"] = u, v, w, theta
+
+        def step():
+            pl_.step(u, v, w, t, theta0=theta, out=out)
+            t.copy_(out["t"])
+        return step, out
+
+    res = {}
+    for name, pl_ in (("placed", plan), ("plain", plain)):
+        for x, x0 in zip((u, v, w, theta), state0):
+            x.copy_(x0)
+        step, out = runner(pl_)
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        K = args.steps
+        s_ = torch.cuda.Stream(device=dev)
+        s_.wait_stream(torch.cuda.current_stream(dev))
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.stream(s_):
+            with torch.cuda.graph(g, stream=s_):
+                for _ in range(K):
+                    step()
+        torch.cuda.current_stream(dev).wait_stream(s_)
+        ms, clk = _time_graph(g, dist, local_rank, rank, dev)
+        res[name] = (ms / K, clk, pl_.status())
+        del g
+    # e2e of the placed step: state in from pinned host memory, state and coefficients out
+    host_in = {k: x.cpu().pin_memory() for k, x in (("u", u), ("v", v), ("w", w), ("theta", theta), ("t", t))}
+    o2 = plan.empty_fields()
+    host_out = {k: torch.empty(x.shape, dtype=x.dtype, pin_memory=True) for k, x in o2.items()}
+    d_in = {k: torch.empty_like(x, device=dev) for k, x in host_in.items()}
+    ke = max(3, min(args.steps, 10))
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(ke):
+        for k in host_in:
+            d_in[k].copy_(host_in[k], non_blocking=True)
+        plan.step(d_in["u"], d_in["v"], d_in["w"], d_in["t"], theta0=d_in["theta"], out=o2)
+        for k in host_out:
+            host_out[k].copy_(o2[k], non_blocking=True)
+        for k in ("u", "v", "w", "theta", "t"):
+            host_in[k], host_out[k] = host_out[k], host_in[k]
+    e1.record()
+    torch.cuda.synchronize()
+    ems = max_over_ranks(e0.elapsed_time(e1) / ke, dist, dev)
+    if rank != 0:
+        return
+    ms_step, clk, status = res["placed"]
+    peak, peak_kind = _peaks()
+    cpu = None
+    if not args.no_cpu:
+        secs = _placed_cpu(args.shape, 1)
+        cpu = {"value": cells / secs / 1e6, "unit": UNIT, "cores": _threads(), "kind": "port",
+               "sample": f"1 full {nx}x{ny}x{nz} step of the numpy oracle after 1 untimed step"}
+    # compulsory bytes per cell-step, FP32: plain 284 + theta 32 + LES pre-pass 12, and the
+    # painted solid fractions read once per stage (4 arrays, 48 B)
+    alg = (284.0 + 32.0 + 12.0 + 48.0) * cells
+    line = {"metric": METRIC, "value": world * cells / (ms_step * 1e-3) / 1e6, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": PLACED_DESC.format(nx, ny, nz), "cells": cells,
+                       "inputs_vs_l2": "working set ~1 GB > 126 MB L2 (no flush)", "parallelism": "replicas",
+                       "graph": f"{args.steps} steps, 1 replay"},
+            "plain_same_case": {"ms_per_step": res["plain"][0],
+                                "value": cells / (res["plain"][0] * 1e-3) / 1e6, "status": res["plain"][2]},
+            "roofline": {"bound": "hbm", "kernel": "whole step", "achieved": alg / (ms_step * 1e-3) / 1e9,
+                         "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                         "frac": alg / (ms_step * 1e-3) / 1e9 / peak, "traffic": None, "alg_bytes_per_step": alg},
+            "cpu_baseline": cpu,
+            "e2e": {"value": world * cells / (ems * 1e-3) / 1e6, "unit": UNIT,
+                    "h2d_bytes_per_step": int(sum(x.numel() * x.element_size() for x in host_in.values())),
+                    "d2h_bytes_per_step": int(sum(x.numel() * x.element_size() for x in host_out.values())),
+                    "ms_per_step": ems, "steps": ke},
+            "gpu_launches": launches_per_step(plan) * args.steps, "clocks": clk, "status": status}
+    print(json.dumps(line), flush=True)
+
+
 def run_reference_2d(args, rank):
     from aerolume_b200.ns2d.workloads import cylinder_tunnel, heated_cylinder, sweep_instances
     if rank != 0:
@@ -922,7 +1090,7 @@ def main():
     ap.add_argument("--steps", type=int, default=None, help="timed steps (default 20; 400 for cylinder2d, "
                                                              "10 for sweep2d)")
     ap.add_argument("--workload", default="box3d",
-                    choices=["box3d", "cylinder2d", "heated2d", "sweep2d", "fields3d", "masks3d"])
+                    choices=["box3d", "placed3d", "cylinder2d", "heated2d", "sweep2d", "fields3d", "masks3d"])
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--shape", type=int, nargs=3, default=list(SHAPE), help="nx ny nz (2:1:1)")
@@ -931,8 +1099,8 @@ def main():
                     help="sweep2d with N > 1: split the 64 instances over the ranks instead of replicating them")
     args = ap.parse_args()
     if args.steps is None:
-        args.steps = {"box3d": 20, "cylinder2d": 400, "heated2d": 400, "sweep2d": 10, "fields3d": 20,
-                      "masks3d": 10}[args.workload]
+        args.steps = {"box3d": 20, "placed3d": 20, "cylinder2d": 400, "heated2d": 400, "sweep2d": 10,
+                      "fields3d": 20, "masks3d": 10}[args.workload]
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
@@ -943,6 +1111,8 @@ def main():
             run_reference_fields(args, rank)
         elif args.workload == "masks3d":
             run_reference_masks(args, rank)
+        elif args.workload == "placed3d":
+            run_reference_placed(args, rank)
         else:
             run_reference_2d(args, rank)
         return
@@ -954,8 +1124,8 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     try:
-        {"box3d": run_ours, "cylinder2d": run_2d, "heated2d": run_2d, "sweep2d": run_sweep, "fields3d": run_fields,
-         "masks3d": run_masks}[args.workload](
+        {"box3d": run_ours, "placed3d": run_placed, "cylinder2d": run_2d, "heated2d": run_2d, "sweep2d": run_sweep,
+         "fields3d": run_fields, "masks3d": run_masks}[args.workload](
             args, rank, world, local_rank)
     finally:
         if world > 1:
