@@ -95,23 +95,26 @@ __global__ void copy_u_kernel(const T *__restrict__ u, T *__restrict__ out, int 
 // T <- clamp(T + kP (e - e_prev) + kI dt e, -tmax, tmax) with e = target - ud, and the swirl
 // amplitude swirl ud |ud|.
 template <typename T>
-__global__ void __launch_bounds__(256) fan_begin_kernel(const __grid_constant__ FanBeginParams<T> P) {
+__global__ void __launch_bounds__(1024) fan_begin_kernel(const __grid_constant__ FanBeginParams<T> P) {
   aero::pdl_wait();
-  __shared__ double red[3][8];
+  __shared__ double red[3][32];
   const auto &F = P.fan[blockIdx.x];
   const int nx = P.nx, ny = P.ny;
   const int k0 = F.win[0], j0 = F.win[2], i0 = F.win[4];
   const int wz = F.win[1] - k0, wy = F.win[3] - j0, wx = F.win[5] - i0;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   for (int c = 0; c < 3; ++c) {
-    // face window of component c: (wz + [c == 2]) x (wy + [c == 1]) x (wx + [c == 0])
+    // face window of component c: (wz + [c == 2]) x (wy + [c == 1]) x (wx + [c == 0]); the
+    // faces spread over all threads with 32-bit index arithmetic, four loads in flight each
     const int ez = wz + (c == 2), ey = wy + (c == 1), ex = wx + (c == 0);
-    const size_t n = (size_t)ez * ey * ex;
     const T *vel = c == 0 ? P.u0 : (c == 1 ? P.v0 : P.w0);
     const int rowlen = c == 0 ? nx + 1 : nx, rows = c == 1 ? ny + 1 : ny;
+    const int n = ez * ey * ex;
     double acc = 0.0;
-    for (size_t e = tid; e < n; e += blockDim.x) {
-      const int x = (int)(e % ex), y = (int)((e / ex) % ey), z = (int)(e / ((size_t)ex * ey));
+#pragma unroll 4
+    for (int e = tid; e < n; e += blockDim.x) {
+      const int x = e % ex, r = e / ex;
+      const int y = r % ey, z = r / ey;
       acc += (double)F.m[c][e] * (double)vel[((size_t)(k0 + z) * rows + (j0 + y)) * rowlen + (i0 + x)];
     }
     acc = warp_sum(acc);
@@ -622,7 +625,7 @@ cudaError_t launch_copy_u(const T *u, T *out, int nx, int ny, int nz, int pitch,
 template <typename T>
 cudaError_t launch_fan_begin(const FanBeginParams<T> &P, cudaStream_t s) {
   if (P.nfan <= 0) return cudaSuccess;
-  (void)aero::launch_k(fan_begin_kernel<T>, P.nfan, 256, 0, s, P);
+  (void)aero::launch_k(fan_begin_kernel<T>, P.nfan, 1024, 0, s, P);
   return cudaGetLastError();
 }
 
