@@ -223,3 +223,33 @@ def test_inputs_off_a_16_byte_boundary_give_the_same_step():
     torch.cuda.synchronize()
     for f in ("u", "v", "w", "p", "theta", "dye", "dt"):
         assert _rel(b[f], a[f].double().cpu().numpy()) < 1e-6, f
+
+
+def _divergence(u, v, w, h):
+    return ((u[..., 1:] - u[..., :-1]) + (v[:, 1:] - v[:, :-1]) + (w[1:] - w[:-1])) / h
+
+
+def test_largest_grid_step_is_divergence_free():
+    """The plain run the learned closure is judged against, 512 x 256 x 256 FP32 (33.5 M
+    cells, 512-point x lines in the transforms): a projected seeded state and one full step
+    (WALE, heat, smoke) stay finite and the device status stays clean.  max |div u| h / U of
+    the projected noise field is at the reference's FP32 level (4e-7 quoted; 1.2e-7 measured,
+    1e-6 asserted); after the step, whose last projection removes the O(1) divergence the
+    penalisation leaves at the body, it is 1.0e-5 (FP64: 2e-14), 5e-5 asserted."""
+    from aerolume_b200.ns3d.plan import Ns3dPlan
+    from aerolume_b200.ns3d.workloads import box_on_moving_floor, initial_state
+    ops, geom, th, src, _ = box_on_moving_floor(512, 256, 256, dtype="float32", seed=2)
+    plan = Ns3dPlan(ops, geom, th, src, smoke=True)
+    u, v, w = initial_state(ops, seed=2)
+    plan.project(u, v, w)
+    h = ops.h
+    assert _divergence(u, v, w, h).abs().max().item() * h < 1e-6
+    theta = torch.zeros(256, 256, 512, device="cuda")
+    dye = torch.zeros(256, 256, 512, device="cuda")
+    out = plan.step(u, v, w, torch.zeros((), device="cuda"), theta0=theta, dye0=dye)
+    torch.cuda.synchronize()
+    assert plan.status() == 0
+    for k in ("u", "v", "w", "p", "theta", "dye"):
+        assert torch.isfinite(out[k]).all(), k
+    assert _divergence(out["u"], out["v"], out["w"], h).abs().max().item() * h < 5e-5
+    assert out["theta"].max().item() > 0.0            # the hot body heats the fluid next to it
