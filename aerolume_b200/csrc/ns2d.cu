@@ -168,6 +168,7 @@ struct StageParams {
   int buoy_u, buoy_v;
   const T *vol_u, *vol_v;
   T *nut_out;
+  T *up_out, *vp_out;          // the stage-start (projected) face velocities, for the theta stage
   int nbody;
   double *partials;            // this stage's [block][4 nbody]
   unsigned long long *nut_max; // nu-only pass: max nu_t (ordered bits)
@@ -402,6 +403,12 @@ __global__ void __launch_bounds__(NT) stage2d_kernel(const __grid_constant__ Sta
       v_face(ny, vv[1], vpen[1], dv[1], vidx[1], vsh[1]);
       nvf = 2;
     }
+    if (P.up_out) {  // tile coordinates: u[j][i] -> U[j - j0 + 2][i - i0 + 2], v likewise
+      P.up_out[(size_t)j * (nx + 1) + i] = U[ty + 2][tx + 2];
+      if (i == nx - 1) P.up_out[(size_t)j * (nx + 1) + nx] = U[ty + 2][tx + 3];
+      P.vp_out[(size_t)j * nx + i] = V[ty + 2][tx + 2];
+      if (j == ny - 1) P.vp_out[(size_t)ny * nx + i] = V[ty + 3][tx + 2];
+    }
     P.uh[(size_t)j * (nx + 1) + i] = uv[0];
     if (nuf == 2 && !P.periodic) P.uh[(size_t)j * (nx + 1) + nx] = uv[1];
     if (P.periodic && i == 0) P.uh[(size_t)j * (nx + 1) + nx] = uv[0];
@@ -556,7 +563,7 @@ struct ThetaParams {
   T kappa, inv_prt, theta_in, eta_t;
   const T *thp, *th0;         // stage-start and step-start theta (ny, nx)
   T *th;                      // the stage's theta
-  const T *up, *vp, *psi;     // stage-start velocity: u_hat and the previous psi, or u0 / v0
+  const T *upf, *vpf;         // stage-start face velocities (ny, nx+1), (ny+1, nx)
   const T *nut;               // (ny, nx) nu_t of the stage, NULL without LES
   int mode[4];                // AERO_TH2_* of left, right, bottom, top
   T wval[4];
@@ -659,12 +666,8 @@ __global__ void __launch_bounds__(NT) theta2d_kernel(const __grid_constant__ The
   if (in) {
     const int r = ty + 2, c = tx + 2;
     const T ctr = S[r][c];
-    auto uface = [&](int f) {
-      return P.psi ? projected_u<T>(P.up, P.psi, nx, P.periodic, P.inv_h, j, f) : __ldg(P.up + (size_t)j * (nx + 1) + f);
-    };
-    auto vface = [&](int f) {
-      return P.psi ? projected_v<T>(P.vp, P.psi, nx, ny, P.periodic, P.inv_h, f, i) : __ldg(P.vp + (size_t)f * nx + i);
-    };
+    auto uface = [&](int f) { return __ldg(P.upf + (size_t)j * (nx + 1) + f); };
+    auto vface = [&](int f) { return __ldg(P.vpf + (size_t)f * nx + i); };
     const T fx0 = muscl_flux<T>(S[r][c - 2], S[r][c - 1], ctr, S[r][c + 1], uface(i));
     const T fx1 = muscl_flux<T>(S[r][c - 1], ctr, S[r][c + 1], S[r][c + 2], uface(i + 1));
     const T fy0 = muscl_flux<T>(S[r - 2][c], S[r - 1][c], ctr, S[r + 1][c], vface(j));
@@ -869,7 +872,11 @@ struct AeroNs2dPlan {
   size_t esz;
   size_t nu, nv, nc;          // element counts of u, v and cells
   size_t off_uh, off_vh, off_up, off_vp, off_pa, off_small, off_scalars, off_zero, off_partials, total;
-  size_t off_nut, off_tb0, off_tb1, off_hpart, off_rpart;  // heat transfer only
+  size_t off_nut, off_tb0, off_tb1, off_hpart, off_rpart, off_upf, off_vpf;  // heat transfer only
+  // heat transfer: each theta stage runs on a side stream, forked after its stage kernel and
+  // joined before the next one, so it overlaps the stage's pressure solve
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork[3] = {}, ev_join[3] = {};
   AxisInfo ax[2];             // x (n = nx), y (n = ny)
   int gx, gy, nblocks, nq;
 };
@@ -1027,6 +1034,8 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
     S.vol_u = c.has_vol ? static_cast<const T *>(g->vol_u) : nullptr;
     S.vol_v = c.has_vol ? static_cast<const T *>(g->vol_v) : nullptr;
     S.nut_out = les ? nutb : nullptr;
+    S.up_out = reinterpret_cast<T *>(ws + p->off_upf);
+    S.vp_out = reinterpret_cast<T *>(ws + p->off_vpf);
     TP.nx = nx;
     TP.ny = ny;
     TP.periodic = c.periodic;
@@ -1077,22 +1086,28 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
     P.partials = partials + (size_t)st * p->nblocks * std::max(p->nq, 1);
     P.dt_here = st == 0;
     const T *th_in = st == 0 ? static_cast<const T *>(f->theta0) : tb[(st - 1) % 2];
-    if (thermal) P.thp = th_in;
+    if (thermal) {
+      P.thp = th_in;
+      // the previous theta stage reads this stage's outputs of the last one (nu_t, face velocities)
+      if (st > 0) AERO_CUDA_TRY(cudaStreamWaitEvent(s, p->ev_join[st - 1], 0));
+    }
     (void)aero::launch_k(stage2d_kernel<T, false>, grid, block, 0, s, P);
     AERO_CUDA_TRY(cudaGetLastError());
-    if (thermal) {  // before the transforms overwrite the previous psi
+    if (thermal) {  // theta of this stage on the side stream, beside the pressure solve
       ThetaParams<T> Q = TP;
       Q.thp = th_in;
       Q.th = st == 2 ? static_cast<T *>(f->theta) : tb[st % 2];
-      Q.up = P.up;
-      Q.vp = P.vp;
-      Q.psi = P.psi;
+      Q.upf = S.up_out;
+      Q.vpf = S.vp_out;
       Q.a = P.a;
       Q.b = P.b;
       Q.heat_part = reinterpret_cast<double *>(ws + p->off_hpart) + (size_t)st * p->nblocks * std::max(c.n_temp, 1);
       Q.rep_part = st == 2 ? reinterpret_cast<double *>(ws + p->off_rpart) : nullptr;
-      (void)aero::launch_k(theta2d_kernel<T>, grid, block, 0, s, Q);
+      AERO_CUDA_TRY(cudaEventRecord(p->ev_fork[st], s));
+      AERO_CUDA_TRY(cudaStreamWaitEvent(p->side, p->ev_fork[st], 0));
+      (void)aero::launch_k(theta2d_kernel<T>, grid, block, 0, p->side, Q);
       AERO_CUDA_TRY(cudaGetLastError());
+      AERO_CUDA_TRY(cudaEventRecord(p->ev_join[st], p->side));
     }
     const int acc_mode = st == 0 ? 0 : (st == 1 ? 1 : 2);
     if (fused) {
@@ -1122,6 +1137,7 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
     }
   }
   if (thermal) {
+    AERO_CUDA_TRY(cudaStreamWaitEvent(s, p->ev_join[2], 0));
     ReportParams<T> R{};
     R.nx = nx;
     R.ny = ny;
@@ -1251,6 +1267,17 @@ int aero_ns2d_plan_create(const AeroNs2dConfig *cfg, AeroNs2dPlan **plan) {
     p->off_tb1 = take(p->nc * e);
     p->off_hpart = take(sizeof(double) * 3 * (size_t)p->nblocks * std::max(c.n_temp, 1));
     p->off_rpart = take(sizeof(double) * (size_t)p->nblocks * (2 + c.n_flux));
+    p->off_upf = take(p->nu * e);
+    p->off_vpf = take(p->nv * e);
+    bool ok = cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking) == cudaSuccess;
+    for (int q = 0; q < 3 && ok; ++q)
+      ok = cudaEventCreateWithFlags(&p->ev_fork[q], cudaEventDisableTiming) == cudaSuccess &&
+           cudaEventCreateWithFlags(&p->ev_join[q], cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) {
+      (void)cudaGetLastError();
+      aero_ns2d_plan_destroy(p);
+      return set_error(AERO_ECUDA, "cannot create the heat-transfer side stream");
+    }
   }
   aero_host::axis_setup(p->ax[0], c.nx, c.periodic != 0, e);
   aero_host::axis_setup(p->ax[1], c.ny, c.periodic != 0, e);
@@ -1260,7 +1287,15 @@ int aero_ns2d_plan_create(const AeroNs2dConfig *cfg, AeroNs2dPlan **plan) {
   return AERO_OK;
 }
 
-void aero_ns2d_plan_destroy(AeroNs2dPlan *plan) { delete plan; }
+void aero_ns2d_plan_destroy(AeroNs2dPlan *plan) {
+  if (!plan) return;
+  for (int q = 0; q < 3; ++q) {
+    if (plan->ev_fork[q]) cudaEventDestroy(plan->ev_fork[q]);
+    if (plan->ev_join[q]) cudaEventDestroy(plan->ev_join[q]);
+  }
+  if (plan->side) cudaStreamDestroy(plan->side);
+  delete plan;
+}
 
 size_t aero_ns2d_workspace_bytes(const AeroNs2dPlan *plan) { return plan ? plan->total : 0; }
 
