@@ -103,8 +103,6 @@ struct SdfParams {
   int *votes;                // (nface) outward-side tally
   const int *orient;         // the mesh's orientation sign
   T *out;                    // (npt) signed distance
-  int *bad_index;            // set when a face names a vertex out of range (the access is
-                             // clamped to vertex 0; the host checks the faces beforehand)
 };
 
 template <typename T>
@@ -126,14 +124,12 @@ __device__ __forceinline__ void point_of(const SdfParams<T> &P, long long q, T &
 
 template <typename T>
 __device__ __forceinline__ Tri<T> load_tri(const SdfParams<T> &P, int t) {
+  // the caller checks the faces (the Python layer does, before the upload); an index out of
+  // range is clamped to vertex 0 here so that no access leaves the vertex array
   int id[3];
   for (int c = 0; c < 3; ++c) {
-    int v = P.faces[3 * t + c];
-    if (v < 0 || v >= P.nvert) {
-      atomicExch(P.bad_index, 1);
-      v = 0;
-    }
-    id[c] = v;
+    const int v = P.faces[3 * t + c];
+    id[c] = (v < 0 || v >= P.nvert) ? 0 : v;
   }
   const T *a = P.verts + 3 * (size_t)id[0], *b = P.verts + 3 * (size_t)id[1], *c = P.verts + 3 * (size_t)id[2];
   return Tri<T>{a[0], a[1], a[2], b[0], b[1], b[2], c[0], c[1], c[2]};
@@ -351,7 +347,6 @@ int sdf_pass(const T *verts, int nvert, const int32_t *faces, int nface, const T
   P.votes = reinterpret_cast<int *>(take(sizeof(int) * (nface + 1)));
   int *misc = reinterpret_cast<int *>(take(2 * sizeof(int)));
   P.orient = misc;
-  P.bad_index = misc + 1;
   P.out = out;
   const unsigned blocks = (unsigned)((npt + NT - 1) / NT);
   if (nface > 0) {

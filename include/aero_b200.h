@@ -272,7 +272,8 @@ typedef struct {
 } AeroMaskConfig;
 
 /* One immersed mesh (ns3d/config.py:81 ImmersedMesh): device vertices (nvert, 3) in the
- * config dtype, device faces (nface, 3) of vertex indices in 0 .. nvert-1, rigid spin. */
+ * config dtype, device faces (nface, 3) of vertex indices in 0 .. nvert-1 (the caller checks
+ * them: the kernels clamp an index out of range to vertex 0 instead of faulting), rigid spin. */
 typedef struct {
   const void *vertices;
   int32_t nvert;

@@ -102,3 +102,21 @@ def test_box_masks_at_bench_size_equal_closed_form(dtype):
     assert tuple(g.window) == tuple(geom.window)
     for n in NAMES:
         _cmp(getattr(g, n), getattr(geom, n), TOL[dtype], n)
+
+
+def test_bad_meshes_are_refused():
+    """A face naming a vertex that does not exist, a mesh without faces and more than eight
+    bodies raise before anything is launched."""
+    from aerolume_b200.ns3d.masks import build_geometry3d, mesh_signed_distance
+    meta, ops, bodies = masks_case(Z, "box_floor_64")
+    v, f = bodies[0].vertices, bodies[0].faces
+    bad = f.copy()
+    bad[3, 1] = len(v)
+    with pytest.raises(ValueError):
+        build_geometry3d([(v, bad)], ops, device="cuda")
+    with pytest.raises(ValueError):
+        build_geometry3d([(v, f[:0])], ops, device="cuda")
+    with pytest.raises(RuntimeError):
+        build_geometry3d([(v, f)] * 9, ops, device="cuda")
+    with pytest.raises(ValueError):
+        mesh_signed_distance(v, bad, torch.zeros(4, 3, device="cuda", dtype=torch.float64))
