@@ -132,3 +132,26 @@ def test_poisson2d_solves_exactly(shape):
         psi = plan.poisson_solve(f)
         lap = O2.PoissonSolver2D.laplacian(psi.cpu().numpy(), 0.05, per)
         assert np.abs(lap - f.cpu().numpy()).max() < 1e-9 * f.abs().max().item()
+
+
+@pytest.mark.parametrize("name", ["cylinder_upwind_f64", "cylinder_heated_f64", "periodic_cold_body_f64"])
+def test_given_dt_matches_oracle(name):
+    """dt passed in (``step_full(..., dt)``): used as given, against the oracle's step with the
+    same dt (with heat transfer its dt limits do not apply either)."""
+    meta, plan, ins, arr = _setup(name)
+    _, ops, geom, _ = load_case2d(name)
+    tp = thermal2d_from_case(meta, arr)
+    dt_val = 0.6 * float(arr["out1_dt"])
+    out = plan.step(**ins, dt=torch.tensor(dt_val, device="cuda", dtype=torch.float64))
+    torch.cuda.synchronize()
+    ps = O2.PoissonSolver2D(ops.nx, ops.ny, ops.h, ops.periodic, np.float64)
+    t0 = np.float64(arr["in_t"])
+    if tp is None:
+        r = O2.step2d(arr["in_u"], arr["in_v"], t0, geom, ops, ps, dye=arr.get("in_dye"), dt=np.float64(dt_val))
+    else:
+        r = O2.step2d_thermal(arr["in_u"], arr["in_v"], t0, arr["in_theta"], geom, ops, ps, tp, dt=np.float64(dt_val))
+    assert float(out["dt"]) == dt_val
+    for f, ref in (("u", r.u), ("v", r.v), ("p", r.p)):
+        assert _rel(out[f], ref) < 1e-10, (f, _rel(out[f], ref))
+    if tp is not None:
+        assert _rel(out["theta"], r.theta) < 1e-10

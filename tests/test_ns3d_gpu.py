@@ -253,3 +253,25 @@ def test_largest_grid_step_is_divergence_free():
         assert torch.isfinite(out[k]).all(), k
     assert _divergence(out["u"], out["v"], out["w"], h).abs().max().item() * h < 5e-5
     assert out["theta"].max().item() > 0.0            # the hot body heats the fluid next to it
+
+
+@pytest.mark.parametrize("name", ["tunnel_wale_heat_smoke_f64", "periodic_vreman_f64", "closed_central_cavity_f64"])
+def test_given_dt_matches_oracle(name):
+    """dt passed in (the solver's fixed-dt and restart paths, core.py:765 ``dt=``): the step uses
+    it as given, against the oracle's step with the same dt; the heat-transfer limits and the
+    CFL rule do not touch it."""
+    meta, plan, ins, arr = _plan_and_inputs(name)
+    npd = np.float64
+    dt_val = 0.6 * float(arr["out1_dt"])
+    dt = torch.tensor(dt_val, device="cuda", dtype=torch.float64)
+    out = plan.step(ins["u0"], ins["v0"], ins["w0"], ins["t0"], theta0=ins.get("theta0"), dye0=ins["dye0"], dt=dt)
+    torch.cuda.synchronize()
+    _, ops, geom, th, src, _ = load_case(name)
+    ps = O.PoissonSolver3D(ops.nx, ops.ny, ops.nz, ops.h, ops.periodic_axes, npd)
+    r = O.step3d_phys(arr["in_u"], arr["in_v"], arr["in_w"], npd(arr["in_t"]), geom, ops, ps, th=th,
+                      theta=arr.get("in_theta"), dt=npd(dt_val))
+    assert float(out["dt"]) == dt_val
+    for f, ref in (("u", r.u), ("v", r.v), ("w", r.w), ("p", r.p)):
+        assert _rel(out[f], ref) < 1e-10, (f, _rel(out[f], ref))
+    if th is not None:
+        assert _rel(out["theta"], r.theta) < 1e-10
