@@ -119,7 +119,7 @@ struct Dt2dThermal {
   double kappa, inv_prt, two_over_h, diff_over_h2, abs_ri, cfl, h;
 };
 
-template <typename T>
+template <typename T, bool HEAT>
 __device__ __forceinline__ T dt2d_value(int mode, const T *dt_in, double dt_fixed, const unsigned long long *bits,
                                         double cfl_h, double nu, double visc_h2, int les, const Dt2dThermal &th) {
   if (mode == 2) return *dt_in;
@@ -132,7 +132,7 @@ __device__ __forceinline__ T dt2d_value(int mode, const T *dt_in, double dt_fixe
   const T nut = les ? T(nu) + nut_max : T(nu);
   const T dv = T(visc_h2) / nut;
   dt = dv < dt ? dv : dt;
-  if (th.on) {
+  if (HEAT && th.on) {
     const T kap = les ? T(th.kappa) + nut_max * T(th.inv_prt) : T(th.kappa);
     const T speed = usum > T(0) || usum != usum ? usum : T(0);
     const T rate = speed * T(th.two_over_h) + kap * T(th.diff_over_h2);
@@ -183,8 +183,10 @@ struct StageParams {
 };
 
 // One RK stage of the u- and v-faces of a 32 x 8 tile; NU_ONLY: only the maximum eddy
-// viscosity of the tile's cells (the first stage's dt needs it before the update).
-template <typename T, bool NU_ONLY>
+// viscosity of the tile's cells (the first stage's dt needs it before the update); HEAT: the
+// heat-transfer instantiation (thermal dt limits, buoyancy and its force share, nu_t and the
+// stage-start face velocities handed to the theta stage), so the plain step carries none of it.
+template <typename T, bool NU_ONLY, bool HEAT>
 __global__ void __launch_bounds__(NT) stage2d_kernel(const __grid_constant__ StageParams<T> P) {
   aero::pdl_wait();
   __shared__ T U[UY][UX];
@@ -197,7 +199,7 @@ __global__ void __launch_bounds__(NT) stage2d_kernel(const __grid_constant__ Sta
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
   const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
   const bool tunnel = !P.periodic && !P.closed;
-  const T dt = P.dt_here ? dt2d_value<T>(P.dt_mode, P.dt_in, P.dt_fixed, P.dt_bits, P.dt_cfl_h, P.dt_nu, P.dt_visc_h2,
+  const T dt = P.dt_here ? dt2d_value<T, HEAT>(P.dt_mode, P.dt_in, P.dt_fixed, P.dt_bits, P.dt_cfl_h, P.dt_nu, P.dt_visc_h2,
                                          P.dt_les, P.dt_th)
                          : *P.dt;
   if (P.dt_here && blockIdx.x == 0 && blockIdx.y == 0 && tid == 0) *P.dt_store = dt;
@@ -265,7 +267,7 @@ __global__ void __launch_bounds__(NT) stage2d_kernel(const __grid_constant__ Sta
         nu = nu * (T(1) - chi);
       }
       NU[r][c] = nu;
-      if (!NU_ONLY && P.nut_out && r >= 1 && r <= TY && c >= 1 && c <= TX && jc < ny && ic < nx)
+      if (HEAT && !NU_ONLY && P.nut_out && r >= 1 && r <= TY && c >= 1 && c <= TX && jc < ny && ic < nx)
         P.nut_out[(size_t)jc * nx + ic] = nu;
       TXX[r][c] = T(2) * nu * g11;
       TYY[r][c] = T(2) * nu * g22;
@@ -331,7 +333,7 @@ __global__ void __launch_bounds__(NT) stage2d_kernel(const __grid_constant__ Sta
       uh = un;
       pen = true;
     }
-    if (P.buoy_u) {  // face average of theta (0 on boundary faces of a bounded domain)
+    if (HEAT && P.buoy_u) {  // face average of theta (0 on boundary faces of a bounded domain)
       T tf;
       const size_t tr = (size_t)j * nx;
       if (fi > 0 && fi < nx) tf = T(0.5) * (P.thp[tr + fi] + P.thp[tr + fi - 1]);
@@ -370,7 +372,7 @@ __global__ void __launch_bounds__(NT) stage2d_kernel(const __grid_constant__ Sta
       vh = vn;
       pen = true;
     }
-    if (P.buoy_v) {
+    if (HEAT && P.buoy_v) {
       T tf;
       if (fj > 0 && fj < ny) tf = T(0.5) * (P.thp[(size_t)fj * nx + i] + P.thp[(size_t)(fj - 1) * nx + i]);
       else tf = P.periodic ? T(0.5) * (P.thp[i] + P.thp[(size_t)(ny - 1) * nx + i]) : T(0);
@@ -403,7 +405,7 @@ __global__ void __launch_bounds__(NT) stage2d_kernel(const __grid_constant__ Sta
       v_face(ny, vv[1], vpen[1], dv[1], vidx[1], vsh[1]);
       nvf = 2;
     }
-    if (P.up_out) {  // tile coordinates: u[j][i] -> U[j - j0 + 2][i - i0 + 2], v likewise
+    if (HEAT && P.up_out) {  // tile coordinates: u[j][i] -> U[j - j0 + 2][i - i0 + 2], v likewise
       P.up_out[(size_t)j * (nx + 1) + i] = U[ty + 2][tx + 2];
       if (i == nx - 1) P.up_out[(size_t)j * (nx + 1) + nx] = U[ty + 2][tx + 3];
       P.vp_out[(size_t)j * nx + i] = V[ty + 2][tx + 2];
@@ -1005,7 +1007,7 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
       N.up = u0;
       N.vp = v0;
       N.nut_max = bits + aero::SC_NUTMAX;
-      (void)aero::launch_k(stage2d_kernel<T, true>, grid, block, 0, s, N);
+      (void)aero::launch_k(stage2d_kernel<T, true, false>, grid, block, 0, s, N);
       AERO_CUDA_TRY(cudaGetLastError());
     }
   }
@@ -1091,7 +1093,10 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
       // the previous theta stage reads this stage's outputs of the last one (nu_t, face velocities)
       if (st > 0) AERO_CUDA_TRY(cudaStreamWaitEvent(s, p->ev_join[st - 1], 0));
     }
-    (void)aero::launch_k(stage2d_kernel<T, false>, grid, block, 0, s, P);
+    if (thermal)
+      (void)aero::launch_k(stage2d_kernel<T, false, true>, grid, block, 0, s, P);
+    else
+      (void)aero::launch_k(stage2d_kernel<T, false, false>, grid, block, 0, s, P);
     AERO_CUDA_TRY(cudaGetLastError());
     if (thermal) {  // theta of this stage on the side stream, beside the pressure solve
       ThetaParams<T> Q = TP;
