@@ -5,8 +5,10 @@
 //
 // Per body and staggered grid (u, v, w faces and cells of the body window), one thread per
 // grid point scans all triangles of the body, staged in shared memory 256 at a time: the
-// nearest triangle (first index of the smallest squared distance) and the generalised
-// winding number (sum of signed solid angles; inside when its magnitude exceeds 1/2).  Each
+// nearest triangle (first index of the smallest squared distance; a triangle whose bounding
+// ball lies farther than the nearest distance so far is skipped, which cannot change the
+// selection) and the generalised winding number (sum of signed solid angles over every
+// triangle; inside when its magnitude exceeds 1/2).  Each
 // point nearest to a face's interior and off its plane votes for the face's outward side
 // (integer atomics, so the tally is exact); a second pass gives a point within the plane
 // zone of its face that face's signed plane distance with the voted side (else the mesh's
@@ -29,6 +31,7 @@ constexpr int TCH = 256;  // triangles per shared-memory chunk
 template <typename T>
 struct Tri {
   T ax, ay, az, bx, by, bz, cx, cy, cz;
+  T mx, my, mz, rad;  // a ball holding the triangle: its centroid and the largest vertex distance
 };
 
 // squared distance of p to the triangle (geometry.py:68-109)
@@ -132,7 +135,16 @@ __device__ __forceinline__ Tri<T> load_tri(const SdfParams<T> &P, int t) {
     id[c] = (v < 0 || v >= P.nvert) ? 0 : v;
   }
   const T *a = P.verts + 3 * (size_t)id[0], *b = P.verts + 3 * (size_t)id[1], *c = P.verts + 3 * (size_t)id[2];
-  return Tri<T>{a[0], a[1], a[2], b[0], b[1], b[2], c[0], c[1], c[2]};
+  Tri<T> r{a[0], a[1], a[2], b[0], b[1], b[2], c[0], c[1], c[2], T(0), T(0), T(0), T(0)};
+  r.mx = (r.ax + r.bx + r.cx) * T(1.0 / 3.0);
+  r.my = (r.ay + r.by + r.cy) * T(1.0 / 3.0);
+  r.mz = (r.az + r.bz + r.cz) * T(1.0 / 3.0);
+  auto d2 = [&](T x, T y, T z) { return (x - r.mx) * (x - r.mx) + (y - r.my) * (y - r.my) + (z - r.mz) * (z - r.mz); };
+  T r2 = d2(r.ax, r.ay, r.az);
+  r2 = fmax(r2, d2(r.bx, r.by, r.bz));
+  r2 = fmax(r2, d2(r.cx, r.cy, r.cz));
+  r.rad = sqrt(r2);
+  return r;
 }
 
 // nearest triangle, winding number, distance, plane distance and the face votes
@@ -145,6 +157,7 @@ __global__ void __launch_bounds__(NT) sdf_search_kernel(const __grid_constant__ 
   T px = T(0), py = T(0), pz = T(0);
   if (live) point_of<T>(P, q, px, py, pz);
   T dmin = std::numeric_limits<T>::infinity();  // nearest so far: the first index of the minimum
+  T smin = dmin;                                // its square root, for the ball test
   int imin = 0;
   T wsum = T(0);
   for (int t0 = 0; t0 < P.nface; t0 += TCH) {
@@ -156,10 +169,19 @@ __global__ void __launch_bounds__(NT) sdf_search_kernel(const __grid_constant__ 
       T ws = T(0);
       for (int e = 0; e < n; ++e) {
         const Tri<T> t = S[e];
-        const T d2 = tri_d2<T>(px, py, pz, t);
-        if (d2 < dmin) {
-          dmin = d2;
-          imin = t0 + e;
+        // the triangle lies in its ball, so its distance is at least |p - m| - rad; when that
+        // exceeds the nearest distance so far (with a 5e-5 relative margin for rounding) it
+        // cannot be the nearest and its exact distance is skipped.  The winding number still
+        // takes every triangle.
+        const T qx = px - t.mx, qy = py - t.my, qz = pz - t.mz;
+        const T lim = smin + t.rad;
+        if (!(qx * qx + qy * qy + qz * qz > lim * lim * T(1.0001))) {
+          const T d2 = tri_d2<T>(px, py, pz, t);
+          if (d2 < dmin) {
+            dmin = d2;
+            smin = sqrt(d2);
+            imin = t0 + e;
+          }
         }
         ws += solid_angle<T>(px, py, pz, t);
       }
