@@ -155,3 +155,49 @@ def test_given_dt_matches_oracle(name):
         assert _rel(out[f], ref) < 1e-10, (f, _rel(out[f], ref))
     if tp is not None:
         assert _rel(out["theta"], r.theta) < 1e-10
+
+
+def test_two_temperature_bodies_split_heat_like_oracle():
+    """Two temperature bodies sharing the window (the heat split by their shares w_t,
+    physics.py:733-757), built from the heated-cylinder case: theta and both bodies' heat
+    against the oracle in FP64."""
+    import dataclasses
+    from aerolume_b200.ns2d.plan import Ns2dPlan
+    meta, ops, geom, arr = load_case2d("cylinder_heated_f64")
+    tp = thermal2d_from_case(meta, arr)
+    wy, wx = tp.chi_t.shape
+    share = np.linspace(0.2, 0.8, wx)[None, :] * np.ones((wy, 1))
+    tp2 = dataclasses.replace(tp, temp_ids=(0, 1), w_t=np.stack([share, 1.0 - share]),
+                              a_t=tp.chi_t * (0.5 + 0.5 * share))
+    plan = Ns2dPlan(ops, geom, thermal=tp2)
+    dt = torch.float64
+    out = plan.step(_dev(arr["in_u"], dt), _dev(arr["in_v"], dt), _dev(arr["in_t"], dt),
+                    theta0=_dev(arr["in_theta"], dt))
+    torch.cuda.synchronize()
+    ps = O2.PoissonSolver2D(ops.nx, ops.ny, ops.h, ops.periodic, np.float64)
+    r = O2.step2d_thermal(arr["in_u"], arr["in_v"], np.float64(arr["in_t"]), arr["in_theta"], geom, ops, ps, tp2)
+    assert _rel(out["theta"], r.theta) < 1e-10
+    assert _rel(out["u"], r.u) < 1e-10
+    ref = r.report["heat"]
+    assert ref.shape == (2,) and np.abs(ref).min() > 0
+    assert np.abs(out["heat"].cpu().numpy() - ref).max() <= 1e-9 * np.abs(ref).max()
+
+
+def test_dye_with_heat_transfer_follows_the_step_velocity():
+    """A plan with both dye and heat transfer: theta as without dye, and the dye advanced with
+    the step's final velocity and dt and cleared in the solids (core.py:959-962)."""
+    from aerolume_b200.ns2d.plan import Ns2dPlan
+    meta, ops, geom, arr = load_case2d("cylinder_heated_f64")
+    tp = thermal2d_from_case(meta, arr)
+    ops.dye_inlet = np.linspace(0.0, 1.0, ops.ny)            # an inlet comb for the dye
+    plan = Ns2dPlan(ops, geom, dye=True, thermal=tp)
+    dt = torch.float64
+    g = np.random.default_rng(7)
+    dye0 = g.uniform(0.0, 1.0, (ops.ny, ops.nx))
+    out = plan.step(_dev(arr["in_u"], dt), _dev(arr["in_v"], dt), _dev(arr["in_t"], dt),
+                    dye0=_dev(dye0, dt), theta0=_dev(arr["in_theta"], dt))
+    torch.cuda.synchronize()
+    assert _rel(out["theta"], arr["out1_theta"]) < 1e-10
+    u, v, step_dt = (out[k].cpu().numpy() for k in ("u", "v", "dt"))
+    want = O2.zero_dye_in_solids(O2.advect_dye2d(dye0, u, v, step_dt, ops), geom)
+    assert _rel(out["dye"], want) < 1e-12
