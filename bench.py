@@ -83,20 +83,19 @@ def _config(nx, ny, nz, extra=None):
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region (median SM clock, throttle reasons)."""
+    """nvidia-smi sampling during the timed region (median SM clock, throttle reasons); the
+    samples come back through a pipe (about 100 bytes every 100 ms)."""
 
     def __init__(self, index):
         self.proc = None
-        self.path = ROOT / "gpurun_out" / f"clocks_{os.getpid()}.csv"
         try:
-            self.path.parent.mkdir(exist_ok=True)
-            self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={index}",
                  "--query-gpu=clocks.sm,clocks.max.sm,clocks_event_reasons.active,"
                  "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
-                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.fh, stderr=subprocess.DEVNULL)
+                 "--format=csv,noheader,nounits", "-lms", "100"], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.proc = None
 
@@ -105,15 +104,11 @@ class Clocks:
             return None
         self.proc.terminate()
         try:
-            self.proc.wait(timeout=5)
+            text, _ = self.proc.communicate(timeout=5)
         except Exception:
             self.proc.kill()
-        self.fh.close()
-        rows = [r.split(",") for r in self.path.read_text().splitlines() if r.strip()]
-        try:
-            self.path.unlink()
-        except OSError:
-            pass
+            text, _ = self.proc.communicate()
+        rows = [r.split(",") for r in (text or "").splitlines() if r.strip()]
         sm = [float(r[0]) for r in rows if r[0].strip().replace(".", "").isdigit()]
         if not sm:
             return None

@@ -44,7 +44,7 @@ extern "C" {
 
 #define AERO_OK 0
 #define AERO_EINVAL -1        /* invalid argument or inconsistent configuration     */
-#define AERO_EUNSUPPORTED -2  /* a feature this build does not implement: no fallback */
+#define AERO_EUNSUPPORTED -2  /* a feature the library does not implement: no fallback */
 #define AERO_ECUDA -3         /* a CUDA launch or runtime call failed                */
 
 #define AERO_MAX_BODIES 8

@@ -230,7 +230,7 @@ def _divergence(u, v, w, h):
 
 
 def test_largest_grid_step_is_divergence_free():
-    """The plain run the learned closure is judged against, 512 x 256 x 256 FP32 (33.5 M
+    """The plain run the learned closure is compared with, 512 x 256 x 256 FP32 (33.5 M
     cells, 512-point x lines in the transforms): a projected seeded state and one full step
     (WALE, heat, smoke) stay finite and the device status stays clean.  max |div u| h / U of
     the projected noise field is at the reference's FP32 level (4e-7 quoted; 1.2e-7 measured,
