@@ -38,7 +38,7 @@ EXPORTS = ("aero_abi_version", "aero_last_error", "aero_ns3d_plan_create", "aero
            "aero_ns2d_plan_create", "aero_ns2d_plan_destroy", "aero_ns2d_workspace_bytes",
            "aero_ns2d_workspace_init", "aero_ns2d_step", "aero_ns2d_poisson_solve", "aero_ns3d_fields",
            "aero_ns3d_probe", "aero_ns3d_masks_workspace_bytes", "aero_ns3d_build_masks",
-           "aero_mesh_sdf_workspace_bytes", "aero_mesh_signed_distance")
+           "aero_mesh_sdf_workspace_bytes", "aero_mesh_signed_distance", "aero_record_history", "aero_welford")
 
 
 class Ns3dConfig(C.Structure):
@@ -199,6 +199,13 @@ def lib() -> C.CDLL:
     L.aero_mesh_signed_distance.argtypes = [C.c_int32, C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_void_p,
                                             C.c_int64, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]
     L.aero_mesh_signed_distance.restype = C.c_int
+    L.aero_record_history.argtypes = [C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p,
+                                      C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p,
+                                      C.c_void_p, C.c_void_p]
+    L.aero_record_history.restype = C.c_int
+    L.aero_welford.argtypes = [C.c_int32, C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                               C.POINTER(C.c_void_p), C.POINTER(C.c_int64), C.c_void_p, C.c_void_p, C.c_void_p]
+    L.aero_welford.restype = C.c_int
     L.aero_debug_check.restype = C.c_int
     for name in ("aero_ns3d_plan_create", "aero_ns3d_workspace_init", "aero_ns3d_step", "aero_ns3d_step_traced",
                  "aero_ns3d_smoke",

@@ -23,6 +23,8 @@
  *   aero_ns3d_build_masks      ns3d/geometry.py:385 build_geometry3d with its exact signed
  *                              distance (geometry.py:229 grid_signed_distance, use_shared=False)
  *   aero_mesh_signed_distance  ns3d/geometry.py:126 mesh_signed_distance
+ *   aero_record_history        ns3d/solver.py:706 FlowSolver3D._record (history ring rows)
+ *   aero_welford               ns3d/solver.py:732 FlowSolver3D._welford (running means)
  *   aero_ns2d_plan_create      ns2d/core.py:182 make_operators (the per-config constants)
  *   aero_ns2d_step             ns2d/core.py:815 step_full (heat transfer its only placed
  *                              physics: physics.py:623-884, the report of core.py:974
@@ -299,6 +301,23 @@ size_t aero_mesh_sdf_workspace_bytes(int32_t dtype, int32_t nface, int64_t npoin
 int aero_mesh_signed_distance(int32_t dtype, const void *vertices, int32_t nvert, const int32_t *faces, int32_t nface,
                               const void *points, int64_t npoints, double plane_zone, void *out, void *workspace,
                               void *stream);
+
+/* ---- per-step bookkeeping (ns3d/solver.py:706-744) --------------------------------- */
+
+/* One history row: hist[slot] = [t, sum over bodies of coeffs (nbody, 6)] at slot = *hist_n
+ * mod capacity, body_c = coeffs (when non-NULL), phist[slot] = [t, extra (n_extra)] (when
+ * phist is non-NULL), *hist_n += 1, and *pending += dt (FP64, when pending is non-NULL).  t,
+ * dt, coeffs, extra, hist, phist are device arrays of dtype; hist_n a device int64. */
+int aero_record_history(int32_t dtype, const void *t, const void *dt, const void *coeffs, int32_t nbody,
+                        void *body_c, void *hist, int64_t capacity, int64_t *hist_n, const void *extra,
+                        int32_t n_extra, void *phist, double *pending, void *stream);
+
+/* The time-weighted Welford update of nfield (<= 5) fields x[f] (count[f] elements) into
+ * mean[f], m2[f] with weight w = *pending: r = w / (*time + w), mean += d r, m2 += d (x -
+ * mean) w; then *time += w, *pending = 0.  The pointer arrays are host arrays of device
+ * pointers; pending and time are device FP64 scalars. */
+int aero_welford(int32_t dtype, int32_t nfield, const void *const *x, void *const *mean, void *const *m2,
+                 const int64_t *count, double *pending, double *time, void *stream);
 
 /* Device-side status word of the last step on this workspace (0 = fine; bit 0: a
  * non-finite value reached a reduction).  Reads through a host copy: synchronises. */
