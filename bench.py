@@ -33,6 +33,9 @@ million trilinear probes of the speed field are timed beside it.
 velocity-regulated fan, a warm jet and a vent, a painted block, the PID step controller; no
 smoke, which jets and vents leave to the caller), with the same plan without them beside it.
 
+``--workload record3d`` measures the per-step bookkeeping (ns3d/solver.py:706-744): the history
+row and a running-mean sample of u, v, w, p and theta on the 256 x 128 x 128 grid.
+
 ``--workload masks3d`` measures mask construction (ns3d/geometry.py:385-495 with the exact
 signed distance): the masks, solid velocity and force weights of a closed 9024-triangle
 sphere of diameter 1 at 32 cells per diameter, rebuilt as a live attitude edit does.
@@ -1054,6 +1057,124 @@ def run_placed(args, rank, world, local_rank):
     print(json.dumps(line), flush=True)
 
 
+
+# ---------------------------------------------------------------------------------------
+# per-step bookkeeping (history rows, running means)
+# ---------------------------------------------------------------------------------------
+RECORD_METRIC = "Mcell-samples/s of the running-mean update (u, v, w, p, theta) on 1 B200"
+RECORD_UNIT = "Mcell/s"
+
+
+def _record_state(shape, device, dtype="float32"):
+    import torch
+    from types import SimpleNamespace
+    nx, ny, nz = shape
+    tdt = torch.float64 if dtype == "float64" else torch.float32
+    g = torch.Generator(device="cpu").manual_seed(5)
+    shapes = {"u": (nz, ny, nx + 1), "v": (nz, ny + 1, nx), "w": (nz + 1, ny, nx), "p": (nz, ny, nx),
+              "t": (nz, ny, nx)}
+    f = {k: torch.randn(sh, generator=g).to(device, tdt) for k, sh in shapes.items()}
+    avg = {"time": torch.zeros((), device=device, dtype=torch.float64),
+           "pending": torch.zeros((), device=device, dtype=torch.float64)}
+    for k, sh in shapes.items():
+        avg[k] = torch.zeros(sh, device=device, dtype=tdt)
+        avg[k + "2"] = torch.zeros(sh, device=device, dtype=tdt)
+    self = SimpleNamespace(dtype=tdt, _body_c=torch.zeros(1, 6, device=device, dtype=tdt),
+                           _hist=torch.zeros(4096, 7, device=device, dtype=tdt),
+                           _hist_n=torch.zeros((), device=device, dtype=torch.int64), _phist=None,
+                           _phist_walls=False, _avg_on=True, _avg=avg, _theta=f["t"], _phys=None)
+    new = SimpleNamespace(u=f["u"], v=f["v"], w=f["w"], p=f["p"], t=torch.ones((), device=device, dtype=tdt),
+                          dt=torch.full((), 0.01, device=device, dtype=tdt))
+    bc = torch.zeros(1, 6, device=device, dtype=tdt)
+    return self, new, bc, f, avg
+
+
+def run_record(args, rank, world, local_rank):
+    import torch
+    from aerolume_b200.ns3d.record import record
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    nx, ny, nz = args.shape
+    cells = nx * ny * nz
+    self, new, bc, f, avg = _record_state(args.shape, dev)
+    for _ in range(args.warmup):
+        record(self, new, bc, True)
+    torch.cuda.synchronize()
+    K = args.steps
+    s_ = torch.cuda.Stream(device=dev)
+    s_.wait_stream(torch.cuda.current_stream(dev))
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(s_):
+        with torch.cuda.graph(g, stream=s_):
+            for _ in range(K):
+                record(self, new, bc, True)
+    torch.cuda.current_stream(dev).wait_stream(s_)
+    ms, clk = _time_graph(g, dist, local_rank, rank, dev)
+    if rank != 0:
+        return
+    peak, peak_kind = _peaks()
+    # compulsory bytes of one sample: each field read once and its mean and second moment read
+    # and written once (5 words per element), FP32
+    elems = sum(x.numel() for x in f.values())
+    alg = 4.0 * 5 * elems
+    achieved = alg / (ms / K * 1e-3) / 1e9
+    cpu = None
+    if not args.no_cpu:
+        cpu = _record_cpu(args.shape)
+    line = {"metric": RECORD_METRIC, "value": world * cells * K / (ms * 1e-3) / 1e6, "unit": RECORD_UNIT,
+            "n_gpus": world, "steps": K, "warmup": args.warmup, "ms_per_step": ms / K, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"history row and running-mean sample of u, v, w, p, theta at {nx}x{ny}x{nz} FP32",
+                       "inputs_vs_l2": f"{alg / 1e6:.0f} MB per sample > 126 MB L2", "parallelism": "replicas",
+                       "graph": f"{K} samples, 1 replay"},
+            "roofline": {"bound": "hbm", "kernel": "welford_kernel", "achieved": achieved, "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                         "alg_bytes_per_launch": alg},
+            "cpu_baseline": cpu,
+            "e2e": None, "gpu_launches": 3 * K, "clocks": clk}
+    print(json.dumps(line), flush=True)
+
+
+def _record_cpu(shape):
+    """The numpy oracle's sample (history row + Welford of five fields) on the full grid."""
+    from oracle import record3d as R
+    nx, ny, nz = shape
+    rng = np.random.default_rng(5)
+    shapes = {"u": (nz, ny, nx + 1), "v": (nz, ny + 1, nx), "w": (nz + 1, ny, nx), "p": (nz, ny, nx),
+              "t": (nz, ny, nx)}
+    f = {k: rng.standard_normal(sh).astype(np.float32) for k, sh in shapes.items()}
+    avg = {"time": np.float64(0), "pending": np.float64(0)}
+    for k, sh in shapes.items():
+        avg[k], avg[k + "2"] = np.zeros(sh, np.float32), np.zeros(sh, np.float32)
+    buf = {"hist": np.zeros((4096, 7), np.float32), "hist_n": 0, "body_c": np.zeros((1, 6), np.float32),
+           "phist": None, "avg": avg}
+    bc = np.zeros((1, 6), np.float32)
+    R.record(buf, 1.0, 0.01, bc, True, fields=f)
+    t0 = time.perf_counter()
+    R.record(buf, 1.0, 0.01, bc, True, fields=f)
+    secs = time.perf_counter() - t0
+    return {"value": nx * ny * nz / secs / 1e6, "unit": RECORD_UNIT, "cores": _threads(), "kind": "port",
+            "sample": f"one full {nx}x{ny}x{nz} sample of the numpy oracle after 1 untimed sample"}
+
+
+def run_reference_record(args, rank):
+    if rank != 0:
+        return
+    nx, ny, nz = args.shape
+    cpu = _record_cpu(args.shape)
+    val = cpu["value"]
+    line = {"impl": "reference", "metric": RECORD_METRIC, "value": val, "unit": RECORD_UNIT, "n_gpus": args.gpus,
+            "steps": 1, "warmup": 1, "ms_per_step": nx * ny * nz / val / 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"history row and running-mean sample of u, v, w, p, theta at {nx}x{ny}x{nz} FP32"},
+            "cpu_baseline": cpu, "e2e": {"value": val, "unit": RECORD_UNIT, "h2d_bytes_per_step": 0,
+                                         "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
 def run_reference_2d(args, rank):
     from aerolume_b200.ns2d.workloads import cylinder_tunnel, heated_cylinder, sweep_instances
     if rank != 0:
@@ -1086,7 +1207,8 @@ def main():
     ap.add_argument("--steps", type=int, default=None, help="timed steps (default 20; 400 for cylinder2d, "
                                                              "10 for sweep2d)")
     ap.add_argument("--workload", default="box3d",
-                    choices=["box3d", "placed3d", "cylinder2d", "heated2d", "sweep2d", "fields3d", "masks3d"])
+                    choices=["box3d", "placed3d", "cylinder2d", "heated2d", "sweep2d", "fields3d", "masks3d",
+                             "record3d"])
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--shape", type=int, nargs=3, default=list(SHAPE), help="nx ny nz (2:1:1)")
@@ -1096,7 +1218,7 @@ def main():
     args = ap.parse_args()
     if args.steps is None:
         args.steps = {"box3d": 20, "placed3d": 20, "cylinder2d": 400, "heated2d": 400, "sweep2d": 10,
-                      "fields3d": 20, "masks3d": 10}[args.workload]
+                      "fields3d": 20, "masks3d": 10, "record3d": 20}[args.workload]
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
@@ -1109,6 +1231,8 @@ def main():
             run_reference_masks(args, rank)
         elif args.workload == "placed3d":
             run_reference_placed(args, rank)
+        elif args.workload == "record3d":
+            run_reference_record(args, rank)
         else:
             run_reference_2d(args, rank)
         return
@@ -1121,7 +1245,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     try:
         {"box3d": run_ours, "placed3d": run_placed, "cylinder2d": run_2d, "heated2d": run_2d, "sweep2d": run_sweep,
-         "fields3d": run_fields, "masks3d": run_masks}[args.workload](
+         "fields3d": run_fields, "masks3d": run_masks, "record3d": run_record}[args.workload](
             args, rank, world, local_rank)
     finally:
         if world > 1:
