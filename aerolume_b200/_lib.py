@@ -14,10 +14,11 @@ import os
 
 LIB_PATH = Path(__file__).resolve().parent / (
     "libaero_b200_checked.so" if os.environ.get("AERO_B200_CHECKED") == "1" else "libaero_b200.so")
-ABI_VERSION = 3
+ABI_VERSION = 4
 MAX_BODIES = 8
 MAX_FANS = 4
 MAX_PORTS = 4
+MAX_HEATERS = 4
 TRACE_EVENTS = 19
 # output fields of aero_ns3d_fields, in its order
 FIELD_NAMES = ("uc", "vc", "wc", "speed", "vorticity", "q", "nut")
@@ -65,7 +66,7 @@ class Ns3dConfig(C.Structure):
         ("pulse_on", C.c_double), ("pulse_period", C.c_double),
         ("u_floor", C.c_double), ("pid", C.c_int32), ("pid_target", C.c_double), ("paint", C.c_int32),
         ("nfan", C.c_int32), ("fan_swirl", C.c_int32),
-        ("nport", C.c_int32), ("port_source", C.c_double), ("port_leak", C.c_double),
+        ("nport", C.c_int32), ("port_source", C.c_double), ("port_leak", C.c_double), ("nheat", C.c_int32),
     ]
 
 
@@ -82,12 +83,16 @@ class Ns3dPort(C.Structure):
         [(n, C.c_void_p) for n in ("f_u", "f_v", "f_w", "m")]
 
 
+class Ns3dHeater(C.Structure):
+    _fields_ = [("window", C.c_int32 * 6), ("q", C.c_void_p)]
+
+
 class Ns3dGeom(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in (
         "chi_u", "chi_v", "chi_w", "chi_c", "a_u", "a_v", "a_w", "k_u", "k_v", "k_w",
         "chi_t", "a_t", "w_t", "adia_u", "adia_v", "adia_w", "vol_w", "skin", "dye_weight", "u_inlet",
         "paint_u", "paint_v", "paint_w", "paint_c")] + \
-        [("fans", C.c_void_p), ("ports", C.c_void_p)]
+        [("fans", C.c_void_p), ("ports", C.c_void_p), ("heaters", C.c_void_p)]
 
 
 class Ns3dFields(C.Structure):

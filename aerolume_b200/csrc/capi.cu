@@ -381,6 +381,11 @@ int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom
     d.f[2] = static_cast<const T *>(Q.f_w);
     d.m = static_cast<const T *>(Q.m);
   }
+  S.nheat = thermal ? c.nheat : 0;
+  for (int q = 0; q < S.nheat; ++q) {
+    for (int e = 0; e < 6; ++e) S.heat[q].win[e] = g->heaters[q].window[e];
+    S.heat[q].q = static_cast<const T *>(g->heaters[q].q);
+  }
   S.a_u = static_cast<const T *>(g->a_u);
   S.a_v = static_cast<const T *>(g->a_v);
   S.a_w = static_cast<const T *>(g->a_w);
@@ -804,6 +809,9 @@ int aero_ns3d_plan_create(const AeroNs3dConfig *cfg, AeroNs3dPlan **plan) {
   if (c.pid && !(c.pid_target >= 0.1 && c.pid_target <= 1.0)) return fail(AERO_EINVAL, "pid_target must be in [0.1, 1]");
   if (c.nfan < 0 || c.nfan > AERO_MAX_FANS)
     return fail(AERO_EUNSUPPORTED, "at most " + std::to_string(AERO_MAX_FANS) + " fans");
+  if (c.nheat < 0 || c.nheat > AERO_MAX_HEATERS)
+    return fail(AERO_EUNSUPPORTED, "at most " + std::to_string(AERO_MAX_HEATERS) + " volumetric heaters");
+  if (c.nheat > 0 && !c.thermal) return fail(AERO_EINVAL, "heaters need heat transfer");
   if (c.nport < 0 || c.nport > AERO_MAX_PORTS)
     return fail(AERO_EUNSUPPORTED, "at most " + std::to_string(AERO_MAX_PORTS) + " jets and vents");
   if (c.nport > 0 && c.smoke)
@@ -901,6 +909,16 @@ int aero_ns3d_step_traced(const AeroNs3dPlan *plan, const AeroNs3dFields *f, con
   if (c.paint && (!g->paint_u || !g->paint_v || !g->paint_w || (c.smoke && !g->paint_c)))
     return fail(AERO_EINVAL, "missing paint masks");
   if (c.pid && (!f->pid_dt_prev || !f->pid_e1 || !f->pid_e2)) return fail(AERO_EINVAL, "missing PID state");
+  if (c.nheat > 0) {
+    if (!g->heaters) return fail(AERO_EINVAL, "missing heater descriptors");
+    for (int q = 0; q < c.nheat; ++q) {
+      const AeroNs3dHeater &Hq = g->heaters[q];
+      if (window_empty(Hq.window) || Hq.window[0] < 0 || Hq.window[1] > c.nz || Hq.window[2] < 0 ||
+          Hq.window[3] > c.ny || Hq.window[4] < 0 || Hq.window[5] > c.nx)
+        return fail(AERO_EINVAL, "heater window empty or outside the domain");
+      if (!Hq.q) return fail(AERO_EINVAL, "missing heater density");
+    }
+  }
   if (c.nport > 0) {
     if (!g->ports) return fail(AERO_EINVAL, "missing port descriptors");
     for (int q = 0; q < c.nport; ++q) {

@@ -115,6 +115,11 @@ struct StageParams {
   int nport;
   T port_leak;
   PortSource<T> port[AERO_MAX_PORTS];
+  int nheat;                        // volumetric heaters: cell window and source density
+  struct {
+    int win[6];
+    const T *q;
+  } heat[AERO_MAX_HEATERS];
 };
 
 struct DtParams {

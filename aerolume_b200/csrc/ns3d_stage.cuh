@@ -192,8 +192,8 @@ struct StageSmem {
 
 // UPWIND, LES and THERMAL are the plan's advection scheme, LES switch and heat switch, fixed at
 // compile time so that each configuration's body is straight-line code; PLACED adds the placed
-// physics that acts inside a stage (fans, jets and vents, painted solids), which the other instantiations
-// leave out entirely.
+// physics that acts inside a stage (fans, jets and vents, painted solids, volumetric heaters),
+// which the other instantiations leave out entirely.
 template <typename T, bool UPWIND, bool LES, bool THERMAL, bool PLACED>
 __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) stage_kernel(const __grid_constant__ StageParams<T> P) {
   aero::pdl_wait();
@@ -614,6 +614,14 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) stage_kernel(c
         const size_t ic = ((size_t)k * ny + j) * nx + i;
         T ch = (a == T(0) ? c : lerp_t<T>(c, t0v, a)) - bdt * D;
         const bool in_body = (wcol & 4) && k >= wk0 && k < wk1;
+        // volumetric heaters, then the heat-flux skins (physics.py:692-697)
+        for (int q = 0; q < (PLACED ? P.nheat : 0); ++q) {
+          const auto &Hq = P.heat[q];
+          if (k >= Hq.win[0] && k < Hq.win[1] && j >= Hq.win[2] && j < Hq.win[3] && i >= Hq.win[4] && i < Hq.win[5])
+            ch = ch + (bdt * P.kappa) * Hq.q[((size_t)(k - Hq.win[0]) * (Hq.win[3] - Hq.win[2]) + (j - Hq.win[2])) *
+                                                 (Hq.win[5] - Hq.win[4]) +
+                                             (i - Hq.win[4])];
+        }
         if (in_body) {
           wt = ((size_t)(k - wk0) * wyn + (j - wj0)) * wxn + (i - wi0);
           if (P.skin) ch = ch + (bdt * P.kappa) * P.skin[wt];
@@ -740,7 +748,7 @@ cudaError_t launch_stage(const StageParams<T> &P, cudaStream_t s) {
       launch_stage_cfg<T, false, true, false, true>,   launch_stage_cfg<T, false, true, true, true>,
       launch_stage_cfg<T, true, false, false, true>,   launch_stage_cfg<T, true, false, true, true>,
       launch_stage_cfg<T, true, true, false, true>,    launch_stage_cfg<T, true, true, true, true>};
-  const bool placed = P.paint_u != nullptr || P.nfan > 0 || P.nport > 0;
+  const bool placed = P.paint_u != nullptr || P.nfan > 0 || P.nport > 0 || P.nheat > 0;
   const int idx = (placed ? 8 : 0) + (P.upwind ? 4 : 0) + (P.les != AERO_LES_NONE ? 2 : 0) + (P.thermal ? 1 : 0);
   return table[idx](P, s);
 }

@@ -12,8 +12,8 @@ these instead (solver.py:161-166 ``load_kernels``; solver.py:583-595 ``fast_step
   tensors, as fused.py:371 / 378-502 do.
 * ``fast_dye`` is the MUSCL advection of one smoke channel (fused.py:553-565).
 
-Placed physics that the B200 step does not implement (volumetric heat sources, diagnostics
-rows) raises instead of being computed differently; heat transfer, fans, jets and vents,
+Placed physics that the B200 step does not implement (diagnostics rows) raises instead of
+being computed differently; heat transfer with its volumetric heaters, fans, jets and vents,
 painted solids and the PID step controller run in the step.
 """
 from __future__ import annotations

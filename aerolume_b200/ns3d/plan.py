@@ -3,9 +3,9 @@
 :class:`Ns3dPlan` reads the reference's objects by attribute (``Ops3D``, ``Geometry3D``,
 ``ThermalOps``, ``DyeSources``: the containers of :mod:`aerolume_b200.ns3d.types` or the
 reference's own), validates what the B200 step supports, uploads the window masks once
-and owns the device workspace.  Unsupported physics (fans, ports, paint, heat sources, a
-PID step controller, more than eight bodies) raises ``RuntimeError``: there is no
-fallback to a CPU or plain-torch path.
+and owns the device workspace.  What the step does not support (more than eight bodies, four
+fans, four jets / vents or four heaters; jets and vents together with the smoke update)
+raises ``RuntimeError``: there is no fallback to a CPU or plain-torch path.
 """
 from __future__ import annotations
 
@@ -171,8 +171,23 @@ class Ns3dPlan:
     # -------------------------------------------------------------------- set-up
     def _thermal_config(self, cfg, g, th, up):
         srcs = getattr(th, "sources", None)
-        if srcs is not None and len(getattr(srcs, "items", [])):
-            raise RuntimeError("volumetric heat sources are not supported by the B200 step")
+        items = list(getattr(srcs, "items", srcs) or [])   # a HeatSourceSet, or (window, density) pairs
+        if len(items) > _lib.MAX_HEATERS:
+            raise RuntimeError(f"the B200 step supports at most {_lib.MAX_HEATERS} volumetric heaters")
+        if items:
+            arr = (_lib.Ns3dHeater * len(items))()
+            for q, (win, dens) in enumerate(items):
+                win = tuple(int(x) for x in win)
+                shape = (win[1] - win[0], win[3] - win[2], win[5] - win[4])
+                t = up(dens)
+                if tuple(t.shape) != shape:
+                    raise RuntimeError(f"heater {q} density has shape {tuple(t.shape)}, expected {shape}")
+                for e in range(6):
+                    arr[q].window[e] = win[e]
+                arr[q].q = t.data_ptr()
+            cfg.nheat = len(items)
+            self._heat_arr = arr
+            g.heaters = C.cast(arr, C.c_void_p)
         cfg.thermal = 1
         cfg.kappa, cfg.pe, cfg.ri, cfg.prt = float(th.kappa), float(th.pe), float(th.ri), float(th.prt)
         cfg.eta_t = _f(th.eta)

@@ -133,6 +133,7 @@ class ThermalOps:
     h: float
     symmetry: bool = False
     heat_max: float | None = None
+    sources: tuple = ()          # volumetric heaters: (cell window, density (wz, wy, wx)) pairs
 
 
 @dataclass

@@ -42,7 +42,7 @@
 extern "C" {
 #endif
 
-#define AERO_ABI_VERSION 3
+#define AERO_ABI_VERSION 4
 
 #define AERO_OK 0
 #define AERO_EINVAL -1        /* invalid argument or inconsistent configuration     */
@@ -52,6 +52,7 @@ extern "C" {
 #define AERO_MAX_BODIES 8
 #define AERO_MAX_FANS 4
 #define AERO_MAX_PORTS 4
+#define AERO_MAX_HEATERS 4
 
 enum { AERO_F32 = 0, AERO_F64 = 1 };
 enum { AERO_ADV_UPWIND3 = 0, AERO_ADV_CENTRAL = 1 };
@@ -118,6 +119,7 @@ typedef struct AeroNs3dConfig {
   int32_t nport;                /* jets and vents (geom ports; physics.py:981-1072)         */
   double port_source;           /* their net mass flux in outlet-face units (h sum m)       */
   double port_leak;             /* uniform scalar leak of an unbalanced closed box (Q / V)  */
+  int32_t nheat;                /* volumetric heaters (geom heaters; physics.py:464-491)    */
 } AeroNs3dConfig;
 
 /* One actuator disc (ns3d/physics.py:831-979): its cell window, the force, swirl and
@@ -147,6 +149,14 @@ typedef struct AeroNs3dPort {
   const void *m;                /* cell weights over the window                            */
 } AeroNs3dPort;
 
+/* One volumetric heater (ns3d/physics.py:464-491 HeatSourceSet): its cell window and the
+ * source density on the window's cells (wz, wy, wx; conduction units, times kappa in the heat
+ * equation), device, of the plan's dtype. */
+typedef struct AeroNs3dHeater {
+  int32_t window[6];            /* k0, k1, j0, j1, i0, i1                                  */
+  const void *q;
+} AeroNs3dHeater;
+
 /* Window masks and constant inputs (device pointers of the plan's dtype; NULL when absent).
  * Shapes are those of ns3d/geometry.py:275-303 and ns3d/physics.py:314-461. */
 typedef struct AeroNs3dGeom {
@@ -163,6 +173,7 @@ typedef struct AeroNs3dGeom {
   const void *paint_u, *paint_v, *paint_w, *paint_c;
   const AeroNs3dFan *fans;      /* host array of cfg.nfan descriptors, read at every step  */
   const AeroNs3dPort *ports;    /* host array of cfg.nport descriptors                     */
+  const AeroNs3dHeater *heaters; /* host array of cfg.nheat descriptors                  */
 } AeroNs3dGeom;
 
 /* State in and out (device pointers of the plan's dtype).  u may alias u0, v v0, w w0 and

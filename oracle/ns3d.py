@@ -652,6 +652,8 @@ def theta_stage(th, c_prev, c0, up, vp, wp, a, bdt, wgt, ops, nut, heat_acc, por
     base = c_prev if a == 0.0 else lerp(c_prev, c0, a)
     ch = base - bdt * D
     bk = T(bdt * T(th.kappa))
+    for win, q in getattr(th, "sources", ()) or ():   # volumetric heaters (physics.py:693-694)
+        ch[_face_slices(win, "c")] += bk * q
     g = th.geom
     if g.skin is not None:
         ch[_face_slices(g.window, "c")] += bk * g.skin

@@ -48,7 +48,8 @@ def load_case(name):
                              flux_rate=np.asarray(t["flux_rate"], np.float64))
         th = ThermalOps(kappa=t["kappa"], pe=t["pe"], ri=t["ri"], prt=t["prt"], eta=t["eta"],
                         side_kinds=tuple(t["side_kinds"]), side_vals=tuple(t["side_vals"]), geom=tg,
-                        h=meta["h"], symmetry=meta["symmetry"], heat_max=t["heat_max"])
+                        h=meta["h"], symmetry=meta["symmetry"], heat_max=t["heat_max"],
+                        sources=tuple((tuple(w), arr[f"th_src{q}"].astype(dt)) for q, w in enumerate(t.get("sources", []))))
     src = None
     if "dye" in meta:
         src = DyeSources(tuple(meta["dye"]["window"]), arr["dye_weight"].astype(dt), tuple(meta["dye"]["pulse"]))

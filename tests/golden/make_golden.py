@@ -31,8 +31,8 @@ REF = Path(os.environ.get("AEROLUME_REF", "/root/reference"))
 sys.path.insert(0, str(REF / "src"))
 
 from aerolume.solvers.ns3d import core  # noqa: E402
-from aerolume.solvers.ns3d.config import (DyeRake, Fan3D, ImmersedMesh, Port3D, SolverConfig3D,  # noqa: E402
-                                          ThermalConfig3D)
+from aerolume.solvers.ns3d.config import (DyeRake, Fan3D, HeatSource3D, ImmersedMesh, Port3D,  # noqa: E402
+                                          SolverConfig3D, ThermalConfig3D)
 from aerolume.solvers.ns3d.dye import advect_dye3d, apply_solids_and_sources, build_dye_sources  # noqa: E402
 from aerolume.solvers.ns3d.geometry import body_window3d, build_geometry3d  # noqa: E402
 from aerolume.solvers.ns3d.physics import PaintLayer, Physics3D  # noqa: E402
@@ -104,6 +104,10 @@ def extract(ops, geom, phys, src):
             val = getattr(tg, name)
             if val is not None:
                 arrays["th_" + name] = _np(val)
+        if th.sources.items:
+            meta["thermal"]["sources"] = [list(win) for win, _ in th.sources.items]
+            for q, (_, dens) in enumerate(th.sources.items):
+                arrays[f"th_src{q}"] = _np(dens)
         if tg.adia is not None:
             for n, a in zip("uvw", tg.adia):
                 arrays["th_adia_" + n] = _np(a)
@@ -299,6 +303,16 @@ def main():
                                     speed=0.6, theta=1.0, name="inflow")],
                       thermal=ThermalConfig3D(prandtl=0.71, richardson=0.5))
     run_case("closed_jet_leak_f64", closed_jet, dtype="float64", steps=3, seed=13, amp=0.05)
+    # volumetric heaters: a box heater behind the heated body and a cooling ball in the tunnel,
+    # and a box heater warming a still closed box (the heaters' step limit sets dt)
+    heaters = [HeatSource3D(kind="box", center=(2.2, 1.0, 0.3), size=(0.5, 0.4, 0.3), power=2.0, name="heater"),
+               HeatSource3D(kind="sphere", center=(3.0, 0.8, 0.9), size=(0.3, 0.3, 0.3), power=-1.5, name="cooler")]
+    run_case("tunnel_heaters_f64", dict(tunnel, heat_sources=heaters), dtype="float64", steps=3, seed=14, amp=0.1)
+    run_case("tunnel_heaters_f32", dict(tunnel, heat_sources=heaters), dtype="float32", steps=3, seed=14, amp=0.1)
+    still = dict(grid, nx=14, ny=10, nz=10, re=300.0, domain="closed", bc_x="noslip", bc_y="noslip",
+                 bc_zmin="noslip", bc_zmax="noslip", thermal=ThermalConfig3D(prandtl=0.71, richardson=1.0),
+                 heat_sources=[HeatSource3D(kind="box", center=(1.2, 0.8, 0.4), size=(0.5, 0.5, 0.3), power=30.0)])
+    run_case("closed_heater_still_f64", still, dtype="float64", steps=3, seed=15, amp=1e-4)
     if not names or "poisson" in names:
         poisson_cases()
     for p in sorted(HERE.glob("*.npz")):

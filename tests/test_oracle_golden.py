@@ -138,3 +138,20 @@ def test_port_fixtures_exercise_the_ports():
     assert _rel(r.theta, arr["out1_theta"]) > 1e-4
     meta, *_ = load_case("closed_jet_leak_f64")
     assert meta["ports"]["leak"] > 0
+
+
+def test_heater_fixtures_exercise_the_heaters():
+    """Leaving the volumetric heaters out moves theta well outside the tolerances, and in the
+    still closed box the heaters' step limit sets dt (the CFL and diffusion limits are looser)."""
+    import dataclasses
+    meta, ops, geom, th, src, arr = load_case("tunnel_heaters_f64")
+    ps = O.PoissonSolver3D(ops.nx, ops.ny, ops.nz, ops.h, ops.periodic_axes, np.float64)
+    r = O.step3d_phys(arr["in_u"], arr["in_v"], arr["in_w"], np.float64(arr["in_t"]), geom, ops, ps,
+                      th=dataclasses.replace(th, sources=()), theta=arr["in_theta"])
+    assert len(th.sources) == 2
+    assert _rel(r.theta, arr["out1_theta"]) > 1e-4          # 2e-4: far above 1e-10 (FP64), 1e-5 (FP32)
+    meta, ops, geom, th, src, arr = load_case("closed_heater_still_f64")
+    ps = O.PoissonSolver3D(ops.nx, ops.ny, ops.nz, ops.h, ops.periodic_axes, np.float64)
+    r = O.step3d_phys(arr["in_u"], arr["in_v"], arr["in_w"], np.float64(arr["in_t"]), geom, ops, ps,
+                      th=dataclasses.replace(th, heat_max=None, sources=()), theta=arr["in_theta"])
+    assert float(r.dt) > 1.5 * float(arr["out1_dt"])
