@@ -311,7 +311,7 @@ def main():
     run_case("tunnel_heaters_f32", dict(tunnel, heat_sources=heaters), dtype="float32", steps=3, seed=14, amp=0.1)
     still = dict(grid, nx=14, ny=10, nz=10, re=300.0, domain="closed", bc_x="noslip", bc_y="noslip",
                  bc_zmin="noslip", bc_zmax="noslip", thermal=ThermalConfig3D(prandtl=0.71, richardson=1.0),
-                 heat_sources=[HeatSource3D(kind="box", center=(1.2, 0.8, 0.4), size=(0.5, 0.5, 0.3), power=30.0)])
+                 heat_sources=[HeatSource3D(kind="box", center=(1.2, 0.8, 0.4), size=(0.5, 0.5, 0.3), power=300.0)])
     run_case("closed_heater_still_f64", still, dtype="float64", steps=3, seed=15, amp=1e-4)
     if not names or "poisson" in names:
         poisson_cases()
