@@ -39,7 +39,8 @@ EXPORTS = ("aero_abi_version", "aero_last_error", "aero_ns3d_plan_create", "aero
            "aero_ns2d_plan_create", "aero_ns2d_plan_destroy", "aero_ns2d_workspace_bytes",
            "aero_ns2d_workspace_init", "aero_ns2d_step", "aero_ns2d_poisson_solve", "aero_ns3d_fields",
            "aero_ns3d_probe", "aero_ns3d_masks_workspace_bytes", "aero_ns3d_build_masks",
-           "aero_mesh_sdf_workspace_bytes", "aero_mesh_signed_distance", "aero_record_history", "aero_welford")
+           "aero_mesh_sdf_workspace_bytes", "aero_mesh_signed_distance", "aero_record_history", "aero_welford",
+           "aero_smoke_emitters")
 
 
 class Ns3dConfig(C.Structure):
@@ -129,6 +130,10 @@ class Ns2dFields(C.Structure):
                                           "flow_heat")]
 
 
+class SmokeEmitter(C.Structure):
+    _fields_ = [("window", C.c_int32 * 6), ("channel", C.c_int32), ("weight", C.c_void_p), ("params", C.c_void_p)]
+
+
 class MaskConfig(C.Structure):
     _fields_ = [
         ("abi_version", C.c_int32), ("dtype", C.c_int32), ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
@@ -211,6 +216,9 @@ def lib() -> C.CDLL:
     L.aero_welford.argtypes = [C.c_int32, C.c_int32, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
                                C.POINTER(C.c_void_p), C.POINTER(C.c_int64), C.c_void_p, C.c_void_p, C.c_void_p]
     L.aero_welford.restype = C.c_int
+    L.aero_smoke_emitters.argtypes = [C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_void_p), C.c_int32,
+                                      C.POINTER(SmokeEmitter), C.c_int32, C.c_void_p, C.c_void_p]
+    L.aero_smoke_emitters.restype = C.c_int
     L.aero_debug_check.restype = C.c_int
     for name in ("aero_ns3d_plan_create", "aero_ns3d_workspace_init", "aero_ns3d_step", "aero_ns3d_step_traced",
                  "aero_ns3d_smoke",

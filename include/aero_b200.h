@@ -24,6 +24,7 @@
  *                              distance (geometry.py:229 grid_signed_distance, use_shared=False)
  *   aero_mesh_signed_distance  ns3d/geometry.py:126 mesh_signed_distance
  *   aero_record_history        ns3d/solver.py:706 FlowSolver3D._record (history ring rows)
+ *   aero_smoke_emitters        ns3d/emitters.py:200 apply_smoke_sources (smoke emitters)
  *   aero_welford               ns3d/solver.py:732 FlowSolver3D._welford (running means)
  *   aero_ns2d_plan_create      ns2d/core.py:182 make_operators (the per-config constants)
  *   aero_ns2d_step             ns2d/core.py:815 step_full (heat transfer its only placed
@@ -312,6 +313,22 @@ size_t aero_mesh_sdf_workspace_bytes(int32_t dtype, int32_t nface, int64_t npoin
 int aero_mesh_signed_distance(int32_t dtype, const void *vertices, int32_t nvert, const int32_t *faces, int32_t nface,
                               const void *points, int64_t npoints, double plane_zone, void *out, void *workspace,
                               void *stream);
+
+/* ---- smoke emitters (ns3d/emitters.py:57-87, 200-210) ------------------------------- */
+
+/* One field emitter: its cell window, the smoke channel it feeds, the weights on the window
+ * (wz, wy, wx) and its device parameters [rate, start, stop, period, t_on] (dtype). */
+typedef struct {
+  int32_t window[6];
+  int32_t channel;
+  const void *weight, *params;
+} AeroSmokeEmitter;
+
+/* In order, each emitter relaxes its channel towards its rate inside its window while its
+ * release switch is on at the device time t: c += w on (rate - c).  channels is a host array
+ * of nchannel device pointers to (nz, ny, nx) arrays of dtype. */
+int aero_smoke_emitters(int32_t dtype, int32_t nz, int32_t ny, int32_t nx, void *const *channels, int32_t nchannel,
+                        const AeroSmokeEmitter *emitters, int32_t nemit, const void *t, void *stream);
 
 /* ---- per-step bookkeeping (ns3d/solver.py:706-744) --------------------------------- */
 
