@@ -121,8 +121,8 @@ class Clocks:
                 "samples": len(sm)}
 
 
-def oracle_sample(nx, ny, nz, steps):
-    """Wall time of ``steps`` oracle steps (after one untimed step) on the full workload."""
+def oracle_sample(nx, ny, nz, steps, warm=1):
+    """Wall time of ``steps`` oracle steps (after ``warm`` untimed steps) on the full workload."""
     from aerolume_b200.ns3d.workloads import box_on_moving_floor, initial_state
     from oracle import ns3d as O
     ops, geom, th, src, _ = box_on_moving_floor(nx, ny, nz, dtype="float32")
@@ -139,7 +139,8 @@ def oracle_sample(nx, ny, nz, steps):
         c = O.apply_solids_and_sources(O.advect_dye3d(dye, r.u, r.v, r.w, r.dt, ops), r.t, geom, src)
         return r.u, r.v, r.w, r.t, r.theta, c
 
-    u, v, w, t, theta, dye = one(u, v, w, t, theta, dye)
+    for _ in range(warm):
+        u, v, w, t, theta, dye = one(u, v, w, t, theta, dye)
     t0 = time.perf_counter()
     for _ in range(steps):
         u, v, w, t, theta, dye = one(u, v, w, t, theta, dye)
@@ -159,11 +160,12 @@ def run_reference(args, rank):
     if rank != 0:
         return
     steps = max(1, min(args.steps, 3))
-    secs = oracle_sample(nx, ny, nz, steps)
+    warm = max(1, min(args.warmup, 3))   # a numpy step takes seconds: both bounded
+    secs = oracle_sample(nx, ny, nz, steps, warm)
     val = nx * ny * nz * steps / secs / 1e6
-    sample = f"{steps} full {nx}x{ny}x{nz} steps of the numpy oracle after 1 untimed step"
+    sample = f"{steps} full {nx}x{ny}x{nz} steps of the numpy oracle after {warm} untimed steps"
     line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": steps, "warmup": 1, "ms_per_step": 1e3 * secs / steps, "higher_is_better": True,
+            "steps": steps, "warmup": warm, "ms_per_step": 1e3 * secs / steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": _config(nx, ny, nz),
             "cpu_baseline": {"value": val, "unit": UNIT, "cores": _threads(), "kind": "port", "sample": sample},
