@@ -14,7 +14,7 @@ import os
 
 LIB_PATH = Path(__file__).resolve().parent / (
     "libaero_b200_checked.so" if os.environ.get("AERO_B200_CHECKED") == "1" else "libaero_b200.so")
-ABI_VERSION = 4
+ABI_VERSION = 5
 MAX_BODIES = 8
 MAX_FANS = 4
 MAX_PORTS = 4
@@ -40,7 +40,11 @@ EXPORTS = ("aero_abi_version", "aero_last_error", "aero_ns3d_plan_create", "aero
            "aero_ns2d_workspace_init", "aero_ns2d_step", "aero_ns2d_poisson_solve", "aero_ns3d_fields",
            "aero_ns3d_probe", "aero_ns3d_masks_workspace_bytes", "aero_ns3d_build_masks",
            "aero_mesh_sdf_workspace_bytes", "aero_mesh_signed_distance", "aero_record_history", "aero_welford",
-           "aero_smoke_emitters")
+           "aero_smoke_emitters", "aero_closure_pairs", "aero_closure_features", "aero_closure_normalise",
+           "aero_mlp_forward", "aero_mlp_train_workspace_bytes", "aero_mlp_gradients", "aero_mlp_train_step",
+           "aero_closure_eddy_viscosity", "aero_ns3d_closure_counts")
+
+CLOSURE_IN, CLOSURE_OUT, CLOSURE_HIDDEN, CLOSURE_NPARAM = 10, 6, 128, 35206
 
 
 class Ns3dConfig(C.Structure):
@@ -68,6 +72,7 @@ class Ns3dConfig(C.Structure):
         ("u_floor", C.c_double), ("pid", C.c_int32), ("pid_target", C.c_double), ("paint", C.c_int32),
         ("nfan", C.c_int32), ("fan_swirl", C.c_int32),
         ("nport", C.c_int32), ("port_source", C.c_double), ("port_leak", C.c_double), ("nheat", C.c_int32),
+        ("closure", C.c_int32),
     ]
 
 
@@ -93,7 +98,13 @@ class Ns3dGeom(C.Structure):
         "chi_u", "chi_v", "chi_w", "chi_c", "a_u", "a_v", "a_w", "k_u", "k_v", "k_w",
         "chi_t", "a_t", "w_t", "adia_u", "adia_v", "adia_w", "vol_w", "skin", "dye_weight", "u_inlet",
         "paint_u", "paint_v", "paint_w", "paint_c")] + \
-        [("fans", C.c_void_p), ("ports", C.c_void_p), ("heaters", C.c_void_p)]
+        [("fans", C.c_void_p), ("ports", C.c_void_p), ("heaters", C.c_void_p), ("closure", C.c_void_p)]
+
+
+class ClosureModel(C.Structure):
+    _fields_ = [("params", C.c_void_p), ("params_bf16", C.c_void_p),
+                ("in_mean", C.c_float * 10), ("in_std", C.c_float * 10), ("in_lo", C.c_float * 10),
+                ("in_hi", C.c_float * 10), ("out_mean", C.c_float * 6), ("out_std", C.c_float * 6)]
 
 
 class Ns3dFields(C.Structure):
@@ -121,7 +132,7 @@ class Ns2dConfig(C.Structure):
 class Ns2dGeom(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in ("chi_u", "chi_v", "chi_c", "a_u", "a_v", "k_u", "k_v", "u_inlet",
                                           "dye_inlet", "chi_t", "a_t", "w_t", "ins_u", "ins_v", "q_skin", "w_f",
-                                          "vol_u", "vol_v")]
+                                          "vol_u", "vol_v", "nu", "eta", "kappa", "eta_t")]
 
 
 class Ns2dFields(C.Structure):
@@ -220,6 +231,21 @@ def lib() -> C.CDLL:
                                       C.POINTER(SmokeEmitter), C.c_int32, C.c_void_p, C.c_void_p]
     L.aero_smoke_emitters.restype = C.c_int
     L.aero_debug_check.restype = C.c_int
+    vp, i64, i32 = C.c_void_p, C.c_int64, C.c_int32
+    L.aero_closure_pairs.argtypes = [i32, i32, vp, vp, vp, C.c_double, vp, vp, vp, vp]
+    L.aero_closure_features.argtypes = [i64, vp, C.c_double, vp, vp, vp, vp, vp, vp]
+    L.aero_closure_normalise.argtypes = [i64, vp, vp, C.POINTER(ClosureModel), vp, vp, vp]
+    L.aero_mlp_forward.argtypes = [C.POINTER(ClosureModel), vp, i64, vp, vp, vp]
+    L.aero_mlp_train_workspace_bytes.argtypes = [i32]
+    L.aero_mlp_train_workspace_bytes.restype = C.c_size_t
+    L.aero_mlp_train_step.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, i32, i32, C.c_float, vp, vp, vp, vp]
+    L.aero_ns3d_closure_counts.argtypes = [vp, vp, C.POINTER(C.c_uint32), vp]
+    L.aero_mlp_gradients.argtypes = [vp, vp, vp, vp, vp, vp, i32, vp, vp, vp, vp]
+    L.aero_closure_eddy_viscosity.argtypes = [C.POINTER(ClosureModel), vp, i64, C.c_double, vp, vp, vp, vp, vp]
+    for name in ("aero_closure_pairs", "aero_closure_features", "aero_closure_normalise", "aero_mlp_forward",
+                 "aero_mlp_gradients", "aero_mlp_train_step", "aero_closure_eddy_viscosity",
+                 "aero_ns3d_closure_counts"):
+        getattr(L, name).restype = C.c_int
     for name in ("aero_ns3d_plan_create", "aero_ns3d_workspace_init", "aero_ns3d_step", "aero_ns3d_step_traced",
                  "aero_ns3d_smoke",
                  "aero_ns3d_poisson_solve",

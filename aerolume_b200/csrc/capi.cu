@@ -79,7 +79,7 @@ struct AeroNs3dPlan {
   size_t esz;                     // bytes per element
   size_t nu, nv, nw, nc;          // element counts of u, v, w and cell arrays
   size_t off_uh, off_vh, off_wh, off_up, off_vp, off_wp, off_tha, off_thb, off_pa, off_nu;
-  size_t off_small, off_scalars, off_status, off_partials, off_psum, total;
+  size_t off_small, off_scalars, off_status, off_partials, off_psum, off_grad, off_counts, total;
   AxisInfo ax[3];
   int zc, zc_nu, nblocks, nq;    // z-planes per CTA of the stage and eddy-viscosity kernels
   int pu, pn;                     // row pitches of the stage-start u copy and of nu
@@ -328,6 +328,18 @@ int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom
   NP.wny = c.window[3] - c.window[2];
   NP.chi_c = static_cast<const T *>(g->chi_c);
   NP.nu = nu_buf;
+  // the learned closure: the eddy-viscosity kernel leaves the gradients for the closure's pass,
+  // which replaces WALE's nu_t where the learned stress applies (FP32 plans only)
+  const int64_t grad_plane = (int64_t)(nz + 2) * (ny + 2) * p->pn;
+  if (c.closure) {
+    NP.grad = reinterpret_cast<float *>(ws + p->off_grad);
+    NP.grad_plane = grad_plane;
+  }
+  auto closure_pass = [&](unsigned long long *nut_max) -> int {
+    return aero_host::closure_nu(g->closure, reinterpret_cast<const float *>(ws + p->off_grad), grad_plane, nx + 2,
+                                 ny + 2, nz + 2, p->pn, c.h, reinterpret_cast<float *>(nu_buf), nut_max,
+                                 reinterpret_cast<unsigned int *>(ws + p->off_counts), status, s);
+  };
   S.dt = small;
   S.u0 = u0;
   S.v0 = v0;
@@ -426,8 +438,12 @@ int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom
     N.vp = v0;
     N.wp = w0;
     nu_views(v0, w0, N);
-    N.nut_max = need_max ? bits + aero::SC_NUTMAX : nullptr;
+    N.nut_max = need_max && !c.closure ? bits + aero::SC_NUTMAX : nullptr;
     CUDA_TRY(aero::launch_nu<T>(N, s));
+    if (c.closure) {
+      const int rc = closure_pass(need_max ? bits + aero::SC_NUTMAX : nullptr);
+      if (rc) return rc;
+    }
   }
 
   aero::DtParams D{};
@@ -519,6 +535,10 @@ int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom
       nu_views(vp, wp, N);
       N.nut_max = nullptr;
       CUDA_TRY(aero::launch_nu<T>(N, s));
+      if (c.closure) {
+        const int rc = closure_pass(nullptr);
+        if (rc) return rc;
+      }
     }
     CUDA_TRY(mark(2 + 5 * st));
     aero::StageParams<T> P = S;
@@ -780,6 +800,8 @@ int aero_ns3d_plan_create(const AeroNs3dConfig *cfg, AeroNs3dPlan **plan) {
   if (!(c.h > 0) || !std::isfinite(c.h)) return fail(AERO_EINVAL, "cell size h must be positive");
   if (c.advection != AERO_ADV_UPWIND3 && c.advection != AERO_ADV_CENTRAL) return fail(AERO_EINVAL, "unknown advection");
   if (c.les < AERO_LES_NONE || c.les > AERO_LES_VREMAN) return fail(AERO_EINVAL, "unknown turbulence model");
+  if (c.closure && (c.les != AERO_LES_WALE || c.dtype != AERO_F32))
+    return fail(AERO_EINVAL, "the learned closure runs on WALE (its fallback) in FP32 plans");
   if (c.nbody < 0 || c.nbody > AERO_MAX_BODIES)
     return fail(AERO_EUNSUPPORTED, "at most " + std::to_string(AERO_MAX_BODIES) + " bodies");
   for (int comp = 0; comp < 3; ++comp)
@@ -844,6 +866,8 @@ int aero_ns3d_plan_create(const AeroNs3dConfig *cfg, AeroNs3dPlan **plan) {
   p->off_thb = take(c.thermal ? p->nc * e : 0);
   p->off_pa = take(p->nc * e);
   p->off_nu = take(c.les != AERO_LES_NONE ? (nz + 2) * (ny + 2) * (size_t)p->pn * e : 0);
+  p->off_grad = take(c.closure ? 9 * (nz + 2) * (ny + 2) * (size_t)p->pn * sizeof(float) : 0);
+  p->off_counts = take(c.closure ? 4 * sizeof(unsigned int) : 0);
   p->off_small = take(8 * e);
   p->off_scalars = take(sizeof(double) * aero::SC_COUNT);
   p->off_status = take(sizeof(int) * 4);
@@ -906,6 +930,8 @@ int aero_ns3d_step_traced(const AeroNs3dPlan *plan, const AeroNs3dFields *f, con
     if (c.thermal && c.has_skin && !g->skin) return fail(AERO_EINVAL, "missing heat-flux skin");
   }
   if (c.thermal && !f->heat_rate && c.nbody > 0) return fail(AERO_EINVAL, "missing heat-rate output");
+  if (c.closure && (!g->closure || !g->closure->params || !g->closure->params_bf16))
+    return fail(AERO_EINVAL, "the learned closure needs its model");
   if (c.paint && (!g->paint_u || !g->paint_v || !g->paint_w || (c.smoke && !g->paint_c)))
     return fail(AERO_EINVAL, "missing paint masks");
   if (c.pid && (!f->pid_dt_prev || !f->pid_e1 || !f->pid_e2)) return fail(AERO_EINVAL, "missing PID state");
@@ -971,6 +997,19 @@ int aero_ns3d_poisson_solve_static(const AeroNs3dPlan *plan, const void *f, void
   auto s = static_cast<cudaStream_t>(stream);
   return plan->cfg.dtype == AERO_F64 ? poisson_static_impl<double>(plan, f, psi, s)
                                      : poisson_static_impl<float>(plan, f, psi, s);
+}
+
+int aero_ns3d_closure_counts(const AeroNs3dPlan *plan, const void *workspace, uint32_t out[2], void *stream) {
+  if (!plan || !workspace || !out) return fail(AERO_EINVAL, "null argument");
+  if (!plan->cfg.closure) return fail(AERO_EINVAL, "the plan has no learned closure");
+  uint32_t h[2] = {0, 0};
+  auto s = static_cast<cudaStream_t>(stream);
+  CUDA_TRY(cudaMemcpyAsync(h, static_cast<const unsigned char *>(workspace) + plan->off_counts, sizeof(h),
+                           cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(cudaStreamSynchronize(s));
+  out[0] = h[0];
+  out[1] = h[1];
+  return AERO_OK;
 }
 
 int aero_ns3d_fields(const AeroNs3dPlan *plan, const void *u, const void *v, const void *w, const AeroNs3dGeom *g,

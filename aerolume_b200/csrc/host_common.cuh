@@ -14,6 +14,12 @@ namespace aero_host {
 // Stores msg as the calling thread's aero_last_error() and returns code (defined in capi.cu).
 int set_error(int code, const std::string &msg);
 
+// The learned closure's eddy-viscosity pass of the 3D step (closure.cu): over the padded
+// (nzp, nyp, pitch) cells whose gradient and window factor the eddy-viscosity kernel left in
+// grad (9 components, `plane` apart), nu_t of the learned stress where it applies.
+int closure_nu(const AeroClosureModel *m, const float *grad, int64_t plane, int nxp, int nyp, int nzp, int pitch,
+               double delta, float *nu, unsigned long long *nut_max, unsigned int *counts, int *status, cudaStream_t s);
+
 constexpr size_t ALIGN = 256;
 inline size_t align_up(size_t x) { return (x + ALIGN - 1) & ~(ALIGN - 1); }
 

@@ -160,6 +160,10 @@ struct StageParams {
   int has_win, win[4];         // j0, j1, i0, i1
   const T *chi_u, *chi_v, *chi_c, *a_u, *a_v, *k_u, *k_v;
   T eta;
+  // the caller's 0-d device scalars nu and eta (NULL: the plan's constants), read at every
+  // launch so that a live Re change reaches a captured graph; inv_h2 = 1 / h^2
+  const T *live_nu, *live_eta, *live_kappa;
+  T inv_h2;
   // heat transfer: buoyancy -Ri theta g on the faces from the stage-start theta, after the
   // penalisation (core.py:774-813), with the solids' share (vol_u / vol_v, else chi) booked
   // against the body force; nut_out (ny, nx) receives nu_t of the stage for the heat equation
@@ -199,9 +203,17 @@ __global__ void __launch_bounds__(NT) stage2d_kernel(const __grid_constant__ Sta
   const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
   const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
   const bool tunnel = !P.periodic && !P.closed;
-  const T dt = P.dt_here ? dt2d_value<T, HEAT>(P.dt_mode, P.dt_in, P.dt_fixed, P.dt_bits, P.dt_cfl_h, P.dt_nu, P.dt_visc_h2,
-                                         P.dt_les, P.dt_th)
-                         : *P.dt;
+  const T nuh2 = P.live_nu ? __ldg(P.live_nu) * P.inv_h2 : P.nuh2;
+  const T eta = P.live_eta ? __ldg(P.live_eta) : P.eta;
+  T dt;
+  if (P.dt_here) {
+    Dt2dThermal dth = P.dt_th;
+    if (HEAT && P.live_kappa) dth.kappa = (double)__ldg(P.live_kappa);
+    dt = dt2d_value<T, HEAT>(P.dt_mode, P.dt_in, P.dt_fixed, P.dt_bits, P.dt_cfl_h,
+                             P.live_nu ? (double)__ldg(P.live_nu) : P.dt_nu, P.dt_visc_h2, P.dt_les, dth);
+  } else {
+    dt = *P.dt;
+  }
   if (P.dt_here && blockIdx.x == 0 && blockIdx.y == 0 && tid == 0) *P.dt_store = dt;
   const T bdt = dt * P.b;
   // outlet balance (core.py:352-359): every block with outlet faces sums the whole outlet
@@ -290,7 +302,7 @@ __global__ void __launch_bounds__(NT) stage2d_kernel(const __grid_constant__ Sta
   if (NU_ONLY) return;
   const int j = j0 + ty, i = i0 + tx;
   const bool in = j < ny && i < nx;
-  const T k_pen = bdt / P.eta;
+  const T k_pen = bdt / eta;
   const bool wblock = P.has_win && P.nbody > 0;
   double fq[4] = {0.0, 0.0, 0.0, 0.0};  // this thread's force sums of body `bsel`
   // ---- u-faces (j, i) and, for the last column, (j, nx)
@@ -305,7 +317,7 @@ __global__ void __launch_bounds__(NT) stage2d_kernel(const __grid_constant__ Sta
     T lu = (((fxl - fxr) + gyb) - gyt) * P.kadv;
     T ring = ((row[c + 1] + row[c - 1]) + U[r + 1][c]) + U[r - 1][c];
     ring = ring + T(-4) * row[c];
-    lu = lu + ring * P.nuh2;
+    lu = lu + ring * nuh2;
     if (P.les) {
       const int cc = fi - i0 + 1, cr = j - j0 + 1;  // cell fi in TXX, corner row j in TXY
       lu = lu + (((TXX[cr][cc] - TXX[cr][cc - 1]) + TXY[cr][fi - i0]) - TXY[cr - 1][fi - i0]) * P.inv_h;
@@ -355,7 +367,7 @@ __global__ void __launch_bounds__(NT) stage2d_kernel(const __grid_constant__ Sta
     T lv = (((fxl - fxr) + gyb) - gyt) * P.kadv;
     T ring = ((row[c + 1] + row[c - 1]) + V[r + 1][c]) + V[r - 1][c];
     ring = ring + T(-4) * row[c];
-    lv = lv + ring * P.nuh2;
+    lv = lv + ring * nuh2;
     if (P.les) {
       const int cc = i - i0 + 1, cr = fj - j0 + 1;  // cell row fj in TYY, corner row fj in TXY
       lv = lv + (((TXY[cr - 1][i - i0 + 1] - TXY[cr - 1][i - i0]) + TYY[cr][cc]) - TYY[cr - 1][cc]) * P.inv_h;
@@ -563,6 +575,7 @@ struct ThetaParams {
   int nx, ny, periodic, closed;
   T inv_h, inv_half;          // 1 / h, 2 / h
   T kappa, inv_prt, theta_in, eta_t;
+  const T *live_kappa, *live_eta_t;  // the caller's device kappa / thermal eta (NULL: the constants)
   const T *thp, *th0;         // stage-start and step-start theta (ny, nx)
   T *th;                      // the stage's theta
   const T *upf, *vpf;         // stage-start face velocities (ny, nx+1), (ny+1, nx)
@@ -600,8 +613,14 @@ __device__ __forceinline__ T theta_at(const ThetaParams<T> &P, int j, int i) {
 // diffusivity on the x-face (j, f): kappa (+ the face average of nu_t / Pr_t), times the
 // insulation factor inside the window (physics.py:700-718)
 template <typename T>
+__device__ __forceinline__ T kappa_of(const ThetaParams<T> &P) {
+  return P.live_kappa ? __ldg(P.live_kappa) : P.kappa;
+}
+
+template <typename T>
 __device__ __forceinline__ T kx_face(const ThetaParams<T> &P, int j, int f) {
-  T k = P.kappa;
+  const T kap = kappa_of<T>(P);
+  T k = kap;
   const int nx = P.nx;
   if (P.nut) {
     const T *row = P.nut + (size_t)j * nx;
@@ -609,7 +628,7 @@ __device__ __forceinline__ T kx_face(const ThetaParams<T> &P, int j, int f) {
     if (f > 0 && f < nx) avg = T(0.5) * (__ldg(row + f) * P.inv_prt + __ldg(row + f - 1) * P.inv_prt);
     else if (P.periodic) avg = T(0.5) * (__ldg(row) * P.inv_prt + __ldg(row + nx - 1) * P.inv_prt);
     else avg = __ldg(row + (f == 0 ? 0 : nx - 1)) * P.inv_prt;
-    k = P.kappa + avg;
+    k = kap + avg;
   }
   if (P.ins_u && j >= P.win[0] && j < P.win[1] && f >= P.win[2] && f <= P.win[3])
     k = k * __ldg(P.ins_u + (size_t)(j - P.win[0]) * (P.win[3] - P.win[2] + 1) + (f - P.win[2]));
@@ -618,7 +637,8 @@ __device__ __forceinline__ T kx_face(const ThetaParams<T> &P, int j, int f) {
 
 template <typename T>
 __device__ __forceinline__ T ky_face(const ThetaParams<T> &P, int f, int i) {
-  T k = P.kappa;
+  const T kap = kappa_of<T>(P);
+  T k = kap;
   const int nx = P.nx, ny = P.ny;
   if (P.nut) {
     T avg;
@@ -628,7 +648,7 @@ __device__ __forceinline__ T ky_face(const ThetaParams<T> &P, int f, int i) {
       avg = T(0.5) * (__ldg(P.nut + i) * P.inv_prt + __ldg(P.nut + (size_t)(ny - 1) * nx + i) * P.inv_prt);
     else
       avg = __ldg(P.nut + (size_t)(f == 0 ? 0 : ny - 1) * nx + i) * P.inv_prt;
-    k = P.kappa + avg;
+    k = kap + avg;
   }
   if (P.ins_v && f >= P.win[0] && f <= P.win[1] && i >= P.win[2] && i < P.win[3])
     k = k * __ldg(P.ins_v + (size_t)(f - P.win[0]) * (P.win[3] - P.win[2]) + (i - P.win[2]));
@@ -700,13 +720,13 @@ __global__ void __launch_bounds__(NT) theta2d_kernel(const __grid_constant__ The
     const bool inwin = P.has_win && j >= P.win[0] && j < P.win[1] && i >= P.win[2] && i < P.win[3];
     const size_t widx = inwin ? (size_t)(j - P.win[0]) * (P.win[3] - P.win[2]) + (i - P.win[2]) : 0;
     const size_t wsz = (size_t)(P.win[1] - P.win[0]) * (P.win[3] - P.win[2]);
-    if (inwin && P.q_skin) lt = lt + P.kappa * __ldg(P.q_skin + widx);
+    if (inwin && P.q_skin) lt = lt + kappa_of<T>(P) * __ldg(P.q_skin + widx);
     const T bdt = *P.dt * P.b;
     const size_t g = (size_t)j * nx + i;
     const T t0 = __ldg(P.th0 + g);
     T th = (P.a == T(0) ? ctr : lerp_t<T>(ctr, t0, P.a)) + lt * bdt;
     if (inwin && nh > 0) {
-      const T kt = bdt / P.eta_t;
+      const T kt = bdt / (P.live_eta_t ? __ldg(P.live_eta_t) : P.eta_t);
       const T tn = (th + kt * __ldg(P.a_t + widx)) / (T(1) + kt * __ldg(P.chi_t + widx));
       const double d = (double)(tn - th);
       for (int b = 0; b < nh; ++b) acc[b] = (double)__ldg(P.w_t + (size_t)b * wsz + widx) * d;
@@ -741,6 +761,7 @@ template <typename T>
 struct ReportParams {
   int nx, ny, periodic, closed, nblocks, n_temp, n_flux;
   T h, h2, kappa, theta_in;
+  const T *live_kappa;        // the caller's device kappa (NULL: the constant)
   double hd;
   int mode[4];
   T wval[4];
@@ -808,9 +829,9 @@ __global__ void heat_report2d_kernel(const __grid_constant__ ReportParams<T> P) 
                                                       : side == 2 ? (size_t)e : (size_t)(ny - 1) * nx + e;
           s += (double)(P.wval[side] - P.theta[g]);
         }
-        rate = (double)(T(2) * P.kappa) * warp_sum(s);
+        rate = (double)(T(2) * (P.live_kappa ? __ldg(P.live_kappa) : P.kappa)) * warp_sum(s);
       } else if (mode == AERO_TH2_HEAT_FLUX) {
-        rate = (double)((P.kappa * P.wval[side]) * T((double)n * P.hd));
+        rate = (double)(((P.live_kappa ? __ldg(P.live_kappa) : P.kappa) * P.wval[side]) * T((double)n * P.hd));
       }
       if (lane == 0) P.wall_heat[side] = rate;
       continue;
@@ -974,6 +995,10 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
   S.inv_h = T(1.0 / c.h);
   S.kadv = T((c.advection == AERO_ADV_UPWIND3 ? 7.0 / 24.0 : 0.25) / c.h);
   S.nuh2 = T(c.nu) * T(1.0 / (c.h * c.h));
+  S.inv_h2 = T(1.0 / (c.h * c.h));
+  S.live_nu = static_cast<const T *>(g->nu);
+  S.live_eta = static_cast<const T *>(g->eta);
+  S.live_kappa = c.thermal ? static_cast<const T *>(g->kappa) : nullptr;
   S.cfac = T(c.les == AERO_LES_VREMAN ? c.les_c * c.h * c.h : c.les_c * c.les_c * c.h * c.h);
   S.ru = rules2<T>(c, 0);
   S.rv = rules2<T>(c, 1);
@@ -1048,6 +1073,8 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
     TP.inv_prt = T(1.0 / c.prt);
     TP.theta_in = T(c.theta_in);
     TP.eta_t = T(c.eta_t);
+    TP.live_kappa = static_cast<const T *>(g->kappa);
+    TP.live_eta_t = static_cast<const T *>(g->eta_t);
     TP.th0 = static_cast<const T *>(f->theta0);
     TP.nut = les ? nutb : nullptr;
     for (int q = 0; q < 4; ++q) {
@@ -1155,6 +1182,7 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
     R.hd = c.h;
     R.h2 = T(c.h * c.h);
     R.kappa = T(c.kappa);
+    R.live_kappa = static_cast<const T *>(g->kappa);
     R.theta_in = T(c.theta_in);
     for (int q = 0; q < 4; ++q) {
       R.mode[q] = c.wall_mode[q];

@@ -39,6 +39,10 @@ struct NuParams {
   const T *chi_c;
   T *nu;                      // (nz+2, ny+2, nx+2): cells -1..n of every axis
   unsigned long long *nut_max;  // or NULL
+  // learned closure: the eight gradient components and the window factor (1 - chi_c) of every
+  // cell, at the nu array's index, components grad_plane apart (FP32; NULL: not written)
+  float *grad;
+  int64_t grad_plane;
 };
 
 // An actuator disc as the stage kernel sees it: its window, force and swirl weights on the

@@ -155,12 +155,20 @@ __global__ void __launch_bounds__(TX *TY) nu_kernel(const __grid_constant__ NuPa
                 qq;
       g[2][2] = -(g[0][0] + g[1][1]);
       T nu = eddy_viscosity<T>(g, MODEL, P.cd2);
+      T fac = T(1);
       if (P.has_win && kn >= P.win[0] && kn < P.win[1] && cj >= P.win[2] && cj < P.win[3] && ci >= P.win[4] &&
           ci < P.win[5]) {
         const T chi = P.chi_c[((size_t)(kn - P.win[0]) * P.wny + (cj - P.win[2])) * P.wnx + (ci - P.win[4])];
-        nu = nu * (T(1) - chi);
+        fac = T(1) - chi;
+        nu = nu * fac;
       }
-      P.nu[((size_t)q * (ny + 2) + (cj + 1)) * P.nu_pitch + (ci + 1)] = nu;
+      const size_t at = ((size_t)q * (ny + 2) + (cj + 1)) * P.nu_pitch + (ci + 1);
+      P.nu[at] = nu;
+      if (P.grad) {  // the learned closure's inputs
+        const T gg[9] = {g[0][0], g[0][1], g[0][2], g[1][0], g[1][1], g[1][2], g[2][0], g[2][1], fac};
+#pragma unroll
+        for (int c = 0; c < 9; ++c) P.grad[c * P.grad_plane + at] = (float)gg[c];
+      }
       mx = (nu > mx || nu != nu) ? nu : mx;
     }
     if (pre) {

@@ -108,7 +108,6 @@ class Ns2dPlan:
             raise RuntimeError("the Werner-Wengle wall model is not supported by the B200 step")
         L = _lib.lib()
         self.dtype = _torch_dtype(ops)
-        self.ops, self.geom = ops, geom
         self.dye = bool(dye)
         nx, ny = int(ops.nx), int(ops.ny)
         self.shape = (ny, nx)
@@ -174,6 +173,20 @@ class Ns2dPlan:
             g.dye_inlet = up(d_in, (ny,)).data_ptr()
         if thermal is not None:
             self._thermal_config(cfg, g, thermal, up)
+
+        def live(x):
+            """The reference's 0-d device scalar itself (its set_reynolds fills it in place, so a
+            captured step follows a live Re change), else None (the constant in cfg)."""
+            ok = torch.is_tensor(x) and x.numel() == 1 and x.device == dev and x.dtype == dt and x.is_contiguous()
+            if not ok:
+                return None
+            self._keep.append(x)          # held while the plan lives, whatever happens to ops
+            return x.data_ptr()
+
+        g.nu, g.eta = live(getattr(ops, "nu", None)), live(getattr(ops, "eta", None))
+        ph = getattr(ops, "phys", None)
+        if thermal is not None and ph is not None:
+            g.kappa, g.eta_t = live(getattr(ph, "kappa", None)), live(getattr(ph, "eta_t", None))
         self.cfg = cfg
         self.geom_c = g
         handle = C.c_void_p()

@@ -11,6 +11,7 @@ traces raise instead of being computed differently.
 """
 from __future__ import annotations
 
+import weakref
 from typing import Any, NamedTuple
 
 import torch
@@ -31,15 +32,31 @@ class State(NamedTuple):
     ctrl: Any = None
 
 
-_PLANS: dict = {}
+_PLANS: dict = {}   # id(ops) -> {(id(geom), dye): (plan, geom)}, most recent last
+_KEEP = 2
 
 
 def _plan_for(ops, geom, dye, device):
-    key = (id(ops), id(geom), dye)
-    entry = _PLANS.get(key)
+    """The plan of (ops, geom, dye).  A plan reads the reference's device scalars ops.nu,
+    ops.eta, phys.kappa and phys.eta_t at every launch, so an in-place ``set_reynolds``
+    (core.py:167-176) needs no new plan and a captured graph stays valid, as in the reference;
+    a ``set_bodies`` that builds a new geometry (and re-captures, solver.py:1050-1080) gets a
+    new plan.  Each solver's ``ops`` keeps its ``_KEEP`` most recent plans; older ones are
+    dropped with their device workspace, and all of them when ``ops`` itself is collected."""
+    bucket = _PLANS.get(id(ops))
+    if bucket is None:
+        bucket = _PLANS[id(ops)] = {}
+        try:
+            weakref.finalize(ops, _PLANS.pop, id(ops), None)
+        except TypeError:        # not weak-referenceable: its bucket stays bounded by _KEEP
+            pass
+    key = (id(geom), dye)
+    entry = bucket.pop(key, None)
     if entry is None:
-        entry = (Ns2dPlan(ops, geom, dye=dye, device=device), ops, geom)   # keeps ops / geom alive
-        _PLANS[key] = entry
+        entry = (Ns2dPlan(ops, geom, dye=dye, device=device), geom)   # the entry keeps geom alive
+    bucket[key] = entry
+    while len(bucket) > _KEEP:
+        del bucket[next(iter(bucket))]
     return entry[0]
 
 

@@ -24,12 +24,39 @@ from .plan import Ns3dPlan
 from .types import Geometry3D, State3D, StepOut3D
 
 
+def _live_key(ops, thermal):
+    """The plan constants that the reference changes in place on a live edit, as host values:
+    ``set_reynolds`` (core.py:140-144) writes ``ops.nu_value`` (and ``ops.nu`` / ``ops.eta`` from
+    the same Re), ``ThermalOps.set_reynolds`` (physics.py:580-586) writes ``pe`` / ``kappa`` (and
+    the thermal eta from the same Pe), and ``FlowSolver3D.set_bodies`` (solver.py:1659-1700) may
+    swap ``thermal.geom``.  Host attributes only: reading a device tensor here would synchronise
+    the stream, which a graph capture forbids."""
+    key = (float(ops.nu_value),)
+    if thermal is not None:
+        key += (float(thermal.kappa), float(thermal.pe), id(getattr(thermal, "geom", None)))
+    return key
+
+
 class B200Kernels:
-    """What ``load_kernels`` returns: the scheme plus plans cached by configuration."""
+    """What ``load_kernels`` returns: the scheme plus the plans of the latest configurations.
+
+    A plan holds its constants from creation, so a plan is looked up by the identities of the
+    objects it was built from and by :func:`_live_key`: after ``set_inflow`` or a ``set_bodies``
+    that replaces the thermal masks the next step builds a new plan (the reference re-captures
+    its graphs on both, solver.py:1656, :1699).  At most ``keep`` plans of each kind stay
+    cached; older ones are dropped with their device workspace."""
+
+    keep = 2
 
     def __init__(self, scheme, device, dtype):
         self.scheme, self.device, self.dtype = scheme, device, dtype
         self._plans = {}
+
+    def _remember(self, key, entry):
+        same = [k for k in self._plans if k[0] == key[0]]
+        for k in same[: max(0, len(same) - self.keep + 1)]:
+            del self._plans[k]
+        self._plans[key] = entry
 
     def plan_for(self, geom, ops, phys=None):
         thermal = getattr(phys, "thermal", None) if phys is not None else None
@@ -37,13 +64,13 @@ class B200Kernels:
         pid = getattr(phys, "pid", None) if phys is not None else None
         fans = getattr(phys, "fans", None) if phys is not None else None
         ports = getattr(phys, "ports", None) if phys is not None else None
-        key = ("step", id(geom), id(ops), id(thermal), id(paint), id(pid), id(fans), id(ports))
+        key = ("step", id(geom), id(ops), id(thermal), id(paint), id(pid), id(fans), id(ports)) + _live_key(ops, thermal)
         entry = self._plans.get(key)
         if entry is None:
             plan = Ns3dPlan(ops, geom, thermal, None, device=self.device, paint=paint, pid=pid, fans=fans, ports=ports,
                             u_floor=float(getattr(phys, "u_floor", 0.0) or 0.0) if phys is not None else 0.0)
             entry = (plan, geom, ops, thermal, paint, pid, fans, ports)   # the objects stay alive with their plan
-            self._plans[key] = entry
+            self._remember(key, entry)
         return entry[0]
 
     def dye_plan_for(self, ops):
@@ -52,7 +79,7 @@ class B200Kernels:
         if entry is None:
             plan = Ns3dPlan(ops, Geometry3D((0, 0, 0, 0, 0, 0)), None, None, smoke=True, device=self.device)
             entry = (plan, ops)
-            self._plans[key] = entry
+            self._remember(key, entry)
         return entry[0]
 
 

@@ -47,7 +47,7 @@ class Ns3dPlan:
     """
 
     def __init__(self, ops, geom, thermal=None, dye_src=None, *, smoke: bool = False, device=None, paint=None,
-                 pid=None, u_floor: float = 0.0, fans=None, ports=None):
+                 pid=None, u_floor: float = 0.0, fans=None, ports=None, closure=None):
         self.device = torch.device(device) if device is not None else torch.device("cuda")
         if self.device.type != "cuda":
             raise RuntimeError("the B200 step runs on a CUDA device only (no CPU fallback)")
@@ -155,6 +155,15 @@ class Ns3dPlan:
         self.ports = ports if ports is not None and len(ports) else None
         if self.ports is not None:
             self._port_config(cfg, g, self.ports, up)
+        # the learned subgrid closure (a ClosureModel): its nu_t replaces WALE's where it applies;
+        # the plan keeps the model's standardisation constants of this moment and reads its
+        # parameters from the model's tensors at every step
+        self.closure = closure
+        if closure is not None:
+            cfg.closure = 1
+            self._closure_c = closure.cstruct()
+            g.closure = C.addressof(self._closure_c)
+            self._keep.extend([closure.params, closure.params_bf16])
         self.cfg = cfg
         self.geom_c = g
         handle = C.c_void_p()
@@ -467,6 +476,14 @@ class Ns3dPlan:
                                            C.c_void_p(w.data_ptr()), C.c_void_p(psi.data_ptr()),
                                            C.c_void_p(self.ws_ptr), self._stream()), "aero_ns3d_project")
         return psi
+
+    def closure_counts(self):
+        """(cells evaluated, cells that kept WALE) of the closure passes since the workspace was
+        initialised (synchronises)."""
+        out = (C.c_uint32 * 2)()
+        check(_lib.lib().aero_ns3d_closure_counts(self._handle, C.c_void_p(self.ws_ptr), out, self._stream()),
+              "aero_ns3d_closure_counts")
+        return int(out[0]), int(out[1])
 
     def status(self) -> int:
         """Device status word of the last step (synchronises): 0, or bit 0 = non-finite value."""

@@ -155,20 +155,133 @@ def _threads():
         return os.cpu_count() or 1
 
 
+# ---------------------------------------------------------------------------------------
+# The reference itself (Aerolume installed unmodified under baseline/_ref): its FlowSolver3D
+# on the host cores (the CPU baseline) and on the GPU (the bar of the plain drop-in)
+# ---------------------------------------------------------------------------------------
+
+REF_DIR = ROOT / "baseline" / "_ref"
+
+
+def _reference_api():
+    """The reference's public 3D solver API from baseline/_ref (ImportError when absent)."""
+    if not (REF_DIR / "aerolume" / "solvers" / "ns3d" / "solver.py").exists():
+        raise ImportError("baseline/_ref holds no installed reference")
+    if str(REF_DIR) not in sys.path:
+        sys.path.insert(0, str(REF_DIR))
+    from aerolume.solvers.ns3d.config import DyeRake, ImmersedMesh, SolverConfig3D, ThermalConfig3D
+    from aerolume.solvers.ns3d.solver import FlowSolver3D
+    return DyeRake, ImmersedMesh, SolverConfig3D, ThermalConfig3D, FlowSolver3D
+
+
+def _box_mesh(size, center):
+    """(vertices (8, 3), faces (12, 3)) of an axis-aligned box, wound outward."""
+    lx, ly, lz = size
+    cx, cy, cz = center
+    v = np.array([[cx + sx * lx / 2, cy + sy * ly / 2, cz + sz * lz / 2]
+                  for sz in (-1, 1) for sy in (-1, 1) for sx in (-1, 1)], dtype=np.float64)
+    f = np.array([[0, 2, 1], [1, 2, 3], [4, 5, 6], [5, 7, 6], [0, 1, 4], [1, 5, 4],
+                  [2, 6, 3], [3, 6, 7], [0, 4, 2], [2, 4, 6], [1, 3, 5], [3, 7, 5]], dtype=np.int64)
+    return v, f
+
+
+def reference_box_config(nx, ny, nz, device):
+    """The reference's SolverConfig3D of the box-on-moving-floor workload (the same case that
+    aerolume_b200.ns3d.workloads.box_on_moving_floor builds for the B200 step)."""
+    DyeRake, ImmersedMesh, SolverConfig3D, ThermalConfig3D, _ = _reference_api()
+    h = 8.0 / nx
+    v, f = _box_mesh((1.0, 1.0, 0.5), (2.5, 2.0, 0.25))
+    box = ImmersedMesh(v, f, name="box", thermal="temperature", thermal_value=1.0)
+    rng = np.random.default_rng(0)
+    ys = np.sort(rng.uniform(1.2, 2.8, 16))
+    zs = rng.uniform(0.1, 0.45, 16)
+    rake = DyeRake("rake", [(1.25, float(y), float(z)) for y, z in zip(ys, zs)], radius=1.25 * h)
+    return SolverConfig3D(nx=nx, ny=ny, nz=nz, h=h, x0=0.0, y0=0.0, z0=0.0, re=1e4, bodies=[box], bc_zmin="moving",
+                          ground_speed=1.0, turbulence="wale", thermal=ThermalConfig3D(prandtl=0.71, richardson=0.2),
+                          dye=True, dye_rake=rake, ref_area=0.5, moment_ref=(2.5, 2.0, 0.0), dtype="float32",
+                          device=device, perturb=False)
+
+
+def time_reference_cpu(nx, ny, nz, steps, warm, threads=None, repeats=3):
+    """Best-of-``repeats`` wall time per step of the reference's FlowSolver3D.advance on the host
+    (device "cpu", FP32; advance flushes denormals itself, ns3d/solver.py:998), after ``warm``
+    untimed steps: the method of validation/bench_ns3d.py:73-101."""
+    import torch
+    *_, FlowSolver3D = _reference_api()
+    old = torch.get_num_threads()
+    torch.set_num_threads(threads or os.cpu_count() or 1)
+    try:
+        s = FlowSolver3D(reference_box_config(nx, ny, nz, "cpu"))
+        s.advance(warm)
+        best = float("inf")
+        for _ in range(repeats):
+            t0 = time.perf_counter()
+            s.advance(steps)
+            best = min(best, (time.perf_counter() - t0) / steps)
+        return best, torch.get_num_threads()
+    finally:
+        torch.set_num_threads(old)
+
+
+def time_reference_gpu(nx, ny, nz, dev, steps=200, repeats=3):
+    """The reference's own PyTorch CUDA step on this GPU (fused NVRTC kernels, cuBLAS Poisson,
+    10-step CUDA graphs): best of ``repeats`` runs of ``advance(steps)`` after a 30-step warm-up
+    (NVRTC compile, graph capture), as validation/bench_ns3d.py:73-101 times it, with CUDA
+    events around each run.  Returns a dict for the bench line."""
+    import torch
+    try:
+        *_, FlowSolver3D = _reference_api()
+    except ImportError as exc:
+        return {"unavailable": str(exc)}
+    with torch.cuda.device(dev):
+        s = FlowSolver3D(reference_box_config(nx, ny, nz, f"cuda:{dev.index}"))
+        s.advance(30)
+        torch.cuda.synchronize()
+        clocks = Clocks(dev.index)
+        time.sleep(0.3)
+        best = float("inf")
+        for _ in range(repeats):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            a.record()
+            s.advance(steps)
+            b.record()
+            torch.cuda.synchronize()
+            best = min(best, a.elapsed_time(b) / steps)
+        clk = clocks.stop()
+        out = {"value": nx * ny * nz / (best * 1e-3) / 1e6, "unit": UNIT, "ms_per_step": best, "steps": steps,
+               "repeats": repeats, "fused_kernels": bool(getattr(s, "uses_fused_kernels", False)),
+               "cuda_graphs": bool(getattr(s, "uses_cuda_graphs", False)),
+               "fused_error": getattr(s, "fused_error", None), "clocks": clk,
+               "how": "reference FlowSolver3D.advance on this GPU (baseline/_ref, unmodified), best of "
+                      f"{repeats} x {steps} steps after 30 warm-up steps, CUDA events"}
+        del s
+        import gc
+        gc.collect()
+        torch.cuda.empty_cache()
+    return out
+
+
 def run_reference(args, rank):
+    """``--impl reference``: the reference's own CPU path (FlowSolver3D on the host cores)."""
     nx, ny, nz = args.shape
     if rank != 0:
         return
-    steps = max(1, min(args.steps, 3))
-    warm = max(1, min(args.warmup, 3))   # a numpy step takes seconds: both bounded
-    secs = oracle_sample(nx, ny, nz, steps, warm)
-    val = nx * ny * nz * steps / secs / 1e6
-    sample = f"{steps} full {nx}x{ny}x{nz} steps of the numpy oracle after {warm} untimed steps"
+    steps = max(1, min(args.steps, 5))
+    warm = max(1, min(args.warmup, 3))   # a reference CPU step takes about a second: both bounded
+    try:
+        per_step, cores = time_reference_cpu(nx, ny, nz, steps, warm)
+    except ImportError as exc:
+        print(json.dumps({"impl": "reference", "unavailable": f"reference not installed: {exc}"}), flush=True)
+        return
+    val = nx * ny * nz / per_step / 1e6
+    sample = (f"best of 3 x {steps} full {nx}x{ny}x{nz} steps of the reference's FlowSolver3D.advance "
+              f"(device cpu, FP32, {cores} threads) after {warm} untimed steps")
     line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": steps, "warmup": warm, "ms_per_step": 1e3 * secs / steps, "higher_is_better": True,
+            "steps": steps, "warmup": warm, "ms_per_step": 1e3 * per_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": _config(nx, ny, nz),
-            "cpu_baseline": {"value": val, "unit": UNIT, "cores": _threads(), "kind": "port", "sample": sample},
+            "cpu_baseline": {"value": val, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
             "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -314,13 +427,25 @@ def run_ours(args, rank, world, local_rank):
     achieved = alg / (phases["stage_kernel"] * 1e-3) / 1e9
     ms_step = ms / K
     value = world * cells * K / (ms * 1e-3) / 1e6
+    # the reference's own PyTorch CUDA step on this GPU, after our timed region
+    ref_gpu = None if args.no_ref_gpu else time_reference_gpu(nx, ny, nz, dev)
+    if ref_gpu and "value" in ref_gpu:
+        ref_gpu["speedup_of_value"] = value / ref_gpu["value"]
+        if e2e:
+            ref_gpu["speedup_of_e2e"] = e2e["value"] / ref_gpu["value"]
     sample_steps = 2
     if args.no_cpu:
         cpu = None
     else:
-        secs = oracle_sample(nx, ny, nz, sample_steps)
-        cpu = {"value": cells * sample_steps / secs / 1e6, "unit": UNIT, "cores": _threads(), "kind": "port",
-               "sample": f"{sample_steps} full {nx}x{ny}x{nz} steps of the numpy oracle after 1 untimed step"}
+        try:
+            per_step, cores = time_reference_cpu(nx, ny, nz, sample_steps, 1)
+            cpu = {"value": cells / per_step / 1e6, "unit": UNIT, "cores": cores, "kind": "reference",
+                   "sample": f"best of 3 x {sample_steps} full {nx}x{ny}x{nz} steps of the reference's "
+                             f"FlowSolver3D.advance (device cpu, FP32, {cores} threads) after 1 untimed step"}
+        except ImportError:
+            secs = oracle_sample(nx, ny, nz, sample_steps)
+            cpu = {"value": cells * sample_steps / secs / 1e6, "unit": UNIT, "cores": _threads(), "kind": "port",
+                   "sample": f"{sample_steps} full {nx}x{ny}x{nz} steps of the numpy oracle after 1 untimed step"}
     # DRAM bytes per stage_kernel launch (mean of the three stages) from the committed ncu
     # summary of this workload; None for other shapes
     traffic = None
@@ -336,7 +461,7 @@ def run_ours(args, rank, world, local_rank):
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "alg_bytes_per_launch": alg},
             "phases_ms": phases, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches_per_step(plan) * K,
-            "clocks": clk, "status": status}
+            "clocks": clk, "status": status, "reference_gpu": ref_gpu}
     print(json.dumps(line), flush=True)
 
 
@@ -1215,6 +1340,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--shape", type=int, nargs=3, default=list(SHAPE), help="nx ny nz (2:1:1)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-ref-gpu", action="store_true", help="skip timing the reference's CUDA step")
     ap.add_argument("--shard", action="store_true",
                     help="sweep2d with N > 1: split the 64 instances over the ranks instead of replicating them")
     args = ap.parse_args()

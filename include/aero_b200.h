@@ -32,6 +32,8 @@
  *                              _report), with the dye update of its lines 959-962
  *                              (core.py:703 advect_dye, core.py:779 _zero_dye_in_solids)
  *   aero_ns2d_poisson_solve    ns2d/poisson.py:126 PoissonSolver.solve
+ *   aero_closure_*, aero_mlp_* (no counterpart: the learned subgrid closure, which stands in
+ *                              for ns3d/core.py:448 eddy_viscosity3d (WALE) where it applies)
  */
 #ifndef AERO_B200_H
 #define AERO_B200_H
@@ -43,7 +45,7 @@
 extern "C" {
 #endif
 
-#define AERO_ABI_VERSION 4
+#define AERO_ABI_VERSION 5
 
 #define AERO_OK 0
 #define AERO_EINVAL -1        /* invalid argument or inconsistent configuration     */
@@ -121,6 +123,9 @@ typedef struct AeroNs3dConfig {
   double port_source;           /* their net mass flux in outlet-face units (h sum m)       */
   double port_leak;             /* uniform scalar leak of an unbalanced closed box (Q / V)  */
   int32_t nheat;                /* volumetric heaters (geom heaters; physics.py:464-491)    */
+  /* learned subgrid closure (geom closure): the eddy viscosity of an MLP's subgrid stress in
+   * place of WALE where it applies, WALE elsewhere; les must be AERO_LES_WALE, dtype FP32 */
+  int32_t closure;
 } AeroNs3dConfig;
 
 /* One actuator disc (ns3d/physics.py:831-979): its cell window, the force, swirl and
@@ -175,6 +180,7 @@ typedef struct AeroNs3dGeom {
   const AeroNs3dFan *fans;      /* host array of cfg.nfan descriptors, read at every step  */
   const AeroNs3dPort *ports;    /* host array of cfg.nport descriptors                     */
   const AeroNs3dHeater *heaters; /* host array of cfg.nheat descriptors                  */
+  const struct AeroClosureModel *closure; /* the trained closure when cfg.closure (host struct) */
 } AeroNs3dGeom;
 
 /* State in and out (device pointers of the plan's dtype).  u may alias u0, v v0, w w0 and
@@ -347,8 +353,82 @@ int aero_record_history(int32_t dtype, const void *t, const void *dt, const void
 int aero_welford(int32_t dtype, int32_t nfield, const void *const *x, void *const *mean, void *const *m2,
                  const int64_t *count, double *pending, double *time, void *stream);
 
+/* ---- learned subgrid closure ---------------------------------------------------------
+ * No counterpart in the reference: a per-cell MLP (10 inputs -> 3 x 128 SiLU -> 6 outputs)
+ * from the filtered velocity gradient to the subgrid stress, trained on pairs that the plain
+ * step makes by box-filtering its own fine periodic runs, run on the tensor cores in BF16 with
+ * FP32 accumulation.  In the step it replaces the WALE eddy viscosity of ns3d/core.py:448-482
+ * (ns3d/fused.py:102-132 ns3d_nut_wale) by the eddy viscosity with the learned stress's
+ * dissipation, nu_t = -tau:S / (2 S:S); WALE stays wherever that dissipation is not positive
+ * or an input lies outside its training range.
+ *
+ * Inputs of a gradient g (g33 = -(g11 + g22)): g11, g12, g13, g21, g22, g23, g31, g32 over |g|,
+ * (|W|^2 - |S|^2) / |g|^2 and sqrt(6) tr(S^3) / |S|^3 (S, W the symmetric and antisymmetric
+ * parts); outputs tau_xx, tau_yy, tau_zz, tau_xy, tau_xz, tau_yz over Delta^2 |g|^2, Delta the
+ * filter width (the grid spacing of the step).  Inputs and outputs are standardised with the
+ * model's means and standard deviations. */
+#define AERO_CLOSURE_IN 10
+#define AERO_CLOSURE_OUT 6
+#define AERO_CLOSURE_HIDDEN 128
+/* FP32 master parameters of the MLP, one flat array in this order: W1 (128, 10), b1 (128),
+ * W2 (128, 128), b2 (128), W3 (128, 128), b3 (128), W4 (6, 128), b4 (6); weights row-major
+ * [out][in].  The kernels read the BF16 copy of the weights (same offsets) and the FP32 biases. */
+#define AERO_CLOSURE_NPARAM 35206
+typedef struct AeroClosureModel {
+  const float *params;          /* device, AERO_CLOSURE_NPARAM FP32                         */
+  const void *params_bf16;      /* device, AERO_CLOSURE_NPARAM BF16 (the weights' copy)      */
+  float in_mean[AERO_CLOSURE_IN], in_std[AERO_CLOSURE_IN];
+  float in_lo[AERO_CLOSURE_IN], in_hi[AERO_CLOSURE_IN];     /* training range of the raw inputs */
+  float out_mean[AERO_CLOSURE_OUT], out_std[AERO_CLOSURE_OUT];
+} AeroClosureModel;
+
+/* Training pairs of an n^3 periodic FP32 state (u (n, n, n+1), v (n, n+1, n), w (n+1, n, n),
+ * cell size h) filtered by factor^3 boxes onto m^3 = (n / factor)^3 cells: g8 (8, m^3) the
+ * gradient of the filtered velocity by the step's own stencil (core.py:400-445) at spacing
+ * Delta = factor h, tau (6, m^3) the subgrid stress mean(u_a u_b) - mean(u_a) mean(u_b) of the
+ * cell-centred velocities.  work: 3 m^3 floats.  n % factor == 0. */
+int aero_closure_pairs(int32_t n, int32_t factor, const float *u, const float *v, const float *w, double h, float *g8,
+                       float *tau, float *work, void *stream);
+/* Raw inputs feat (n, 10), the output scale Delta^2 |g|^2 and validity (uint8) of n gradients
+ * g8 (8, n); with tau (6, n) non-NULL also the scaled targets (n, 6). */
+int aero_closure_features(int64_t n, const float *g8, double delta, const float *tau, float *feat, float *scale,
+                          uint8_t *valid, float *target, void *stream);
+/* Standardised BF16 inputs x (n, 16; columns 10..15 zero) and, with target non-NULL, FP32
+ * targets t (n, 6) with the model's means and standard deviations. */
+int aero_closure_normalise(int64_t n, const float *feat, const float *target, const AeroClosureModel *m, void *x,
+                           float *t, void *stream);
+/* The MLP on n standardised BF16 inputs x (n, 16): standardised outputs y (n, 6), FP32.
+ * status: device int, bit 2 set when a tensor-core wait ran out. */
+int aero_mlp_forward(const AeroClosureModel *m, const void *x, int64_t n, float *y, int32_t *status, void *stream);
+/* Device bytes of the training workspace for a batch (a multiple of 128). */
+size_t aero_mlp_train_workspace_bytes(int32_t batch);
+/* Gradient of the batch's mean squared error (over the batch rows idx and the 6 outputs) with
+ * respect to the parameters, added to grad (FP32, AERO_CLOSURE_NPARAM), by the tensor-core
+ * forward and backward passes; loss (device double) += the batch's sum of squared errors. */
+int aero_mlp_gradients(const float *params, const void *params_bf16, float *grad, const void *x, const float *t,
+                       const int32_t *idx, int32_t batch, double *loss, void *workspace, int32_t *status, void *stream);
+/* One Adam step (lr, beta1 0.9, beta2 0.999, eps 1e-8, step count `step` >= 1) on the batch
+ * rows idx (batch) of the standardised pairs (x, t): forward, mean squared error, backward,
+ * all on the tensor cores; params (FP32) and params_bf16 updated in place, adam_m / adam_v the
+ * moments (FP32, AERO_CLOSURE_NPARAM each), grad (FP32, zero on entry and on return); loss
+ * (device double) += the batch's sum of squared errors.  workspace: 256-byte aligned. */
+int aero_mlp_train_step(float *params, void *params_bf16, float *adam_m, float *adam_v, float *grad, const void *x,
+                        const float *t, const int32_t *idx, int32_t batch, int32_t step, float lr, double *loss,
+                        void *workspace, int32_t *status, void *stream);
+/* The closure's eddy-viscosity pass on n cells: grad9 (9, n) holds each cell's gradient (g11,
+ * g12, g13, g21, g22, g23, g31, g32) and window factor (1 - chi_c); nu (n) holds the WALE nu_t on
+ * entry and the closure's nu_t where it applies on return.  nut_max (device, NULL to skip)
+ * receives the maximum as the ordered bits of a double; counts (device, 2, NULL to skip) adds
+ * the cells evaluated and the cells that kept WALE.  delta: the grid spacing. */
+int aero_closure_eddy_viscosity(const AeroClosureModel *m, const float *grad9, int64_t n, double delta, float *nu,
+                                unsigned long long *nut_max, uint32_t *counts, int32_t *status, void *stream);
+/* Cells the last closure step evaluated and cells that kept WALE, summed over its eddy-viscosity
+ * passes since the workspace was initialised (reads through a host copy: synchronises). */
+int aero_ns3d_closure_counts(const AeroNs3dPlan *plan, const void *workspace, uint32_t out[2], void *stream);
+
 /* Device-side status word of the last step on this workspace (0 = fine; bit 0: a
- * non-finite value reached a reduction).  Reads through a host copy: synchronises. */
+ * non-finite value reached a reduction; bit 1: a plane load timed out; bit 2: a tensor-core
+ * wait of the closure timed out).  Reads through a host copy: synchronises. */
 int aero_ns3d_read_status(const AeroNs3dPlan *plan, const void *workspace, int32_t *status, void *stream);
 
 /* The checked build (libaero_b200_checked.so, compiled with AERO_BOUNDS_CHECK) records the
@@ -413,6 +493,10 @@ typedef struct {
    * ins_v (wy+1, wx); heat-flux skins q_skin (wy, wx) and weights w_f (n_flux, wy, wx);
    * area fractions vol_u, vol_v for the buoyancy share */
   const void *chi_t, *a_t, *w_t, *ins_u, *ins_v, *q_skin, *w_f, *vol_u, *vol_v;
+  /* the reference's live 0-d device scalars ops.nu, ops.eta, phys.kappa, phys.eta_t
+   * (ns2d/core.py:167-176 set_reynolds fills them in place while a captured graph stays
+   * valid), read by every launch; NULL: the config's nu, eta, kappa, eta_t */
+  const void *nu, *eta, *kappa, *eta_t;
 } AeroNs2dGeom;
 
 /* Step inputs (u0, v0, t0, dye0) and outputs; u / v may alias u0 / v0. */

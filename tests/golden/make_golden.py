@@ -1,8 +1,8 @@
 """Generate the golden vectors that pin the oracle to the reference (run in the build container).
 
-Usage (the reference must be importable; it is read, never modified)::
+Usage (the reference checkout is named by ``AEROLUME_REF``; it is read, never modified)::
 
-    PYTHONPATH=/root/reference/src PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden.py [case ...]
+    AEROLUME_REF=<reference checkout> PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden.py [case ...]
 
 (no case names: every case and the Poisson fixtures).
 
@@ -27,7 +27,9 @@ import numpy as np
 import torch
 
 HERE = Path(__file__).resolve().parent
-REF = Path(os.environ.get("AEROLUME_REF", "/root/reference"))
+if "AEROLUME_REF" not in os.environ:
+    sys.exit("set AEROLUME_REF to the reference checkout (the directory holding src/aerolume)")
+REF = Path(os.environ["AEROLUME_REF"])
 sys.path.insert(0, str(REF / "src"))
 
 from aerolume.solvers.ns3d import core  # noqa: E402
@@ -236,6 +238,19 @@ def main():
                   thermal=ThermalConfig3D(prandtl=0.71, richardson=0.2), ref_area=0.125, moment_ref=(1.25, 1.0, 0.0))
     run_case("tunnel_wale_heat_smoke_f64", tunnel, dtype="float64", rake=rake, steps=3)
     run_case("tunnel_wale_heat_smoke_f32", tunnel, dtype="float32", rake=rake, steps=3)
+    # the same physics on a grid that the stage kernel splits into two z-chunks of 16 planes
+    # and whose middle x-y tile (i0 = 32, j0 = 8) touches no domain side: 72 x 24 x 32, h = 1/8,
+    # a 1 x 1 x 0.5 box on the moving floor, WALE, heat, a four-nozzle rake
+    hm = 1.0 / 8.0
+    mid_box = ImmersedMesh(*box_mesh(1.0, 1.0, 0.5, (2.5, 1.5, 0.25)), name="box", thermal="temperature",
+                           thermal_value=1.0)
+    mid_rake = DyeRake("rake", [(1.25, 0.9, 0.15), (1.25, 1.3, 0.3), (1.25, 1.7, 0.2), (1.25, 2.1, 0.4)],
+                       radius=1.25 * hm)
+    mid = {"nx": 72, "ny": 24, "nz": 32, "h": hm, "x0": 0.0, "y0": 0.0, "z0": 0.0, "re": 1e4, "bodies": [mid_box],
+           "bc_zmin": "moving", "ground_speed": 1.0, "turbulence": "wale",
+           "thermal": ThermalConfig3D(prandtl=0.71, richardson=0.2), "ref_area": 0.5, "moment_ref": (2.5, 1.5, 0.0)}
+    run_case("tunnel_mid_f64", mid, dtype="float64", rake=mid_rake, seed=16, amp=0.05)
+    run_case("tunnel_mid_f32", mid, dtype="float32", rake=mid_rake, seed=16, amp=0.05)
 
     adia = ImmersedMesh(*box_mesh(0.5, 0.5, 0.5, (1.25, 0.0, 0.75)), name="adia")
     sym = dict(grid, y0=0.0, re=5e3, bodies=[adia], bc_y="symmetry_ymin", bc_zmax="noslip", turbulence="smagorinsky",

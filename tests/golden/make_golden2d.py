@@ -1,8 +1,8 @@
 """Generate the golden vectors that pin the 2D oracle to the reference (run in the build container).
 
-Usage (the reference must be importable; it is read, never modified)::
+Usage (the reference checkout is named by ``AEROLUME_REF``; it is read, never modified)::
 
-    PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden2d.py
+    AEROLUME_REF=<reference checkout> PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden2d.py
 
 Each case builds a configuration with the reference's own 2D API (``SolverConfig``,
 ``make_operators``, ``build_geometry``), starts from the reference's initial state plus seeded
@@ -24,7 +24,9 @@ import numpy as np
 import torch
 
 HERE = Path(__file__).resolve().parent
-REF = Path(os.environ.get("AEROLUME_REF", "/root/reference"))
+if "AEROLUME_REF" not in os.environ:
+    sys.exit("set AEROLUME_REF to the reference checkout (the directory holding src/aerolume)")
+REF = Path(os.environ["AEROLUME_REF"])
 sys.path.insert(0, str(REF / "src"))
 
 from aerolume.solvers.ns2d import core  # noqa: E402
