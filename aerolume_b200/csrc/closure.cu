@@ -147,6 +147,15 @@ __device__ __forceinline__ float tanh_fast(float x) {
   return y;
 }
 __device__ __forceinline__ float silu(float x) { return x * fmaf(0.5f, tanh_fast(0.5f * x), 0.5f); }
+// the same on a pair of BF16 pre-activations, in BF16 arithmetic (tanh.approx.bf16x2): the
+// hidden activations the network runs on, forward and (recomputed) backward
+__device__ __forceinline__ __nv_bfloat162 silu2(__nv_bfloat162 z) {
+  const __nv_bfloat162 half = __floats2bfloat162_rn(0.5f, 0.5f);
+  const __nv_bfloat162 a = __hmul2(z, half);
+  __nv_bfloat162 t;
+  asm("tanh.approx.bf16x2 %0, %1;" : "=r"(*reinterpret_cast<uint32_t *>(&t)) : "r"(*reinterpret_cast<const uint32_t *>(&a)));
+  return __hmul2(z, __hfma2(t, half, half));
+}
 // d silu / dx = s + x s (1 - s)
 __device__ __forceinline__ float silu_grad(float x) {
   const float s = fmaf(0.5f, tanh_fast(0.5f * x), 0.5f);
@@ -285,19 +294,17 @@ __device__ __forceinline__ void hidden_epilogue(FwdSmem &S, const float *bias, _
     tmem_ld32(tl + c0, v);
 #pragma unroll
     for (int i = 0; i < 32; ++i) v[i] += bias[c0 + i];
-    if (zpre) {
 #pragma unroll
-      for (int i = 0; i < 32; i += 8) {
-        __align__(16) __nv_bfloat162 p[4];
+    for (int i = 0; i < 32; i += 8) {
+      __align__(16) __nv_bfloat162 z[4], h[4];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) p[q] = __floats2bfloat162_rn(v[i + 2 * q], v[i + 2 * q + 1]);
-        *reinterpret_cast<uint4 *>(zpre + c0 + i) = *reinterpret_cast<const uint4 *>(p);
+      for (int q = 0; q < 4; ++q) {
+        z[q] = __floats2bfloat162_rn(v[i + 2 * q], v[i + 2 * q + 1]);
+        h[q] = silu2(z[q]);
       }
+      if (zpre) *reinterpret_cast<uint4 *>(zpre + c0 + i) = *reinterpret_cast<const uint4 *>(z);
+      *reinterpret_cast<uint4 *>(S.a + kmaj(r, c0 + i, NH)) = *reinterpret_cast<const uint4 *>(h);
     }
-#pragma unroll
-    for (int i = 0; i < 32; ++i) v[i] = silu(__bfloat162float(__float2bfloat16_rn(v[i])));
-#pragma unroll
-    for (int i = 0; i < 32; i += 8) store8(S.a, r, c0 + i, NH, v + i);
   }
 }
 
@@ -344,7 +351,7 @@ __device__ __forceinline__ bool fwd_tile(FwdSmem &S, uint32_t &phase, int *statu
 // batched inference on given inputs (n rows of KIN BF16 inputs, already normalised)
 // ------------------------------------------------------------------------------------------
 
-__global__ void __launch_bounds__(NTHREADS, 1) mlp_forward_kernel(MlpWeights W, const __nv_bfloat16 *x, int64_t n,
+__global__ void __launch_bounds__(NTHREADS, 2) mlp_forward_kernel(MlpWeights W, const __nv_bfloat16 *x, int64_t n,
                                                                   float *y, int *status) {
   pdl_wait();
   extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -387,7 +394,7 @@ struct TrainFwdParams {
   int *status;
 };
 
-__global__ void __launch_bounds__(NTHREADS, 1) mlp_train_forward_kernel(const __grid_constant__ TrainFwdParams P) {
+__global__ void __launch_bounds__(NTHREADS, 2) mlp_train_forward_kernel(const __grid_constant__ TrainFwdParams P) {
   pdl_wait();
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   FwdSmem &S = *reinterpret_cast<FwdSmem *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -547,11 +554,13 @@ __global__ void __launch_bounds__(NTHREADS, 1) mlp_train_backward_kernel(const _
         raw = L == 1 ? *reinterpret_cast<const uint4 *>(P.x + (size_t)P.idx[b] * KIN + c0)
                      : *reinterpret_cast<const uint4 *>(P.zin + (size_t)b * NH + c0);
       }
-      const __nv_bfloat16 *v = reinterpret_cast<const __nv_bfloat16 *>(&raw);
-      for (int i = 0; i < 8; ++i) {
-        const float hv = L == 1 ? __bfloat162float(v[i]) : silu(__bfloat162float(v[i]));
-        *reinterpret_cast<__nv_bfloat16 *>(S.ht + kmaj(c0 + i, tid, ROWS)) = __float2bfloat16_rn(valid ? hv : 0.f);
+      if (L != 1) {   // h = silu(z) exactly as the forward pass formed it
+        __nv_bfloat162 *pr = reinterpret_cast<__nv_bfloat162 *>(&raw);
+        for (int q = 0; q < 4; ++q) pr[q] = silu2(pr[q]);
       }
+      const __nv_bfloat16 *v = reinterpret_cast<const __nv_bfloat16 *>(&raw);
+      for (int i = 0; i < 8; ++i)
+        *reinterpret_cast<__nv_bfloat16 *>(S.ht + kmaj(c0 + i, tid, ROWS)) = valid ? v[i] : __float2bfloat16_rn(0.f);
     }
     operands_ready();
     if (tid == 0) {
@@ -805,7 +814,7 @@ __device__ __forceinline__ void max_atomic_f32(unsigned long long *dst, float v)
   atomicMax(dst, (unsigned long long)__double_as_longlong(d));
 }
 
-__global__ void __launch_bounds__(NTHREADS, 1) closure_nu_kernel(const __grid_constant__ ClosureStepParams P) {
+__global__ void __launch_bounds__(NTHREADS, 2) closure_nu_kernel(const __grid_constant__ ClosureStepParams P) {
   pdl_wait();
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   FwdSmem &S = *reinterpret_cast<FwdSmem *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -970,7 +979,9 @@ int aero_host::closure_nu(const AeroClosureModel *m, const float *grad, int64_t 
   P.counts = counts;
   P.status = status;
   const int64_t tiles = (plane + ROWS - 1) / ROWS;
-  const int grid = (int)std::min<int64_t>(tiles, nsm);
+  // two CTAs per SM (shared memory and tensor memory allow it): one CTA's epilogue runs
+  // while the other's MMAs do
+  const int grid = (int)std::min<int64_t>(tiles, 2 * (int64_t)nsm);
   AERO_CUDA_TRY(aero::launch_k(closure_nu_kernel, grid, NTHREADS, FWD_SMEM, s, P));
   return AERO_OK;
 }
@@ -1021,7 +1032,7 @@ int aero_mlp_forward(const AeroClosureModel *m, const void *x, int64_t n, float 
   const int rc = prepare(&nsm);
   if (rc) return rc;
   const int64_t tiles = (n + ROWS - 1) / ROWS;
-  AERO_CUDA_TRY(aero::launch_k(mlp_forward_kernel, (int)std::min<int64_t>(tiles, nsm), NTHREADS, FWD_SMEM,
+  AERO_CUDA_TRY(aero::launch_k(mlp_forward_kernel, (int)std::min<int64_t>(tiles, 2 * (int64_t)nsm), NTHREADS, FWD_SMEM,
                                static_cast<cudaStream_t>(stream), weights_of(m->params, m->params_bf16),
                                static_cast<const __nv_bfloat16 *>(x), n, y, reinterpret_cast<int *>(status)));
   return AERO_OK;
@@ -1051,7 +1062,7 @@ int aero_mlp_gradients(const float *params, const void *params_bf16, float *grad
   auto *dza = reinterpret_cast<__nv_bfloat16 *>(ws + aero_host::align_up(3 * b * NH * 2) + aero_host::align_up(b * KOUT * 2));
   auto *dzb = dza + aero_host::align_up(b * NH * 2) / 2;
   const auto *pb = static_cast<const __nv_bfloat16 *>(params_bf16);
-  const int tiles = batch / ROWS, grid = std::min(tiles, nsm);
+  const int tiles = batch / ROWS, grid = std::min(tiles, nsm);   // the backward kernels hold 512 TMEM columns
   TrainFwdParams F{};
   F.W = weights_of(params, params_bf16);
   F.x = static_cast<const __nv_bfloat16 *>(x);
@@ -1062,7 +1073,7 @@ int aero_mlp_gradients(const float *params, const void *params_bf16, float *grad
   F.dy = dy;
   F.loss = loss;
   F.status = reinterpret_cast<int *>(status);
-  AERO_CUDA_TRY(aero::launch_k(mlp_train_forward_kernel, grid, NTHREADS, FWD_SMEM, s, F));
+  AERO_CUDA_TRY(aero::launch_k(mlp_train_forward_kernel, std::min(tiles, 2 * nsm), NTHREADS, FWD_SMEM, s, F));
   const size_t zs = b * NH;
   struct L {
     int layer;

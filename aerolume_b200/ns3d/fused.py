@@ -73,14 +73,27 @@ class B200Kernels:
             self._remember(key, entry)
         return entry[0]
 
-    def dye_plan_for(self, ops):
-        key = ("dye", id(ops))
+    def dye_plan_for(self, ops, shape=None):
+        """The smoke-only plan of ``ops`` (or, for an ``ops`` that carries no grid, as the
+        reference's kernel self-test passes, of the field shape (nz, ny, nx))."""
+        key = ("dye", id(ops), shape)
         entry = self._plans.get(key)
         if entry is None:
-            plan = Ns3dPlan(ops, Geometry3D((0, 0, 0, 0, 0, 0)), None, None, smoke=True, device=self.device)
+            grid_ops = ops if hasattr(ops, "ghost") else _smoke_ops(ops, shape, self.dtype)
+            plan = Ns3dPlan(grid_ops, Geometry3D((0, 0, 0, 0, 0, 0)), None, None, smoke=True, device=self.device)
             entry = (plan, ops)
             self._remember(key, entry)
         return entry[0]
+
+
+def _smoke_ops(ops, shape, dtype):
+    """Operators of a smoke-only plan from the attributes the smoke update reads (cell size and
+    periodic axes) and the field shape."""
+    from .setup import make_ops
+    nz, ny, nx = shape
+    o = make_ops(nx, ny, nz, float(ops.h), re=1.0, dtype="float64" if dtype == torch.float64 else "float32")
+    o.periodic_axes = tuple(bool(x) for x in getattr(ops, "periodic_axes", (False, False, False)))
+    return o
 
 
 def load_kernels(scheme: str, device: torch.device, dtype: torch.dtype) -> B200Kernels:
@@ -127,4 +140,30 @@ def fast_step_phys(state, geom, ops, kern, dt=None, *, phys=None, theta=None, di
 def fast_dye(c, u, v, w, dt, ops, kern):
     """MUSCL / van Leer advection of one smoke channel with the step's velocity and dt."""
     dt = _dt_arg(dt, c)
-    return kern.dye_plan_for(ops).smoke_step(c, u, v, w, dt, dt, solids=False, sources=False)
+    return kern.dye_plan_for(ops, tuple(c.shape)).smoke_step(c, u, v, w, dt, dt, solids=False, sources=False)
+
+
+def check_dye_kernels(kern, device, dtype):
+    """The reference's self-test hook of the smoke kernels (fused.py:528-550): runs the B200
+    smoke update once on a small random field and raises RuntimeError when the library fails or
+    gives a non-finite or unbounded result (the solver then keeps its own smoke scheme)."""
+    from types import SimpleNamespace
+    try:
+        g = torch.Generator(device=device).manual_seed(7)
+        c = torch.rand((6, 5, 7), generator=g, device=device, dtype=dtype)
+        u = torch.randn((6, 5, 8), generator=g, device=device, dtype=dtype) * 0.1
+        v = torch.randn((6, 6, 7), generator=g, device=device, dtype=dtype) * 0.1
+        w = torch.randn((7, 5, 7), generator=g, device=device, dtype=dtype) * 0.1
+        out = fast_dye(c, u, v, w, torch.tensor(0.05, device=device, dtype=dtype),
+                       SimpleNamespace(periodic_axes=(False, False, False), h=0.1), kern)
+    except Exception as exc:
+        raise RuntimeError(f"B200 smoke kernels unavailable ({type(exc).__name__}: {exc})") from exc
+    if not (bool(torch.isfinite(out).all()) and float(out.max()) <= 1.0 and float(out.min()) >= 0.0):
+        raise RuntimeError("B200 smoke kernel self-test gave an out-of-range result")
+
+
+def check_theta_kernels(kern, device, dtype):
+    """The reference's self-test hook of the heat-equation kernels (fused.py:505-525): the B200
+    step advances theta inside ``fast_step_phys``, so this only checks that the library loads."""
+    from .. import _lib
+    _lib.lib()

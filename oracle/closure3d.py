@@ -13,8 +13,9 @@ the closure that the library computes around the network:
 * ``eddy_viscosity``: the closure's nu_t given the network's standardised outputs, with the
   fallback to the WALE value (the reference's core.py:448-482 model) where the learned
   dissipation is not positive or an input leaves the training range.
-* ``mlp``: the network in float32 with its operands rounded to bfloat16 between layers (the
-  precision the tensor-core kernels run at), for the kernels' tolerance checks.
+* ``mlp``: the network in float32 with its operands rounded to bfloat16 between layers and its
+  SiLU, x (1 + tanh(x / 2)) / 2, rounded to bfloat16 at each operation (the precision the
+  tensor-core kernels run at), for the kernels' tolerance checks.
 """
 from __future__ import annotations
 
@@ -111,7 +112,7 @@ def mlp(params, x, layout):
     for q in (1, 2, 3):
         z = h @ bf(views[f"w{q}"]).T + views[f"b{q}"]
         z = bf(z)
-        h = bf(z * torch.sigmoid(z))
+        h = bf(z * bf(0.5 * bf(torch.tanh(0.5 * z)) + 0.5))   # SiLU in BF16 arithmetic
     y = h @ bf(views["w4"]).T + views["b4"]
     return y.numpy().astype(np.float64)
 

@@ -33,7 +33,8 @@ def _torch_mlp(params, x):
     h = x[:, :10].to(torch.float32)
     for q in (1, 2, 3):
         z = bf(h @ bf(v[f"w{q}"]).T + v[f"b{q}"])
-        h = bf(z * torch.sigmoid(z))
+        # SiLU in BF16 arithmetic, as the kernels form it: z (1 + tanh(z / 2)) / 2
+        h = bf(z * bf(0.5 * bf(torch.tanh(0.5 * z)) + 0.5))
     return h @ bf(v["w4"]).T + v["b4"]
 
 
