@@ -42,7 +42,10 @@ EXPORTS = ("aero_abi_version", "aero_last_error", "aero_ns3d_plan_create", "aero
            "aero_mesh_sdf_workspace_bytes", "aero_mesh_signed_distance", "aero_record_history", "aero_welford",
            "aero_smoke_emitters", "aero_closure_pairs", "aero_closure_features", "aero_closure_normalise",
            "aero_mlp_forward", "aero_mlp_train_workspace_bytes", "aero_mlp_gradients", "aero_mlp_train_step",
-           "aero_closure_eddy_viscosity", "aero_ns3d_closure_counts")
+           "aero_closure_eddy_viscosity", "aero_ns3d_closure_counts", "aero_ns2d_sweep_create",
+           "aero_ns2d_sweep_destroy", "aero_ns2d_sweep_workspace_bytes", "aero_ns2d_sweep_init",
+           "aero_ns2d_sweep_step", "aero_ns2d_sweep_read_status", "aero_ns2d_sweep_set_barrier",
+           "aero_ns2d_sweep_info")
 
 CLOSURE_IN, CLOSURE_OUT, CLOSURE_HIDDEN, CLOSURE_NPARAM = 10, 6, 128, 35206
 
@@ -99,6 +102,10 @@ class Ns3dGeom(C.Structure):
         "chi_t", "a_t", "w_t", "adia_u", "adia_v", "adia_w", "vol_w", "skin", "dye_weight", "u_inlet",
         "paint_u", "paint_v", "paint_w", "paint_c")] + \
         [("fans", C.c_void_p), ("ports", C.c_void_p), ("heaters", C.c_void_p), ("closure", C.c_void_p)]
+
+
+class SweepTuning(C.Structure):
+    _fields_ = [("lcap", C.c_int32), ("ctas_per_sm", C.c_int32), ("order", C.c_int32)]
 
 
 class ClosureModel(C.Structure):
@@ -239,9 +246,23 @@ def lib() -> C.CDLL:
     L.aero_mlp_train_workspace_bytes.argtypes = [i32]
     L.aero_mlp_train_workspace_bytes.restype = C.c_size_t
     L.aero_mlp_train_step.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp, i32, i32, C.c_float, vp, vp, vp, vp]
-    L.aero_ns3d_closure_counts.argtypes = [vp, vp, C.POINTER(C.c_uint32), vp]
+    L.aero_ns3d_closure_counts.argtypes = [vp, vp, C.POINTER(C.c_uint64), vp]
     L.aero_mlp_gradients.argtypes = [vp, vp, vp, vp, vp, vp, i32, vp, vp, vp, vp]
     L.aero_closure_eddy_viscosity.argtypes = [C.POINTER(ClosureModel), vp, i64, C.c_double, vp, vp, vp, vp, vp]
+    L.aero_ns2d_sweep_create.argtypes = [i32, C.POINTER(vp), C.POINTER(Ns2dFields), C.POINTER(Ns2dGeom),
+                                         C.POINTER(vp), C.POINTER(SweepTuning), C.POINTER(vp)]
+    L.aero_ns2d_sweep_destroy.argtypes = [vp]
+    L.aero_ns2d_sweep_destroy.restype = None
+    L.aero_ns2d_sweep_workspace_bytes.argtypes = [vp]
+    L.aero_ns2d_sweep_workspace_bytes.restype = C.c_size_t
+    L.aero_ns2d_sweep_init.argtypes = [vp, vp, vp]
+    L.aero_ns2d_sweep_step.argtypes = [vp, vp, vp]
+    L.aero_ns2d_sweep_read_status.argtypes = [vp, vp, C.POINTER(C.c_int32), vp]
+    L.aero_ns2d_sweep_set_barrier.argtypes = [vp, i32, i32]
+    L.aero_ns2d_sweep_info.argtypes = [vp, C.POINTER(C.c_int64)]
+    for name in ("aero_ns2d_sweep_create", "aero_ns2d_sweep_init", "aero_ns2d_sweep_step", "aero_ns2d_sweep_read_status",
+                 "aero_ns2d_sweep_set_barrier", "aero_ns2d_sweep_info"):
+        getattr(L, name).restype = C.c_int
     for name in ("aero_closure_pairs", "aero_closure_features", "aero_closure_normalise", "aero_mlp_forward",
                  "aero_mlp_gradients", "aero_mlp_train_step", "aero_closure_eddy_viscosity",
                  "aero_ns3d_closure_counts"):

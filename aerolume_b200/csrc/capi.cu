@@ -338,7 +338,7 @@ int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom
   auto closure_pass = [&](unsigned long long *nut_max) -> int {
     return aero_host::closure_nu(g->closure, reinterpret_cast<const float *>(ws + p->off_grad), grad_plane, nx + 2,
                                  ny + 2, nz + 2, p->pn, c.h, reinterpret_cast<float *>(nu_buf), nut_max,
-                                 reinterpret_cast<unsigned int *>(ws + p->off_counts), status, s);
+                                 reinterpret_cast<unsigned long long *>(ws + p->off_counts), status, s);
   };
   S.dt = small;
   S.u0 = u0;
@@ -867,7 +867,7 @@ int aero_ns3d_plan_create(const AeroNs3dConfig *cfg, AeroNs3dPlan **plan) {
   p->off_pa = take(p->nc * e);
   p->off_nu = take(c.les != AERO_LES_NONE ? (nz + 2) * (ny + 2) * (size_t)p->pn * e : 0);
   p->off_grad = take(c.closure ? 9 * (nz + 2) * (ny + 2) * (size_t)p->pn * sizeof(float) : 0);
-  p->off_counts = take(c.closure ? 4 * sizeof(unsigned int) : 0);
+  p->off_counts = take(c.closure ? 2 * sizeof(unsigned long long) : 0);
   p->off_small = take(8 * e);
   p->off_scalars = take(sizeof(double) * aero::SC_COUNT);
   p->off_status = take(sizeof(int) * 4);
@@ -999,10 +999,10 @@ int aero_ns3d_poisson_solve_static(const AeroNs3dPlan *plan, const void *f, void
                                      : poisson_static_impl<float>(plan, f, psi, s);
 }
 
-int aero_ns3d_closure_counts(const AeroNs3dPlan *plan, const void *workspace, uint32_t out[2], void *stream) {
+int aero_ns3d_closure_counts(const AeroNs3dPlan *plan, const void *workspace, uint64_t out[2], void *stream) {
   if (!plan || !workspace || !out) return fail(AERO_EINVAL, "null argument");
   if (!plan->cfg.closure) return fail(AERO_EINVAL, "the plan has no learned closure");
-  uint32_t h[2] = {0, 0};
+  uint64_t h[2] = {0, 0};
   auto s = static_cast<cudaStream_t>(stream);
   CUDA_TRY(cudaMemcpyAsync(h, static_cast<const unsigned char *>(workspace) + plan->off_counts, sizeof(h),
                            cudaMemcpyDeviceToHost, s));

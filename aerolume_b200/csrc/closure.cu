@@ -804,7 +804,7 @@ struct ClosureStepParams {
   float delta;                // filter width (the cell size)
   float *nu;                  // (nzp, nyp, pitch) nu_t: WALE in, closure out
   unsigned long long *nut_max;
-  unsigned int *counts;       // [0] cells evaluated, [1] cells that kept WALE
+  unsigned long long *counts; // [0] cells evaluated, [1] cells that kept WALE
   int *status;
 };
 
@@ -824,7 +824,7 @@ __global__ void __launch_bounds__(NTHREADS, 2) closure_nu_kernel(const __grid_co
   const int64_t total = P.plane;
   const int64_t ntiles = (total + ROWS - 1) / ROWS;
   float mx = 0.f;
-  unsigned int n_eval = 0, n_wale = 0;
+  unsigned long long n_eval = 0, n_wale = 0;
   for (int64_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
     const int64_t e = t * ROWS + threadIdx.x;
     const int i = (int)(e % P.pitch);
@@ -959,7 +959,7 @@ int grid_for(int64_t items, int per_block = 256) {
 
 // the closure's pass in the step (declared in host_common.cuh)
 int aero_host::closure_nu(const AeroClosureModel *m, const float *grad, int64_t plane, int nxp, int nyp, int nzp,
-                          int pitch, double delta, float *nu, unsigned long long *nut_max, unsigned int *counts,
+                          int pitch, double delta, float *nu, unsigned long long *nut_max, unsigned long long *counts,
                           int *status, cudaStream_t s) {
   int nsm = 0;
   const int rc = prepare(&nsm);
@@ -1121,12 +1121,13 @@ int aero_mlp_train_step(float *params, void *params_bf16, float *adam_m, float *
 }
 
 int aero_closure_eddy_viscosity(const AeroClosureModel *m, const float *grad9, int64_t n, double delta, float *nu,
-                                unsigned long long *nut_max, uint32_t *counts, int32_t *status, void *stream) {
+                                unsigned long long *nut_max, uint64_t *counts, int32_t *status, void *stream) {
   if (!m || !m->params || !m->params_bf16 || !grad9 || !nu || !status)
     return aero_host::set_error(AERO_EINVAL, "null argument");
   if (n <= 0) return AERO_OK;
   if (n > INT32_MAX) return aero_host::set_error(AERO_EINVAL, "too many cells for one call");
-  return aero_host::closure_nu(m, grad9, n, (int)n, 1, 1, (int)n, delta, nu, nut_max, counts,
+  return aero_host::closure_nu(m, grad9, n, (int)n, 1, 1, (int)n, delta, nu, nut_max,
+                               reinterpret_cast<unsigned long long *>(counts),
                                reinterpret_cast<int *>(status), static_cast<cudaStream_t>(stream));
 }
 

@@ -18,7 +18,8 @@ int set_error(int code, const std::string &msg);
 // (nzp, nyp, pitch) cells whose gradient and window factor the eddy-viscosity kernel left in
 // grad (9 components, `plane` apart), nu_t of the learned stress where it applies.
 int closure_nu(const AeroClosureModel *m, const float *grad, int64_t plane, int nxp, int nyp, int nzp, int pitch,
-               double delta, float *nu, unsigned long long *nut_max, unsigned int *counts, int *status, cudaStream_t s);
+               double delta, float *nu, unsigned long long *nut_max, unsigned long long *counts, int *status,
+               cudaStream_t s);
 
 constexpr size_t ALIGN = 256;
 inline size_t align_up(size_t x) { return (x + ALIGN - 1) & ~(ALIGN - 1); }

@@ -16,9 +16,14 @@
 // blend, the inlet / outlet balance, the implicit Brinkman penalisation and the bodies'
 // force partials.  The Poisson solve runs the transform kernels of poisson.cu on the grid
 // as (nz, ny, nx) = (ny, 1, nx): x forward, y forward-solve-inverse, x inverse.
+#include <cstring>
+#include <type_traits>
+#include <vector>
+
 #include "host_common.cuh"
 #include "ns3d.cuh"
 #include "stencil.cuh"
+#include "transform.cuh"
 
 namespace aero {
 namespace ns2d {
@@ -48,37 +53,46 @@ __device__ __forceinline__ T padded2f(const Rules2<T> &r, int j, int i, const Lo
   return sy * (sx * x + cx) + cy;
 }
 
-template <typename T>
+// NC: read through the non-coherent read-only path (__ldg), right for a launch that does not
+// write the array; the batched sweep's persistent kernel, which rewrites psi and the stage
+// values between its phases, reads them with coherent loads (NC = false).
+template <bool NC, typename T>
+__device__ __forceinline__ T ldx(const T *p) {
+  if constexpr (NC) return __ldg(p);
+  else return *p;
+}
+
+template <typename T, bool NC = true>
 __device__ __forceinline__ T padded2(const T *__restrict__ f, const Rules2<T> &r, int j, int i) {
-  return padded2f<T>(r, j, i, [&](int mj, int mi) { return __ldg(f + (size_t)mj * r.p0 + mi); });
+  return padded2f<T>(r, j, i, [&](int mj, int mi) { return ldx<NC>(f + (size_t)mj * r.p0 + mi); });
 }
 
 // The projected velocity u = u_hat - grad psi on the u-face (j, fi) and the v-face (fj, i),
 // the correction of ns2d/core.py:632-646 (boundary-normal faces of a bounded domain keep
 // u_hat; a periodic domain wraps psi); correct2d_kernel writes the same values.
-template <typename T>
+template <typename T, bool NC = true>
 __device__ __forceinline__ T projected_u(const T *__restrict__ uh, const T *__restrict__ psi, int nx, int periodic,
                                          T inv_h, int j, int fi) {
   const size_t c = (size_t)j * nx;
-  const T x = __ldg(uh + (size_t)j * (nx + 1) + fi);
+  const T x = ldx<NC>(uh + (size_t)j * (nx + 1) + fi);
   if (periodic) {
     const int ii = fi == nx ? 0 : fi, il = ii == 0 ? nx - 1 : ii - 1;
-    return x - (__ldg(psi + c + ii) - __ldg(psi + c + il)) * inv_h;
+    return x - (ldx<NC>(psi + c + ii) - ldx<NC>(psi + c + il)) * inv_h;
   }
   if (fi == 0 || fi == nx) return x;
-  return x - (__ldg(psi + c + fi) - __ldg(psi + c + fi - 1)) * inv_h;
+  return x - (ldx<NC>(psi + c + fi) - ldx<NC>(psi + c + fi - 1)) * inv_h;
 }
 
-template <typename T>
+template <typename T, bool NC = true>
 __device__ __forceinline__ T projected_v(const T *__restrict__ vh, const T *__restrict__ psi, int nx, int ny,
                                          int periodic, T inv_h, int fj, int i) {
-  const T x = __ldg(vh + (size_t)fj * nx + i);
+  const T x = ldx<NC>(vh + (size_t)fj * nx + i);
   if (periodic) {
     const int jj = fj == ny ? 0 : fj, jl = jj == 0 ? ny - 1 : jj - 1;
-    return x - (__ldg(psi + (size_t)jj * nx + i) - __ldg(psi + (size_t)jl * nx + i)) * inv_h;
+    return x - (ldx<NC>(psi + (size_t)jj * nx + i) - ldx<NC>(psi + (size_t)jl * nx + i)) * inv_h;
   }
   if (fj == 0 || fj == ny) return x;
-  return x - (__ldg(psi + (size_t)fj * nx + i) - __ldg(psi + (size_t)(fj - 1) * nx + i)) * inv_h;
+  return x - (ldx<NC>(psi + (size_t)fj * nx + i) - ldx<NC>(psi + (size_t)(fj - 1) * nx + i)) * inv_h;
 }
 
 // Eddy viscosity of the 2D gradient (core.py:469-500); cfac = c^2 h^2 (Smagorinsky, WALE)
@@ -190,9 +204,12 @@ struct StageParams {
 // viscosity of the tile's cells (the first stage's dt needs it before the update); HEAT: the
 // heat-transfer instantiation (thermal dt limits, buoyancy and its force share, nu_t and the
 // stage-start face velocities handed to the theta stage), so the plain step carries none of it.
-template <typename T, bool NU_ONLY, bool HEAT>
-__global__ void __launch_bounds__(NT) stage2d_kernel(const __grid_constant__ StageParams<T> P) {
-  aero::pdl_wait();
+//
+// The body takes its tile (bx, by) of a gx-wide grid and its thread tid (0 .. NT-1)
+// explicitly: stage2d_kernel runs it as one launch per instance, the batched sweep's
+// persistent kernel (sweep2d.cu) as one work item among every instance's tiles.
+template <typename T, bool NU_ONLY, bool HEAT, bool NC = true>
+__device__ __forceinline__ void stage2d_body(const StageParams<T> &P, int bx, int by, int gx, int tid_) {
   __shared__ T U[UY][UX];
   __shared__ T V[VY][VX];
   __shared__ T NU[CY][CX], TXX[CY][CX], TYY[CY][CX];
@@ -200,8 +217,8 @@ __global__ void __launch_bounds__(NT) stage2d_kernel(const __grid_constant__ Sta
   __shared__ double red[NT / 32][MAXQ];
   __shared__ T corr_s;
   const int nx = P.nx, ny = P.ny;
-  const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * TX + tx;
-  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
+  const int tid = tid_, tx = tid % TX, ty = tid / TX;
+  const int i0 = bx * TX, j0 = by * TY;
   const bool tunnel = !P.periodic && !P.closed;
   const T nuh2 = P.live_nu ? __ldg(P.live_nu) * P.inv_h2 : P.nuh2;
   const T eta = P.live_eta ? __ldg(P.live_eta) : P.eta;
@@ -214,15 +231,15 @@ __global__ void __launch_bounds__(NT) stage2d_kernel(const __grid_constant__ Sta
   } else {
     dt = *P.dt;
   }
-  if (P.dt_here && blockIdx.x == 0 && blockIdx.y == 0 && tid == 0) *P.dt_store = dt;
+  if (P.dt_here && bx == 0 && by == 0 && tid == 0) *P.dt_store = dt;
   const T bdt = dt * P.b;
   // outlet balance (core.py:352-359): every block with outlet faces sums the whole outlet
   // column of the stage value in the same fixed order, so all agree
   if (!NU_ONLY && tunnel && i0 + TX >= nx && tid < 32) {
     double s_in = 0.0, s_out = 0.0;
     for (int j = tid; j < ny; j += 32) {
-      const T un = P.psi ? projected_u<T>(P.up, P.psi, nx, P.periodic, P.inv_h, j, nx) : P.up[(size_t)j * (nx + 1) + nx];
-      const T un1 = P.psi ? projected_u<T>(P.up, P.psi, nx, P.periodic, P.inv_h, j, nx - 1)
+      const T un = P.psi ? projected_u<T, NC>(P.up, P.psi, nx, P.periodic, P.inv_h, j, nx) : P.up[(size_t)j * (nx + 1) + nx];
+      const T un1 = P.psi ? projected_u<T, NC>(P.up, P.psi, nx, P.periodic, P.inv_h, j, nx - 1)
                           : P.up[(size_t)j * (nx + 1) + nx - 1];
       const T lu = (un1 - un) * P.inv_h;
       const T uo = P.a == T(0) ? un : lerp_t<T>(un, P.u0[(size_t)j * (nx + 1) + nx], P.a);
@@ -237,23 +254,23 @@ __global__ void __launch_bounds__(NT) stage2d_kernel(const __grid_constant__ Sta
     for (int e = tid; e < UY * UX; e += NT) {
       const int r = e / UX, c = e - r * UX;
       U[r][c] = padded2f<T>(P.ru, j0 - 2 + r, i0 - 2 + c, [&](int mj, int mi) {
-        return projected_u<T>(P.up, P.psi, nx, P.periodic, P.inv_h, mj, mi);
+        return projected_u<T, NC>(P.up, P.psi, nx, P.periodic, P.inv_h, mj, mi);
       });
     }
     for (int e = tid; e < VY * VX; e += NT) {
       const int r = e / VX, c = e - r * VX;
       V[r][c] = padded2f<T>(P.rv, j0 - 2 + r, i0 - 2 + c, [&](int mj, int mi) {
-        return projected_v<T>(P.vp, P.psi, nx, ny, P.periodic, P.inv_h, mj, mi);
+        return projected_v<T, NC>(P.vp, P.psi, nx, ny, P.periodic, P.inv_h, mj, mi);
       });
     }
   } else {
     for (int e = tid; e < UY * UX; e += NT) {
       const int r = e / UX, c = e - r * UX;
-      U[r][c] = padded2<T>(P.up, P.ru, j0 - 2 + r, i0 - 2 + c);
+      U[r][c] = padded2<T, NC>(P.up, P.ru, j0 - 2 + r, i0 - 2 + c);
     }
     for (int e = tid; e < VY * VX; e += NT) {
       const int r = e / VX, c = e - r * VX;
-      V[r][c] = padded2<T>(P.vp, P.rv, j0 - 2 + r, i0 - 2 + c);
+      V[r][c] = padded2<T, NC>(P.vp, P.rv, j0 - 2 + r, i0 - 2 + c);
     }
   }
   __syncthreads();
@@ -461,19 +478,23 @@ __global__ void __launch_bounds__(NT) stage2d_kernel(const __grid_constant__ Sta
     if (tid < nq) {
       double s = 0.0;
       for (int wv = 0; wv < NT / 32; ++wv) s += red[wv][tid];
-      P.partials[(size_t)(blockIdx.y * gridDim.x + blockIdx.x) * nq + tid] = s;
+      P.partials[(size_t)(by * gx + bx) * nq + tid] = s;
     }
   }
+}
+
+template <typename T, bool NU_ONLY, bool HEAT>
+__global__ void __launch_bounds__(NT) stage2d_kernel(const __grid_constant__ StageParams<T> P) {
+  aero::pdl_wait();
+  stage2d_body<T, NU_ONLY, HEAT>(P, blockIdx.x, blockIdx.y, gridDim.x, threadIdx.y * TX + threadIdx.x);
 }
 
 // u <- uh - grad psi (core.py:643-660); one thread per cell column, the thread of the last
 // column also does the last u-face and the thread of the last row the last v-face
 template <typename T>
-__global__ void correct2d_kernel(int nx, int ny, int periodic, T inv_h, const T *__restrict__ uh,
-                                 const T *__restrict__ vh, const T *__restrict__ psi, T *__restrict__ u,
-                                 T *__restrict__ v) {
-  aero::pdl_wait();
-  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+__device__ __forceinline__ void correct2d_body(int nx, int ny, int periodic, T inv_h, const T *__restrict__ uh,
+                                               const T *__restrict__ vh, const T *__restrict__ psi, T *__restrict__ u,
+                                               T *__restrict__ v, int i, int j) {
   if (i >= nx || j >= ny) return;
   const size_t c = (size_t)j * nx;
   for (int fi = i; fi <= (i == nx - 1 ? nx : i); ++fi) {
@@ -504,16 +525,29 @@ __global__ void correct2d_kernel(int nx, int ny, int periodic, T inv_h, const T 
   }
 }
 
+template <typename T>
+__global__ void correct2d_kernel(int nx, int ny, int periodic, T inv_h, const T *__restrict__ uh,
+                                 const T *__restrict__ vh, const T *__restrict__ psi, T *__restrict__ u,
+                                 T *__restrict__ v) {
+  aero::pdl_wait();
+  correct2d_body<T>(nx, ny, periodic, inv_h, uh, vh, psi, u, v, blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y);
+}
+
 // ((u_{i+1} - u_i) + v_{j+1}) - v_j, over h (core.py:620-622)
 template <typename T>
-__global__ void divergence2d_kernel(int nx, int ny, T inv_h, const T *__restrict__ u, const T *__restrict__ v,
-                                    T *__restrict__ div) {
-  aero::pdl_wait();
-  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+__device__ __forceinline__ void divergence2d_body(int nx, int ny, T inv_h, const T *__restrict__ u,
+                                                  const T *__restrict__ v, T *__restrict__ div, int i, int j) {
   if (i >= nx || j >= ny) return;
   const size_t ru = (size_t)j * (nx + 1);
   div[(size_t)j * nx + i] =
       (((u[ru + i + 1] - u[ru + i]) + v[(size_t)(j + 1) * nx + i]) - v[(size_t)j * nx + i]) * inv_h;
+}
+
+template <typename T>
+__global__ void divergence2d_kernel(int nx, int ny, T inv_h, const T *__restrict__ u, const T *__restrict__ v,
+                                    T *__restrict__ div) {
+  aero::pdl_wait();
+  divergence2d_body<T>(nx, ny, inv_h, u, v, div, blockIdx.x * blockDim.x + threadIdx.x, blockIdx.y);
 }
 
 template <typename T>
@@ -855,19 +889,19 @@ __global__ void heat_report2d_kernel(const __grid_constant__ ReportParams<T> P) 
 
 // Coefficients [Cd, Cl, Cm] per body from the stage partials in a fixed order, t + dt, dt
 template <typename T>
-__global__ void finalize2d_kernel(const double *__restrict__ partials, int nblocks, int nbody, double h,
-                                  double force_ref, const T *dt, const T *t0, T *t_out, T *dt_out, T *coeffs) {
-  aero::pdl_wait();
+__device__ __forceinline__ void finalize2d_body(const double *__restrict__ partials, int nblocks, int nbody, double h,
+                                                double force_ref, const T *dt, const T *t0, T *t_out, T *dt_out,
+                                                T *coeffs, int tid, int nthr) {
   __shared__ double tot[MAXQ];
   const int nq = 4 * nbody;
-  for (int q = threadIdx.x >> 5; q < nq; q += blockDim.x >> 5) {
+  for (int q = tid >> 5; q < nq; q += nthr >> 5) {
     double s = 0.0;
-    for (int e = threadIdx.x & 31; e < 3 * nblocks; e += 32) s += partials[(size_t)e * nq + q];
+    for (int e = tid & 31; e < 3 * nblocks; e += 32) s += partials[(size_t)e * nq + q];
     s = warp_sum(s);
-    if ((threadIdx.x & 31) == 0) tot[q] = s;
+    if ((tid & 31) == 0) tot[q] = s;
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
+  if (tid == 0) {
     const T d = *dt;
     *t_out = *t0 + d;
     *dt_out = d;
@@ -880,6 +914,202 @@ __global__ void finalize2d_kernel(const double *__restrict__ partials, int nbloc
     }
   }
 }
+
+template <typename T>
+__global__ void finalize2d_kernel(const double *__restrict__ partials, int nblocks, int nbody, double h,
+                                  double force_ref, const T *dt, const T *t0, T *t_out, T *dt_out, T *coeffs) {
+  aero::pdl_wait();
+  finalize2d_body<T>(partials, nblocks, nbody, h, force_ref, dt, t0, t_out, dt_out, coeffs, threadIdx.x, blockDim.x);
+}
+
+// ---------------------------------------------------------------------------------------
+// The batched sweep: every instance's step as one persistent launch
+// ---------------------------------------------------------------------------------------
+//
+// aero_ns2d_step of each instance is recorded as its sequence of operations (the launches it
+// would make: zeroing the maxima, the maxima, the three stage kernels with their transform
+// passes, the correction, the finalisation), each with its parameters and its grid of work
+// items.  Phase p of the sweep is operation p of every instance; one persistent kernel runs
+// the phases in order, its CTAs taking the work items of all instances' operations of the
+// phase (a grid-stride loop over their concatenation), with a grid barrier between phases.
+// Every work item runs the same device body as the single-instance launch (stage2d_body,
+// the transform bodies, correct2d_body, ...) on the same tile, so each instance's result is
+// bit-identical to stepping it alone.
+
+namespace sweep {
+
+enum Kind : int { ZERO = 0, MAXABS = 1, STAGE = 2, POW2 = 3, LINE = 4, DIV = 5, PSIACC = 6, CORRECT = 7, FINAL = 8 };
+
+struct ZeroArgs { double *p; int n; };
+struct MaxArgs { MaxJobs<float> J; int njobs; long long chunk; };
+struct DivArgs { int nx, ny; float inv_h; const float *u, *v; float *div; };
+struct PsiArgs { const float *psi; float *pw; long long n; float wgt; int mode; const float *dt; };
+struct CorrArgs { int nx, ny, periodic; float inv_h; const float *uh, *vh, *psi; float *u, *v; };
+struct FinalArgs {
+  const double *partials;
+  int nblocks, nbody;
+  double h, force_ref;
+  const float *dt, *t0;
+  float *t_out, *dt_out, *coeffs;
+};
+
+struct Op {
+  int kind, gx, gy, n;   // n: the transform length of POW2
+  union Args {
+    StageParams<float> st;
+    TransformParams<float> tr;
+    ZeroArgs zero;
+    MaxArgs mx;
+    DivArgs dv;
+    PsiArgs pa;
+    CorrArgs co;
+    FinalArgs fi;
+  } a;
+};
+
+// the recording of one instance's step (host)
+struct Recorder {
+  std::vector<Op> ops;
+  int lcap;   // log2 of the widest power-of-two transform tile
+};
+
+struct Tables {
+  const Op *ops;
+  const int *phase_first, *phase_count, *op_index;
+  const long long *phase_items, *op_prefix;
+  int nphase;
+  unsigned int *bar;   // [0] arrivals, [1] generation
+  int *status;         // bit 0: a grid barrier ran out
+  int spin_limit, extra;
+};
+
+constexpr int NTHR = 256;
+constexpr long long MAX_CHUNK = 2048;   // elements of one work item of the maxima
+
+// Grid-wide barrier between phases: arrivals counted atomically, the last one bumps the
+// generation; the others poll it (bounded: after spin_limit polls bit 0 of the status is set
+// and every CTA returns).  extra > 0 asks for more arrivals than CTAs (a test of the bound).
+__device__ __forceinline__ bool grid_barrier(const Tables &T) {
+  __shared__ int ok_s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned int *gen = T.bar + 1;
+    const unsigned int g0 = *gen;
+    __threadfence();
+    const unsigned int expect = gridDim.x + (unsigned int)T.extra;
+    int ok = 1;
+    if (atomicAdd(T.bar, 1u) == expect - 1u) {
+      atomicExch(T.bar, 0u);
+      __threadfence();
+      atomicAdd(T.bar + 1, 1u);
+    } else {
+      int it = 0;
+      while (*gen == g0) {
+        if (++it >= T.spin_limit) {
+          ok = 0;
+          atomicOr(T.status, 1);
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    ok_s = ok;
+  }
+  __syncthreads();
+  return ok_s != 0;
+}
+
+template <int N, int LCAP>
+struct Cap {
+  static constexpr int L2 = Pow2Tile<float, N>::LOG2L < LCAP ? Pow2Tile<float, N>::LOG2L : LCAP;
+};
+
+template <int LCAP>
+__device__ __forceinline__ void run_pow2(const TransformParams<float> &P, int n, int bx, int by, unsigned char *sm) {
+  switch (n) {
+    case 64: pow2_transform_body<float, 64, Cap<64, LCAP>::L2>(P, bx, by, sm); break;
+    case 128: pow2_transform_body<float, 128, Cap<128, LCAP>::L2>(P, bx, by, sm); break;
+    case 256: pow2_transform_body<float, 256, Cap<256, LCAP>::L2>(P, bx, by, sm); break;
+    case 512: pow2_transform_body<float, 512, Cap<512, LCAP>::L2>(P, bx, by, sm); break;
+    case 1024: pow2_transform_body<float, 1024, Cap<1024, LCAP>::L2>(P, bx, by, sm); break;
+    default: pow2_transform_body<float, 2048, Cap<2048, LCAP>::L2>(P, bx, by, sm); break;
+  }
+}
+
+template <int LCAP>
+__global__ void __launch_bounds__(NTHR, 2) sweep2d_kernel(const __grid_constant__ Tables T) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int tid = threadIdx.x;
+  for (int ph = 0; ph < T.nphase; ++ph) {
+    const long long items = T.phase_items[ph];
+    const int f = T.phase_first[ph], c = T.phase_count[ph];
+    for (long long g = blockIdx.x; g < items; g += gridDim.x) {
+      int lo = 0, hi = c - 1;   // the operation whose items hold g
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (T.op_prefix[f + mid] <= g) lo = mid;
+        else hi = mid - 1;
+      }
+      const Op &op = T.ops[T.op_index[f + lo]];
+      const long long b = g - T.op_prefix[f + lo];
+      const int bx = (int)(b % op.gx), by = (int)(b / op.gx);
+      switch (op.kind) {
+        case ZERO:
+          if (tid < op.a.zero.n) op.a.zero.p[tid] = 0.0;
+          break;
+        case MAXABS: {
+          const MaxJob<float> &q = op.a.mx.J.job[by];
+          const long long e0 = (long long)bx * op.a.mx.chunk, e1 = min(e0 + op.a.mx.chunk, (long long)q.n);
+          float m = 0.f;
+          for (long long e = e0 + tid; e < e1; e += NTHR) {
+            const float v = fabsf(__ldg(q.a + e));
+            m = (v > m || v != v) ? v : m;
+          }
+          block_max_atomic<float>(m, q.out);
+          break;
+        }
+        case STAGE: stage2d_body<float, false, false, false>(op.a.st, bx, by, op.gx, tid); break;
+        case POW2: run_pow2<LCAP>(op.a.tr, op.n, bx, by, smem_raw); break;
+        case LINE: line_transform_body<float>(op.a.tr, bx, by, smem_raw); break;
+        case DIV: {
+          const DivArgs &a = op.a.dv;
+          divergence2d_body<float>(a.nx, a.ny, a.inv_h, a.u, a.v, a.div, bx * NTHR + tid, by);
+          break;
+        }
+        case PSIACC: {
+          const PsiArgs &a = op.a.pa;
+          const float rdt = a.mode == 2 ? 1.f / *a.dt : 1.f;
+          const long long e = b * NTHR + tid;
+          if (e < a.n) {
+            if (a.mode == 0) {
+              a.pw[e] = a.psi[e] * a.wgt;
+            } else {
+              const float sum = a.pw[e] + a.wgt * a.psi[e];
+              a.pw[e] = a.mode == 2 ? sum * rdt : sum;
+            }
+          }
+          break;
+        }
+        case CORRECT: {
+          const CorrArgs &a = op.a.co;
+          correct2d_body<float>(a.nx, a.ny, a.periodic, a.inv_h, a.uh, a.vh, a.psi, a.u, a.v, bx * NTHR + tid, by);
+          break;
+        }
+        default: {
+          const FinalArgs &a = op.a.fi;
+          finalize2d_body<float>(a.partials, a.nblocks, a.nbody, a.h, a.force_ref, a.dt, a.t0, a.t_out, a.dt_out,
+                                 a.coeffs, tid, NTHR);
+          break;
+        }
+      }
+      __syncthreads();   // the item's shared memory is free for the next one
+    }
+    if (!grid_barrier(T)) return;
+  }
+}
+
+}  // namespace sweep
 
 }  // namespace ns2d
 }  // namespace aero
@@ -923,9 +1153,45 @@ aero::ns2d::Rules2<T> rules2(const AeroNs2dConfig &c, int comp) {
 }
 
 // psi = L^{-1} f: x forward, y forward-solve-inverse, x inverse on the (ny, 1, nx) view
+using aero::ns2d::sweep::Op;
+using aero::ns2d::sweep::Recorder;
+
+Op new_op(int kind, long long gx, int gy) {
+  Op o;
+  std::memset(&o, 0, sizeof(o));
+  o.kind = kind;
+  o.gx = (int)std::max<long long>(gx, 1);
+  o.gy = std::max(gy, 1);
+  return o;
+}
+
+// one transform pass as a sweep operation (power-of-two tiles no wider than 2^lcap lines)
+int record_transform(Recorder *rec, const aero::TransformParams<float> &P) {
+  namespace sw = aero::ns2d::sweep;
+  const int n = P.A.n;
+  const size_t lines_x = (size_t)P.nz * P.ny;
+  const int gy = P.axis == 0 ? 1 : (P.axis == 1 ? P.nz : P.ny);
+  if (P.A.method == 0 && aero::transform_pow2(n)) {
+    if (n < 64) return set_error(AERO_EUNSUPPORTED, "the persistent sweep needs transform lengths of at least 64");
+    const int l2 = std::min(aero::fft::tile_log2L(n, 4), rec->lcap), L = 1 << l2;
+    Op o = new_op(sw::POW2, P.axis == 0 ? (long long)((lines_x + L - 1) / L) : (P.nx + L - 1) / L, gy);
+    o.n = n;
+    o.a.tr = P;
+    rec->ops.push_back(o);
+    return AERO_OK;
+  }
+  if (P.fuse_div || P.p_acc) return set_error(AERO_EINVAL, "fused transform passes need power-of-two axes");
+  const int L = P.L;
+  Op o = new_op(sw::LINE, P.axis == 0 ? (long long)((lines_x + L - 1) / L) : (P.nx + L - 1) / L, gy);
+  o.n = n;
+  o.a.tr = P;
+  rec->ops.push_back(o);
+  return AERO_OK;
+}
+
 template <typename T>
 int poisson2d_passes(const AeroNs2dPlan *p, const T *f, T *psi, unsigned char *ws, cudaStream_t s,
-                     const aero::TransformParams<T> *fuse = nullptr) {
+                     const aero::TransformParams<T> *fuse = nullptr, Recorder *rec = nullptr) {
   const AeroNs2dConfig &c = p->cfg;
   const int axes[3] = {0, 2, 0}, modes[3] = {0, 2, 1};
   for (int q = 0; q < 3; ++q) {
@@ -954,6 +1220,13 @@ int poisson2d_passes(const AeroNs2dPlan *p, const T *f, T *psi, unsigned char *w
     const AxisInfo &x = p->ax[axes[q] == 0 ? 0 : 1];
     P.L = x.L;
     P.A = aero_host::axis_view<T>(x, ws);
+    if (rec) {
+      if constexpr (std::is_same<T, float>::value) {
+        const int rc = record_transform(rec, P);
+        if (rc) return rc;
+      }
+      continue;
+    }
     AERO_CUDA_TRY(aero::launch_transform<T>(P, s));
   }
   return AERO_OK;
@@ -966,10 +1239,13 @@ int init2d_impl(const AeroNs2dPlan *p, unsigned char *ws, cudaStream_t s) {
   return AERO_OK;
 }
 
+// One step of the plan, launched on s; with rec (FP32 plans of the batched sweep: no LES,
+// heat transfer or dye, the CFL time step) the launches are recorded instead of made.
 template <typename T>
 int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGeom *g, const void *dt_in,
-                unsigned char *ws, cudaStream_t s) {
+                unsigned char *ws, cudaStream_t s, Recorder *rec = nullptr) {
   using namespace aero::ns2d;
+  namespace sw = aero::ns2d::sweep;
   const AeroNs2dConfig &c = p->cfg;
   const int nx = c.nx, ny = c.ny;
   const T *u0 = static_cast<const T *>(f->u0), *v0 = static_cast<const T *>(f->v0);
@@ -1020,13 +1296,30 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
   S.eta = T(c.eta);
   S.nbody = has_win ? c.nbody : 0;
   const dim3 grid(p->gx, p->gy), block(TX, TY);
+  if (rec && (!std::is_same<T, float>::value || les || thermal || c.dye || dt_mode != 0))
+    return set_error(AERO_EUNSUPPORTED, "the persistent sweep runs FP32 plans without LES, heat transfer or dye, "
+                                        "with the CFL time step");
   if (dt_mode == 0) {
-    AERO_CUDA_TRY(cudaMemsetAsync(sc, 0, 8 * sizeof(double), s));
     aero::MaxJobs<T> J{};
     J.job[0] = {u0, p->nu, bits + aero::SC_MAXU};
     J.job[1] = {v0, p->nv, bits + aero::SC_MAXV};
     if (thermal) J.job[2] = {static_cast<const T *>(f->theta0), p->nc, bits + aero::SC_MAXT};
-    AERO_CUDA_TRY(aero::launch_absmax_multi<T>(J, thermal ? 3 : 2, s));
+    if (rec) {
+      if constexpr (std::is_same<T, float>::value) {
+        Op z = new_op(sw::ZERO, 1, 1);
+        z.a.zero = {sc, 8};
+        rec->ops.push_back(z);
+        const long long nmax = (long long)std::max(p->nu, p->nv);
+        Op m = new_op(sw::MAXABS, (nmax + sw::MAX_CHUNK - 1) / sw::MAX_CHUNK, 2);
+        m.a.mx.J = J;
+        m.a.mx.njobs = 2;
+        m.a.mx.chunk = sw::MAX_CHUNK;
+        rec->ops.push_back(m);
+      }
+    } else {
+      AERO_CUDA_TRY(cudaMemsetAsync(sc, 0, 8 * sizeof(double), s));
+      AERO_CUDA_TRY(aero::launch_absmax_multi<T>(J, thermal ? 3 : 2, s));
+    }
     if (les) {
       StageParams<T> N = S;
       N.up = u0;
@@ -1120,11 +1413,19 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
       // the previous theta stage reads this stage's outputs of the last one (nu_t, face velocities)
       if (st > 0) AERO_CUDA_TRY(cudaStreamWaitEvent(s, p->ev_join[st - 1], 0));
     }
-    if (thermal)
-      (void)aero::launch_k(stage2d_kernel<T, false, true>, grid, block, 0, s, P);
-    else
-      (void)aero::launch_k(stage2d_kernel<T, false, false>, grid, block, 0, s, P);
-    AERO_CUDA_TRY(cudaGetLastError());
+    if (rec) {
+      if constexpr (std::is_same<T, float>::value) {
+        Op o = new_op(sw::STAGE, p->gx, p->gy);
+        o.a.st = P;
+        rec->ops.push_back(o);
+      }
+    } else {
+      if (thermal)
+        (void)aero::launch_k(stage2d_kernel<T, false, true>, grid, block, 0, s, P);
+      else
+        (void)aero::launch_k(stage2d_kernel<T, false, false>, grid, block, 0, s, P);
+      AERO_CUDA_TRY(cudaGetLastError());
+    }
     if (thermal) {  // theta of this stage on the side stream, beside the pressure solve
       ThetaParams<T> Q = TP;
       Q.thp = th_in;
@@ -1152,8 +1453,19 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
       F.wgt = T(RK[st][2]);
       F.acc_mode = acc_mode;
       F.dt = small;
-      const int rc = poisson2d_passes<T>(p, nullptr, pa, ws, s, &F);
+      const int rc = poisson2d_passes<T>(p, nullptr, pa, ws, s, &F, rec);
       if (rc) return rc;
+    } else if (rec) {
+      if constexpr (std::is_same<T, float>::value) {
+        Op d = new_op(sw::DIV, (nx + sw::NTHR - 1) / sw::NTHR, ny);
+        d.a.dv = {nx, ny, T(1.0 / c.h), ub[st % 2], vb[st % 2], pa};
+        rec->ops.push_back(d);
+        const int rc = poisson2d_passes<T>(p, pa, pa, ws, s, nullptr, rec);
+        if (rc) return rc;
+        Op a = new_op(sw::PSIACC, ((long long)p->nc + sw::NTHR - 1) / sw::NTHR, 1);
+        a.a.pa = {pa, p_out, (long long)p->nc, T(RK[st][2]), acc_mode, small};
+        rec->ops.push_back(a);
+      }
     } else {
       (void)aero::launch_k(divergence2d_kernel<T>, dim3((nx + 127) / 128, ny), 128, 0, s, nx, ny, T(1.0 / c.h),
                            ub[st % 2], vb[st % 2], pa);
@@ -1162,7 +1474,14 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
       if (rc) return rc;
       AERO_CUDA_TRY(aero::launch_psi_accumulate<T>(pa, p_out, p->nc, T(RK[st][2]), acc_mode, small, s));
     }
-    if (st == 2) {
+    if (st == 2 && rec) {
+      if constexpr (std::is_same<T, float>::value) {
+        Op o = new_op(sw::CORRECT, (nx + sw::NTHR - 1) / sw::NTHR, ny);
+        o.a.co = {nx, ny, c.periodic, T(1.0 / c.h), ub[st % 2], vb[st % 2], pa, static_cast<T *>(f->u),
+                  static_cast<T *>(f->v)};
+        rec->ops.push_back(o);
+      }
+    } else if (st == 2) {
       (void)aero::launch_k(correct2d_kernel<T>, dim3((nx + 127) / 128, ny), 128, 0, s, nx, ny, c.periodic,
                            T(1.0 / c.h), ub[st % 2], vb[st % 2], pa, static_cast<T *>(f->u), static_cast<T *>(f->v));
       AERO_CUDA_TRY(cudaGetLastError());
@@ -1220,6 +1539,15 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
     D.chi_c = static_cast<const T *>(g->chi_c);
     (void)aero::launch_k(dye2d_kernel<T>, dim3((nx + 127) / 128, ny), 128, 0, s, D);
     AERO_CUDA_TRY(cudaGetLastError());
+  }
+  if (rec) {
+    if constexpr (std::is_same<T, float>::value) {
+      Op o = new_op(sw::FINAL, 1, 1);
+      o.a.fi = {partials, p->nblocks, S.nbody, c.h, c.force_ref, small, static_cast<const T *>(f->t0),
+                static_cast<T *>(f->t), static_cast<T *>(f->dt), static_cast<T *>(f->coeffs)};
+      rec->ops.push_back(o);
+    }
+    return AERO_OK;
   }
   (void)aero::launch_k(finalize2d_kernel<T>, 1, 256, 0, s, partials, p->nblocks, S.nbody, c.h, c.force_ref, small,
                                          static_cast<const T *>(f->t0), static_cast<T *>(f->t),
@@ -1375,6 +1703,220 @@ int aero_ns2d_poisson_solve(const AeroNs2dPlan *plan, const void *f, void *psi, 
   return plan->cfg.dtype == AERO_F64
              ? poisson2d_passes<double>(plan, static_cast<const double *>(f), static_cast<double *>(psi), ws, s)
              : poisson2d_passes<float>(plan, static_cast<const float *>(f), static_cast<float *>(psi), ws, s);
+}
+
+}  // extern "C"
+
+
+// ---------------------------------------------------------------------------------------
+// the batched sweep (C ABI)
+// ---------------------------------------------------------------------------------------
+
+struct AeroNs2dSweep {
+  std::vector<Op> ops;
+  std::vector<int> phase_first, phase_count, op_index;
+  std::vector<long long> phase_items, op_prefix;
+  int nphase = 0, lcap = 2, ctas_per_sm = 1, order = 0, grid = 0;
+  size_t smem = 0;
+  size_t off_ops = 0, off_pf = 0, off_pc = 0, off_oi = 0, off_pi = 0, off_op = 0, total = 0;
+  int spin_limit = 1 << 26, extra = 0;
+};
+
+namespace {
+
+using SweepKernel = void (*)(const aero::ns2d::sweep::Tables);
+
+SweepKernel sweep_kernel(int lcap) {
+  switch (lcap) {
+    case 1: return aero::ns2d::sweep::sweep2d_kernel<1>;
+    case 2: return aero::ns2d::sweep::sweep2d_kernel<2>;
+    default: return aero::ns2d::sweep::sweep2d_kernel<3>;
+  }
+}
+
+size_t op_smem(const Op &o, int lcap) {
+  namespace sw = aero::ns2d::sweep;
+  if (o.kind == sw::POW2) {
+    const int l2 = std::min(aero::fft::tile_log2L(o.n, 4), lcap), L = 1 << l2;
+    const size_t e = sizeof(float);
+    return (size_t)o.n * 2 * e + ((((size_t)o.n * (L + 1) * e) + 15) & ~size_t(15)) + 2 * (size_t)o.n * (L / 2) * 2 * e;
+  }
+  if (o.kind == sw::LINE) return aero::transform_smem_bytes<float>(o.n, o.a.tr.L);
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int aero_ns2d_sweep_create(int32_t n, const AeroNs2dPlan *const *plans, const AeroNs2dFields *fields,
+                           const AeroNs2dGeom *geoms, void *const *workspaces, const AeroSweepTuning *tuning,
+                           AeroNs2dSweep **sweep) {
+  if (!plans || !fields || !geoms || !workspaces || !sweep || n < 1) return set_error(AERO_EINVAL, "null argument");
+  *sweep = nullptr;
+  const int lcap = tuning ? tuning->lcap : 2, cps = tuning ? tuning->ctas_per_sm : 1, order = tuning ? tuning->order : 1;
+  if (lcap < 1 || lcap > 3 || cps < 1 || cps > 4 || order < 0 || order > 1)
+    return set_error(AERO_EINVAL, "tuning: lcap 1..3, ctas_per_sm 1..4, order 0..1");
+  std::vector<std::vector<Op>> per(n);
+  std::vector<long long> size(n);
+  for (int k = 0; k < n; ++k) {
+    if (!plans[k] || !workspaces[k]) return set_error(AERO_EINVAL, "null plan or workspace");
+    if (plans[k]->cfg.dtype != AERO_F32) return set_error(AERO_EUNSUPPORTED, "the persistent sweep runs FP32 plans");
+    Recorder rec;
+    rec.lcap = lcap;
+    const int rc = step2d_impl<float>(plans[k], &fields[k], &geoms[k], nullptr,
+                                      static_cast<unsigned char *>(workspaces[k]), nullptr, &rec);
+    if (rc) return rc;
+    per[k] = std::move(rec.ops);
+    size[k] = (long long)plans[k]->cfg.nx * plans[k]->cfg.ny;
+  }
+  std::vector<int> inst(n);
+  for (int k = 0; k < n; ++k) inst[k] = k;
+  if (order == 1)   // largest instances first: their work items start first in every phase
+    std::stable_sort(inst.begin(), inst.end(), [&](int a, int b) { return size[a] > size[b]; });
+  auto *S = new AeroNs2dSweep();
+  S->lcap = lcap;
+  S->ctas_per_sm = cps;
+  S->order = order;
+  size_t longest = 0;
+  for (auto &v : per) longest = std::max(longest, v.size());
+  S->nphase = (int)longest;
+  for (int ph = 0; ph < S->nphase; ++ph) {
+    S->phase_first.push_back((int)S->op_index.size());
+    long long items = 0;
+    int count = 0;
+    for (int k : inst) {
+      if ((size_t)ph >= per[k].size()) continue;
+      const Op &o = per[k][ph];
+      S->op_index.push_back((int)S->ops.size());
+      S->op_prefix.push_back(items);
+      S->ops.push_back(o);
+      S->smem = std::max(S->smem, op_smem(o, lcap));
+      items += (long long)o.gx * o.gy;
+      ++count;
+    }
+    S->phase_count.push_back(count);
+    S->phase_items.push_back(items);
+  }
+  size_t off = aero_host::ALIGN;   // [0, 256): barrier words and the status word
+  auto take = [&](size_t bytes) {
+    const size_t o = off;
+    off = aero_host::align_up(off + bytes);
+    return o;
+  };
+  S->off_ops = take(S->ops.size() * sizeof(Op));
+  S->off_pf = take(S->phase_first.size() * sizeof(int));
+  S->off_pc = take(S->phase_count.size() * sizeof(int));
+  S->off_oi = take(S->op_index.size() * sizeof(int));
+  S->off_pi = take(S->phase_items.size() * sizeof(long long));
+  S->off_op = take(S->op_prefix.size() * sizeof(long long));
+  S->total = off;
+  // co-resident CTAs: every CTA waits at the grid barriers
+  int dev = 0, nsm = 0, occ = 0;
+  const SweepKernel kern = sweep_kernel(lcap);
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(S->smem, 1));
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, aero::ns2d::sweep::NTHR, S->smem);
+  if (e != cudaSuccess || occ < 1) {
+    delete S;
+    return set_error(AERO_ECUDA, std::string("persistent sweep kernel does not fit an SM: ") +
+                                     (e != cudaSuccess ? cudaGetErrorString(e) : "no resident block"));
+  }
+  S->grid = nsm * std::min(occ, cps);
+  *sweep = S;
+  return AERO_OK;
+}
+
+void aero_ns2d_sweep_destroy(AeroNs2dSweep *sweep) { delete sweep; }
+
+size_t aero_ns2d_sweep_workspace_bytes(const AeroNs2dSweep *sweep) { return sweep ? sweep->total : 0; }
+
+int aero_ns2d_sweep_init(const AeroNs2dSweep *sweep, void *workspace, void *stream) {
+  if (!sweep || !workspace) return set_error(AERO_EINVAL, "null argument");
+  if (reinterpret_cast<uintptr_t>(workspace) % aero_host::ALIGN)
+    return set_error(AERO_EINVAL, "workspace must be 256-byte aligned");
+  auto *ws = static_cast<unsigned char *>(workspace);
+  auto s = static_cast<cudaStream_t>(stream);
+  const AeroNs2dSweep &S = *sweep;
+  AERO_CUDA_TRY(cudaMemsetAsync(ws, 0, aero_host::ALIGN, s));
+  AERO_CUDA_TRY(cudaMemcpyAsync(ws + S.off_ops, S.ops.data(), S.ops.size() * sizeof(Op), cudaMemcpyHostToDevice, s));
+  AERO_CUDA_TRY(cudaMemcpyAsync(ws + S.off_pf, S.phase_first.data(), S.phase_first.size() * sizeof(int),
+                                cudaMemcpyHostToDevice, s));
+  AERO_CUDA_TRY(cudaMemcpyAsync(ws + S.off_pc, S.phase_count.data(), S.phase_count.size() * sizeof(int),
+                                cudaMemcpyHostToDevice, s));
+  AERO_CUDA_TRY(cudaMemcpyAsync(ws + S.off_oi, S.op_index.data(), S.op_index.size() * sizeof(int),
+                                cudaMemcpyHostToDevice, s));
+  AERO_CUDA_TRY(cudaMemcpyAsync(ws + S.off_pi, S.phase_items.data(), S.phase_items.size() * sizeof(long long),
+                                cudaMemcpyHostToDevice, s));
+  AERO_CUDA_TRY(cudaMemcpyAsync(ws + S.off_op, S.op_prefix.data(), S.op_prefix.size() * sizeof(long long),
+                                cudaMemcpyHostToDevice, s));
+  AERO_CUDA_TRY(cudaStreamSynchronize(s));   // the host tables are pageable: finish before returning
+  return AERO_OK;
+}
+
+int aero_ns2d_sweep_step(const AeroNs2dSweep *sweep, void *workspace, void *stream) {
+  if (!sweep || !workspace) return set_error(AERO_EINVAL, "null argument");
+  namespace sw = aero::ns2d::sweep;
+  auto *ws = static_cast<unsigned char *>(workspace);
+  auto s = static_cast<cudaStream_t>(stream);
+  const AeroNs2dSweep &S = *sweep;
+  sw::Tables T{};
+  T.ops = reinterpret_cast<const Op *>(ws + S.off_ops);
+  T.phase_first = reinterpret_cast<const int *>(ws + S.off_pf);
+  T.phase_count = reinterpret_cast<const int *>(ws + S.off_pc);
+  T.op_index = reinterpret_cast<const int *>(ws + S.off_oi);
+  T.phase_items = reinterpret_cast<const long long *>(ws + S.off_pi);
+  T.op_prefix = reinterpret_cast<const long long *>(ws + S.off_op);
+  T.nphase = S.nphase;
+  T.bar = reinterpret_cast<unsigned int *>(ws);
+  T.status = reinterpret_cast<int *>(ws + 16);
+  T.spin_limit = S.spin_limit;
+  T.extra = S.extra;
+  AERO_CUDA_TRY(cudaMemsetAsync(ws, 0, 2 * sizeof(unsigned int), s));   // barrier arrivals and generation
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(S.grid);
+  cfg.blockDim = dim3(sw::NTHR);
+  cfg.dynamicSmemBytes = S.smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;   // all CTAs resident together (they meet at barriers)
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  AERO_CUDA_TRY(cudaLaunchKernelEx(&cfg, sweep_kernel(S.lcap), T));
+  return AERO_OK;
+}
+
+int aero_ns2d_sweep_read_status(const AeroNs2dSweep *sweep, void *workspace, int32_t *status, void *stream) {
+  if (!sweep || !workspace || !status) return set_error(AERO_EINVAL, "null argument");
+  auto s = static_cast<cudaStream_t>(stream);
+  AERO_CUDA_TRY(cudaMemcpyAsync(status, static_cast<unsigned char *>(workspace) + 16, sizeof(int32_t),
+                                cudaMemcpyDeviceToHost, s));
+  AERO_CUDA_TRY(cudaStreamSynchronize(s));
+  AERO_CUDA_TRY(cudaMemsetAsync(static_cast<unsigned char *>(workspace) + 16, 0, sizeof(int32_t), s));
+  return AERO_OK;
+}
+
+int aero_ns2d_sweep_set_barrier(AeroNs2dSweep *sweep, int32_t spin_limit, int32_t extra) {
+  if (!sweep || spin_limit < 1 || extra < 0) return set_error(AERO_EINVAL, "bad barrier settings");
+  sweep->spin_limit = spin_limit;
+  sweep->extra = extra;
+  return AERO_OK;
+}
+
+int aero_ns2d_sweep_info(const AeroNs2dSweep *sweep, int64_t out[6]) {
+  if (!sweep || !out) return set_error(AERO_EINVAL, "null argument");
+  long long items = 0;
+  for (long long x : sweep->phase_items) items += x;
+  out[0] = sweep->nphase;
+  out[1] = (int64_t)sweep->ops.size();
+  out[2] = items;
+  out[3] = sweep->grid;
+  out[4] = (int64_t)sweep->smem;
+  out[5] = sweep->lcap;
+  return AERO_OK;
 }
 
 }  // extern "C"

@@ -190,7 +190,7 @@ class ClosureModel:
         n = grad9.shape[1]
         nu = nu_wale.clone()
         mx = torch.zeros(1, device=self.device, dtype=torch.float64)
-        counts = torch.zeros(2, device=self.device, dtype=torch.int32)
+        counts = torch.zeros(2, device=self.device, dtype=torch.int64)
         status = torch.zeros(1, device=self.device, dtype=torch.int32)
         m = self.cstruct()
         check(_lib.lib().aero_closure_eddy_viscosity(C.byref(m), _p(grad9.contiguous()), n, float(delta), _p(nu),

@@ -480,7 +480,7 @@ class Ns3dPlan:
     def closure_counts(self):
         """(cells evaluated, cells that kept WALE) of the closure passes since the workspace was
         initialised (synchronises)."""
-        out = (C.c_uint32 * 2)()
+        out = (C.c_uint64 * 2)()
         check(_lib.lib().aero_ns3d_closure_counts(self._handle, C.c_void_p(self.ws_ptr), out, self._stream()),
               "aero_ns3d_closure_counts")
         return int(out[0]), int(out[1])

@@ -32,6 +32,8 @@
  *                              _report), with the dye update of its lines 959-962
  *                              (core.py:703 advect_dye, core.py:779 _zero_dye_in_solids)
  *   aero_ns2d_poisson_solve    ns2d/poisson.py:126 PoissonSolver.solve
+ *   aero_ns2d_sweep_*          (no counterpart: many 2D instances in one persistent launch; the
+ *                              reference loops ns2d/solver.py:489 advance over them)
  *   aero_closure_*, aero_mlp_* (no counterpart: the learned subgrid closure, which stands in
  *                              for ns3d/core.py:448 eddy_viscosity3d (WALE) where it applies)
  */
@@ -418,13 +420,13 @@ int aero_mlp_train_step(float *params, void *params_bf16, float *adam_m, float *
 /* The closure's eddy-viscosity pass on n cells: grad9 (9, n) holds each cell's gradient (g11,
  * g12, g13, g21, g22, g23, g31, g32) and window factor (1 - chi_c); nu (n) holds the WALE nu_t on
  * entry and the closure's nu_t where it applies on return.  nut_max (device, NULL to skip)
- * receives the maximum as the ordered bits of a double; counts (device, 2, NULL to skip) adds
+ * receives the maximum as the ordered bits of a double; counts (device, 2 x uint64, NULL to skip) adds
  * the cells evaluated and the cells that kept WALE.  delta: the grid spacing. */
 int aero_closure_eddy_viscosity(const AeroClosureModel *m, const float *grad9, int64_t n, double delta, float *nu,
-                                unsigned long long *nut_max, uint32_t *counts, int32_t *status, void *stream);
+                                unsigned long long *nut_max, uint64_t *counts, int32_t *status, void *stream);
 /* Cells the last closure step evaluated and cells that kept WALE, summed over its eddy-viscosity
  * passes since the workspace was initialised (reads through a host copy: synchronises). */
-int aero_ns3d_closure_counts(const AeroNs3dPlan *plan, const void *workspace, uint32_t out[2], void *stream);
+int aero_ns3d_closure_counts(const AeroNs3dPlan *plan, const void *workspace, uint64_t out[2], void *stream);
 
 /* Device-side status word of the last step on this workspace (0 = fine; bit 0: a
  * non-finite value reached a reduction; bit 1: a plane load timed out; bit 2: a tensor-core
@@ -524,6 +526,40 @@ int aero_ns2d_step(const AeroNs2dPlan *plan, const AeroNs2dFields *f, const Aero
 
 /* psi with L psi = f, zero mean ((ny, nx) device arrays; may alias). */
 int aero_ns2d_poisson_solve(const AeroNs2dPlan *plan, const void *f, void *psi, void *workspace, void *stream);
+
+/* ---- the batched sweep: many 2D instances in one persistent launch ---------------------
+ * No counterpart in the reference, which steps its solver once per instance (ns2d/solver.py:489
+ * advance, core.py:815 step_full each).  A sweep records the step of each instance (plan,
+ * fields, geometry, workspace: the arguments of aero_ns2d_step, bound at creation, like a
+ * captured graph) as its sequence of operations, and aero_ns2d_sweep_step runs operation p of
+ * every instance as phase p of one persistent cooperative kernel: the CTAs (co-resident, as
+ * many per SM as the tuning asks and the kernel allows) take the work items of all instances'
+ * operations, a grid barrier between phases.  Every instance's result is bit-identical to its
+ * own aero_ns2d_step.  FP32 plans without LES, heat transfer or dye, with the CFL time step,
+ * transform lengths of at least 64.  Tuning: lcap the log2 of the widest power-of-two transform
+ * tile (1..3), ctas_per_sm (1..4), order 0 (the instances' order) or 1 (largest first). */
+typedef struct AeroNs2dSweep AeroNs2dSweep;
+typedef struct {
+  int32_t lcap, ctas_per_sm, order;
+} AeroSweepTuning;
+int aero_ns2d_sweep_create(int32_t n, const AeroNs2dPlan *const *plans, const AeroNs2dFields *fields,
+                           const AeroNs2dGeom *geoms, void *const *workspaces, const AeroSweepTuning *tuning,
+                           AeroNs2dSweep **sweep);
+void aero_ns2d_sweep_destroy(AeroNs2dSweep *sweep);
+/* Device bytes of the sweep's operation tables (256-byte aligned workspace). */
+size_t aero_ns2d_sweep_workspace_bytes(const AeroNs2dSweep *sweep);
+/* Upload the tables into the workspace (synchronises the stream once). */
+int aero_ns2d_sweep_init(const AeroNs2dSweep *sweep, void *workspace, void *stream);
+/* One step of every instance: one persistent launch (capturable in a CUDA graph). */
+int aero_ns2d_sweep_step(const AeroNs2dSweep *sweep, void *workspace, void *stream);
+/* Status word since the last read (bit 0: a grid barrier ran out; the launch then stopped);
+ * synchronises, then clears it. */
+int aero_ns2d_sweep_read_status(const AeroNs2dSweep *sweep, void *workspace, int32_t *status, void *stream);
+/* The barrier's bound (polls before giving up) and, for tests of that bound, extra arrivals to
+ * wait for that never come (0 in use). */
+int aero_ns2d_sweep_set_barrier(AeroNs2dSweep *sweep, int32_t spin_limit, int32_t extra);
+/* [phases, operations, work items per step, CTAs, dynamic shared bytes, lcap] */
+int aero_ns2d_sweep_info(const AeroNs2dSweep *sweep, int64_t out[6]);
 
 #ifdef __cplusplus
 }

@@ -127,5 +127,10 @@ def eddy_viscosity(y, g8, fac, nu_wale, delta, out_mean, out_std, in_lo, in_hi, 
             + 2.0 * ((tau[:, 3] * S[:, 0, 1] + tau[:, 4] * S[:, 0, 2]) + tau[:, 5] * S[:, 1, 2]))
     s2 = (S * S).sum((1, 2))
     used = inside & (eps > 0)
-    nu = np.where(used, np.asarray(fac) * eps / (2.0 * np.where(used, s2, 1.0)), np.asarray(nu_wale, np.float64))
-    return nu, used
+    safe = 2.0 * np.where(used, s2, 1.0)
+    nu = np.where(used, np.asarray(fac) * eps / safe, np.asarray(nu_wale, np.float64))
+    # the size of the dissipation's terms, sum |tau_ij S_ij|, as an eddy viscosity: the scale of
+    # the rounding error of nu (eps is a sum of terms of either sign)
+    terms = (np.abs(tau[:, 0] * S[:, 0, 0]) + np.abs(tau[:, 1] * S[:, 1, 1]) + np.abs(tau[:, 2] * S[:, 2, 2])
+             + 2.0 * (np.abs(tau[:, 3] * S[:, 0, 1]) + np.abs(tau[:, 4] * S[:, 0, 2]) + np.abs(tau[:, 5] * S[:, 1, 2])))
+    return nu, used, np.asarray(fac) * terms / safe

@@ -145,16 +145,19 @@ def test_closure_eddy_viscosity_matches_oracle():
     f, _, ok, _ = OC.features(g8.astype(np.float32).astype(np.float64), 0.05)
     x = np.where(ok[:, None], (f - m.in_mean) / m.in_std, 0.0)
     y = OC.mlp(m.params.cpu().numpy(), x, _layout())
-    ref, used = OC.eddy_viscosity(y, g8.astype(np.float32), fac.astype(np.float32), nu_wale.cpu().numpy(), 0.05,
-                                  m.out_mean, m.out_std, m.in_lo, m.in_hi)
+    ref, used, scale = OC.eddy_viscosity(y, g8.astype(np.float32), fac.astype(np.float32), nu_wale.cpu().numpy(),
+                                         0.05, m.out_mean, m.out_std, m.in_lo, m.in_hi)
     got = nu.cpu().numpy()
     kept = got == nu_wale.cpu().numpy()
     agree = (kept == ~used).mean()
     assert agree > 0.995, agree                            # borderline dissipation signs may flip
     both = used & ~kept
     assert both.sum() > 0.2 * n and (~used).sum() > 0.05 * n
-    rel = np.abs(got[both] - ref[both]) / np.abs(ref[both])
+    # BF16 operands: nu within a few per cent of the scale of the dissipation's terms (the
+    # dissipation itself can be a small difference of them), and of nu itself at the median
+    rel = np.abs(got[both] - ref[both]) / scale[both]
     assert np.quantile(rel, 0.99) < 5e-2, np.quantile(rel, 0.99)
+    assert np.median(np.abs(got[both] - ref[both]) / np.abs(ref[both])) < 1e-2
     assert counts[0] == n and abs(counts[1] - int(kept.sum())) <= 0
     assert abs(mx - got.max()) <= 1e-6 * got.max()
 

@@ -197,23 +197,59 @@ def test_sweep_grid_step_matches_oracle(grid):
     assert np.abs(got - r.coeffs).max() <= 1e-4 * max(1.0, np.abs(r.coeffs).max()), (got, r.coeffs)
 
 
-def test_sweep_streams_equal_the_per_instance_loop():
-    """The batched sweep (64 seeded NACA instances, 16 streams, captured in one CUDA graph)
-    gives every instance exactly what its own plan gives when the instances are stepped one
-    after another: fields and coefficients bit for bit after five steps."""
+def _run(sw, snap, schedule, steps, graph):
+    sw.restore(snap)
+    if graph:
+        g = sw.capture(steps, schedule)
+        g.replay()
+    else:
+        for _ in range(steps):
+            sw.step(schedule)
+    torch.cuda.synchronize()
+    return [(s["u"].clone(), s["v"].clone(), s["t"].clone(), s["out"]["coeffs"].clone()) for s in sw.states]
+
+
+def test_sweep_schedules_equal_the_per_instance_loop():
+    """The batched sweep (64 seeded NACA instances on five grid sizes) as one persistent launch
+    per step (its launch shape picked by the autotuner, captured in one CUDA graph) and spread
+    over 16 streams give every instance exactly what its own plan gives when the instances are
+    stepped one after another: fields, time and coefficients bit for bit after five steps."""
     from aerolume_b200.ns2d.sweep import Sweep2D
     from aerolume_b200.ns2d.workloads import sweep_instances
     sw = Sweep2D(sweep_instances(64, seed=0))
     snap = sw.snapshot()
-    g = sw.capture(5, "streams")
-    g.replay()
-    torch.cuda.synchronize()
-    got = [(s["u"].clone(), s["v"].clone(), s["t"].clone(), s["out"]["coeffs"].clone()) for s in sw.states]
-    sw.restore(snap)
-    for _ in range(5):
-        sw.step("loop")
-    torch.cuda.synchronize()
-    for k, (s, (u, v, t, c)) in enumerate(zip(sw.states, got)):
-        assert torch.equal(s["u"], u) and torch.equal(s["v"], v), k
-        assert torch.equal(s["t"], t) and torch.equal(s["out"]["coeffs"], c), k
+    table = sw.tune(candidates=[(1, 2, 1), (2, 2, 1), (3, 1, 0)], steps=2)
+    assert sw.tuning is not None and any(r[1] is not None for r in table)
+    ref = _run(sw, snap, "loop", 5, graph=False)
+    for schedule, graph in (("persistent", True), ("persistent", False), ("streams", True)):
+        got = _run(sw, snap, schedule, 5, graph)
+        for k, (a, b) in enumerate(zip(got, ref)):
+            for x, y in zip(a, b):
+                assert torch.equal(x, y), (schedule, graph, k)
+        if schedule == "persistent":
+            assert sw.status() == 0
     assert all(float(s["t"]) > 0 for s in sw.states)
+
+
+def test_sweep_barrier_gives_up_and_reports():
+    """The persistent launch's grid barrier waits for arrivals that never come (the test hook
+    asks for one CTA more than the launch has): every CTA gives up after the bounded wait, the
+    status word reports it, and the next launch with the barrier restored runs normally and
+    matches the per-instance loop."""
+    from aerolume_b200.ns2d.sweep import Sweep2D
+    from aerolume_b200.ns2d.workloads import sweep_instances
+    insts = [i for i in sweep_instances(64, seed=0) if i[0].nx == 256][:2]
+    sw = Sweep2D(insts)
+    snap = sw.snapshot()
+    sw.use_persistent(2, 1, 1)
+    sw.set_barrier(2000, extra=1)
+    sw.step("persistent")
+    torch.cuda.synchronize()
+    assert sw.status() & 1
+    sw.set_barrier(1 << 26, extra=0)
+    got = _run(sw, snap, "persistent", 3, graph=False)
+    assert sw.status() == 0
+    ref = _run(sw, snap, "loop", 3, graph=False)
+    for a, b in zip(got, ref):
+        for x, y in zip(a, b):
+            assert torch.equal(x, y)
