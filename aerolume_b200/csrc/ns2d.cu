@@ -1037,8 +1037,10 @@ __device__ __forceinline__ void run_pow2(const TransformParams<float> &P, int n,
   }
 }
 
-template <int LCAP>
-__global__ void __launch_bounds__(NTHR, 2) sweep2d_kernel(const __grid_constant__ Tables T) {
+// MINB: CTAs per SM the register allocation is capped for (2: up to 128 registers, no spills;
+// 3: up to 80, a few spills); the autotuner measures both.
+template <int LCAP, int MINB>
+__global__ void __launch_bounds__(NTHR, MINB) sweep2d_kernel(const __grid_constant__ Tables T) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int tid = threadIdx.x;
   for (int ph = 0; ph < T.nphase; ++ph) {
@@ -1066,7 +1068,12 @@ __global__ void __launch_bounds__(NTHR, 2) sweep2d_kernel(const __grid_constant_
             const float v = fabsf(__ldg(q.a + e));
             m = (v > m || v != v) ? v : m;
           }
-          block_max_atomic<float>(m, q.out);
+          // block maximum (NaN wins), one atomic on the ordered bits of the double
+          for (int o = 16; o > 0; o >>= 1) {
+            const float other = __shfl_xor_sync(0xffffffffu, m, o);
+            m = (other > m || other != other) ? other : m;
+          }
+          if ((tid & 31) == 0) atomic_max_nonneg(q.out, (double)m);
           break;
         }
         case STAGE: stage2d_body<float, false, false, false>(op.a.st, bx, by, op.gx, tid); break;
@@ -1726,11 +1733,20 @@ namespace {
 
 using SweepKernel = void (*)(const aero::ns2d::sweep::Tables);
 
-SweepKernel sweep_kernel(int lcap) {
+// the kernel of a tuning: widest transform tile 2^lcap, registers capped for 2 or for 3 CTAs per SM
+SweepKernel sweep_kernel(int lcap, int cps) {
+  namespace sw = aero::ns2d::sweep;
+  if (cps >= 3) {
+    switch (lcap) {
+      case 1: return sw::sweep2d_kernel<1, 3>;
+      case 2: return sw::sweep2d_kernel<2, 3>;
+      default: return sw::sweep2d_kernel<3, 3>;
+    }
+  }
   switch (lcap) {
-    case 1: return aero::ns2d::sweep::sweep2d_kernel<1>;
-    case 2: return aero::ns2d::sweep::sweep2d_kernel<2>;
-    default: return aero::ns2d::sweep::sweep2d_kernel<3>;
+    case 1: return sw::sweep2d_kernel<1, 2>;
+    case 2: return sw::sweep2d_kernel<2, 2>;
+    default: return sw::sweep2d_kernel<3, 2>;
   }
 }
 
@@ -1755,8 +1771,8 @@ int aero_ns2d_sweep_create(int32_t n, const AeroNs2dPlan *const *plans, const Ae
   if (!plans || !fields || !geoms || !workspaces || !sweep || n < 1) return set_error(AERO_EINVAL, "null argument");
   *sweep = nullptr;
   const int lcap = tuning ? tuning->lcap : 2, cps = tuning ? tuning->ctas_per_sm : 1, order = tuning ? tuning->order : 1;
-  if (lcap < 1 || lcap > 3 || cps < 1 || cps > 4 || order < 0 || order > 1)
-    return set_error(AERO_EINVAL, "tuning: lcap 1..3, ctas_per_sm 1..4, order 0..1");
+  if (lcap < 1 || lcap > 3 || cps < 1 || cps > 3 || order < 0 || order > 1)
+    return set_error(AERO_EINVAL, "tuning: lcap 1..3, ctas_per_sm 1..3, order 0..1");
   std::vector<std::vector<Op>> per(n);
   std::vector<long long> size(n);
   for (int k = 0; k < n; ++k) {
@@ -1813,7 +1829,7 @@ int aero_ns2d_sweep_create(int32_t n, const AeroNs2dPlan *const *plans, const Ae
   S->total = off;
   // co-resident CTAs: every CTA waits at the grid barriers
   int dev = 0, nsm = 0, occ = 0;
-  const SweepKernel kern = sweep_kernel(lcap);
+  const SweepKernel kern = sweep_kernel(lcap, cps);
   cudaError_t e = cudaGetDevice(&dev);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   if (e == cudaSuccess)
@@ -1885,7 +1901,7 @@ int aero_ns2d_sweep_step(const AeroNs2dSweep *sweep, void *workspace, void *stre
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  AERO_CUDA_TRY(cudaLaunchKernelEx(&cfg, sweep_kernel(S.lcap), T));
+  AERO_CUDA_TRY(cudaLaunchKernelEx(&cfg, sweep_kernel(S.lcap, S.ctas_per_sm), T));
   return AERO_OK;
 }
 

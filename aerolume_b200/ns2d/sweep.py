@@ -76,7 +76,7 @@ class Sweep2D:
             f.coeffs = out["coeffs"].data_ptr()
         return f
 
-    def build_persistent(self, lcap=2, ctas_per_sm=2, order=1):
+    def build_persistent(self, lcap=2, ctas_per_sm=3, order=1):
         """The persistent launch of the current instances with these launch choices."""
         L = _lib.lib()
         n = len(self.plans)
@@ -97,7 +97,7 @@ class Sweep2D:
         return {"handle": handle, "raw": raw, "ptr": ptr, "tuning": (int(lcap), int(ctas_per_sm), int(order)),
                 "info": dict(zip(("phases", "operations", "items", "ctas", "smem", "lcap"), list(info)))}
 
-    def use_persistent(self, lcap=2, ctas_per_sm=2, order=1):
+    def use_persistent(self, lcap=2, ctas_per_sm=3, order=1):
         self._release()
         self._persistent = self.build_persistent(lcap, ctas_per_sm, order)
         self.tuning = self._persistent["tuning"]
@@ -185,7 +185,7 @@ class Sweep2D:
         sweep steps (CUDA events, after ``warmup``), keep the fastest, and put every instance's
         state back as it was.  Returns the table of (candidate, ms per step)."""
         if candidates is None:
-            candidates = list(itertools.product((1, 2, 3), (1, 2), (0, 1)))
+            candidates = list(itertools.product((1, 2, 3), (2, 3), (0, 1)))
         snap = self.snapshot()
         table = []
         for cand in candidates:

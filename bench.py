@@ -76,6 +76,113 @@ def _peaks():
     return 6650.0, "fallback"
 
 
+def _tensor_peak():
+    """(bf16 dense TFLOP/s burst, kind): MEASURED_PEAKS.json's cuBLAS figure, else the fallback."""
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        if "bf16_tflops" in d:
+            return float(d["bf16_tflops"]), "measured"
+    return 1590.0, "fallback"
+
+
+def run_closure(args, rank, world, local_rank):
+    """The learned-closure step (the box case with the closure's eddy viscosity in place of WALE
+    where it applies), K steps in one graph; and its dominant kernel, the closure's pass over the
+    padded grid, timed alone against the tensor-core peak."""
+    import ctypes as C
+
+    import torch
+    from aerolume_b200 import _lib
+    from aerolume_b200.ns3d.closure import ClosureModel
+    from aerolume_b200.ns3d.plan import Ns3dPlan
+    from aerolume_b200.ns3d.workloads import box_on_moving_floor, initial_state
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    nx, ny, nz = args.shape
+    cells = nx * ny * nz
+    ops, geom, th, src, _ = box_on_moving_floor(nx, ny, nz, dtype="float32", seed=0)
+    model = ClosureModel(device=dev, seed=0)
+    model.out_std[:] = 0.02      # an untrained network: outputs of the subgrid stress's size
+    plan = Ns3dPlan(ops, geom, th, src, smoke=True, device=dev, closure=model)
+    u, v, w = initial_state(ops, seed=rank, device=dev)
+    plan.project(u, v, w)
+    theta = torch.zeros(nz, ny, nx, device=dev)
+    dyes = [torch.zeros(nz, ny, nx, device=dev), torch.zeros(nz, ny, nx, device=dev)]
+    t = torch.zeros((), device=dev)
+    out = plan.empty_fields()
+    out["u"], out["v"], out["w"], out["theta"] = u, v, w, theta
+
+    def step(j):
+        out["dye"] = dyes[(j + 1) % 2]
+        plan.step(u, v, w, t, theta0=theta, dye0=dyes[j % 2], out=out)
+        t.copy_(out["t"])
+
+    for j in range(args.warmup):
+        step(j)
+    torch.cuda.synchronize()
+    K = args.steps
+    s = torch.cuda.Stream(device=dev)
+    s.wait_stream(torch.cuda.current_stream(dev))
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(s):
+        with torch.cuda.graph(g, stream=s):
+            for j in range(K):
+                step(args.warmup + j)
+    torch.cuda.current_stream(dev).wait_stream(s)
+    ms, clk = _time_graph(g, dist, local_rank, rank, dev)
+    ev, wale = plan.closure_counts()
+    status = plan.status()
+    # the closure's pass alone on the padded grid's worth of cells (seeded gradients)
+    n = (nz + 2) * (ny + 2) * (nx + 2)
+    gen = torch.Generator(device=dev).manual_seed(1)
+    grad9 = torch.randn(9, n, device=dev, generator=gen)
+    grad9[8] = 1.0
+    nu0 = torch.zeros(n, device=dev)
+    nu = torch.empty_like(nu0)
+    st = torch.zeros(1, device=dev, dtype=torch.int32)
+    m = model.cstruct()
+    L = _lib.lib()
+    stream = C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    reps = 10
+
+    def one():
+        _lib.check(L.aero_closure_eddy_viscosity(C.byref(m), C.c_void_p(grad9.data_ptr()), n, float(ops.h),
+                                                 C.c_void_p(nu.data_ptr()), None, None, C.c_void_p(st.data_ptr()),
+                                                 stream), "aero_closure_eddy_viscosity")
+
+    for _ in range(3):
+        one()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(reps):
+        one()
+    b.record()
+    torch.cuda.synchronize()
+    pass_ms = a.elapsed_time(b) / reps
+    if rank != 0:
+        return
+    peak, peak_kind = _tensor_peak()
+    flops = 2.0 * 36864 * n          # padded 16 -> 128 -> 128 -> 128 -> 16 layers, 2 FLOP per MAC
+    line = {"metric": METRIC, "value": world * cells * K / (ms * 1e-3) / 1e6, "unit": UNIT, "n_gpus": world, "steps": K,
+            "warmup": args.warmup, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 step, bf16 MLP (fp32 accumulate)", "data": "synthetic",
+            "config": _config(nx, ny, nz, {"plain_variant": "learned closure (WALE fallback per cell)",
+                                           "graph": f"{K} steps, 1 replay",
+                                           "network": "untrained (seeded) weights: the cost does not depend on them"}),
+            "closure_cells_evaluated": ev, "closure_wale_fraction": wale / max(ev, 1),
+            "roofline": {"bound": "tensor", "kernel": "closure_nu_kernel (the closure's pass, timed alone)",
+                         "achieved": flops / (pass_ms * 1e-3) / 1e12, "peak": peak, "peak_kind": peak_kind,
+                         "unit": "TFLOP/s", "frac": flops / (pass_ms * 1e-3) / 1e12 / peak, "traffic": None,
+                         "flops_per_launch": flops, "ms_per_launch": pass_ms, "cells_per_launch": n},
+            "cpu_baseline": None, "e2e": None, "gpu_launches": (launches_per_step(plan) + 3) * K, "clocks": clk,
+            "status": status}
+    print(json.dumps(line), flush=True)
+
+
 def _config(nx, ny, nz, extra=None):
     cfg = {"workload": f"box on moving floor {nx}x{ny}x{nz} FP32, WALE, Boussinesq heat, 1 smoke rake",
            "cells": nx * ny * nz, "grid": [nx, ny, nz], "inputs_vs_l2": "working set ~1 GB > 126 MB L2 (no flush)",
@@ -646,9 +753,13 @@ def run_2d(args, rank, world, local_rank):
 
 
 def run_sweep(args, rank, world, local_rank):
+    """The batched sweep: 64 NACA instances advanced by one persistent launch per step (its launch
+    shape picked by Sweep2D.tune), K steps in one CUDA graph; beside it the same plans spread over
+    16 streams and looped one after another (each in its own graph), and the e2e figure with
+    every instance's state copied in from and its time and coefficients out to host memory."""
     import torch
-    from aerolume_b200.ns2d.plan import Ns2dPlan
-    from aerolume_b200.ns2d.workloads import initial_state, sweep_instances
+    from aerolume_b200.ns2d.sweep import Sweep2D
+    from aerolume_b200.ns2d.workloads import sweep_instances
     dist = None
     if world > 1:
         import torch.distributed as dist
@@ -660,58 +771,53 @@ def run_sweep(args, rank, world, local_rank):
     else:
         mine = list(range(len(all_insts)))
     insts = [all_insts[k] for k in mine]
-    plans, states = [], []
-    for k, (ops, geom, _) in enumerate(insts):
-        plan = Ns2dPlan(ops, geom, device=dev)
-        u, v = initial_state(ops, plan, seed=1000 * rank + k, noise=1e-3)
-        out = plan.empty_fields()
-        out["u"], out["v"] = u, v
-        plans.append(plan)
-        states.append((u, v, torch.zeros((), device=dev), out))
-    cells = sum(o.nx * o.ny for o, _, _ in insts)
-    nstream = 16
-    streams = [torch.cuda.Stream(device=dev) for _ in range(nstream)]
-
-    def one(k):
-        u, v, t, out = states[k]
-        plans[k].step(u, v, t, out=out)
-        t.copy_(out["t"])
-
-    def sweep_step(main):
-        for q in range(nstream):
-            streams[q].wait_stream(main)
-        for k in range(len(plans)):
-            with torch.cuda.stream(streams[k % nstream]):
-                one(k)
-        for q in range(nstream):
-            main.wait_stream(streams[q])
-
-    main = torch.cuda.current_stream(dev)
-    for _ in range(args.warmup):
-        sweep_step(main)
-    torch.cuda.synchronize()
+    sw = Sweep2D(insts, device=dev, seeds=[1000 * rank + k for k in range(len(insts))])
+    cells = sw.cells
+    snap = sw.snapshot()
+    tune_table = sw.tune()
     K = args.steps
-    s = torch.cuda.Stream(device=dev)
-    s.wait_stream(main)
-    g = torch.cuda.CUDAGraph()
-    with torch.cuda.stream(s):
-        with torch.cuda.graph(g, stream=s):
-            for _ in range(K):
-                sweep_step(s)
-    main.wait_stream(s)
+    for _ in range(args.warmup):
+        sw.step("persistent")
+    torch.cuda.synchronize()
+    g = sw.capture(K, "persistent")
     ms, clk = _time_graph(g, dist, local_rank, rank, dev)
-    # the same plans looped one instance after another on one stream
-    gl = torch.cuda.CUDAGraph()
-    s.wait_stream(main)
-    with torch.cuda.stream(s):
-        with torch.cuda.graph(gl, stream=s):
-            for _ in range(K):
-                for k in range(len(plans)):
-                    one(k)
-    main.wait_stream(s)
-    ms_loop, _ = _time_graph(gl, dist, local_rank, rank, dev)
-    # per-instance results (lift and drag after the timed steps) gathered to rank 0
-    coeffs = {mine[k]: [float(x) for x in states[k][3]["coeffs"].reshape(-1)[:2].tolist()] for k in range(len(plans))}
+    status = sw.status()
+    coeffs = {mine[k]: [float(x) for x in sw.states[k]["out"]["coeffs"].reshape(-1)[:2].tolist()]
+              for k in range(len(insts))}
+    del g
+    timings = {}
+    for sched in ("streams", "loop"):
+        sw.restore(snap)
+        for _ in range(args.warmup):
+            sw.step(sched)
+        gs = sw.capture(K, sched)
+        timings[sched], _ = _time_graph(gs, dist, local_rank, rank, dev)
+        del gs
+    # e2e: host state in, host results out, every step, through the sweep's public calls
+    sw.restore(snap)
+    host_in = [(s["u"].cpu().pin_memory(), s["v"].cpu().pin_memory(), s["t"].cpu().pin_memory()) for s in sw.states]
+    host_out = [(torch.empty(s["t"].shape, dtype=s["t"].dtype).pin_memory(),
+                 torch.empty(s["out"]["coeffs"].shape, dtype=s["out"]["coeffs"].dtype).pin_memory())
+                for s in sw.states]
+    h2d = sum(a.numel() * a.element_size() + b.numel() * b.element_size() + c.numel() * c.element_size()
+              for a, b, c in host_in)
+    d2h = sum(a.numel() * a.element_size() + b.numel() * b.element_size() for a, b in host_out)
+    ke = max(3, min(K, 10))
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(ke):
+        for s, (hu, hv, ht) in zip(sw.states, host_in):
+            s["u"].copy_(hu, non_blocking=True)
+            s["v"].copy_(hv, non_blocking=True)
+            s["t"].copy_(ht, non_blocking=True)
+        sw.step("persistent")
+        for s, (ht, hc) in zip(sw.states, host_out):
+            ht.copy_(s["t"], non_blocking=True)
+            hc.copy_(s["out"]["coeffs"], non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    ems = max_over_ranks(e0.elapsed_time(e1) / ke, dist, dev)
     coeffs = gather_results(coeffs, dist)
     total_cells = sum(o.nx * o.ny for o, _, _ in all_insts) if args.shard else world * cells
     if rank != 0:
@@ -728,6 +834,7 @@ def run_sweep(args, rank, world, local_rank):
     grids = {}
     for o, _, _ in insts:
         grids[f"{o.nx}x{o.ny}"] = grids.get(f"{o.nx}x{o.ny}", 0) + 1
+    info = sw._persistent["info"]
     line = {"metric": METRIC, "value": total_cells * K / (ms * 1e-3) / 1e6, "unit": UNIT, "n_gpus": world,
             "steps": K, "warmup": args.warmup, "ms_per_step": ms / K, "higher_is_better": True,
             "scaling": "strong" if args.shard else "weak",
@@ -736,15 +843,28 @@ def run_sweep(args, rank, world, local_rank):
                                    "upwind3, CFL 0.5, no LES", "cells": cells, "grids": grids,
                        "inputs_vs_l2": f"{cells * 4 * 10 / 1e6:.0f} MB of state + workspace > 126 MB L2 (no flush)",
                        "parallelism": "instances sharded over the ranks" if args.shard else "replicas",
-                       "graph": f"{K} sweep steps (64 instances each) over 16 streams, 1 replay"},
+                       "graph": f"{K} sweep steps, each one persistent launch, 1 replay"},
+            "persistent": {"tuning": {"lcap": sw.tuning[0], "ctas_per_sm": sw.tuning[1],
+                                      "order": "largest first" if sw.tuning[2] else "as given"},
+                           "phases": info["phases"], "operations": info["operations"],
+                           "work_items_per_step": info["items"], "ctas": info["ctas"],
+                           "dynamic_smem": info["smem"], "status": status,
+                           "autotuner": [{"lcap": c[0], "ctas_per_sm": c[1], "order": c[2], "ms_per_step": t}
+                                         for c, t, _ in tune_table]},
             "instances": len(coeffs), "instances_per_rank": len(mine) if not args.shard else "size-balanced shard",
-            "looped": {"value": total_cells * K / (ms_loop * 1e-3) / 1e6, "unit": UNIT, "ms_per_step": ms_loop / K,
-                       "how": "the same plans one after another on one stream, one graph"},
-            "roofline": {"bound": "hbm", "kernel": "whole sweep step", "achieved": alg / (ms / K * 1e-3) / 1e9,
-                         "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+            "streams": {"value": total_cells * K / (timings["streams"] * 1e-3) / 1e6, "unit": UNIT,
+                        "ms_per_step": timings["streams"] / K, "how": "each instance's own launches over 16 streams"},
+            "looped": {"value": total_cells * K / (timings["loop"] * 1e-3) / 1e6, "unit": UNIT,
+                       "ms_per_step": timings["loop"] / K,
+                       "how": "the plain per-instance loop: the same plans one after another on one stream"},
+            "speedup_vs_loop": timings["loop"] / ms,
+            "roofline": {"bound": "hbm", "kernel": "sweep2d_kernel (the whole sweep step)",
+                         "achieved": alg / (ms / K * 1e-3) / 1e9, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                          "frac": alg / (ms / K * 1e-3) / 1e9 / peak, "traffic": None, "alg_bytes_per_step": alg},
-            "cpu_baseline": cpu, "e2e": None,
-            "gpu_launches": sum(_launches_2d(p) for p in plans) * K, "clocks": clk}
+            "cpu_baseline": cpu,
+            "e2e": {"value": total_cells / (ems * 1e-3) / 1e6, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h), "ms_per_step": ems, "steps": ke},
+            "gpu_launches": K, "clocks": clk}
     print(json.dumps(line), flush=True)
 
 
@@ -1335,7 +1455,7 @@ def main():
                                                              "10 for sweep2d)")
     ap.add_argument("--workload", default="box3d",
                     choices=["box3d", "placed3d", "cylinder2d", "heated2d", "sweep2d", "fields3d", "masks3d",
-                             "record3d"])
+                             "record3d", "closure3d"])
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--shape", type=int, nargs=3, default=list(SHAPE), help="nx ny nz (2:1:1)")
@@ -1346,12 +1466,12 @@ def main():
     args = ap.parse_args()
     if args.steps is None:
         args.steps = {"box3d": 20, "placed3d": 20, "cylinder2d": 400, "heated2d": 400, "sweep2d": 10,
-                      "fields3d": 20, "masks3d": 10, "record3d": 20}[args.workload]
+                      "fields3d": 20, "masks3d": 10, "record3d": 20, "closure3d": 20}[args.workload]
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
-        if args.workload == "box3d":
+        if args.workload in ("box3d", "closure3d"):   # the reference has no learned closure: its WALE step
             run_reference(args, rank)
         elif args.workload == "fields3d":
             run_reference_fields(args, rank)
@@ -1373,7 +1493,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     try:
         {"box3d": run_ours, "placed3d": run_placed, "cylinder2d": run_2d, "heated2d": run_2d, "sweep2d": run_sweep,
-         "fields3d": run_fields, "masks3d": run_masks, "record3d": run_record}[args.workload](
+         "fields3d": run_fields, "masks3d": run_masks, "record3d": run_record, "closure3d": run_closure}[args.workload](
             args, rank, world, local_rank)
     finally:
         if world > 1:

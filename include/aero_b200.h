@@ -537,7 +537,8 @@ int aero_ns2d_poisson_solve(const AeroNs2dPlan *plan, const void *f, void *psi, 
  * operations, a grid barrier between phases.  Every instance's result is bit-identical to its
  * own aero_ns2d_step.  FP32 plans without LES, heat transfer or dye, with the CFL time step,
  * transform lengths of at least 64.  Tuning: lcap the log2 of the widest power-of-two transform
- * tile (1..3), ctas_per_sm (1..4), order 0 (the instances' order) or 1 (largest first). */
+ * tile (1..3), ctas_per_sm (1..3; 3 compiles the kernel for fewer registers per thread), order 0
+ * (the instances' order) or 1 (largest first). */
 typedef struct AeroNs2dSweep AeroNs2dSweep;
 typedef struct {
   int32_t lcap, ctas_per_sm, order;
