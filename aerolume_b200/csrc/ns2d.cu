@@ -953,7 +953,7 @@ struct FinalArgs {
   float *t_out, *dt_out, *coeffs;
 };
 
-struct Op {
+struct alignas(16) Op {
   int kind, gx, gy, n;   // n: the transform length of POW2
   union Args {
     StageParams<float> st;
@@ -984,6 +984,7 @@ struct Tables {
 };
 
 constexpr int NTHR = 256;
+constexpr int EW = 8;   // elements per thread of an elementwise work item (divergence, psi, correction)
 constexpr long long MAX_CHUNK = 2048;   // elements of one work item of the maxima
 
 // Grid-wide barrier between phases: arrivals counted atomically, the last one bumps the
@@ -1053,7 +1054,16 @@ __global__ void __launch_bounds__(NTHR, MINB) sweep2d_kernel(const __grid_consta
         if (T.op_prefix[f + mid] <= g) lo = mid;
         else hi = mid - 1;
       }
-      const Op &op = T.ops[T.op_index[f + lo]];
+      // the item's operation into shared memory: the bodies then read its parameters from a
+      // space their global stores cannot alias, so they stay in registers instead of being
+      // reloaded after every store (the previous item ended with a block barrier)
+      __shared__ Op op_s;
+      {
+        const uint4 *src = reinterpret_cast<const uint4 *>(T.ops + T.op_index[f + lo]);
+        for (int q = tid; q < (int)(sizeof(Op) / 16); q += NTHR) reinterpret_cast<uint4 *>(&op_s)[q] = src[q];
+      }
+      __syncthreads();
+      const Op &op = op_s;
       const long long b = g - T.op_prefix[f + lo];
       const int bx = (int)(b % op.gx), by = (int)(b / op.gx);
       switch (op.kind) {
@@ -1081,26 +1091,34 @@ __global__ void __launch_bounds__(NTHR, MINB) sweep2d_kernel(const __grid_consta
         case LINE: line_transform_body<float>(op.a.tr, bx, by, smem_raw); break;
         case DIV: {
           const DivArgs &a = op.a.dv;
-          divergence2d_body<float>(a.nx, a.ny, a.inv_h, a.u, a.v, a.div, bx * NTHR + tid, by);
+#pragma unroll
+          for (int k = 0; k < EW; ++k)
+            divergence2d_body<float>(a.nx, a.ny, a.inv_h, a.u, a.v, a.div, (bx * EW + k) * NTHR + tid, by);
           break;
         }
         case PSIACC: {
           const PsiArgs &a = op.a.pa;
           const float rdt = a.mode == 2 ? 1.f / *a.dt : 1.f;
-          const long long e = b * NTHR + tid;
-          if (e < a.n) {
-            if (a.mode == 0) {
-              a.pw[e] = a.psi[e] * a.wgt;
-            } else {
-              const float sum = a.pw[e] + a.wgt * a.psi[e];
-              a.pw[e] = a.mode == 2 ? sum * rdt : sum;
+#pragma unroll
+          for (int k = 0; k < EW; ++k) {
+            const long long e = (b * EW + k) * NTHR + tid;
+            if (e < a.n) {
+              if (a.mode == 0) {
+                a.pw[e] = a.psi[e] * a.wgt;
+              } else {
+                const float sum = a.pw[e] + a.wgt * a.psi[e];
+                a.pw[e] = a.mode == 2 ? sum * rdt : sum;
+              }
             }
           }
           break;
         }
         case CORRECT: {
           const CorrArgs &a = op.a.co;
-          correct2d_body<float>(a.nx, a.ny, a.periodic, a.inv_h, a.uh, a.vh, a.psi, a.u, a.v, bx * NTHR + tid, by);
+#pragma unroll
+          for (int k = 0; k < EW; ++k)
+            correct2d_body<float>(a.nx, a.ny, a.periodic, a.inv_h, a.uh, a.vh, a.psi, a.u, a.v,
+                                  (bx * EW + k) * NTHR + tid, by);
           break;
         }
         default: {
@@ -1464,12 +1482,12 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
       if (rc) return rc;
     } else if (rec) {
       if constexpr (std::is_same<T, float>::value) {
-        Op d = new_op(sw::DIV, (nx + sw::NTHR - 1) / sw::NTHR, ny);
+        Op d = new_op(sw::DIV, (nx + sw::NTHR * sw::EW - 1) / (sw::NTHR * sw::EW), ny);
         d.a.dv = {nx, ny, T(1.0 / c.h), ub[st % 2], vb[st % 2], pa};
         rec->ops.push_back(d);
         const int rc = poisson2d_passes<T>(p, pa, pa, ws, s, nullptr, rec);
         if (rc) return rc;
-        Op a = new_op(sw::PSIACC, ((long long)p->nc + sw::NTHR - 1) / sw::NTHR, 1);
+        Op a = new_op(sw::PSIACC, ((long long)p->nc + sw::NTHR * sw::EW - 1) / (sw::NTHR * sw::EW), 1);
         a.a.pa = {pa, p_out, (long long)p->nc, T(RK[st][2]), acc_mode, small};
         rec->ops.push_back(a);
       }
@@ -1483,7 +1501,7 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
     }
     if (st == 2 && rec) {
       if constexpr (std::is_same<T, float>::value) {
-        Op o = new_op(sw::CORRECT, (nx + sw::NTHR - 1) / sw::NTHR, ny);
+        Op o = new_op(sw::CORRECT, (nx + sw::NTHR * sw::EW - 1) / (sw::NTHR * sw::EW), ny);
         o.a.co = {nx, ny, c.periodic, T(1.0 / c.h), ub[st % 2], vb[st % 2], pa, static_cast<T *>(f->u),
                   static_cast<T *>(f->v)};
         rec->ops.push_back(o);
