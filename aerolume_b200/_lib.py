@@ -45,7 +45,7 @@ EXPORTS = ("aero_abi_version", "aero_last_error", "aero_ns3d_plan_create", "aero
            "aero_closure_eddy_viscosity", "aero_ns3d_closure_counts", "aero_ns2d_sweep_create",
            "aero_ns2d_sweep_destroy", "aero_ns2d_sweep_workspace_bytes", "aero_ns2d_sweep_init",
            "aero_ns2d_sweep_step", "aero_ns2d_sweep_read_status", "aero_ns2d_sweep_set_barrier",
-           "aero_ns2d_sweep_info")
+           "aero_ns2d_sweep_info", "aero_ns3d_set_wait_bound")
 
 CLOSURE_IN, CLOSURE_OUT, CLOSURE_HIDDEN, CLOSURE_NPARAM = 10, 6, 128, 35206
 
@@ -259,6 +259,8 @@ def lib() -> C.CDLL:
     L.aero_ns2d_sweep_step.argtypes = [vp, vp, vp]
     L.aero_ns2d_sweep_read_status.argtypes = [vp, vp, C.POINTER(C.c_int32), vp]
     L.aero_ns2d_sweep_set_barrier.argtypes = [vp, i32, i32]
+    L.aero_ns3d_set_wait_bound.argtypes = [vp, i32, i32]
+    L.aero_ns3d_set_wait_bound.restype = C.c_int
     L.aero_ns2d_sweep_info.argtypes = [vp, C.POINTER(C.c_int64)]
     for name in ("aero_ns2d_sweep_create", "aero_ns2d_sweep_init", "aero_ns2d_sweep_step", "aero_ns2d_sweep_read_status",
                  "aero_ns2d_sweep_set_barrier", "aero_ns2d_sweep_info"):

@@ -83,6 +83,7 @@ struct AeroNs3dPlan {
   AxisInfo ax[3];
   int zc, zc_nu, nblocks, nq;    // z-planes per CTA of the stage and eddy-viscosity kernels
   int pu, pn;                     // row pitches of the stage-start u copy and of nu
+  int wait_limit = 0, wait_extra_tx = 0;  // plane-wait bound (0: default) and its test hook
 };
 
 namespace {
@@ -280,6 +281,8 @@ int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom
   S.rv = comp_rules<T>(c, 1);
   S.rw = comp_rules<T>(c, 2);
   S.status = status;
+  S.wait_limit = p->wait_limit;
+  S.wait_extra_tx = p->wait_extra_tx;
   S.nu_pitch = p->pn;
   S.px = c.periodic[0];
   S.py = c.periodic[1];
@@ -303,6 +306,8 @@ int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom
   NP.rv = comp_rules<T>(c, 1);
   NP.rw = comp_rules<T>(c, 2);
   NP.status = status;
+  NP.wait_limit = p->wait_limit;
+  NP.wait_extra_tx = p->wait_extra_tx;
   NP.nu_pitch = p->pn;
   const bool f64 = sizeof(T) == 8;
   // TMA views: stage-start u copy and nu are fixed workspace buffers; v, w, theta change by stage
@@ -1067,6 +1072,14 @@ int aero_ns3d_read_status(const AeroNs3dPlan *plan, const void *workspace, int32
                            cudaMemcpyDeviceToHost, s));
   CUDA_TRY(cudaStreamSynchronize(s));
   *status = v;
+  return AERO_OK;
+}
+
+int aero_ns3d_set_wait_bound(AeroNs3dPlan *plan, int32_t spin_limit, int32_t test_extra_bytes) {
+  if (!plan || spin_limit < 0 || test_extra_bytes < 0 || test_extra_bytes > 4096)
+    return fail(AERO_EINVAL, "bad wait bound");
+  plan->wait_limit = spin_limit;
+  plan->wait_extra_tx = test_extra_bytes;
   return AERO_OK;
 }
 

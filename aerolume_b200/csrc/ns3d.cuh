@@ -30,6 +30,9 @@ struct NuParams {
   CUtensorMap map_u, map_v, map_w;  // TMA views of the stage-start velocity (use_tma)
   int use_tma;
   int *status;
+  // polls of a plane's barrier before the CTA gives up (status bit 1), drains its copies in
+  // flight and returns; wait_extra_tx > 0 only in the test of that bound (bytes that never arrive)
+  int wait_limit, wait_extra_tx;
   int nu_pitch;
   int nx, ny, nz, zc, les;
   T inv_h, cd2;
@@ -85,6 +88,7 @@ struct StageParams {
   CUtensorMap map_u, map_v, map_w, map_th, map_nu;  // TMA views (use_tma)
   int use_tma;
   int *status;
+  int wait_limit, wait_extra_tx;  // as in NuParams
   int nu_pitch;
   int nx, ny, nz, zc;
   T h, inv_h;

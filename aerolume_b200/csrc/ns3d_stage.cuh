@@ -66,7 +66,8 @@ __global__ void __launch_bounds__(TX *TY) nu_kernel(const __grid_constant__ NuPa
   const T inv = P.inv_h;
   // tile entry (ly, lx) <-> x index i0 - 4 + lx (face for u, cell for v / w), y index j0 - 2 + ly
   const bool interior_xy = i0 - 2 >= 0 && i0 + TX <= nx && j0 - 2 >= 0 && j0 + TY <= ny;
-  const uint32_t bytes = 3u * QX * QY * sizeof(T);
+  const uint32_t bytes = 3u * QX * QY * sizeof(T) + (uint32_t)P.wait_extra_tx;
+  const int limit = P.wait_limit > 0 ? P.wait_limit : (1 << 24);
   auto SL = [&](int kp) { return (kp - qb + 2) & (QSLOT - 1); };
   auto issue = [&](int kp) {
     const int s = SL(kp);
@@ -92,9 +93,16 @@ __global__ void __launch_bounds__(TX *TY) nu_kernel(const __grid_constant__ NuPa
         S.vel[2][s][e] = padded<T>(P.wp, P.rw, kp, gj, gi);
     }
   };
-  auto await_plane = [&](int kp) {
+  auto await_plane = [&](int kp) -> bool {
     const int m = kp - qb + 2;
-    mbar_wait_bounded(&S.bar[SL(kp)], (uint32_t)((m / QSLOT) & 1), P.status);
+    return mbar_wait_bounded(&S.bar[SL(kp)], (uint32_t)((m / QSLOT) & 1), P.status, limit);
+  };
+  // after a wait ran out (the CTA agrees on that at its next barrier): let the copies it issued,
+  // planes up to `last`, land (bounded again) and return without writing further cells
+  auto drain = [&](int last) {
+    if (tid == 0)
+      for (int kp = max(qb - 2, last - QSLOT + 1); kp <= last; ++kp)
+        mbar_wait_bounded(&S.bar[SL(kp)], (uint32_t)(((kp - qb + 2) / QSLOT) & 1), nullptr, limit);
   };
   if (tid == 0) {
     for (int q = 0; q < QSLOT; ++q) mbar_init(&S.bar[q], 1);
@@ -105,17 +113,21 @@ __global__ void __launch_bounds__(TX *TY) nu_kernel(const __grid_constant__ NuPa
   // any iteration needs is qe - 1.  Iteration q issues plane q + AHEAD, so the ring holds
   // planes q - 2 .. q + AHEAD (QSLOT of them) and the slot it refills (plane q - 3) was last
   // read in iteration q - 1, which ended with a barrier.
+  bool ok = true;
   if (P.use_tma) {
     if (tid == 0)
       for (int kp = qb - 2; kp <= min(qb + AHEAD - 1, qe - 1); ++kp) issue(kp);
-    for (int kp = qb - 2; kp <= qb; ++kp) {
-      await_plane(kp);
-      fill(kp, false);
+    for (int kp = qb - 2; kp <= qb && ok; ++kp) {
+      ok = await_plane(kp);
+      if (ok) fill(kp, false);
     }
   } else {
     for (int kp = qb - 2; kp <= qb; ++kp) fill(kp, true);
   }
-  __syncthreads();
+  if (__syncthreads_or(!ok)) {
+    drain(min(qb + AHEAD - 1, qe - 1));
+    return;
+  }
 #define V3(c, dz, yy, xx) S.vel[c][SL(kn + (dz))][(yy) * QX + (xx)]
   T mx = T(0);
   for (int q = qb; q < qe; ++q) {
@@ -173,13 +185,16 @@ __global__ void __launch_bounds__(TX *TY) nu_kernel(const __grid_constant__ NuPa
     }
     if (pre) {
       if (P.use_tma) {
-        await_plane(q + 1);
-        fill(q + 1, false);
+        ok = await_plane(q + 1);
+        if (ok) fill(q + 1, false);
       } else {
         fill(q + 1, true);
       }
     }
-    __syncthreads();
+    if (__syncthreads_or(!ok)) {
+      drain(min(q + AHEAD, qe - 1));
+      return;
+    }
   }
 #undef V3
   if (P.nut_max) block_max_atomic<T>(mx, P.nut_max);
@@ -222,7 +237,9 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) stage_kernel(c
   // ---- plane slots: plane kp of every field (and nu cell plane kp - 1) lives in slot SL(kp)
   // tile entry (ly, lx) <-> x index i0 - 4 + lx, y index j0 - 2 + ly
   const bool interior_xy = i0 - 2 >= 0 && i0 + TX + 2 <= nx && j0 - 2 >= 0 && j0 + TY + 2 <= ny;
-  const uint32_t bytes = (uint32_t)sizeof(T) * ((3u + (thermal ? 1u : 0u)) * PPL + (les ? (uint32_t)(NUX * NUY) : 0u));
+  const uint32_t bytes = (uint32_t)sizeof(T) * ((3u + (thermal ? 1u : 0u)) * PPL + (les ? (uint32_t)(NUX * NUY) : 0u)) +
+                         (uint32_t)P.wait_extra_tx;
+  const int limit = P.wait_limit > 0 ? P.wait_limit : (1 << 24);
   auto SL = [&](int kp) { return (kp - kb + 2) % NSLOT; };
   auto issue = [&](int kp) {
     const int s = SL(kp);
@@ -257,9 +274,16 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) stage_kernel(c
       }
     }
   };
-  auto await_plane = [&](int kp) {
+  auto await_plane = [&](int kp) -> bool {
     const int m = kp - kb + 2;
-    mbar_wait_bounded(&S.bar[SL(kp)], (uint32_t)((m / NSLOT) & 1), P.status);
+    return mbar_wait_bounded(&S.bar[SL(kp)], (uint32_t)((m / NSLOT) & 1), P.status, limit);
+  };
+  // after a wait ran out: let the copies issued so far (planes up to `last`) land, then return
+  // with the rest of the chunk unwritten (the status word tells the host)
+  auto drain = [&](int last) {
+    if (tid == 0)
+      for (int kp = max(kb - 2, last - NSLOT + 1); kp <= last; ++kp)
+        mbar_wait_bounded(&S.bar[SL(kp)], (uint32_t)(((kp - kb + 2) / NSLOT) & 1), nullptr, limit);
   };
 #define VEL(c, dz, yy, xx) S.vel[c][SL(kc + (dz))][(yy) * PX + (xx)]
 #define TH(dz, yy, xx) S.th[SL(kc + (dz))][(yy) * PX + (xx)]
@@ -321,17 +345,21 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) stage_kernel(c
     mbar_fence_init();
   }
   __syncthreads();
+  bool ok = true;
   if (P.use_tma) {
     if (tid == 0)
       for (int kp = kb - 2; kp <= kb + 2; ++kp) issue(kp);
-    for (int kp = kb - 2; kp <= kb + 2; ++kp) {
-      await_plane(kp);
-      fill(kp, false);
+    for (int kp = kb - 2; kp <= kb + 2 && ok; ++kp) {
+      ok = await_plane(kp);
+      if (ok) fill(kp, false);
     }
   } else {
     for (int kp = kb - 2; kp <= kb + 2; ++kp) fill(kp, true);
   }
-  __syncthreads();
+  if (__syncthreads_or(!ok)) {
+    drain(kb + 2);
+    return;
+  }
   {
     const int kc = kb - 1;
     if (valid) z_interface(kc);
@@ -696,13 +724,16 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) stage_kernel(c
     }
     if (pre) {
       if (P.use_tma) {
-        await_plane(k + 3);
-        fill(k + 3, false);
+        ok = await_plane(k + 3);
+        if (ok) fill(k + 3, false);
       } else {
         fill(k + 3, true);
       }
     }
-    __syncthreads();
+    if (__syncthreads_or(!ok)) {
+      drain(min(k + 3, ke + 1));
+      return;
+    }
   }
 
   if (P.has_win && P.partials) {

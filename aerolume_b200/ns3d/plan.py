@@ -486,11 +486,18 @@ class Ns3dPlan:
         return int(out[0]), int(out[1])
 
     def status(self) -> int:
-        """Device status word of the last step (synchronises): 0, or bit 0 = non-finite value."""
+        """Device status word of the last step (synchronises): 0, or bit 0 = non-finite value,
+        bit 1 = a plane load's wait ran out, bit 2 = a tensor-core wait of the closure ran out."""
         v = C.c_int32()
         check(_lib.lib().aero_ns3d_read_status(self._handle, C.c_void_p(self.ws_ptr), C.byref(v), self._stream()),
               "aero_ns3d_read_status")
         return int(v.value)
+
+    def set_wait_bound(self, spin_limit: int = 0, test_extra_bytes: int = 0) -> None:
+        """Polls of a plane wait before the kernel gives up (0: the default); test_extra_bytes > 0
+        makes every plane wait for bytes that never arrive (tests of the bound only)."""
+        check(_lib.lib().aero_ns3d_set_wait_bound(self._handle, int(spin_limit), int(test_extra_bytes)),
+              "aero_ns3d_set_wait_bound")
 
 
 __all__ = ["Ns3dPlan"]

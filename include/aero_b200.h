@@ -432,6 +432,13 @@ int aero_ns3d_closure_counts(const AeroNs3dPlan *plan, const void *workspace, ui
  * non-finite value reached a reduction; bit 1: a plane load timed out; bit 2: a tensor-core
  * wait of the closure timed out).  Reads through a host copy: synchronises. */
 int aero_ns3d_read_status(const AeroNs3dPlan *plan, const void *workspace, int32_t *status, void *stream);
+/* Bound of the plane waits of the eddy-viscosity and stage kernels: polls of a plane's barrier
+ * before a CTA gives up, sets bit 1 of the status word, lets the copies it issued land and
+ * returns with the rest of its chunk unwritten (0: the default, 2^24 polls).
+ * test_extra_bytes > 0 is for tests of that bound only: every plane then waits for that many
+ * bytes more than its copies bring, so every wait runs out (0 in use; at most 4096).
+ * (No counterpart in the reference, which has no bounded waits.) */
+int aero_ns3d_set_wait_bound(AeroNs3dPlan *plan, int32_t spin_limit, int32_t test_extra_bytes);
 
 /* The checked build (libaero_b200_checked.so, compiled with AERO_BOUNDS_CHECK) records the
  * first out-of-range shared- or global-memory index a kernel would have used -- (code, index,

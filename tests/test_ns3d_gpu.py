@@ -255,6 +255,37 @@ def test_largest_grid_step_is_divergence_free():
     assert out["theta"].max().item() > 0.0            # the hot body heats the fluid next to it
 
 
+def test_plane_wait_that_runs_out_stops_the_kernel_and_reports():
+    """Every plane of the eddy-viscosity and stage kernels made to wait for 16 bytes that never
+    arrive, with a bound of 2048 polls: each CTA gives up, lets its copies land and returns;
+    the status word carries bit 1, and the same plan with the default bound then gives the
+    normal step bit for bit (the context stays usable)."""
+    from aerolume_b200.ns3d.plan import Ns3dPlan
+    from aerolume_b200.ns3d.workloads import box_on_moving_floor, initial_state
+    ops, geom, th, src, _ = box_on_moving_floor(64, 32, 32, dtype="float32", seed=6)
+    plan = Ns3dPlan(ops, geom, th, src, smoke=True)
+    u, v, w = initial_state(ops, seed=6, noise=0.05)
+    plan.project(u, v, w)
+    theta = torch.zeros(32, 32, 64, device="cuda")
+    dye = torch.zeros(32, 32, 64, device="cuda")
+    t0 = torch.zeros((), device="cuda")
+
+    def step():
+        out = plan.step(u, v, w, t0, theta0=theta, dye0=dye)
+        return {k: out[k].clone() for k in ("u", "v", "w", "p", "theta", "dye", "dt")}
+
+    a = step()
+    assert plan.status() == 0
+    plan.set_wait_bound(2048, 16)
+    step()
+    assert plan.status() & 2
+    plan.set_wait_bound(0, 0)
+    b = step()
+    assert plan.status() == 0
+    for k in a:
+        assert torch.equal(a[k], b[k]), k
+
+
 @pytest.mark.parametrize("name", ["tunnel_wale_heat_smoke_f64", "periodic_vreman_f64", "closed_central_cavity_f64"])
 def test_given_dt_matches_oracle(name):
     """dt passed in (the solver's fixed-dt and restart paths, core.py:765 ``dt=``): the step uses
