@@ -14,7 +14,7 @@ import os
 
 LIB_PATH = Path(__file__).resolve().parent / (
     "libaero_b200_checked.so" if os.environ.get("AERO_B200_CHECKED") == "1" else "libaero_b200.so")
-ABI_VERSION = 5
+ABI_VERSION = 6
 MAX_BODIES = 8
 MAX_FANS = 4
 MAX_PORTS = 4
@@ -105,7 +105,8 @@ class Ns3dGeom(C.Structure):
 
 
 class SweepTuning(C.Structure):
-    _fields_ = [("lcap", C.c_int32), ("ctas_per_sm", C.c_int32), ("order", C.c_int32)]
+    _fields_ = [("lcap", C.c_int32), ("ctas_per_sm", C.c_int32), ("order", C.c_int32), ("schedule", C.c_int32),
+                ("tiles", C.c_int32)]
 
 
 class ClosureModel(C.Structure):

@@ -955,6 +955,12 @@ struct FinalArgs {
 
 struct alignas(16) Op {
   int kind, gx, gy, n;   // n: the transform length of POW2
+  // the instance, and how many of its work items (of its earlier operations) end before this
+  // operation may start: the dependency the schedules without grid barriers wait for
+  int inst, need;
+  // tiled operations (stage, transforms): tiles along x of the single-instance grid, and how
+  // many consecutive ones a work item runs (gx = ceil(tgx / tiles) work items along x)
+  int tgx, tiles;
   union Args {
     StageParams<float> st;
     TransformParams<float> tr;
@@ -970,22 +976,60 @@ struct alignas(16) Op {
 // the recording of one instance's step (host)
 struct Recorder {
   std::vector<Op> ops;
-  int lcap;   // log2 of the widest power-of-two transform tile
+  int lcap;    // log2 of the widest power-of-two transform tile
+  int tiles;   // tiles per work item of the stage and transform operations
 };
+
+// Schedules: BARRIER runs phase p (operation p of every instance) between grid barriers;
+// COUNTERS and QUEUE drop the barriers: a work item waits only until its own instance has
+// finished the items of its earlier operations (a per-instance counter of finished items),
+// COUNTERS with the items dealt round robin to the CTAs, QUEUE with the CTAs taking the next
+// item from a global counter.  Items are numbered phase by phase, so every item an item waits
+// for has a smaller number and was taken earlier by a CTA that is running (all CTAs are
+// co-resident): the smallest unfinished item can always go on, and nothing deadlocks.
+enum Schedule : int { BARRIER = 0, COUNTERS = 1, QUEUE = 2 };
 
 struct Tables {
   const Op *ops;
-  const int *phase_first, *phase_count, *op_index;
-  const long long *phase_items, *op_prefix;
-  int nphase;
-  unsigned int *bar;   // [0] arrivals, [1] generation
-  int *status;         // bit 0: a grid barrier ran out
+  const int *item_op;                       // operation of every work item (phase by phase)
+  const long long *op_first;                // first work item of every operation
+  const long long *phase_base, *phase_items;
+  long long total;                          // work items of one step
+  int nphase, sched;
+  unsigned int *bar;         // [0] arrivals, [1] generation (BARRIER)
+  unsigned long long *queue; // next work item (QUEUE)
+  unsigned int *done;        // finished work items of every instance (COUNTERS, QUEUE)
+  int *status;               // bit 0: a wait ran out (the launch then stopped)
   int spin_limit, extra;
 };
 
 constexpr int NTHR = 256;
 constexpr int EW = 8;   // elements per thread of an elementwise work item (divergence, psi, correction)
 constexpr long long MAX_CHUNK = 2048;   // elements of one work item of the maxima
+
+// Wait (thread 0 for the CTA) until instance `inst` has finished `need` work items; bounded,
+// and cut short once another CTA has given up (bit 0 of the status word).
+__device__ __forceinline__ bool await_instance(const Tables &T, int inst, int need) {
+  __shared__ int ok_s;
+  if (threadIdx.x == 0) {
+    int ok = 1, it = 0;
+    const unsigned int target = (unsigned int)need + (unsigned int)T.extra;
+    unsigned int got;
+    for (;;) {
+      asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(got) : "l"(T.done + inst) : "memory");
+      if (got >= target) break;
+      if (++it >= T.spin_limit || *(volatile int *)T.status & 1) {
+        ok = 0;
+        atomicOr(T.status, 1);
+        break;
+      }
+      __nanosleep(32);
+    }
+    ok_s = ok;
+  }
+  __syncthreads();
+  return ok_s != 0;
+}
 
 // Grid-wide barrier between phases: arrivals counted atomically, the last one bumps the
 // generation; the others poll it (bounded: after spin_limit polls bit 0 of the status is set
@@ -1043,28 +1087,47 @@ __device__ __forceinline__ void run_pow2(const TransformParams<float> &P, int n,
 template <int LCAP, int MINB>
 __global__ void __launch_bounds__(NTHR, MINB) sweep2d_kernel(const __grid_constant__ Tables T) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  // the current operation in shared memory: the bodies then read its parameters from a space
+  // their global stores cannot alias, so they stay in registers instead of being reloaded
+  // after every store; restaged only when the operation changes
+  __shared__ Op op_s;
+  __shared__ long long item_s;
   const int tid = threadIdx.x;
-  for (int ph = 0; ph < T.nphase; ++ph) {
-    const long long items = T.phase_items[ph];
-    const int f = T.phase_first[ph], c = T.phase_count[ph];
-    for (long long g = blockIdx.x; g < items; g += gridDim.x) {
-      int lo = 0, hi = c - 1;   // the operation whose items hold g
-      while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (T.op_prefix[f + mid] <= g) lo = mid;
-        else hi = mid - 1;
+  int ph = 0, cur = -1;
+  long long l = blockIdx.x, next = blockIdx.x;
+  for (;;) {
+    long long g;
+    if (T.sched == BARRIER) {
+      while (ph < T.nphase && l >= T.phase_items[ph]) {
+        if (!grid_barrier(T)) return;
+        ++ph;
+        l = blockIdx.x;
       }
-      // the item's operation into shared memory: the bodies then read its parameters from a
-      // space their global stores cannot alias, so they stay in registers instead of being
-      // reloaded after every store (the previous item ended with a block barrier)
-      __shared__ Op op_s;
-      {
-        const uint4 *src = reinterpret_cast<const uint4 *>(T.ops + T.op_index[f + lo]);
-        for (int q = tid; q < (int)(sizeof(Op) / 16); q += NTHR) reinterpret_cast<uint4 *>(&op_s)[q] = src[q];
+      if (ph >= T.nphase) return;
+      g = T.phase_base[ph] + l;
+      l += gridDim.x;
+    } else {
+      if (T.sched == QUEUE) {
+        if (tid == 0) item_s = (long long)atomicAdd(T.queue, 1ull);
+        __syncthreads();
+        next = item_s;
       }
+      g = next;
+      if (g >= T.total) return;
+      next += gridDim.x;
+    }
+    const int o = T.item_op[g];
+    if (o != cur) {
+      const uint4 *src = reinterpret_cast<const uint4 *>(T.ops + o);
+      for (int q = tid; q < (int)(sizeof(Op) / 16); q += NTHR) reinterpret_cast<uint4 *>(&op_s)[q] = src[q];
+      cur = o;
       __syncthreads();
-      const Op &op = op_s;
-      const long long b = g - T.op_prefix[f + lo];
+    }
+    const Op &op = op_s;
+    const int inst = op.inst;   // read before the next item may restage op_s
+    if (T.sched != BARRIER && !await_instance(T, inst, op.need)) return;
+    {
+      const long long b = g - T.op_first[o];
       const int bx = (int)(b % op.gx), by = (int)(b / op.gx);
       switch (op.kind) {
         case ZERO:
@@ -1074,21 +1137,36 @@ __global__ void __launch_bounds__(NTHR, MINB) sweep2d_kernel(const __grid_consta
           const MaxJob<float> &q = op.a.mx.J.job[by];
           const long long e0 = (long long)bx * op.a.mx.chunk, e1 = min(e0 + op.a.mx.chunk, (long long)q.n);
           float m = 0.f;
-          for (long long e = e0 + tid; e < e1; e += NTHR) {
-            const float v = fabsf(__ldg(q.a + e));
+          for (long long e = e0 + tid; e < e1; e += NTHR) {   // coherent loads: written in this launch
+            const float v = fabsf(q.a[e]);
             m = (v > m || v != v) ? v : m;
           }
           // block maximum (NaN wins), one atomic on the ordered bits of the double
-          for (int o = 16; o > 0; o >>= 1) {
-            const float other = __shfl_xor_sync(0xffffffffu, m, o);
+          for (int sh = 16; sh > 0; sh >>= 1) {
+            const float other = __shfl_xor_sync(0xffffffffu, m, sh);
             m = (other > m || other != other) ? other : m;
           }
           if ((tid & 31) == 0) atomic_max_nonneg(q.out, (double)m);
           break;
         }
-        case STAGE: stage2d_body<float, false, false, false>(op.a.st, bx, by, op.gx, tid); break;
-        case POW2: run_pow2<LCAP>(op.a.tr, op.n, bx, by, smem_raw); break;
-        case LINE: line_transform_body<float>(op.a.tr, bx, by, smem_raw); break;
+        case STAGE:
+          for (int t = 0, tb = bx * op.tiles; t < op.tiles && tb < op.tgx; ++t, ++tb) {
+            if (t) __syncthreads();   // the previous tile's shared memory is free
+            stage2d_body<float, false, false, false>(op.a.st, tb, by, op.tgx, tid);
+          }
+          break;
+        case POW2:
+          for (int t = 0, tb = bx * op.tiles; t < op.tiles && tb < op.tgx; ++t, ++tb) {
+            if (t) __syncthreads();
+            run_pow2<LCAP>(op.a.tr, op.n, tb, by, smem_raw);
+          }
+          break;
+        case LINE:
+          for (int t = 0, tb = bx * op.tiles; t < op.tiles && tb < op.tgx; ++t, ++tb) {
+            if (t) __syncthreads();
+            line_transform_body<float>(op.a.tr, tb, by, smem_raw);
+          }
+          break;
         case DIV: {
           const DivArgs &a = op.a.dv;
 #pragma unroll
@@ -1128,11 +1206,15 @@ __global__ void __launch_bounds__(NTHR, MINB) sweep2d_kernel(const __grid_consta
           break;
         }
       }
-      __syncthreads();   // the item's shared memory is free for the next one
     }
-    if (!grid_barrier(T)) return;
+    __syncthreads();   // the item's shared memory is free for the next one
+    if (T.sched != BARRIER && tid == 0) {   // publish: the item's writes, then the count
+      __threadfence();
+      atomicAdd(T.done + inst, 1u);
+    }
   }
 }
+
 
 }  // namespace sweep
 
@@ -1190,6 +1272,14 @@ Op new_op(int kind, long long gx, int gy) {
   return o;
 }
 
+// a tiled operation: tgx tiles along x, `tiles` of them per work item
+Op new_tiled_op(int kind, long long tgx, int gy, int tiles) {
+  Op o = new_op(kind, (tgx + tiles - 1) / tiles, gy);
+  o.tgx = (int)std::max<long long>(tgx, 1);
+  o.tiles = tiles;
+  return o;
+}
+
 // one transform pass as a sweep operation (power-of-two tiles no wider than 2^lcap lines)
 int record_transform(Recorder *rec, const aero::TransformParams<float> &P) {
   namespace sw = aero::ns2d::sweep;
@@ -1199,7 +1289,8 @@ int record_transform(Recorder *rec, const aero::TransformParams<float> &P) {
   if (P.A.method == 0 && aero::transform_pow2(n)) {
     if (n < 64) return set_error(AERO_EUNSUPPORTED, "the persistent sweep needs transform lengths of at least 64");
     const int l2 = std::min(aero::fft::tile_log2L(n, 4), rec->lcap), L = 1 << l2;
-    Op o = new_op(sw::POW2, P.axis == 0 ? (long long)((lines_x + L - 1) / L) : (P.nx + L - 1) / L, gy);
+    Op o = new_tiled_op(sw::POW2, P.axis == 0 ? (long long)((lines_x + L - 1) / L) : (P.nx + L - 1) / L, gy,
+                        rec->tiles);
     o.n = n;
     o.a.tr = P;
     rec->ops.push_back(o);
@@ -1207,7 +1298,8 @@ int record_transform(Recorder *rec, const aero::TransformParams<float> &P) {
   }
   if (P.fuse_div || P.p_acc) return set_error(AERO_EINVAL, "fused transform passes need power-of-two axes");
   const int L = P.L;
-  Op o = new_op(sw::LINE, P.axis == 0 ? (long long)((lines_x + L - 1) / L) : (P.nx + L - 1) / L, gy);
+  Op o = new_tiled_op(sw::LINE, P.axis == 0 ? (long long)((lines_x + L - 1) / L) : (P.nx + L - 1) / L, gy,
+                      rec->tiles);
   o.n = n;
   o.a.tr = P;
   rec->ops.push_back(o);
@@ -1440,7 +1532,7 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
     }
     if (rec) {
       if constexpr (std::is_same<T, float>::value) {
-        Op o = new_op(sw::STAGE, p->gx, p->gy);
+        Op o = new_tiled_op(sw::STAGE, p->gx, p->gy, rec->tiles);
         o.a.st = P;
         rec->ops.push_back(o);
       }
@@ -1738,12 +1830,15 @@ int aero_ns2d_poisson_solve(const AeroNs2dPlan *plan, const void *f, void *psi, 
 // ---------------------------------------------------------------------------------------
 
 struct AeroNs2dSweep {
-  std::vector<Op> ops;
-  std::vector<int> phase_first, phase_count, op_index;
-  std::vector<long long> phase_items, op_prefix;
-  int nphase = 0, lcap = 2, ctas_per_sm = 1, order = 0, grid = 0;
+  std::vector<Op> ops;                          // phase by phase
+  std::vector<int> item_op;                     // operation of every work item
+  std::vector<long long> op_first, phase_base, phase_items;
+  long long items = 0;
+  int n = 0, nphase = 0, lcap = 2, ctas_per_sm = 1, order = 0, sched = 0, grid = 0;
   size_t smem = 0;
-  size_t off_ops = 0, off_pf = 0, off_pc = 0, off_oi = 0, off_pi = 0, off_op = 0, total = 0;
+  // workspace: [0, 4) status, [16, 24) barrier words, [24, 32) queue, [32, 32 + 4 n) finished
+  // items per instance (all but the status reset before every step), then the tables
+  size_t sync_bytes = 0, off_ops = 0, off_io = 0, off_of = 0, off_pb = 0, off_pi = 0, total = 0;
   int spin_limit = 1 << 26, extra = 0;
 };
 
@@ -1751,10 +1846,17 @@ namespace {
 
 using SweepKernel = void (*)(const aero::ns2d::sweep::Tables);
 
-// the kernel of a tuning: widest transform tile 2^lcap, registers capped for 2 or for 3 CTAs per SM
+// the kernel of a tuning: widest transform tile 2^lcap, registers capped for 2, 3 or 4 CTAs per SM
 SweepKernel sweep_kernel(int lcap, int cps) {
   namespace sw = aero::ns2d::sweep;
-  if (cps >= 3) {
+  if (cps >= 4) {
+    switch (lcap) {
+      case 1: return sw::sweep2d_kernel<1, 4>;
+      case 2: return sw::sweep2d_kernel<2, 4>;
+      default: return sw::sweep2d_kernel<3, 4>;
+    }
+  }
+  if (cps == 3) {
     switch (lcap) {
       case 1: return sw::sweep2d_kernel<1, 3>;
       case 2: return sw::sweep2d_kernel<2, 3>;
@@ -1789,8 +1891,10 @@ int aero_ns2d_sweep_create(int32_t n, const AeroNs2dPlan *const *plans, const Ae
   if (!plans || !fields || !geoms || !workspaces || !sweep || n < 1) return set_error(AERO_EINVAL, "null argument");
   *sweep = nullptr;
   const int lcap = tuning ? tuning->lcap : 2, cps = tuning ? tuning->ctas_per_sm : 1, order = tuning ? tuning->order : 1;
-  if (lcap < 1 || lcap > 3 || cps < 1 || cps > 3 || order < 0 || order > 1)
-    return set_error(AERO_EINVAL, "tuning: lcap 1..3, ctas_per_sm 1..3, order 0..1");
+  const int sched = tuning ? tuning->schedule : 1, tiles = tuning ? tuning->tiles : 1;
+  if (lcap < 1 || lcap > 3 || cps < 1 || cps > 4 || order < 0 || order > 1 || sched < 0 || sched > 2 || tiles < 1 ||
+      tiles > 8)
+    return set_error(AERO_EINVAL, "tuning: lcap 1..3, ctas_per_sm 1..4, order 0..1, schedule 0..2, tiles 1..8");
   std::vector<std::vector<Op>> per(n);
   std::vector<long long> size(n);
   for (int k = 0; k < n; ++k) {
@@ -1798,6 +1902,7 @@ int aero_ns2d_sweep_create(int32_t n, const AeroNs2dPlan *const *plans, const Ae
     if (plans[k]->cfg.dtype != AERO_F32) return set_error(AERO_EUNSUPPORTED, "the persistent sweep runs FP32 plans");
     Recorder rec;
     rec.lcap = lcap;
+    rec.tiles = tiles;
     const int rc = step2d_impl<float>(plans[k], &fields[k], &geoms[k], nullptr,
                                       static_cast<unsigned char *>(workspaces[k]), nullptr, &rec);
     if (rc) return rc;
@@ -1809,41 +1914,49 @@ int aero_ns2d_sweep_create(int32_t n, const AeroNs2dPlan *const *plans, const Ae
   if (order == 1)   // largest instances first: their work items start first in every phase
     std::stable_sort(inst.begin(), inst.end(), [&](int a, int b) { return size[a] > size[b]; });
   auto *S = new AeroNs2dSweep();
+  S->n = n;
   S->lcap = lcap;
   S->ctas_per_sm = cps;
   S->order = order;
+  S->sched = sched;
   size_t longest = 0;
   for (auto &v : per) longest = std::max(longest, v.size());
   S->nphase = (int)longest;
+  std::vector<long long> seen(n, 0);   // work items of each instance's operations so far
   for (int ph = 0; ph < S->nphase; ++ph) {
-    S->phase_first.push_back((int)S->op_index.size());
-    long long items = 0;
-    int count = 0;
+    S->phase_base.push_back(S->items);
     for (int k : inst) {
       if ((size_t)ph >= per[k].size()) continue;
-      const Op &o = per[k][ph];
-      S->op_index.push_back((int)S->ops.size());
-      S->op_prefix.push_back(items);
+      Op o = per[k][ph];
+      const long long cnt = (long long)o.gx * o.gy;
+      o.inst = k;
+      o.need = (int)seen[k];
+      seen[k] += cnt;
+      S->op_first.push_back(S->items);
+      S->item_op.insert(S->item_op.end(), (size_t)cnt, (int)S->ops.size());
       S->ops.push_back(o);
       S->smem = std::max(S->smem, op_smem(o, lcap));
-      items += (long long)o.gx * o.gy;
-      ++count;
+      S->items += cnt;
     }
-    S->phase_count.push_back(count);
-    S->phase_items.push_back(items);
+    S->phase_items.push_back(S->items - S->phase_base.back());
   }
-  size_t off = aero_host::ALIGN;   // [0, 256): barrier words and the status word
+  for (long long x : seen)
+    if (x >= (1ll << 31)) {
+      delete S;
+      return set_error(AERO_EUNSUPPORTED, "an instance has more than 2^31 work items per step");
+    }
+  S->sync_bytes = aero_host::align_up(32 + 4 * (size_t)n);
+  size_t off = S->sync_bytes;
   auto take = [&](size_t bytes) {
     const size_t o = off;
     off = aero_host::align_up(off + bytes);
     return o;
   };
   S->off_ops = take(S->ops.size() * sizeof(Op));
-  S->off_pf = take(S->phase_first.size() * sizeof(int));
-  S->off_pc = take(S->phase_count.size() * sizeof(int));
-  S->off_oi = take(S->op_index.size() * sizeof(int));
+  S->off_io = take(S->item_op.size() * sizeof(int));
+  S->off_of = take(S->op_first.size() * sizeof(long long));
+  S->off_pb = take(S->phase_base.size() * sizeof(long long));
   S->off_pi = take(S->phase_items.size() * sizeof(long long));
-  S->off_op = take(S->op_prefix.size() * sizeof(long long));
   S->total = off;
   // co-resident CTAs: every CTA waits at the grid barriers
   int dev = 0, nsm = 0, occ = 0;
@@ -1874,17 +1987,15 @@ int aero_ns2d_sweep_init(const AeroNs2dSweep *sweep, void *workspace, void *stre
   auto *ws = static_cast<unsigned char *>(workspace);
   auto s = static_cast<cudaStream_t>(stream);
   const AeroNs2dSweep &S = *sweep;
-  AERO_CUDA_TRY(cudaMemsetAsync(ws, 0, aero_host::ALIGN, s));
+  AERO_CUDA_TRY(cudaMemsetAsync(ws, 0, S.sync_bytes, s));
   AERO_CUDA_TRY(cudaMemcpyAsync(ws + S.off_ops, S.ops.data(), S.ops.size() * sizeof(Op), cudaMemcpyHostToDevice, s));
-  AERO_CUDA_TRY(cudaMemcpyAsync(ws + S.off_pf, S.phase_first.data(), S.phase_first.size() * sizeof(int),
+  AERO_CUDA_TRY(cudaMemcpyAsync(ws + S.off_io, S.item_op.data(), S.item_op.size() * sizeof(int),
                                 cudaMemcpyHostToDevice, s));
-  AERO_CUDA_TRY(cudaMemcpyAsync(ws + S.off_pc, S.phase_count.data(), S.phase_count.size() * sizeof(int),
+  AERO_CUDA_TRY(cudaMemcpyAsync(ws + S.off_of, S.op_first.data(), S.op_first.size() * sizeof(long long),
                                 cudaMemcpyHostToDevice, s));
-  AERO_CUDA_TRY(cudaMemcpyAsync(ws + S.off_oi, S.op_index.data(), S.op_index.size() * sizeof(int),
+  AERO_CUDA_TRY(cudaMemcpyAsync(ws + S.off_pb, S.phase_base.data(), S.phase_base.size() * sizeof(long long),
                                 cudaMemcpyHostToDevice, s));
   AERO_CUDA_TRY(cudaMemcpyAsync(ws + S.off_pi, S.phase_items.data(), S.phase_items.size() * sizeof(long long),
-                                cudaMemcpyHostToDevice, s));
-  AERO_CUDA_TRY(cudaMemcpyAsync(ws + S.off_op, S.op_prefix.data(), S.op_prefix.size() * sizeof(long long),
                                 cudaMemcpyHostToDevice, s));
   AERO_CUDA_TRY(cudaStreamSynchronize(s));   // the host tables are pageable: finish before returning
   return AERO_OK;
@@ -1898,17 +2009,21 @@ int aero_ns2d_sweep_step(const AeroNs2dSweep *sweep, void *workspace, void *stre
   const AeroNs2dSweep &S = *sweep;
   sw::Tables T{};
   T.ops = reinterpret_cast<const Op *>(ws + S.off_ops);
-  T.phase_first = reinterpret_cast<const int *>(ws + S.off_pf);
-  T.phase_count = reinterpret_cast<const int *>(ws + S.off_pc);
-  T.op_index = reinterpret_cast<const int *>(ws + S.off_oi);
+  T.item_op = reinterpret_cast<const int *>(ws + S.off_io);
+  T.op_first = reinterpret_cast<const long long *>(ws + S.off_of);
+  T.phase_base = reinterpret_cast<const long long *>(ws + S.off_pb);
   T.phase_items = reinterpret_cast<const long long *>(ws + S.off_pi);
-  T.op_prefix = reinterpret_cast<const long long *>(ws + S.off_op);
+  T.total = S.items;
   T.nphase = S.nphase;
-  T.bar = reinterpret_cast<unsigned int *>(ws);
-  T.status = reinterpret_cast<int *>(ws + 16);
+  T.sched = S.sched;
+  T.status = reinterpret_cast<int *>(ws);
+  T.bar = reinterpret_cast<unsigned int *>(ws + 16);
+  T.queue = reinterpret_cast<unsigned long long *>(ws + 24);
+  T.done = reinterpret_cast<unsigned int *>(ws + 32);
   T.spin_limit = S.spin_limit;
   T.extra = S.extra;
-  AERO_CUDA_TRY(cudaMemsetAsync(ws, 0, 2 * sizeof(unsigned int), s));   // barrier arrivals and generation
+  // barrier words, queue and finished-item counters start at zero (the status word is kept)
+  AERO_CUDA_TRY(cudaMemsetAsync(ws + 16, 0, 16 + 4 * (size_t)S.n, s));
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(S.grid);
   cfg.blockDim = dim3(sw::NTHR);
@@ -1926,10 +2041,9 @@ int aero_ns2d_sweep_step(const AeroNs2dSweep *sweep, void *workspace, void *stre
 int aero_ns2d_sweep_read_status(const AeroNs2dSweep *sweep, void *workspace, int32_t *status, void *stream) {
   if (!sweep || !workspace || !status) return set_error(AERO_EINVAL, "null argument");
   auto s = static_cast<cudaStream_t>(stream);
-  AERO_CUDA_TRY(cudaMemcpyAsync(status, static_cast<unsigned char *>(workspace) + 16, sizeof(int32_t),
-                                cudaMemcpyDeviceToHost, s));
+  AERO_CUDA_TRY(cudaMemcpyAsync(status, workspace, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
   AERO_CUDA_TRY(cudaStreamSynchronize(s));
-  AERO_CUDA_TRY(cudaMemsetAsync(static_cast<unsigned char *>(workspace) + 16, 0, sizeof(int32_t), s));
+  AERO_CUDA_TRY(cudaMemsetAsync(workspace, 0, sizeof(int32_t), s));
   return AERO_OK;
 }
 
@@ -1942,11 +2056,9 @@ int aero_ns2d_sweep_set_barrier(AeroNs2dSweep *sweep, int32_t spin_limit, int32_
 
 int aero_ns2d_sweep_info(const AeroNs2dSweep *sweep, int64_t out[6]) {
   if (!sweep || !out) return set_error(AERO_EINVAL, "null argument");
-  long long items = 0;
-  for (long long x : sweep->phase_items) items += x;
   out[0] = sweep->nphase;
   out[1] = (int64_t)sweep->ops.size();
-  out[2] = items;
+  out[2] = sweep->items;
   out[3] = sweep->grid;
   out[4] = (int64_t)sweep->smem;
   out[5] = sweep->lcap;

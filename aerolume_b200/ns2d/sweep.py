@@ -9,10 +9,12 @@ to the per-instance loop bit for bit).
 
 Schedules:
 
-* ``"persistent"`` -- one persistent launch per sweep step (``aero_ns2d_sweep_step``): phase p
-  of the launch is operation p of every instance's step, the co-resident CTAs take the work
-  items of all instances' operations, a grid barrier (bounded: it gives up and reports instead
-  of spinning forever) between phases.  :meth:`tune` picks its tile width, CTAs per SM and
+* ``"persistent"`` -- one persistent launch per sweep step (``aero_ns2d_sweep_step``): the
+  co-resident CTAs take the work items of all instances' operations, numbered phase by phase
+  (phase p: operation p of every instance's step).  Between them either a grid barrier per
+  phase or, without barriers, a per-instance count of finished items that each item waits on
+  (its own instance's earlier operations only); every wait is bounded (it gives up and reports
+  instead of spinning forever).  :meth:`tune` picks the schedule, tile width, CTAs per SM and
   instance order by timing them.
 * ``"streams"`` -- each instance's own launches, the instances spread over ``nstream`` CUDA
   streams (largest first, round robin).
@@ -76,15 +78,18 @@ class Sweep2D:
             f.coeffs = out["coeffs"].data_ptr()
         return f
 
-    def build_persistent(self, lcap=2, ctas_per_sm=3, order=1):
-        """The persistent launch of the current instances with these launch choices."""
+    SCHEDULES = {"barrier": 0, "counters": 1, "queue": 2}
+
+    def build_persistent(self, lcap=2, ctas_per_sm=3, order=1, schedule="counters", tiles=1):
+        """The persistent launch of the current instances with these launch choices (schedule:
+        "barrier", "counters" or "queue"; tiles: stage or transform tiles per work item)."""
         L = _lib.lib()
         n = len(self.plans)
         plans = (C.c_void_p * n)(*[p._handle.value for p in self.plans])
         fields = (_lib.Ns2dFields * n)(*[self._fields(k) for k in range(n)])
         geoms = (_lib.Ns2dGeom * n)(*[p.geom_c for p in self.plans])
         wss = (C.c_void_p * n)(*[p.ws_ptr for p in self.plans])
-        tun = _lib.SweepTuning(int(lcap), int(ctas_per_sm), int(order))
+        tun = _lib.SweepTuning(int(lcap), int(ctas_per_sm), int(order), self.SCHEDULES[schedule], int(tiles))
         handle = C.c_void_p()
         check(L.aero_ns2d_sweep_create(n, plans, fields, geoms, wss, C.byref(tun), C.byref(handle)),
               "aero_ns2d_sweep_create")
@@ -94,12 +99,13 @@ class Sweep2D:
         check(L.aero_ns2d_sweep_init(handle, C.c_void_p(ptr), self._stream()), "aero_ns2d_sweep_init")
         info = (C.c_int64 * 6)()
         check(L.aero_ns2d_sweep_info(handle, info), "aero_ns2d_sweep_info")
-        return {"handle": handle, "raw": raw, "ptr": ptr, "tuning": (int(lcap), int(ctas_per_sm), int(order)),
+        return {"handle": handle, "raw": raw, "ptr": ptr,
+                "tuning": (int(lcap), int(ctas_per_sm), int(order), schedule, int(tiles)),
                 "info": dict(zip(("phases", "operations", "items", "ctas", "smem", "lcap"), list(info)))}
 
-    def use_persistent(self, lcap=2, ctas_per_sm=3, order=1):
+    def use_persistent(self, lcap=2, ctas_per_sm=3, order=1, schedule="counters", tiles=1):
         self._release()
-        self._persistent = self.build_persistent(lcap, ctas_per_sm, order)
+        self._persistent = self.build_persistent(lcap, ctas_per_sm, order, schedule, tiles)
         self.tuning = self._persistent["tuning"]
         return self._persistent["info"]
 
@@ -181,11 +187,11 @@ class Sweep2D:
 
     # ------------------------------------------------------------------ the autotuner
     def tune(self, candidates=None, steps=3, warmup=1):
-        """Time each candidate (lcap, ctas_per_sm, order) of the persistent launch over ``steps``
+        """Time each candidate (lcap, ctas_per_sm, order, schedule, tiles) of the persistent launch over ``steps``
         sweep steps (CUDA events, after ``warmup``), keep the fastest, and put every instance's
         state back as it was.  Returns the table of (candidate, ms per step)."""
         if candidates is None:
-            candidates = list(itertools.product((1, 2, 3), (2, 3), (0, 1)))
+            candidates = list(itertools.product((1, 2, 3), (3, 4), (0, 1), ("barrier", "queue"), (1, 2, 4)))
         snap = self.snapshot()
         table = []
         for cand in candidates:
@@ -194,6 +200,7 @@ class Sweep2D:
             except RuntimeError as exc:          # a launch shape that does not fit is skipped
                 table.append((cand, None, str(exc)))
                 continue
+            cand = obj["tuning"]                 # every choice spelled out
             for _ in range(warmup):
                 self._persistent_step(obj)
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

@@ -845,11 +845,13 @@ def run_sweep(args, rank, world, local_rank):
                        "parallelism": "instances sharded over the ranks" if args.shard else "replicas",
                        "graph": f"{K} sweep steps, each one persistent launch, 1 replay"},
             "persistent": {"tuning": {"lcap": sw.tuning[0], "ctas_per_sm": sw.tuning[1],
-                                      "order": "largest first" if sw.tuning[2] else "as given"},
+                                      "order": "largest first" if sw.tuning[2] else "as given",
+                                      "schedule": sw.tuning[3], "tiles_per_item": sw.tuning[4]},
                            "phases": info["phases"], "operations": info["operations"],
                            "work_items_per_step": info["items"], "ctas": info["ctas"],
                            "dynamic_smem": info["smem"], "status": status,
-                           "autotuner": [{"lcap": c[0], "ctas_per_sm": c[1], "order": c[2], "ms_per_step": t}
+                           "autotuner": [{"lcap": c[0], "ctas_per_sm": c[1], "order": c[2], "schedule": c[3],
+                                          "tiles": c[4], "ms_per_step": t}
                                          for c, t, _ in tune_table]},
             "instances": len(coeffs), "instances_per_rank": len(mine) if not args.shard else "size-balanced shard",
             "streams": {"value": total_cells * K / (timings["streams"] * 1e-3) / 1e6, "unit": UNIT,

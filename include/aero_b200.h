@@ -47,7 +47,7 @@
 extern "C" {
 #endif
 
-#define AERO_ABI_VERSION 5
+#define AERO_ABI_VERSION 6
 
 #define AERO_OK 0
 #define AERO_EINVAL -1        /* invalid argument or inconsistent configuration     */
@@ -538,17 +538,20 @@ int aero_ns2d_poisson_solve(const AeroNs2dPlan *plan, const void *f, void *psi, 
  * No counterpart in the reference, which steps its solver once per instance (ns2d/solver.py:489
  * advance, core.py:815 step_full each).  A sweep records the step of each instance (plan,
  * fields, geometry, workspace: the arguments of aero_ns2d_step, bound at creation, like a
- * captured graph) as its sequence of operations, and aero_ns2d_sweep_step runs operation p of
- * every instance as phase p of one persistent cooperative kernel: the CTAs (co-resident, as
- * many per SM as the tuning asks and the kernel allows) take the work items of all instances'
- * operations, a grid barrier between phases.  Every instance's result is bit-identical to its
- * own aero_ns2d_step.  FP32 plans without LES, heat transfer or dye, with the CFL time step,
+ * captured graph) as its sequence of operations, and aero_ns2d_sweep_step runs all of them in
+ * one persistent cooperative kernel: the CTAs (co-resident, as many per SM as the tuning asks
+ * and the kernel allows) take the work items of all instances' operations, numbered phase by
+ * phase (phase p: operation p of every instance).  Every instance's result is bit-identical to
+ * its own aero_ns2d_step.  FP32 plans without LES, heat transfer or dye, with the CFL time step,
  * transform lengths of at least 64.  Tuning: lcap the log2 of the widest power-of-two transform
- * tile (1..3), ctas_per_sm (1..3; 3 compiles the kernel for fewer registers per thread), order 0
- * (the instances' order) or 1 (largest first). */
+ * tile (1..3), ctas_per_sm (1..4; 3 and 4 compile the kernel for fewer registers per thread),
+ * order 0 (the instances' order) or 1 (largest first), schedule 0 (a grid barrier between
+ * phases), 1 (no barriers: an item waits until its own instance has finished its earlier
+ * operations, items dealt round robin to the CTAs) or 2 (as 1, the CTAs taking items from a
+ * queue), tiles (1..8) the stage or transform tiles one work item runs. */
 typedef struct AeroNs2dSweep AeroNs2dSweep;
 typedef struct {
-  int32_t lcap, ctas_per_sm, order;
+  int32_t lcap, ctas_per_sm, order, schedule, tiles;
 } AeroSweepTuning;
 int aero_ns2d_sweep_create(int32_t n, const AeroNs2dPlan *const *plans, const AeroNs2dFields *fields,
                            const AeroNs2dGeom *geoms, void *const *workspaces, const AeroSweepTuning *tuning,
@@ -560,11 +563,11 @@ size_t aero_ns2d_sweep_workspace_bytes(const AeroNs2dSweep *sweep);
 int aero_ns2d_sweep_init(const AeroNs2dSweep *sweep, void *workspace, void *stream);
 /* One step of every instance: one persistent launch (capturable in a CUDA graph). */
 int aero_ns2d_sweep_step(const AeroNs2dSweep *sweep, void *workspace, void *stream);
-/* Status word since the last read (bit 0: a grid barrier ran out; the launch then stopped);
- * synchronises, then clears it. */
+/* Status word since the last read (bit 0: a grid barrier or an instance wait ran out; the
+ * launch then stopped); synchronises, then clears it. */
 int aero_ns2d_sweep_read_status(const AeroNs2dSweep *sweep, void *workspace, int32_t *status, void *stream);
-/* The barrier's bound (polls before giving up) and, for tests of that bound, extra arrivals to
- * wait for that never come (0 in use). */
+/* The bound of the waits (polls before giving up) and, for tests of that bound, extra arrivals
+ * (barrier) or finished items (instance waits) to wait for that never come (0 in use). */
 int aero_ns2d_sweep_set_barrier(AeroNs2dSweep *sweep, int32_t spin_limit, int32_t extra);
 /* [phases, operations, work items per step, CTAs, dynamic shared bytes, lcap] */
 int aero_ns2d_sweep_info(const AeroNs2dSweep *sweep, int64_t out[6]);

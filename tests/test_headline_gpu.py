@@ -211,37 +211,48 @@ def _run(sw, snap, schedule, steps, graph):
 
 def test_sweep_schedules_equal_the_per_instance_loop():
     """The batched sweep (64 seeded NACA instances on five grid sizes) as one persistent launch
-    per step (its launch shape picked by the autotuner, captured in one CUDA graph) and spread
-    over 16 streams give every instance exactly what its own plan gives when the instances are
-    stepped one after another: fields, time and coefficients bit for bit after five steps."""
+    per step -- with a grid barrier per phase, with per-instance counters of finished items
+    (items dealt round robin, or taken from a queue), and the shape the autotuner picks, in and
+    out of a CUDA graph -- and spread over 16 streams give every instance exactly what its own
+    plan gives when the instances are stepped one after another: fields, time and coefficients
+    bit for bit after five steps."""
     from aerolume_b200.ns2d.sweep import Sweep2D
     from aerolume_b200.ns2d.workloads import sweep_instances
     sw = Sweep2D(sweep_instances(64, seed=0))
     snap = sw.snapshot()
-    table = sw.tune(candidates=[(1, 2, 1), (2, 2, 1), (3, 1, 0)], steps=2)
-    assert sw.tuning is not None and any(r[1] is not None for r in table)
     ref = _run(sw, snap, "loop", 5, graph=False)
-    for schedule, graph in (("persistent", True), ("persistent", False), ("streams", True)):
+
+    def check(schedule, graph, tag):
         got = _run(sw, snap, schedule, 5, graph)
         for k, (a, b) in enumerate(zip(got, ref)):
             for x, y in zip(a, b):
-                assert torch.equal(x, y), (schedule, graph, k)
+                assert torch.equal(x, y), (tag, graph, k)
         if schedule == "persistent":
-            assert sw.status() == 0
+            assert sw.status() == 0, tag
+
+    for cand in ((2, 2, 1, "barrier", 1), (3, 3, 0, "counters", 2), (1, 4, 1, "queue", 4)):
+        sw.use_persistent(*cand)
+        check("persistent", True, cand)
+    table = sw.tune(candidates=[(1, 2, 1, "barrier", 2), (2, 2, 1, "counters", 1), (3, 1, 0, "queue", 4)], steps=2)
+    assert sw.tuning is not None and any(r[1] is not None for r in table)
+    check("persistent", False, sw.tuning)
+    check("streams", True, "streams")
     assert all(float(s["t"]) > 0 for s in sw.states)
 
 
-def test_sweep_barrier_gives_up_and_reports():
-    """The persistent launch's grid barrier waits for arrivals that never come (the test hook
-    asks for one CTA more than the launch has): every CTA gives up after the bounded wait, the
-    status word reports it, and the next launch with the barrier restored runs normally and
-    matches the per-instance loop."""
+@pytest.mark.parametrize("schedule", ["barrier", "counters", "queue"])
+def test_sweep_barrier_gives_up_and_reports(schedule):
+    """The persistent launch's waits for arrivals that never come (the test hook asks for one
+    CTA more than the launch has at a grid barrier, or one finished item more than an instance
+    has before every item): every CTA gives up after the bounded wait, the status word reports
+    it, and the next launch with the bound restored runs normally and matches the per-instance
+    loop."""
     from aerolume_b200.ns2d.sweep import Sweep2D
     from aerolume_b200.ns2d.workloads import sweep_instances
     insts = [i for i in sweep_instances(64, seed=0) if i[0].nx == 256][:2]
     sw = Sweep2D(insts)
     snap = sw.snapshot()
-    sw.use_persistent(2, 1, 1)
+    sw.use_persistent(2, 1, 1, schedule)
     sw.set_barrier(2000, extra=1)
     sw.step("persistent")
     torch.cuda.synchronize()
