@@ -118,7 +118,8 @@ class ClosureModel(C.Structure):
 class Ns3dFields(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in (
         "u0", "v0", "w0", "theta0", "dye0", "t0",
-        "u", "v", "w", "p", "theta", "dye", "t", "dt", "coeffs", "heat_rate", "pid_dt_prev", "pid_e1", "pid_e2")]
+        "u", "v", "w", "p", "theta", "dye", "t", "dt", "coeffs", "heat_rate", "pid_dt_prev", "pid_e1", "pid_e2",
+        "div_sq")]
 
 
 class Ns2dConfig(C.Structure):

@@ -79,7 +79,7 @@ struct AeroNs3dPlan {
   size_t esz;                     // bytes per element
   size_t nu, nv, nw, nc;          // element counts of u, v, w and cell arrays
   size_t off_uh, off_vh, off_wh, off_up, off_vp, off_wp, off_tha, off_thb, off_pa, off_nu;
-  size_t off_small, off_scalars, off_status, off_partials, off_psum, off_grad, off_counts, total;
+  size_t off_small, off_scalars, off_status, off_partials, off_psum, off_grad, off_counts, off_sumsq, total;
   AxisInfo ax[3];
   int zc, zc_nu, nblocks, nq;    // z-planes per CTA of the stage and eddy-viscosity kernels
   int pu, pn;                     // row pitches of the stage-start u copy and of nu
@@ -562,7 +562,10 @@ int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom
     CUDA_TRY(aero::launch_stage<T>(P, s));
     CUDA_TRY(mark(3 + 5 * st));
     const int acc_mode = st == 0 ? 0 : (st == 1 ? 1 : 2);
-    if (p->ax[0].method == 0 && aero::transform_pow2(nx) && c.nport == 0) {
+    // a diagnostics row needs the last stage's right-hand side as an array: that stage then
+    // takes the unfused projection
+    const bool want_div_sq = f->div_sq != nullptr && st == 2;
+    if (p->ax[0].method == 0 && aero::transform_pow2(nx) && c.nport == 0 && !want_div_sq) {
       // the first x pass forms div(u_hat) itself, the last one folds psi into p
       aero::TransformParams<T> F{};
       F.fuse_div = 1;
@@ -584,6 +587,9 @@ int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom
       CUDA_TRY(aero::launch_divergence<T>(uh, vh, wh, nx, ny, nz, c.periodic[0], c.periodic[1], c.periodic[2],
                                           T(1.0 / c.h), pa, s));
       CUDA_TRY(aero::launch_port_continuity<T>(pa, nx, ny, S.nport, S.port, s));  // div - m (jets, vents)
+      if (want_div_sq)
+        CUDA_TRY(aero::launch_sumsq<T>(pa, p->nc, reinterpret_cast<double *>(ws + p->off_sumsq),
+                                       static_cast<T *>(f->div_sq), s));
       CUDA_TRY(mark(4 + 5 * st));
       const int rc = poisson_passes<T>(p, pa, pa, ws, s);
       if (rc) return rc;
@@ -886,6 +892,7 @@ int aero_ns3d_plan_create(const AeroNs3dConfig *cfg, AeroNs3dPlan **plan) {
   p->nq = c.nbody * 9 + (c.thermal ? c.n_tbody : 0);
   p->off_partials = take(sizeof(double) * 3 * (size_t)p->nblocks * std::max(p->nq, 1));
   p->off_psum = take(sizeof(double) * 8 * PLANE_PARTS);
+  p->off_sumsq = take(sizeof(double) * aero::SUMSQ_PARTS);
   const int ns[3] = {c.nx, c.ny, c.nz};
   for (int a = 0; a < 3; ++a) {
     AxisInfo &x = p->ax[a];

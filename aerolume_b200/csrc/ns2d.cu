@@ -1095,6 +1095,10 @@ __global__ void __launch_bounds__(NTHR, MINB) sweep2d_kernel(const __grid_consta
   const int tid = threadIdx.x;
   int ph = 0, cur = -1;
   long long l = blockIdx.x, next = blockIdx.x;
+  // QUEUE: thread 0 claims the item after the current one while the current one runs (claims
+  // stay in queue order, so the argument against deadlock holds for claimed items)
+  unsigned long long pending = 0;
+  if (T.sched == QUEUE && tid == 0) pending = atomicAdd(T.queue, 1ull);
   for (;;) {
     long long g;
     if (T.sched == BARRIER) {
@@ -1108,7 +1112,10 @@ __global__ void __launch_bounds__(NTHR, MINB) sweep2d_kernel(const __grid_consta
       l += gridDim.x;
     } else {
       if (T.sched == QUEUE) {
-        if (tid == 0) item_s = (long long)atomicAdd(T.queue, 1ull);
+        if (tid == 0) {
+          item_s = (long long)pending;
+          pending = atomicAdd(T.queue, 1ull);
+        }
         __syncthreads();
         next = item_s;
       }

@@ -251,6 +251,10 @@ cudaError_t launch_outlet_corr(const double *, const double *, const double *, c
                                double, double, double, double, T *, cudaStream_t);
 template <typename T>
 cudaError_t launch_divergence(const T *, const T *, const T *, int, int, int, int, int, int, T, T *, cudaStream_t);
+// sum of squares of a[0, n) into the device scalar out (FP64 partials of SUMSQ_PARTS blocks)
+constexpr int SUMSQ_PARTS = 2 * 148;
+template <typename T>
+cudaError_t launch_sumsq(const T *a, size_t n, double *part, T *out, cudaStream_t s);
 template <typename T> cudaError_t launch_correct(const CorrectParams<T> &, cudaStream_t);
 template <typename T> cudaError_t launch_smoke(const SmokeParams<T> &, cudaStream_t);
 template <typename T> cudaError_t launch_finalize(const FinalizeParams<T> &, cudaStream_t);

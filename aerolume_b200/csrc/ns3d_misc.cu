@@ -522,6 +522,44 @@ __global__ void partials_reduce_kernel(const double *__restrict__ partials, int 
   }
 }
 
+// Diagnostics: sum of squares of an array (physics.py:1303-1305 (div * div).sum()), in FP64 with
+// a fixed block count and thread-to-element mapping, then one block adding the block sums in
+// order: the same value on every run.
+template <typename T>
+__global__ void sumsq_partial_kernel(const T *__restrict__ a, size_t n, double *__restrict__ part) {
+  aero::pdl_wait();
+  double acc = 0.0;
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+    const double x = (double)a[e];
+    acc += x * x;
+  }
+  acc = warp_sum(acc);
+  __shared__ double red[32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+    part[blockIdx.x] = t;
+  }
+}
+
+template <typename T>
+__global__ void sumsq_final_kernel(const double *__restrict__ part, int nparts, T *out) {
+  aero::pdl_wait();
+  double acc = 0.0;
+  for (int q = threadIdx.x; q < nparts; q += blockDim.x) acc += part[q];
+  acc = warp_sum(acc);
+  __shared__ double red[32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+    *out = T(t);
+  }
+}
+
 template <typename T>
 __global__ void finalize_kernel(const FinalizeParams<T> P) {
   aero::pdl_wait();
@@ -668,6 +706,15 @@ cudaError_t launch_divergence(const T *u, const T *v, const T *w, int nx, int ny
 }
 
 template <typename T>
+cudaError_t launch_sumsq(const T *a, size_t n, double *part, T *out, cudaStream_t s) {
+  (void)aero::launch_k(sumsq_partial_kernel<T>, SUMSQ_PARTS, 256, 0, s, a, n, part);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  (void)aero::launch_k(sumsq_final_kernel<T>, 1, 256, 0, s, (const double *)part, SUMSQ_PARTS, out);
+  return cudaGetLastError();
+}
+
+template <typename T>
 cudaError_t launch_correct(const CorrectParams<T> &P, cudaStream_t s) {
   (void)aero::launch_k(correct_kernel<T>, dim3((P.nx + 127) / 128, P.ny + 1, P.nz + 1), 128, 0, s, P);
   return cudaGetLastError();
@@ -710,6 +757,7 @@ cudaError_t launch_psi_accumulate(const T *psi, T *pw, size_t n, T wgt, int mode
   template cudaError_t launch_divergence<T>(const T *, const T *, const T *, int, int, int, int, int, int, T, T *,    \
                                             cudaStream_t);                                                           \
   template cudaError_t launch_correct<T>(const CorrectParams<T> &, cudaStream_t);                                   \
+  template cudaError_t launch_sumsq<T>(const T *, size_t, double *, T *, cudaStream_t);                              \
   template cudaError_t launch_smoke<T>(const SmokeParams<T> &, cudaStream_t);                                       \
   template cudaError_t launch_finalize<T>(const FinalizeParams<T> &, cudaStream_t);                                 \
   template cudaError_t launch_psi_accumulate<T>(const T *, T *, size_t, T, int, const T *, cudaStream_t);

@@ -12,9 +12,10 @@ these instead (solver.py:161-166 ``load_kernels``; solver.py:583-595 ``fast_step
   tensors, as fused.py:371 / 378-502 do.
 * ``fast_dye`` is the MUSCL advection of one smoke channel (fused.py:553-565).
 
-Placed physics that the B200 step does not implement (diagnostics rows) raises instead of
-being computed differently; heat transfer with its volumetric heaters, fans, jets and vents,
-painted solids and the PID step controller run in the step.
+Heat transfer with its volumetric heaters, fans, jets and vents, painted solids and the PID
+step controller run in the step; with ``diag`` the step also leaves the squared norm of the last
+stage's projection right-hand side in ``phys.div_pre`` (physics.py:1303-1305), which the
+solver's diagnostics row reads.
 """
 from __future__ import annotations
 
@@ -124,13 +125,13 @@ def fast_step(state, geom, ops, kern):
 
 def fast_step_phys(state, geom, ops, kern, dt=None, *, phys=None, theta=None, diag=False, theta_kernels=True):
     """One step with the placed physics the B200 step implements (heat transfer, fans, jets and
-    vents, painted solids, the PID step controller)."""
-    if diag:
-        raise RuntimeError("diagnostics rows are not produced by the B200 step")
+    vents, painted solids, the PID step controller); ``diag`` records the last stage's
+    projection right-hand side norm in ``phys.div_pre`` as fused.py:480-482 does."""
     plan = kern.plan_for(geom, ops, phys)
     thermal = plan.thermal is not None and theta is not None
+    div_sq = getattr(phys, "div_pre", None) if diag and phys is not None else None
     out = plan.step(state.u, state.v, state.w, state.t, theta0=theta if thermal else None,
-                    dt=_dt_arg(dt, state.t))
+                    dt=_dt_arg(dt, state.t), div_sq=div_sq)
     if thermal and torch.is_tensor(getattr(plan.thermal, "heat_rate", None)):
         plan.thermal.heat_rate.copy_(out["heat_rate"])  # the reference leaves the rates there
     new = State3D(out["u"], out["v"], out["w"], out["p"], out["t"], out["dt"])

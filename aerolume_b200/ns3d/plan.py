@@ -341,13 +341,15 @@ class Ns3dPlan:
             raise RuntimeError(f"{name} has shape {tuple(t.shape)}, expected {tuple(shape)}")
 
     # -------------------------------------------------------------------- calls
-    def step(self, u0, v0, w0, t0, *, theta0=None, dye0=None, out=None, dt=None, events=None):
+    def step(self, u0, v0, w0, t0, *, theta0=None, dye0=None, out=None, dt=None, events=None, div_sq=None):
         """One step (plus the smoke update when the plan has smoke); returns the output dict.
 
         ``out`` (from :meth:`empty_fields`) may hold ``u0 / v0 / w0 / theta0`` themselves
         (in-place update); ``dt`` is None (CFL rule on the device) or a 0-d device tensor.
         ``events``: a list of ``torch.cuda.Event(enable_timing=True)`` recorded at the step's
-        phase boundaries (``aero_ns3d_step_traced``)."""
+        phase boundaries (``aero_ns3d_step_traced``).  ``div_sq``: a 0-d device tensor that
+        receives the sum of squares of the last stage's projection right-hand side (the
+        diagnostics row's ``poisson_residual`` denominator), or None."""
         nz, ny, nx = self.shape
         self._check("u0", u0, (nz, ny, nx + 1))
         self._check("v0", v0, (nz, ny + 1, nx))
@@ -370,6 +372,9 @@ class Ns3dPlan:
             f.dye0, f.dye = dye0.data_ptr(), out["dye"].data_ptr()
         if self.pid is not None:
             f.pid_dt_prev, f.pid_e1, f.pid_e2 = (getattr(self.pid, n).data_ptr() for n in ("dt_prev", "e1", "e2"))
+        if div_sq is not None:
+            self._check("div_sq", div_sq, ())
+            f.div_sq = div_sq.data_ptr()
         dtp = None
         if dt is not None:
             self._check("dt", dt, ())

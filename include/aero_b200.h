@@ -196,6 +196,11 @@ typedef struct AeroNs3dFields {
   /* PID controller state (0-d scalars of the plan's dtype, read and updated in place by a
    * step whose dt comes from the rule; dt_prev <= 0 means "first step") */
   void *pid_dt_prev, *pid_e1, *pid_e2;
+  /* diagnostics (NULL: not computed): a 0-d scalar of the plan's dtype that receives the sum
+   * of squares of the last stage's projection right-hand side -- the divergence of the stage
+   * value minus the jets' and vents' mass sources (physics.py:1303-1305 record_divergence,
+   * called by fused.py:480-482 on the last stage when the solver records a diagnostics row) */
+  void *div_sq;
 } AeroNs3dFields;
 
 typedef struct AeroNs3dPlan AeroNs3dPlan;

@@ -858,7 +858,8 @@ def dt_rule(u0, v0, w0, ops, nut_max, th, theta, u_floor=0.0, pid=None):
 
 class StepResult:
     """What one step returns: new u, v, w, p, t, dt, per-body coefficients (nb, 6),
-    theta (or None), heat rates (nb) (or None), and the per-stage traces."""
+    theta (or None), heat rates (nb) (or None), the per-stage traces, and div_pre, the sum of
+    squares of the last stage's projection right-hand side (the diagnostics row's input)."""
 
     def __init__(self, **kw):
         self.__dict__.update(kw)
@@ -935,6 +936,8 @@ def step3d_phys(u0, v0, w0, t, geom, ops, poisson, *, th=None, theta=None, dt=No
         div = divergence3d(uh, vh, wh, ops.h)
         if ports is not None:
             div = port_continuity(ports, div)
+        if s == 2:   # Physics3D.record_divergence (physics.py:1303-1305), fused.py:480-482
+            div_pre = float(np.sum(np.asarray(div, np.float64) ** 2))
         psi = poisson.solve(div)
         gx, gy, gz = pressure_gradient(psi, ops)
         if trace:
@@ -955,7 +958,7 @@ def step3d_phys(u0, v0, w0, t, geom, ops, poisson, *, th=None, theta=None, dt=No
         if getattr(th.geom, "flux_rate", None) is not None:
             heat_rate = heat_rate + np.asarray(th.geom.flux_rate, np.float64) * (2.0 if ops.symmetry else 1.0)
     return StepResult(u=up, v=vp, w=wp, p=p, t=T(t + dt), dt=dt, coeffs=coeffs, theta=tp if thermal else None,
-                      heat_rate=heat_rate, stages=stages, nut_stage1=nut_stage1)
+                      heat_rate=heat_rate, stages=stages, nut_stage1=nut_stage1, div_pre=div_pre)
 
 
 # ---------------------------------------------------------------------------

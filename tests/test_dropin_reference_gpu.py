@@ -54,14 +54,14 @@ def _box(C, center):
     return C.ImmersedMesh(v, f, name="box", thermal="temperature", thermal_value=1.0)
 
 
-def _config(C, dtype):
+def _config(C, dtype, diagnostics=False):
     h = 1.0 / 8.0
     rake = C.DyeRake("rake", [(1.0, 1.0, 0.2), (1.0, 1.5, 0.3), (1.0, 2.0, 0.25)], radius=1.25 * h)
     return C.SolverConfig3D(nx=48, ny=24, nz=24, h=h, x0=0.0, y0=0.0, z0=0.0, re=1e4,
                             bodies=[_box(C, (2.0, 1.5, 0.25))], bc_zmin="moving", ground_speed=1.0,
                             turbulence="wale", thermal=C.ThermalConfig3D(prandtl=0.71, richardson=0.2), dye=True,
                             dye_rake=rake, ref_area=0.5, moment_ref=(2.0, 1.5, 0.0), dtype=dtype, device="cuda",
-                            perturb=True)
+                            perturb=True, diagnostics=diagnostics)
 
 
 def _fields(s):
@@ -117,3 +117,31 @@ def test_reference_solver_through_the_b200_seam(dtype, tol):
     # (the unmodified reference solver may drop to eager itself when torch's caching allocator
     # refuses one of its captures; the values above are compared either way)
     assert ours.uses_cuda_graphs
+
+
+@pytest.mark.parametrize("dtype,tol", [("float64", 1e-9), ("float32", 2e-4)])
+def test_reference_diagnostics_through_the_b200_seam(dtype, tol):
+    """The reference solver with ``diagnostics`` on (a device row every 10-step block,
+    solver.py:747-783) through the B200 seam: the step leaves the last stage's projection
+    right-hand side norm in ``phys.div_pre`` as the reference's fused step does, so the rows
+    agree -- time, dt, CFL, the velocity maxima, the change norms of every field and the heat
+    stored -- and the Poisson residual, a round-off quantity, is at round-off in both."""
+    C, F, S = _ref()
+    cfg = _config(C, dtype, diagnostics=True)
+    ref = S.FlowSolver3D(cfg)
+    with b200_seam():
+        ours = S.FlowSolver3D(cfg)
+    ref.advance(30)
+    with b200_seam():
+        ours.advance(30)
+    torch.cuda.synchronize()
+    a, b = ref.diagnostics(), ours.diagnostics()
+    assert len(a["t"]) == len(b["t"]) == 3
+    pa, pb = float(ref._phys.div_pre), float(ours._phys.div_pre)
+    assert pa > 0.0 and abs(pa - pb) <= 10 * tol * pa, (pa, pb)
+    keys = ["t", "dt", "cfl", "umax", "heat_storage"] + [f"d{f}_{n}" for f in "uvwp" for n in ("l2", "rms", "max")]
+    for k in keys:
+        sc = max(np.abs(a[k]).max(), 1e-30)
+        assert np.abs(a[k] - b[k]).max() <= 50 * tol * sc, (k, a[k], b[k])
+    small = 1e-4 if dtype == "float32" else 1e-10
+    assert np.all(a["poisson_residual"] < small) and np.all(b["poisson_residual"] < small)

@@ -286,6 +286,27 @@ def test_plane_wait_that_runs_out_stops_the_kernel_and_reports():
         assert torch.equal(a[k], b[k]), k
 
 
+@pytest.mark.parametrize("name", ["tunnel_wale_heat_smoke_f64", "ports_heat_f64", "tunnel_mid_f32", "periodic_vreman_f64"])
+def test_diagnostics_divergence_norm_matches_oracle(name):
+    """A diagnostics step (the solver's ``diag``: fused.py:480-482, physics.py:1303-1305): the sum
+    of squares of the last stage's projection right-hand side (minus the jets' and vents' mass
+    sources) against the oracle's, and the step itself still the reference's."""
+    from test_oracle_golden import _run
+    meta, plan, ins, arr = _plan_and_inputs(name)
+    div_sq = torch.zeros((), device="cuda", dtype=plan.dtype)
+    out = plan.step(ins["u0"], ins["v0"], ins["w0"], ins["t0"], theta0=ins.get("theta0"), dye0=ins["dye0"],
+                    div_sq=div_sq)
+    torch.cuda.synchronize()
+    _, _, outs = _run(name)
+    ref = outs[0].div_pre
+    assert ref > 0.0
+    tol = TOL[meta["dtype"]]
+    assert abs(float(div_sq) - ref) <= (1e-10 if meta["dtype"] == "float64" else 1e-4) * ref, (float(div_sq), ref)
+    for f in ("u", "v", "w", "p"):
+        assert _rel(out[f], arr["out1_" + f]) < tol, f
+    assert plan.status() == 0
+
+
 @pytest.mark.parametrize("name", ["tunnel_wale_heat_smoke_f64", "periodic_vreman_f64", "closed_central_cavity_f64"])
 def test_given_dt_matches_oracle(name):
     """dt passed in (the solver's fixed-dt and restart paths, core.py:765 ``dt=``): the step uses
