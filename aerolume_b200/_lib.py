@@ -135,19 +135,24 @@ class Ns2dConfig(C.Structure):
         ("gravity", C.c_double * 2), ("eta_t", C.c_double), ("theta_in", C.c_double),
         ("wall_mode", C.c_int32 * 4), ("wall_value", C.c_double * 4), ("diff_coef", C.c_double),
         ("n_temp", C.c_int32), ("n_flux", C.c_int32), ("has_ins", C.c_int32), ("has_vol", C.c_int32),
+        ("nfan", C.c_int32), ("heaters", C.c_int32), ("paint", C.c_int32), ("pid", C.c_int32),
     ]
 
 
 class Ns2dGeom(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in ("chi_u", "chi_v", "chi_c", "a_u", "a_v", "k_u", "k_v", "u_inlet",
                                           "dye_inlet", "chi_t", "a_t", "w_t", "ins_u", "ins_v", "q_skin", "w_f",
-                                          "vol_u", "vol_v", "nu", "eta", "kappa", "eta_t")]
+                                          "vol_u", "vol_v", "nu", "eta", "kappa", "eta_t", "fan_gu", "fan_gv",
+                                          "fan_phi", "fan_dir", "fan_value", "fan_width", "fan_kp", "fan_ki",
+                                          "fan_dpmax", "fan_isvel", "fan_isthrust", "u_floor", "heat", "heat_max",
+                                          "paint_c", "paint_u", "paint_v", "paint_wu", "paint_wv")]
 
 
 class Ns2dFields(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in ("u0", "v0", "t0", "dye0", "u", "v", "p", "t", "dt", "dye", "coeffs",
                                           "theta0", "theta", "heat", "theta_wall", "wall_heat", "heat_storage",
-                                          "flow_heat")]
+                                          "flow_heat", "dt_prev", "ctrl0", "ctrl", "fan_thrust", "fan_ud",
+                                          "paint_force")]
 
 
 class SmokeEmitter(C.Structure):

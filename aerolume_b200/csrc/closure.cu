@@ -814,43 +814,188 @@ __device__ __forceinline__ void max_atomic_f32(unsigned long long *dst, float v)
   atomicMax(dst, (unsigned long long)__double_as_longlong(d));
 }
 
-__global__ void __launch_bounds__(NTHREADS, 2) closure_nu_kernel(const __grid_constant__ ClosureStepParams P) {
+// The deployed pass keeps four 128-row pipelines in flight per SM inside one CTA of 512
+// threads: the four warpgroups share one copy of the weights (72 KB) and each owns its input
+// and activation operands (36 KB), its 128 tensor-memory columns (all 512 of the SM) and its
+// mbarrier, and synchronises only its own 128 threads (named barriers 1..4).  While one
+// warpgroup runs an epilogue the tensor cores run another's layer, so the latency of the
+// MMA -> epilogue -> MMA chain of a tile is hidden by the other three.  (Two CTAs of one
+// pipeline each held two weight copies and ran two pipelines per SM.)
+constexpr int NPIPE = 4;
+
+struct PipeSmem {
+  alignas(1024) unsigned char a0[ROWS * KIN * 2];
+  alignas(1024) unsigned char a[ROWS * NH * 2];
+};
+
+struct Fwd4Smem {
+  alignas(1024) unsigned char w1[NH * KIN * 2];
+  alignas(1024) unsigned char w2[NH * NH * 2];
+  alignas(1024) unsigned char w3[NH * NH * 2];
+  alignas(1024) unsigned char w4[KOUT * NH * 2];
+  PipeSmem pipe[NPIPE];
+  alignas(16) float b1[NH], b2[NH], b3[NH], b4[KOUT];
+  uint64_t bar[NPIPE];
+  uint32_t tmem;
+};
+
+// barrier of the 128 threads of warpgroup `wg` (named barrier 1 + wg; 0 is __syncthreads)
+__device__ __forceinline__ void wg_sync(int wg) { asm volatile("bar.sync %0, 128;" ::"r"(wg + 1) : "memory"); }
+// the same, true in every thread when `pred` holds in any of them
+__device__ __forceinline__ bool wg_sync_or(int wg, bool pred) {
+  uint32_t out;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 q, %1, 0;\n\tbar.red.or.pred p, %2, 128, q;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(out)
+      : "r"((uint32_t)pred), "r"(wg + 1)
+      : "memory");
+  return out != 0;
+}
+
+struct Pipe {
+  unsigned char *a0, *a;
+  uint64_t *bar;
+  uint32_t tmem;   // tensor-memory address of this pipeline's first column
+  int wg, r;       // warpgroup and the row (lane) of this thread
+};
+
+__device__ __forceinline__ void pipe_ready(const Pipe &q) {
+  fence_proxy_async();
+  tc_fence_before();
+  wg_sync(q.wg);
+  tc_fence_after();
+}
+
+// the pipeline's leader polls the MMA barrier (bounded); the other 127 threads sleep at the
+// named barrier instead of spending issue slots on polls of their own
+__device__ __forceinline__ bool pipe_wait(const Pipe &q, uint32_t &phase, int *status) {
+  const bool ok = q.r != 0 || mbar_wait_bounded(q.bar, phase, nullptr, 1 << 22);
+  phase ^= 1u;
+  const bool bad = wg_sync_or(q.wg, !ok);
+  if (bad && q.r == 0 && status) atomicOr(status, STATUS_TIMEOUT);
+  tc_fence_after();
+  return !bad;
+}
+
+__device__ __forceinline__ void pipe_epilogue(const Pipe &q, const float *bias) {
+  const uint32_t tl = q.tmem + ((uint32_t)(((threadIdx.x >> 5) & 3) * 32) << 16);
+#pragma unroll 1
+  for (int c0 = 0; c0 < NH; c0 += 32) {
+    float v[32];
+    tmem_ld32(tl + c0, v);
+#pragma unroll
+    for (int i = 0; i < 32; i += 4) {   // the bias in 16-byte loads
+      const float4 b = *reinterpret_cast<const float4 *>(bias + c0 + i);
+      v[i] += b.x;
+      v[i + 1] += b.y;
+      v[i + 2] += b.z;
+      v[i + 3] += b.w;
+    }
+#pragma unroll
+    for (int i = 0; i < 32; i += 8) {
+      __align__(16) __nv_bfloat162 h[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) h[k] = silu2(__floats2bfloat162_rn(v[i + 2 * k], v[i + 2 * k + 1]));
+      *reinterpret_cast<uint4 *>(q.a + kmaj(q.r, c0 + i, NH)) = *reinterpret_cast<const uint4 *>(h);
+    }
+  }
+}
+
+// the four layers of one tile of this pipeline (inputs in q.a0); false when a wait ran out
+__device__ __forceinline__ bool pipe_tile(const Pipe &q, const Fwd4Smem &S, uint32_t &phase, int *status, float *y) {
+  const bool lead = q.r == 0;
+  pipe_ready(q);
+  if (lead) {
+    gemm_issue(q.tmem, q.a0, S.w1, KIN, NH, false);
+    mma_commit(q.bar);
+  }
+  if (!pipe_wait(q, phase, status)) return false;
+  pipe_epilogue(q, S.b1);
+  pipe_ready(q);
+  if (lead) {
+    gemm_issue(q.tmem, q.a, S.w2, NH, NH, false);
+    mma_commit(q.bar);
+  }
+  if (!pipe_wait(q, phase, status)) return false;
+  pipe_epilogue(q, S.b2);
+  pipe_ready(q);
+  if (lead) {
+    gemm_issue(q.tmem, q.a, S.w3, NH, NH, false);
+    mma_commit(q.bar);
+  }
+  if (!pipe_wait(q, phase, status)) return false;
+  pipe_epilogue(q, S.b3);
+  pipe_ready(q);
+  if (lead) {
+    gemm_issue(q.tmem, q.a, S.w4, NH, KOUT, false);
+    mma_commit(q.bar);
+  }
+  if (!pipe_wait(q, phase, status)) return false;
+  tmem_ld16(q.tmem + ((uint32_t)(((threadIdx.x >> 5) & 3) * 32) << 16), y);
+#pragma unroll
+  for (int i = 0; i < KOUT; ++i) y[i] += S.b4[i];
+  tc_fence_before();
+  return true;
+}
+
+__global__ void __launch_bounds__(NPIPE * ROWS, 1) closure_nu_kernel(const __grid_constant__ ClosureStepParams P) {
   pdl_wait();
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  FwdSmem &S = *reinterpret_cast<FwdSmem *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-  fwd_setup(S, P.W);
+  Fwd4Smem &S = *reinterpret_cast<Fwd4Smem *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  // weights, biases, barriers and all 512 tensor-memory columns, for the whole CTA
+  load_w(S.w1, P.W.w1, NH, NIN, NH, KIN);
+  load_w(S.w2, P.W.w2, NH, NH, NH, NH);
+  load_w(S.w3, P.W.w3, NH, NH, NH, NH);
+  load_w(S.w4, P.W.w4, NOUT, NH, KOUT, NH);
+  for (int e = threadIdx.x; e < NH; e += blockDim.x) {
+    S.b1[e] = P.W.b1[e];
+    S.b2[e] = P.W.b2[e];
+    S.b3[e] = P.W.b3[e];
+  }
+  for (int e = threadIdx.x; e < KOUT; e += blockDim.x) S.b4[e] = e < NOUT ? P.W.b4[e] : 0.f;
+  if (threadIdx.x < 32) tmem_alloc(&S.tmem, NPIPE * NH);
+  if (threadIdx.x == 0) {
+    for (int w = 0; w < NPIPE; ++w) mbar_init(&S.bar[w], 1);
+    mbar_fence_init();
+  }
+  fence_proxy_async();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const int wg = threadIdx.x / ROWS;
+  const Pipe q{S.pipe[wg].a0, S.pipe[wg].a, &S.bar[wg], S.tmem + (uint32_t)(wg * NH), wg, (int)(threadIdx.x % ROWS)};
   uint32_t phase = 0;
   bool ok = true;
   const int64_t total = P.plane;
   const int64_t ntiles = (total + ROWS - 1) / ROWS;
   float mx = 0.f;
   unsigned long long n_eval = 0, n_wale = 0;
-  for (int64_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-    const int64_t e = t * ROWS + threadIdx.x;
+  for (int64_t t = (int64_t)blockIdx.x * NPIPE + wg; t < ntiles && ok; t += (int64_t)gridDim.x * NPIPE) {
+    const int64_t e = t * ROWS + q.r;
     const int i = (int)(e % P.pitch);
     const bool cell = e < total && i < P.nxp;
     float g[8], f[NIN], fac = 0.f;
     Grad G;
     bool use = false;
     if (cell) {
-      for (int q = 0; q < 8; ++q) g[q] = P.grad[q * P.plane + e];
+      for (int c = 0; c < 8; ++c) g[c] = P.grad[c * P.plane + e];
       fac = P.grad[8 * P.plane + e];
       use = features(g, f, G);
-      for (int q = 0; q < NIN; ++q) use = use && f[q] >= P.N.in_lo[q] && f[q] <= P.N.in_hi[q];
+      for (int c = 0; c < NIN; ++c) use = use && f[c] >= P.N.in_lo[c] && f[c] <= P.N.in_hi[c];
     }
     float xin[KIN];
-    for (int q = 0; q < KIN; ++q) xin[q] = (use && q < NIN) ? (f[q] - P.N.in_mean[q]) / P.N.in_std[q] : 0.f;
-    store8(S.a0, threadIdx.x, 0, KIN, xin);
-    store8(S.a0, threadIdx.x, 8, KIN, xin + 8);
+    for (int c = 0; c < KIN; ++c) xin[c] = (use && c < NIN) ? (f[c] - P.N.in_mean[c]) / P.N.in_std[c] : 0.f;
+    store8(q.a0, q.r, 0, KIN, xin);
+    store8(q.a0, q.r, 8, KIN, xin + 8);
     float y[KOUT];
-    ok = fwd_tile(S, phase, P.status, y, nullptr, nullptr, nullptr);
+    ok = pipe_tile(q, S, phase, P.status, y);
     if (!ok || !cell) continue;
     ++n_eval;
     float nut = P.nu[e];
     if (use) {
       const float sc = P.delta * P.delta * G.g2;
       float tau[NOUT];
-      for (int q = 0; q < NOUT; ++q) tau[q] = sc * fmaf(y[q], P.N.out_std[q], P.N.out_mean[q]);
+      for (int c = 0; c < NOUT; ++c) tau[c] = sc * fmaf(y[c], P.N.out_std[c], P.N.out_mean[c]);
       const float eps = -((tau[0] * G.S[0][0] + tau[1] * G.S[1][1] + tau[2] * G.S[2][2]) +
                           2.f * ((tau[3] * G.S[0][1] + tau[4] * G.S[0][2]) + tau[5] * G.S[1][2]));
       if (eps > 0.f && isfinite(eps)) {
@@ -863,7 +1008,12 @@ __global__ void __launch_bounds__(NTHREADS, 2) closure_nu_kernel(const __grid_co
     if (!use) ++n_wale;
     mx = (nut > mx || nut != nut) ? nut : mx;
   }
-  fwd_teardown(S, phase, ok);
+  // a pipeline that gave up waits (bounded) for its last MMA before the memory is freed
+  if (!ok) mbar_wait_bounded(q.bar, phase, nullptr, 1 << 22);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (threadIdx.x < 32) tmem_free(S.tmem, NPIPE * NH);
   // block maximum and counts
   for (int o = 16; o > 0; o >>= 1) {
     const float other = __shfl_xor_sync(0xffffffffu, mx, o);
@@ -902,6 +1052,7 @@ constexpr int64_t OFF_W1 = 0, OFF_B1 = 1280, OFF_W2 = 1408, OFF_B2 = 17792, OFF_
 static_assert(NPARAM == AERO_CLOSURE_NPARAM, "parameter layout");
 
 constexpr size_t FWD_SMEM = sizeof(FwdSmem) + 1024, BWD_SMEM = sizeof(BwdSmem) + 1024;
+constexpr size_t FWD4_SMEM = sizeof(Fwd4Smem) + 1024;
 
 MlpWeights weights_of(const float *p, const void *pb) {
   const auto *b = static_cast<const __nv_bfloat16 *>(pb);
@@ -934,7 +1085,7 @@ int prepare(int *nsm) {
     AERO_CUDA_TRY(cudaFuncSetAttribute(mlp_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FWD_SMEM));
     AERO_CUDA_TRY(
         cudaFuncSetAttribute(mlp_train_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FWD_SMEM));
-    AERO_CUDA_TRY(cudaFuncSetAttribute(closure_nu_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FWD_SMEM));
+    AERO_CUDA_TRY(cudaFuncSetAttribute(closure_nu_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FWD4_SMEM));
     AERO_CUDA_TRY(
         cudaFuncSetAttribute(mlp_train_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)BWD_SMEM));
     AERO_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -981,8 +1132,8 @@ int aero_host::closure_nu(const AeroClosureModel *m, const float *grad, int64_t 
   const int64_t tiles = (plane + ROWS - 1) / ROWS;
   // two CTAs per SM (shared memory and tensor memory allow it): one CTA's epilogue runs
   // while the other's MMAs do
-  const int grid = (int)std::min<int64_t>(tiles, 2 * (int64_t)nsm);
-  AERO_CUDA_TRY(aero::launch_k(closure_nu_kernel, grid, NTHREADS, FWD_SMEM, s, P));
+  const int grid = (int)std::min<int64_t>((tiles + NPIPE - 1) / NPIPE, (int64_t)nsm);   // one CTA per SM
+  AERO_CUDA_TRY(aero::launch_k(closure_nu_kernel, grid, NPIPE * ROWS, FWD4_SMEM, s, P));
   return AERO_OK;
 }
 

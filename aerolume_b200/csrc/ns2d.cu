@@ -133,9 +133,19 @@ struct Dt2dThermal {
   double kappa, inv_prt, two_over_h, diff_over_h2, abs_ri, cfl, h;
 };
 
+// placed physics in the step bound (physics.py:851-884): fans (and jets) put their speed
+// scale u_floor into the CFL bound and the temperature bound; heaters add the two bounds of a
+// parcel heated from rest (heat_max > 0: present)
+template <typename T>
+struct Dt2dPlaced {
+  int fans;
+  T u_floor, heat_max;
+};
+
 template <typename T, bool HEAT>
 __device__ __forceinline__ T dt2d_value(int mode, const T *dt_in, double dt_fixed, const unsigned long long *bits,
-                                        double cfl_h, double nu, double visc_h2, int les, const Dt2dThermal &th) {
+                                        double cfl_h, double nu, double visc_h2, int les, const Dt2dThermal &th,
+                                        const Dt2dPlaced<T> &pl = Dt2dPlaced<T>{0, T(0), T(-1)}) {
   if (mode == 2) return *dt_in;
   if (mode == 1) return T(dt_fixed);
   const T usum = T(as_double(bits[SC_MAXU])) + T(as_double(bits[SC_MAXV]));
@@ -146,9 +156,14 @@ __device__ __forceinline__ T dt2d_value(int mode, const T *dt_in, double dt_fixe
   const T nut = les ? T(nu) + nut_max : T(nu);
   const T dv = T(visc_h2) / nut;
   dt = dv < dt ? dv : dt;
+  if (pl.fans) {
+    const T uf = pl.u_floor > T(1e-6) ? pl.u_floor : T(1e-6);
+    const T l0 = T(cfl_h) / uf;
+    dt = l0 < dt ? l0 : dt;
+  }
   if (HEAT && th.on) {
     const T kap = les ? T(th.kappa) + nut_max * T(th.inv_prt) : T(th.kappa);
-    const T speed = usum > T(0) || usum != usum ? usum : T(0);
+    const T speed = usum > pl.u_floor || usum != usum ? usum : pl.u_floor;
     const T rate = speed * T(th.two_over_h) + kap * T(th.diff_over_h2);
     const T l1 = T(1) / rate;
     dt = l1 < dt ? l1 : dt;
@@ -156,6 +171,15 @@ __device__ __forceinline__ T dt2d_value(int mode, const T *dt_in, double dt_fixe
     acc = acc > T(1e-12) || acc != acc ? acc : T(1e-12);
     const T l2 = T(th.cfl) * sqrt(T(th.h) / acc);
     dt = l2 < dt ? l2 : dt;
+    if (pl.heat_max >= T(0)) {
+      const T sm = pl.heat_max > T(1e-12) ? pl.heat_max : T(1e-12);
+      const T l3 = T(1) / sm;
+      dt = l3 < dt ? l3 : dt;
+      T den = T(th.abs_ri) * sm;
+      den = den > T(1e-12) ? den : T(1e-12);
+      const T l4 = pow(T(6.0 * th.cfl * th.h) / den, T(1.0 / 3.0));
+      dt = l4 < dt ? l4 : dt;
+    }
   }
   return dt;
 }
@@ -198,6 +222,14 @@ struct StageParams {
   const unsigned long long *dt_bits;
   double dt_fixed, dt_cfl_h, dt_nu, dt_visc_h2;
   T *dt_store;
+  // placed physics (PLACED instantiations only): the fans' forces per unit thrust and this
+  // step's thrusts (core.py:875-882); the paint layer's implicit penalisation after the bodies,
+  // its force weights and the paint's per-block impulse sums [u, v] of this stage
+  // (physics.py:675-683, core.py:807-811)
+  int nfan;
+  const T *fan_gu, *fan_gv, *fan_thrust;
+  const T *paint_u, *paint_v, *paint_wu, *paint_wv;
+  double *paint_part;
 };
 
 // One RK stage of the u- and v-faces of a 32 x 8 tile; NU_ONLY: only the maximum eddy
@@ -208,7 +240,7 @@ struct StageParams {
 // The body takes its tile (bx, by) of a gx-wide grid and its thread tid (0 .. NT-1)
 // explicitly: stage2d_kernel runs it as one launch per instance, the batched sweep's
 // persistent kernel (sweep2d.cu) as one work item among every instance's tiles.
-template <typename T, bool NU_ONLY, bool HEAT, bool NC = true>
+template <typename T, bool NU_ONLY, bool HEAT, bool NC = true, bool PLACED = false>
 __device__ __forceinline__ void stage2d_body(const StageParams<T> &P, int bx, int by, int gx, int tid_) {
   __shared__ T U[UY][UX];
   __shared__ T V[VY][VX];
@@ -322,6 +354,7 @@ __device__ __forceinline__ void stage2d_body(const StageParams<T> &P, int bx, in
   const T k_pen = bdt / eta;
   const bool wblock = P.has_win && P.nbody > 0;
   double fq[4] = {0.0, 0.0, 0.0, 0.0};  // this thread's force sums of body `bsel`
+  double pimp = 0.0, pimp_v = 0.0;      // this thread's paint impulse (weighted) of u and v faces
   // ---- u-faces (j, i) and, for the last column, (j, nx)
   auto u_face = [&](int fi, T &out, bool &pen, T &du, int &widx, T &sh) {
     const int r = j - j0 + 2, c = fi - i0 + 2;
@@ -343,6 +376,12 @@ __device__ __forceinline__ void stage2d_body(const StageParams<T> &P, int bx, in
       if (fi == 0) lu = T(0);
       if (fi == nx) lu = P.closed ? T(0) : (row[c - 1] - row[c]) * P.inv_h;
     }
+    if (PLACED && P.nfan) {   // + sum_f thrust_f g_f (physics.py:671-672, core.py:880-882)
+      const size_t gg = (size_t)j * (nx + 1) + fi, nfu = (size_t)ny * (nx + 1);
+      T ff = P.fan_thrust[0] * P.fan_gu[gg];
+      for (int q = 1; q < P.nfan; ++q) ff = ff + P.fan_thrust[q] * P.fan_gu[q * nfu + gg];
+      lu = lu + ff;
+    }
     const T up = row[c];
     const size_t g = (size_t)j * (nx + 1) + fi;
     T uh = (P.a == T(0) ? up : lerp_t<T>(up, P.u0[g], P.a)) + lu * bdt;
@@ -362,6 +401,11 @@ __device__ __forceinline__ void stage2d_body(const StageParams<T> &P, int bx, in
       uh = un;
       pen = true;
     }
+    if (PLACED && P.paint_u) {   // the paint, after the bodies: (u + k * 0) / (1 + k chi)
+      const T pu = P.paint_u[g], un = uh / (T(1) + k_pen * pu);
+      pimp += (double)((un - uh) * P.paint_wu[g]) * (double)P.w;
+      uh = un;
+    }
     if (HEAT && P.buoy_u) {  // face average of theta (0 on boundary faces of a bounded domain)
       T tf;
       const size_t tr = (size_t)j * nx;
@@ -370,6 +414,7 @@ __device__ __forceinline__ void stage2d_body(const StageParams<T> &P, int bx, in
       const T fu = tf * P.ri_gx;
       uh = uh + bdt * fu;
       if (pen) sh = fu * (P.vol_u ? P.vol_u[widx] : P.chi_u[widx]) * (bdt * P.w);
+      if (PLACED && P.paint_u) pimp += (double)((fu * P.paint_u[g]) * P.paint_wu[g]) * (double)(bdt * P.w);
     }
     out = uh;
   };
@@ -390,6 +435,12 @@ __device__ __forceinline__ void stage2d_body(const StageParams<T> &P, int bx, in
       lv = lv + (((TXY[cr - 1][i - i0 + 1] - TXY[cr - 1][i - i0]) + TYY[cr][cc]) - TYY[cr - 1][cc]) * P.inv_h;
     }
     if (!P.periodic && (fj == 0 || fj == ny)) lv = T(0);
+    if (PLACED && P.nfan) {
+      const size_t gg = (size_t)fj * nx + i, nfv = (size_t)(ny + 1) * nx;
+      T ff = P.fan_thrust[0] * P.fan_gv[gg];
+      for (int q = 1; q < P.nfan; ++q) ff = ff + P.fan_thrust[q] * P.fan_gv[q * nfv + gg];
+      lv = lv + ff;
+    }
     const T vp = row[c];
     const size_t g = (size_t)fj * nx + i;
     T vh = (P.a == T(0) ? vp : lerp_t<T>(vp, P.v0[g], P.a)) + lv * bdt;
@@ -401,6 +452,11 @@ __device__ __forceinline__ void stage2d_body(const StageParams<T> &P, int bx, in
       vh = vn;
       pen = true;
     }
+    if (PLACED && P.paint_v) {
+      const T pv = P.paint_v[g], vn = vh / (T(1) + k_pen * pv);
+      pimp_v += (double)((vn - vh) * P.paint_wv[g]) * (double)P.w;
+      vh = vn;
+    }
     if (HEAT && P.buoy_v) {
       T tf;
       if (fj > 0 && fj < ny) tf = T(0.5) * (P.thp[(size_t)fj * nx + i] + P.thp[(size_t)(fj - 1) * nx + i]);
@@ -408,6 +464,7 @@ __device__ __forceinline__ void stage2d_body(const StageParams<T> &P, int bx, in
       const T fv = tf * P.ri_gy;
       vh = vh + bdt * fv;
       if (pen) sh = fv * (P.vol_v ? P.vol_v[widx] : P.chi_v[widx]) * (bdt * P.w);
+      if (PLACED && P.paint_v) pimp_v += (double)((fv * P.paint_v[g]) * P.paint_wv[g]) * (double)(bdt * P.w);
     }
     out = vh;
   };
@@ -481,12 +538,28 @@ __device__ __forceinline__ void stage2d_body(const StageParams<T> &P, int bx, in
       P.partials[(size_t)(by * gx + bx) * nq + tid] = s;
     }
   }
+  // ---- the paint's impulse sums of this block (per warp, then in order)
+  if (PLACED && P.paint_part) {
+    __shared__ double pred[NT / 32][2];
+    const int warp = tid >> 5, lane = tid & 31;
+    const double a = warp_sum(pimp), b = warp_sum(pimp_v);
+    if (lane == 0) {
+      pred[warp][0] = a;
+      pred[warp][1] = b;
+    }
+    __syncthreads();
+    if (tid < 2) {
+      double t = 0.0;
+      for (int wv = 0; wv < NT / 32; ++wv) t += pred[wv][tid];
+      P.paint_part[(size_t)(by * gx + bx) * 2 + tid] = t;
+    }
+  }
 }
 
-template <typename T, bool NU_ONLY, bool HEAT>
+template <typename T, bool NU_ONLY, bool HEAT, bool PLACED = false>
 __global__ void __launch_bounds__(NT) stage2d_kernel(const __grid_constant__ StageParams<T> P) {
   aero::pdl_wait();
-  stage2d_body<T, NU_ONLY, HEAT>(P, blockIdx.x, blockIdx.y, gridDim.x, threadIdx.y * TX + threadIdx.x);
+  stage2d_body<T, NU_ONLY, HEAT, true, PLACED>(P, blockIdx.x, blockIdx.y, gridDim.x, threadIdx.y * TX + threadIdx.x);
 }
 
 // u <- uh - grad psi (core.py:643-660); one thread per cell column, the thread of the last
@@ -558,6 +631,7 @@ struct DyeParams {
   T *c;
   int has_win, win[4];
   const T *chi_c;
+  const T *paint_c;                  // painted cells hold no smoke (core.py:958-959; NULL: none)
 };
 
 template <typename T>
@@ -595,7 +669,135 @@ __global__ void dye2d_kernel(const __grid_constant__ DyeParams<T> P) {
     const T chi = P.chi_c[(size_t)(j - P.win[0]) * (P.win[3] - P.win[2]) + (i - P.win[2])];
     out = out * (chi <= T(0.5) ? T(1) : T(0));
   }
+  if (P.paint_c) out = out * (P.paint_c[(size_t)j * nx + i] <= T(0.5) ? T(1) : T(0));
   P.c[(size_t)j * nx + i] = out;
+}
+
+// ---------------------------------------------------------------------------------------
+// placed physics before the first stage: the step (with the fans' and heaters' bounds and the
+// PID controller) and the fans' PI controllers (core.py:856-878, physics.py:640-672, 851-884,
+// diagnostics.py:104-124), one block
+// ---------------------------------------------------------------------------------------
+
+template <typename T>
+struct Control2dParams {
+  int nx, ny, nfan, pid, dt_mode, les, heat;
+  const T *dt_in;
+  double dt_fixed, cfl_h, nu, visc_h2;
+  const unsigned long long *bits;
+  const T *live_nu, *live_kappa;
+  Dt2dThermal th;
+  const T *u_floor, *heat_max;        // 0-d (heat_max NULL: no heaters)
+  const T *dt_prev, *ctrl0;           // the previous step (<= 0: first) and the controller memory
+  T *ctrl;                            // new memory (2 + 2 nfan)
+  const T *u0, *v0;
+  const T *fan_phi, *fan_dir, *fan_value, *fan_width, *fan_kp, *fan_ki, *fan_dpmax, *fan_isvel, *fan_isthrust;
+  T *thrust, *thrust_out, *ud_out;    // this step's thrusts (for the stages), the reported ones, disc speeds
+  T *dt_out;
+};
+
+constexpr double PID_TARGET = 0.9, PID_KP = 0.10, PID_KI = 0.25, PID_KD = 0.02, PID_MAX_GROWTH = 1.03;
+
+template <typename T, bool HEAT>
+__global__ void __launch_bounds__(1024) control2d_kernel(const __grid_constant__ Control2dParams<T> P) {
+  aero::pdl_wait();
+  __shared__ double red[32][2 * AERO_MAX_FANS];
+  const int tid = threadIdx.x, nx = P.nx, ny = P.ny;
+  const size_t nc = (size_t)nx * ny;
+  // disc velocities: the footprint-weighted cell-centred velocity of every fan, each thread a
+  // fixed set of cells, then the warps and the block in order
+  for (int f = 0; f < P.nfan; ++f) {
+    const T *phi = P.fan_phi + (size_t)f * nc;
+    double su = 0.0, sv = 0.0;
+    for (size_t e = tid; e < nc; e += blockDim.x) {
+      const T wgt = phi[e];
+      if (wgt != T(0)) {
+        const int j = (int)(e / nx), i = (int)(e - (size_t)j * nx);
+        const T uc = T(0.5) * (P.u0[(size_t)j * (nx + 1) + i + 1] + P.u0[(size_t)j * (nx + 1) + i]);
+        const T vc = T(0.5) * (P.v0[(size_t)(j + 1) * nx + i] + P.v0[(size_t)j * nx + i]);
+        su += (double)(wgt * uc);
+        sv += (double)(wgt * vc);
+      }
+    }
+    su = warp_sum(su);
+    sv = warp_sum(sv);
+    if ((tid & 31) == 0) {
+      red[tid >> 5][2 * f] = su;
+      red[tid >> 5][2 * f + 1] = sv;
+    }
+  }
+  __syncthreads();
+  if (tid != 0) return;
+  T dt;
+  if (P.dt_mode == 2) {
+    dt = *P.dt_in;
+  } else if (P.dt_mode == 1) {
+    dt = T(P.dt_fixed);
+  } else {
+    const Dt2dPlaced<T> pl{P.nfan > 0, *P.u_floor, P.heat_max ? *P.heat_max : T(-1)};
+    Dt2dThermal th = P.th;
+    if (HEAT && P.live_kappa) th.kappa = (double)*P.live_kappa;
+    dt = dt2d_value<T, HEAT>(0, nullptr, 0.0, P.bits, P.cfl_h, P.live_nu ? (double)*P.live_nu : P.nu, P.visc_h2,
+                             P.les, th, pl);
+  }
+  const int nctrl = 2 + 2 * P.nfan;
+  if (P.ctrl)
+    for (int q = 0; q < nctrl; ++q) P.ctrl[q] = P.ctrl0[q];
+  if (P.pid && P.dt_mode == 0) {   // e = log(target / dt_prev); the first step takes the target
+    const T target = T(PID_TARGET) * dt;
+    const T prev = *P.dt_prev;
+    const bool first = prev <= T(0);
+    const T safe = first ? target : prev;
+    T e = log(target / safe);
+    const T e1 = P.ctrl0[0], e2 = P.ctrl0[1];
+    T step = (T(PID_KI) * e + T(PID_KP) * (e - e1)) + T(PID_KD) * ((e - T(2) * e1) + e2);
+    const T cap = T(log(PID_MAX_GROWTH));
+    step = step < cap ? step : cap;
+    const T grown = safe * exp(step);
+    dt = first ? target : (grown < dt ? grown : dt);
+    P.ctrl[0] = first ? T(0) : e;
+    P.ctrl[1] = e1;
+  }
+  *P.dt_out = dt;
+  for (int f = 0; f < P.nfan; ++f) {
+    double ua = 0.0, va = 0.0;
+    for (int w = 0; w < 32; ++w) {
+      ua += red[w][2 * f];
+      va += red[w][2 * f + 1];
+    }
+    const T ud = T(ua) * P.fan_dir[2 * f] + T(va) * P.fan_dir[2 * f + 1];
+    const T value = P.fan_value[f], width = P.fan_width[f], ki = P.fan_ki[f], dpmax = P.fan_dpmax[f];
+    const T err = value - ud, ilim = dpmax / ki;
+    T integ = P.ctrl0[2 + 2 * f] + (err * dt) * P.fan_isvel[f];
+    integ = integ < ilim ? integ : ilim;
+    integ = integ > -ilim ? integ : -ilim;
+    T dp = P.fan_kp[f] * err + ki * integ;
+    dp = dp < dpmax ? dp : dpmax;
+    dp = dp > -dpmax ? dp : -dpmax;
+    const T fixed = P.fan_isthrust[f] > T(0) ? value : value * width;
+    const T thrust = P.fan_isvel[f] > T(0) ? dp * width : fixed;
+    P.thrust[f] = thrust;
+    if (P.thrust_out) P.thrust_out[f] = thrust;
+    if (P.ud_out) P.ud_out[f] = ud;
+    if (P.ctrl) {
+      P.ctrl[2 + 2 * f] = integ;
+      P.ctrl[3 + 2 * f] = thrust / width;
+    }
+  }
+}
+
+// The painted obstacles' force coefficients [Cd, Cl] from the stages' impulse sums
+// (core.py:1001-1002): one warp per component, a fixed lane order.
+template <typename T>
+__global__ void paint_force2d_kernel(const double *__restrict__ part, int nblocks, double h2, double force_ref,
+                                     const T *dt, T *out) {
+  aero::pdl_wait();
+  const int c = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (c >= 2) return;
+  double s = 0.0;
+  for (int q = lane; q < 3 * nblocks; q += 32) s += part[(size_t)q * 2 + c];
+  s = warp_sum(s);
+  if (lane == 0) out[c] = T(s) * (T(-h2) / ((*dt * T(0.5)) * T(force_ref)));
 }
 
 
@@ -623,6 +825,9 @@ struct ThetaParams {
   const T *dt;
   double *heat_part;          // (nblocks, n_temp) of this stage
   double *rep_part;           // last stage: (nblocks, 2 + n_flux) = sum theta, sum theta0, wall weights
+  // placed physics: the heaters' density (ny, nx), added after the diffusion (physics.py:721-722),
+  // and the paint's face fractions, which scale the face diffusivity by 1 - chi (:715-717)
+  const T *heat, *paint_u, *paint_v;
 };
 
 // theta at (j, i) with the ghosts of scalar.py:63-78: periodic wrap; else the first / last
@@ -664,6 +869,7 @@ __device__ __forceinline__ T kx_face(const ThetaParams<T> &P, int j, int f) {
     else avg = __ldg(row + (f == 0 ? 0 : nx - 1)) * P.inv_prt;
     k = kap + avg;
   }
+  if (P.paint_u) k = k * (T(1) - __ldg(P.paint_u + (size_t)j * (nx + 1) + f));   // painted solids insulate
   if (P.ins_u && j >= P.win[0] && j < P.win[1] && f >= P.win[2] && f <= P.win[3])
     k = k * __ldg(P.ins_u + (size_t)(j - P.win[0]) * (P.win[3] - P.win[2] + 1) + (f - P.win[2]));
   return k;
@@ -684,6 +890,7 @@ __device__ __forceinline__ T ky_face(const ThetaParams<T> &P, int f, int i) {
       avg = __ldg(P.nut + (size_t)(f == 0 ? 0 : ny - 1) * nx + i) * P.inv_prt;
     k = kap + avg;
   }
+  if (P.paint_v) k = k * (T(1) - __ldg(P.paint_v + (size_t)f * nx + i));
   if (P.ins_v && f >= P.win[0] && f <= P.win[1] && i >= P.win[2] && i < P.win[3])
     k = k * __ldg(P.ins_v + (size_t)(f - P.win[0]) * (P.win[3] - P.win[2]) + (i - P.win[2]));
   return k;
@@ -751,6 +958,7 @@ __global__ void __launch_bounds__(NT) theta2d_kernel(const __grid_constant__ The
     };
     const T ld = (((dfx(i) - dfx(i + 1)) + dfy(j)) - dfy(j + 1)) * P.inv_h;
     lt = lt + ld;
+    if (P.heat) lt = lt + __ldg(P.heat + (size_t)j * nx + i);
     const bool inwin = P.has_win && j >= P.win[0] && j < P.win[1] && i >= P.win[2] && i < P.win[3];
     const size_t widx = inwin ? (size_t)(j - P.win[0]) * (P.win[3] - P.win[2]) + (i - P.win[2]) : 0;
     const size_t wsz = (size_t)(P.win[1] - P.win[0]) * (P.win[3] - P.win[2]);
@@ -1240,6 +1448,7 @@ struct AeroNs2dPlan {
   size_t nu, nv, nc;          // element counts of u, v and cells
   size_t off_uh, off_vh, off_up, off_vp, off_pa, off_small, off_scalars, off_zero, off_partials, total;
   size_t off_nut, off_tb0, off_tb1, off_hpart, off_rpart, off_upf, off_vpf;  // heat transfer only
+  size_t off_thrust = 0, off_ppart = 0;   // placed physics: the fans' thrusts, the paint's impulse sums
   // heat transfer: each theta stage runs on a side stream, forked after its stage kernel and
   // joined before the next one, so it overlaps the stage's pressure solve
   cudaStream_t side = nullptr;
@@ -1420,9 +1629,27 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
   S.eta = T(c.eta);
   S.nbody = has_win ? c.nbody : 0;
   const dim3 grid(p->gx, p->gy), block(TX, TY);
-  if (rec && (!std::is_same<T, float>::value || les || thermal || c.dye || dt_mode != 0))
-    return set_error(AERO_EUNSUPPORTED, "the persistent sweep runs FP32 plans without LES, heat transfer or dye, "
-                                        "with the CFL time step");
+  const bool placed = c.nfan || c.pid || c.paint || c.heaters;
+  if (rec && (!std::is_same<T, float>::value || les || thermal || c.dye || dt_mode != 0 || placed))
+    return set_error(AERO_EUNSUPPORTED, "the persistent sweep runs FP32 plans without LES, heat transfer, dye or "
+                                        "placed physics, with the CFL time step");
+  if ((c.nfan || c.pid) && (!f->ctrl0 || !f->ctrl || (c.pid && !f->dt_prev)))
+    return set_error(AERO_EINVAL, "fans and the PID step need the controller memory (ctrl0, ctrl) and dt_prev");
+  // fans, the PID controller and the heaters' bounds act on the step before the first stage:
+  // the control kernel computes dt (and the thrusts) and the stages read it
+  const bool control = c.nfan || (dt_mode == 0 && (c.pid || c.heaters));
+  if (placed) {
+    S.nfan = c.nfan;
+    S.fan_gu = static_cast<const T *>(g->fan_gu);
+    S.fan_gv = static_cast<const T *>(g->fan_gv);
+    S.fan_thrust = c.nfan ? reinterpret_cast<const T *>(ws + p->off_thrust) : nullptr;
+    if (c.paint) {
+      S.paint_u = static_cast<const T *>(g->paint_u);
+      S.paint_v = static_cast<const T *>(g->paint_v);
+      S.paint_wu = static_cast<const T *>(g->paint_wu);
+      S.paint_wv = static_cast<const T *>(g->paint_wv);
+    }
+  }
   if (dt_mode == 0) {
     aero::MaxJobs<T> J{};
     J.job[0] = {u0, p->nu, bits + aero::SC_MAXU};
@@ -1465,6 +1692,56 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
   S.dt_store = small;
   if (thermal && dt_mode == 0)
     S.dt_th = Dt2dThermal{1, c.kappa, 1.0 / c.prt, 2.0 / c.h, c.diff_coef / (c.h * c.h), std::fabs(c.ri), c.cfl, c.h};
+  if (control) {
+    Control2dParams<T> K{};
+    K.nx = nx;
+    K.ny = ny;
+    K.nfan = c.nfan;
+    K.pid = c.pid;
+    K.dt_mode = dt_mode;
+    K.les = les ? 1 : 0;
+    K.dt_in = static_cast<const T *>(dt_in);
+    K.dt_fixed = c.dt_fixed;
+    K.cfl_h = c.cfl * c.h;
+    K.nu = c.nu;
+    K.visc_h2 = 0.25 * c.h * c.h;
+    K.bits = bits;
+    K.live_nu = static_cast<const T *>(g->nu);
+    K.live_kappa = thermal ? static_cast<const T *>(g->kappa) : nullptr;
+    K.th = S.dt_th;
+    K.u_floor = static_cast<const T *>(g->u_floor);
+    K.heat_max = c.heaters ? static_cast<const T *>(g->heat_max) : nullptr;
+    K.dt_prev = static_cast<const T *>(f->dt_prev);
+    K.ctrl0 = static_cast<const T *>(f->ctrl0);
+    K.ctrl = static_cast<T *>(f->ctrl);
+    K.u0 = u0;
+    K.v0 = v0;
+    K.fan_phi = static_cast<const T *>(g->fan_phi);
+    K.fan_dir = static_cast<const T *>(g->fan_dir);
+    K.fan_value = static_cast<const T *>(g->fan_value);
+    K.fan_width = static_cast<const T *>(g->fan_width);
+    K.fan_kp = static_cast<const T *>(g->fan_kp);
+    K.fan_ki = static_cast<const T *>(g->fan_ki);
+    K.fan_dpmax = static_cast<const T *>(g->fan_dpmax);
+    K.fan_isvel = static_cast<const T *>(g->fan_isvel);
+    K.fan_isthrust = static_cast<const T *>(g->fan_isthrust);
+    K.thrust = c.nfan ? reinterpret_cast<T *>(ws + p->off_thrust) : nullptr;
+    K.thrust_out = static_cast<T *>(f->fan_thrust);
+    K.ud_out = static_cast<T *>(f->fan_ud);
+    K.dt_out = small;
+    if (!K.u_floor) return set_error(AERO_EINVAL, "placed physics needs the u_floor scalar");
+    if (c.nfan && !(K.fan_phi && K.fan_dir && K.fan_value && K.fan_width && K.fan_kp && K.fan_ki && K.fan_dpmax &&
+                    K.fan_isvel && K.fan_isthrust && S.fan_gu && S.fan_gv))
+      return set_error(AERO_EINVAL, "a fan array is missing");
+    if (c.heaters && !K.heat_max) return set_error(AERO_EINVAL, "heaters need heat_max");
+    if (thermal)
+      (void)aero::launch_k(control2d_kernel<T, true>, 1, 1024, 0, s, K);
+    else
+      (void)aero::launch_k(control2d_kernel<T, false>, 1, 1024, 0, s, K);
+    AERO_CUDA_TRY(cudaGetLastError());
+  }
+  if (c.paint && !(S.paint_u && S.paint_v && S.paint_wu && S.paint_wv && g->paint_c))
+    return set_error(AERO_EINVAL, "a paint array is missing");
   // heat transfer: buoyancy in the stage kernel, theta in its own kernel after it
   T *nutb = thermal ? reinterpret_cast<T *>(ws + p->off_nut) : nullptr;
   T *tb[2] = {thermal ? reinterpret_cast<T *>(ws + p->off_tb0) : nullptr,
@@ -1530,7 +1807,8 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
     P.b = T(RK[st][1]);
     P.w = T(RK[st][2]);
     P.partials = partials + (size_t)st * p->nblocks * std::max(p->nq, 1);
-    P.dt_here = st == 0;
+    P.dt_here = st == 0 && !control;
+    P.paint_part = c.paint ? reinterpret_cast<double *>(ws + p->off_ppart) + (size_t)st * p->nblocks * 2 : nullptr;
     const T *th_in = st == 0 ? static_cast<const T *>(f->theta0) : tb[(st - 1) % 2];
     if (thermal) {
       P.thp = th_in;
@@ -1544,7 +1822,10 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
         rec->ops.push_back(o);
       }
     } else {
-      if (thermal)
+      if (placed)
+        (void)(thermal ? aero::launch_k(stage2d_kernel<T, false, true, true>, grid, block, 0, s, P)
+                       : aero::launch_k(stage2d_kernel<T, false, false, true>, grid, block, 0, s, P));
+      else if (thermal)
         (void)aero::launch_k(stage2d_kernel<T, false, true>, grid, block, 0, s, P);
       else
         (void)aero::launch_k(stage2d_kernel<T, false, false>, grid, block, 0, s, P);
@@ -1560,6 +1841,9 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
       Q.b = P.b;
       Q.heat_part = reinterpret_cast<double *>(ws + p->off_hpart) + (size_t)st * p->nblocks * std::max(c.n_temp, 1);
       Q.rep_part = st == 2 ? reinterpret_cast<double *>(ws + p->off_rpart) : nullptr;
+      Q.heat = c.heaters ? static_cast<const T *>(g->heat) : nullptr;
+      Q.paint_u = c.paint ? static_cast<const T *>(g->paint_u) : nullptr;
+      Q.paint_v = c.paint ? static_cast<const T *>(g->paint_v) : nullptr;
       AERO_CUDA_TRY(cudaEventRecord(p->ev_fork[st], s));
       AERO_CUDA_TRY(cudaStreamWaitEvent(p->side, p->ev_fork[st], 0));
       (void)aero::launch_k(theta2d_kernel<T>, grid, block, 0, p->side, Q);
@@ -1661,6 +1945,7 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
     D.has_win = has_win;
     for (int q = 0; q < 4; ++q) D.win[q] = c.window[q];
     D.chi_c = static_cast<const T *>(g->chi_c);
+    D.paint_c = c.paint ? static_cast<const T *>(g->paint_c) : nullptr;
     (void)aero::launch_k(dye2d_kernel<T>, dim3((nx + 127) / 128, ny), 128, 0, s, D);
     AERO_CUDA_TRY(cudaGetLastError());
   }
@@ -1672,6 +1957,11 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
       rec->ops.push_back(o);
     }
     return AERO_OK;
+  }
+  if (c.paint && f->paint_force) {
+    (void)aero::launch_k(paint_force2d_kernel<T>, 1, 64, 0, s, (const double *)(ws + p->off_ppart), p->nblocks,
+                         c.h * c.h, c.force_ref, (const T *)small, static_cast<T *>(f->paint_force));
+    AERO_CUDA_TRY(cudaGetLastError());
   }
   (void)aero::launch_k(finalize2d_kernel<T>, 1, 256, 0, s, partials, p->nblocks, S.nbody, c.h, c.force_ref, small,
                                          static_cast<const T *>(f->t0), static_cast<T *>(f->t),
@@ -1719,6 +2009,9 @@ int aero_ns2d_plan_create(const AeroNs2dConfig *cfg, AeroNs2dPlan **plan) {
     if (!(c.prt > 0)) return set_error(AERO_EINVAL, "turbulent Prandtl number must be positive");
     if (c.n_temp && !(c.eta_t > 0)) return set_error(AERO_EINVAL, "eta_t must be positive");
   }
+  if (c.nfan < 0 || c.nfan > AERO_MAX_FANS)
+    return set_error(AERO_EUNSUPPORTED, "at most " + std::to_string(AERO_MAX_FANS) + " fans");
+  if (c.heaters && !c.thermal) return set_error(AERO_EINVAL, "heaters need heat transfer");
   auto *p = new AeroNs2dPlan();
   p->cfg = c;
   const size_t e = c.dtype == AERO_F64 ? 8 : 4;
@@ -1746,6 +2039,8 @@ int aero_ns2d_plan_create(const AeroNs2dConfig *cfg, AeroNs2dPlan **plan) {
   p->nblocks = p->gx * p->gy;
   p->nq = has_win ? 4 * c.nbody : 0;
   p->off_partials = take(sizeof(double) * 3 * (size_t)p->nblocks * std::max(p->nq, 1));
+  if (c.nfan) p->off_thrust = take((size_t)c.nfan * e);
+  if (c.paint) p->off_ppart = take(sizeof(double) * 3 * (size_t)p->nblocks * 2);
   if (c.thermal) {
     p->off_nut = take(p->nc * e);
     p->off_tb0 = take(p->nc * e);

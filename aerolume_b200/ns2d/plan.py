@@ -5,10 +5,10 @@ src/aerolume/solvers/ns2d/core.py:67-108 and geometry.py:160-182, or the contain
 :mod:`aerolume_b200.ns2d.types`), turns the boundary types into the ghost-cell rules of
 core.py:271-325, uploads the window masks once and owns the device workspace.  Heat
 transfer comes from ``thermal=`` (a :class:`~aerolume_b200.ns2d.types.Thermal2D`) or from the
-reference's ``ops.phys`` with ``geom.thermal`` when heat transfer is all it places; other
-placed physics (heat sources, fans, ports, paint, emitters, the PID step controller), the
-wall model and body forcing raise ``RuntimeError``: there is no fallback to a CPU or
-plain-torch path.
+reference's ``ops.phys`` with ``geom.thermal``; fans, heaters, painted obstacles and the PID
+step come from ``placed=`` (a :class:`~aerolume_b200.ns2d.types.Placed2D`) or from ``ops.phys``
+itself.  Jets and vents, smoke channels with emitters, the wall model and body forcing raise
+``RuntimeError``: there is no fallback to a CPU or plain-torch path.
 """
 from __future__ import annotations
 
@@ -20,6 +20,8 @@ import torch
 from .. import _lib
 from .._lib import ADV, F32, F64, GHOST, LES, MAX_BODIES, THETA2_MODE, check
 from .types import Thermal2D
+
+MAX_FANS = 4
 
 
 def _f(x) -> float:
@@ -60,18 +62,17 @@ def ghost_rules(ops):
     return ((ux, uy), (vx, vy))
 
 
-def thermal_from_physics(ph, geom) -> Thermal2D:
+def thermal_from_physics(ph, geom):
     """The heat transfer of the reference's 2D ``Physics`` (physics.py:291-345) and
-    ``geom.thermal``; raises when the physics places anything the B200 step does not run."""
-    others = [n for n, on in (("heat sources", getattr(ph, "heat", None) is not None),
-                              ("ports", bool(getattr(ph, "ports", None))), ("paint", bool(getattr(ph, "paint", False))),
-                              ("fans", int(getattr(ph, "nfan", 0) or 0) > 0),
-                              ("smoke groups", int(getattr(ph, "n_dye", 0) or 0) > 0 or bool(getattr(ph, "comb", False))),
-                              ("the PID step controller", bool(getattr(ph, "pid", False)))) if on]
+    ``geom.thermal`` (None when it has none); raises when the physics places anything the B200
+    step does not run (jets and vents, smoke channels with emitters)."""
+    others = [n for n, on in (("ports", bool(getattr(ph, "ports", None))),
+                              ("smoke groups", int(getattr(ph, "n_dye", 0) or 0) > 0 or bool(getattr(ph, "comb", False))))
+              if on]
     if others:
         raise RuntimeError("placed physics (" + ", ".join(others) + ") is not in the B200 2D step")
     if not getattr(ph, "thermal", False):
-        raise RuntimeError("placed physics without heat transfer is not in the B200 2D step")
+        return None
     tg = getattr(geom, "thermal", None)
     kw = {}
     if tg is not None and not geom.empty:
@@ -90,7 +91,7 @@ class Ns2dPlan:
     """Plan + device tensors for one 2D (ops, geom) configuration; ``dye`` turns on the dye
     update after each step, ``thermal`` (a :class:`Thermal2D`) heat transfer."""
 
-    def __init__(self, ops, geom, *, dye: bool = False, thermal=None, device=None):
+    def __init__(self, ops, geom, *, dye: bool = False, thermal=None, placed=None, device=None):
         self.device = torch.device(device) if device is not None else torch.device("cuda")
         if self.device.type != "cuda":
             raise RuntimeError("the B200 step runs on a CUDA device only (no CPU fallback)")
@@ -99,9 +100,10 @@ class Ns2dPlan:
         if self.device.index is None:
             self.device = torch.device("cuda", torch.cuda.current_device())
         if getattr(ops, "phys", None) is not None:
-            if thermal is not None:
-                raise RuntimeError("heat transfer comes either from ops.phys or from thermal=, not both")
+            if thermal is not None or placed is not None:
+                raise RuntimeError("placed physics comes either from ops.phys or from thermal= / placed=, not both")
             thermal = thermal_from_physics(ops.phys, geom)
+            placed = ops.phys
         if getattr(ops, "forcing", None) is not None:
             raise RuntimeError("a uniform body force (verification forcing) is not supported by the B200 step")
         if getattr(ops, "wall_model", False):
@@ -173,6 +175,11 @@ class Ns2dPlan:
             g.dye_inlet = up(d_in, (ny,)).data_ptr()
         if thermal is not None:
             self._thermal_config(cfg, g, thermal, up)
+        self.placed = placed
+        self.nfan = 0
+        self.pid = False
+        if placed is not None:
+            self._placed_config(cfg, g, placed, thermal is not None, up)
 
         def live(x):
             """The reference's 0-d device scalar itself (its set_reynolds fills it in place, so a
@@ -232,6 +239,51 @@ class Ns2dPlan:
                 g.vol_v = up(th.vol_v, (wy + 1, wx)).data_ptr()
         cfg.n_temp, cfg.n_flux = self.n_temp, self.n_flux
 
+    def _placed_config(self, cfg, g, pl, thermal, up):
+        """Fans, heaters, paint and the PID step (physics.py:70-140): the reference's tensors are
+        used in place when they already live on the device in the plan's dtype (a live paint
+        stroke or fan setting then reaches the next step), else uploaded."""
+        ny, nx = self.shape
+        dev, dt = self.device, self.dtype
+
+        def arr(x, shape):
+            if torch.is_tensor(x) and x.device == dev and x.dtype == dt and x.is_contiguous() and tuple(x.shape) == shape:
+                self._keep.append(x)
+                return x.data_ptr()
+            return up(x, shape).data_ptr()
+
+        nfan = int(getattr(pl, "nfan", 0) or 0)
+        if nfan > MAX_FANS:
+            raise RuntimeError(f"the B200 2D step supports at most {MAX_FANS} fans")
+        self.nfan = cfg.nfan = nfan
+        if nfan:
+            g.fan_gu = arr(pl.fan_gu, (nfan, ny, nx + 1))
+            g.fan_gv = arr(pl.fan_gv, (nfan, ny + 1, nx))
+            g.fan_phi = arr(pl.fan_phi, (nfan, ny, nx))
+            g.fan_dir = arr(pl.fan_dir, (nfan, 2))
+            for name in ("fan_value", "fan_width", "fan_kp", "fan_ki", "fan_dpmax", "fan_isvel", "fan_isthrust"):
+                setattr(g, name, arr(getattr(pl, name), (nfan,)))
+        g.u_floor = arr(getattr(pl, "u_floor", 0.0) if getattr(pl, "u_floor", None) is not None else 0.0, ())
+        if getattr(pl, "heat", None) is not None:
+            if not thermal:
+                raise RuntimeError("heaters need heat transfer")
+            cfg.heaters = 1
+            g.heat = arr(pl.heat, (ny, nx))
+            g.heat_max = arr(pl.heat_max, ())
+        if bool(getattr(pl, "paint", False)):
+            cfg.paint = 1
+            g.paint_c = arr(pl.paint_c, (ny, nx))
+            for name, shape in (("paint_u", (ny, nx + 1)), ("paint_v", (ny + 1, nx)), ("paint_wu", (ny, nx + 1)),
+                                ("paint_wv", (ny + 1, nx))):
+                setattr(g, name, arr(getattr(pl, name), shape))
+        self.pid = bool(getattr(pl, "pid", False))
+        cfg.pid = int(self.pid)
+
+    @property
+    def ctrl_size(self):
+        """Length of the controller memory (core.py State.ctrl): 0, or 2 + 2 nfan."""
+        return 2 + 2 * self.nfan if (self.pid or self.nfan) else 0
+
     def _stream(self):
         return C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
 
@@ -258,6 +310,13 @@ class Ns2dPlan:
             out.update(theta=torch.empty(ny, nx, **kw), heat=torch.zeros(self.n_temp, **d64),
                        theta_wall=torch.zeros(self.n_flux, **d64), wall_heat=torch.zeros(4, **d64),
                        heat_storage=torch.zeros(1, **d64), flow_heat=torch.zeros(2, **d64))
+        if self.ctrl_size:
+            out["ctrl"] = torch.zeros(self.ctrl_size, **kw)
+        if self.nfan:
+            out["fan_thrust"] = torch.zeros(self.nfan, **kw)
+            out["fan_ud"] = torch.zeros(self.nfan, **kw)
+        if self.cfg.paint:
+            out["paint_force"] = torch.zeros(2, **kw)
         return out
 
     def _check(self, name, t, shape):
@@ -266,11 +325,14 @@ class Ns2dPlan:
         if tuple(t.shape) != tuple(shape):
             raise RuntimeError(f"{name} has shape {tuple(t.shape)}, expected {tuple(shape)}")
 
-    def step(self, u0, v0, t0, *, dye0=None, theta0=None, out=None, dt=None):
+    def step(self, u0, v0, t0, *, dye0=None, theta0=None, out=None, dt=None, ctrl0=None, dt_prev=None):
         """One step (plus the dye update when the plan has dye, theta and the heat report
         (float64: heat, theta_wall, wall_heat, heat_storage, flow_heat) with heat transfer);
         returns the output dict.  ``out`` may hold u0 / v0 / theta0 themselves (in-place
-        update); ``dt`` is None (CFL rule on the device) or a 0-d device tensor."""
+        update); ``dt`` is None (CFL rule on the device) or a 0-d device tensor.  With fans or
+        the PID step, ``ctrl0`` is the controller memory (``ctrl_size``) and ``dt_prev`` the
+        previous step (0-d; 0 on the first); ``out`` then also holds the new ``ctrl``, the
+        fans' ``fan_thrust`` / ``fan_ud`` and the paint's ``paint_force``."""
         ny, nx = self.shape
         self._check("u0", u0, (ny, nx + 1))
         self._check("v0", v0, (ny + 1, nx))
@@ -300,6 +362,20 @@ class Ns2dPlan:
                     setattr(f, name, t.data_ptr())
         elif theta0 is not None:
             raise RuntimeError("theta0 given to a plan without heat transfer")
+        if self.ctrl_size:
+            if ctrl0 is None:
+                raise RuntimeError("this plan has fans or the PID step: ctrl0 is required")
+            self._check("ctrl0", ctrl0, (self.ctrl_size,))
+            f.ctrl0, f.ctrl = ctrl0.data_ptr(), out["ctrl"].data_ptr()
+            if dt_prev is None:
+                dt_prev = torch.zeros((), device=self.device, dtype=self.dtype)
+                self._keep_dt_prev = dt_prev
+            self._check("dt_prev", dt_prev, ())
+            f.dt_prev = dt_prev.data_ptr()
+        if self.nfan:
+            f.fan_thrust, f.fan_ud = out["fan_thrust"].data_ptr(), out["fan_ud"].data_ptr()
+        if self.cfg.paint:
+            f.paint_force = out["paint_force"].data_ptr()
         dtp = None
         if dt is not None:
             self._check("dt", dt, ())

@@ -4,10 +4,12 @@ served by the B200 step.
 ``FlowSolver`` imports ``step_full`` at module import (ns2d/solver.py:44-57) and calls it as
 ``step_full(state, geom, ops, None, out=..., diag=...)`` (solver.py:384-408); rebinding
 ``aerolume.solvers.ns2d.solver.step_full`` to this function swaps the step.  It returns
-``(State, coeffs (nbody, 3))`` of new tensors like the reference.  With heat transfer
-(``ops.phys`` placing heat transfer only) theta advances too and ``out`` receives the heat
-report of core.py:974-995.  Other placed physics, the wall model, diagnostics rows and
-traces raise instead of being computed differently.
+``(State, coeffs (nbody, 3))`` of new tensors like the reference.  With heat transfer theta
+advances too and ``out`` receives the heat report of core.py:974-995; fans, heaters, painted
+obstacles and the PID step of ``ops.phys`` run in the step, ``state.ctrl`` carries the
+controllers' memory and ``out`` receives ``fan_thrust``, ``fan_ud`` and ``paint_force`` as
+core.py:998-1002 fills them.  Jets and vents, smoke channels with emitters, the wall model,
+diagnostics rows and traces raise instead of being computed differently.
 """
 from __future__ import annotations
 
@@ -20,7 +22,7 @@ from .plan import Ns2dPlan
 
 
 class State(NamedTuple):
-    """The reference's 2D state (core.py:111-130); dye_extra and ctrl stay None."""
+    """The reference's 2D state (core.py:111-130); dye_extra stays None."""
     u: Any
     v: Any
     p: Any
@@ -50,7 +52,9 @@ def _plan_for(ops, geom, dye, device):
             weakref.finalize(ops, _PLANS.pop, id(ops), None)
         except TypeError:        # not weak-referenceable: its bucket stays bounded by _KEEP
             pass
-    key = (id(geom), dye)
+    ph = getattr(ops, "phys", None)
+    # the paint layer appears with the first stroke (physics.py:542-549): a new plan then
+    key = (id(geom), dye, id(getattr(ph, "paint_u", None)) if ph is not None else 0)
     entry = bucket.pop(key, None)
     if entry is None:
         entry = (Ns2dPlan(ops, geom, dye=dye, device=device), geom)   # the entry keeps geom alive
@@ -64,24 +68,32 @@ def step_full(state, geom, ops, dt=None, *, out=None, diag=False, trace=None):
     """One SSP-RK3 step (plus the dye update when the state carries dye)."""
     if diag or trace is not None:
         raise RuntimeError("diagnostics rows and stage traces are not produced by the B200 step")
-    for name in ("dye_extra", "ctrl"):
-        if getattr(state, name, None) is not None:
-            raise RuntimeError(f"placed-physics state {name!r} is not in the B200 2D step")
+    if getattr(state, "dye_extra", None) is not None:
+        raise RuntimeError("placed-physics state 'dye_extra' is not in the B200 2D step")
     theta = getattr(state, "theta", None)
     if theta is not None and getattr(ops, "phys", None) is None:
         raise RuntimeError("state.theta without heat transfer in ops.phys")
     plan = _plan_for(ops, geom, state.dye is not None, state.u.device)
     if (plan.thermal is None) != (theta is None):
         raise RuntimeError("state.theta must be given exactly when ops.phys has heat transfer")
+    ctrl = getattr(state, "ctrl", None)
+    if (ctrl is None) != (plan.ctrl_size == 0):
+        raise RuntimeError("state.ctrl must be given exactly when ops.phys has fans or the PID step")
     if dt is not None and not torch.is_tensor(dt):
         dt = torch.tensor(float(dt), device=state.u.device, dtype=state.u.dtype)
-    res = plan.step(state.u, state.v, state.t, dye0=state.dye, theta0=theta, dt=dt)
-    new = State(res["u"], res["v"], res["p"], res.get("dye"), res["t"], res["dt"], res.get("theta"))
+    res = plan.step(state.u, state.v, state.t, dye0=state.dye, theta0=theta, dt=dt, ctrl0=ctrl,
+                    dt_prev=state.dt if ctrl is not None else None)
+    new = State(res["u"], res["v"], res["p"], res.get("dye"), res["t"], res["dt"], res.get("theta"), None,
+                res.get("ctrl"))
     if out is not None and plan.thermal is not None:
         keys = (["heat"] if plan.n_temp else []) + (["theta_wall"] if plan.n_flux else []) + [
             "wall_heat", "heat_storage", "flow_heat"]
         for k in keys:
             out[k] = res[k].to(state.u.dtype)
+    if out is not None:
+        for k in ("fan_thrust", "fan_ud", "paint_force"):
+            if k in res:
+                out[k] = res[k]
     coeffs = res["coeffs"] if plan.nbody and plan.has_win else torch.zeros(0, 3, device=state.u.device,
                                                                           dtype=state.u.dtype)
     return new, coeffs

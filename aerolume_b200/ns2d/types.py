@@ -93,3 +93,33 @@ class Thermal2D:
     w_f: Any = None              # (n_flux, wy, wx) wall-temperature weights
     vol_u: Any = None            # (wy, wx + 1) solid area fractions for the buoyancy share
     vol_v: Any = None            # (wy + 1, wx)
+
+
+@dataclass
+class Placed2D:
+    """Fans, heaters, painted obstacles and the PID step of a 2D solve: the fields of the
+    reference's ``Physics`` with the same names (src/aerolume/solvers/ns2d/physics.py:70-140),
+    full-grid arrays.  The reference's own ``ops.phys`` serves as well (its tensors are then
+    read in place at every step, so strokes of the paint brush and live fan settings apply)."""
+    nfan: int = 0
+    fan_gu: Any = None           # (nfan, ny, nx + 1) force per unit thrust on the u faces
+    fan_gv: Any = None           # (nfan, ny + 1, nx)
+    fan_phi: Any = None          # (nfan, ny, nx) disc-averaging weight
+    fan_dir: Any = None          # (nfan, 2)
+    fan_value: Any = None        # (nfan,) thrust / pressure jump / target speed
+    fan_width: Any = None
+    fan_kp: Any = None
+    fan_ki: Any = None
+    fan_dpmax: Any = None
+    fan_isvel: Any = None
+    fan_isthrust: Any = None
+    u_floor: Any = 0.0           # the sources' speed scale
+    heat: Any = None             # (ny, nx) heater density (heat transfer only)
+    heat_max: Any = None
+    paint: bool = False
+    paint_c: Any = None          # (ny, nx), (ny, nx + 1), (ny + 1, nx) solid fractions
+    paint_u: Any = None
+    paint_v: Any = None
+    paint_wu: Any = None         # the paint's force weights on the faces
+    paint_wv: Any = None
+    pid: bool = False

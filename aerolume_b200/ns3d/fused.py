@@ -52,6 +52,10 @@ class B200Kernels:
     def __init__(self, scheme, device, dtype):
         self.scheme, self.device, self.dtype = scheme, device, dtype
         self._plans = {}
+        # the learned subgrid closure (a trained ClosureModel) for WALE steps, or None; set it
+        # on the handle the solver holds (``solver._kern.closure = model``): the next step
+        # builds its plan with it
+        self.closure = None
 
     def _remember(self, key, entry):
         same = [k for k in self._plans if k[0] == key[0]]
@@ -65,11 +69,14 @@ class B200Kernels:
         pid = getattr(phys, "pid", None) if phys is not None else None
         fans = getattr(phys, "fans", None) if phys is not None else None
         ports = getattr(phys, "ports", None) if phys is not None else None
-        key = ("step", id(geom), id(ops), id(thermal), id(paint), id(pid), id(fans), id(ports)) + _live_key(ops, thermal)
+        closure = self.closure if getattr(ops, "turbulence", None) == "wale" else None
+        key = ("step", id(geom), id(ops), id(thermal), id(paint), id(pid), id(fans), id(ports),
+               id(closure)) + _live_key(ops, thermal)
         entry = self._plans.get(key)
         if entry is None:
             plan = Ns3dPlan(ops, geom, thermal, None, device=self.device, paint=paint, pid=pid, fans=fans, ports=ports,
-                            u_floor=float(getattr(phys, "u_floor", 0.0) or 0.0) if phys is not None else 0.0)
+                            u_floor=float(getattr(phys, "u_floor", 0.0) or 0.0) if phys is not None else 0.0,
+                            closure=closure)
             entry = (plan, geom, ops, thermal, paint, pid, fans, ports)   # the objects stay alive with their plan
             self._remember(key, entry)
         return entry[0]

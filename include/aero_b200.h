@@ -489,6 +489,11 @@ typedef struct {
   double diff_coef;             /* largest diffusion coefficient (physics.py:833-848)      */
   int32_t n_temp, n_flux;       /* temperature bodies, heat-flux bodies                    */
   int32_t has_ins, has_vol;     /* insulation factors / area fractions present             */
+  /* placed physics besides heat transfer (ns2d/physics.py:70-140): actuator-strip fans with
+   * their PI controllers (<= AERO_MAX_FANS), heaters (thermal plans), a paint layer of drawn
+   * obstacles, the PID-controlled step (diagnostics.py:104-124); their fields are in
+   * AeroNs2dGeom, the controller memory in AeroNs2dFields */
+  int32_t nfan, heaters, paint, pid;
 } AeroNs2dConfig;
 
 /* temperature boundary modes of a 2D side (ns2d/scalar.py:96-146) */
@@ -511,6 +516,16 @@ typedef struct {
    * (ns2d/core.py:167-176 set_reynolds fills them in place while a captured graph stays
    * valid), read by every launch; NULL: the config's nu, eta, kappa, eta_t */
   const void *nu, *eta, *kappa, *eta_t;
+  /* placed physics (the reference's Physics tensors, read at every launch, plan dtype):
+   * fans: force per unit thrust fan_gu (nfan, ny, nx+1), fan_gv (nfan, ny+1, nx), averaging
+   * weight fan_phi (nfan, ny, nx), direction fan_dir (nfan, 2), and per fan value, width,
+   * kp, ki, dpmax, isvel, isthrust (nfan); the sources' speed floor u_floor (0-d);
+   * heaters: density heat (ny, nx) and its maximum heat_max (0-d); paint: paint_c (ny, nx),
+   * paint_u (ny, nx+1), paint_v (ny+1, nx) and their force weights paint_wu, paint_wv */
+  const void *fan_gu, *fan_gv, *fan_phi, *fan_dir, *fan_value, *fan_width, *fan_kp, *fan_ki, *fan_dpmax,
+      *fan_isvel, *fan_isthrust, *u_floor;
+  const void *heat, *heat_max;
+  const void *paint_c, *paint_u, *paint_v, *paint_wu, *paint_wv;
 } AeroNs2dGeom;
 
 /* Step inputs (u0, v0, t0, dye0) and outputs; u / v may alias u0 / v0. */
@@ -524,6 +539,12 @@ typedef struct {
    * top sides (4), heat storage (1), flow heat in at the inlet / out at the outlet (2) */
   const void *theta0;
   void *theta, *heat, *theta_wall, *wall_heat, *heat_storage, *flow_heat;
+  /* placed physics (plan dtype): the previous step's dt (0-d; <= 0: first step) and the
+   * controller memory in / out (2 + 2 nfan: the PID's last two errors, then per fan its
+   * integral and pressure jump; core.py State.ctrl); out: the fans' thrust and disc velocity
+   * (nfan each) and the painted obstacles' force coefficients [Cd, Cl] (2) */
+  const void *dt_prev, *ctrl0;
+  void *ctrl, *fan_thrust, *fan_ud, *paint_force;
 } AeroNs2dFields;
 
 int aero_ns2d_plan_create(const AeroNs2dConfig *cfg, AeroNs2dPlan **plan);

@@ -727,3 +727,243 @@ def step2d_thermal(u0, v0, t, theta0, geom, ops, poisson, tp, *, dt=None):
     res.theta = thp
     res.report = heat_report2d(theta0, thp, up, heat_acc, geom, tp, ops, dt)
     return res
+
+
+# ---------------------------------------------------------------------------
+# placed physics besides heat: fans, heaters, painted obstacles, the PID step
+# (physics.py:434-496, 578-694, 696-730, 805-884; diagnostics.py:104-124; core.py:815-1003)
+# ---------------------------------------------------------------------------
+
+PID_TARGET, PID_GAINS, PID_MAX_GROWTH = 0.9, (0.10, 0.25, 0.02), 1.03    # diagnostics.py:46-48
+FAN_CTRL_OFFSET = 2                                                     # physics.py:140
+
+
+@dataclass
+class Placed2D:
+    """The reference's 2D ``Physics`` fields of fans, heaters, paint and the PID step
+    (physics.py:70-140), as numpy arrays of the step's dtype."""
+    nfan: int = 0
+    fan_gu: np.ndarray | None = None        # (nf, ny, nx + 1) force per unit thrust
+    fan_gv: np.ndarray | None = None        # (nf, ny + 1, nx)
+    fan_phi: np.ndarray | None = None       # (nf, ny, nx) averaging weight
+    fan_dir: np.ndarray | None = None       # (nf, 2)
+    fan_value: np.ndarray | None = None
+    fan_width: np.ndarray | None = None
+    fan_kp: np.ndarray | None = None
+    fan_ki: np.ndarray | None = None
+    fan_dpmax: np.ndarray | None = None
+    fan_isvel: np.ndarray | None = None
+    fan_isthrust: np.ndarray | None = None
+    pid: bool = False
+    u_floor: float = 0.0
+    heat: np.ndarray | None = None          # (ny, nx) heat-rate density
+    heat_max: float | None = None
+    paint_c: np.ndarray | None = None
+    paint_u: np.ndarray | None = None
+    paint_v: np.ndarray | None = None
+    paint_wu: np.ndarray | None = None
+    paint_wv: np.ndarray | None = None
+
+    @property
+    def paint(self):
+        return self.paint_u is not None
+
+
+def pid_dt2d(dt_limit, dt_prev, ctrl):
+    """diagnostics.py:104-124: the PID-controlled step and the new controller memory."""
+    T = type(dt_limit)
+    kp, ki, kd = (T(g) for g in PID_GAINS)
+    target = T(PID_TARGET) * dt_limit
+    first = dt_prev <= 0
+    safe_prev = target if first else T(dt_prev)
+    e = np.log(T(target / safe_prev))
+    e1, e2 = ctrl[0], ctrl[1]
+    step = ki * e + kp * (e - e1) + kd * ((e - T(2.0) * e1) + e2)
+    grow = np.exp(min(step, T(np.log(PID_MAX_GROWTH))))
+    dt = target if first else min(safe_prev * grow, dt_limit)
+    e = T(0.0) if first else e
+    new = ctrl.copy()
+    new[0], new[1] = e, e1
+    return T(dt), new
+
+
+def fan_control2d(u, v, ctrl, dt, pl):
+    """physics.py:640-672: disc velocities, the PI controller, the thrusts and the new memory."""
+    T = u.dtype.type
+    uc = T(0.5) * (u[:, 1:] + u[:, :-1])
+    vc = T(0.5) * (v[1:] + v[:-1])
+    ua = np.einsum("kij,ij->k", pl.fan_phi, uc)
+    va = np.einsum("kij,ij->k", pl.fan_phi, vc)
+    ud = ua * pl.fan_dir[:, 0] + va * pl.fan_dir[:, 1]
+    o = FAN_CTRL_OFFSET
+    integ = ctrl[o::2]
+    err = pl.fan_value - ud
+    ilim = pl.fan_dpmax / pl.fan_ki
+    integ_new = np.maximum(np.minimum(integ + err * T(dt) * pl.fan_isvel, ilim), -ilim)
+    dp_pi = np.maximum(np.minimum(pl.fan_kp * err + pl.fan_ki * integ_new, pl.fan_dpmax), -pl.fan_dpmax)
+    thrust_fixed = np.where(pl.fan_isthrust > 0, pl.fan_value, pl.fan_value * pl.fan_width)
+    thrust = np.where(pl.fan_isvel > 0, dp_pi * pl.fan_width, thrust_fixed)
+    dp = thrust / pl.fan_width
+    new = np.concatenate([ctrl[:o], np.stack([integ_new, dp], axis=1).reshape(-1)]).astype(u.dtype)
+    return thrust.astype(u.dtype), new, ud.astype(u.dtype)
+
+
+def placed_dt_limit2d(dt, u, v, theta, nut_max, tp, pl, ops):
+    """physics.py:851-884 with the sources' speed floor and the heaters' bounds."""
+    T = u.dtype.type
+    if pl is not None and pl.nfan:
+        dt = min(dt, T(ops.cfl) * T(ops.h) / max(T(pl.u_floor), T(1e-6)))
+    if tp is not None and theta is not None:
+        kap = T(tp.kappa) if nut_max is None else T(tp.kappa) + nut_max * T(1.0 / tp.prt)
+        u_floor = T(pl.u_floor) if pl is not None else T(0.0)
+        speed = max(np.abs(u).max() + np.abs(v).max(), u_floor)
+        rate = speed * T(2.0 / ops.h) + kap * T(tp.diff_coef / (ops.h * ops.h))
+        dt = min(dt, T(1.0) / rate)
+        acc = T(abs(tp.ri)) * np.abs(theta).max()
+        dt = min(dt, T(ops.cfl) * np.sqrt(T(ops.h) / max(acc, T(1e-12))))
+        if pl is not None and pl.heat_max is not None:
+            s_max = max(T(pl.heat_max), T(1e-12))
+            dt = min(dt, T(1.0) / s_max)
+            dt = min(dt, (T(6.0 * ops.cfl * ops.h) / max(T(abs(tp.ri)) * s_max, T(1e-12))) ** T(1.0 / 3.0))
+    return T(dt)
+
+
+def theta_rhs2d_placed(th, u, v, nut, geom, tp, pl, ops):
+    """physics.py:696-730 with the heaters and the paint's insulation."""
+    T = th.dtype.type
+    ny, nx = th.shape
+    fx, fy = tvd_fluxes(th, u, v, ops, tp.theta_in)
+    lt = flux_divergence(fx, fy, ops.h)
+    kappa = T(tp.kappa)
+    insulated = tp.ins_u is not None and not geom.empty
+    paint = pl is not None and pl.paint
+    if nut is not None:
+        nc = nut[1:-1, 1:-1] * T(1.0 / tp.prt)
+        kx = kappa + face_average_x(nc, ops)
+        ky = kappa + face_average_y(nc, ops)
+    elif paint or insulated:
+        kx = np.full((ny, nx + 1), kappa, dtype=th.dtype)
+        ky = np.full((ny + 1, nx), kappa, dtype=th.dtype)
+    else:
+        kx = ky = kappa
+    if paint:
+        kx = kx * (T(1.0) - pl.paint_u)
+        ky = ky * (T(1.0) - pl.paint_v)
+    if insulated:
+        j0, j1, i0, i1 = geom.window
+        kx = kx.copy()
+        ky = ky.copy()
+        kx[j0:j1, i0:i1 + 1] = kx[j0:j1, i0:i1 + 1] * tp.ins_u
+        ky[j0:j1 + 1, i0:i1] = ky[j0:j1 + 1, i0:i1] * tp.ins_v
+    Fx, Fy = diffusive_fluxes(th, kx, ky, ops, tp.wall_modes, tp.wall_values)
+    lt = lt + flux_divergence(Fx, Fy, ops.h)
+    if pl is not None and pl.heat is not None:
+        lt = lt + pl.heat
+    if tp.flux_ids and not geom.empty:
+        j0, j1, i0, i1 = geom.window
+        lt = lt.copy()
+        lt[j0:j1, i0:i1] = lt[j0:j1, i0:i1] + kappa * tp.q_skin
+    return lt
+
+
+def step2d_placed(u0, v0, t, geom, ops, poisson, *, tp=None, pl=None, theta0=None, dye=None, dt_prev=0.0,
+                  ctrl=None, dt=None):
+    """One SSP-RK3 step (core.py:815-969) with heat transfer (``tp``), fans, heaters, painted
+    obstacles and the PID step (``pl``); ``ctrl`` is the controller memory (PID errors, then
+    (integral, pressure jump) per fan) and ``dt_prev`` the previous step (0: first)."""
+    T = u0.dtype.type
+    up, vp = u0, v0
+    thermal = tp is not None and theta0 is not None
+    thp = theta0
+    acc_u = acc_v = psi_w = heat_acc = paint_acc = None
+    fan_f = fan_thrust = fan_ud = None
+    les = ops.turbulence != "none"
+    paint = pl is not None and pl.paint
+    for s, ((a, b), w) in enumerate(zip(SSP_RK3, FORCE_WEIGHTS)):
+        lu, lv, nut_max = momentum_rhs2d(up, vp, geom, ops)
+        nut = sgs_divergence2d.nut if (les and thermal) else None
+        if s == 0:
+            if dt is None:
+                if ops.dt_fixed is not None:
+                    dt = T(ops.dt_fixed)
+                else:
+                    dt = cfl_dt2d(u0, v0, ops, nut_max)
+                    if pl is not None or thermal:
+                        dt = placed_dt_limit2d(dt, u0, v0, theta0, nut_max, tp if thermal else None, pl, ops)
+                    if pl is not None and pl.pid:
+                        dt, ctrl = pid_dt2d(T(dt), dt_prev, ctrl)
+            dt = T(dt)
+            if pl is not None and pl.nfan:
+                fan_thrust, ctrl, fan_ud = fan_control2d(u0, v0, ctrl, dt, pl)
+                fan_f = (np.einsum("k,kij->ij", fan_thrust, pl.fan_gu), np.einsum("k,kij->ij", fan_thrust, pl.fan_gv))
+        if fan_f is not None:
+            lu = lu + fan_f[0]
+            lv = lv + fan_f[1]
+        lt = theta_rhs2d_placed(thp, up, vp, nut, geom, tp, pl, ops) if thermal else None
+        bdt = dt * T(b)
+        if a == 0.0:
+            uh = up + lu * bdt
+            vh = vp + lv * bdt
+        else:
+            uh = lerp(up, u0, a) + lu * bdt
+            vh = lerp(vp, v0, a) + lv * bdt
+        if lt is not None:
+            thh = (thp if a == 0.0 else lerp(thp, theta0, a)) + lt * bdt
+        if not ops.periodic:
+            uh = inlet_outlet(uh, ops)
+        if not geom.empty:
+            uh, vh, du, dv = penalise2d(uh, vh, geom, ops, bdt)
+            acc_u = du * T(w) if acc_u is None else acc_u + du * T(w)
+            acc_v = dv * T(w) if acc_v is None else acc_v + dv * T(w)
+        if paint:   # physics.py:675-683: the paint's implicit penalisation and impulse
+            k = T(bdt / T(ops.eta))
+            un = uh / (T(1.0) + k * pl.paint_u)
+            vn = vh / (T(1.0) + k * pl.paint_v)
+            imp = np.array([((un - uh) * pl.paint_wu).sum(), ((vn - vh) * pl.paint_wv).sum()], dtype=np.float64)
+            paint_acc = imp * float(T(w)) if paint_acc is None else paint_acc + imp * float(T(w))
+            uh, vh = un, vn
+        if thermal and tp.ri != 0.0:  # core.py:774-813
+            fu, fv = buoyancy2d(thp, tp, ops)
+            if fu is not None:
+                uh = uh + bdt * fu
+            if fv is not None:
+                vh = vh + bdt * fv
+            if not geom.empty:
+                j0, j1, i0, i1 = geom.window
+                vu = tp.vol_u if tp.vol_u is not None else geom.chi_u
+                vv = tp.vol_v if tp.vol_v is not None else geom.chi_v
+                if fu is not None:
+                    acc_u = acc_u + fu[j0:j1, i0:i1 + 1] * vu * T(bdt * T(w))
+                if fv is not None:
+                    acc_v = acc_v + fv[j0:j1 + 1, i0:i1] * vv * T(bdt * T(w))
+            if paint and paint_acc is not None:
+                su = float((fu * pl.paint_u * pl.paint_wu).sum()) if fu is not None else 0.0
+                sv = float((fv * pl.paint_v * pl.paint_wv).sum()) if fv is not None else 0.0
+                paint_acc = paint_acc + np.array([su, sv]) * float(bdt * T(w))
+        if ops.periodic and (paint or not geom.empty):
+            uh, vh = apply_boundary_values(uh, vh, ops)
+        if lt is not None:
+            thh, heat = penalise_theta2d(thh, geom, tp, bdt)
+            if heat is not None:
+                heat_acc = heat * float(T(w)) if heat_acc is None else heat_acc + heat * float(T(w))
+            thp = thh
+        up, vp, psi = project2d(uh, vh, ops, poisson)
+        psi_w = psi * T(w) if psi_w is None else psi_w + T(w) * psi
+    p = psi_w * (T(1.0) / dt)
+    coeffs = force_coefficients2d(acc_u, acc_v, geom, ops, dt)
+    new_dye = None
+    if dye is not None:
+        new_dye = zero_dye_in_solids(advect_dye2d(dye, up, vp, dt, ops), geom)
+        if paint:
+            new_dye = new_dye * (pl.paint_c <= 0.5).astype(new_dye.dtype)
+    res = StepResult2D(up, vp, p, np.asarray(t + dt, dtype=u0.dtype), np.asarray(dt, dtype=u0.dtype), coeffs,
+                       new_dye)
+    res.theta = thp if thermal else None
+    res.ctrl = ctrl
+    res.report = heat_report2d(theta0, thp, up, heat_acc, geom, tp, ops, dt) if thermal else {}
+    if fan_thrust is not None:
+        res.report["fan_thrust"] = fan_thrust
+        res.report["fan_ud"] = fan_ud
+    if paint_acc is not None:
+        res.report["paint_force"] = paint_acc * float(-(ops.h * ops.h) / (float(dt) * 0.5 * ops.force_ref))
+    return res

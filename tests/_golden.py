@@ -131,6 +131,19 @@ def thermal2d_from_case(meta, arr):
                      flux_ids=tuple(t.get("flux_ids", ())), **g)
 
 
+def placed2d_from_case(meta, arr):
+    """The oracle's Placed2D (fans, heaters, paint, the PID step) of a 2D golden case, or None."""
+    from oracle.ns2d import Placed2D
+    pm = meta.get("placed")
+    if pm is None or not (pm["nfan"] or pm["pid"] or pm["paint"] or pm["heat"]):
+        return None
+    dt = np.float64 if meta["dtype"] == "float64" else np.float32
+    kw = {n: arr[n].astype(dt) for n in ("fan_gu", "fan_gv", "fan_phi", "fan_dir", "fan_value", "fan_width", "fan_kp",
+                                         "fan_ki", "fan_dpmax", "fan_isvel", "fan_isthrust", "heat", "paint_c",
+                                         "paint_u", "paint_v", "paint_wu", "paint_wv") if n in arr}
+    return Placed2D(nfan=pm["nfan"], pid=pm["pid"], u_floor=pm["u_floor"], heat_max=pm.get("heat_max"), **kw)
+
+
 def load_masks():
     """(npz, case tags) of masks3d.npz."""
     z = np.load(GOLDEN / "masks3d.npz")

@@ -30,7 +30,9 @@ REF = Path(os.environ["AEROLUME_REF"])
 sys.path.insert(0, str(REF / "src"))
 
 from aerolume.solvers.ns2d import core  # noqa: E402
-from aerolume.solvers.ns2d.config import ImmersedBody, SolverConfig, ThermalConfig, WallBC  # noqa: E402
+from aerolume.solvers.ns2d import physics as phx  # noqa: E402
+from aerolume.solvers.ns2d.config import (FanSpec, HeatSourceSpec, ImmersedBody, SolverConfig,  # noqa: E402
+                                          ThermalConfig, WallBC)
 from aerolume.solvers.ns2d.geometry import build_geometry  # noqa: E402
 from aerolume.solvers.ns2d.poisson import PoissonSolver  # noqa: E402
 
@@ -78,14 +80,40 @@ def extract(ops, geom):
                 val = getattr(tg, name)
                 if val is not None:
                     arrays["th_" + name] = _np(val)
+    if ph is not None:
+        # the placed physics besides heat transfer: fans, heaters, paint, the PID step
+        meta["placed"] = {"nfan": ph.nfan, "pid": bool(ph.pid), "paint": bool(ph.paint), "ctrl_size": ph.ctrl_size,
+                          "u_floor": float(ph.u_floor), "heat": ph.heat is not None}
+        if ph.nfan:
+            for name in ("fan_gu", "fan_gv", "fan_phi", "fan_dir", "fan_value", "fan_width", "fan_kp", "fan_ki",
+                         "fan_dpmax", "fan_isvel", "fan_isthrust"):
+                arrays[name] = _np(getattr(ph, name))
+        if ph.heat is not None:
+            arrays["heat"] = _np(ph.heat)
+            meta["placed"]["heat_max"] = float(ph.heat_max)
+        if ph.paint:
+            for name in ("paint_c", "paint_u", "paint_v", "paint_wu", "paint_wv"):
+                arrays[name] = _np(getattr(ph, name))
     return meta, arrays
 
 
-def _run_case(name, cfg_kw, *, dtype="float64", amp=0.1, seed=1, steps=1):
+def _paint(ops, sdf):
+    """A painted obstacle ``sdf(x, y) < 0`` on the grid of ``ops`` (the app's brush,
+    physics.py:542-575), then the combined penalisation it enters."""
+    if ops.phys is None:
+        ops.phys = phx.empty_physics(ops)
+    phx.ensure_paint(ops.phys, ops)
+    phx.paint_brush(ops.phys, ops, sdf, 1.5, False)
+    phx.combine_penalisation(ops.phys)
+
+
+def _run_case(name, cfg_kw, *, dtype="float64", amp=0.1, seed=1, steps=1, paint=None):
     cfg64 = SolverConfig(**{**cfg_kw, "dtype": "float64", "device": "cpu", "perturb": False})
     cfg = SolverConfig(**{**cfg_kw, "dtype": dtype, "device": "cpu", "perturb": False})
     ops64 = core.make_operators(cfg64)
     ops = core.make_operators(cfg)
+    if paint is not None:
+        _paint(ops, paint)
     geom = build_geometry(cfg.bodies, ops)
     s64 = core.init_state(cfg64, ops64, perturb=False)
     g = torch.Generator().manual_seed(seed)
@@ -103,10 +131,16 @@ def _run_case(name, cfg_kw, *, dtype="float64", amp=0.1, seed=1, steps=1):
     theta = None
     if cfg.thermal is not None:
         theta = (0.3 * torch.randn((cfg.ny, cfg.nx), generator=g, dtype=torch.float64)).to(tdt)
+    ctrl = None
+    if ops.phys is not None and ops.phys.ctrl_size:
+        ctrl = torch.zeros(ops.phys.ctrl_size, dtype=tdt)
+        ctrl[:2] = (0.2 * torch.randn(2, generator=g, dtype=torch.float64)).to(tdt)   # PID memory e1, e2
     state = core.State(u.to(tdt), v.to(tdt), torch.zeros(cfg.ny, cfg.nx, dtype=tdt), dye,
-                       torch.tensor(0.37, dtype=tdt), zero.clone(), theta)
+                       torch.tensor(0.37, dtype=tdt), zero.clone(), theta, None, ctrl)
     meta, arrays = extract(ops, geom)
     arrays.update({"in_u": _np(state.u), "in_v": _np(state.v), "in_t": _np(state.t)})
+    if ctrl is not None:
+        arrays["in_ctrl"] = _np(ctrl)
     if dye is not None:
         arrays["in_dye"] = _np(dye)
     if theta is not None:
@@ -123,8 +157,10 @@ def _run_case(name, cfg_kw, *, dtype="float64", amp=0.1, seed=1, steps=1):
                     arrays["out1_dye"] = _np(st.dye)
                 if st.theta is not None:
                     arrays["out1_theta"] = _np(st.theta)
-                    for key, val in rep.items():
-                        arrays["out1_rep_" + key] = _np(val)
+                for key, val in rep.items():
+                    arrays["out1_rep_" + key] = _np(val)
+                if st.ctrl is not None:
+                    arrays["out1_ctrl"] = _np(st.ctrl)
     meta["steps"] = steps
     if steps > 1:
         arrays.update({"outN_u": _np(st.u), "outN_v": _np(st.v), "outN_p": _np(st.p), "outN_t": _np(st.t)})
@@ -132,6 +168,9 @@ def _run_case(name, cfg_kw, *, dtype="float64", amp=0.1, seed=1, steps=1):
             arrays["outN_dye"] = _np(st.dye)
         if st.theta is not None:
             arrays["outN_theta"] = _np(st.theta)
+        if st.ctrl is not None:
+            arrays["outN_ctrl"] = _np(st.ctrl)
+            arrays["outN_dt"] = _np(st.dt)
     store = {k: (np.asarray(x, dtype=np.float32) if dtype == "float32" and np.asarray(x).dtype == np.float64
                  else np.asarray(x)) for k, x in arrays.items()}
     np.savez_compressed(HERE / f"ns2d_{name}.npz", meta=np.array(json.dumps(meta)), **store)
@@ -210,6 +249,22 @@ def main():
                                         "bodies": [cold], "periodic": True, "dye": False, "moment_ref": (1.0, 1.2),
                                         "thermal": ThermalConfig(prandtl=0.71, richardson=0.8)},
              dtype="float64", amp=0.2, seed=7, steps=3)
+    # placed physics besides heat: a velocity-regulated fan and a thrust fan with the PID step in
+    # the cylinder tunnel (three steps: the controller's first step, then two regulated ones)
+    fans = [FanSpec((1.0, 1.2), direction=(1.0, 0.0), width=0.8, mode="velocity", value=1.3, name="reg"),
+            FanSpec((5.5, 3.0), direction=(0.6, -0.8), width=0.6, mode="thrust", value=0.4, name="push")]
+    fan_case = dict(tunnel, fans=fans, adaptive_dt="pid")
+    run_case("tunnel_fans_pid_f64", fan_case, dtype="float64", amp=0.05, seed=8, steps=3)
+    run_case("tunnel_fans_pid_f32", fan_case, dtype="float32", amp=0.05, seed=8, steps=3)
+    # a heater and a painted obstacle in the heated cavity, with smoke (paint clears it)
+    heaters = [HeatSourceSpec((2.8, 1.6), kind="rect", size=(0.4, 0.2), power=0.6, name="strip"),
+               HeatSourceSpec((1.0, 0.5), kind="disc", size=(0.2,), power=-0.3, name="cooler")]
+    heater_case = dict(cavity, bodies=[ins], heat_sources=heaters, dye=True)
+
+    def block(x, y):
+        return torch.maximum((x - 3.2).abs() - 0.25, (y - 0.8).abs() - 0.3)
+    run_case("cavity_heater_paint_f64", heater_case, dtype="float64", amp=0.1, seed=9, steps=3, paint=block)
+    run_case("cavity_heater_paint_f32", heater_case, dtype="float32", amp=0.1, seed=9, steps=3, paint=block)
     if not names or "poisson" in names:
         poisson_cases()
 

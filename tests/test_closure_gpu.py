@@ -214,3 +214,35 @@ def test_closure_step_uses_the_model():
     ev, wale = plan_c.closure_counts()
     assert 0 < wale < ev
     assert not torch.equal(a["u"], b["u"])
+
+
+def test_closure_through_the_seam():
+    """The drop-in handle carries the model (``kern.closure``): its WALE step then runs the
+    closure -- bit for bit the plain step when the model's range is empty, as above -- and a
+    plan without it is kept apart in the cache."""
+    from types import SimpleNamespace
+
+    from aerolume_b200.ns3d.fused import fast_step_phys, load_kernels
+    from aerolume_b200.ns3d.types import State3D
+    from aerolume_b200.ns3d.workloads import box_on_moving_floor, initial_state
+    ops, geom, th, _, _ = box_on_moving_floor(64, 32, 32, dtype="float32", seed=7)
+    u, v, w = initial_state(ops, seed=7, noise=0.05)
+    kern = load_kernels("upwind3", torch.device("cuda"), torch.float32)
+    kern.plan_for(geom, ops, SimpleNamespace(thermal=th)).project(u, v, w)
+    st = State3D(u, v, w, torch.zeros(32, 32, 64, device="cuda"), torch.zeros((), device="cuda"),
+                 torch.zeros((), device="cuda"))
+    theta = torch.zeros(32, 32, 64, device="cuda")
+    phys = SimpleNamespace(thermal=th, paint=None, pid=None, fans=None, ports=None, u_floor=0.0)
+    plain = fast_step_phys(st, geom, ops, kern, phys=phys, theta=theta)
+    m = _model(51)
+    m.in_lo[:] = 1.0
+    m.in_hi[:] = -1.0
+    kern.closure = m
+    learned = fast_step_phys(st, geom, ops, kern, phys=phys, theta=theta)
+    torch.cuda.synchronize()
+    for a, b in ((plain.state.u, learned.state.u), (plain.state.p, learned.state.p), (plain.theta, learned.theta)):
+        assert torch.equal(a, b)
+    plan = kern.plan_for(geom, ops, phys)
+    assert plan.closure is m
+    ev, wale = plan.closure_counts()
+    assert ev > 0 and wale == ev

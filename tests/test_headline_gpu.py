@@ -8,8 +8,9 @@ these tests hold the CUDA step to the oracle on the benchmark grids themselves:
   x-y tiles that skip the ghost fill;
 * the same builders at 80 x 40 x 40 in FP64 and FP32 (two z-chunks, interior tiles);
 * one step of each grid of the batched 2D sweep (384 x 192 ... 1024 x 512, the radix-3 transform
-  path among them) against the 2D oracle, and the sweep's multi-stream schedule against the
-  plain per-instance loop (bit-identical).
+  path among them) against the 2D oracle, and the sweep's persistent schedules (grid barrier,
+  per-instance counters, work queue) and its multi-stream schedule against the plain
+  per-instance loop (bit-identical).
 """
 from __future__ import annotations
 

@@ -5,7 +5,7 @@ import numpy as np
 import pytest
 import torch
 
-from _golden import CASES_2D, GOLDEN, load_case2d, thermal2d_from_case
+from _golden import CASES_2D, GOLDEN, load_case2d, placed2d_from_case, thermal2d_from_case
 from oracle import ns2d as O2
 
 pytestmark = pytest.mark.gpu
@@ -31,12 +31,16 @@ def _setup(name):
     from aerolume_b200.ns2d.plan import Ns2dPlan
     meta, ops, geom, arr = load_case2d(name)
     dt = torch.float64 if meta["dtype"] == "float64" else torch.float32
-    plan = Ns2dPlan(ops, geom, dye="in_dye" in arr, thermal=thermal2d_from_case(meta, arr))
+    plan = Ns2dPlan(ops, geom, dye="in_dye" in arr, thermal=thermal2d_from_case(meta, arr),
+                    placed=placed2d_from_case(meta, arr))
     ins = {"u0": _dev(arr["in_u"], dt), "v0": _dev(arr["in_v"], dt), "t0": _dev(arr["in_t"], dt)}
     if "in_dye" in arr:
         ins["dye0"] = _dev(arr["in_dye"], dt)
     if "in_theta" in arr:
         ins["theta0"] = _dev(arr["in_theta"], dt)
+    if "in_ctrl" in arr:   # the controllers' memory and the previous step (0: the first)
+        ins["ctrl0"] = _dev(arr["in_ctrl"], dt)
+        ins["dt_prev"] = torch.zeros((), device="cuda", dtype=dt)
     return meta, plan, ins, arr
 
 
@@ -76,19 +80,31 @@ def test_step2d_matches_reference(name):
     if "out1_theta" in arr:
         assert _rel(out["theta"], arr["out1_theta"]) < tol, _rel(out["theta"], arr["out1_theta"])
         _check_report(out, arr, meta)
+    # fans, paint and the controllers (core.py:998-1002, State.ctrl)
+    for key, ref_key in (("fan_thrust", "out1_rep_fan_thrust"), ("fan_ud", "out1_rep_fan_ud"),
+                         ("paint_force", "out1_rep_paint_force"), ("ctrl", "out1_ctrl")):
+        if ref_key in arr:
+            ref = np.asarray(arr[ref_key], np.float64)
+            got = out[key].double().cpu().numpy()
+            assert np.abs(got - ref).max() <= TOL_COEFF[meta["dtype"]] * max(1.0, np.abs(ref).max()), (key, got, ref)
+    assert plan.status() == 0 if hasattr(plan, "status") else True
 
 
-@pytest.mark.parametrize("name", [c for c in CASES_2D if c.startswith("cylinder") or "heated" in c or "cold" in c])
+@pytest.mark.parametrize("name", [c for c in CASES_2D if c.startswith(("cylinder", "tunnel_fans", "cavity_heater"))
+                                  or "heated" in c or "cold" in c])
 def test_three_steps_in_place_match_reference(name):
     meta, plan, ins, arr = _setup(name)
     u, v, t, dye, theta = ins["u0"], ins["v0"], ins["t0"], ins.get("dye0"), ins.get("theta0")
+    ctrl, dt_prev = ins.get("ctrl0"), ins.get("dt_prev")
     out = plan.empty_fields()
     for _ in range(3):
         out["u"], out["v"] = u, v             # in-place velocity update
         if theta is not None:
             out["theta"] = theta              # and theta in place
-        res = plan.step(u, v, t, dye0=dye, theta0=theta, out=out)
+        res = plan.step(u, v, t, dye0=dye, theta0=theta, out=out, ctrl0=ctrl, dt_prev=dt_prev)
         t = res["t"].clone()
+        if ctrl is not None:
+            ctrl, dt_prev = res["ctrl"].clone(), res["dt"].clone()
         if dye is not None:
             dye, res["dye"] = res["dye"], dye  # ping-pong the dye
     torch.cuda.synchronize()
@@ -99,6 +115,8 @@ def test_three_steps_in_place_match_reference(name):
         assert _rel(dye, arr["outN_dye"]) < tol
     if theta is not None:
         assert _rel(theta, arr["outN_theta"]) < tol, _rel(theta, arr["outN_theta"])
+    if ctrl is not None:
+        assert _rel(ctrl, arr["outN_ctrl"]) < tol and _rel(dt_prev, arr["outN_dt"]) < tol
 
 
 def _poisson_plan(nx, ny, h, periodic, dtype):

@@ -4,7 +4,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from _golden import CASES_2D, GOLDEN, load_case2d, thermal2d_from_case
+from _golden import CASES_2D, GOLDEN, load_case2d, placed2d_from_case, thermal2d_from_case
 from oracle import ns2d as O2
 
 # float64: the restatement agrees with the reference to round-off; float32: to the FP32 step
@@ -23,10 +23,16 @@ def _run(name, steps=1):
     u, v, t = arr["in_u"], arr["in_v"], arr["in_t"]
     dye = arr.get("in_dye")
     tp = thermal2d_from_case(meta, arr)
+    pl = placed2d_from_case(meta, arr)
     theta = arr.get("in_theta")
+    ctrl, dt_prev = arr.get("in_ctrl"), 0.0
     outs = []
     for _ in range(steps):
-        if tp is not None:
+        if pl is not None:
+            r = O2.step2d_placed(u, v, t, geom, ops, ps, tp=tp, pl=pl, theta0=theta, dye=dye, dt_prev=dt_prev,
+                                 ctrl=ctrl)
+            theta, ctrl, dt_prev = r.theta, r.ctrl, float(r.dt)
+        elif tp is not None:
             r = O2.step2d_thermal(u, v, t, theta, geom, ops, ps, tp)
             theta = r.theta
         else:
@@ -40,7 +46,7 @@ def _run(name, steps=1):
 def test_oracle2d_one_step_matches_reference(name):
     meta, arr, (r,) = _run(name)
     tol = TOL[meta["dtype"]]
-    if "thermal" in meta and meta["dtype"] == "float32":
+    if ("thermal" in meta or "placed" in meta) and meta["dtype"] == "float32":
         tol = 1e-5  # numpy's FP32 sums and limiter against torch's: round-off of the FP32 step
     for k, got in (("u", r.u), ("v", r.v), ("p", r.p)):
         assert _rel(got, arr[f"out1_{k}"]) < tol, (k, _rel(got, arr[f"out1_{k}"]))
@@ -52,18 +58,23 @@ def test_oracle2d_one_step_matches_reference(name):
         assert _rel(r.dye, arr["out1_dye"]) < tol
     if "out1_theta" in arr:
         assert _rel(r.theta, arr["out1_theta"]) < tol, _rel(r.theta, arr["out1_theta"])
-        for key in [k[len("out1_rep_"):] for k in arr if k.startswith("out1_rep_")]:
-            ref = arr["out1_rep_" + key]
-            err = np.abs(np.asarray(r.report[key], np.float64) - ref).max() / max(1.0, np.abs(ref).max())
-            assert err < (1e-10 if meta["dtype"] == "float64" else 1e-4), (key, err)
+    for key in [k[len("out1_rep_"):] for k in arr if k.startswith("out1_rep_")]:
+        ref = arr["out1_rep_" + key]
+        err = np.abs(np.asarray(r.report[key], np.float64) - ref).max() / max(1.0, np.abs(ref).max())
+        assert err < (1e-10 if meta["dtype"] == "float64" else 1e-4), (key, err)
+    if "out1_ctrl" in arr:
+        assert np.abs(np.asarray(r.ctrl, np.float64) - arr["out1_ctrl"]).max() < 10 * tol, (r.ctrl, arr["out1_ctrl"])
 
 
-@pytest.mark.parametrize("name", [c for c in CASES_2D if c.startswith("cylinder")])
+@pytest.mark.parametrize("name", [c for c in CASES_2D if c.startswith(("cylinder", "tunnel_fans", "cavity_heater"))])
 def test_oracle2d_three_steps_match_reference(name):
     meta, arr, outs = _run(name, steps=3)
     tol = 10 * TOL[meta["dtype"]]
+    if "placed" in meta and meta["dtype"] == "float32":
+        tol = 1e-4
     r = outs[-1]
-    for k, got in (("u", r.u), ("v", r.v), ("p", r.p), ("dye", r.dye), ("theta", getattr(r, "theta", None))):
+    for k, got in (("u", r.u), ("v", r.v), ("p", r.p), ("dye", r.dye), ("theta", getattr(r, "theta", None)),
+                   ("ctrl", getattr(r, "ctrl", None)), ("dt", r.dt)):
         if f"outN_{k}" in arr:
             assert _rel(got, arr[f"outN_{k}"]) < tol, (k, _rel(got, arr[f"outN_{k}"]))
 

@@ -32,8 +32,10 @@ def test_step_full_refuses_diagnostics_and_placed_physics():
         step_full(st._replace(theta=1), None, None)
 
 
-def test_thermal_from_physics_takes_heat_only():
-    """The 2D plan reads heat transfer off the reference's Physics and refuses the rest."""
+def test_thermal_from_physics_takes_heat_and_refuses_ports_and_smoke_groups():
+    """The 2D plan reads heat transfer off the reference's Physics (fans, heaters, paint and
+    the PID step are read by the plan itself), returns None without heat transfer, and refuses
+    jets / vents and smoke channels with emitters."""
     from aerolume_b200.ns2d.plan import thermal_from_physics
     from aerolume_b200.ns2d.types import Geometry2D
     geom = Geometry2D((2, 6, 3, 9), nbody=1)
@@ -48,8 +50,10 @@ def test_thermal_from_physics_takes_heat_only():
     th = thermal_from_physics(ph, geom)
     assert th.temp_ids == (0,) and th.wall_modes[0] == "inlet" and abs(th.kappa - 0.01) < 1e-9
     assert th.a_t is geom.thermal.a_t and th.wall_values == (0.0, 0.0, 0.0, 0.0)
-    for name, val in (("nfan", 1), ("pid", True), ("paint", True), ("ports", [1]), ("heat", torch.ones(2)),
-                      ("n_dye", 2), ("thermal", False)):
+    for name, val in (("nfan", 1), ("pid", True), ("paint", True), ("heat", torch.ones(2))):
+        assert thermal_from_physics(types.SimpleNamespace(**{**vars(ph), name: val}), geom) is not None
+    assert thermal_from_physics(types.SimpleNamespace(**{**vars(ph), "thermal": False}), geom) is None
+    for name, val in (("ports", [1]), ("n_dye", 2), ("comb", True)):
         with pytest.raises(RuntimeError):
             thermal_from_physics(types.SimpleNamespace(**{**vars(ph), name: val}), geom)
 
@@ -175,3 +179,42 @@ def test_fast_step_phys_runs_the_placed_physics(name):
     if pid is not None:
         got = np.array([float(pid.dt_prev), float(pid.e1), float(pid.e2)])
         assert np.abs(got - arr["pid1"]).max() <= 1e-10 * max(1.0, np.abs(arr["pid1"]).max())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["tunnel_fans_pid_f64", "cavity_heater_paint_f64"])
+def test_step_full_fans_heaters_paint_pid_match_reference(name):
+    """step_full with ops.phys carrying fans and the PID step, or heaters and a paint layer (the
+    reference's 2D Physics attribute names): three steps chained through State.ctrl and
+    State.dt as the solver chains them, against the reference's own steps; the fans' and the
+    paint's reports in ``out``."""
+    from _golden import placed2d_from_case, thermal2d_from_case
+    from aerolume_b200.ns2d.step import State, step_full
+    meta, ops, geom, arr = load_case2d(name)
+    dt = torch.float64
+    th = thermal2d_from_case(meta, arr)
+    pl = placed2d_from_case(meta, arr)
+    ph = types.SimpleNamespace(**{k: getattr(pl, k) for k in vars(pl)}, ports=[], n_dye=0, comb=False,
+                               paint=pl.paint, thermal=th is not None)
+    if th is not None:
+        for k in ("kappa", "ri", "prt", "gravity", "eta_t", "theta_in", "wall_modes", "wall_values", "diff_coef"):
+            setattr(ph, k, getattr(th, k))
+        geom.thermal = th
+    ops.phys = ph
+    ny, nx = ops.ny, ops.nx
+    st = State(_dev(arr["in_u"], dt), _dev(arr["in_v"], dt), torch.zeros(ny, nx, device="cuda", dtype=dt),
+               _dev(arr["in_dye"], dt) if "in_dye" in arr else None, _dev(arr["in_t"], dt),
+               torch.zeros((), device="cuda", dtype=dt), _dev(arr["in_theta"], dt) if th is not None else None, None,
+               _dev(arr["in_ctrl"], dt) if "in_ctrl" in arr else None)
+    out = {}
+    new, _ = step_full(st, geom, ops, None, out=out)
+    for key in ("fan_thrust", "fan_ud", "paint_force"):
+        if f"out1_rep_{key}" in arr:
+            ref = arr[f"out1_rep_{key}"]
+            assert np.abs(out[key].cpu().numpy() - ref).max() <= 1e-9 * max(1.0, np.abs(ref).max()), key
+    for _ in range(2):
+        new, _ = step_full(new, geom, ops, None)
+    torch.cuda.synchronize()
+    for k in ("u", "v", "p", "t", "dt", "theta", "ctrl", "dye"):
+        if f"outN_{k}" in arr:
+            assert _rel(getattr(new, k), arr[f"outN_{k}"]) < 1e-9, k
