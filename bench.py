@@ -610,6 +610,22 @@ def _time_graph(g, dist, local_rank, rank, dev):
     return max_over_ranks(ms, dist, dev), clk
 
 
+def cpu_baseline_2d(workload, port_sample, cells, what):
+    """The 2D lines' cpu_baseline: the reference's own 2D solver on the host cores (kind
+    "reference"), or, when baseline/_ref holds no reference, the numpy oracle port."""
+    try:
+        steps = 10
+        per_step, cores, ref_cells, _ = time_reference_cpu_2d(workload, steps, 2)
+        return {"value": ref_cells / per_step / 1e6, "unit": UNIT, "cores": cores, "kind": "reference",
+                "sample": f"best of 3 x {steps} {what} of the reference's 2D FlowSolver.advance (device cpu, FP32) "
+                          "after 2 untimed steps"}
+    except ImportError:
+        steps = 10
+        secs = port_sample(steps)
+        return {"value": cells * steps / secs / 1e6, "unit": UNIT, "cores": _threads(), "kind": "port",
+                "sample": f"{steps} {what} of the numpy 2D oracle after 1 untimed step"}
+
+
 def oracle2d_sample(ops, geom, steps, seed=0, thermal=None):
     """Wall time of ``steps`` 2D oracle steps (after one untimed step); with ``thermal`` the
     heat-transfer step, theta starting at 0."""
@@ -729,10 +745,8 @@ def run_2d(args, rank, world, local_rank):
     ms_step = ms / K
     cpu = None
     if not args.no_cpu:
-        steps_cpu = 20
-        secs = oracle2d_sample(ops, geom, steps_cpu, thermal=thermal)
-        cpu = {"value": cells * steps_cpu / secs / 1e6, "unit": UNIT, "cores": _threads(), "kind": "port",
-               "sample": f"{steps_cpu} full {nx}x{ny} steps of the numpy 2D oracle after 1 untimed step"}
+        cpu = cpu_baseline_2d(args.workload, lambda n: oracle2d_sample(ops, geom, n, thermal=thermal), cells,
+                              f"full {nx}x{ny} steps")
     line = {"metric": METRIC, "value": world * cells * K / (ms * 1e-3) / 1e6, "unit": UNIT, "n_gpus": world,
             "steps": K, "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -826,11 +840,9 @@ def run_sweep(args, rank, world, local_rank):
     alg = 228.0 * cells
     cpu = None
     if not args.no_cpu:
-        ops0, geom0, _ = min(insts, key=lambda x: x[0].nx)
-        steps_cpu = 10
-        secs = oracle2d_sample(ops0, geom0, steps_cpu)
-        cpu = {"value": ops0.nx * ops0.ny * steps_cpu / secs / 1e6, "unit": UNIT, "cores": _threads(),
-               "kind": "port", "sample": f"{steps_cpu} steps of one {ops0.nx}x{ops0.ny} instance of the numpy 2D oracle"}
+        ops0, geom0, _ = all_insts[0]
+        cpu = cpu_baseline_2d("sweep2d", lambda n: oracle2d_sample(ops0, geom0, n), ops0.nx * ops0.ny,
+                              f"steps of the sweep's first ({ops0.nx}x{ops0.ny}) instance")
     grids = {}
     for o, _, _ in insts:
         grids[f"{o.nx}x{o.ny}"] = grids.get(f"{o.nx}x{o.ny}", 0) + 1
@@ -1424,28 +1436,69 @@ def run_reference_record(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def reference_2d_config(workload, device):
+    """The reference's 2D SolverConfig of a 2D bench workload: the cylinder tunnel (config [0]),
+    the same with the cylinder held at theta = 1, or the sweep's first NACA instance."""
+    from aerolume_b200.ns2d.workloads import circle, naca4, sweep_instances
+    _reference_api()                                  # baseline/_ref on the path (ImportError if absent)
+    import aerolume.solvers.ns2d.config as C2
+    kw = dict(bc_top="slip", bc_bottom="slip", advection="upwind3", cfl=0.5, dtype="float32", device=device,
+              dye=False, perturb=False)
+    if workload == "sweep2d":
+        ops, _, prm = sweep_instances(64, seed=0)[0]
+        body = C2.ImmersedBody(naca4(prm["t"], prm["m"], prm["p"], prm["alpha"]), name="naca")
+        return C2.SolverConfig(nx=ops.nx, ny=ops.ny, h=8.0 / ops.nx, x0=0.0, y0=0.0, re=prm["re"], bodies=[body],
+                               force_ref=1.0, moment_ref=(2.0, 2.0), **kw), f"{ops.nx}x{ops.ny}"
+    thermal = None
+    cyl = C2.ImmersedBody(circle(2.0, 2.0, 0.25, 256), name="cylinder",
+                          **({"thermal": "temperature", "thermal_value": 1.0} if workload == "heated2d" else {}))
+    if workload == "heated2d":
+        thermal = C2.ThermalConfig(prandtl=0.71, richardson=0.5)
+    return C2.SolverConfig(nx=256, ny=128, h=1.0 / 32.0, x0=0.0, y0=0.0, re=200.0, bodies=[cyl], force_ref=0.5,
+                           moment_ref=(2.0, 2.0), thermal=thermal, **kw), "256x128"
+
+
+def time_reference_cpu_2d(workload, steps, warm, repeats=3):
+    """Best-of-``repeats`` wall time per step of the reference's 2D FlowSolver.advance on the
+    host cores (device "cpu", FP32, all threads) after ``warm`` untimed steps."""
+    import torch
+    _reference_api()
+    import aerolume.solvers.ns2d.solver as S2
+    cfg, grid = reference_2d_config(workload, "cpu")
+    old = torch.get_num_threads()
+    torch.set_num_threads(os.cpu_count() or 1)
+    try:
+        s = S2.FlowSolver(cfg)
+        s.advance(warm)
+        best = float("inf")
+        for _ in range(repeats):
+            t0 = time.perf_counter()
+            s.advance(steps)
+            best = min(best, (time.perf_counter() - t0) / steps)
+        return best, torch.get_num_threads(), cfg.nx * cfg.ny, grid
+    finally:
+        torch.set_num_threads(old)
+
+
 def run_reference_2d(args, rank):
-    from aerolume_b200.ns2d.workloads import cylinder_tunnel, heated_cylinder, sweep_instances
+    """``--impl reference`` of the 2D workloads: the reference's own 2D solver on the host cores."""
     if rank != 0:
         return
-    thermal = None
-    if args.workload == "cylinder2d":
-        ops, geom = cylinder_tunnel(256, 128, "float32")
-        desc = "cylinder D=0.5 at (2,2), 256x128 FP32, Re_D 100, slip walls, upwind3, CFL 0.5"
-    elif args.workload == "heated2d":
-        ops, geom, thermal = heated_cylinder(256, 128, "float32")
-        desc = HEATED_2D
-    else:
-        ops, geom, _ = min(sweep_instances(64, seed=0), key=lambda x: x[0].nx)
-        desc = f"one {ops.nx}x{ops.ny} instance of the batched NACA sweep"
-    steps = max(1, min(args.steps, 20))
-    secs = oracle2d_sample(ops, geom, steps, thermal=thermal)
-    val = ops.nx * ops.ny * steps / secs / 1e6
+    steps = max(1, min(args.steps, 50))
+    try:
+        per_step, cores, cells, grid = time_reference_cpu_2d(args.workload, steps, 2)
+    except ImportError as exc:
+        print(json.dumps({"impl": "reference", "unavailable": f"reference not installed: {exc}"}), flush=True)
+        return
+    desc = {"cylinder2d": "cylinder D=0.5 at (2,2), 256x128 FP32, Re_D 100, slip walls, upwind3, CFL 0.5",
+            "heated2d": HEATED_2D}.get(args.workload, f"one {grid} instance of the batched NACA sweep")
+    val = cells / per_step / 1e6
+    sample = (f"best of 3 x {steps} steps of the reference's 2D FlowSolver.advance (device cpu, FP32, {cores} "
+              f"threads) on {desc} after 2 untimed steps")
     line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
-            "warmup": 1, "ms_per_step": 1e3 * secs / steps, "higher_is_better": True, "scaling": "weak",
+            "warmup": 2, "ms_per_step": 1e3 * per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": {"workload": desc},
-            "cpu_baseline": {"value": val, "unit": UNIT, "cores": _threads(), "kind": "port",
-                             "sample": f"{steps} steps of the numpy 2D oracle after 1 untimed step"},
+            "cpu_baseline": {"value": val, "unit": UNIT, "cores": cores, "kind": "reference", "sample": sample},
             "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
