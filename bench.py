@@ -788,7 +788,13 @@ def run_sweep(args, rank, world, local_rank):
     sw = Sweep2D(insts, device=dev, seeds=[1000 * rank + k for k in range(len(insts))])
     cells = sw.cells
     snap = sw.snapshot()
-    tune_table = sw.tune()
+    if args.tuning:   # a given launch shape instead of the autotuner (lcap,ctas_per_sm,order,schedule,tiles)
+        lcap, cps, order, sched, tiles = args.tuning.split(",")
+        cand = (int(lcap), int(cps), int(order), sched, int(tiles))
+        sw.use_persistent(*cand)
+        tune_table = [(sw.tuning, None, "given")]
+    else:
+        tune_table = sw.tune()
     K = args.steps
     for _ in range(args.warmup):
         sw.step("persistent")
@@ -1516,6 +1522,8 @@ def main():
     ap.add_argument("--shape", type=int, nargs=3, default=list(SHAPE), help="nx ny nz (2:1:1)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-ref-gpu", action="store_true", help="skip timing the reference's CUDA step")
+    ap.add_argument("--tuning", default=None,
+                    help="sweep2d: lcap,ctas_per_sm,order,schedule,tiles instead of the autotuner (e.g. 2,3,1,queue,4)")
     ap.add_argument("--shard", action="store_true",
                     help="sweep2d with N > 1: split the 64 instances over the ranks instead of replicating them")
     args = ap.parse_args()
