@@ -230,6 +230,9 @@ struct StageParams {
   const T *fan_gu, *fan_gv, *fan_thrust;
   const T *paint_u, *paint_v, *paint_wu, *paint_wv;
   double *paint_part;
+  // the combined penalisation of jets / vents and paint, (u + k xa) / (1 + k xchi) (xa NULL:
+  // paint alone), and the ports' net volume flow joining the outlet balance (core.py:352-356)
+  const T *xchi_u, *xa_u, *xchi_v, *xa_v, *q_net;
 };
 
 // One RK stage of the u- and v-faces of a 32 x 8 tile; NU_ONLY: only the maximum eddy
@@ -280,6 +283,7 @@ __device__ __forceinline__ void stage2d_body(const StageParams<T> &P, int bx, in
     }
     s_in = warp_sum(s_in);
     s_out = warp_sum(s_out);
+    if (PLACED && P.q_net) s_in = s_in + (double)(*P.q_net * P.inv_h);
     if (tid == 0) corr_s = T((s_in - s_out) / (double)ny);
   }
   if (P.psi) {  // the previous stage's projection, applied while staging the tile
@@ -401,9 +405,9 @@ __device__ __forceinline__ void stage2d_body(const StageParams<T> &P, int bx, in
       uh = un;
       pen = true;
     }
-    if (PLACED && P.paint_u) {   // the paint, after the bodies: (u + k * 0) / (1 + k chi)
-      const T pu = P.paint_u[g], un = uh / (T(1) + k_pen * pu);
-      pimp += (double)((un - uh) * P.paint_wu[g]) * (double)P.w;
+    if (PLACED && P.xchi_u) {   // jets / vents and paint, after the bodies (physics.py:675-683)
+      const T un = (uh + k_pen * (P.xa_u ? P.xa_u[g] : T(0))) / (T(1) + k_pen * P.xchi_u[g]);
+      if (P.paint_wu) pimp += (double)((un - uh) * P.paint_wu[g]) * (double)P.w;
       uh = un;
     }
     if (HEAT && P.buoy_u) {  // face average of theta (0 on boundary faces of a bounded domain)
@@ -452,9 +456,9 @@ __device__ __forceinline__ void stage2d_body(const StageParams<T> &P, int bx, in
       vh = vn;
       pen = true;
     }
-    if (PLACED && P.paint_v) {
-      const T pv = P.paint_v[g], vn = vh / (T(1) + k_pen * pv);
-      pimp_v += (double)((vn - vh) * P.paint_wv[g]) * (double)P.w;
+    if (PLACED && P.xchi_v) {
+      const T vn = (vh + k_pen * (P.xa_v ? P.xa_v[g] : T(0))) / (T(1) + k_pen * P.xchi_v[g]);
+      if (P.paint_wv) pimp_v += (double)((vn - vh) * P.paint_wv[g]) * (double)P.w;
       vh = vn;
     }
     if (HEAT && P.buoy_v) {
@@ -681,7 +685,7 @@ __global__ void dye2d_kernel(const __grid_constant__ DyeParams<T> P) {
 
 template <typename T>
 struct Control2dParams {
-  int nx, ny, nfan, pid, dt_mode, les, heat;
+  int nx, ny, nfan, pid, dt_mode, les, heat, ports;
   const T *dt_in;
   double dt_fixed, cfl_h, nu, visc_h2;
   const unsigned long long *bits;
@@ -734,7 +738,7 @@ __global__ void __launch_bounds__(1024) control2d_kernel(const __grid_constant__
   } else if (P.dt_mode == 1) {
     dt = T(P.dt_fixed);
   } else {
-    const Dt2dPlaced<T> pl{P.nfan > 0, *P.u_floor, P.heat_max ? *P.heat_max : T(-1)};
+    const Dt2dPlaced<T> pl{P.nfan > 0 || P.ports, *P.u_floor, P.heat_max ? *P.heat_max : T(-1)};
     Dt2dThermal th = P.th;
     if (HEAT && P.live_kappa) th.kappa = (double)*P.live_kappa;
     dt = dt2d_value<T, HEAT>(0, nullptr, 0.0, P.bits, P.cfl_h, P.live_nu ? (double)*P.live_nu : P.nu, P.visc_h2,
@@ -786,6 +790,14 @@ __global__ void __launch_bounds__(1024) control2d_kernel(const __grid_constant__
   }
 }
 
+// The projection's right-hand side with the ports' mass source: div - src (core.py:636-638)
+template <typename T>
+__global__ void port_source2d_kernel(T *__restrict__ rhs, const T *__restrict__ src, size_t n) {
+  aero::pdl_wait();
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x)
+    rhs[e] = rhs[e] - src[e];
+}
+
 // The painted obstacles' force coefficients [Cd, Cl] from the stages' impulse sums
 // (core.py:1001-1002): one warp per component, a fixed lane order.
 template <typename T>
@@ -804,7 +816,7 @@ __global__ void paint_force2d_kernel(const double *__restrict__ part, int nblock
 // ---------------------------------------------------------------------------------------
 // heat transfer (ns2d/physics.py:623-923 with scalar.py:34-146)
 // ---------------------------------------------------------------------------------------
-constexpr int MAXR = 2 * AERO_MAX_BODIES + 2;  // per-block partials: heat, then sums and wall weights
+constexpr int MAXR = 2 * AERO_MAX_BODIES + 3;  // per-block partials: heat, then sums, wall weights, vent sum
 
 template <typename T>
 struct ThetaParams {
@@ -828,6 +840,12 @@ struct ThetaParams {
   // placed physics: the heaters' density (ny, nx), added after the diffusion (physics.py:721-722),
   // and the paint's face fractions, which scale the face diffusivity by 1 - chi (:715-717)
   const T *heat, *paint_u, *paint_v;
+  // jets and vents: the vents' sinks src_neg (ny, nx), whose fluid leaves with its heat
+  // (physics.py:727-728); the jets' penalisation toward their temperature (:753-756) with the
+  // stage's per-block sums of the increments (jet_part); the last stage also sums
+  // src_neg theta for the vent heat (one more rep_part entry)
+  const T *src_neg, *pt_chi, *pt_a;
+  double *jet_part;
 };
 
 // theta at (j, i) with the ghosts of scalar.py:63-78: periodic wrap; else the first / last
@@ -922,7 +940,8 @@ __global__ void __launch_bounds__(NT) theta2d_kernel(const __grid_constant__ The
   __syncthreads();
   const int j = j0 + ty, i = i0 + tx;
   const bool in = j < ny && i < nx;
-  const int nh = P.n_temp, nr = P.rep_part ? 2 + P.n_flux : 0;
+  const int nh = P.n_temp, nr = P.rep_part ? 2 + P.n_flux + (P.src_neg ? 1 : 0) : 0;
+  double jet = 0.0;
   double acc[MAXR];
 #pragma unroll
   for (int q = 0; q < MAXR; ++q) acc[q] = 0.0;
@@ -963,6 +982,7 @@ __global__ void __launch_bounds__(NT) theta2d_kernel(const __grid_constant__ The
     const size_t widx = inwin ? (size_t)(j - P.win[0]) * (P.win[3] - P.win[2]) + (i - P.win[2]) : 0;
     const size_t wsz = (size_t)(P.win[1] - P.win[0]) * (P.win[3] - P.win[2]);
     if (inwin && P.q_skin) lt = lt + kappa_of<T>(P) * __ldg(P.q_skin + widx);
+    if (P.src_neg) lt = lt + __ldg(P.src_neg + (size_t)j * nx + i) * ctr;
     const T bdt = *P.dt * P.b;
     const size_t g = (size_t)j * nx + i;
     const T t0 = __ldg(P.th0 + g);
@@ -974,13 +994,31 @@ __global__ void __launch_bounds__(NT) theta2d_kernel(const __grid_constant__ The
       for (int b = 0; b < nh; ++b) acc[b] = (double)__ldg(P.w_t + (size_t)b * wsz + widx) * d;
       th = tn;
     }
+    if (P.pt_chi) {
+      const T kt = bdt / (P.live_eta_t ? __ldg(P.live_eta_t) : P.eta_t);
+      const T tn = (th + kt * __ldg(P.pt_a + g)) / (T(1) + kt * __ldg(P.pt_chi + g));
+      jet = (double)(tn - th);
+      th = tn;
+    }
     if (nr) {
       acc[nh] = (double)th;
       acc[nh + 1] = (double)t0;
       if (inwin)
         for (int b = 0; b < P.n_flux; ++b) acc[nh + 2 + b] = (double)__ldg(P.w_f + (size_t)b * wsz + widx) * (double)th;
+      if (P.src_neg) acc[nh + 2 + P.n_flux] = (double)(__ldg(P.src_neg + g) * th);
     }
     P.th[g] = th;
+  }
+  if (P.jet_part) {   // the jets' heat of this stage: per warp, then the block in order
+    __shared__ double jred[NT / 32];
+    const double js = warp_sum(jet);
+    if ((tid & 31) == 0) jred[tid >> 5] = js;
+    __syncthreads();
+    if (tid == 0) {
+      double t = 0.0;
+      for (int w = 0; w < NT / 32; ++w) t += jred[w];
+      P.jet_part[(size_t)blockIdx.y * gridDim.x + blockIdx.x] = t;
+    }
   }
   const int nq = nh + nr;
   if (nq == 0) return;
@@ -1009,9 +1047,12 @@ struct ReportParams {
   T wval[4];
   T wgt[3];
   const double *heat_part;    // (3, nblocks, n_temp)
-  const double *rep_part;     // (nblocks, 2 + n_flux)
+  const double *rep_part;     // (nblocks, 2 + n_flux (+1 with ports))
   const T *theta, *u, *dt;
   double *heat, *theta_wall, *wall_heat, *heat_storage, *flow_heat;
+  int ports;                  // jets and vents: the vent heat, and (jet_part) the jets' heat
+  const double *jet_part;     // (3, nblocks) or NULL
+  double *jet_heat, *vent_heat;
 };
 
 // The step's heat report (core.py:974-995, physics.py:760-794): one block, each warp takes
@@ -1024,9 +1065,27 @@ __global__ void heat_report2d_kernel(const __grid_constant__ ReportParams<T> P) 
   const int nx = P.nx, ny = P.ny, lane = threadIdx.x & 31, nwarp = blockDim.x >> 5;
   const T dt = *P.dt;
   const double per_dt = (double)(P.h2 / dt);
-  const int nh = P.n_temp, nr = 2 + P.n_flux, nb = P.nblocks;
-  const int ntask = nh + 1 + P.n_flux + 4 + 1;
+  const int nh = P.n_temp, nr = 2 + P.n_flux + (P.ports ? 1 : 0), nb = P.nblocks;
+  const int ntask = nh + 1 + P.n_flux + 4 + 1 + (P.ports ? 2 : 0);
   for (int task = threadIdx.x >> 5; task < ntask; task += nwarp) {
+    if (P.ports && task >= ntask - 2) {
+      if (task == ntask - 2) {   // heat leaving with the vents' fluid: -sum src_neg theta h^2
+        double s = 0.0;
+        for (int e = lane; e < nb; e += 32) s += P.rep_part[(size_t)e * nr + 2 + P.n_flux];
+        s = warp_sum(s);
+        if (lane == 0 && P.vent_heat) P.vent_heat[0] = -s * (double)P.h2;
+      } else if (P.jet_part) {   // the jets' heat: the weighted stage sums times h^2 / dt
+        double tot = 0.0;
+        for (int st = 0; st < 3; ++st) {
+          double s = 0.0;
+          for (int e = lane; e < nb; e += 32) s += P.jet_part[(size_t)st * nb + e];
+          s = warp_sum(s);
+          tot = st == 0 ? s * (double)P.wgt[0] : tot + s * (double)P.wgt[st];
+        }
+        if (lane == 0 && P.jet_heat) P.jet_heat[0] = tot * per_dt;
+      }
+      continue;
+    }
     if (task < nh) {  // heat of temperature body `task`
       const int b = task;
       double tot = 0.0;
@@ -1448,7 +1507,7 @@ struct AeroNs2dPlan {
   size_t nu, nv, nc;          // element counts of u, v and cells
   size_t off_uh, off_vh, off_up, off_vp, off_pa, off_small, off_scalars, off_zero, off_partials, total;
   size_t off_nut, off_tb0, off_tb1, off_hpart, off_rpart, off_upf, off_vpf;  // heat transfer only
-  size_t off_thrust = 0, off_ppart = 0;   // placed physics: the fans' thrusts, the paint's impulse sums
+  size_t off_thrust = 0, off_ppart = 0, off_jpart = 0;   // fans' thrusts, paint's impulse and jets' heat sums
   // heat transfer: each theta stage runs on a side stream, forked after its stage kernel and
   // joined before the next one, so it overlaps the stage's pressure solve
   cudaStream_t side = nullptr;
@@ -1629,7 +1688,7 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
   S.eta = T(c.eta);
   S.nbody = has_win ? c.nbody : 0;
   const dim3 grid(p->gx, p->gy), block(TX, TY);
-  const bool placed = c.nfan || c.pid || c.paint || c.heaters;
+  const bool placed = c.nfan || c.pid || c.paint || c.heaters || c.ports;
   if (rec && (!std::is_same<T, float>::value || les || thermal || c.dye || dt_mode != 0 || placed))
     return set_error(AERO_EUNSUPPORTED, "the persistent sweep runs FP32 plans without LES, heat transfer, dye or "
                                         "placed physics, with the CFL time step");
@@ -1637,7 +1696,7 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
     return set_error(AERO_EINVAL, "fans and the PID step need the controller memory (ctrl0, ctrl) and dt_prev");
   // fans, the PID controller and the heaters' bounds act on the step before the first stage:
   // the control kernel computes dt (and the thrusts) and the stages read it
-  const bool control = c.nfan || (dt_mode == 0 && (c.pid || c.heaters));
+  const bool control = c.nfan || (dt_mode == 0 && (c.pid || c.heaters || c.ports));
   if (placed) {
     S.nfan = c.nfan;
     S.fan_gu = static_cast<const T *>(g->fan_gu);
@@ -1648,6 +1707,18 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
       S.paint_v = static_cast<const T *>(g->paint_v);
       S.paint_wu = static_cast<const T *>(g->paint_wu);
       S.paint_wv = static_cast<const T *>(g->paint_wv);
+    }
+    if (c.ports) {   // the combined port / paint penalisation
+      S.xchi_u = static_cast<const T *>(g->xchi_u);
+      S.xa_u = static_cast<const T *>(g->xa_u);
+      S.xchi_v = static_cast<const T *>(g->xchi_v);
+      S.xa_v = static_cast<const T *>(g->xa_v);
+      S.q_net = static_cast<const T *>(g->q_net);
+      if (!(S.xchi_u && S.xa_u && S.xchi_v && S.xa_v && S.q_net && g->src && g->src_neg))
+        return set_error(AERO_EINVAL, "a jets / vents array is missing");
+    } else if (c.paint) {
+      S.xchi_u = S.paint_u;
+      S.xchi_v = S.paint_v;
     }
   }
   if (dt_mode == 0) {
@@ -1698,6 +1769,7 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
     K.ny = ny;
     K.nfan = c.nfan;
     K.pid = c.pid;
+    K.ports = c.ports;
     K.dt_mode = dt_mode;
     K.les = les ? 1 : 0;
     K.dt_in = static_cast<const T *>(dt_in);
@@ -1791,7 +1863,7 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
   // ---- stages
   static const double RK[3][3] = {{0.0, 1.0, 1.0 / 6.0}, {0.75, 0.25, 2.0 / 3.0}, {1.0 / 3.0, 2.0 / 3.0, 1.0}};
   T *p_out = static_cast<T *>(f->p);
-  const bool fused = p->ax[0].method == 0 && aero::transform_pow2(nx);
+  const bool fused = p->ax[0].method == 0 && aero::transform_pow2(nx) && !c.ports;
   // stage values alternate between two buffer pairs; stages 2 and 3 project the previous
   // stage's value themselves while staging it (P.psi), so only the last stage runs
   // correct2d_kernel, into the caller's u, v
@@ -1844,6 +1916,10 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
       Q.heat = c.heaters ? static_cast<const T *>(g->heat) : nullptr;
       Q.paint_u = c.paint ? static_cast<const T *>(g->paint_u) : nullptr;
       Q.paint_v = c.paint ? static_cast<const T *>(g->paint_v) : nullptr;
+      Q.src_neg = c.ports ? static_cast<const T *>(g->src_neg) : nullptr;
+      Q.pt_chi = c.ports ? static_cast<const T *>(g->pt_chi) : nullptr;
+      Q.pt_a = c.ports ? static_cast<const T *>(g->pt_a) : nullptr;
+      Q.jet_part = Q.pt_chi ? reinterpret_cast<double *>(ws + p->off_jpart) + (size_t)st * p->nblocks : nullptr;
       AERO_CUDA_TRY(cudaEventRecord(p->ev_fork[st], s));
       AERO_CUDA_TRY(cudaStreamWaitEvent(p->side, p->ev_fork[st], 0));
       (void)aero::launch_k(theta2d_kernel<T>, grid, block, 0, p->side, Q);
@@ -1878,6 +1954,11 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
       (void)aero::launch_k(divergence2d_kernel<T>, dim3((nx + 127) / 128, ny), 128, 0, s, nx, ny, T(1.0 / c.h),
                            ub[st % 2], vb[st % 2], pa);
       AERO_CUDA_TRY(cudaGetLastError());
+      if (c.ports) {
+        (void)aero::launch_k(port_source2d_kernel<T>, (int)std::min<size_t>((p->nc + 255) / 256, 148 * 8), 256, 0, s,
+                             pa, static_cast<const T *>(g->src), p->nc);
+        AERO_CUDA_TRY(cudaGetLastError());
+      }
       const int rc = poisson2d_passes<T>(p, pa, pa, ws, s);
       if (rc) return rc;
       AERO_CUDA_TRY(aero::launch_psi_accumulate<T>(pa, p_out, p->nc, T(RK[st][2]), acc_mode, small, s));
@@ -1926,6 +2007,10 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
     R.wall_heat = static_cast<double *>(f->wall_heat);
     R.heat_storage = static_cast<double *>(f->heat_storage);
     R.flow_heat = static_cast<double *>(f->flow_heat);
+    R.ports = c.ports;
+    R.jet_part = c.ports && g->pt_chi ? reinterpret_cast<const double *>(ws + p->off_jpart) : nullptr;
+    R.jet_heat = static_cast<double *>(f->jet_heat);
+    R.vent_heat = static_cast<double *>(f->vent_heat);
     (void)aero::launch_k(heat_report2d_kernel<T>, 1, 256, 0, s, R);
     AERO_CUDA_TRY(cudaGetLastError());
   }
@@ -2041,12 +2126,13 @@ int aero_ns2d_plan_create(const AeroNs2dConfig *cfg, AeroNs2dPlan **plan) {
   p->off_partials = take(sizeof(double) * 3 * (size_t)p->nblocks * std::max(p->nq, 1));
   if (c.nfan) p->off_thrust = take((size_t)c.nfan * e);
   if (c.paint) p->off_ppart = take(sizeof(double) * 3 * (size_t)p->nblocks * 2);
+  if (c.ports && c.thermal) p->off_jpart = take(sizeof(double) * 3 * (size_t)p->nblocks);
   if (c.thermal) {
     p->off_nut = take(p->nc * e);
     p->off_tb0 = take(p->nc * e);
     p->off_tb1 = take(p->nc * e);
     p->off_hpart = take(sizeof(double) * 3 * (size_t)p->nblocks * std::max(c.n_temp, 1));
-    p->off_rpart = take(sizeof(double) * (size_t)p->nblocks * (2 + c.n_flux));
+    p->off_rpart = take(sizeof(double) * (size_t)p->nblocks * (3 + c.n_flux));
     p->off_upf = take(p->nu * e);
     p->off_vpf = take(p->nv * e);
     bool ok = cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking) == cudaSuccess;

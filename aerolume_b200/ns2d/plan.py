@@ -5,10 +5,10 @@ src/aerolume/solvers/ns2d/core.py:67-108 and geometry.py:160-182, or the contain
 :mod:`aerolume_b200.ns2d.types`), turns the boundary types into the ghost-cell rules of
 core.py:271-325, uploads the window masks once and owns the device workspace.  Heat
 transfer comes from ``thermal=`` (a :class:`~aerolume_b200.ns2d.types.Thermal2D`) or from the
-reference's ``ops.phys`` with ``geom.thermal``; fans, heaters, painted obstacles and the PID
-step come from ``placed=`` (a :class:`~aerolume_b200.ns2d.types.Placed2D`) or from ``ops.phys``
-itself.  Jets and vents, smoke channels with emitters, the wall model and body forcing raise
-``RuntimeError``: there is no fallback to a CPU or plain-torch path.
+reference's ``ops.phys`` with ``geom.thermal``; fans, heaters, painted obstacles, jets and
+vents and the PID step come from ``placed=`` (a :class:`~aerolume_b200.ns2d.types.Placed2D`)
+or from ``ops.phys`` itself.  Smoke channels with emitters (or port smoke), the wall model and
+body forcing raise ``RuntimeError``: there is no fallback to a CPU or plain-torch path.
 """
 from __future__ import annotations
 
@@ -65,9 +65,8 @@ def ghost_rules(ops):
 def thermal_from_physics(ph, geom):
     """The heat transfer of the reference's 2D ``Physics`` (physics.py:291-345) and
     ``geom.thermal`` (None when it has none); raises when the physics places anything the B200
-    step does not run (jets and vents, smoke channels with emitters)."""
-    others = [n for n, on in (("ports", bool(getattr(ph, "ports", None))),
-                              ("smoke groups", int(getattr(ph, "n_dye", 0) or 0) > 0 or bool(getattr(ph, "comb", False))))
+    step does not run (smoke channels with emitters or port smoke)."""
+    others = [n for n, on in (("smoke groups", int(getattr(ph, "n_dye", 0) or 0) > 0 or bool(getattr(ph, "comb", False))),)
               if on]
     if others:
         raise RuntimeError("placed physics (" + ", ".join(others) + ") is not in the B200 2D step")
@@ -278,6 +277,16 @@ class Ns2dPlan:
                 setattr(g, name, arr(getattr(pl, name), shape))
         self.pid = bool(getattr(pl, "pid", False))
         cfg.pid = int(self.pid)
+        self.ports = bool(getattr(pl, "ports", False))
+        if self.ports:   # jets and vents (physics.py:362-433) with the combined penalisation
+            cfg.ports = 1
+            for name, shape in (("xchi_u", (ny, nx + 1)), ("xa_u", (ny, nx + 1)), ("xchi_v", (ny + 1, nx)),
+                                ("xa_v", (ny + 1, nx)), ("src", (ny, nx)), ("src_neg", (ny, nx))):
+                setattr(g, name, arr(getattr(pl, name), shape))
+            g.q_net = arr(getattr(pl, "q_net", 0.0), ())
+            if thermal and getattr(pl, "pt_chi", None) is not None:
+                g.pt_chi = arr(pl.pt_chi, (ny, nx))
+                g.pt_a = arr(pl.pt_a, (ny, nx))
 
     @property
     def ctrl_size(self):
@@ -317,6 +326,11 @@ class Ns2dPlan:
             out["fan_ud"] = torch.zeros(self.nfan, **kw)
         if self.cfg.paint:
             out["paint_force"] = torch.zeros(2, **kw)
+        if self.cfg.ports and self.thermal is not None:
+            d64 = dict(device=self.device, dtype=torch.float64)
+            out["vent_heat"] = torch.zeros(1, **d64)
+            if self.geom_c.pt_chi:
+                out["jet_heat"] = torch.zeros(1, **d64)
         return out
 
     def _check(self, name, t, shape):
@@ -376,6 +390,9 @@ class Ns2dPlan:
             f.fan_thrust, f.fan_ud = out["fan_thrust"].data_ptr(), out["fan_ud"].data_ptr()
         if self.cfg.paint:
             f.paint_force = out["paint_force"].data_ptr()
+        for name in ("vent_heat", "jet_heat"):
+            if name in out:
+                setattr(f, name, out[name].data_ptr())
         dtp = None
         if dt is not None:
             self._check("dt", dt, ())

@@ -6,10 +6,11 @@ served by the B200 step.
 ``aerolume.solvers.ns2d.solver.step_full`` to this function swaps the step.  It returns
 ``(State, coeffs (nbody, 3))`` of new tensors like the reference.  With heat transfer theta
 advances too and ``out`` receives the heat report of core.py:974-995; fans, heaters, painted
-obstacles and the PID step of ``ops.phys`` run in the step, ``state.ctrl`` carries the
-controllers' memory and ``out`` receives ``fan_thrust``, ``fan_ud`` and ``paint_force`` as
-core.py:998-1002 fills them.  Jets and vents, smoke channels with emitters, the wall model,
-diagnostics rows and traces raise instead of being computed differently.
+obstacles, jets and vents and the PID step of ``ops.phys`` run in the step, ``state.ctrl``
+carries the controllers' memory and ``out`` receives ``fan_thrust``, ``fan_ud``,
+``paint_force``, ``vent_heat`` and ``jet_heat`` as core.py:987-1002 fills them.  Smoke channels
+with emitters or port smoke, the wall model, diagnostics rows and traces raise instead of
+being computed differently.
 """
 from __future__ import annotations
 
@@ -91,7 +92,7 @@ def step_full(state, geom, ops, dt=None, *, out=None, diag=False, trace=None):
         for k in keys:
             out[k] = res[k].to(state.u.dtype)
     if out is not None:
-        for k in ("fan_thrust", "fan_ud", "paint_force"):
+        for k in ("fan_thrust", "fan_ud", "paint_force", "vent_heat", "jet_heat"):
             if k in res:
                 out[k] = res[k]
     coeffs = res["coeffs"] if plan.nbody and plan.has_win else torch.zeros(0, 3, device=state.u.device,

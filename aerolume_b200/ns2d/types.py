@@ -123,3 +123,13 @@ class Placed2D:
     paint_wu: Any = None         # the paint's force weights on the faces
     paint_wv: Any = None
     pid: bool = False
+    ports: bool = False          # jets and vents: the combined port / paint penalisation on the
+    xchi_u: Any = None           # faces, the ports' mass source, the vents' sinks, the net
+    xa_u: Any = None             # volume flow and the jets' temperature penalisation
+    xchi_v: Any = None
+    xa_v: Any = None
+    src: Any = None
+    src_neg: Any = None
+    q_net: Any = 0.0
+    pt_chi: Any = None
+    pt_a: Any = None

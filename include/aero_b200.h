@@ -494,6 +494,7 @@ typedef struct {
    * obstacles, the PID-controlled step (diagnostics.py:104-124); their fields are in
    * AeroNs2dGeom, the controller memory in AeroNs2dFields */
   int32_t nfan, heaters, paint, pid;
+  int32_t ports;                /* jets and vents (physics.py:362-433)                      */
 } AeroNs2dConfig;
 
 /* temperature boundary modes of a 2D side (ns2d/scalar.py:96-146) */
@@ -526,6 +527,11 @@ typedef struct {
       *fan_isvel, *fan_isthrust, *u_floor;
   const void *heat, *heat_max;
   const void *paint_c, *paint_u, *paint_v, *paint_wu, *paint_wv;
+  /* jets and vents, with paint the combined penalisation: xchi_u, xa_u (ny, nx+1), xchi_v,
+   * xa_v (ny+1, nx) (paint alone: xchi = paint, xa NULL); the ports' mass source src and the
+   * vents' sinks src_neg (ny, nx), their net volume flow q_net (0-d), the jets' temperature
+   * penalisation pt_chi, pt_a (ny, nx; NULL without heat transfer or jets) */
+  const void *xchi_u, *xa_u, *xchi_v, *xa_v, *src, *src_neg, *q_net, *pt_chi, *pt_a;
 } AeroNs2dGeom;
 
 /* Step inputs (u0, v0, t0, dye0) and outputs; u / v may alias u0 / v0. */
@@ -545,6 +551,9 @@ typedef struct {
    * (nfan each) and the painted obstacles' force coefficients [Cd, Cl] (2) */
   const void *dt_prev, *ctrl0;
   void *ctrl, *fan_thrust, *fan_ud, *paint_force;
+  /* jets and vents with heat transfer (double, 1 each): the heat the jets add and the heat
+   * leaving with the vents' fluid (core.py:990-993) */
+  void *jet_heat, *vent_heat;
 } AeroNs2dFields;
 
 int aero_ns2d_plan_create(const AeroNs2dConfig *cfg, AeroNs2dPlan **plan);

@@ -763,6 +763,19 @@ class Placed2D:
     paint_v: np.ndarray | None = None
     paint_wu: np.ndarray | None = None
     paint_wv: np.ndarray | None = None
+    # jets and vents (physics.py:362-433): the combined port / paint penalisation (xchi, xa on
+    # the faces), the mass source of the projection, the vents' sinks (with the uniform leak of
+    # a closed box), the net volume flow, the jets' temperature penalisation
+    ports: bool = False
+    xchi_u: np.ndarray | None = None
+    xa_u: np.ndarray | None = None
+    xchi_v: np.ndarray | None = None
+    xa_v: np.ndarray | None = None
+    src: np.ndarray | None = None
+    src_neg: np.ndarray | None = None
+    q_net: float = 0.0
+    pt_chi: np.ndarray | None = None
+    pt_a: np.ndarray | None = None
 
     @property
     def paint(self):
@@ -811,7 +824,7 @@ def fan_control2d(u, v, ctrl, dt, pl):
 def placed_dt_limit2d(dt, u, v, theta, nut_max, tp, pl, ops):
     """physics.py:851-884 with the sources' speed floor and the heaters' bounds."""
     T = u.dtype.type
-    if pl is not None and pl.nfan:
+    if pl is not None and (pl.nfan or pl.ports):
         dt = min(dt, T(ops.cfl) * T(ops.h) / max(T(pl.u_floor), T(1e-6)))
     if tp is not None and theta is not None:
         kap = T(tp.kappa) if nut_max is None else T(tp.kappa) + nut_max * T(1.0 / tp.prt)
@@ -863,6 +876,8 @@ def theta_rhs2d_placed(th, u, v, nut, geom, tp, pl, ops):
         j0, j1, i0, i1 = geom.window
         lt = lt.copy()
         lt[j0:j1, i0:i1] = lt[j0:j1, i0:i1] + kappa * tp.q_skin
+    if pl is not None and pl.ports:
+        lt = lt + pl.src_neg * th                 # fluid leaving through a vent takes its heat along
     return lt
 
 
@@ -875,10 +890,11 @@ def step2d_placed(u0, v0, t, geom, ops, poisson, *, tp=None, pl=None, theta0=Non
     up, vp = u0, v0
     thermal = tp is not None and theta0 is not None
     thp = theta0
-    acc_u = acc_v = psi_w = heat_acc = paint_acc = None
+    acc_u = acc_v = psi_w = heat_acc = paint_acc = jet_acc = None
     fan_f = fan_thrust = fan_ud = None
     les = ops.turbulence != "none"
     paint = pl is not None and pl.paint
+    ports = pl is not None and pl.ports
     for s, ((a, b), w) in enumerate(zip(SSP_RK3, FORCE_WEIGHTS)):
         lu, lv, nut_max = momentum_rhs2d(up, vp, geom, ops)
         nut = sgs_divergence2d.nut if (les and thermal) else None
@@ -910,17 +926,30 @@ def step2d_placed(u0, v0, t, geom, ops, poisson, *, tp=None, pl=None, theta0=Non
         if lt is not None:
             thh = (thp if a == 0.0 else lerp(thp, theta0, a)) + lt * bdt
         if not ops.periodic:
-            uh = inlet_outlet(uh, ops)
+            if ports and not ops.closed:   # core.py:352-356: the outflow also carries the ports' net flow
+                T_ = uh.dtype.type
+                uh = uh.copy()
+                corr = ((np.asarray(ops.u_inlet, dtype=uh.dtype).sum(dtype=uh.dtype) + T_(pl.q_net) * T_(1.0 / ops.h))
+                        - uh[:, -1].sum(dtype=uh.dtype)) / T_(ops.ny)
+                uh[:, 0] = np.asarray(ops.u_inlet, dtype=uh.dtype)
+                uh[:, -1] = uh[:, -1] + corr
+            else:
+                uh = inlet_outlet(uh, ops)
         if not geom.empty:
             uh, vh, du, dv = penalise2d(uh, vh, geom, ops, bdt)
             acc_u = du * T(w) if acc_u is None else acc_u + du * T(w)
             acc_v = dv * T(w) if acc_v is None else acc_v + dv * T(w)
-        if paint:   # physics.py:675-683: the paint's implicit penalisation and impulse
+        if paint or ports:   # physics.py:675-683: the combined penalisation, the paint's impulse
             k = T(bdt / T(ops.eta))
-            un = uh / (T(1.0) + k * pl.paint_u)
-            vn = vh / (T(1.0) + k * pl.paint_v)
-            imp = np.array([((un - uh) * pl.paint_wu).sum(), ((vn - vh) * pl.paint_wv).sum()], dtype=np.float64)
-            paint_acc = imp * float(T(w)) if paint_acc is None else paint_acc + imp * float(T(w))
+            if ports:
+                un = (uh + k * pl.xa_u) / (T(1.0) + k * pl.xchi_u)
+                vn = (vh + k * pl.xa_v) / (T(1.0) + k * pl.xchi_v)
+            else:
+                un = uh / (T(1.0) + k * pl.paint_u)
+                vn = vh / (T(1.0) + k * pl.paint_v)
+            if paint:
+                imp = np.array([((un - uh) * pl.paint_wu).sum(), ((vn - vh) * pl.paint_wv).sum()], dtype=np.float64)
+                paint_acc = imp * float(T(w)) if paint_acc is None else paint_acc + imp * float(T(w))
             uh, vh = un, vn
         if thermal and tp.ri != 0.0:  # core.py:774-813
             fu, fv = buoyancy2d(thp, tp, ops)
@@ -940,14 +969,24 @@ def step2d_placed(u0, v0, t, geom, ops, poisson, *, tp=None, pl=None, theta0=Non
                 su = float((fu * pl.paint_u * pl.paint_wu).sum()) if fu is not None else 0.0
                 sv = float((fv * pl.paint_v * pl.paint_wv).sum()) if fv is not None else 0.0
                 paint_acc = paint_acc + np.array([su, sv]) * float(bdt * T(w))
-        if ops.periodic and (paint or not geom.empty):
+        if ops.periodic and (paint or ports or not geom.empty):
             uh, vh = apply_boundary_values(uh, vh, ops)
         if lt is not None:
             thh, heat = penalise_theta2d(thh, geom, tp, bdt)
             if heat is not None:
                 heat_acc = heat * float(T(w)) if heat_acc is None else heat_acc + heat * float(T(w))
+            if ports and pl.pt_chi is not None:   # physics.py:753-756: the jets' temperature
+                kt = T(bdt / T(tp.eta_t))
+                tn = (thh + kt * pl.pt_a) / (T(1.0) + kt * pl.pt_chi)
+                jh = float((tn - thh).astype(np.float64).sum())
+                jet_acc = jh * float(T(w)) if jet_acc is None else jet_acc + jh * float(T(w))
+                thh = tn
             thp = thh
-        up, vp, psi = project2d(uh, vh, ops, poisson)
+        if ports:   # core.py:626-642: div u = the ports' mass source
+            psi = poisson.solve(divergence2d(uh, vh, ops.h) - pl.src)
+            up, vp = correct2d(uh, vh, psi, ops)
+        else:
+            up, vp, psi = project2d(uh, vh, ops, poisson)
         psi_w = psi * T(w) if psi_w is None else psi_w + T(w) * psi
     p = psi_w * (T(1.0) / dt)
     coeffs = force_coefficients2d(acc_u, acc_v, geom, ops, dt)
@@ -961,6 +1000,11 @@ def step2d_placed(u0, v0, t, geom, ops, poisson, *, tp=None, pl=None, theta0=Non
     res.theta = thp if thermal else None
     res.ctrl = ctrl
     res.report = heat_report2d(theta0, thp, up, heat_acc, geom, tp, ops, dt) if thermal else {}
+    if thermal and ports:
+        h2 = ops.h * ops.h
+        res.report["vent_heat"] = np.array([-float((pl.src_neg * thp).astype(np.float64).sum()) * h2])
+        if jet_acc is not None:
+            res.report["jet_heat"] = np.array([jet_acc * h2 / float(dt)])
     if fan_thrust is not None:
         res.report["fan_thrust"] = fan_thrust
         res.report["fan_ud"] = fan_ud

@@ -135,13 +135,15 @@ def placed2d_from_case(meta, arr):
     """The oracle's Placed2D (fans, heaters, paint, the PID step) of a 2D golden case, or None."""
     from oracle.ns2d import Placed2D
     pm = meta.get("placed")
-    if pm is None or not (pm["nfan"] or pm["pid"] or pm["paint"] or pm["heat"]):
+    if pm is None or not (pm["nfan"] or pm["pid"] or pm["paint"] or pm["heat"] or pm.get("ports")):
         return None
     dt = np.float64 if meta["dtype"] == "float64" else np.float32
     kw = {n: arr[n].astype(dt) for n in ("fan_gu", "fan_gv", "fan_phi", "fan_dir", "fan_value", "fan_width", "fan_kp",
                                          "fan_ki", "fan_dpmax", "fan_isvel", "fan_isthrust", "heat", "paint_c",
-                                         "paint_u", "paint_v", "paint_wu", "paint_wv") if n in arr}
-    return Placed2D(nfan=pm["nfan"], pid=pm["pid"], u_floor=pm["u_floor"], heat_max=pm.get("heat_max"), **kw)
+                                         "paint_u", "paint_v", "paint_wu", "paint_wv", "xchi_u", "xa_u", "xchi_v",
+                                         "xa_v", "src", "src_neg", "pt_chi", "pt_a") if n in arr}
+    return Placed2D(nfan=pm["nfan"], pid=pm["pid"], u_floor=pm["u_floor"], heat_max=pm.get("heat_max"),
+                    ports=bool(pm.get("ports")), q_net=pm.get("q_net", 0.0), **kw)
 
 
 def load_masks():

@@ -31,8 +31,8 @@ sys.path.insert(0, str(REF / "src"))
 
 from aerolume.solvers.ns2d import core  # noqa: E402
 from aerolume.solvers.ns2d import physics as phx  # noqa: E402
-from aerolume.solvers.ns2d.config import (FanSpec, HeatSourceSpec, ImmersedBody, SolverConfig,  # noqa: E402
-                                          ThermalConfig, WallBC)
+from aerolume.solvers.ns2d.config import (FanSpec, HeatSourceSpec, ImmersedBody, PortSpec,  # noqa: E402
+                                          SolverConfig, ThermalConfig, WallBC)
 from aerolume.solvers.ns2d.geometry import build_geometry  # noqa: E402
 from aerolume.solvers.ns2d.poisson import PoissonSolver  # noqa: E402
 
@@ -83,7 +83,16 @@ def extract(ops, geom):
     if ph is not None:
         # the placed physics besides heat transfer: fans, heaters, paint, the PID step
         meta["placed"] = {"nfan": ph.nfan, "pid": bool(ph.pid), "paint": bool(ph.paint), "ctrl_size": ph.ctrl_size,
-                          "u_floor": float(ph.u_floor), "heat": ph.heat is not None}
+                          "u_floor": float(ph.u_floor), "heat": ph.heat is not None, "ports": bool(ph.ports)}
+        if ph.ports:
+            meta["placed"]["q_net"] = float(ph.q_net)
+            for name in ("src", "src_neg", "pchi_u", "pa_u", "pchi_v", "pa_v"):
+                arrays[name] = _np(getattr(ph, name))
+            if ph.pt_chi is not None:
+                arrays["pt_chi"], arrays["pt_a"] = _np(ph.pt_chi), _np(ph.pt_a)
+        if ph.ports or ph.paint:
+            for name in ("xchi_u", "xa_u", "xchi_v", "xa_v"):
+                arrays[name] = _np(getattr(ph, name))
         if ph.nfan:
             for name in ("fan_gu", "fan_gv", "fan_phi", "fan_dir", "fan_value", "fan_width", "fan_kp", "fan_ki",
                          "fan_dpmax", "fan_isvel", "fan_isthrust"):
@@ -265,6 +274,17 @@ def main():
         return torch.maximum((x - 3.2).abs() - 0.25, (y - 0.8).abs() - 0.3)
     run_case("cavity_heater_paint_f64", heater_case, dtype="float64", amp=0.1, seed=9, steps=3, paint=block)
     run_case("cavity_heater_paint_f32", heater_case, dtype="float32", amp=0.1, seed=9, steps=3, paint=block)
+    # jets and vents: a warm jet and a vent in the heated tunnel (the outlet balance takes the
+    # net port flow); an unbalanced jet in a closed heated box with a painted block (the uniform
+    # sink, the combined port / paint penalisation, the paint's force share)
+    ports = [PortSpec((0.8, 3.2), direction=(1.0, -0.3), size=0.3, speed=1.5, kind="jet", theta=1.0, name="jet"),
+             PortSpec((5.0, 0.7), direction=(0.0, -1.0), size=0.4, speed=0.6, kind="vent", name="vent")]
+    port_case = dict(tunnel, bodies=[hot], ports=ports, dye=True, thermal=ThermalConfig(prandtl=0.71, richardson=0.3))
+    run_case("tunnel_ports_heat_f64", port_case, dtype="float64", amp=0.05, seed=10, steps=3)
+    run_case("tunnel_ports_heat_f32", port_case, dtype="float32", amp=0.05, seed=10, steps=3)
+    box_jet = dict(cavity, bodies=[ins], ports=[PortSpec((0.4, 0.5), direction=(1.0, 0.2), size=0.25, speed=1.0,
+                                                         kind="jet", theta=0.8, name="jet")], dye=True)
+    run_case("closed_jet_paint_f64", box_jet, dtype="float64", amp=0.1, seed=11, steps=3, paint=block)
     if not names or "poisson" in names:
         poisson_cases()
 

@@ -82,7 +82,8 @@ def test_step2d_matches_reference(name):
         _check_report(out, arr, meta)
     # fans, paint and the controllers (core.py:998-1002, State.ctrl)
     for key, ref_key in (("fan_thrust", "out1_rep_fan_thrust"), ("fan_ud", "out1_rep_fan_ud"),
-                         ("paint_force", "out1_rep_paint_force"), ("ctrl", "out1_ctrl")):
+                         ("paint_force", "out1_rep_paint_force"), ("ctrl", "out1_ctrl"),
+                         ("vent_heat", "out1_rep_vent_heat"), ("jet_heat", "out1_rep_jet_heat")):
         if ref_key in arr:
             ref = np.asarray(arr[ref_key], np.float64)
             got = out[key].double().cpu().numpy()
@@ -90,7 +91,8 @@ def test_step2d_matches_reference(name):
     assert plan.status() == 0 if hasattr(plan, "status") else True
 
 
-@pytest.mark.parametrize("name", [c for c in CASES_2D if c.startswith(("cylinder", "tunnel_fans", "cavity_heater"))
+@pytest.mark.parametrize("name", [c for c in CASES_2D if c.startswith(("cylinder", "tunnel_fans", "cavity_heater",
+                                                                        "tunnel_ports", "closed_jet"))
                                   or "heated" in c or "cold" in c])
 def test_three_steps_in_place_match_reference(name):
     meta, plan, ins, arr = _setup(name)

@@ -66,7 +66,8 @@ def test_oracle2d_one_step_matches_reference(name):
         assert np.abs(np.asarray(r.ctrl, np.float64) - arr["out1_ctrl"]).max() < 10 * tol, (r.ctrl, arr["out1_ctrl"])
 
 
-@pytest.mark.parametrize("name", [c for c in CASES_2D if c.startswith(("cylinder", "tunnel_fans", "cavity_heater"))])
+@pytest.mark.parametrize("name", [c for c in CASES_2D if c.startswith(("cylinder", "tunnel_fans", "cavity_heater",
+                                                                        "tunnel_ports", "closed_jet"))])
 def test_oracle2d_three_steps_match_reference(name):
     meta, arr, outs = _run(name, steps=3)
     tol = 10 * TOL[meta["dtype"]]

@@ -32,10 +32,10 @@ def test_step_full_refuses_diagnostics_and_placed_physics():
         step_full(st._replace(theta=1), None, None)
 
 
-def test_thermal_from_physics_takes_heat_and_refuses_ports_and_smoke_groups():
-    """The 2D plan reads heat transfer off the reference's Physics (fans, heaters, paint and
-    the PID step are read by the plan itself), returns None without heat transfer, and refuses
-    jets / vents and smoke channels with emitters."""
+def test_thermal_from_physics_takes_heat_and_refuses_smoke_groups():
+    """The 2D plan reads heat transfer off the reference's Physics (fans, heaters, paint, jets
+    and vents and the PID step are read by the plan itself), returns None without heat
+    transfer, and refuses smoke channels with emitters."""
     from aerolume_b200.ns2d.plan import thermal_from_physics
     from aerolume_b200.ns2d.types import Geometry2D
     geom = Geometry2D((2, 6, 3, 9), nbody=1)
@@ -53,7 +53,8 @@ def test_thermal_from_physics_takes_heat_and_refuses_ports_and_smoke_groups():
     for name, val in (("nfan", 1), ("pid", True), ("paint", True), ("heat", torch.ones(2))):
         assert thermal_from_physics(types.SimpleNamespace(**{**vars(ph), name: val}), geom) is not None
     assert thermal_from_physics(types.SimpleNamespace(**{**vars(ph), "thermal": False}), geom) is None
-    for name, val in (("ports", [1]), ("n_dye", 2), ("comb", True)):
+    assert thermal_from_physics(types.SimpleNamespace(**{**vars(ph), "ports": True}), geom) is not None
+    for name, val in (("n_dye", 2), ("comb", True)):
         with pytest.raises(RuntimeError):
             thermal_from_physics(types.SimpleNamespace(**{**vars(ph), name: val}), geom)
 
@@ -182,7 +183,8 @@ def test_fast_step_phys_runs_the_placed_physics(name):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["tunnel_fans_pid_f64", "cavity_heater_paint_f64"])
+@pytest.mark.parametrize("name", ["tunnel_fans_pid_f64", "cavity_heater_paint_f64", "tunnel_ports_heat_f64",
+                                  "closed_jet_paint_f64"])
 def test_step_full_fans_heaters_paint_pid_match_reference(name):
     """step_full with ops.phys carrying fans and the PID step, or heaters and a paint layer (the
     reference's 2D Physics attribute names): three steps chained through State.ctrl and
@@ -194,8 +196,8 @@ def test_step_full_fans_heaters_paint_pid_match_reference(name):
     dt = torch.float64
     th = thermal2d_from_case(meta, arr)
     pl = placed2d_from_case(meta, arr)
-    ph = types.SimpleNamespace(**{k: getattr(pl, k) for k in vars(pl)}, ports=[], n_dye=0, comb=False,
-                               paint=pl.paint, thermal=th is not None)
+    ph = types.SimpleNamespace(**{k: getattr(pl, k) for k in vars(pl)}, n_dye=0, comb=False, paint=pl.paint,
+                               thermal=th is not None)
     if th is not None:
         for k in ("kappa", "ri", "prt", "gravity", "eta_t", "theta_in", "wall_modes", "wall_values", "diff_coef"):
             setattr(ph, k, getattr(th, k))
@@ -208,7 +210,7 @@ def test_step_full_fans_heaters_paint_pid_match_reference(name):
                _dev(arr["in_ctrl"], dt) if "in_ctrl" in arr else None)
     out = {}
     new, _ = step_full(st, geom, ops, None, out=out)
-    for key in ("fan_thrust", "fan_ud", "paint_force"):
+    for key in ("fan_thrust", "fan_ud", "paint_force", "vent_heat", "jet_heat"):
         if f"out1_rep_{key}" in arr:
             ref = arr[f"out1_rep_{key}"]
             assert np.abs(out[key].cpu().numpy() - ref).max() <= 1e-9 * max(1.0, np.abs(ref).max()), key
