@@ -136,7 +136,8 @@ class Ns2dConfig(C.Structure):
         ("wall_mode", C.c_int32 * 4), ("wall_value", C.c_double * 4), ("diff_coef", C.c_double),
         ("n_temp", C.c_int32), ("n_flux", C.c_int32), ("has_ins", C.c_int32), ("has_vol", C.c_int32),
         ("nfan", C.c_int32), ("heaters", C.c_int32), ("paint", C.c_int32), ("pid", C.c_int32),
-        ("ports", C.c_int32),
+        ("ports", C.c_int32), ("dye_channels", C.c_int32), ("n_groups", C.c_int32),
+        ("group_channel", C.c_int32 * 8),
     ]
 
 
@@ -147,14 +148,17 @@ class Ns2dGeom(C.Structure):
                                           "fan_phi", "fan_dir", "fan_value", "fan_width", "fan_kp", "fan_ki",
                                           "fan_dpmax", "fan_isvel", "fan_isthrust", "u_floor", "heat", "heat_max",
                                           "paint_c", "paint_u", "paint_v", "paint_wu", "paint_wv", "xchi_u", "xa_u",
-                                          "xchi_v", "xa_v", "src", "src_neg", "q_net", "pt_chi", "pt_a")]
+                                          "xchi_v", "xa_v", "src", "src_neg", "q_net", "pt_chi", "pt_a",
+                                          "dye_inflow")] + [
+        ("group_w", C.c_void_p * 8), ("group_target", C.c_void_p * 8), ("group_timing", C.c_void_p * 8),
+        ("port_dye", C.c_void_p * 4)]
 
 
 class Ns2dFields(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in ("u0", "v0", "t0", "dye0", "u", "v", "p", "t", "dt", "dye", "coeffs",
                                           "theta0", "theta", "heat", "theta_wall", "wall_heat", "heat_storage",
                                           "flow_heat", "dt_prev", "ctrl0", "ctrl", "fan_thrust", "fan_ud",
-                                          "paint_force", "jet_heat", "vent_heat")]
+                                          "paint_force", "jet_heat", "vent_heat", "dye_extra0", "dye_extra")]
 
 
 class SmokeEmitter(C.Structure):

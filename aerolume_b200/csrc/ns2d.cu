@@ -678,6 +678,101 @@ __global__ void dye2d_kernel(const __grid_constant__ DyeParams<T> P) {
 }
 
 // ---------------------------------------------------------------------------------------
+// smoke channels with emitter groups and smoking jets (physics.py:795-830): every channel one
+// forward-Euler step of the bounded (MUSCL / van Leer) advection with the end-of-step velocity
+// (scalar.py:42-88: the channel's inlet value left of a tunnel), the vents' sink, the emitter
+// groups relaxing their footprint to their concentration while on, the jets relaxing theirs to
+// 1, solids and paint cleared, the floor and the cap
+// ---------------------------------------------------------------------------------------
+
+constexpr int MAX_DYE_CH = AERO_MAX_DYE_CHANNELS, MAX_DYE_GRP = AERO_MAX_DYE_GROUPS;
+
+template <typename T>
+struct DyeChannelsParams {
+  int nx, ny, periodic, closed, nch, ngroup;
+  T inv_h;
+  const T *c0[MAX_DYE_CH];
+  T *c[MAX_DYE_CH];
+  const T *u, *v, *dt, *t0;          // the emitters' clock is the new time t0 + dt
+  const T *inflow;                   // (nch, ny) inlet values, or NULL (zeros)
+  const T *src_neg;                  // vents' sinks (ny, nx), or NULL
+  int gch[MAX_DYE_GRP];
+  const T *gw[MAX_DYE_GRP], *gtarget[MAX_DYE_GRP], *gtiming[MAX_DYE_GRP];
+  const T *port_w[MAX_DYE_CH];
+  int has_win, win[4];
+  const T *chi_c, *paint_c;
+};
+
+// 1 while an emitter group releases at time t (physics.py:795-802; the remainder with the
+// divisor's sign)
+template <typename T>
+__device__ __forceinline__ T emitter_on(T t, const T *timing) {
+  const T start = timing[0], stop = timing[1], period = timing[2], duty = timing[3];
+  const bool active = t >= start && t < stop;
+  const T safe = period > T(0) ? period : T(1);
+  T r = fmod(t - start, safe);
+  if (r != T(0) && ((safe < T(0)) != (r < T(0)))) r = r + safe;
+  const T phase = r / safe;
+  return (active && (period <= T(0) || phase < duty)) ? T(1) : T(0);
+}
+
+template <typename T>
+__global__ void dye_channels2d_kernel(const __grid_constant__ DyeChannelsParams<T> P) {
+  aero::pdl_wait();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+  const int nx = P.nx, ny = P.ny;
+  if (i >= nx || j >= ny) return;
+  const size_t g = (size_t)j * nx + i;
+  const T dt = *P.dt;
+  T out[MAX_DYE_CH];
+  for (int ch = 0; ch < P.nch; ++ch) {
+    const T *c0 = P.c0[ch];
+    auto at = [&](int jj, int ii) -> T {
+      if (P.periodic) {
+        ii = ii < 0 ? ii + nx : (ii >= nx ? ii - nx : ii);
+        jj = jj < 0 ? jj + ny : (jj >= ny ? jj - ny : jj);
+      } else {
+        jj = jj < 0 ? 0 : (jj >= ny ? ny - 1 : jj);
+        if (ii < 0) {
+          if (!P.closed) return P.inflow ? P.inflow[(size_t)ch * ny + jj] : T(0);
+          ii = 0;
+        }
+        if (ii >= nx) ii = nx - 1;
+      }
+      return __ldg(c0 + (size_t)jj * nx + ii);
+    };
+    const T c = at(j, i);
+    const T fx0 = muscl_flux<T>(at(j, i - 2), at(j, i - 1), c, at(j, i + 1), P.u[(size_t)j * (nx + 1) + i]);
+    const T fx1 = muscl_flux<T>(at(j, i - 1), c, at(j, i + 1), at(j, i + 2), P.u[(size_t)j * (nx + 1) + i + 1]);
+    const T fy0 = muscl_flux<T>(at(j - 2, i), at(j - 1, i), c, at(j + 1, i), P.v[g]);
+    const T fy1 = muscl_flux<T>(at(j - 1, i), c, at(j + 1, i), at(j + 2, i), P.v[(size_t)(j + 1) * nx + i]);
+    T cn = c + dt * ((((fx0 - fx1) + fy0) - fy1) * P.inv_h);
+    if (P.src_neg) cn = cn + (dt * P.src_neg[g]) * cn;
+    out[ch] = cn;
+  }
+  if (P.ngroup) {
+    const T t = *P.t0 + dt;
+    for (int q = 0; q < P.ngroup; ++q) {
+      const int ch = P.gch[q];
+      const T w = P.gw[q][g] * emitter_on<T>(t, P.gtiming[q]);
+      out[ch] = out[ch] + w * (P.gtarget[q][g] - out[ch]);
+    }
+  }
+  for (int ch = 0; ch < P.nch; ++ch)
+    if (P.port_w[ch]) out[ch] = out[ch] + P.port_w[ch][g] * (T(1) - out[ch]);
+  bool keep = true;
+  if (P.has_win && j >= P.win[0] && j < P.win[1] && i >= P.win[2] && i < P.win[3])
+    keep = P.chi_c[(size_t)(j - P.win[0]) * (P.win[3] - P.win[2]) + (i - P.win[2])] <= T(0.5);
+  const bool paint_keep = !P.paint_c || P.paint_c[g] <= T(0.5);
+  for (int ch = 0; ch < P.nch; ++ch) {
+    T x = out[ch] * (keep ? T(1) : T(0));
+    x = x * (paint_keep ? T(1) : T(0));
+    x = x > T(1e-6) ? x : T(0);
+    P.c[ch][g] = x < T(1) ? x : T(1);
+  }
+}
+
+// ---------------------------------------------------------------------------------------
 // placed physics before the first stage: the step (with the fans' and heaters' bounds and the
 // PID controller) and the fans' PI controllers (core.py:856-878, physics.py:640-672, 851-884,
 // diagnostics.py:104-124), one block
@@ -1688,7 +1783,9 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
   S.eta = T(c.eta);
   S.nbody = has_win ? c.nbody : 0;
   const dim3 grid(p->gx, p->gy), block(TX, TY);
-  const bool placed = c.nfan || c.pid || c.paint || c.heaters || c.ports;
+  const bool placed = c.nfan || c.pid || c.paint || c.heaters || c.ports || c.dye_channels;
+  if (c.dye_channels > 0 && c.dye && c.dye_channels > 1 && !(f->dye_extra0 && f->dye_extra))
+    return set_error(AERO_EINVAL, "smoke channels 1.. need dye_extra0 / dye_extra");
   if (rec && (!std::is_same<T, float>::value || les || thermal || c.dye || dt_mode != 0 || placed))
     return set_error(AERO_EUNSUPPORTED, "the persistent sweep runs FP32 plans without LES, heat transfer, dye or "
                                         "placed physics, with the CFL time step");
@@ -2015,7 +2112,39 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
     AERO_CUDA_TRY(cudaGetLastError());
   }
   // ---- dye with the step's final velocity
-  if (c.dye) {
+  if (c.dye && c.dye_channels > 0) {   // smoke channels with emitter groups and smoking jets
+    DyeChannelsParams<T> D{};
+    D.nx = nx;
+    D.ny = ny;
+    D.periodic = c.periodic;
+    D.closed = c.closed;
+    D.nch = c.dye_channels;
+    D.ngroup = c.n_groups;
+    D.inv_h = T(1.0 / c.h);
+    for (int ch = 0; ch < c.dye_channels; ++ch) {
+      D.c0[ch] = ch == 0 ? static_cast<const T *>(f->dye0) : static_cast<const T *>(f->dye_extra0) + (size_t)(ch - 1) * p->nc;
+      D.c[ch] = ch == 0 ? static_cast<T *>(f->dye) : static_cast<T *>(f->dye_extra) + (size_t)(ch - 1) * p->nc;
+      D.port_w[ch] = static_cast<const T *>(g->port_dye[ch]);
+    }
+    D.u = static_cast<const T *>(f->u);
+    D.v = static_cast<const T *>(f->v);
+    D.dt = small;
+    D.t0 = static_cast<const T *>(f->t0);
+    D.inflow = static_cast<const T *>(g->dye_inflow);
+    D.src_neg = c.ports ? static_cast<const T *>(g->src_neg) : nullptr;
+    for (int q = 0; q < c.n_groups; ++q) {
+      D.gch[q] = c.group_channel[q];
+      D.gw[q] = static_cast<const T *>(g->group_w[q]);
+      D.gtarget[q] = static_cast<const T *>(g->group_target[q]);
+      D.gtiming[q] = static_cast<const T *>(g->group_timing[q]);
+    }
+    D.has_win = has_win;
+    for (int q = 0; q < 4; ++q) D.win[q] = c.window[q];
+    D.chi_c = static_cast<const T *>(g->chi_c);
+    D.paint_c = c.paint ? static_cast<const T *>(g->paint_c) : nullptr;
+    (void)aero::launch_k(dye_channels2d_kernel<T>, dim3((nx + 127) / 128, ny), 128, 0, s, D);
+    AERO_CUDA_TRY(cudaGetLastError());
+  } else if (c.dye) {
     DyeParams<T> D{};
     D.nx = nx;
     D.ny = ny;
@@ -2097,6 +2226,12 @@ int aero_ns2d_plan_create(const AeroNs2dConfig *cfg, AeroNs2dPlan **plan) {
   if (c.nfan < 0 || c.nfan > AERO_MAX_FANS)
     return set_error(AERO_EUNSUPPORTED, "at most " + std::to_string(AERO_MAX_FANS) + " fans");
   if (c.heaters && !c.thermal) return set_error(AERO_EINVAL, "heaters need heat transfer");
+  if (c.dye_channels < 0 || c.dye_channels > AERO_MAX_DYE_CHANNELS || c.n_groups < 0 ||
+      c.n_groups > AERO_MAX_DYE_GROUPS || (c.dye_channels > 0 && !c.dye))
+    return set_error(AERO_EINVAL, "smoke channels: 1..4 with dye on, at most 8 emitter groups");
+  for (int q = 0; q < c.n_groups; ++q)
+    if (c.group_channel[q] < 0 || c.group_channel[q] >= c.dye_channels)
+      return set_error(AERO_EINVAL, "an emitter group's channel is out of range");
   auto *p = new AeroNs2dPlan();
   p->cfg = c;
   const size_t e = c.dtype == AERO_F64 ? 8 : 4;

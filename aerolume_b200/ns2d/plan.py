@@ -6,8 +6,8 @@ src/aerolume/solvers/ns2d/core.py:67-108 and geometry.py:160-182, or the contain
 core.py:271-325, uploads the window masks once and owns the device workspace.  Heat
 transfer comes from ``thermal=`` (a :class:`~aerolume_b200.ns2d.types.Thermal2D`) or from the
 reference's ``ops.phys`` with ``geom.thermal``; fans, heaters, painted obstacles, jets and
-vents and the PID step come from ``placed=`` (a :class:`~aerolume_b200.ns2d.types.Placed2D`)
-or from ``ops.phys`` itself.  Smoke channels with emitters (or port smoke), the wall model and
+vents, smoke channels with emitters and smoking jets and the PID step come from ``placed=`` (a
+:class:`~aerolume_b200.ns2d.types.Placed2D`) or from ``ops.phys`` itself.  The wall model and
 body forcing raise ``RuntimeError``: there is no fallback to a CPU or plain-torch path.
 """
 from __future__ import annotations
@@ -64,12 +64,7 @@ def ghost_rules(ops):
 
 def thermal_from_physics(ph, geom):
     """The heat transfer of the reference's 2D ``Physics`` (physics.py:291-345) and
-    ``geom.thermal`` (None when it has none); raises when the physics places anything the B200
-    step does not run (smoke channels with emitters or port smoke)."""
-    others = [n for n, on in (("smoke groups", int(getattr(ph, "n_dye", 0) or 0) > 0 or bool(getattr(ph, "comb", False))),)
-              if on]
-    if others:
-        raise RuntimeError("placed physics (" + ", ".join(others) + ") is not in the B200 2D step")
+    ``geom.thermal`` (None when it has none)."""
     if not getattr(ph, "thermal", False):
         return None
     tg = getattr(geom, "thermal", None)
@@ -177,6 +172,7 @@ class Ns2dPlan:
         self.placed = placed
         self.nfan = 0
         self.pid = False
+        self.dye_channels = 0
         if placed is not None:
             self._placed_config(cfg, g, placed, thermal is not None, up)
 
@@ -287,6 +283,29 @@ class Ns2dPlan:
             if thermal and getattr(pl, "pt_chi", None) is not None:
                 g.pt_chi = arr(pl.pt_chi, (ny, nx))
                 g.pt_a = arr(pl.pt_a, (ny, nx))
+        n_dye = int(getattr(pl, "n_dye", 0) or 0)
+        self.dye_channels = n_dye
+        if n_dye:   # smoke channels with emitter groups and smoking jets (physics.py:497-540)
+            if n_dye > 4:
+                raise RuntimeError("the B200 2D step carries at most 4 smoke channels")
+            if not self.dye:
+                raise RuntimeError("smoke channels need the plan's dye")
+            cfg.dye_channels = n_dye
+            if getattr(pl, "dye_inflow", None) is not None:
+                g.dye_inflow = arr(pl.dye_inflow, (n_dye, ny))
+            groups = list(getattr(pl, "groups", None) or [])
+            if len(groups) > 8:
+                raise RuntimeError("the B200 2D step takes at most 8 emitter groups")
+            cfg.n_groups = len(groups)
+            for q, grp in enumerate(groups):
+                ch, w, target, timing = grp if isinstance(grp, tuple) else (grp.channel, grp.weight, grp.target,
+                                                                            grp.timing)
+                cfg.group_channel[q] = int(ch)
+                g.group_w[q] = arr(w, (ny, nx))
+                g.group_target[q] = arr(target, (ny, nx))
+                g.group_timing[q] = arr(timing, (4,))
+            for ch, w in (getattr(pl, "port_dye", None) or {}).items():
+                g.port_dye[int(ch)] = arr(w, (ny, nx))
 
     @property
     def ctrl_size(self):
@@ -314,6 +333,8 @@ class Ns2dPlan:
                "coeffs": torch.zeros(max(self.nbody, 1), 3, **kw)[: self.nbody]}
         if self.dye:
             out["dye"] = torch.empty(ny, nx, **kw)
+            if self.dye_channels > 1:
+                out["dye_extra"] = torch.empty(self.dye_channels - 1, ny, nx, **kw)
         if self.thermal is not None:
             d64 = dict(device=self.device, dtype=torch.float64)
             out.update(theta=torch.empty(ny, nx, **kw), heat=torch.zeros(self.n_temp, **d64),
@@ -339,7 +360,8 @@ class Ns2dPlan:
         if tuple(t.shape) != tuple(shape):
             raise RuntimeError(f"{name} has shape {tuple(t.shape)}, expected {tuple(shape)}")
 
-    def step(self, u0, v0, t0, *, dye0=None, theta0=None, out=None, dt=None, ctrl0=None, dt_prev=None):
+    def step(self, u0, v0, t0, *, dye0=None, theta0=None, out=None, dt=None, ctrl0=None, dt_prev=None,
+             dye_extra0=None):
         """One step (plus the dye update when the plan has dye, theta and the heat report
         (float64: heat, theta_wall, wall_heat, heat_storage, flow_heat) with heat transfer);
         returns the output dict.  ``out`` may hold u0 / v0 / theta0 themselves (in-place
@@ -363,6 +385,11 @@ class Ns2dPlan:
                 raise RuntimeError("this plan has dye: dye0 is required")
             self._check("dye0", dye0, (ny, nx))
             f.dye0, f.dye = dye0.data_ptr(), out["dye"].data_ptr()
+            if self.dye_channels > 1:   # smoke channels 1.. (State.dye_extra)
+                if dye_extra0 is None:
+                    raise RuntimeError("this plan has several smoke channels: dye_extra0 is required")
+                self._check("dye_extra0", dye_extra0, (self.dye_channels - 1, ny, nx))
+                f.dye_extra0, f.dye_extra = dye_extra0.data_ptr(), out["dye_extra"].data_ptr()
         if self.thermal is not None:
             if theta0 is None:
                 raise RuntimeError("this plan has heat transfer: theta0 is required")

@@ -6,11 +6,11 @@ served by the B200 step.
 ``aerolume.solvers.ns2d.solver.step_full`` to this function swaps the step.  It returns
 ``(State, coeffs (nbody, 3))`` of new tensors like the reference.  With heat transfer theta
 advances too and ``out`` receives the heat report of core.py:974-995; fans, heaters, painted
-obstacles, jets and vents and the PID step of ``ops.phys`` run in the step, ``state.ctrl``
-carries the controllers' memory and ``out`` receives ``fan_thrust``, ``fan_ud``,
-``paint_force``, ``vent_heat`` and ``jet_heat`` as core.py:987-1002 fills them.  Smoke channels
-with emitters or port smoke, the wall model, diagnostics rows and traces raise instead of
-being computed differently.
+obstacles, jets and vents, smoke channels with emitters and the PID step of ``ops.phys`` run in
+the step, ``state.ctrl`` carries the controllers' memory, ``state.dye_extra`` the smoke
+channels after the first, and ``out`` receives ``fan_thrust``, ``fan_ud``, ``paint_force``,
+``vent_heat`` and ``jet_heat`` as core.py:987-1002 fills them.  The wall model, diagnostics rows
+and traces raise instead of being computed differently.
 """
 from __future__ import annotations
 
@@ -23,7 +23,7 @@ from .plan import Ns2dPlan
 
 
 class State(NamedTuple):
-    """The reference's 2D state (core.py:111-130); dye_extra stays None."""
+    """The reference's 2D state (core.py:111-130)."""
     u: Any
     v: Any
     p: Any
@@ -69,8 +69,6 @@ def step_full(state, geom, ops, dt=None, *, out=None, diag=False, trace=None):
     """One SSP-RK3 step (plus the dye update when the state carries dye)."""
     if diag or trace is not None:
         raise RuntimeError("diagnostics rows and stage traces are not produced by the B200 step")
-    if getattr(state, "dye_extra", None) is not None:
-        raise RuntimeError("placed-physics state 'dye_extra' is not in the B200 2D step")
     theta = getattr(state, "theta", None)
     if theta is not None and getattr(ops, "phys", None) is None:
         raise RuntimeError("state.theta without heat transfer in ops.phys")
@@ -82,10 +80,13 @@ def step_full(state, geom, ops, dt=None, *, out=None, diag=False, trace=None):
         raise RuntimeError("state.ctrl must be given exactly when ops.phys has fans or the PID step")
     if dt is not None and not torch.is_tensor(dt):
         dt = torch.tensor(float(dt), device=state.u.device, dtype=state.u.dtype)
+    extra = getattr(state, "dye_extra", None)
+    if (extra is not None) != (plan.dye_channels > 1):
+        raise RuntimeError("state.dye_extra must be given exactly when ops.phys has several smoke channels")
     res = plan.step(state.u, state.v, state.t, dye0=state.dye, theta0=theta, dt=dt, ctrl0=ctrl,
-                    dt_prev=state.dt if ctrl is not None else None)
-    new = State(res["u"], res["v"], res["p"], res.get("dye"), res["t"], res["dt"], res.get("theta"), None,
-                res.get("ctrl"))
+                    dt_prev=state.dt if ctrl is not None else None, dye_extra0=extra)
+    new = State(res["u"], res["v"], res["p"], res.get("dye"), res["t"], res["dt"], res.get("theta"),
+                res.get("dye_extra"), res.get("ctrl"))
     if out is not None and plan.thermal is not None:
         keys = (["heat"] if plan.n_temp else []) + (["theta_wall"] if plan.n_flux else []) + [
             "wall_heat", "heat_storage", "flow_heat"]

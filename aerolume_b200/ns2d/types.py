@@ -133,3 +133,7 @@ class Placed2D:
     q_net: Any = 0.0
     pt_chi: Any = None
     pt_a: Any = None
+    n_dye: int = 0               # smoke channels (0: the single comb channel of the plain step)
+    dye_inflow: Any = None       # (n_dye, ny) the channels' inlet values
+    groups: Any = None           # emitter groups: (channel, weight, target, timing) or DyeGroup
+    port_dye: Any = None         # {channel: (ny, nx) smoking jets' weight}

@@ -495,7 +495,15 @@ typedef struct {
    * AeroNs2dGeom, the controller memory in AeroNs2dFields */
   int32_t nfan, heaters, paint, pid;
   int32_t ports;                /* jets and vents (physics.py:362-433)                      */
+  /* smoke channels with emitter groups and smoking jets (physics.py:497-540, 805-830; 0: the
+   * single comb channel of `dye`): channels (<= AERO_MAX_DYE_CHANNELS; channel 0 is dye, the
+   * others dye_extra), emitter groups (<= AERO_MAX_DYE_GROUPS) and the channel of each */
+  int32_t dye_channels, n_groups;
+  int32_t group_channel[8];
 } AeroNs2dConfig;
+
+#define AERO_MAX_DYE_CHANNELS 4
+#define AERO_MAX_DYE_GROUPS 8
 
 /* temperature boundary modes of a 2D side (ns2d/scalar.py:96-146) */
 enum { AERO_TH2_ADIABATIC = 0, AERO_TH2_TEMPERATURE = 1, AERO_TH2_HEAT_FLUX = 2, AERO_TH2_INLET = 3,
@@ -532,6 +540,12 @@ typedef struct {
    * vents' sinks src_neg (ny, nx), their net volume flow q_net (0-d), the jets' temperature
    * penalisation pt_chi, pt_a (ny, nx; NULL without heat transfer or jets) */
   const void *xchi_u, *xa_u, *xchi_v, *xa_v, *src, *src_neg, *q_net, *pt_chi, *pt_a;
+  /* smoke channels: inlet values (dye_channels, ny) (NULL: zeros); per emitter group its
+   * weight and target (ny, nx) and timing [start, stop, period, duty]; per channel the smoking
+   * jets' weight (ny, nx) or NULL */
+  const void *dye_inflow;
+  const void *group_w[8], *group_target[8], *group_timing[8];
+  const void *port_dye[4];
 } AeroNs2dGeom;
 
 /* Step inputs (u0, v0, t0, dye0) and outputs; u / v may alias u0 / v0. */
@@ -554,6 +568,10 @@ typedef struct {
   /* jets and vents with heat transfer (double, 1 each): the heat the jets add and the heat
    * leaving with the vents' fluid (core.py:990-993) */
   void *jet_heat, *vent_heat;
+  /* smoke channels 1 .. dye_channels - 1 in and out ((dye_channels - 1, ny, nx); channel 0 is
+   * dye0 / dye) */
+  const void *dye_extra0;
+  void *dye_extra;
 } AeroNs2dFields;
 
 int aero_ns2d_plan_create(const AeroNs2dConfig *cfg, AeroNs2dPlan **plan);

@@ -776,6 +776,13 @@ class Placed2D:
     q_net: float = 0.0
     pt_chi: np.ndarray | None = None
     pt_a: np.ndarray | None = None
+    # smoke channels (physics.py:497-540, 795-830): the channels' inlet values (n, ny), the
+    # emitter groups [(channel, weight, target, timing)] in the reference's sorted order and the
+    # smoking jets' weights {channel: (ny, nx)}
+    n_dye: int = 0
+    dye_inflow: np.ndarray | None = None
+    groups: list = None
+    port_dye: dict = None
 
     @property
     def paint(self):
@@ -881,8 +888,70 @@ def theta_rhs2d_placed(th, u, v, nut, geom, tp, pl, ops):
     return lt
 
 
+def emitter_on2d(t, timing):
+    """physics.py:795-802: 1 while an emitter group releases at time t."""
+    T = type(t)
+    start, stop, period, duty = (T(x) for x in timing)
+    active = (t >= start) and (t < stop)
+    safe = period if period > 0 else T(1.0)
+    r = np.fmod(T(t - start), safe)
+    if r != 0 and ((safe < 0) != (r < 0)):
+        r = r + safe
+    phase = T(r / safe)
+    return T(1.0) if (active and (period <= 0 or phase < duty)) else T(0.0)
+
+
+def _dye_fluxes2d(c, u, v, ops, inflow):
+    """scalar.py:42-83 for one channel: the limited (van Leer) face values with the inlet
+    value left of a tunnel (inflow: (ny,)), replicated cells elsewhere, wrap when periodic."""
+    T = c.dtype.type
+    ny, nx = c.shape
+    if ops.periodic:
+        cx = np.concatenate([c[:, -2:], c, c[:, :2]], axis=1)
+        cy = np.concatenate([c[-2:], c, c[:2]], axis=0)
+    else:
+        right = np.repeat(c[:, -1:], 2, axis=1)
+        left = np.repeat(c[:, :1], 2, axis=1) if ops.closed else np.repeat(inflow.reshape(ny, 1), 2, axis=1)
+        cx = np.concatenate([left, c, right], axis=1)
+        cy = np.concatenate([np.repeat(c[:1], 2, axis=0), c, np.repeat(c[-1:], 2, axis=0)], axis=0)
+    s = _van_leer_scalar(cx[:, 1:-1] - cx[:, :-2], cx[:, 2:] - cx[:, 1:-1])
+    left_v = cx[:, 1:-2] + T(0.5) * s[:, :-1]
+    right_v = cx[:, 2:-1] - T(0.5) * s[:, 1:]
+    fx = u * np.where(u > 0, left_v, right_v)
+    s = _van_leer_scalar(cy[1:-1] - cy[:-2], cy[2:] - cy[1:-1])
+    low = cy[1:-2] + T(0.5) * s[:-1]
+    high = cy[2:-1] - T(0.5) * s[1:]
+    fy = v * np.where(v > 0, low, high)
+    return fx, fy
+
+
+def update_dye2d(chans, u, v, dt, t, geom, pl, ops):
+    """physics.py:805-830: every smoke channel one forward-Euler step with the end-of-step
+    velocity, the vents' sink, the emitter groups and smoking jets, solids and paint, the floor."""
+    T = u.dtype.type
+    out = []
+    for ch, c in enumerate(chans):
+        fx, fy = _dye_fluxes2d(c, u, v, ops, pl.dye_inflow[ch].astype(c.dtype))
+        c = c + T(dt) * flux_divergence(fx, fy, ops.h)
+        if pl.ports:
+            c = c + (T(dt) * pl.src_neg) * c
+        out.append(c)
+    for ch, w, target, timing in pl.groups or []:
+        on = emitter_on2d(T(t), timing)
+        out[ch] = out[ch] + (w * on) * (target - out[ch])
+    for ch, w in (pl.port_dye or {}).items():
+        out[ch] = out[ch] + w * (T(1.0) - out[ch])
+    res = []
+    for c in out:
+        c = zero_dye_in_solids(c, geom) if not geom.empty else c
+        if pl.paint:
+            c = c * (pl.paint_c <= 0.5).astype(c.dtype)
+        res.append(np.minimum(np.where(c > T(1e-6), c, T(0.0)), T(1.0)))
+    return res
+
+
 def step2d_placed(u0, v0, t, geom, ops, poisson, *, tp=None, pl=None, theta0=None, dye=None, dt_prev=0.0,
-                  ctrl=None, dt=None):
+                  ctrl=None, dt=None, dye_extra=None):
     """One SSP-RK3 step (core.py:815-969) with heat transfer (``tp``), fans, heaters, painted
     obstacles and the PID step (``pl``); ``ctrl`` is the controller memory (PID errors, then
     (integral, pressure jump) per fan) and ``dt_prev`` the previous step (0: first)."""
@@ -990,13 +1059,19 @@ def step2d_placed(u0, v0, t, geom, ops, poisson, *, tp=None, pl=None, theta0=Non
         psi_w = psi * T(w) if psi_w is None else psi_w + T(w) * psi
     p = psi_w * (T(1.0) / dt)
     coeffs = force_coefficients2d(acc_u, acc_v, geom, ops, dt)
-    new_dye = None
-    if dye is not None:
+    new_dye = new_extra = None
+    if dye is not None and pl is not None and pl.n_dye:
+        chans = [dye] + (list(dye_extra) if dye_extra is not None else [])
+        res_ch = update_dye2d(chans, up, vp, dt, T(t + dt), geom, pl, ops)
+        new_dye = res_ch[0]
+        new_extra = np.stack(res_ch[1:]) if len(res_ch) > 1 else None
+    elif dye is not None:
         new_dye = zero_dye_in_solids(advect_dye2d(dye, up, vp, dt, ops), geom)
         if paint:
             new_dye = new_dye * (pl.paint_c <= 0.5).astype(new_dye.dtype)
     res = StepResult2D(up, vp, p, np.asarray(t + dt, dtype=u0.dtype), np.asarray(dt, dtype=u0.dtype), coeffs,
                        new_dye)
+    res.dye_extra = new_extra
     res.theta = thp if thermal else None
     res.ctrl = ctrl
     res.report = heat_report2d(theta0, thp, up, heat_acc, geom, tp, ops, dt) if thermal else {}

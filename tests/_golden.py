@@ -135,15 +135,22 @@ def placed2d_from_case(meta, arr):
     """The oracle's Placed2D (fans, heaters, paint, the PID step) of a 2D golden case, or None."""
     from oracle.ns2d import Placed2D
     pm = meta.get("placed")
-    if pm is None or not (pm["nfan"] or pm["pid"] or pm["paint"] or pm["heat"] or pm.get("ports")):
+    if pm is None or not (pm["nfan"] or pm["pid"] or pm["paint"] or pm["heat"] or pm.get("ports") or pm.get("n_dye")):
         return None
     dt = np.float64 if meta["dtype"] == "float64" else np.float32
     kw = {n: arr[n].astype(dt) for n in ("fan_gu", "fan_gv", "fan_phi", "fan_dir", "fan_value", "fan_width", "fan_kp",
                                          "fan_ki", "fan_dpmax", "fan_isvel", "fan_isthrust", "heat", "paint_c",
                                          "paint_u", "paint_v", "paint_wu", "paint_wv", "xchi_u", "xa_u", "xchi_v",
                                          "xa_v", "src", "src_neg", "pt_chi", "pt_a") if n in arr}
-    return Placed2D(nfan=pm["nfan"], pid=pm["pid"], u_floor=pm["u_floor"], heat_max=pm.get("heat_max"),
-                    ports=bool(pm.get("ports")), q_net=pm.get("q_net", 0.0), **kw)
+    pl = Placed2D(nfan=pm["nfan"], pid=pm["pid"], u_floor=pm["u_floor"], heat_max=pm.get("heat_max"),
+                  ports=bool(pm.get("ports")), q_net=pm.get("q_net", 0.0), **kw)
+    if pm.get("n_dye"):
+        pl.n_dye = pm["n_dye"]
+        pl.dye_inflow = arr["dye_inflow"].astype(dt)
+        pl.groups = [(ch, arr[f"group{q}_w"].astype(dt), arr[f"group{q}_target"].astype(dt),
+                      arr[f"group{q}_timing"].astype(dt)) for q, ch in enumerate(pm["groups"])]
+        pl.port_dye = {c: arr[f"port_dye{c}"].astype(dt) for c in pm["port_dye"]}
+    return pl
 
 
 def load_masks():

@@ -31,8 +31,8 @@ sys.path.insert(0, str(REF / "src"))
 
 from aerolume.solvers.ns2d import core  # noqa: E402
 from aerolume.solvers.ns2d import physics as phx  # noqa: E402
-from aerolume.solvers.ns2d.config import (FanSpec, HeatSourceSpec, ImmersedBody, PortSpec,  # noqa: E402
-                                          SolverConfig, ThermalConfig, WallBC)
+from aerolume.solvers.ns2d.config import (EmitterSpec, FanSpec, HeatSourceSpec, ImmersedBody,  # noqa: E402
+                                          PortSpec, SolverConfig, ThermalConfig, WallBC)
 from aerolume.solvers.ns2d.geometry import build_geometry  # noqa: E402
 from aerolume.solvers.ns2d.poisson import PoissonSolver  # noqa: E402
 
@@ -93,6 +93,16 @@ def extract(ops, geom):
         if ph.ports or ph.paint:
             for name in ("xchi_u", "xa_u", "xchi_v", "xa_v"):
                 arrays[name] = _np(getattr(ph, name))
+        if ph.n_dye:   # smoke channels with emitter groups and port smoke (physics.py:497-540)
+            meta["placed"]["n_dye"] = ph.n_dye
+            meta["placed"]["groups"] = [int(g.channel) for g in ph.groups]
+            meta["placed"]["port_dye"] = sorted(int(c) for c in ph.port_dye)
+            arrays["dye_inflow"] = _np(ph.dye_inflow)[..., 0]
+            for q, g in enumerate(ph.groups):
+                arrays[f"group{q}_w"], arrays[f"group{q}_target"] = _np(g.weight), _np(g.target)
+                arrays[f"group{q}_timing"] = _np(g.timing)
+            for c, w in ph.port_dye.items():
+                arrays[f"port_dye{c}"] = _np(w)
         if ph.nfan:
             for name in ("fan_gu", "fan_gv", "fan_phi", "fan_dir", "fan_value", "fan_width", "fan_kp", "fan_ki",
                          "fan_dpmax", "fan_isvel", "fan_isthrust"):
@@ -132,10 +142,15 @@ def _run_case(name, cfg_kw, *, dtype="float64", amp=0.1, seed=1, steps=1, paint=
     u, v, _ = core.project(u, v, ops64)
     tdt = ops.dtype
     dye = None
-    if cfg.dye:
+    dye_extra = None
+    if cfg.dye or cfg.dye_channels:
         dye = torch.rand((cfg.ny, cfg.nx), generator=g, dtype=torch.float64)
         dye[dye < 0.3] = 0.0
         dye = dye.to(tdt)
+        if cfg.dye_channels > 1:
+            dye_extra = torch.rand((cfg.dye_channels - 1, cfg.ny, cfg.nx), generator=g, dtype=torch.float64)
+            dye_extra[dye_extra < 0.5] = 0.0
+            dye_extra = dye_extra.to(tdt)
     zero = torch.zeros((), dtype=tdt)
     theta = None
     if cfg.thermal is not None:
@@ -145,11 +160,13 @@ def _run_case(name, cfg_kw, *, dtype="float64", amp=0.1, seed=1, steps=1, paint=
         ctrl = torch.zeros(ops.phys.ctrl_size, dtype=tdt)
         ctrl[:2] = (0.2 * torch.randn(2, generator=g, dtype=torch.float64)).to(tdt)   # PID memory e1, e2
     state = core.State(u.to(tdt), v.to(tdt), torch.zeros(cfg.ny, cfg.nx, dtype=tdt), dye,
-                       torch.tensor(0.37, dtype=tdt), zero.clone(), theta, None, ctrl)
+                       torch.tensor(0.37, dtype=tdt), zero.clone(), theta, dye_extra, ctrl)
     meta, arrays = extract(ops, geom)
     arrays.update({"in_u": _np(state.u), "in_v": _np(state.v), "in_t": _np(state.t)})
     if ctrl is not None:
         arrays["in_ctrl"] = _np(ctrl)
+    if dye_extra is not None:
+        arrays["in_dye_extra"] = _np(dye_extra)
     if dye is not None:
         arrays["in_dye"] = _np(dye)
     if theta is not None:
@@ -170,6 +187,8 @@ def _run_case(name, cfg_kw, *, dtype="float64", amp=0.1, seed=1, steps=1, paint=
                     arrays["out1_rep_" + key] = _np(val)
                 if st.ctrl is not None:
                     arrays["out1_ctrl"] = _np(st.ctrl)
+                if st.dye_extra is not None:
+                    arrays["out1_dye_extra"] = _np(st.dye_extra)
     meta["steps"] = steps
     if steps > 1:
         arrays.update({"outN_u": _np(st.u), "outN_v": _np(st.v), "outN_p": _np(st.p), "outN_t": _np(st.t)})
@@ -180,6 +199,8 @@ def _run_case(name, cfg_kw, *, dtype="float64", amp=0.1, seed=1, steps=1, paint=
         if st.ctrl is not None:
             arrays["outN_ctrl"] = _np(st.ctrl)
             arrays["outN_dt"] = _np(st.dt)
+        if st.dye_extra is not None:
+            arrays["outN_dye_extra"] = _np(st.dye_extra)
     store = {k: (np.asarray(x, dtype=np.float32) if dtype == "float32" and np.asarray(x).dtype == np.float64
                  else np.asarray(x)) for k, x in arrays.items()}
     np.savez_compressed(HERE / f"ns2d_{name}.npz", meta=np.array(json.dumps(meta)), **store)
@@ -285,6 +306,17 @@ def main():
     box_jet = dict(cavity, bodies=[ins], ports=[PortSpec((0.4, 0.5), direction=(1.0, 0.2), size=0.25, speed=1.0,
                                                          kind="jet", theta=0.8, name="jet")], dye=True)
     run_case("closed_jet_paint_f64", box_jet, dtype="float64", amp=0.1, seed=11, steps=3, paint=block)
+    # smoke channels: a pulsed rake on channel 0 beside the inlet comb, a line emitter on channel
+    # 1 that switches on during the run, a smoking jet on channel 2 and a vent
+    emitters = [EmitterSpec((1.0, 1.0), kind="rake", end=(1.0, 3.0), count=6, channel=0, rate=0.8, pulse_period=0.1,
+                            pulse_duty=0.5),
+                EmitterSpec((3.0, 3.2), kind="line", end=(4.5, 3.4), channel=1, rate=0.6, start=0.38),
+                EmitterSpec((5.5, 1.0), kind="disc", size=(0.3,), channel=1, rate=1.0, stop=0.4)]
+    smoke_ports = [PortSpec((0.8, 0.8), direction=(1.0, 0.4), size=0.3, speed=1.2, kind="jet", dye_channel=2),
+                   PortSpec((6.0, 3.3), direction=(0.0, 1.0), size=0.4, speed=0.5, kind="vent")]
+    smoke_case = dict(tunnel, emitters=emitters, ports=smoke_ports, dye=True)
+    run_case("tunnel_smoke_channels_f64", smoke_case, dtype="float64", amp=0.05, seed=12, steps=3)
+    run_case("tunnel_smoke_channels_f32", smoke_case, dtype="float32", amp=0.05, seed=12, steps=3)
     if not names or "poisson" in names:
         poisson_cases()
 

@@ -38,6 +38,8 @@ def _setup(name):
         ins["dye0"] = _dev(arr["in_dye"], dt)
     if "in_theta" in arr:
         ins["theta0"] = _dev(arr["in_theta"], dt)
+    if "in_dye_extra" in arr:   # smoke channels 1..
+        ins["dye_extra0"] = _dev(arr["in_dye_extra"], dt)
     if "in_ctrl" in arr:   # the controllers' memory and the previous step (0: the first)
         ins["ctrl0"] = _dev(arr["in_ctrl"], dt)
         ins["dt_prev"] = torch.zeros((), device="cuda", dtype=dt)
@@ -77,6 +79,8 @@ def test_step2d_matches_reference(name):
         assert _rel(out["coeffs"], arr["out1_coeffs"]) < TOL_COEFF[meta["dtype"]]
     if "out1_dye" in arr:
         assert _rel(out["dye"], arr["out1_dye"]) < tol
+    if "out1_dye_extra" in arr:
+        assert _rel(out["dye_extra"], arr["out1_dye_extra"]) < tol
     if "out1_theta" in arr:
         assert _rel(out["theta"], arr["out1_theta"]) < tol, _rel(out["theta"], arr["out1_theta"])
         _check_report(out, arr, meta)
@@ -92,23 +96,26 @@ def test_step2d_matches_reference(name):
 
 
 @pytest.mark.parametrize("name", [c for c in CASES_2D if c.startswith(("cylinder", "tunnel_fans", "cavity_heater",
-                                                                        "tunnel_ports", "closed_jet"))
+                                                                        "tunnel_ports", "closed_jet",
+                                                                        "tunnel_smoke"))
                                   or "heated" in c or "cold" in c])
 def test_three_steps_in_place_match_reference(name):
     meta, plan, ins, arr = _setup(name)
     u, v, t, dye, theta = ins["u0"], ins["v0"], ins["t0"], ins.get("dye0"), ins.get("theta0")
-    ctrl, dt_prev = ins.get("ctrl0"), ins.get("dt_prev")
+    ctrl, dt_prev, extra = ins.get("ctrl0"), ins.get("dt_prev"), ins.get("dye_extra0")
     out = plan.empty_fields()
     for _ in range(3):
         out["u"], out["v"] = u, v             # in-place velocity update
         if theta is not None:
             out["theta"] = theta              # and theta in place
-        res = plan.step(u, v, t, dye0=dye, theta0=theta, out=out, ctrl0=ctrl, dt_prev=dt_prev)
+        res = plan.step(u, v, t, dye0=dye, theta0=theta, out=out, ctrl0=ctrl, dt_prev=dt_prev, dye_extra0=extra)
         t = res["t"].clone()
         if ctrl is not None:
             ctrl, dt_prev = res["ctrl"].clone(), res["dt"].clone()
         if dye is not None:
             dye, res["dye"] = res["dye"], dye  # ping-pong the dye
+        if extra is not None:
+            extra, res["dye_extra"] = res["dye_extra"], extra
     torch.cuda.synchronize()
     tol = 10 * TOL[meta["dtype"]]
     for k, got in (("u", u), ("v", v), ("p", res["p"]), ("t", t)):
@@ -119,6 +126,8 @@ def test_three_steps_in_place_match_reference(name):
         assert _rel(theta, arr["outN_theta"]) < tol, _rel(theta, arr["outN_theta"])
     if ctrl is not None:
         assert _rel(ctrl, arr["outN_ctrl"]) < tol and _rel(dt_prev, arr["outN_dt"]) < tol
+    if extra is not None:
+        assert _rel(extra, arr["outN_dye_extra"]) < tol
 
 
 def _poisson_plan(nx, ny, h, periodic, dtype):

@@ -25,13 +25,13 @@ def _run(name, steps=1):
     tp = thermal2d_from_case(meta, arr)
     pl = placed2d_from_case(meta, arr)
     theta = arr.get("in_theta")
-    ctrl, dt_prev = arr.get("in_ctrl"), 0.0
+    ctrl, dt_prev, extra = arr.get("in_ctrl"), 0.0, arr.get("in_dye_extra")
     outs = []
     for _ in range(steps):
         if pl is not None:
             r = O2.step2d_placed(u, v, t, geom, ops, ps, tp=tp, pl=pl, theta0=theta, dye=dye, dt_prev=dt_prev,
-                                 ctrl=ctrl)
-            theta, ctrl, dt_prev = r.theta, r.ctrl, float(r.dt)
+                                 ctrl=ctrl, dye_extra=extra)
+            theta, ctrl, dt_prev, extra = r.theta, r.ctrl, float(r.dt), r.dye_extra
         elif tp is not None:
             r = O2.step2d_thermal(u, v, t, theta, geom, ops, ps, tp)
             theta = r.theta
@@ -56,6 +56,8 @@ def test_oracle2d_one_step_matches_reference(name):
         assert _rel(r.coeffs, arr["out1_coeffs"]) < (1e-10 if meta["dtype"] == "float64" else 1e-4)
     if "out1_dye" in arr:
         assert _rel(r.dye, arr["out1_dye"]) < tol
+    if "out1_dye_extra" in arr:
+        assert _rel(r.dye_extra, arr["out1_dye_extra"]) < tol
     if "out1_theta" in arr:
         assert _rel(r.theta, arr["out1_theta"]) < tol, _rel(r.theta, arr["out1_theta"])
     for key in [k[len("out1_rep_"):] for k in arr if k.startswith("out1_rep_")]:
@@ -67,7 +69,8 @@ def test_oracle2d_one_step_matches_reference(name):
 
 
 @pytest.mark.parametrize("name", [c for c in CASES_2D if c.startswith(("cylinder", "tunnel_fans", "cavity_heater",
-                                                                        "tunnel_ports", "closed_jet"))])
+                                                                        "tunnel_ports", "closed_jet",
+                                                                        "tunnel_smoke"))])
 def test_oracle2d_three_steps_match_reference(name):
     meta, arr, outs = _run(name, steps=3)
     tol = 10 * TOL[meta["dtype"]]
@@ -75,7 +78,7 @@ def test_oracle2d_three_steps_match_reference(name):
         tol = 1e-4
     r = outs[-1]
     for k, got in (("u", r.u), ("v", r.v), ("p", r.p), ("dye", r.dye), ("theta", getattr(r, "theta", None)),
-                   ("ctrl", getattr(r, "ctrl", None)), ("dt", r.dt)):
+                   ("ctrl", getattr(r, "ctrl", None)), ("dt", r.dt), ("dye_extra", getattr(r, "dye_extra", None))):
         if f"outN_{k}" in arr:
             assert _rel(got, arr[f"outN_{k}"]) < tol, (k, _rel(got, arr[f"outN_{k}"]))
 

@@ -32,10 +32,10 @@ def test_step_full_refuses_diagnostics_and_placed_physics():
         step_full(st._replace(theta=1), None, None)
 
 
-def test_thermal_from_physics_takes_heat_and_refuses_smoke_groups():
+def test_thermal_from_physics_takes_heat_transfer():
     """The 2D plan reads heat transfer off the reference's Physics (fans, heaters, paint, jets
-    and vents and the PID step are read by the plan itself), returns None without heat
-    transfer, and refuses smoke channels with emitters."""
+    and vents, smoke channels and the PID step are read by the plan itself) and returns None
+    without heat transfer."""
     from aerolume_b200.ns2d.plan import thermal_from_physics
     from aerolume_b200.ns2d.types import Geometry2D
     geom = Geometry2D((2, 6, 3, 9), nbody=1)
@@ -53,10 +53,8 @@ def test_thermal_from_physics_takes_heat_and_refuses_smoke_groups():
     for name, val in (("nfan", 1), ("pid", True), ("paint", True), ("heat", torch.ones(2))):
         assert thermal_from_physics(types.SimpleNamespace(**{**vars(ph), name: val}), geom) is not None
     assert thermal_from_physics(types.SimpleNamespace(**{**vars(ph), "thermal": False}), geom) is None
-    assert thermal_from_physics(types.SimpleNamespace(**{**vars(ph), "ports": True}), geom) is not None
-    for name, val in (("n_dye", 2), ("comb", True)):
-        with pytest.raises(RuntimeError):
-            thermal_from_physics(types.SimpleNamespace(**{**vars(ph), name: val}), geom)
+    for name, val in (("ports", True), ("n_dye", 2), ("comb", True)):
+        assert thermal_from_physics(types.SimpleNamespace(**{**vars(ph), name: val}), geom) is not None
 
 
 def _dev(x, dt):
@@ -184,7 +182,7 @@ def test_fast_step_phys_runs_the_placed_physics(name):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", ["tunnel_fans_pid_f64", "cavity_heater_paint_f64", "tunnel_ports_heat_f64",
-                                  "closed_jet_paint_f64"])
+                                  "closed_jet_paint_f64", "tunnel_smoke_channels_f64"])
 def test_step_full_fans_heaters_paint_pid_match_reference(name):
     """step_full with ops.phys carrying fans and the PID step, or heaters and a paint layer (the
     reference's 2D Physics attribute names): three steps chained through State.ctrl and
@@ -196,7 +194,7 @@ def test_step_full_fans_heaters_paint_pid_match_reference(name):
     dt = torch.float64
     th = thermal2d_from_case(meta, arr)
     pl = placed2d_from_case(meta, arr)
-    ph = types.SimpleNamespace(**{k: getattr(pl, k) for k in vars(pl)}, n_dye=0, comb=False, paint=pl.paint,
+    ph = types.SimpleNamespace(**{k: getattr(pl, k) for k in vars(pl)}, comb=False, paint=pl.paint,
                                thermal=th is not None)
     if th is not None:
         for k in ("kappa", "ri", "prt", "gravity", "eta_t", "theta_in", "wall_modes", "wall_values", "diff_coef"):
@@ -206,7 +204,8 @@ def test_step_full_fans_heaters_paint_pid_match_reference(name):
     ny, nx = ops.ny, ops.nx
     st = State(_dev(arr["in_u"], dt), _dev(arr["in_v"], dt), torch.zeros(ny, nx, device="cuda", dtype=dt),
                _dev(arr["in_dye"], dt) if "in_dye" in arr else None, _dev(arr["in_t"], dt),
-               torch.zeros((), device="cuda", dtype=dt), _dev(arr["in_theta"], dt) if th is not None else None, None,
+               torch.zeros((), device="cuda", dtype=dt), _dev(arr["in_theta"], dt) if th is not None else None,
+               _dev(arr["in_dye_extra"], dt) if "in_dye_extra" in arr else None,
                _dev(arr["in_ctrl"], dt) if "in_ctrl" in arr else None)
     out = {}
     new, _ = step_full(st, geom, ops, None, out=out)
@@ -217,6 +216,6 @@ def test_step_full_fans_heaters_paint_pid_match_reference(name):
     for _ in range(2):
         new, _ = step_full(new, geom, ops, None)
     torch.cuda.synchronize()
-    for k in ("u", "v", "p", "t", "dt", "theta", "ctrl", "dye"):
+    for k in ("u", "v", "p", "t", "dt", "theta", "ctrl", "dye", "dye_extra"):
         if f"outN_{k}" in arr:
             assert _rel(getattr(new, k), arr[f"outN_{k}"]) < 1e-9, k
