@@ -137,7 +137,7 @@ class Ns2dConfig(C.Structure):
         ("n_temp", C.c_int32), ("n_flux", C.c_int32), ("has_ins", C.c_int32), ("has_vol", C.c_int32),
         ("nfan", C.c_int32), ("heaters", C.c_int32), ("paint", C.c_int32), ("pid", C.c_int32),
         ("ports", C.c_int32), ("dye_channels", C.c_int32), ("n_groups", C.c_int32),
-        ("group_channel", C.c_int32 * 8),
+        ("group_channel", C.c_int32 * 8), ("wall_model", C.c_int32), ("wall_ground_speed", C.c_double),
     ]
 
 

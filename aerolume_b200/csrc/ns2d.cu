@@ -233,7 +233,22 @@ struct StageParams {
   // the combined penalisation of jets / vents and paint, (u + k xa) / (1 + k xchi) (xa NULL:
   // paint alone), and the ports' net volume flow joining the outlet balance (core.py:352-356)
   const T *xchi_u, *xa_u, *xchi_v, *xa_v, *q_net;
+  // the Werner-Wengle wall shear (bit 0 bottom, 1 top, 2 left, 3 right), the floor's speed and
+  // the constant nu when no live scalar is given
+  int wall_model;
+  T wall_ground, nu_c, h_c;
 };
+
+// core.py:510-533: the Werner-Wengle shear above the resolved one at distance y, signed like us
+template <typename T>
+__device__ __forceinline__ T wall_shear_excess(T us, T nu_over_y) {
+  const T a = us < T(0) ? -us : us;
+  const T lam = a * nu_over_y;
+  const T ww = pow((a * pow(nu_over_y, T(1.0 / 7.0))) * T(1.0 / 8.3), T(2.0 / (1.0 + 1.0 / 7.0)));
+  const T d = ww - lam > T(0) ? ww - lam : T(0);
+  const T sg = us > T(0) ? T(1) : (us < T(0) ? T(-1) : T(0));
+  return sg * d;
+}
 
 // One RK stage of the u- and v-faces of a 32 x 8 tile; NU_ONLY: only the maximum eddy
 // viscosity of the tile's cells (the first stage's dt needs it before the update); HEAT: the
@@ -376,6 +391,13 @@ __device__ __forceinline__ void stage2d_body(const StageParams<T> &P, int bx, in
       const int cc = fi - i0 + 1, cr = j - j0 + 1;  // cell fi in TXX, corner row j in TXY
       lu = lu + (((TXX[cr][cc] - TXX[cr][cc - 1]) + TXY[cr][fi - i0]) - TXY[cr - 1][fi - i0]) * P.inv_h;
     }
+    if (PLACED && P.wall_model && (j == 0 || j == ny - 1)) {   // the walls' excess shear, tau / h
+      const T nuy = (P.live_nu ? __ldg(P.live_nu) : P.nu_c) / (T(0.5) * P.h_c);
+      T f = T(0);
+      if (j == 0 && (P.wall_model & 1)) f = -wall_shear_excess<T>(row[c] - P.wall_ground, nuy) * P.inv_h;
+      if (j == ny - 1 && (P.wall_model & 2)) f = -wall_shear_excess<T>(row[c], nuy) * P.inv_h;
+      lu = lu + f;
+    }
     if (!P.periodic) {
       if (fi == 0) lu = T(0);
       if (fi == nx) lu = P.closed ? T(0) : (row[c - 1] - row[c]) * P.inv_h;
@@ -437,6 +459,13 @@ __device__ __forceinline__ void stage2d_body(const StageParams<T> &P, int bx, in
     if (P.les) {
       const int cc = i - i0 + 1, cr = fj - j0 + 1;  // cell row fj in TYY, corner row fj in TXY
       lv = lv + (((TXY[cr - 1][i - i0 + 1] - TXY[cr - 1][i - i0]) + TYY[cr][cc]) - TYY[cr - 1][cc]) * P.inv_h;
+    }
+    if (PLACED && (P.wall_model & 12) && (i == 0 || i == nx - 1)) {
+      const T nuy = (P.live_nu ? __ldg(P.live_nu) : P.nu_c) / (T(0.5) * P.h_c);
+      T f = T(0);
+      if (i == 0 && (P.wall_model & 4)) f = -wall_shear_excess<T>(row[c], nuy) * P.inv_h;
+      if (i == nx - 1 && (P.wall_model & 8)) f = -wall_shear_excess<T>(row[c], nuy) * P.inv_h;
+      lv = lv + f;
     }
     if (!P.periodic && (fj == 0 || fj == ny)) lv = T(0);
     if (PLACED && P.nfan) {
@@ -1783,7 +1812,11 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
   S.eta = T(c.eta);
   S.nbody = has_win ? c.nbody : 0;
   const dim3 grid(p->gx, p->gy), block(TX, TY);
-  const bool placed = c.nfan || c.pid || c.paint || c.heaters || c.ports || c.dye_channels;
+  const bool placed = c.nfan || c.pid || c.paint || c.heaters || c.ports || c.dye_channels || c.wall_model;
+  S.wall_model = c.wall_model;
+  S.wall_ground = T(c.wall_ground_speed);
+  S.nu_c = T(c.nu);
+  S.h_c = T(c.h);
   if (c.dye_channels > 0 && c.dye && c.dye_channels > 1 && !(f->dye_extra0 && f->dye_extra))
     return set_error(AERO_EINVAL, "smoke channels 1.. need dye_extra0 / dye_extra");
   if (rec && (!std::is_same<T, float>::value || les || thermal || c.dye || dt_mode != 0 || placed))

@@ -7,8 +7,9 @@ core.py:271-325, uploads the window masks once and owns the device workspace.  H
 transfer comes from ``thermal=`` (a :class:`~aerolume_b200.ns2d.types.Thermal2D`) or from the
 reference's ``ops.phys`` with ``geom.thermal``; fans, heaters, painted obstacles, jets and
 vents, smoke channels with emitters and smoking jets and the PID step come from ``placed=`` (a
-:class:`~aerolume_b200.ns2d.types.Placed2D`) or from ``ops.phys`` itself.  The wall model and
-body forcing raise ``RuntimeError``: there is no fallback to a CPU or plain-torch path.
+:class:`~aerolume_b200.ns2d.types.Placed2D`) or from ``ops.phys`` itself; ``ops.wall_model``
+adds the Werner-Wengle wall shear.  Body forcing raises ``RuntimeError``: there is no fallback
+to a CPU or plain-torch path.
 """
 from __future__ import annotations
 
@@ -100,8 +101,6 @@ class Ns2dPlan:
             placed = ops.phys
         if getattr(ops, "forcing", None) is not None:
             raise RuntimeError("a uniform body force (verification forcing) is not supported by the B200 step")
-        if getattr(ops, "wall_model", False):
-            raise RuntimeError("the Werner-Wengle wall model is not supported by the B200 step")
         L = _lib.lib()
         self.dtype = _torch_dtype(ops)
         self.dye = bool(dye)
@@ -143,6 +142,17 @@ class Ns2dPlan:
             cfg.window[q] = win[q] if self.has_win else 0
         cfg.nbody = self.nbody if self.has_win else 0
         cfg.dye = int(self.dye)
+        if getattr(ops, "wall_model", False):   # the Werner-Wengle shear (core.py:536-564)
+            bits = 0
+            if ops.bc_bottom in ("noslip", "moving"):
+                bits |= 1
+                if ops.bc_bottom == "moving":
+                    cfg.wall_ground_speed = float(ops.ground_speed)
+            if ops.bc_top == "noslip":
+                bits |= 2
+            if getattr(ops, "closed", False) and (ops.bc_left == "noslip" or ops.bc_right == "noslip"):
+                bits |= (4 if ops.bc_left == "noslip" else 0) | (8 if ops.bc_right == "noslip" else 0)
+            cfg.wall_model = bits
         self.thermal = thermal
         self.n_temp = self.n_flux = 0
         self._keep = []

@@ -46,6 +46,7 @@ class Ops2D:
     force_ref: float = 1.0
     moment_ref: tuple = (0.25, 0.0)
     dtype: str = "float32"
+    wall_model: bool = False     # the Werner-Wengle shear on the no-slip domain walls (core.py:505-564)
 
 
 @dataclass

@@ -500,6 +500,10 @@ typedef struct {
    * others dye_extra), emitter groups (<= AERO_MAX_DYE_GROUPS) and the channel of each */
   int32_t dye_channels, n_groups;
   int32_t group_channel[8];
+  /* the Werner-Wengle shear on the no-slip domain walls (core.py:505-564): bit 0 bottom, 1 top,
+   * 2 left, 3 right (0: off); the floor's speed when the bottom moves */
+  int32_t wall_model;
+  double wall_ground_speed;
 } AeroNs2dConfig;
 
 #define AERO_MAX_DYE_CHANNELS 4

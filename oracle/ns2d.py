@@ -211,6 +211,39 @@ def sgs_divergence2d(U, V, geom, ops):
     return fu, fv, nut.max()
 
 
+WW_A, WW_B = 8.3, 1.0 / 7.0                                        # core.py:510-511
+
+
+def wall_shear_excess2d(us, y, nu):
+    """core.py:517-533: the Werner-Wengle shear above the resolved one, signed like us."""
+    T = us.dtype.type
+    a = np.abs(us)
+    tau_lam = a * T(T(nu) / T(y))
+    tau_ww = (a * (T(T(nu) / T(y)) ** T(WW_B)) * T(1.0 / WW_A)) ** T(2.0 / (1.0 + WW_B))
+    return np.sign(us) * np.maximum(tau_ww - tau_lam, T(0.0))
+
+
+def wall_model_force2d(u, v, ops):
+    """core.py:536-564: the excess shear on the face rows next to the no-slip domain walls."""
+    T = u.dtype.type
+    y = 0.5 * ops.h
+    inv_h = T(1.0 / ops.h)
+    fu = np.zeros_like(u)
+    if ops.bc_bottom in ("noslip", "moving"):
+        us = u[:1] - T(ops.ground_speed) if ops.bc_bottom == "moving" else u[:1]
+        fu[:1] = -wall_shear_excess2d(us, y, ops.nu) * inv_h
+    if ops.bc_top == "noslip":
+        fu[-1:] = -wall_shear_excess2d(u[-1:], y, ops.nu) * inv_h
+    if not ops.closed or (ops.bc_left != "noslip" and ops.bc_right != "noslip"):
+        return fu, None
+    fv = np.zeros_like(v)
+    if ops.bc_left == "noslip":
+        fv[:, :1] = -wall_shear_excess2d(v[:, :1], y, ops.nu) * inv_h
+    if ops.bc_right == "noslip":
+        fv[:, -1:] = -wall_shear_excess2d(v[:, -1:], y, ops.nu) * inv_h
+    return fu, fv
+
+
 def momentum_rhs2d(u, v, geom, ops):
     """(Lu, Lv, nut_max) with the boundary rows / columns set (core.py:571-613)."""
     T = u.dtype.type
@@ -224,6 +257,11 @@ def momentum_rhs2d(u, v, geom, ops):
         fu, fv, nut_max = sgs_divergence2d(U, V, geom, ops)
         lu = lu + fu
         lv = lv + fv
+    if getattr(ops, "wall_model", False):
+        wu, wv = wall_model_force2d(u, v, ops)
+        lu = lu + wu
+        if wv is not None:
+            lv = lv + wv
     if ops.periodic:
         return lu, lv, nut_max
     lu = lu.copy()

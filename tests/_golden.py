@@ -98,7 +98,8 @@ def load_case2d(name):
                 turbulence=meta["turbulence"], les_c=meta["les_c"], nu=meta["nu"], eta=meta["eta"], cfl=meta["cfl"],
                 dt_fixed=meta["dt_fixed"], u_inlet=arr["u_inlet"].astype(dt),
                 dye_inlet=arr["dye_inlet"].astype(dt) if "dye_inlet" in arr else None,
-                force_ref=meta["force_ref"], moment_ref=tuple(meta["moment_ref"]), dtype=meta["dtype"])
+                force_ref=meta["force_ref"], moment_ref=tuple(meta["moment_ref"]), dtype=meta["dtype"],
+                wall_model=bool(meta.get("wall_model", False)))
     geom = Geometry2D(tuple(meta["window"]), nbody=meta["nbody"])
     if not geom.empty:
         for n in ("chi_u", "chi_v", "chi_c", "a_u", "a_v", "k_u", "k_v"):

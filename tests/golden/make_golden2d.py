@@ -58,6 +58,7 @@ def extract(ops, geom):
         "turbulence": ops.turbulence, "les_c": float(ops.les_c), "nu": float(ops.nu), "eta": float(ops.eta),
         "cfl": float(ops.cfl), "dt_fixed": ops.dt_fixed, "force_ref": float(ops.force_ref),
         "moment_ref": list(ops.moment_ref), "window": list(geom.window), "nbody": int(geom.nbody),
+        "wall_model": bool(ops.wall_model),
         "dtype": "float64" if ops.dtype == torch.float64 else "float32",
     }
     arrays = {"u_inlet": _np(ops.u_inlet)[:, 0]}
@@ -317,6 +318,14 @@ def main():
     smoke_case = dict(tunnel, emitters=emitters, ports=smoke_ports, dye=True)
     run_case("tunnel_smoke_channels_f64", smoke_case, dtype="float64", amp=0.05, seed=12, steps=3)
     run_case("tunnel_smoke_channels_f32", smoke_case, dtype="float32", amp=0.05, seed=12, steps=3)
+    # the Werner-Wengle wall shear on a coarse closed room (a moving floor, no-slip sides and top)
+    room = {"nx": 40, "ny": 24, "h": 0.1, "x0": 0.0, "y0": 0.0, "re": 20000.0,
+            "bodies": [ImmersedBody(square(1.6, 1.0, 0.25), name="block")],
+            "domain": "closed", "bc_bottom": "moving", "ground_speed": 1.0, "bc_left": "noslip", "bc_right": "noslip",
+            "bc_top": "noslip", "turbulence": "wale", "dye": False, "moment_ref": (1.6, 1.0),
+            "wall_model": "werner_wengle"}
+    run_case("closed_wall_model_f64", room, dtype="float64", amp=0.5, seed=13, steps=3)
+    run_case("closed_wall_model_f32", room, dtype="float32", amp=0.5, seed=13, steps=3)
     if not names or "poisson" in names:
         poisson_cases()
 

@@ -97,7 +97,7 @@ def test_step2d_matches_reference(name):
 
 @pytest.mark.parametrize("name", [c for c in CASES_2D if c.startswith(("cylinder", "tunnel_fans", "cavity_heater",
                                                                         "tunnel_ports", "closed_jet",
-                                                                        "tunnel_smoke"))
+                                                                        "tunnel_smoke", "closed_wall"))
                                   or "heated" in c or "cold" in c])
 def test_three_steps_in_place_match_reference(name):
     meta, plan, ins, arr = _setup(name)

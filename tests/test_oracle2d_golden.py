@@ -70,7 +70,7 @@ def test_oracle2d_one_step_matches_reference(name):
 
 @pytest.mark.parametrize("name", [c for c in CASES_2D if c.startswith(("cylinder", "tunnel_fans", "cavity_heater",
                                                                         "tunnel_ports", "closed_jet",
-                                                                        "tunnel_smoke"))])
+                                                                        "tunnel_smoke", "closed_wall"))])
 def test_oracle2d_three_steps_match_reference(name):
     meta, arr, outs = _run(name, steps=3)
     tol = 10 * TOL[meta["dtype"]]
