@@ -75,7 +75,7 @@ class Ns3dConfig(C.Structure):
         ("u_floor", C.c_double), ("pid", C.c_int32), ("pid_target", C.c_double), ("paint", C.c_int32),
         ("nfan", C.c_int32), ("fan_swirl", C.c_int32),
         ("nport", C.c_int32), ("port_source", C.c_double), ("port_leak", C.c_double), ("nheat", C.c_int32),
-        ("closure", C.c_int32),
+        ("closure", C.c_int32), ("forcing", C.c_int32), ("force", C.c_double * 3),
     ]
 
 
@@ -138,6 +138,7 @@ class Ns2dConfig(C.Structure):
         ("nfan", C.c_int32), ("heaters", C.c_int32), ("paint", C.c_int32), ("pid", C.c_int32),
         ("ports", C.c_int32), ("dye_channels", C.c_int32), ("n_groups", C.c_int32),
         ("group_channel", C.c_int32 * 8), ("wall_model", C.c_int32), ("wall_ground_speed", C.c_double),
+        ("forcing", C.c_int32), ("force", C.c_double * 2),
     ]
 
 

@@ -283,6 +283,8 @@ int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom
   S.status = status;
   S.wait_limit = p->wait_limit;
   S.wait_extra_tx = p->wait_extra_tx;
+  S.forcing = c.forcing;
+  for (int q = 0; q < 3; ++q) S.force[q] = T(c.force[q]);
   S.nu_pitch = p->pn;
   S.px = c.periodic[0];
   S.py = c.periodic[1];

@@ -237,6 +237,8 @@ struct StageParams {
   // the constant nu when no live scalar is given
   int wall_model;
   T wall_ground, nu_c, h_c;
+  int forcing;                 // the verification cases' uniform body force (core.py:597-599)
+  T force_u, force_v;
 };
 
 // core.py:510-533: the Werner-Wengle shear above the resolved one at distance y, signed like us
@@ -391,6 +393,7 @@ __device__ __forceinline__ void stage2d_body(const StageParams<T> &P, int bx, in
       const int cc = fi - i0 + 1, cr = j - j0 + 1;  // cell fi in TXX, corner row j in TXY
       lu = lu + (((TXX[cr][cc] - TXX[cr][cc - 1]) + TXY[cr][fi - i0]) - TXY[cr - 1][fi - i0]) * P.inv_h;
     }
+    if (PLACED && P.forcing) lu = lu + P.force_u;
     if (PLACED && P.wall_model && (j == 0 || j == ny - 1)) {   // the walls' excess shear, tau / h
       const T nuy = (P.live_nu ? __ldg(P.live_nu) : P.nu_c) / (T(0.5) * P.h_c);
       T f = T(0);
@@ -460,6 +463,7 @@ __device__ __forceinline__ void stage2d_body(const StageParams<T> &P, int bx, in
       const int cc = i - i0 + 1, cr = fj - j0 + 1;  // cell row fj in TYY, corner row fj in TXY
       lv = lv + (((TXY[cr - 1][i - i0 + 1] - TXY[cr - 1][i - i0]) + TYY[cr][cc]) - TYY[cr - 1][cc]) * P.inv_h;
     }
+    if (PLACED && P.forcing) lv = lv + P.force_v;
     if (PLACED && (P.wall_model & 12) && (i == 0 || i == nx - 1)) {
       const T nuy = (P.live_nu ? __ldg(P.live_nu) : P.nu_c) / (T(0.5) * P.h_c);
       T f = T(0);
@@ -1812,7 +1816,11 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
   S.eta = T(c.eta);
   S.nbody = has_win ? c.nbody : 0;
   const dim3 grid(p->gx, p->gy), block(TX, TY);
-  const bool placed = c.nfan || c.pid || c.paint || c.heaters || c.ports || c.dye_channels || c.wall_model;
+  const bool placed =
+      c.nfan || c.pid || c.paint || c.heaters || c.ports || c.dye_channels || c.wall_model || c.forcing;
+  S.forcing = c.forcing;
+  S.force_u = T(c.force[0]);
+  S.force_v = T(c.force[1]);
   S.wall_model = c.wall_model;
   S.wall_ground = T(c.wall_ground_speed);
   S.nu_c = T(c.nu);

@@ -89,6 +89,8 @@ struct StageParams {
   int use_tma;
   int *status;
   int wait_limit, wait_extra_tx;  // as in NuParams
+  int forcing;                    // the verification cases' uniform body force (core.py:565-566)
+  T force[3];
   int nu_pitch;
   int nx, ny, nz, zc;
   T h, inv_h;

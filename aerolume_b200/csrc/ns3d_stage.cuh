@@ -473,6 +473,11 @@ __global__ void __launch_bounds__(TX *TY, sizeof(T) == 4 ? 3 : 2) stage_kernel(c
           lw = lw + (((((n13r * s13r - z13_l) + n23r * s23r) - z23_l) + z33) - z33_l) * inv;
         }
       }
+      if (PLACED && P.forcing) {   // + the uniform body force, after the subgrid stress
+        lu = lu + P.force[0];
+        lv = lv + P.force[1];
+        lw = lw + P.force[2];
+      }
 
       // ================= actuator discs (physics.py:944-952): + f T (+ s amp), fan by fan
       for (int q = 0; q < (PLACED ? P.nfan : 0); ++q) {
@@ -787,7 +792,7 @@ cudaError_t launch_stage(const StageParams<T> &P, cudaStream_t s) {
       launch_stage_cfg<T, false, true, false, true>,   launch_stage_cfg<T, false, true, true, true>,
       launch_stage_cfg<T, true, false, false, true>,   launch_stage_cfg<T, true, false, true, true>,
       launch_stage_cfg<T, true, true, false, true>,    launch_stage_cfg<T, true, true, true, true>};
-  const bool placed = P.paint_u != nullptr || P.nfan > 0 || P.nport > 0 || P.nheat > 0;
+  const bool placed = P.paint_u != nullptr || P.nfan > 0 || P.nport > 0 || P.nheat > 0 || P.forcing;
   const int idx = (placed ? 8 : 0) + (P.upwind ? 4 : 0) + (P.les != AERO_LES_NONE ? 2 : 0) + (P.thermal ? 1 : 0);
   return table[idx](P, s);
 }

@@ -8,8 +8,8 @@ transfer comes from ``thermal=`` (a :class:`~aerolume_b200.ns2d.types.Thermal2D`
 reference's ``ops.phys`` with ``geom.thermal``; fans, heaters, painted obstacles, jets and
 vents, smoke channels with emitters and smoking jets and the PID step come from ``placed=`` (a
 :class:`~aerolume_b200.ns2d.types.Placed2D`) or from ``ops.phys`` itself; ``ops.wall_model``
-adds the Werner-Wengle wall shear.  Body forcing raises ``RuntimeError``: there is no fallback
-to a CPU or plain-torch path.
+adds the Werner-Wengle wall shear and ``ops.forcing`` a uniform body force.  There is no
+fallback to a CPU or plain-torch path.
 """
 from __future__ import annotations
 
@@ -99,8 +99,6 @@ class Ns2dPlan:
                 raise RuntimeError("placed physics comes either from ops.phys or from thermal= / placed=, not both")
             thermal = thermal_from_physics(ops.phys, geom)
             placed = ops.phys
-        if getattr(ops, "forcing", None) is not None:
-            raise RuntimeError("a uniform body force (verification forcing) is not supported by the B200 step")
         L = _lib.lib()
         self.dtype = _torch_dtype(ops)
         self.dye = bool(dye)
@@ -142,6 +140,9 @@ class Ns2dPlan:
             cfg.window[q] = win[q] if self.has_win else 0
         cfg.nbody = self.nbody if self.has_win else 0
         cfg.dye = int(self.dye)
+        if getattr(ops, "forcing", None) is not None:   # the verification cases' uniform body force
+            cfg.forcing = 1
+            cfg.force[0], cfg.force[1] = _f(ops.forcing[0]), _f(ops.forcing[1])
         if getattr(ops, "wall_model", False):   # the Werner-Wengle shear (core.py:536-564)
             bits = 0
             if ops.bc_bottom in ("noslip", "moving"):

@@ -47,6 +47,7 @@ class Ops2D:
     moment_ref: tuple = (0.25, 0.0)
     dtype: str = "float32"
     wall_model: bool = False     # the Werner-Wengle shear on the no-slip domain walls (core.py:505-564)
+    forcing: Any = None          # uniform body force (fx, fy) of the verification cases (core.py:102)
 
 
 @dataclass

@@ -95,8 +95,10 @@ class Ns3dPlan:
         for q in range(3):
             cfg.moment_ref[q] = float(ops.moment_ref[q])
         cfg.y0 = float(ops.y0)
-        if getattr(ops, "forcing", None) is not None:
-            raise RuntimeError("a uniform body force (verification forcing) is not supported by the B200 step")
+        if getattr(ops, "forcing", None) is not None:   # the verification cases' uniform body force
+            cfg.forcing = 1
+            for q in range(3):
+                cfg.force[q] = _f(ops.forcing[q])
         self.nbody = int(geom.nbody)
         win = tuple(int(x) for x in geom.window)
         self.has_win = not _window_empty(win) and self.nbody > 0

@@ -71,6 +71,7 @@ class Ops3D:
     span_ref: float = 1.0
     moment_ref: tuple = (0.0, 0.0, 0.0)
     dtype: str = "float32"
+    forcing: Any = None          # uniform body force (fx, fy, fz) of the verification cases (core.py:106)
 
     @property
     def periodic(self) -> bool:

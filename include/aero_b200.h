@@ -128,6 +128,10 @@ typedef struct AeroNs3dConfig {
   /* learned subgrid closure (geom closure): the eddy viscosity of an MLP's subgrid stress in
    * place of WALE where it applies, WALE elsewhere; les must be AERO_LES_WALE, dtype FP32 */
   int32_t closure;
+  /* a uniform body force added to the tendencies (the verification cases' ops.forcing,
+   * ns3d/core.py:565-566; forcing = 0: none) */
+  int32_t forcing;
+  double force[3];
 } AeroNs3dConfig;
 
 /* One actuator disc (ns3d/physics.py:831-979): its cell window, the force, swirl and
@@ -504,6 +508,10 @@ typedef struct {
    * 2 left, 3 right (0: off); the floor's speed when the bottom moves */
   int32_t wall_model;
   double wall_ground_speed;
+  /* a uniform body force added to the tendencies (the verification cases' ops.forcing,
+   * core.py:597-599; forcing = 0: none) */
+  int32_t forcing;
+  double force[2];
 } AeroNs2dConfig;
 
 #define AERO_MAX_DYE_CHANNELS 4

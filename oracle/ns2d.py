@@ -257,6 +257,9 @@ def momentum_rhs2d(u, v, geom, ops):
         fu, fv, nut_max = sgs_divergence2d(U, V, geom, ops)
         lu = lu + fu
         lv = lv + fv
+    if getattr(ops, "forcing", None) is not None:   # the verification cases' uniform body force
+        lu = lu + T(ops.forcing[0])
+        lv = lv + T(ops.forcing[1])
     if getattr(ops, "wall_model", False):
         wu, wv = wall_model_force2d(u, v, ops)
         lu = lu + wu

@@ -361,6 +361,8 @@ def momentum_rhs3d(u, v, w, geom, ops, sources=None):
     if ops.turbulence != "none":
         fu, fv, fw, nut, nut_max = sgs_divergence3d(U, V, W, geom, ops)
         lu, lv, lw = lu + fu, lv + fv, lw + fw
+    if getattr(ops, "forcing", None) is not None:   # the verification cases' uniform body force
+        lu, lv, lw = lu + T(ops.forcing[0]), lv + T(ops.forcing[1]), lw + T(ops.forcing[2])
     if sources is not None:
         lu, lv, lw = sources(lu, lv, lw)
     lu, lv, lw = boundary_tendencies(u, lu, lv, lw, ops)

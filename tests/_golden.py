@@ -22,7 +22,8 @@ def ops_from_meta(meta, arr):
                 les_c=meta["les_c"], nu_value=meta["nu_value"], eta=meta["eta"], cfl=meta["cfl"],
                 dt_fixed=meta["dt_fixed"], ghost=ghost, u_inlet=arr["u_inlet"].astype(dt),
                 ref_area=meta["ref_area"], length_ref=meta["length_ref"], span_ref=meta["span_ref"],
-                moment_ref=tuple(meta["moment_ref"]), dtype=meta["dtype"])
+                moment_ref=tuple(meta["moment_ref"]), dtype=meta["dtype"],
+                forcing=tuple(meta["forcing"]) if meta.get("forcing") else None)
     win = tuple(meta["window"])
     geom = Geometry3D(win, nbody=meta["nbody"])
     if not geom.empty:
@@ -99,7 +100,8 @@ def load_case2d(name):
                 dt_fixed=meta["dt_fixed"], u_inlet=arr["u_inlet"].astype(dt),
                 dye_inlet=arr["dye_inlet"].astype(dt) if "dye_inlet" in arr else None,
                 force_ref=meta["force_ref"], moment_ref=tuple(meta["moment_ref"]), dtype=meta["dtype"],
-                wall_model=bool(meta.get("wall_model", False)))
+                wall_model=bool(meta.get("wall_model", False)),
+                forcing=tuple(meta["forcing"]) if meta.get("forcing") else None)
     geom = Geometry2D(tuple(meta["window"]), nbody=meta["nbody"])
     if not geom.empty:
         for n in ("chi_u", "chi_v", "chi_c", "a_u", "a_v", "k_u", "k_v"):

@@ -88,6 +88,7 @@ def extract(ops, geom, phys, src):
         "ref_area": ops.ref_area, "length_ref": ops.length_ref, "span_ref": ops.span_ref,
         "moment_ref": list(ops.moment_ref), "window": list(geom.window), "nbody": int(geom.nbody),
         "dtype": "float64" if ops.dtype == torch.float64 else "float32",
+        "forcing": list(ops.forcing) if getattr(ops, "forcing", None) is not None else None,
     }
     arrays = {"u_inlet": _np(ops.u_inlet)[..., 0]}
     if not geom.empty:
@@ -145,12 +146,15 @@ def extract(ops, geom, phys, src):
     return meta, arrays
 
 
-def _run_case(name, cfg_kw, *, dtype="float64", amp=0.1, seed=1, rake=None, steps=1, strokes=()):
-    """One fixture; ``strokes`` are PaintLayer.stroke keyword sets (painted solids)."""
+def _run_case(name, cfg_kw, *, dtype="float64", amp=0.1, seed=1, rake=None, steps=1, strokes=(), forcing=None):
+    """One fixture; ``strokes`` are PaintLayer.stroke keyword sets (painted solids); ``forcing``
+    a uniform body force (the verification cases' ``ops.forcing``)."""
     base = dict(cfg_kw)
     cfg64 = SolverConfig3D(**{**base, "dtype": "float64", "device": "cpu", "perturb": False})
     cfg = SolverConfig3D(**{**base, "dtype": dtype, "device": "cpu", "perturb": False})
     ops = core.make_operators3d(cfg)
+    if forcing is not None:
+        ops.forcing = tuple(forcing)
     window = body_window3d([b.vertices_numpy() for b in cfg.bodies], ops) if cfg.bodies else (0, 0, 0, 0, 0, 0)
     geom = build_geometry3d(cfg.bodies, ops, window=window)
     phys = Physics3D(cfg, ops, geom, cfg.bodies) if cfg.has_placed_physics else None
@@ -263,6 +267,9 @@ def main():
     run_case("periodic_vreman_f64", dict(per, re=2e3, periodic=True, turbulence="vreman",
                                          thermal=ThermalConfig3D(prandtl=0.71, richardson=1.0)),
              dtype="float64", seed=3, amp=0.5)
+    # a uniform body force (the verification cases' forcing) in the periodic box
+    run_case("periodic_forced_f64", dict(per, re=500.0, periodic=True), dtype="float64", seed=14, amp=0.5,
+             forcing=(0.3, -0.1, 0.05))
 
     closed = dict(grid, nx=14, ny=10, nz=10, re=300.0, domain="closed", bc_x="noslip", bc_y="noslip",
                   bc_zmin="noslip", bc_zmax="noslip", advection="central",

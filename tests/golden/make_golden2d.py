@@ -59,6 +59,7 @@ def extract(ops, geom):
         "cfl": float(ops.cfl), "dt_fixed": ops.dt_fixed, "force_ref": float(ops.force_ref),
         "moment_ref": list(ops.moment_ref), "window": list(geom.window), "nbody": int(geom.nbody),
         "wall_model": bool(ops.wall_model),
+        "forcing": list(ops.forcing) if ops.forcing is not None else None,
         "dtype": "float64" if ops.dtype == torch.float64 else "float32",
     }
     arrays = {"u_inlet": _np(ops.u_inlet)[:, 0]}
@@ -127,11 +128,13 @@ def _paint(ops, sdf):
     phx.combine_penalisation(ops.phys)
 
 
-def _run_case(name, cfg_kw, *, dtype="float64", amp=0.1, seed=1, steps=1, paint=None):
+def _run_case(name, cfg_kw, *, dtype="float64", amp=0.1, seed=1, steps=1, paint=None, forcing=None):
     cfg64 = SolverConfig(**{**cfg_kw, "dtype": "float64", "device": "cpu", "perturb": False})
     cfg = SolverConfig(**{**cfg_kw, "dtype": dtype, "device": "cpu", "perturb": False})
     ops64 = core.make_operators(cfg64)
     ops = core.make_operators(cfg)
+    if forcing is not None:   # a uniform body force (the verification cases' ops.forcing)
+        ops.forcing = tuple(forcing)
     if paint is not None:
         _paint(ops, paint)
     geom = build_geometry(cfg.bodies, ops)
@@ -326,6 +329,9 @@ def main():
             "wall_model": "werner_wengle"}
     run_case("closed_wall_model_f64", room, dtype="float64", amp=0.5, seed=13, steps=3)
     run_case("closed_wall_model_f32", room, dtype="float32", amp=0.5, seed=13, steps=3)
+    run_case("periodic_forced_f64", {"nx": 32, "ny": 24, "h": 2.5 / 32, "x0": 0.0, "y0": 0.0, "re": 400.0,
+                                     "bodies": [spin], "periodic": True, "dye": False, "moment_ref": (1.0, 1.2)},
+             dtype="float64", amp=0.3, seed=14, steps=3, forcing=(0.4, -0.2))
     if not names or "poisson" in names:
         poisson_cases()
 
