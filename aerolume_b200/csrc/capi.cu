@@ -95,7 +95,7 @@ aero::AxisTables<T> axis_tables(const AeroNs3dPlan *p, int a, unsigned char *ws)
 
 // psi = L^{-1} f through five passes: x, y forward; z forward-solve-inverse; y, x inverse.
 // Every pass owns whole lines per block, so after the first pass the solve runs in place.
-// `fuse` (power-of-two x axes only) supplies the divergence fusion fields for the first
+// `fuse` (x axes of 2^a or 3 * 2^a cells only) supplies the divergence fusion fields for the first
 // pass and the pressure-accumulation fields for the last one.
 template <typename T>
 int poisson_passes(const AeroNs3dPlan *p, const T *f, T *psi, unsigned char *ws, cudaStream_t s,
@@ -567,7 +567,7 @@ int step_impl(const AeroNs3dPlan *p, const AeroNs3dFields *f, const AeroNs3dGeom
     // a diagnostics row needs the last stage's right-hand side as an array: that stage then
     // takes the unfused projection
     const bool want_div_sq = f->div_sq != nullptr && st == 2;
-    if (p->ax[0].method == 0 && aero::transform_pow2(nx) && c.nport == 0 && !want_div_sq) {
+    if (p->ax[0].method == 0 && aero::transform_tiled(nx) && c.nport == 0 && !want_div_sq) {
       // the first x pass forms div(u_hat) itself, the last one folds psi into p
       aero::TransformParams<T> F{};
       F.fuse_div = 1;

@@ -1,8 +1,9 @@
 // Orthonormal DCT-II / DCT-III / Hartley transforms of a tile of L = 2^LOG2L real lines of
-// length N = 2^a (8 <= N <= 2048), with every length, stride and stage constant at compile
-// time: the Stockham FFT's index arithmetic is shifts and masks, its loops unroll, and no
-// stage table is read at run time.  Used by the Poisson solve (Aerolume ns3d/poisson.py:
-// 74-90 defines the bases: DCT-II for homogeneous Neumann axes, Hartley for periodic ones).
+// length N = 2^a or 3 * 2^a (8 <= N <= 2048), with every length, stride and stage constant at
+// compile time: the Stockham FFT's index arithmetic is shifts, masks and multiplications by
+// constants, its loops unroll, and no stage table is read at run time.  Used by the Poisson
+// solve (Aerolume ns3d/poisson.py:74-90 defines the bases: DCT-II for homogeneous Neumann
+// axes, Hartley for periodic ones).
 //
 //   DCT-II   Makhoul's even/odd reordering, a length-N complex FFT carrying two real lines
 //            at once (real and imaginary parts), then X_k = s_k Re(e^{-i pi k/2N} V_k)
@@ -36,26 +37,33 @@ AERO_HD Cx<T> cmul(Cx<T> a, Cx<T> b) {
 
 constexpr int ilog2(int n) { return n <= 1 ? 0 : 1 + ilog2(n / 2); }
 
-// Stockham plan of N = 2^a: floor(a / 2) radix-4 stages, then one radix-2 stage when a is
-// odd.  Before stage s the span of the finished sub-transforms is 4^s.
+// Stockham plan of N = 2^a or 3 * 2^a: floor(a / 2) radix-4 stages, one radix-2 stage when a
+// is odd, then one radix-3 stage when 3 divides N.  Before stage s the span of the finished
+// sub-transforms is ns(s), a power of two in every stage (the radix-3 stage comes last).
+constexpr bool pow2_len(int n) { return n >= 1 && (n & (n - 1)) == 0; }
+constexpr bool tile_len(int n) { return n >= 8 && n <= 2048 && (pow2_len(n) || (n % 3 == 0 && pow2_len(n / 3) && n / 3 >= 4)); }
+
 template <int N>
 struct Pow2 {
-  static_assert(N >= 8 && N <= 2048 && (N & (N - 1)) == 0, "power-of-two lengths 8..2048");
-  static constexpr int LOG2N = ilog2(N);
-  static constexpr int NST = LOG2N / 2 + (LOG2N & 1);
-  static constexpr int radix(int s) { return s < LOG2N / 2 ? 4 : 2; }
+  static_assert(tile_len(N), "lengths 2^a or 3 * 2^a, 8..2048");
+  static constexpr bool THREE = N % 3 == 0;
+  static constexpr int LOG2P2 = ilog2(THREE ? N / 3 : N);  // log2 of the power-of-two part
+  static constexpr int N4 = LOG2P2 / 2, N2 = LOG2P2 & 1;
+  static constexpr int NST = N4 + N2 + (THREE ? 1 : 0);
+  static constexpr int radix(int s) { return s < N4 ? 4 : (s < N4 + N2 ? 2 : 3); }
+  static constexpr int ns(int s) { return s == 0 ? 1 : ns(s - 1) * radix(s - 1); }
 };
 
 // One Stockham stage over P = 2^LOG2P interleaved complex lines (element m of line p at
 // m * P + p): in -> out.
 template <typename T, int N, int LOG2P, int S, bool INV>
 AERO_HD void stockham_stage(const Cx<T> *in, Cx<T> *out, const Cx<T> *tw, int tid, int nthr) {
-  constexpr int R = Pow2<N>::radix(S), M = N / R, LNS = 2 * S, NS = 1 << LNS, STRIDE = N / (NS * R);
+  constexpr int R = Pow2<N>::radix(S), M = N / R, NS = Pow2<N>::ns(S), STRIDE = N / (NS * R);
   constexpr int P = 1 << LOG2P, ITEMS = M * P;
   const T sgn = INV ? T(1) : T(-1);
   for (int item = tid; item < ITEMS; item += nthr) {
     const int p = item & (P - 1), jj = item >> LOG2P;
-    const int k = jj & (NS - 1), g = jj >> LNS;
+    const int k = jj & (NS - 1), g = jj / NS;  // NS is a power of two
     Cx<T> v[R];
 #pragma unroll
     for (int t = 0; t < R; ++t) v[t] = in[((jj + t * M) << LOG2P) + p];
@@ -75,9 +83,18 @@ AERO_HD void stockham_stage(const Cx<T> *in, Cx<T> *out, const Cx<T> *tw, int ti
       V[2] = {a0.x - a2.x, a0.y - a2.y};
       V[1] = {a1.x + a3.x, a1.y + a3.y};
       V[3] = {a1.x - a3.x, a1.y - a3.y};
-    } else {
+    } else if constexpr (R == 2) {
       V[0] = {v[0].x + v[1].x, v[0].y + v[1].y};
       V[1] = {v[0].x - v[1].x, v[0].y - v[1].y};
+    } else {  // R == 3: X_1,2 = v0 - (v1 + v2) / 2 -+ sgn i (sqrt 3 / 2) (v1 - v2)
+      const T h3 = T(0.866025403784438646763723170752936183);
+      const Cx<T> t1 = {v[1].x + v[2].x, v[1].y + v[2].y};
+      const Cx<T> t2 = {v[0].x - T(0.5) * t1.x, v[0].y - T(0.5) * t1.y};
+      const Cx<T> d = {v[1].x - v[2].x, v[1].y - v[2].y};
+      const Cx<T> t3 = {-sgn * h3 * d.y, sgn * h3 * d.x};  // sgn * i * (sqrt3/2) * d
+      V[0] = {v[0].x + t1.x, v[0].y + t1.y};
+      V[1] = {t2.x + t3.x, t2.y + t3.y};
+      V[2] = {t2.x - t3.x, t2.y - t3.y};
     }
     const int base = g * NS * R + k;
 #pragma unroll
@@ -156,7 +173,7 @@ AERO_HD void transform_tile(T *R, Cx<T> *C0, Cx<T> *C1, const Cx<T> *tw, const A
         R[dst * LD + 2 * p] = z.x;
         R[dst * LD + 2 * p + 1] = z.y;
       } else {
-        const Cx<T> zr = Z[(((N - k) & (N - 1)) << LOG2P) + p];
+        const Cx<T> zr = Z[((k == 0 ? 0 : N - k) << LOG2P) + p];
         const T ar = T(0.5) * (z.x + zr.x), ai = T(0.5) * (z.y - zr.y);   // F_a = (Z_k + conj Z_{N-k}) / 2
         const T br = T(0.5) * (z.y + zr.y), bi = -T(0.5) * (z.x - zr.x);  // F_b = (Z_k - conj Z_{N-k}) / 2i
         T xa, xb;

@@ -1371,7 +1371,7 @@ struct alignas(16) Op {
 // the recording of one instance's step (host)
 struct Recorder {
   std::vector<Op> ops;
-  int lcap;    // log2 of the widest power-of-two transform tile
+  int lcap;    // log2 of the widest compile-time transform tile (lines)
   int tiles;   // tiles per work item of the stage and transform operations
 };
 
@@ -1473,13 +1473,18 @@ __device__ __forceinline__ void run_pow2(const TransformParams<float> &P, int n,
     case 256: pow2_transform_body<float, 256, Cap<256, LCAP>::L2>(P, bx, by, sm); break;
     case 512: pow2_transform_body<float, 512, Cap<512, LCAP>::L2>(P, bx, by, sm); break;
     case 1024: pow2_transform_body<float, 1024, Cap<1024, LCAP>::L2>(P, bx, by, sm); break;
+    case 192: pow2_transform_body<float, 192, Cap<192, LCAP>::L2>(P, bx, by, sm); break;
+    case 384: pow2_transform_body<float, 384, Cap<384, LCAP>::L2>(P, bx, by, sm); break;
+    case 768: pow2_transform_body<float, 768, Cap<768, LCAP>::L2>(P, bx, by, sm); break;
     default: pow2_transform_body<float, 2048, Cap<2048, LCAP>::L2>(P, bx, by, sm); break;
   }
 }
 
 // MINB: CTAs per SM the register allocation is capped for (2: up to 128 registers, no spills;
-// 3: up to 80, a few spills); the autotuner measures both.
-template <int LCAP, int MINB>
+// 3: up to 80, a few spills); the autotuner measures both.  LINE_ITEMS: the sweep has transform
+// passes on run-time stage tables (lengths other than 2^a and 3 * 2^a); without them that body
+// is left out, and with it the registers it needs.
+template <int LCAP, int MINB, bool LINE_ITEMS>
 __global__ void __launch_bounds__(NTHR, MINB) sweep2d_kernel(const __grid_constant__ Tables T) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   // the current operation in shared memory: the bodies then read its parameters from a space
@@ -1564,9 +1569,11 @@ __global__ void __launch_bounds__(NTHR, MINB) sweep2d_kernel(const __grid_consta
           }
           break;
         case LINE:
-          for (int t = 0, tb = bx * op.tiles; t < op.tiles && tb < op.tgx; ++t, ++tb) {
-            if (t) __syncthreads();
-            line_transform_body<float>(op.a.tr, tb, by, smem_raw);
+          if constexpr (LINE_ITEMS) {
+            for (int t = 0, tb = bx * op.tiles; t < op.tiles && tb < op.tgx; ++t, ++tb) {
+              if (t) __syncthreads();
+              line_transform_body<float>(op.a.tr, tb, by, smem_raw);
+            }
           }
           break;
         case DIV: {
@@ -1683,13 +1690,19 @@ Op new_tiled_op(int kind, long long tgx, int gy, int tiles) {
   return o;
 }
 
-// one transform pass as a sweep operation (power-of-two tiles no wider than 2^lcap lines)
+// compile-time tiles inside the persistent sweep kernel: every power of two from 8 and the 3 * 2^a
+// lengths of the sweep's grids (each further length is another inlined body competing for the
+// kernel's registers); other lengths take the run-time stage tables
+bool sweep_tiled(int n) { return aero::transform_tiled(n) && (aero::fft::pow2_len(n) || n == 192 || n == 384 || n == 768); }
+
+// one transform pass as a sweep operation (compile-time tiles of 2^a or 3 * 2^a cells no wider
+// than 2^lcap lines; run-time stage tables for other lengths)
 int record_transform(Recorder *rec, const aero::TransformParams<float> &P) {
   namespace sw = aero::ns2d::sweep;
   const int n = P.A.n;
   const size_t lines_x = (size_t)P.nz * P.ny;
   const int gy = P.axis == 0 ? 1 : (P.axis == 1 ? P.nz : P.ny);
-  if (P.A.method == 0 && aero::transform_pow2(n)) {
+  if (P.A.method == 0 && sweep_tiled(n)) {
     if (n < 64) return set_error(AERO_EUNSUPPORTED, "the persistent sweep needs transform lengths of at least 64");
     const int l2 = std::min(aero::fft::tile_log2L(n, 4), rec->lcap), L = 1 << l2;
     Op o = new_tiled_op(sw::POW2, P.axis == 0 ? (long long)((lines_x + L - 1) / L) : (P.nx + L - 1) / L, gy,
@@ -1699,7 +1712,7 @@ int record_transform(Recorder *rec, const aero::TransformParams<float> &P) {
     rec->ops.push_back(o);
     return AERO_OK;
   }
-  if (P.fuse_div || P.p_acc) return set_error(AERO_EINVAL, "fused transform passes need power-of-two axes");
+  if (P.fuse_div || P.p_acc) return set_error(AERO_EINVAL, "fused transform passes need axes of 2^a or 3 * 2^a cells");
   const int L = P.L;
   Op o = new_tiled_op(sw::LINE, P.axis == 0 ? (long long)((lines_x + L - 1) / L) : (P.nx + L - 1) / L, gy,
                       rec->tiles);
@@ -2001,7 +2014,8 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
   // ---- stages
   static const double RK[3][3] = {{0.0, 1.0, 1.0 / 6.0}, {0.75, 0.25, 2.0 / 3.0}, {1.0 / 3.0, 2.0 / 3.0, 1.0}};
   T *p_out = static_cast<T *>(f->p);
-  const bool fused = p->ax[0].method == 0 && aero::transform_pow2(nx) && !c.ports;
+  // (recorded for the persistent sweep: only the lengths its kernel tiles)
+  const bool fused = p->ax[0].method == 0 && (rec ? sweep_tiled(nx) : aero::transform_tiled(nx)) && !c.ports;
   // stage values alternate between two buffer pairs; stages 2 and 3 project the previous
   // stage's value themselves while staging it (P.psi), so only the last stage runs
   // correct2d_kernel, into the caller's u, v
@@ -2404,33 +2418,40 @@ struct AeroNs2dSweep {
   // items per instance (all but the status reset before every step), then the tables
   size_t sync_bytes = 0, off_ops = 0, off_io = 0, off_of = 0, off_pb = 0, off_pi = 0, total = 0;
   int spin_limit = 1 << 26, extra = 0;
+  bool has_line = false;  // any transform pass on run-time stage tables
 };
 
 namespace {
 
 using SweepKernel = void (*)(const aero::ns2d::sweep::Tables);
 
-// the kernel of a tuning: widest transform tile 2^lcap, registers capped for 2, 3 or 4 CTAs per SM
-SweepKernel sweep_kernel(int lcap, int cps) {
+template <int LCAP, int MINB>
+SweepKernel sweep_kernel_line(bool line) {
   namespace sw = aero::ns2d::sweep;
+  return line ? sw::sweep2d_kernel<LCAP, MINB, true> : sw::sweep2d_kernel<LCAP, MINB, false>;
+}
+
+// the kernel of a tuning: widest transform tile 2^lcap, registers capped for 2, 3 or 4 CTAs per
+// SM, with or without the run-time-table transform body
+SweepKernel sweep_kernel(int lcap, int cps, bool line) {
   if (cps >= 4) {
     switch (lcap) {
-      case 1: return sw::sweep2d_kernel<1, 4>;
-      case 2: return sw::sweep2d_kernel<2, 4>;
-      default: return sw::sweep2d_kernel<3, 4>;
+      case 1: return sweep_kernel_line<1, 4>(line);
+      case 2: return sweep_kernel_line<2, 4>(line);
+      default: return sweep_kernel_line<3, 4>(line);
     }
   }
   if (cps == 3) {
     switch (lcap) {
-      case 1: return sw::sweep2d_kernel<1, 3>;
-      case 2: return sw::sweep2d_kernel<2, 3>;
-      default: return sw::sweep2d_kernel<3, 3>;
+      case 1: return sweep_kernel_line<1, 3>(line);
+      case 2: return sweep_kernel_line<2, 3>(line);
+      default: return sweep_kernel_line<3, 3>(line);
     }
   }
   switch (lcap) {
-    case 1: return sw::sweep2d_kernel<1, 2>;
-    case 2: return sw::sweep2d_kernel<2, 2>;
-    default: return sw::sweep2d_kernel<3, 2>;
+    case 1: return sweep_kernel_line<1, 2>(line);
+    case 2: return sweep_kernel_line<2, 2>(line);
+    default: return sweep_kernel_line<3, 2>(line);
   }
 }
 
@@ -2524,7 +2545,8 @@ int aero_ns2d_sweep_create(int32_t n, const AeroNs2dPlan *const *plans, const Ae
   S->total = off;
   // co-resident CTAs: every CTA waits at the grid barriers
   int dev = 0, nsm = 0, occ = 0;
-  const SweepKernel kern = sweep_kernel(lcap, cps);
+  for (const Op &o : S->ops) S->has_line = S->has_line || o.kind == aero::ns2d::sweep::LINE;
+  const SweepKernel kern = sweep_kernel(lcap, cps, S->has_line);
   cudaError_t e = cudaGetDevice(&dev);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   if (e == cudaSuccess)
@@ -2598,7 +2620,7 @@ int aero_ns2d_sweep_step(const AeroNs2dSweep *sweep, void *workspace, void *stre
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  AERO_CUDA_TRY(cudaLaunchKernelEx(&cfg, sweep_kernel(S.lcap, S.ctas_per_sm), T));
+  AERO_CUDA_TRY(cudaLaunchKernelEx(&cfg, sweep_kernel(S.lcap, S.ctas_per_sm, S.has_line), T));
   return AERO_OK;
 }
 

@@ -263,9 +263,9 @@ template <typename T> cudaError_t launch_finalize(const FinalizeParams<T> &, cud
 template <typename T> cudaError_t launch_psi_accumulate(const T *, T *, size_t, T, int, const T *, cudaStream_t);
 template <typename T> size_t transform_smem_bytes(int, int);
 template <typename T> cudaError_t launch_transform(const TransformParams<T> &, cudaStream_t);
-// true when an axis of n cells runs the compile-time power-of-two transform (8 <= n <= 2048),
-// which also takes the divergence / pressure fusions of TransformParams
-bool transform_pow2(int n);
+// true when an axis of n cells runs the compile-time tile transform (n = 2^a or 3 * 2^a,
+// 8 <= n <= 2048), which also takes the divergence / pressure fusions of TransformParams
+bool transform_tiled(int n);
 template <typename T> cudaError_t launch_fields(const FieldsParams<T> &, cudaStream_t);
 template <typename T>
 cudaError_t launch_probe(const T *, int, int, int, const double *, double, const double *, const T *, long long, T *,

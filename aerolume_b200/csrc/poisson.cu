@@ -38,7 +38,7 @@ cudaError_t launch_pow2(const TransformParams<T> &P, cudaStream_t s) {
   return launch_pow2_tile<T, N, -1>(P, s);
 }
 
-bool transform_pow2(int n) { return n >= 8 && n <= 2048 && (n & (n - 1)) == 0; }
+bool transform_tiled(int n) { return fft::tile_len(n); }
 
 // Tables: twiddles e^{-2 pi i m / n}, DCT post-twiddles s_k e^{-i pi k / 2n}, cos / sin of
 // pi k / 2n, eigenvalues (2 cos(pi k / n) - 2) / h^2 or (2 cos(2 pi k / n) - 2) / h^2,
@@ -85,7 +85,7 @@ size_t transform_smem_bytes(int n, int L) {
 
 template <typename T>
 cudaError_t launch_transform(const TransformParams<T> &P, cudaStream_t s) {
-  if (P.A.method == 0 && transform_pow2(P.A.n)) {
+  if (P.A.method == 0 && transform_tiled(P.A.n)) {
     switch (P.A.n) {
       case 8: return launch_pow2<T, 8>(P, s);
       case 16: return launch_pow2<T, 16>(P, s);
@@ -95,10 +95,18 @@ cudaError_t launch_transform(const TransformParams<T> &P, cudaStream_t s) {
       case 256: return launch_pow2<T, 256>(P, s);
       case 512: return launch_pow2<T, 512>(P, s);
       case 1024: return launch_pow2<T, 1024>(P, s);
-      default: return launch_pow2<T, 2048>(P, s);
+      case 2048: return launch_pow2<T, 2048>(P, s);
+      case 12: return launch_pow2<T, 12>(P, s);
+      case 24: return launch_pow2<T, 24>(P, s);
+      case 48: return launch_pow2<T, 48>(P, s);
+      case 96: return launch_pow2<T, 96>(P, s);
+      case 192: return launch_pow2<T, 192>(P, s);
+      case 384: return launch_pow2<T, 384>(P, s);
+      case 768: return launch_pow2<T, 768>(P, s);
+      default: return launch_pow2<T, 1536>(P, s);
     }
   }
-  if (P.fuse_div || P.p_acc) return cudaErrorInvalidValue;  // fusions exist on power-of-two axes only
+  if (P.fuse_div || P.p_acc) return cudaErrorInvalidValue;  // fusions exist on tiled axes only
   const size_t smem = transform_smem_bytes<T>(P.A.n, P.L);
   static size_t set_to = 0;
   if (smem > set_to) {

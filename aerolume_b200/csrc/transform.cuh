@@ -16,7 +16,8 @@
 //            FFT, un-reordering
 //   DHT      H_k = (Re F_k - Im F_k) / sqrt(n) (an involution: forward = inverse)
 //
-// The FFT is a Stockham autosort with radix 4, 2 and 3 passes (n = 2^a 3^b); any other
+// The FFT is a Stockham autosort with radix 4, 2 and 3 passes (n = 2^a 3^b): compile-time
+// tiles for n = 2^a and 3 * 2^a, run-time stage tables for the other 2^a 3^b; any other
 // length falls back to the dense orthonormal matrix in shared memory.  The z pass runs
 // forward transform, division by lambda_x + lambda_y + lambda_z (zero mode dropped) and
 // inverse transform in one kernel.
@@ -282,7 +283,7 @@ __global__ void __launch_bounds__(256) line_transform_kernel(const TransformPara
 }
 
 // --------------------------------------------------------------------------------------
-// Power-of-two axes: the compile-time tile transform of fft_tile.cuh
+// Axes of 2^a or 3 * 2^a cells: the compile-time tile transform of fft_tile.cuh
 // --------------------------------------------------------------------------------------
 
 struct BlockExec {
@@ -293,10 +294,10 @@ struct BlockExec {
   }
 };
 
-// Tile of L = 2^LOG2L_ lines of N cells (LOG2L_ < 0: the widest tile within ~48 KiB).
+// Tile of L = 2^LOG2L_ lines of N cells, N = 2^a or 3 * 2^a (LOG2L_ < 0: the widest tile
+// within ~48 KiB).
 template <typename T, int N, int LOG2L_ = -1>
 struct Pow2Tile {
-  static constexpr int LOG2N = fft::ilog2(N);
   static constexpr int LOG2L = LOG2L_ >= 0 ? LOG2L_ : fft::tile_log2L(N, (int)sizeof(T)), L = 1 << LOG2L, LD = L + 1;
   static constexpr size_t TW = (size_t)N * 2 * sizeof(T);                        // twiddles
   static constexpr size_t RB = ((size_t)N * LD * sizeof(T) + 15) & ~size_t(15);  // real tile
@@ -304,14 +305,14 @@ struct Pow2Tile {
   static constexpr size_t SMEM = TW + RB + 2 * CB;
 };
 
-// One axis pass over L lines of N = 2^a cells: x lines are rows (r = k ny + j), y / z lines
+// One axis pass over L lines of N = 2^a or 3 * 2^a cells: x lines are rows (r = k ny + j), y / z lines
 // are L consecutive x at fixed k / j.  Mode 0 forward, 1 inverse, 2 forward, division by
 // lambda_x + lambda_y + lambda_z (zero mode dropped) and inverse (z axis).
 template <typename T, int N, int LOG2L_>
 __device__ __forceinline__ void pow2_transform_body(const TransformParams<T> &P, int bx, int by,
                                                     unsigned char *smem_raw) {
   using G = Pow2Tile<T, N, LOG2L_>;
-  constexpr int L = G::L, LD = G::LD, LOG2L = G::LOG2L, LOG2N = G::LOG2N;
+  constexpr int L = G::L, LD = G::LD, LOG2L = G::LOG2L;
   fft::Cx<T> *tw = reinterpret_cast<fft::Cx<T> *>(smem_raw);
   T *R = reinterpret_cast<T *>(smem_raw + G::TW);
   fft::Cx<T> *C0 = reinterpret_cast<fft::Cx<T> *>(smem_raw + G::TW + G::RB);
@@ -352,7 +353,7 @@ __device__ __forceinline__ void pow2_transform_body(const TransformParams<T> &P,
   // ---- load (coalesced along whichever index is contiguous)
   if (P.axis == 0) {
     for (int e = tid; e < N * L; e += nthr) {
-      const int m = e & (N - 1), l = e >> LOG2N;
+      const int m = e % N, l = e / N;  // constant N: shifts / multiplications
       T val = T(0);
       if (l < nl) {
         if (P.fuse_div == 2) {  // 2D: ((u_{i+1} - u_i) + v_{j+1}) - v_j (ns2d/core.py:620-622)
@@ -365,7 +366,7 @@ __device__ __forceinline__ void pow2_transform_body(const TransformParams<T> &P,
                  (P.wh[rowoff[4][l] + m] - P.wh[rowoff[3][l] + m])) *
                 P.inv_h;
         } else {
-          val = P.in[base + ((size_t)l << LOG2N) + m];
+          val = P.in[base + (size_t)l * N + m];
         }
       }
       R[m * LD + l] = val;
@@ -403,9 +404,9 @@ __device__ __forceinline__ void pow2_transform_body(const TransformParams<T> &P,
   if (P.axis == 0) {
     const T rdt = (P.p_acc && P.acc_mode == 2) ? T(1) / *P.dt : T(1);
     for (int e = tid; e < N * L; e += nthr) {
-      const int m = e & (N - 1), l = e >> LOG2N;
+      const int m = e % N, l = e / N;  // constant N: shifts / multiplications
       if (l >= nl) continue;
-      const size_t g = base + ((size_t)l << LOG2N) + m;
+      const size_t g = base + (size_t)l * N + m;
       const T psi = R[m * LD + l];
       P.out[g] = psi;
       if (P.p_acc) {  // step-averaged pressure (core.py:874-875)

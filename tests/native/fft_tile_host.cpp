@@ -2,7 +2,7 @@
 // by thread (256 "threads", one phase after another) so the tests can compare the exact
 // device code path with scipy's orthonormal DCT / Hartley transforms on the CPU.
 //
-//   fft_tile_host <f32|f64> <N> <kind 0 DCT|1 DHT> <inverse 0|1> [narrow 0|1]
+//   fft_tile_host <f32|f64> <N = 2^a or 3 * 2^a> <kind 0 DCT|1 DHT> <inverse 0|1> [narrow 0|1]
 //   stdin: N * L doubles, row m of the tile then the next (L = the tile width for N, or 2 with
 //   narrow = 1), stdout the transformed tile in the same layout.
 #include <cmath>
@@ -69,6 +69,14 @@ int dispatch(int n, int kind, int inverse, int narrow) {
     case 512: return run<T, 512>(kind, inverse, narrow);
     case 1024: return run<T, 1024>(kind, inverse, narrow);
     case 2048: return run<T, 2048>(kind, inverse, narrow);
+    case 12: return run<T, 12>(kind, inverse, narrow);
+    case 24: return run<T, 24>(kind, inverse, narrow);
+    case 48: return run<T, 48>(kind, inverse, narrow);
+    case 96: return run<T, 96>(kind, inverse, narrow);
+    case 192: return run<T, 192>(kind, inverse, narrow);
+    case 384: return run<T, 384>(kind, inverse, narrow);
+    case 768: return run<T, 768>(kind, inverse, narrow);
+    case 1536: return run<T, 1536>(kind, inverse, narrow);
   }
   return 3;
 }

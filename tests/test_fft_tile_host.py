@@ -1,6 +1,6 @@
-"""The Poisson solve's compile-time FFT tile (aerolume_b200/csrc/fft_tile.cuh) executed on
-the CPU through tests/native/fft_tile_host.cpp -- the same phases the GPU runs, thread by
-thread -- against scipy's orthonormal DCT-II / DCT-III and the discrete Hartley transform
+"""The Poisson solve's compile-time FFT tile (aerolume_b200/csrc/fft_tile.cuh; lengths 2^a and
+3 * 2^a) executed on the CPU through tests/native/fft_tile_host.cpp -- the same phases the GPU
+runs, thread by thread -- against scipy's orthonormal DCT-II / DCT-III and the discrete Hartley transform
 that Aerolume's Poisson bases define (ns3d/poisson.py:74-90)."""
 from __future__ import annotations
 
@@ -51,7 +51,7 @@ def _want(x, kind, inverse):
 
 @pytest.mark.parametrize("narrow", [False, True], ids=["wide", "two_lines"])
 @pytest.mark.parametrize("prec", ["f64", "f32"])
-@pytest.mark.parametrize("n", [8, 16, 32, 64, 128, 256, 512, 1024, 2048])
+@pytest.mark.parametrize("n", [8, 16, 32, 64, 128, 256, 512, 1024, 2048, 12, 24, 48, 96, 192, 384, 768, 1536])
 def test_tile_transform_matches_orthonormal_bases(harness, prec, n, narrow):
     rng = np.random.default_rng(n)
     x = rng.standard_normal((n, 2 if narrow else _lines(n, 8 if prec == "f64" else 4)))
