@@ -897,6 +897,17 @@ def run_sweep(args, rank, world, local_rank):
     for o, _, _ in insts:
         grids[f"{o.nx}x{o.ny}"] = grids.get(f"{o.nx}x{o.ny}", 0) + 1
     info = sw._persistent["info"]
+    ref_loop = None
+    if not args.no_ref_gpu and not args.shard:
+        try:
+            ref_ms, ref_cells = time_reference_gpu_sweep(dev)
+            ref_loop = {"ms_per_step": ref_ms, "value": ref_cells / (ref_ms * 1e-3) / 1e6, "unit": UNIT,
+                        "speedup_of_persistent": ref_ms / (ms / K),
+                        "how": "the reference's own 2D FlowSolver.advance (baseline/_ref, unmodified, its CUDA "
+                               "graphs) over the same 64 instances one after another on this GPU, 10 steps each "
+                               "after 3 warm-up steps, CUDA events; the sum of the per-instance step times"}
+        except ImportError as exc:
+            ref_loop = {"unavailable": f"reference not installed: {exc}"}
     line = {"metric": METRIC, "value": total_cells * K / (ms * 1e-3) / 1e6, "unit": UNIT, "n_gpus": world,
             "steps": K, "warmup": args.warmup, "ms_per_step": ms / K, "higher_is_better": True,
             "scaling": "strong" if args.shard else "weak",
@@ -922,6 +933,7 @@ def run_sweep(args, rank, world, local_rank):
                        "ms_per_step": timings["loop"] / K,
                        "how": "the plain per-instance loop: the same plans one after another on one stream"},
             "speedup_vs_loop": timings["loop"] / ms,
+            "reference_gpu_loop": ref_loop,
             "roofline": {"bound": "hbm", "kernel": "sweep2d_kernel (the whole sweep step)",
                          "achieved": alg / (ms / K * 1e-3) / 1e9, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                          "frac": alg / (ms / K * 1e-3) / 1e9 / peak, "traffic": None, "alg_bytes_per_step": alg},
@@ -1486,16 +1498,16 @@ def run_reference_record(args, rank):
     print(json.dumps(line), flush=True)
 
 
-def reference_2d_config(workload, device):
+def reference_2d_config(workload, device, instance=0):
     """The reference's 2D SolverConfig of a 2D bench workload: the cylinder tunnel (config [0]),
-    the same with the cylinder held at theta = 1, or the sweep's first NACA instance."""
+    the same with the cylinder held at theta = 1, or NACA instance ``instance`` of the sweep."""
     from aerolume_b200.ns2d.workloads import circle, naca4, sweep_instances
     _reference_api()                                  # baseline/_ref on the path (ImportError if absent)
     import aerolume.solvers.ns2d.config as C2
     kw = dict(bc_top="slip", bc_bottom="slip", advection="upwind3", cfl=0.5, dtype="float32", device=device,
               dye=False, perturb=False)
     if workload == "sweep2d":
-        ops, _, prm = sweep_instances(64, seed=0)[0]
+        ops, _, prm = sweep_instances(64, seed=0)[instance]
         body = C2.ImmersedBody(naca4(prm["t"], prm["m"], prm["p"], prm["alpha"]), name="naca")
         return C2.SolverConfig(nx=ops.nx, ny=ops.ny, h=8.0 / ops.nx, x0=0.0, y0=0.0, re=prm["re"], bodies=[body],
                                force_ref=1.0, moment_ref=(2.0, 2.0), **kw), f"{ops.nx}x{ops.ny}"
@@ -1506,6 +1518,32 @@ def reference_2d_config(workload, device):
         thermal = C2.ThermalConfig(prandtl=0.71, richardson=0.5)
     return C2.SolverConfig(nx=256, ny=128, h=1.0 / 32.0, x0=0.0, y0=0.0, re=200.0, bodies=[cyl], force_ref=0.5,
                            moment_ref=(2.0, 2.0), thermal=thermal, **kw), "256x128"
+
+
+def time_reference_gpu_sweep(dev, steps=10, warm=3):
+    """The reference's own 2D solver (baseline/_ref, unmodified, FlowSolver.advance with its CUDA
+    graphs) looping over the sweep's 64 instances on this GPU: each instance built, warmed up and
+    timed on its own (CUDA events around ``steps`` steps); the loop's time per sweep step is the
+    sum of the per-instance step times."""
+    import torch
+    _reference_api()
+    import aerolume.solvers.ns2d.solver as S2
+    total, cells = 0.0, 0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for k in range(64):
+        cfg, _ = reference_2d_config("sweep2d", str(dev), k)
+        s = S2.FlowSolver(cfg)
+        s.advance(warm)
+        torch.cuda.synchronize()
+        e0.record()
+        s.advance(steps)
+        e1.record()
+        torch.cuda.synchronize()
+        total += e0.elapsed_time(e1) / steps
+        cells += cfg.nx * cfg.ny
+        del s
+    torch.cuda.empty_cache()
+    return total, cells
 
 
 def time_reference_cpu_2d(workload, steps, warm, repeats=3):
