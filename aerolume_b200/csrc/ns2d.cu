@@ -2014,8 +2014,9 @@ int step2d_impl(const AeroNs2dPlan *p, const AeroNs2dFields *f, const AeroNs2dGe
   // ---- stages
   static const double RK[3][3] = {{0.0, 1.0, 1.0 / 6.0}, {0.75, 0.25, 2.0 / 3.0}, {1.0 / 3.0, 2.0 / 3.0, 1.0}};
   T *p_out = static_cast<T *>(f->p);
-  // (recorded for the persistent sweep: only the lengths its kernel tiles)
-  const bool fused = p->ax[0].method == 0 && (rec ? sweep_tiled(nx) : aero::transform_tiled(nx)) && !c.ports;
+  // the fused projection on the x lengths the persistent sweep's kernel tiles too, so that a
+  // recorded step and a direct one run the same arithmetic (the sweep matches the loop bit for bit)
+  const bool fused = p->ax[0].method == 0 && sweep_tiled(nx) && !c.ports;
   // stage values alternate between two buffer pairs; stages 2 and 3 project the previous
   // stage's value themselves while staging it (P.psi), so only the last stage runs
   // correct2d_kernel, into the caller's u, v
@@ -2434,25 +2435,9 @@ SweepKernel sweep_kernel_line(bool line) {
 // the kernel of a tuning: widest transform tile 2^lcap, registers capped for 2, 3 or 4 CTAs per
 // SM, with or without the run-time-table transform body
 SweepKernel sweep_kernel(int lcap, int cps, bool line) {
-  if (cps >= 4) {
-    switch (lcap) {
-      case 1: return sweep_kernel_line<1, 4>(line);
-      case 2: return sweep_kernel_line<2, 4>(line);
-      default: return sweep_kernel_line<3, 4>(line);
-    }
-  }
-  if (cps == 3) {
-    switch (lcap) {
-      case 1: return sweep_kernel_line<1, 3>(line);
-      case 2: return sweep_kernel_line<2, 3>(line);
-      default: return sweep_kernel_line<3, 3>(line);
-    }
-  }
-  switch (lcap) {
-    case 1: return sweep_kernel_line<1, 2>(line);
-    case 2: return sweep_kernel_line<2, 2>(line);
-    default: return sweep_kernel_line<3, 2>(line);
-  }
+  if (cps >= 4) return lcap == 2 ? sweep_kernel_line<2, 4>(line) : sweep_kernel_line<3, 4>(line);
+  if (cps == 3) return lcap == 2 ? sweep_kernel_line<2, 3>(line) : sweep_kernel_line<3, 3>(line);
+  return lcap == 2 ? sweep_kernel_line<2, 2>(line) : sweep_kernel_line<3, 2>(line);
 }
 
 size_t op_smem(const Op &o, int lcap) {
@@ -2477,9 +2462,9 @@ int aero_ns2d_sweep_create(int32_t n, const AeroNs2dPlan *const *plans, const Ae
   *sweep = nullptr;
   const int lcap = tuning ? tuning->lcap : 2, cps = tuning ? tuning->ctas_per_sm : 1, order = tuning ? tuning->order : 1;
   const int sched = tuning ? tuning->schedule : 1, tiles = tuning ? tuning->tiles : 1;
-  if (lcap < 1 || lcap > 3 || cps < 1 || cps > 4 || order < 0 || order > 1 || sched < 0 || sched > 2 || tiles < 1 ||
+  if (lcap < 2 || lcap > 3 || cps < 1 || cps > 4 || order < 0 || order > 1 || sched < 0 || sched > 2 || tiles < 1 ||
       tiles > 8)
-    return set_error(AERO_EINVAL, "tuning: lcap 1..3, ctas_per_sm 1..4, order 0..1, schedule 0..2, tiles 1..8");
+    return set_error(AERO_EINVAL, "tuning: lcap 2..3, ctas_per_sm 1..4, order 0..1, schedule 0..2, tiles 1..8");
   std::vector<std::vector<Op>> per(n);
   std::vector<long long> size(n);
   for (int k = 0; k < n; ++k) {

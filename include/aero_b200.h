@@ -608,8 +608,8 @@ int aero_ns2d_poisson_solve(const AeroNs2dPlan *plan, const void *f, void *psi, 
  * and the kernel allows) take the work items of all instances' operations, numbered phase by
  * phase (phase p: operation p of every instance).  Every instance's result is bit-identical to
  * its own aero_ns2d_step.  FP32 plans without LES, heat transfer or dye, with the CFL time step,
- * transform lengths of at least 64.  Tuning: lcap the log2 of the widest power-of-two transform
- * tile (1..3), ctas_per_sm (1..4; 3 and 4 compile the kernel for fewer registers per thread),
+ * transform lengths of at least 64.  Tuning: lcap the log2 of the widest compile-time transform
+ * tile in lines (2..3), ctas_per_sm (1..4; 3 and 4 compile the kernel for fewer registers per thread),
  * order 0 (the instances' order) or 1 (largest first), schedule 0 (a grid barrier between
  * phases), 1 (no barriers: an item waits until its own instance has finished its earlier
  * operations, items dealt round robin to the CTAs) or 2 (as 1, the CTAs taking items from a

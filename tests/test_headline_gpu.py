@@ -231,14 +231,39 @@ def test_sweep_schedules_equal_the_per_instance_loop():
         if schedule == "persistent":
             assert sw.status() == 0, tag
 
-    for cand in ((2, 2, 1, "barrier", 1), (3, 3, 0, "counters", 2), (1, 4, 1, "queue", 4)):
+    for cand in ((2, 2, 1, "barrier", 1), (3, 3, 0, "counters", 2), (2, 4, 1, "queue", 4)):
         sw.use_persistent(*cand)
         check("persistent", True, cand)
-    table = sw.tune(candidates=[(1, 2, 1, "barrier", 2), (2, 2, 1, "counters", 1), (3, 1, 0, "queue", 4)], steps=2)
+    table = sw.tune(candidates=[(3, 2, 1, "barrier", 2), (2, 2, 1, "counters", 1), (3, 1, 0, "queue", 4)], steps=2)
     assert sw.tuning is not None and any(r[1] is not None for r in table)
     check("persistent", False, sw.tuning)
     check("streams", True, "streams")
     assert all(float(s["t"]) > 0 for s in sw.states)
+
+
+def test_sweep_with_run_time_table_axes_equals_the_loop():
+    """Instances whose axes the compile-time tiles do not take (288 x 144 and 432 x 216: 9 and 27
+    divide them) beside a power-of-two one: the persistent kernel with the run-time-table
+    transform body gives every instance exactly what its own plan gives, in every schedule."""
+    import numpy as np
+    from aerolume_b200.ns2d.sweep import Sweep2D
+    from aerolume_b200.ns2d.workloads import build_geometry, make_ops, naca4
+    insts = []
+    for k, (nx, ny) in enumerate(((288, 144), (432, 216), (256, 128), (288, 144))):
+        ops = make_ops(nx, ny, 8.0 / nx, 1500.0 + 700.0 * k, force_ref=1.0, moment_ref=(2.0, 2.0), dtype="float32")
+        insts.append((ops, build_geometry([naca4(0.12, 0.02 * k, 0.4, 2.0 + 3.0 * k)], ops), {}))
+    sw = Sweep2D(insts)
+    snap = sw.snapshot()
+    ref = _run(sw, snap, "loop", 4, graph=False)
+    for cand in ((2, 3, 1, "barrier", 1), (3, 4, 0, "queue", 4), (2, 2, 1, "counters", 2)):
+        sw.use_persistent(*cand)
+        assert sw._persistent["info"]["operations"] > 0
+        got = _run(sw, snap, "persistent", 4, graph=True)
+        for k, (a, b) in enumerate(zip(got, ref)):
+            for x, y in zip(a, b):
+                assert torch.equal(x, y), (cand, k)
+        assert sw.status() == 0, cand
+    assert np.all([float(s["t"]) > 0 for s in sw.states])
 
 
 @pytest.mark.parametrize("schedule", ["barrier", "counters", "queue"])
