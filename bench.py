@@ -823,7 +823,7 @@ def run_sweep(args, rank, world, local_rank):
         import torch.distributed as dist
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    all_insts = sweep_instances(64, seed=0)
+    all_insts = sweep_instances(args.instances, seed=0)
     if args.shard:  # the 64 instances split over the ranks (strong scaling), else every rank runs all 64
         mine = shard_instances([o.nx * o.ny for o, _, _ in all_insts], world)[rank]
     else:
@@ -900,11 +900,12 @@ def run_sweep(args, rank, world, local_rank):
     ref_loop = None
     if not args.no_ref_gpu and not args.shard:
         try:
-            ref_ms, ref_cells = time_reference_gpu_sweep(dev)
+            ref_ms, ref_cells = time_reference_gpu_sweep(dev, n=args.instances)
             ref_loop = {"ms_per_step": ref_ms, "value": ref_cells / (ref_ms * 1e-3) / 1e6, "unit": UNIT,
                         "speedup_of_persistent": ref_ms / (ms / K),
                         "how": "the reference's own 2D FlowSolver.advance (baseline/_ref, unmodified, its CUDA "
-                               "graphs) over the same 64 instances one after another on this GPU, 10 steps each "
+                               f"graphs) over the same {args.instances} instances one after another on this GPU, "
+                               "10 steps each "
                                "after 3 warm-up steps, CUDA events; the sum of the per-instance step times"}
         except ImportError as exc:
             ref_loop = {"unavailable": f"reference not installed: {exc}"}
@@ -912,7 +913,8 @@ def run_sweep(args, rank, world, local_rank):
             "steps": K, "warmup": args.warmup, "ms_per_step": ms / K, "higher_is_better": True,
             "scaling": "strong" if args.shard else "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "batched sweep: 64 NACA 4-digit airfoils, seeded grids 256x128..1024x512 FP32, "
+            "config": {"workload": f"batched sweep: {args.instances} NACA 4-digit airfoils, seeded grids "
+                                   "256x128..1024x512 FP32, "
                                    "upwind3, CFL 0.5, no LES", "cells": cells, "grids": grids,
                        "inputs_vs_l2": f"{cells * 4 * 10 / 1e6:.0f} MB of state + workspace > 126 MB L2 (no flush)",
                        "parallelism": "instances sharded over the ranks" if args.shard else "replicas",
@@ -1507,7 +1509,7 @@ def reference_2d_config(workload, device, instance=0):
     kw = dict(bc_top="slip", bc_bottom="slip", advection="upwind3", cfl=0.5, dtype="float32", device=device,
               dye=False, perturb=False)
     if workload == "sweep2d":
-        ops, _, prm = sweep_instances(64, seed=0)[instance]
+        ops, _, prm = sweep_instances(max(64, instance + 1), seed=0)[instance]
         body = C2.ImmersedBody(naca4(prm["t"], prm["m"], prm["p"], prm["alpha"]), name="naca")
         return C2.SolverConfig(nx=ops.nx, ny=ops.ny, h=8.0 / ops.nx, x0=0.0, y0=0.0, re=prm["re"], bodies=[body],
                                force_ref=1.0, moment_ref=(2.0, 2.0), **kw), f"{ops.nx}x{ops.ny}"
@@ -1520,7 +1522,7 @@ def reference_2d_config(workload, device, instance=0):
                            moment_ref=(2.0, 2.0), thermal=thermal, **kw), "256x128"
 
 
-def time_reference_gpu_sweep(dev, steps=10, warm=3):
+def time_reference_gpu_sweep(dev, steps=10, warm=3, n=64):
     """The reference's own 2D solver (baseline/_ref, unmodified, FlowSolver.advance with its CUDA
     graphs) looping over the sweep's 64 instances on this GPU: each instance built, warmed up and
     timed on its own (CUDA events around ``steps`` steps); the loop's time per sweep step is the
@@ -1530,7 +1532,7 @@ def time_reference_gpu_sweep(dev, steps=10, warm=3):
     import aerolume.solvers.ns2d.solver as S2
     total, cells = 0.0, 0
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    for k in range(64):
+    for k in range(n):
         cfg, _ = reference_2d_config("sweep2d", str(dev), k)
         s = S2.FlowSolver(cfg)
         s.advance(warm)
@@ -1606,6 +1608,8 @@ def main():
     ap.add_argument("--no-ref-gpu", action="store_true", help="skip timing the reference's CUDA step")
     ap.add_argument("--tuning", default=None,
                     help="sweep2d: lcap,ctas_per_sm,order,schedule,tiles instead of the autotuner (e.g. 2,3,1,queue,4)")
+    ap.add_argument("--instances", type=int, default=64,
+                    help="sweep2d: instances of the sweep (the first n of the seeded 64; the headline uses 64)")
     ap.add_argument("--shard", action="store_true",
                     help="sweep2d with N > 1: split the 64 instances over the ranks instead of replicating them")
     args = ap.parse_args()
