@@ -1460,9 +1460,24 @@ __device__ __forceinline__ bool grid_barrier(const Tables &T) {
   return ok_s != 0;
 }
 
+// Dynamic shared memory of a compile-time transform tile of 2^l2 lines of n cells (FP32):
+// twiddles, the real tile, two complex buffers.
+constexpr size_t tile_smem(int n, int l2) {
+  return (size_t)n * 8 + ((((size_t)n * ((1u << l2) + 1) * 4) + 15) & ~size_t(15)) + (size_t)n * (1u << l2) * 8;
+}
+// Lines per transform tile of the persistent kernel: the widest tile for n, at most 2^lcap lines;
+// with lcap 2 also no more shared memory than lets 4 CTAs share an SM beside the stage body's
+// static tile (the autotuner weighs 4 CTAs with narrower tiles against 3 with wider ones).
+constexpr size_t TILE_SMEM_4CTA = 44 * 1024;
+constexpr int tile_l2(int n, int lcap) {
+  int l = fft::tile_log2L(n, 4) < lcap ? fft::tile_log2L(n, 4) : lcap;
+  while (lcap == 2 && l > 1 && tile_smem(n, l) > TILE_SMEM_4CTA) --l;
+  return l;
+}
+
 template <int N, int LCAP>
 struct Cap {
-  static constexpr int L2 = Pow2Tile<float, N>::LOG2L < LCAP ? Pow2Tile<float, N>::LOG2L : LCAP;
+  static constexpr int L2 = tile_l2(N, LCAP);
 };
 
 template <int LCAP>
@@ -1704,7 +1719,7 @@ int record_transform(Recorder *rec, const aero::TransformParams<float> &P) {
   const int gy = P.axis == 0 ? 1 : (P.axis == 1 ? P.nz : P.ny);
   if (P.A.method == 0 && sweep_tiled(n)) {
     if (n < 64) return set_error(AERO_EUNSUPPORTED, "the persistent sweep needs transform lengths of at least 64");
-    const int l2 = std::min(aero::fft::tile_log2L(n, 4), rec->lcap), L = 1 << l2;
+    const int l2 = sw::tile_l2(n, rec->lcap), L = 1 << l2;
     Op o = new_tiled_op(sw::POW2, P.axis == 0 ? (long long)((lines_x + L - 1) / L) : (P.nx + L - 1) / L, gy,
                         rec->tiles);
     o.n = n;
@@ -2443,7 +2458,7 @@ SweepKernel sweep_kernel(int lcap, int cps, bool line) {
 size_t op_smem(const Op &o, int lcap) {
   namespace sw = aero::ns2d::sweep;
   if (o.kind == sw::POW2) {
-    const int l2 = std::min(aero::fft::tile_log2L(o.n, 4), lcap), L = 1 << l2;
+    const int l2 = sw::tile_l2(o.n, lcap), L = 1 << l2;
     const size_t e = sizeof(float);
     return (size_t)o.n * 2 * e + ((((size_t)o.n * (L + 1) * e) + 15) & ~size_t(15)) + 2 * (size_t)o.n * (L / 2) * 2 * e;
   }
