@@ -2478,8 +2478,8 @@ int aero_ns2d_sweep_create(int32_t n, const AeroNs2dPlan *const *plans, const Ae
   const int lcap = tuning ? tuning->lcap : 2, cps = tuning ? tuning->ctas_per_sm : 1, order = tuning ? tuning->order : 1;
   const int sched = tuning ? tuning->schedule : 1, tiles = tuning ? tuning->tiles : 1;
   if (lcap < 2 || lcap > 3 || cps < 1 || cps > 4 || order < 0 || order > 1 || sched < 0 || sched > 2 || tiles < 1 ||
-      tiles > 8)
-    return set_error(AERO_EINVAL, "tuning: lcap 2..3, ctas_per_sm 1..4, order 0..1, schedule 0..2, tiles 1..8");
+      tiles > 16)
+    return set_error(AERO_EINVAL, "tuning: lcap 2..3, ctas_per_sm 1..4, order 0..1, schedule 0..2, tiles 1..16");
   std::vector<std::vector<Op>> per(n);
   std::vector<long long> size(n);
   for (int k = 0; k < n; ++k) {

@@ -191,7 +191,7 @@ class Sweep2D:
         sweep steps (CUDA events, after ``warmup``), keep the fastest, and put every instance's
         state back as it was.  Returns the table of (candidate, ms per step)."""
         if candidates is None:
-            candidates = list(itertools.product((2, 3), (3, 4), (0, 1), ("barrier", "queue"), (2, 4, 8)))
+            candidates = list(itertools.product((2, 3), (3, 4), (0, 1), ("barrier", "queue"), (4, 8, 16)))
         snap = self.snapshot()
         table = []
         for cand in candidates:

@@ -613,7 +613,7 @@ int aero_ns2d_poisson_solve(const AeroNs2dPlan *plan, const void *f, void *psi, 
  * order 0 (the instances' order) or 1 (largest first), schedule 0 (a grid barrier between
  * phases), 1 (no barriers: an item waits until its own instance has finished its earlier
  * operations, items dealt round robin to the CTAs) or 2 (as 1, the CTAs taking items from a
- * queue), tiles (1..8) the stage or transform tiles one work item runs. */
+ * queue), tiles (1..16) the stage or transform tiles one work item runs. */
 typedef struct AeroNs2dSweep AeroNs2dSweep;
 typedef struct {
   int32_t lcap, ctas_per_sm, order, schedule, tiles;

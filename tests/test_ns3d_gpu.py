@@ -156,7 +156,7 @@ def test_poisson_matches_reference_for_odd_shapes_and_all_bc_mixes(dtype):
 @pytest.mark.parametrize("n", [(64, 32, 32), (96, 48, 24), (128, 64, 64), (48, 40, 36), (100, 64, 64), (42, 256, 64)])
 def test_poisson_fft_sizes_solve_exactly(n):
     """L psi = f to round-off on the FFT sizes (2^a 3^b) and the dense fallback (5, 7); the last
-    two shapes give the streaming y / z passes a partly filled last tile of every row of tiles."""
+    two shapes give the y / z passes a partly filled last tile in every row of tiles."""
     from aerolume_b200.ns3d.plan import Ns3dPlan
     from aerolume_b200.ns3d.types import Geometry3D
     nx, ny, nz = n
